@@ -1,0 +1,213 @@
+"""Seeded synthetic cases for parity tests.
+
+Each case is a plain dict (the "spec") naming the grid, boundary conditions,
+physics switches and initial condition.  The same spec drives
+  * the Bolt reference run over numpy stand-ins (make_golden.py, this container only),
+  * the numpy oracle (oracle/bolt_oracle.py),
+  * the CUDA path through bolt_b200's physical_system / nonlinear_solver API.
+
+Initial conditions (evaluated at cell centres, ghost cells included):
+  n(q)  = base * (1 + amp * cos(2 pi k1 q1) * cos(2 pi k2 q2)) * (1 + noise * xi(q))
+  f     = n * prod_{d < p_dim} sqrt(m / (2 pi k T_d)) exp(-m (p_d - u_d)^2 / (2 k T_d))
+xi is N(0,1) per interior q-cell from numpy.random.default_rng(seed), extended
+periodically into the ghost cells.
+"""
+
+import copy
+import numpy as np
+
+BASE = dict(
+    q1_start=0.0, q1_end=1.0, q2_start=0.0, q2_end=1.0,
+    N_ghost=3, bc_q1='periodic', bc_q2='periodic',
+    boltzmann_constant=1.0, eps=1.0, mu=1.0,
+    recon_q='weno5', recon_p='weno5',
+    riemann_q='upwind-flux', riemann_p='upwind-flux',
+    source_enabled=True, fields_enabled=False,
+    fields_type='electrodynamic', fields_initialize='fft', fields_solver='fdtd',
+    integrator='RK2', tau=0.01,
+    init=dict(base=1.0, amp=0.0, k1=1, k2=0, noise=0.0, seed=0,
+              T=[1.0, 1.0, 1.0], u=[0.0, 0.0, 0.0]),
+)
+
+
+def make(**kw):
+    s = copy.deepcopy(BASE)
+    init = kw.pop('init', {})
+    s.update(kw)
+    s['init'].update(init)
+    return s
+
+
+CASES = {
+    # 1D1V BGK relaxation, WENO5, RK2, dt=1e-4, 100 steps
+    'c1_1d1v_weno5_rk2': make(
+        N_q1=64, N_q2=1, N_p1=128, N_p2=1, N_p3=1,
+        p1_start=[-10.0], p1_end=[10.0], p2_start=[-0.5], p2_end=[0.5],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=1,
+        tau=0.01, dt=1e-4, steps=100,
+        init=dict(amp=0.01, k1=1, k2=0)),
+    # same, RK4 (restated integrators.RK4 around df_dt_fvm), LLF
+    'c1_1d1v_weno5_rk4_llf': make(
+        N_q1=64, N_q2=1, N_p1=128, N_p2=1, N_p3=1,
+        p1_start=[-10.0], p1_end=[10.0], p2_start=[-0.5], p2_end=[0.5],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=1,
+        tau=0.01, dt=1e-4, steps=20, integrator='RK4',
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+        init=dict(amp=0.01, k1=1, k2=0)),
+    # reduced config 3: 2D3V, BGK tau=0.05, WENO5, RK4
+    'c3_2d3v_weno5_rk4_small': make(
+        N_q1=8, N_q2=8, N_p1=8, N_p2=8, N_p3=8,
+        p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0], p2_end=[6.0],
+        p3_start=[-6.0], p3_end=[6.0], mass=[1.0], charge=[0.0], p_dim=3,
+        tau=0.05, dt=1e-3, steps=3, integrator='RK4',
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+        init=dict(amp=0.05, k1=1, k2=1)),
+    # reduced config 2: 2D2V electromagnetic FDTD, collisionless, RK2 (reference scheme)
+    'c2_2d2v_fdtd_rk2_small': make(
+        N_q1=8, N_q2=8, N_p1=16, N_p2=16, N_p3=1,
+        p1_start=[-8.0], p1_end=[8.0], p2_start=[-8.0], p2_end=[8.0],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0], p_dim=2,
+        source_enabled=False, fields_enabled=True, dt=5e-4, steps=4,
+        init=dict(T=[2.0, 1.0, 1.0], noise=1e-3, seed=0)),
+    # same with RK4: fields advance once per step in stage 2
+    'c2_2d2v_fdtd_rk4_small': make(
+        N_q1=8, N_q2=8, N_p1=16, N_p2=16, N_p3=1,
+        p1_start=[-8.0], p1_end=[8.0], p2_start=[-8.0], p2_end=[8.0],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0], p_dim=2,
+        source_enabled=False, fields_enabled=True, dt=5e-4, steps=3, integrator='RK4',
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+        init=dict(T=[2.0, 1.0, 1.0], noise=1e-3, seed=0)),
+    # minmod in q and p, fields and BGK together
+    'minmod_2d2v_fields_bgk': make(
+        N_q1=8, N_q2=6, N_p1=10, N_p2=8, N_p3=1,
+        p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0], p_dim=2,
+        recon_q='minmod', recon_p='minmod', fields_enabled=True, tau=0.1,
+        dt=1e-3, steps=3, init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=3,
+                                     u=[0.3, -0.2, 0.0])),
+    # PPM in q and p
+    'ppm_2d2v_fields_bgk': make(
+        N_q1=8, N_q2=6, N_p1=10, N_p2=8, N_p3=1,
+        p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0], p_dim=2,
+        recon_q='ppm', recon_p='ppm', fields_enabled=True, tau=0.1,
+        dt=1e-3, steps=3, init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=4,
+                                     u=[0.3, -0.2, 0.0])),
+    # piecewise-constant, 2D3V with fields (exercises the p3 axis)
+    'pc_2d3v_fields': make(
+        N_q1=6, N_q2=4, N_p1=6, N_p2=6, N_p3=4,
+        p1_start=[-4.0], p1_end=[4.0], p2_start=[-4.0], p2_end=[4.0],
+        p3_start=[-4.0], p3_end=[4.0], mass=[1.0], charge=[-1.0], p_dim=3,
+        recon_q='piecewise-constant', recon_p='piecewise-constant',
+        fields_enabled=True, tau=0.2, dt=1e-3, steps=2,
+        init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=5, u=[0.2, 0.1, -0.1])),
+    # Dirichlet inflow along q1, WENO5, BGK, RK2
+    'dirichlet_1d1v_weno5': make(
+        N_q1=16, N_q2=1, N_p1=32, N_p2=1, N_p3=1,
+        p1_start=[-6.0], p1_end=[6.0], p2_start=[-0.5], p2_end=[0.5],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=1,
+        bc_q1='dirichlet', tau=0.05, dt=2e-3, steps=5,
+        dirichlet=dict(left=dict(base=1.5, T=[1.0, 1.0, 1.0], u=[0.5, 0, 0]),
+                       right=dict(base=0.5, T=[2.0, 1.0, 1.0], u=[-0.5, 0, 0])),
+        init=dict(amp=0.1, k1=1, k2=0)),
+    # Dirichlet on both q axes, 2D2V, minmod, collisionless
+    'dirichlet_2d2v_minmod': make(
+        N_q1=8, N_q2=8, N_p1=8, N_p2=8, N_p3=1,
+        p1_start=[-4.0], p1_end=[4.0], p2_start=[-4.0], p2_end=[4.0],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=2,
+        bc_q1='dirichlet', bc_q2='dirichlet', recon_q='minmod', recon_p='minmod',
+        source_enabled=False, dt=2e-3, steps=3,
+        dirichlet=dict(left=dict(base=1.2, T=[1.0, 1.0, 1.0], u=[0.3, 0.1, 0]),
+                       right=dict(base=0.8, T=[1.0, 1.0, 1.0], u=[-0.3, 0, 0]),
+                       bottom=dict(base=1.1, T=[1.0, 1.0, 1.0], u=[0.0, 0.4, 0]),
+                       top=dict(base=0.9, T=[1.0, 1.0, 1.0], u=[0.0, -0.4, 0])),
+        init=dict(amp=0.1, k1=1, k2=1)),
+    # two species with different masses, charges and p-ranges, fields + BGK
+    'two_species_2d2v_fields': make(
+        N_q1=6, N_q2=4, N_p1=8, N_p2=6, N_p3=1,
+        p1_start=[-5.0, -3.0], p1_end=[5.0, 3.0], p2_start=[-5.0, -3.0], p2_end=[5.0, 3.0],
+        p3_start=[-0.5, -0.5], p3_end=[0.5, 0.5], mass=[1.0, 4.0], charge=[-1.0, 1.0],
+        p_dim=2, fields_enabled=True, tau=0.1, dt=1e-3, steps=2,
+        init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=6, T=[1.0, 1.5, 1.0])),
+}
+
+
+# ---------------------------------------------------------------------------
+def _noise(spec, Nq1g, Nq2g):
+    ini = spec['init']
+    Ng = spec['N_ghost']
+    if not ini.get('noise'):
+        return np.zeros((Nq2g, Nq1g))
+    rng = np.random.default_rng(ini.get('seed', 0))
+    xi = rng.standard_normal((spec['N_q2'], spec['N_q1']))
+    j = (np.arange(Nq2g) - Ng) % spec['N_q2']
+    i = (np.arange(Nq1g) - Ng) % spec['N_q1']
+    return xi[j][:, i]
+
+
+def density_q(spec, q1, q2, noise_grid, ini=None):
+    ini = spec['init'] if ini is None else ini
+    n = ini.get('base', 1.0) * (1 + ini.get('amp', 0.0)
+                                * np.cos(2 * np.pi * ini.get('k1', 1) * q1)
+                                * np.cos(2 * np.pi * ini.get('k2', 0) * q2))
+    return n * (1 + ini.get('noise', 0.0) * noise_grid)
+
+
+def maxwellian_p(spec, s, p1, p2, p3, ini=None):
+    """Velocity factor of species s (array over p)."""
+    ini = spec['init'] if ini is None else ini
+    m = spec['mass'][s]
+    k = spec['boltzmann_constant']
+    T = ini.get('T', [1.0, 1.0, 1.0])
+    u = ini.get('u', [0.0, 0.0, 0.0])
+    out = 1.0
+    for d, p in enumerate((p1, p2, p3)[:spec['p_dim']]):
+        out = out * np.sqrt(m / (2 * np.pi * k * T[d])) * np.exp(-m * (p - u[d]) ** 2 / (2 * k * T[d]))
+    return out
+
+
+def _grids(spec):
+    Ng = spec['N_ghost']
+    Nq1g, Nq2g = spec['N_q1'] + 2 * Ng, spec['N_q2'] + 2 * Ng
+    dq1 = (spec['q1_end'] - spec['q1_start']) / spec['N_q1']
+    dq2 = (spec['q2_end'] - spec['q2_start']) / spec['N_q2']
+    q1 = spec['q1_start'] + (np.arange(-Ng, spec['N_q1'] + Ng) + 0.5) * dq1
+    q2 = spec['q2_start'] + (np.arange(-Ng, spec['N_q2'] + Ng) + 0.5) * dq2
+    return Nq1g, Nq2g, q1[None, :], q2[:, None]
+
+
+def _pgrid(spec, s):
+    out = []
+    for d in (1, 2, 3):
+        N = spec['N_p%d' % d]
+        a, b = spec['p%d_start' % d][s], spec['p%d_end' % d][s]
+        out.append(a + (0.5 + np.arange(N)) * ((b - a) / N))
+    p1, p2, p3 = out
+    return p1[None, None, :], p2[None, :, None], p3[:, None, None]
+
+
+def initial_f(spec, ini=None):
+    """f0 in the (Nq2g, Nq1g, Ns, Np3, Np2, Np1) layout, FP64."""
+    Nq1g, Nq2g, q1, q2 = _grids(spec)
+    ns = len(spec['mass'])
+    noise = _noise(spec, Nq1g, Nq2g)
+    n = density_q(spec, q1, q2, noise, ini)
+    f = np.empty((Nq2g, Nq1g, ns, spec['N_p3'], spec['N_p2'], spec['N_p1']))
+    for s in range(ns):
+        p1, p2, p3 = _pgrid(spec, s)
+        f[:, :, s] = n[:, :, None, None, None] * maxwellian_p(spec, s, p1, p2, p3, ini)[None, None]
+    return f
+
+
+def dirichlet_values(spec):
+    """Boundary functions f_left/right/bottom/top as full f-shaped arrays."""
+    out = {}
+    for side, ini in spec.get('dirichlet', {}).items():
+        d = dict(base=1.0, amp=0.0, k1=1, k2=0, noise=0.0)
+        d.update(ini)
+        out[side] = initial_f(spec, d)
+    return out
+
+
+def tau_value(spec):
+    return spec['tau']

@@ -1,0 +1,104 @@
+"""The oracle against fixtures produced by the unmodified Bolt source
+(tests/golden/make_golden.py) and against the analytic known-answer tests of
+Bolt's own unit tests.  CPU only."""
+
+import numpy as np
+import pytest
+
+import cases as C
+from _util import load_golden, rel, interior, moment_errors
+from oracle.bolt_oracle import Oracle, Grid, moment
+
+MOMENTS = ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy')
+
+
+@pytest.mark.parametrize('name', sorted(C.CASES))
+def test_oracle_matches_reference(name):
+    spec = C.CASES[name]
+    G = load_golden(name)
+    g = spec['N_ghost']
+    f0 = C.initial_f(spec)
+    assert rel(interior(f0, g), G['f0']) < 1e-14
+    o = Oracle(spec, f0)
+    o.dirichlet = C.dirichlet_values(spec)
+    fr = o.refresh(o.f)
+    assert rel(fr, G['f0_refreshed']) < 1e-14
+    o.dt = spec['dt']
+    at = getattr(o, 'at_n', None)
+    d = o.dfdt(fr)
+    if at is not None:
+        o.at_n = at
+    assert rel(interior(d, g), G['dfdt0']) < 1e-12
+    if spec['fields_enabled']:
+        assert rel(o.fields.cell, G['fields_cell0']) < 1e-11
+        assert rel(o.fields.yee, G['fields_yee0']) < 1e-11
+    for _ in range(spec['steps']):
+        o.step(spec['dt'])
+    assert rel(interior(o.f, g), G['f_final']) < 1e-12
+    m = {k: interior(o.moments(k), g) for k in MOMENTS}
+    errs = moment_errors(m, {k: G['mom_' + k] for k in MOMENTS})
+    assert max(errs.values()) < 1e-12, errs
+    if spec['fields_enabled']:
+        assert rel(o.fields.cell, G['fields_cell']) < 1e-11
+        assert rel(o.fields.yee, G['fields_yee']) < 1e-11
+    assert abs(o.time_elapsed - float(G['time_elapsed'])) < 1e-15
+
+
+def test_moment_kat():
+    """test_compute_moments.py:76-144: drifting Maxwellian on a 32^3 p-grid
+    over [-10,10]^3, 16^2 q-grid; mean abs error < 1e-13 for n, E, momenta."""
+    spec = C.make(N_q1=16, N_q2=16, N_p1=32, N_p2=32, N_p3=32, N_ghost=0,
+                  p1_start=[-10.0], p1_end=[10.0], p2_start=[-10.0], p2_end=[10.0],
+                  p3_start=[-10.0], p3_end=[10.0], mass=[1.0], charge=[0.0], p_dim=3)
+    gr = Grid(spec)
+    q1, q2 = gr.q1_center, gr.q2_center
+    rho = 1 + 0.01 * np.sin(2 * np.pi * q1 + 4 * np.pi * q2)
+    T = 1 + 0.01 * np.cos(2 * np.pi * q1 + 4 * np.pi * q2)
+    pb = 0.01 * np.exp(-10 * q1 ** 2 - 10 * q2 ** 2)
+    e = lambda a: a[:, :, None, None, None, None]
+    p1, p2, p3 = gr.p1c[None, None], gr.p2c[None, None], gr.p3c[None, None]
+    f = e(rho) * (1 / (2 * np.pi * e(T))) ** 1.5 * np.exp(-(p1 - e(pb)) ** 2 / (2 * e(T))) \
+        * np.exp(-(p2 - e(pb)) ** 2 / (2 * e(T))) * np.exp(-(p3 - e(pb)) ** 2 / (2 * e(T)))
+    n = moment(gr, f, 'density')[..., 0]
+    E = moment(gr, f, 'energy')[..., 0]
+    assert np.mean(np.abs(n - rho)) < 1e-13
+    assert np.mean(np.abs(E - (1.5 * rho * T + 1.5 * rho * pb ** 2))) < 1e-13
+    for name in ('mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk'):
+        assert np.mean(np.abs(moment(gr, f, name)[..., 0] - rho * pb)) < 1e-13
+
+
+def test_periodic_ghost_fill_kat():
+    """test_apply_boundary_conditions.py:131-145 / test_communicate.py:168-182:
+    periodic ghosts equal the analytic periodic function to < 5e-14."""
+    spec = C.make(N_q1=32, N_q2=16, N_p1=2, N_p2=1, N_p3=1, N_ghost=3,
+                  p1_start=[-1.0], p1_end=[1.0], p2_start=[-0.5], p2_end=[0.5],
+                  p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=1)
+    o = Oracle(spec, np.zeros(Grid(spec).fshape))
+    gr = o.g
+    expected = np.sin(2 * np.pi * gr.q1_center + 4 * np.pi * gr.q2_center)
+    f = np.zeros(gr.fshape)
+    f[3:-3, 3:-3] = expected[3:-3, 3:-3, None, None, None, None]
+    out = o.refresh(f)
+    assert np.max(np.abs(out - expected[:, :, None, None, None, None])) < 5e-14
+
+
+def test_rk_orders():
+    """test_time_integrators.py:26-70: df/dt = f integrated to t = 1, slope of
+    log(error) vs log(N) within 0.2 of -2 (RK2) and -4 (RK4), using the
+    oracle's stage formulas."""
+    def rk2(x, dt):
+        x_half = x + x * (dt / 2)
+        return x + x_half * dt
+
+    def rk4(x, dt):
+        k1 = x; k2 = x + 0.5 * k1 * dt; k3 = x + 0.5 * k2 * dt; k4 = x + k3 * dt
+        return x + ((k1 + 2 * k2 + 2 * k3 + k4) / 6) * dt
+    for fn, order, ns in ((rk2, 2, 10 ** np.arange(4)), (rk4, 4, 10 ** np.arange(3))):
+        err = []
+        for n in ns:
+            x = 1.0
+            for _ in range(n):
+                x = fn(x, 1.0 / n)
+            err.append(abs(x - np.e))
+        slope = np.polyfit(np.log10(ns), np.log10(err), 1)[0]
+        assert abs(slope + order) < 0.2
