@@ -1,0 +1,381 @@
+"""Benchmark of the FVM kinetic update on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp32|fp64] [--small]
+
+Workload (one step = one classic RK4 step over the whole phase space):
+  2D3V, N_q1 = N_q2 = 128 on [0,1]^2 periodic, N_p1 = N_p2 = N_p3 = 24 on
+  [-6,6]^3 (226,492,416 cells), f0 = Maxwellian (T = 1) with
+  n = 1 + 0.05 cos(2 pi q1) cos(2 pi q2), BGK tau = 0.05, fields off,
+  WENO5 + LLF, dt = 1e-3; f in FP32 with FP64 moments (the FP64 form is
+  measured as well).  Synthetic data; f (0.99 GB FP32) is larger than L2, so
+  no L2 flush is needed between steps.
+
+--impl reference times the FP64 C/OpenMP restatement of the same path
+(oracle/bolt_oracle_c.c) on all host cores, on a sample of the workload (the
+reference itself is Python over ArrayFire/PETSc and cannot run on the GPU box).
+
+Multi-GPU (torchrun): every rank advances an independent replica of the
+workload (no data-path collective); value = cell-updates of all ranks / the
+slowest rank's time.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+import types
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'cell-updates/s WENO5+LLF RK4: FP64 plain vs FP32/batched/adjoint; % HBM roofline'
+UNIT = 'cell-updates/s'
+HBM_FALLBACK_GBS = 6650.0
+
+
+def workload_spec(small=False):
+    n = 64 if small else 128
+    return dict(
+        N_q1=n, N_q2=n, q1_start=0.0, q1_end=1.0, q2_start=0.0, q2_end=1.0, N_ghost=3,
+        N_p1=24, N_p2=24, N_p3=24, p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0],
+        p2_end=[6.0], p3_start=[-6.0], p3_end=[6.0], mass=[1.0], charge=[0.0], p_dim=3,
+        boltzmann_constant=1.0, tau=0.05, dt=1e-3, recon_q='weno5', recon_p='weno5',
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs', source_enabled=True,
+        fields_enabled=False, fields_type='electrodynamic', fields_initialize='fft',
+        fields_solver='fdtd', integrator='RK4', bc_q1='periodic', bc_q2='periodic',
+        eps=1.0, mu=1.0, amp=0.05)
+
+
+def config_modules(spec, precision):
+    import torch
+    dom = types.ModuleType('domain')
+    for k in ('q1_start', 'q1_end', 'q2_start', 'q2_end', 'N_q1', 'N_q2', 'N_p1', 'N_p2',
+              'N_p3', 'N_ghost', 'p1_start', 'p1_end', 'p2_start', 'p2_end', 'p3_start',
+              'p3_end'):
+        setattr(dom, k, spec[k])
+    bc = types.ModuleType('boundary_conditions')
+    bc.in_q1_left = bc.in_q1_right = 'periodic'
+    bc.in_q2_bottom = bc.in_q2_top = 'periodic'
+    params = types.ModuleType('params')
+    for k, v in dict(fields_type='electrodynamic', fields_initialize='fft', fields_solver='fdtd',
+                     solver_method_in_q='FVM', solver_method_in_p='FVM',
+                     reconstruction_method_in_q='weno5', reconstruction_method_in_p='weno5',
+                     riemann_solver_in_q='lax-friedrichs', riemann_solver_in_p='lax-friedrichs',
+                     p_dim=3, num_devices=1, mass=[1.0], charge=[0.0], boltzmann_constant=1.0,
+                     fields_enabled=False, source_enabled=True, instantaneous_collisions=False,
+                     hybrid_model_enabled=False, eps=1.0, mu=1.0, p_space_grid='cartesian',
+                     time_integrator='RK4', precision=precision).items():
+        setattr(params, k, v)
+    params.tau = lambda q1, q2, p1, p2, p3: spec['tau'] * p1 ** 0 * q1 ** 0
+    ini = types.ModuleType('initialize')
+    amp = spec['amp']
+
+    def initialize_f(q1, q2, p1, p2, p3, params):
+        n = 1 + amp * torch.cos(2 * np.pi * q1) * torch.cos(2 * np.pi * q2)
+        m, k = params.mass, params.boltzmann_constant
+        T = 1.0
+        return n * (m / (2 * np.pi * k * T)) ** 1.5 * torch.exp(-m * p1 ** 2 / (2 * k * T)) \
+            * torch.exp(-m * p2 ** 2 / (2 * k * T)) * torch.exp(-m * p3 ** 2 / (2 * k * T))
+    ini.initialize_f = initialize_f
+    return dom, bc, params, ini
+
+
+def make_solver(spec, precision):
+    from bolt_b200.physical_system import physical_system
+    from bolt_b200.nonlinear_solver import nonlinear_solver
+    import bolt_b200.src.nonrelativistic_boltzmann.advection_terms as adv
+    import bolt_b200.src.nonrelativistic_boltzmann.collision_operator as col
+    import bolt_b200.src.nonrelativistic_boltzmann.moments as mom
+    dom, bc, params, ini = config_modules(spec, precision)
+    return nonlinear_solver(physical_system(dom, bc, params, ini, adv, col.BGK, mom))
+
+
+def interior_cells(spec):
+    return spec['N_q1'] * spec['N_q2'] * spec['N_p1'] * spec['N_p2'] * spec['N_p3'] * len(spec['mass'])
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+            return float(json.load(fh)['hbm_gbs']), 'measured'
+    except Exception:
+        return HBM_FALLBACK_GBS, 'fallback'
+
+
+class ClockSampler(object):
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.index),
+                 '--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+                 'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+                 'clocks_event_reasons.sw_power_cap', '--format=csv,noheader,nounits', '-lms', '100'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == 'active':
+                    reasons.add(nm)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': max(mx),
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def cpu_sample_spec(spec):
+    s = dict(spec)
+    s['N_q1'] = s['N_q2'] = 32
+    return s
+
+
+def time_cpu_reference(spec, steps, warmup, threads):
+    """FP64 C/OpenMP restatement on a 32x32 x 24^3 sample (periodic)."""
+    sys.path.insert(0, os.path.join(ROOT, 'tests', 'golden'))
+    from oracle import c_oracle
+    c_oracle.build()
+    s = cpu_sample_spec(spec)
+    Ng = s['N_ghost']
+    q1 = (np.arange(-Ng, s['N_q1'] + Ng) + 0.5) / s['N_q1']
+    q2 = (np.arange(-Ng, s['N_q2'] + Ng) + 0.5) / s['N_q2']
+    p = -6.0 + (0.5 + np.arange(24)) * 0.5
+    n = 1 + spec['amp'] * np.cos(2 * np.pi * q1)[None, :] * np.cos(2 * np.pi * q2)[:, None]
+    maxw = (2 * np.pi) ** -1.5 * np.exp(-(p[:, None, None] ** 2 + p[None, :, None] ** 2
+                                          + p[None, None, :] ** 2) / 2)
+    f = np.ascontiguousarray(n[:, :, None, None, None, None] * maxw[None, None, None])
+    for _ in range(warmup):
+        c_oracle.rk_step(f, s, s['dt'], 4, threads)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        c_oracle.rk_step(f, s, s['dt'], 4, threads)
+    el = time.perf_counter() - t0
+    cells = interior_cells(s)
+    return cells * steps / el, el / steps, s
+
+
+def run_reference(args, rank, world):
+    spec = workload_spec(args.small)
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    value, sec_per_step, s = time_cpu_reference(spec, args.steps, args.warmup, threads)
+    sample = '%dx%d x 24^3 of the workload (periodic), FP64, %d RK4 steps' % (
+        s['N_q1'], s['N_q2'], args.steps)
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT,
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': sec_per_step * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': 'Bolt FVM 2D3V 128^2 x 24^3 WENO5+LLF RK4 BGK (sampled)',
+                   'parallelism': 'cpu-openmp'},
+        'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': threads, 'kind': 'port',
+                         'sample': sample},
+        'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    spec = workload_spec(args.small)
+    cells = interior_cells(spec)
+    dt = spec['dt']
+    nls = make_solver(spec, args.precision)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        nls.strang_timestep(dt)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = nls.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        time.sleep(0.3)
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            nls.strang_timestep(dt)
+        ev1.record()
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = nls.launch_count() - launches0
+    torch.cuda.synchronize()
+    if world > 1:
+        t = torch.tensor([ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = cells * world / (ms * 1e-3)
+
+    # end-to-end through the public API with host buffers: every step copies
+    # f from pinned host memory, steps, and copies the result back
+    host_in = torch.empty_like(nls._fstore, device='cpu').pin_memory()
+    host_in.copy_(nls._fstore)
+    host_out = torch.empty_like(host_in).pin_memory()
+    in_view = host_in.permute(3, 2, 1, 0)
+    out_view = host_out.permute(3, 2, 1, 0)
+    e2e_steps = max(1, min(args.steps, 10))
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        nls.f = in_view
+        nls.strang_timestep(dt)
+        out_view.copy_(nls.f, non_blocking=True)
+    e1.record()
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    fbytes = host_in.numel() * host_in.element_size()
+    e2e = {'value': cells * world / (e2e_ms * 1e-3), 'unit': UNIT,
+           'h2d_bytes_per_step': fbytes, 'd2h_bytes_per_step': fbytes}
+
+    # FP64 plain form of the same workload (reported beside the FP32 number)
+    fp64 = None
+    if args.precision == 'fp32' and not args.no_fp64:
+        del host_in, host_out
+        nls64 = make_solver(spec, 'fp64')
+        for _ in range(args.warmup):
+            nls64.strang_timestep(dt)
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        n64 = max(1, args.steps // 2)
+        a0.record()
+        for _ in range(n64):
+            nls64.strang_timestep(dt)
+        a1.record()
+        a1.synchronize()
+        ms64 = a0.elapsed_time(a1) / n64
+        if world > 1:
+            t = torch.tensor([ms64], device='cuda')
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms64 = float(t.item())
+        fp64 = {'value': cells * world / (ms64 * 1e-3), 'ms_per_step': ms64,
+                'bytes_per_cell_update': 128}
+        del nls64
+
+    if rank != 0:
+        return
+    word = 4 if args.precision == 'fp32' else 8
+    alg_bytes_per_update = 16 * word          # RK4, accumulator form, moments fused
+    peak, peak_kind = measured_peak()
+    launches_per_step = launches / args.steps
+    qstage_per_step = 4.0
+    achieved = alg_bytes_per_update * cells / (ms * 1e-3) / 1e9
+    roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                'frac': achieved / peak, 'traffic': args.traffic,
+                'peak_kind': peak_kind, 'kernel': 'qstage_kernel (WENO5, 8x8 q-tile)',
+                'alg_bytes_per_launch': alg_bytes_per_update * cells / qstage_per_step,
+                'avg_launch_ms': ms / qstage_per_step}
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, sps, s = time_cpu_reference(spec, 2, 1, threads)
+        cpu = {'value': v, 'unit': UNIT, 'cores': threads, 'kind': 'port',
+               'sample': '%dx%d x 24^3 of the workload, FP64 C/OpenMP restatement, 2 RK4 steps'
+                         % (s['N_q1'], s['N_q2'])}
+    line = {
+        'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32' if args.precision == 'fp32' else 'f64',
+        'data': 'synthetic',
+        'config': {'workload': '2D3V %dx%d x 24^3 (%d cells) Maxwellian n=1+0.05cos(2pi q1)cos(2pi q2),'
+                               ' BGK tau=0.05, WENO5+LLF, RK4, dt=1e-3, %s f + FP64 moments'
+                               % (spec['N_q1'], spec['N_q2'], cells, args.precision.upper()),
+                   'cells': cells, 'l2': 'inputs larger than L2 (f %.2f GB), no flush'
+                                         % (nls._fstore.numel() * word / 1e9),
+                   'parallelism': 'replicas' if world > 1 else 'single'},
+        'roofline': roofline,
+        'cpu_baseline': cpu,
+        'e2e': e2e,
+        'gpu_launches': launches,
+        'launches_per_step': launches_per_step,
+        'clocks': clk.summary(),
+        'fp64_plain': fp64,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=30)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp64'])
+    ap.add_argument('--small', action='store_true', help='64x64 x 24^3 (profiling size)')
+    ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--no-fp64', action='store_true')
+    ap.add_argument('--traffic', type=float, default=None,
+                    help='ncu dram bytes per launch of the dominant kernel (recorded in roofline)')
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,73 @@
+"""Build the CUDA shared library of bolt_b200 (sm_100a) in-tree.
+
+    python -m bolt_b200.build_native          # -> bolt_b200/_native/libbolt_b200.so
+
+The FP64 kernels are compiled with -fmad=false so that their arithmetic
+follows the reference's operation order; the FP32 kernels use FMA and
+approximate division.  The library links the CUDA runtime statically and
+loads cuTensorMapEncodeTiled through the runtime's driver entry point.
+"""
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, 'csrc')
+OUT_DIR = os.path.join(HERE, '_native')
+LIB = os.path.join(OUT_DIR, 'libbolt_b200.so')
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+COMMON = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr',
+          '-I', os.path.join(HERE, '..', 'include')]
+UNITS = [
+    ('kernels_f64.cu', ['-fmad=false']),
+    ('kernels_f32.cu', ['-prec-div=false', '-prec-sqrt=false', '-ftz=true']),
+    ('bolt_capi.cu', []),
+]
+
+
+def nvcc():
+    exe = shutil.which('nvcc') or '/usr/local/cuda/bin/nvcc'
+    if not os.path.exists(exe):
+        raise RuntimeError('nvcc not found')
+    return exe
+
+
+def sources():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+            if f.endswith(('.cu', '.cuh', '.h'))] + \
+        [os.path.join(HERE, '..', 'include', 'bolt_b200.h')]
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(s) <= t for s in sources())
+
+
+def build(force=False, verbose=False, ptxas_v=False):
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(OUT_DIR, exist_ok=True)
+    objs = []
+    for src, extra in UNITS:
+        obj = os.path.join(OUT_DIR, src.replace('.cu', '.o'))
+        cmd = [nvcc()] + ARCH + COMMON + extra + ['-c', os.path.join(CSRC, src), '-o', obj]
+        if ptxas_v:
+            cmd += ['-Xptxas', '-v']
+        if verbose:
+            print(' '.join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    cmd = [nvcc()] + ARCH + ['-shared', '-o', LIB] + objs
+    subprocess.run(cmd, check=True)
+    for o in objs:
+        os.remove(o)
+    return LIB
+
+
+if __name__ == '__main__':
+    build(force='--force' in sys.argv, verbose=True, ptxas_v='--ptxas-v' in sys.argv)
+    print(LIB)

@@ -1,0 +1,675 @@
+// bolt_capi.cu - C ABI of the B200 FVM kinetic update (see include/bolt_b200.h).
+//
+// Host-side orchestration: context (scratch buffers, moment partial sums,
+// fields), TMA descriptors, and the stage sequences of the RK2 midpoint
+// stepper of fvm_operator.py:6-35 and of classic RK4 (integrators.py:15-28)
+// around the fused stage kernels.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "../../include/bolt_b200.h"
+#include "launch.h"
+
+using namespace bolt;
+
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+struct TmapEntry {
+    const void* ptr;
+    CUtensorMap map;
+};
+
+}  // namespace
+
+struct BoltCtx {
+    BoltGrid g;
+    BoltParams p;
+    SpeciesGrid sg;
+    int Nq1g, Nq2g, Np;
+    size_t elem;
+    size_t fcount;          // elements of one ghosted f
+    int tiling, recon_q, recon_p;
+    int bgk, bgk_direct, ntab;
+    int ntiles1, ntiles2, nsplit, chunks_per_split;
+    int use_tma_ok;
+    // scratch
+    void* buf[3];
+    void* kbuf;
+    double* momP[2];        // partial moments [nsplit][5][Ns][Nq2][Nq1]
+    double* jpart;          // partial currents [nsplit][3][Ns][Nq2][Nq1]
+    int cur_mom;            // index of momP holding moments of the current f
+    int cur_nsplit;         // nsplit of that buffer
+    const void* mom_owner;  // f pointer whose moments momP[cur_mom] holds (null: stale)
+    const void* ghost_owner;
+    // fields
+    double *cell, *yee, *ebefore, *J;
+    int at_n;
+    // misc
+    const void* tau_arr;
+    const void* dirichlet[4];
+    int* hflag;             // pinned, mapped
+    int* dflag;
+    int* derr;
+    int sticky;
+    long long launches;
+    size_t scratch_bytes;
+    TmapEntry tmaps[4];
+    int ntmaps;
+};
+
+#define CK(x)                                             \
+    do {                                                  \
+        cudaError_t e_ = (x);                             \
+        if (e_ != cudaSuccess) {                          \
+            ctx->sticky = ctx->sticky ? ctx->sticky : BOLT_ERR_CUDA; \
+            return BOLT_ERR_CUDA;                         \
+        }                                                 \
+    } while (0)
+
+static int dev_alloc(BoltCtx* ctx, void** p, size_t bytes) {
+    if (bytes == 0) {
+        *p = nullptr;
+        return BOLT_OK;
+    }
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+        *p = nullptr;
+        return BOLT_ERR_NOMEM;
+    }
+    ctx->scratch_bytes += bytes;
+    return BOLT_OK;
+}
+
+static const CUtensorMap* get_tmap(BoltCtx* ctx, const void* ptr) {
+    for (int i = 0; i < ctx->ntmaps; ++i)
+        if (ctx->tmaps[i].ptr == ptr) return &ctx->tmaps[i].map;
+    EncodeTiledFn enc = get_encode_fn();
+    if (!enc) return nullptr;
+    TileShape t = tile_shape(ctx->tiling);
+    cuuint64_t dims[3] = {(cuuint64_t)ctx->g.N_s * ctx->Np, (cuuint64_t)ctx->Nq1g,
+                          (cuuint64_t)ctx->Nq2g};
+    cuuint64_t strides[2] = {(cuuint64_t)ctx->g.N_s * ctx->Np * ctx->elem,
+                             (cuuint64_t)ctx->g.N_s * ctx->Np * ctx->elem * ctx->Nq1g};
+    cuuint32_t box[3] = {(cuuint32_t)PW, (cuuint32_t)(t.tq1 + 2 * HALO),
+                         (cuuint32_t)(t.q2 ? t.tq2 + 2 * HALO : 1)};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUtensorMap m;
+    CUresult r = enc(&m, ctx->elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                        : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                     3, const_cast<void*>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return nullptr;
+    int slot = ctx->ntmaps < 4 ? ctx->ntmaps++ : 0;
+    ctx->tmaps[slot].ptr = ptr;
+    ctx->tmaps[slot].map = m;
+    return &ctx->tmaps[slot].map;
+}
+
+extern "C" {
+
+const char* bolt_strerror(int code) {
+    switch (code) {
+        case BOLT_OK: return "ok";
+        case BOLT_ERR_ARG: return "invalid argument";
+        case BOLT_ERR_CUDA: return "CUDA error";
+        case BOLT_ERR_NONFINITE: return "Solver Diverging!";
+        case BOLT_ERR_TIMEOUT: return "device wait timed out";
+        case BOLT_ERR_UNSUPPORTED: return "unsupported configuration";
+        case BOLT_ERR_NOMEM: return "out of device memory";
+        default: return "unknown error";
+    }
+}
+
+int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** out) {
+    if (!grid || !params || !out) return BOLT_ERR_ARG;
+    *out = nullptr;
+    const BoltGrid& g = *grid;
+    const BoltParams& p = *params;
+    if (g.N_q1 < 1 || g.N_q2 < 1 || g.N_p1 < 1 || g.N_p2 < 1 || g.N_p3 < 1 || g.N_ghost < 0 ||
+        g.N_s < 1 || g.N_s > BOLT_MAX_SPECIES)
+        return BOLT_ERR_ARG;
+    if (p.dtype != BOLT_F64 && p.dtype != BOLT_F32) return BOLT_ERR_ARG;
+    if (p.recon_q < 0 || p.recon_q > 3 || p.recon_p < 0 || p.recon_p > 3) return BOLT_ERR_ARG;
+    if (p.integrator != BOLT_RK2 && p.integrator != BOLT_RK4) return BOLT_ERR_ARG;
+    if (p.p_dim < 1 || p.p_dim > 3) return BOLT_ERR_ARG;
+    if ((p.bc_q1 != BOLT_BC_PERIODIC && p.bc_q1 != BOLT_BC_DIRICHLET) ||
+        (p.bc_q2 != BOLT_BC_PERIODIC && p.bc_q2 != BOLT_BC_DIRICHLET))
+        return BOLT_ERR_ARG;
+    if (p.fields_enabled && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
+        return BOLT_ERR_UNSUPPORTED;
+    if (g.N_ghost == 0 && (p.bc_q1 == BOLT_BC_DIRICHLET || p.bc_q2 == BOLT_BC_DIRICHLET))
+        return BOLT_ERR_UNSUPPORTED;
+
+    BoltCtx* ctx = new (std::nothrow) BoltCtx;
+    if (!ctx) return BOLT_ERR_NOMEM;
+    memset(ctx, 0, sizeof(BoltCtx));
+    ctx->g = g;
+    ctx->p = p;
+    ctx->Nq1g = g.N_q1 + 2 * g.N_ghost;
+    ctx->Nq2g = g.N_q2 + 2 * g.N_ghost;
+    ctx->Np = g.N_p1 * g.N_p2 * g.N_p3;
+    ctx->elem = p.dtype == BOLT_F64 ? 8 : 4;
+    ctx->fcount = (size_t)ctx->Nq1g * ctx->Nq2g * g.N_s * ctx->Np;
+    for (int s = 0; s < g.N_s; ++s) {
+        ctx->sg.p1_start[s] = g.p1_start[s];
+        ctx->sg.p2_start[s] = g.p2_start[s];
+        ctx->sg.p3_start[s] = g.p3_start[s];
+        ctx->sg.dp1[s] = g.dp1[s];
+        ctx->sg.dp2[s] = g.dp2[s];
+        ctx->sg.dp3[s] = g.dp3[s];
+        ctx->sg.mass[s] = p.mass[s];
+        ctx->sg.charge[s] = p.charge[s];
+    }
+    // q-tiling: the q2 stencil is skipped only when it contributes exactly
+    // zero (one periodic q2 cell: identical neighbours give identical faces)
+    // and no current along q2 is needed
+    const bool q2_needed = g.N_q2 > 1 || p.bc_q2 != BOLT_BC_PERIODIC || p.fields_enabled;
+    if (g.N_q2 == 1)
+        ctx->tiling = q2_needed ? TILING_1D_Q2 : TILING_1D;
+    else
+        ctx->tiling = TILING_2D;
+    TileShape t = tile_shape(ctx->tiling);
+    ctx->ntiles1 = (g.N_q1 + t.tq1 - 1) / t.tq1;
+    ctx->ntiles2 = (g.N_q2 + t.tq2 - 1) / t.tq2;
+    ctx->recon_q = p.recon_q;
+    ctx->recon_p = p.recon_p;
+    ctx->bgk = p.source_enabled ? 1 : 0;
+    ctx->ntab = g.N_p1 + g.N_p2 + g.N_p3;
+    ctx->bgk_direct = (p.p_dim == 1 ||
+                       (size_t)t.tq1 * t.tq2 * ctx->ntab * sizeof(double) > 64 * 1024) ? 1 : 0;
+    // p-splits: enough CTAs for several waves on 148 SMs
+    const int nchunks = (ctx->Np + PW - 1) / PW;
+    const long long base_ctas = (long long)ctx->ntiles1 * ctx->ntiles2 * g.N_s;
+    long long want = (148LL * 8 + base_ctas - 1) / base_ctas;
+    if (want < 1) want = 1;
+    if (want > nchunks) want = nchunks;
+    ctx->chunks_per_split = (int)((nchunks + want - 1) / want);
+    ctx->nsplit = (nchunks + ctx->chunks_per_split - 1) / ctx->chunks_per_split;
+    const size_t rowbytes = (size_t)g.N_s * ctx->Np * ctx->elem;
+    ctx->use_tma_ok = (g.N_ghost >= HALO) && (rowbytes % 16 == 0) &&
+                      (((size_t)ctx->Np * ctx->elem) % 16 == 0) && get_encode_fn() != nullptr;
+    ctx->at_n = 1;
+
+    int rc = BOLT_OK;
+    const size_t fbytes = ctx->fcount * ctx->elem;
+    const int nbuf = p.integrator == BOLT_RK4 ? 3 : 1;
+    for (int i = 0; i < nbuf && rc == BOLT_OK; ++i) rc = dev_alloc(ctx, &ctx->buf[i], fbytes);
+    if (rc == BOLT_OK && p.fields_enabled) rc = dev_alloc(ctx, &ctx->kbuf, fbytes);
+    const size_t plane = (size_t)g.N_q1 * g.N_q2 * g.N_s;
+    const int nsp = ctx->nsplit > 1 ? ctx->nsplit : 1;
+    for (int i = 0; i < 2 && rc == BOLT_OK; ++i)
+        rc = dev_alloc(ctx, (void**)&ctx->momP[i], (size_t)nsp * kNumMom * plane * sizeof(double));
+    if (rc == BOLT_OK && p.fields_enabled) {
+        const size_t fp = (size_t)ctx->Nq1g * ctx->Nq2g;
+        rc = dev_alloc(ctx, (void**)&ctx->jpart, (size_t)nsp * 3 * plane * sizeof(double));
+        if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->cell, 6 * fp * sizeof(double));
+        if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->yee, 6 * fp * sizeof(double));
+        if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->ebefore, 3 * fp * sizeof(double));
+        if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->J, 3 * fp * sizeof(double));
+        if (rc == BOLT_OK) {
+            cudaMemset(ctx->cell, 0, 6 * fp * sizeof(double));
+            cudaMemset(ctx->yee, 0, 6 * fp * sizeof(double));
+        }
+    }
+    if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->derr, sizeof(int));
+    if (rc == BOLT_OK && cudaMemset(ctx->derr, 0, sizeof(int)) != cudaSuccess) rc = BOLT_ERR_CUDA;
+    if (rc == BOLT_OK) {
+        if (cudaHostAlloc((void**)&ctx->hflag, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostGetDevicePointer((void**)&ctx->dflag, ctx->hflag, 0) != cudaSuccess)
+            rc = BOLT_ERR_CUDA;
+        else
+            *ctx->hflag = 0;
+    }
+    if (rc == BOLT_OK && cudaDeviceSynchronize() != cudaSuccess) rc = BOLT_ERR_CUDA;
+    if (rc != BOLT_OK) {
+        bolt_ctx_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return BOLT_OK;
+}
+
+void bolt_ctx_destroy(BoltCtx* ctx) {
+    if (!ctx) return;
+    for (int i = 0; i < 3; ++i) cudaFree(ctx->buf[i]);
+    cudaFree(ctx->kbuf);
+    cudaFree(ctx->momP[0]);
+    cudaFree(ctx->momP[1]);
+    cudaFree(ctx->jpart);
+    cudaFree(ctx->cell);
+    cudaFree(ctx->yee);
+    cudaFree(ctx->ebefore);
+    cudaFree(ctx->J);
+    cudaFree(ctx->derr);
+    if (ctx->hflag) cudaFreeHost(ctx->hflag);
+    delete ctx;
+}
+
+int bolt_set_tau_array(BoltCtx* ctx, const void* tau_dev) {
+    if (!ctx) return BOLT_ERR_ARG;
+    ctx->tau_arr = tau_dev;
+    return BOLT_OK;
+}
+
+int bolt_set_dirichlet(BoltCtx* ctx, int side, const void* values_dev) {
+    if (!ctx || side < 0 || side > 3) return BOLT_ERR_ARG;
+    ctx->dirichlet[side] = values_dev;
+    ctx->ghost_owner = nullptr;
+    return BOLT_OK;
+}
+
+long long bolt_launch_count(BoltCtx* ctx) { return ctx ? ctx->launches : 0; }
+size_t bolt_scratch_bytes(BoltCtx* ctx) { return ctx ? ctx->scratch_bytes : 0; }
+
+int bolt_divergence_flag(BoltCtx* ctx) {
+    if (!ctx || !ctx->hflag) return 0;
+    return *(volatile int*)ctx->hflag ? 1 : 0;
+}
+
+int bolt_clear_divergence_flag(BoltCtx* ctx) {
+    if (!ctx || !ctx->hflag) return BOLT_ERR_ARG;
+    *(volatile int*)ctx->hflag = 0;
+    return BOLT_OK;
+}
+
+int bolt_status_sync(BoltCtx* ctx, void* stream) {
+    if (!ctx) return BOLT_ERR_ARG;
+    if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return BOLT_ERR_CUDA;
+    int e = 0;
+    if (cudaMemcpy(&e, ctx->derr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return BOLT_ERR_CUDA;
+    if (e) return e;
+    if (ctx->sticky) return ctx->sticky;
+    return BOLT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// internal launch helpers
+// ---------------------------------------------------------------------------
+static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
+    const BoltGrid& g = ctx->g;
+    const int dir1 = ctx->p.bc_q1 == BOLT_BC_DIRICHLET, dir2 = ctx->p.bc_q2 == BOLT_BC_DIRICHLET;
+    if (g.N_ghost == 0) return BOLT_OK;
+    if ((dir1 && (!ctx->dirichlet[0] || !ctx->dirichlet[1])) ||
+        (dir2 && (!ctx->dirichlet[2] || !ctx->dirichlet[3])))
+        return BOLT_ERR_ARG;
+    cudaError_t e;
+    if (ctx->elem == 8)
+        e = launch_ghost_f64(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
+                             ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
+                             g.N_p1, g.N_p2, !dir1, !dir2, dir1, dir2, ctx->sg, st);
+    else
+        e = launch_ghost_f32(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
+                             ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
+                             g.N_p1, g.N_p2, !dir1, !dir2, dir1, dir2, ctx->sg, st);
+    ctx->launches++;
+    CK(e);
+    return BOLT_OK;
+}
+
+static int launch_moments5(BoltCtx* ctx, const void* f, double* part, cudaStream_t st) {
+    const BoltGrid& g = ctx->g;
+    cudaError_t e = ctx->elem == 8
+        ? launch_moments5_f64(f, part, g.N_s, g.N_p1, g.N_p2, g.N_p3, g.N_q1, g.N_q2, g.N_ghost,
+                              ctx->sg, st)
+        : launch_moments5_f32(f, part, g.N_s, g.N_p1, g.N_p2, g.N_p3, g.N_q1, g.N_q2, g.N_ghost,
+                              ctx->sg, st);
+    ctx->launches++;
+    CK(e);
+    return BOLT_OK;
+}
+
+struct StageIO {
+    const void* fs;
+    const void* base1;
+    double c1;
+    void* out1;
+    const void* base2;
+    double c2;
+    void* out2;
+    const double* mom_in;
+    int nsplit_in;
+    double* mom_out;
+    int* flag;
+};
+
+// q-part of one stage.  write_k: out1 <- k_q (no moments, no ghosts).
+static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_j,
+                         cudaStream_t st) {
+    const BoltGrid& g = ctx->g;
+    QStageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.use_tma = 0;
+    if (ctx->use_tma_ok && (((uintptr_t)io.fs) % 16 == 0)) {
+        const CUtensorMap* m = get_tmap(ctx, io.fs);
+        if (m) {
+            a.tmap = *m;
+            a.use_tma = 1;
+        }
+    }
+    a.fs = io.fs;
+    a.base1 = write_k ? nullptr : io.base1;
+    a.base2 = write_k ? nullptr : io.base2;
+    a.out1 = io.out1;
+    a.out2 = write_k ? nullptr : io.out2;
+    a.tau_arr = ctx->tau_arr;
+    a.mom_in = io.mom_in;
+    a.mom_out = write_k ? nullptr : io.mom_out;
+    a.j_out = want_j ? ctx->jpart : nullptr;
+    a.flag = write_k ? nullptr : io.flag;
+    a.err = ctx->derr;
+    a.c1 = io.c1;
+    a.c2 = io.c2;
+    a.tau = ctx->p.tau;
+    a.dq1 = g.dq1;
+    a.dq2 = g.dq2;
+    a.kB = ctx->p.boltzmann_constant;
+    a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost; a.Ns = g.N_s;
+    a.Np1 = g.N_p1; a.Np2 = g.N_p2; a.Np3 = g.N_p3; a.Np = ctx->Np;
+    a.Nq1g = ctx->Nq1g; a.Nq2g = ctx->Nq2g;
+    const TileShape t = tile_shape(ctx->tiling);
+    a.periodic1 = !write_k && ctx->p.bc_q1 == BOLT_BC_PERIODIC && g.N_ghost > 0;
+    a.periodic2 = !write_k && ctx->p.bc_q2 == BOLT_BC_PERIODIC && g.N_ghost > 0 && t.q2;
+    a.nsplit_in = io.nsplit_in;
+    a.nsplit = ctx->nsplit;
+    a.chunks_per_split = ctx->chunks_per_split;
+    a.ntiles1 = ctx->ntiles1;
+    a.p_dim = ctx->p.p_dim;
+    a.want_j = want_j;
+    a.bgk_direct = ctx->bgk_direct;
+    a.sg = ctx->sg;
+    dim3 grid(ctx->ntiles1 * ctx->ntiles2, g.N_s * ctx->nsplit);
+    const size_t smem = qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct, ctx->ntab);
+    cudaError_t e = ctx->elem == 8
+        ? launch_qstage_f64(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st)
+        : launch_qstage_f32(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st);
+    ctx->launches++;
+    CK(e);
+    return BOLT_OK;
+}
+
+static int launch_pstage(BoltCtx* ctx, const StageIO& io, const void* kq, cudaStream_t st) {
+    const BoltGrid& g = ctx->g;
+    PStageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.fs = io.fs;
+    a.kq = kq;
+    a.base1 = io.base1;
+    a.base2 = io.base2;
+    a.out1 = io.out1;
+    a.out2 = io.out2;
+    a.cell = ctx->cell;
+    a.mom_out = io.mom_out;
+    a.flag = io.flag;
+    a.c1 = io.c1;
+    a.c2 = io.c2;
+    a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost; a.Ns = g.N_s;
+    a.Np1 = g.N_p1; a.Np2 = g.N_p2; a.Np3 = g.N_p3; a.Np = ctx->Np;
+    a.Nq1g = ctx->Nq1g; a.Nq2g = ctx->Nq2g;
+    a.periodic1 = io.base1 != nullptr && ctx->p.bc_q1 == BOLT_BC_PERIODIC && g.N_ghost > 0;
+    a.periodic2 = io.base1 != nullptr && ctx->p.bc_q2 == BOLT_BC_PERIODIC && g.N_ghost > 0;
+    a.sg = ctx->sg;
+    const size_t smem = pstage_smem(ctx->Np, ctx->elem);
+    if (smem > 200 * 1024) return BOLT_ERR_UNSUPPORTED;
+    dim3 grid(g.N_q1 * g.N_q2, g.N_s);
+    cudaError_t e = ctx->elem == 8 ? launch_pstage_f64(a, ctx->recon_p, grid, smem, st)
+                                   : launch_pstage_f32(a, ctx->recon_p, grid, smem, st);
+    ctx->launches++;
+    CK(e);
+    return BOLT_OK;
+}
+
+static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st) {
+    const BoltGrid& g = ctx->g;
+    FieldArgs a;
+    memset(&a, 0, sizeof(a));
+    a.yee = ctx->yee;
+    a.cell = ctx->cell;
+    a.ebefore = ctx->ebefore;
+    a.J = ctx->J;
+    a.jpart = ctx->jpart;
+    a.nsplit = nsplit_j;
+    a.Ns = g.N_s; a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost;
+    a.Nq1g = ctx->Nq1g; a.Nq2g = ctx->Nq2g;
+    a.dq1 = g.dq1; a.dq2 = g.dq2; a.dt = dt; a.eps = ctx->p.eps; a.mu = ctx->p.mu;
+    for (int s = 0; s < g.N_s; ++s) {
+        a.charge[s] = ctx->p.charge[s];
+        a.measure[s] = (g.dp3[s] * g.dp2[s]) * g.dp1[s];
+    }
+    CK(launch_fdtd(a, st, &ctx->launches));
+    return BOLT_OK;
+}
+
+// one df/dt evaluation + stage update: q-part (fused combine when there is no
+// p-advection), then p-part when fields are enabled
+static int run_stage(BoltCtx* ctx, StageIO io, int evolve, double dt, cudaStream_t st) {
+    int rc;
+    if (!ctx->p.fields_enabled) {
+        rc = launch_qstage(ctx, io, 0, 0, st);
+    } else {
+        StageIO qio = io;
+        qio.out1 = ctx->kbuf;
+        rc = launch_qstage(ctx, qio, 1, evolve, st);
+        if (rc == BOLT_OK && evolve) rc = launch_fields(ctx, dt, ctx->nsplit, st);
+        if (rc == BOLT_OK) rc = launch_pstage(ctx, io, ctx->kbuf, st);
+    }
+    return rc;
+}
+
+static int ensure_state(BoltCtx* ctx, void* f, cudaStream_t st) {
+    int rc = BOLT_OK;
+    if (ctx->ghost_owner != f) {
+        rc = launch_ghosts(ctx, f, st);
+        if (rc) return rc;
+        ctx->ghost_owner = f;
+        ctx->mom_owner = nullptr;
+    }
+    if (ctx->bgk && ctx->mom_owner != f) {
+        rc = launch_moments5(ctx, f, ctx->momP[ctx->cur_mom], st);
+        if (rc) return rc;
+        ctx->cur_nsplit = 1;
+        ctx->mom_owner = f;
+    }
+    return rc;
+}
+
+static int step_once(BoltCtx* ctx, void* f, double dt, cudaStream_t st) {
+    int rc = ensure_state(ctx, f, st);
+    if (rc) return rc;
+    const int dir = ctx->p.bc_q1 == BOLT_BC_DIRICHLET || ctx->p.bc_q2 == BOLT_BC_DIRICHLET;
+    const int fe = ctx->p.fields_enabled;
+    const int mo_split = fe ? 1 : ctx->nsplit;     // nsplit of partials written by a stage
+    double* mcur = ctx->momP[ctx->cur_mom];
+    double* mnxt = ctx->momP[ctx->cur_mom ^ 1];
+    int nin = ctx->cur_nsplit;
+    StageIO io;
+    memset(&io, 0, sizeof(io));
+    if (ctx->p.integrator == BOLT_RK2) {
+        // fvm_operator.py:22-33: f_half = f + k1*(dt/2); f = f_initial + k2*dt
+        void* A = ctx->buf[0];
+        io.fs = f; io.base1 = f; io.c1 = dt / 2; io.out1 = A;
+        io.mom_in = mcur; io.nsplit_in = nin; io.mom_out = ctx->bgk ? mnxt : nullptr;
+        int ev = fe && !ctx->at_n;
+        rc = run_stage(ctx, io, ev, dt, st);
+        if (fe) ctx->at_n ^= 1;
+        if (!rc && dir) rc = launch_ghosts(ctx, A, st);
+        if (rc) return rc;
+        memset(&io, 0, sizeof(io));
+        io.fs = A; io.base1 = f; io.c1 = dt; io.out1 = f;
+        io.mom_in = mnxt; io.nsplit_in = mo_split; io.mom_out = ctx->bgk ? mcur : nullptr;
+        io.flag = ctx->dflag;
+        ev = fe && !ctx->at_n;
+        rc = run_stage(ctx, io, ev, dt, st);
+        if (fe) ctx->at_n ^= 1;
+        if (!rc && dir) rc = launch_ghosts(ctx, f, st);
+        if (rc) return rc;
+    } else {
+        // classic RK4 (integrators.py:15-28) in accumulator form:
+        //   f1 = f + (dt/2) k1, acc = f + (dt/6) k1
+        //   f2 = f + (dt/2) k2, acc += (dt/3) k2
+        //   f3 = f + dt k3,     acc += (dt/3) k3
+        //   f  = acc + (dt/6) k4
+        // fields (if any) advance once per step, in stage 2
+        void* A = ctx->buf[0];
+        void* B = ctx->buf[1];
+        void* C = ctx->buf[2];
+        const double c_half = 0.5 * dt, c_six = dt / 6.0, c_three = dt / 3.0;
+        struct S {
+            const void* fs; const void* b1; double c1; void* o1; const void* b2; double c2;
+            void* o2; int ev;
+        } stages[4] = {
+            {f, f, c_half, A, f, c_six, C, 0},
+            {A, f, c_half, B, C, c_three, C, 1},
+            {B, f, dt, A, C, c_three, C, 0},
+            {A, C, c_six, f, nullptr, 0.0, nullptr, 0},
+        };
+        double* m_in = mcur;
+        double* m_out = mnxt;
+        for (int k = 0; k < 4; ++k) {
+            memset(&io, 0, sizeof(io));
+            io.fs = stages[k].fs; io.base1 = stages[k].b1; io.c1 = stages[k].c1;
+            io.out1 = stages[k].o1; io.base2 = stages[k].b2; io.c2 = stages[k].c2;
+            io.out2 = stages[k].o2;
+            io.mom_in = m_in; io.nsplit_in = k == 0 ? nin : mo_split;
+            io.mom_out = ctx->bgk ? m_out : nullptr;
+            io.flag = k == 3 ? ctx->dflag : nullptr;
+            rc = run_stage(ctx, io, fe && stages[k].ev, dt, st);
+            if (!rc && dir) rc = launch_ghosts(ctx, stages[k].o1, st);
+            if (rc) return rc;
+            double* tmp = m_in; m_in = m_out; m_out = tmp;
+        }
+        // after 4 swaps m_in (== mcur) holds the moments of the new f
+    }
+    ctx->cur_nsplit = mo_split;
+    ctx->ghost_owner = f;
+    ctx->mom_owner = ctx->bgk ? f : nullptr;
+    return BOLT_OK;
+}
+
+extern "C" {
+
+int bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream) {
+    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+    int rc = launch_ghosts(ctx, f_dev, (cudaStream_t)stream);
+    if (rc) return rc;
+    ctx->ghost_owner = f_dev;
+    ctx->mom_owner = nullptr;
+    return BOLT_OK;
+}
+
+int bolt_invalidate(BoltCtx* ctx) {
+    if (!ctx) return BOLT_ERR_ARG;
+    ctx->ghost_owner = nullptr;
+    ctx->mom_owner = nullptr;
+    return BOLT_OK;
+}
+
+int bolt_step(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
+    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+    return step_once(ctx, f_dev, dt, (cudaStream_t)stream);
+}
+
+int bolt_run(BoltCtx* ctx, void* f_dev, double dt, int n_steps, void* stream) {
+    if (!ctx || !f_dev || n_steps < 0) return BOLT_ERR_ARG;
+    for (int i = 0; i < n_steps; ++i) {
+        int rc = step_once(ctx, f_dev, dt, (cudaStream_t)stream);
+        if (rc) return rc;
+    }
+    return BOLT_OK;
+}
+
+int bolt_dfdt(BoltCtx* ctx, const void* f_dev, void* dfdt_dev, int evolve_fields, double dt,
+              void* stream) {
+    if (!ctx || !f_dev || !dfdt_dev) return BOLT_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = BOLT_OK;
+    double* m = ctx->momP[ctx->cur_mom ^ 1];
+    if (ctx->bgk) rc = launch_moments5(ctx, f_dev, m, st);
+    if (rc) return rc;
+    StageIO io;
+    memset(&io, 0, sizeof(io));
+    io.fs = f_dev;
+    io.mom_in = m;
+    io.nsplit_in = 1;
+    if (!ctx->p.fields_enabled) {
+        io.out1 = dfdt_dev;
+        return launch_qstage(ctx, io, 1, 0, st);
+    }
+    StageIO qio = io;
+    qio.out1 = ctx->kbuf;
+    rc = launch_qstage(ctx, qio, 1, evolve_fields, st);
+    if (!rc && evolve_fields) rc = launch_fields(ctx, dt, ctx->nsplit, st);
+    if (!rc) {
+        io.out1 = dfdt_dev;
+        rc = launch_pstage(ctx, io, ctx->kbuf, st);
+    }
+    return rc;
+}
+
+int bolt_moments(BoltCtx* ctx, const void* f_dev, int moment_id, double* out_dev,
+                 void* stream) {
+    if (!ctx || !f_dev || !out_dev || moment_id < 0 || moment_id > 10) return BOLT_ERR_ARG;
+    const BoltGrid& g = ctx->g;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = ctx->elem == 8
+        ? launch_moment_f64(f_dev, moment_id, out_dev, g.N_s, g.N_p1, g.N_p2, g.N_p3, ctx->Nq1g,
+                            ctx->Nq2g, ctx->sg, st)
+        : launch_moment_f32(f_dev, moment_id, out_dev, g.N_s, g.N_p1, g.N_p2, g.N_p3, ctx->Nq1g,
+                            ctx->Nq2g, ctx->sg, st);
+    ctx->launches++;
+    CK(e);
+    return BOLT_OK;
+}
+
+int bolt_fields_set(BoltCtx* ctx, const double* cell_dev, const double* yee_dev, void* stream) {
+    if (!ctx || !ctx->p.fields_enabled) return BOLT_ERR_ARG;
+    const size_t bytes = 6 * (size_t)ctx->Nq1g * ctx->Nq2g * sizeof(double);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cell_dev) CK(cudaMemcpyAsync(ctx->cell, cell_dev, bytes, cudaMemcpyDeviceToDevice, st));
+    if (yee_dev) CK(cudaMemcpyAsync(ctx->yee, yee_dev, bytes, cudaMemcpyDeviceToDevice, st));
+    return BOLT_OK;
+}
+
+int bolt_fields_get(BoltCtx* ctx, double* cell_dev, double* yee_dev, void* stream) {
+    if (!ctx || !ctx->p.fields_enabled) return BOLT_ERR_ARG;
+    const size_t bytes = 6 * (size_t)ctx->Nq1g * ctx->Nq2g * sizeof(double);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cell_dev) CK(cudaMemcpyAsync(cell_dev, ctx->cell, bytes, cudaMemcpyDeviceToDevice, st));
+    if (yee_dev) CK(cudaMemcpyAsync(yee_dev, ctx->yee, bytes, cudaMemcpyDeviceToDevice, st));
+    return BOLT_OK;
+}
+
+int bolt_get_at_n(BoltCtx* ctx) { return ctx ? ctx->at_n : -1; }
+
+int bolt_set_at_n(BoltCtx* ctx, int at_n) {
+    if (!ctx) return BOLT_ERR_ARG;
+    ctx->at_n = at_n ? 1 : 0;
+    return BOLT_OK;
+}
+
+}  // extern "C"

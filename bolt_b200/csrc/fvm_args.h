@@ -1,0 +1,73 @@
+// fvm_args.h - constants and kernel argument blocks shared by host and device.
+#pragma once
+
+#include <cuda.h>
+#include <stdint.h>
+
+namespace bolt {
+
+constexpr int kMaxSpecies = 8;
+constexpr int PW = 32;          // p-cells per chunk (one per lane)
+constexpr int HALO = 3;         // q-stencil half width incl. face shift
+constexpr int NTHREADS = 256;   // q-stage CTA size (8 warps)
+constexpr int kNumMom = 5;      // n, mom_v1, mom_v2, mom_v3, energy
+
+struct SpeciesGrid {
+    double p1_start[kMaxSpecies], p2_start[kMaxSpecies], p3_start[kMaxSpecies];
+    double dp1[kMaxSpecies], dp2[kMaxSpecies], dp3[kMaxSpecies];
+    double mass[kMaxSpecies], charge[kMaxSpecies];
+};
+
+struct QStageArgs {
+    CUtensorMap tmap;           // 3-D map over fs: (Ns*Np, Nq1g, Nq2g), box (32, TQ1+6, HY)
+    const void* fs;             // stage input (stencil source), ghosted
+    const void* base1;          // out1 = base1 + c1*k   (null: out1 = k)
+    const void* base2;          // out2 = base2 + c2*k   (null: no out2)
+    void* out1;
+    void* out2;
+    const void* tau_arr;        // f-shaped tau or null
+    const double* mom_in;       // partial moments of fs [nsplit_in][5][Ns][Nq2][Nq1]
+    double* mom_out;            // partial moments of out1 [nsplit][5][Ns][Nq2][Nq1] or null
+    double* j_out;              // partial currents [nsplit][3][Ns][Nq2][Nq1] or null
+    int* flag;                  // divergence flag (host-mapped) or null
+    int* err;                   // sticky device error word
+    double c1, c2, tau;
+    double dq1, dq2, kB;
+    int Nq1, Nq2, Ng, Ns, Np1, Np2, Np3, Np, Nq1g, Nq2g;
+    int periodic1, periodic2;   // write wrap-around ghost copies of out1
+    int nsplit_in, nsplit, chunks_per_split, ntiles1;
+    int use_tma, p_dim, want_j;
+    int bgk_direct;             // 1: exp per cell (no per-q-cell exp tables)
+    SpeciesGrid sg;
+};
+
+struct PStageArgs {
+    const void* fs;        // stage input (ghosted)
+    const void* kq;        // q-part of df/dt (ghosted layout, interior valid)
+    const void* base1;
+    const void* base2;
+    void* out1;
+    void* out2;
+    const double* cell;    // cell-centred fields [6][Nq2g][Nq1g]
+    double* mom_out;       // [1][5][Ns][Nq2][Nq1] or null
+    int* flag;
+    double c1, c2;
+    int Nq1, Nq2, Ng, Ns, Np1, Np2, Np3, Np, Nq1g, Nq2g;
+    int periodic1, periodic2;
+    SpeciesGrid sg;
+};
+
+constexpr int PTHREADS = 256;
+
+struct FieldArgs {
+    double* yee;            // [6][Nq2g][Nq1g]
+    double* cell;           // [6][Nq2g][Nq1g]
+    double* ebefore;        // [3][Nq2g][Nq1g]
+    double* J;              // [3][Nq2g][Nq1g]
+    const double* jpart;    // [nsplit][3][Ns][Nq2][Nq1]
+    int nsplit, Ns, Nq1, Nq2, Ng, Nq1g, Nq2g;
+    double dq1, dq2, dt, eps, mu;
+    double charge[kMaxSpecies], measure[kMaxSpecies];
+};
+
+}  // namespace bolt

@@ -1,0 +1,263 @@
+// fvm_common.cuh - device helpers shared by the FVM kernels (sm_100a).
+//
+// Face reconstruction follows Bolt's reconstruction modules
+// (bolt/lib/nonlinear/finite_volume/reconstruction/{weno5,ppm,minmod}.py and
+// reconstruct.py:29-44).  Every method is evaluated for ONE cell, y2, from
+// the five values y0..y4 = f[i-2..i+2] around it, and returns either its right
+// face value (upwind side for C > 0) or its left face value (C <= 0), which is
+// what riemann.py:46-49 selects.  The caller passes the per-lane window
+// offset so the choice is branch-free inside a warp.
+//
+// Two arithmetic flavours:
+//   * exact (FP64 parity build, compiled with -fmad=false): operation order
+//     and constants identical to the reference expressions;
+//   * fast (FP32 build): algebraically identical forms with FMA and
+//     approximate reciprocals (WENO5 smoothness indicators in the factored
+//     13/12 (a-2b+c)^2 + 1/4 (a-4b+3c)^2 form, which expands to the
+//     reference's polynomial).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define BOLT_RECON_PC     0
+#define BOLT_RECON_MINMOD 1
+#define BOLT_RECON_PPM    2
+#define BOLT_RECON_WENO5  3
+
+namespace bolt {
+
+// ---------------------------------------------------------------------------
+// small math helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fast_rcp(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ double fast_rcp(double x) { return 1.0 / x; }
+
+template <typename T> struct Consts;
+template <> struct Consts<double> {
+    static constexpr double c4_3 = 4.0 / 3.0, c19_3 = 19.0 / 3.0, c25_3 = 25.0 / 3.0,
+                            c11_3 = 11.0 / 3.0, c31_3 = 31.0 / 3.0, c10_3 = 10.0 / 3.0;
+};
+template <> struct Consts<float> {
+    static constexpr float c4_3 = 4.0f / 3.0f, c19_3 = 19.0f / 3.0f, c25_3 = 25.0f / 3.0f,
+                           c11_3 = 11.0f / 3.0f, c31_3 = 31.0f / 3.0f, c10_3 = 10.0f / 3.0f;
+};
+
+// Per-lane WENO5 coefficient set: the reference's right-face constants
+// (w = {1/16, 5/8, 5/16}/beta^2, u_r interpolants) when the lane's velocity
+// is positive, the left-face set otherwise (weno5.py:74-92).
+template <typename T>
+struct Weno5Side {
+    T num1, den1, num2, den2, num3, den3;      // w_k = num_k / ((den_k*beta_k)*beta_k)
+    T a10, a11, a12, a20, a21, a22, a30, a31, a32;  // u_k = (a_k0 y + a_k1 y) + a_k2 y
+    __device__ __forceinline__ void set(bool right) {
+        if (right) {
+            num1 = T(1); den1 = T(16); num2 = T(5); den2 = T(8); num3 = T(5); den3 = T(16);
+            a10 = T(0.375);  a11 = T(-1.25); a12 = T(1.875);
+            a20 = T(-0.125); a21 = T(0.75);  a22 = T(0.375);
+            a30 = T(0.375);  a31 = T(0.75);  a32 = T(-0.125);
+        } else {
+            num1 = T(5); den1 = T(16); num2 = T(5); den2 = T(8); num3 = T(1); den3 = T(16);
+            a10 = T(-0.125); a11 = T(0.75);  a12 = T(0.375);
+            a20 = T(0.375);  a21 = T(0.75);  a22 = T(-0.125);
+            a30 = T(1.875);  a31 = T(-1.25); a32 = T(0.375);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// WENO5, exact reference order (weno5.py:58-96)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double weno_beta_exact(double a, double b, double c) {
+    typedef Consts<double> K;
+    double poly = ((((K::c4_3 * a * a - K::c19_3 * a * b) + K::c25_3 * b * b)
+                    + K::c11_3 * a * c) - K::c31_3 * b * c) + K::c10_3 * c * c;
+    return poly + 1e-17 * (((1.0 + fabs(a)) + fabs(b)) + fabs(c));
+}
+
+__device__ __forceinline__ double weno5_exact(double y0, double y1, double y2, double y3,
+                                              double y4, const Weno5Side<double>& S) {
+    double b1 = weno_beta_exact(y0, y1, y2);
+    double b2 = weno_beta_exact(y1, y2, y3);
+    double b3 = weno_beta_exact(y2, y3, y4);
+    double w1 = S.num1 / ((S.den1 * b1) * b1);
+    double w2 = S.num2 / ((S.den2 * b2) * b2);
+    double w3 = S.num3 / ((S.den3 * b3) * b3);
+    double den = (w1 + w2) + w3;
+    double u1 = (S.a10 * y0 + S.a11 * y1) + S.a12 * y2;
+    double u2 = (S.a20 * y1 + S.a21 * y2) + S.a22 * y3;
+    double u3 = (S.a30 * y2 + S.a31 * y3) + S.a32 * y4;
+    return ((w1 * u1 + w2 * u2) + w3 * u3) / den;
+}
+
+// WENO5, fast FP32 form
+__device__ __forceinline__ float weno_beta_fast(float a, float b, float c) {
+    float d1 = fmaf(-2.0f, b, a + c);           // a - 2b + c
+    float d2 = fmaf(3.0f, c, fmaf(-4.0f, b, a));  // a - 4b + 3c
+    float e = 1e-17f * (1.0f + fabsf(a) + fabsf(b) + fabsf(c));
+    return fmaf(13.0f / 12.0f * d1, d1, fmaf(0.25f * d2, d2, e));
+}
+
+__device__ __forceinline__ float weno5_fast(float y0, float y1, float y2, float y3, float y4,
+                                            const Weno5Side<float>& S) {
+    float r1 = fast_rcp(weno_beta_fast(y0, y1, y2));
+    float r2 = fast_rcp(weno_beta_fast(y1, y2, y3));
+    float r3 = fast_rcp(weno_beta_fast(y2, y3, y4));
+    // num/den folded into a single scale per weight
+    float w1 = (S.num1 / S.den1) * r1 * r1;
+    float w2 = (S.num2 / S.den2) * r2 * r2;
+    float w3 = (S.num3 / S.den3) * r3 * r3;
+    float u1 = fmaf(S.a12, y2, fmaf(S.a11, y1, S.a10 * y0));
+    float u2 = fmaf(S.a22, y3, fmaf(S.a21, y2, S.a20 * y1));
+    float u3 = fmaf(S.a32, y4, fmaf(S.a31, y3, S.a30 * y2));
+    float num = fmaf(w3, u3, fmaf(w2, u2, w1 * u1));
+    return num * fast_rcp(w1 + w2 + w3);
+}
+
+// ---------------------------------------------------------------------------
+// minmod / MC limiter, theta = 2 (minmod.py:4-71); sign(0) = +1
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T minmod_slope(T ym, T y, T yp) {
+    T fwd = yp - y;
+    T bwd = y - ym;
+    T cen = bwd + fwd;
+    T x = T(2) * bwd, yy = T(0.5) * cen, z = T(2) * fwd;
+    T m = fmin(fmin(fabs(x), fabs(yy)), fabs(z));
+    T sx = x < T(0) ? T(-1) : T(1);
+    T sy = yy < T(0) ? T(-1) : T(1);
+    T sz = z < T(0) ? T(-1) : T(1);
+    return ((T(0.25) * fabs(sx + sy)) * (sx + sz)) * m;
+}
+
+// ---------------------------------------------------------------------------
+// PPM (ppm.py:58-98): returns right (right=true) or left face of cell y2
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T ppm_dq(T D, T da, T db) {
+    T zero = (db * da <= T(0)) ? T(1) : T(0);
+    T sgn = (D > T(0)) ? T(1) : T(-1);
+    return ((T(1) - zero) * sgn) * fmin(fabs(D), fmin(fabs(da), fabs(db)));
+}
+
+template <typename T>
+__device__ __forceinline__ T ppm_face(T y0, T y1, T y2, T y3, T y4, bool right) {
+    T d0 = T(2) * (y1 - y0), d1 = T(2) * (y2 - y1), d2 = T(2) * (y3 - y2), d3 = T(2) * (y4 - y3);
+    T D1 = T(0.5) * (y2 - y0), D2 = T(0.5) * (y3 - y1), D3 = T(0.5) * (y4 - y2);
+    T DQ1 = ppm_dq(D1, d0, d1), DQ2 = ppm_dq(D2, d1, d2), DQ3 = ppm_dq(D3, d2, d3);
+    T left = T(0.5) * (y2 + y1) - (DQ2 - DQ1) / T(6);
+    T rightv = T(0.5) * (y3 + y2) - (DQ3 - DQ2) / T(6);
+    T c1 = ((rightv - y2) * (y2 - left) <= T(0)) ? T(1) : T(0);
+    T qd = rightv - left;
+    T qe = T(6) * (y2 - T(0.5) * (rightv + left));
+    T c2 = (qd * (qd - qe) < T(0)) ? T(1) : T(0);
+    T c3 = (qd * (qd + qe) < T(0)) ? T(1) : T(0);
+    left = left * (T(1) - c1) + c1 * y2;
+    rightv = rightv * (T(1) - c1) + c1 * y2;
+    left = left * (T(1) - c2) + c2 * (T(3) * y2 - T(2) * rightv);
+    rightv = (rightv * c2 + ((T(1) - c2) * rightv) * (T(1) - c3))
+             + ((T(1) - c2) * c3) * (T(3) * y2 - T(2) * left);
+    return right ? rightv : left;
+}
+
+// ---------------------------------------------------------------------------
+// Unified face value of cell y2 (right face if `right`, else left face)
+// ---------------------------------------------------------------------------
+template <int RECON, bool EXACT, typename T>
+__device__ __forceinline__ T face_value(T y0, T y1, T y2, T y3, T y4, bool right,
+                                        const Weno5Side<T>& S) {
+    if (RECON == BOLT_RECON_PC) {
+        return y2;
+    } else if (RECON == BOLT_RECON_MINMOD) {
+        T s = minmod_slope(y1, y2, y3);
+        return right ? y2 + T(0.5) * s : y2 - T(0.5) * s;
+    } else if (RECON == BOLT_RECON_PPM) {
+        return ppm_face(y0, y1, y2, y3, y4, right);
+    } else {
+        if constexpr (EXACT) {
+            return weno5_exact(double(y0), double(y1), double(y2), double(y3), double(y4),
+                               reinterpret_cast<const Weno5Side<double>&>(S));
+        } else {
+            return weno5_fast(y0, y1, y2, y3, y4, S);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier + TMA (cp.async.bulk.tensor) wrappers.  Waits are bounded: after
+// kWaitCycles clock cycles the wait reports failure and the caller records
+// BOLT_ERR_TIMEOUT instead of hanging.
+// ---------------------------------------------------------------------------
+constexpr long long kWaitCycles = 4000000000LL;   // ~2 s at the boost clock
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// returns false if the barrier did not complete within the time budget
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    for (;;) {
+        for (int it = 0; it < 256; ++it)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (clock64() - t0 > kWaitCycles) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)),
+          "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// warp reductions (FP64)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace bolt

@@ -1,0 +1,672 @@
+// fvm_kernels.cuh - the FVM kernels of the kinetic update (sm_100a).
+//
+// Kernel inventory (templated on the storage type T = double | float and on
+// EXACT = reference operation order, used by the FP64 parity build):
+//
+//   qstage_kernel   q1/q2 advection + BGK relaxation + RK stage combine +
+//                   FP64 partial moments of the stage output.  This is
+//                   df_dt_fvm.py:56-97 (q-part and source) fused with the
+//                   stage update of fvm_operator.py:26,33 / integrators.py:15-28.
+//   pstage_kernel   p1/p2/p3 advection with C_p from the cell-centred fields
+//                   (df_dt_fvm.py:245-323), added to the q-part, then the RK
+//                   combine (used only when fields are enabled).
+//   moments_kernel  compute_moments.py:7-59 for any moment of moments.py.
+//   ghost_kernel    communicate_f + apply_bcs_f (periodic wrap, Dirichlet
+//                   inflow, zero for ghosted outflow cells).
+//   fdtd kernels    fields.py:568-647 / fdtd_explicit.py:9-177 on the Yee grid.
+//
+// Layout: f[q2g][q1g][s][p] with p = (p3, p2, p1) flattened, p1 fastest.
+// The q-stage kernel works on tiles of TQ1 x TQ2 q-cells x 32 consecutive p
+// (one warp lane per p).  A tile plus its 3-cell q-halo is brought into shared
+// memory by one TMA box copy (double-buffered, mbarrier completion), or by
+// coalesced loads with wrap-around indexing when TMA's alignment rules do not
+// hold.  Each CTA owns one q-tile and a contiguous range of p-chunks of one
+// species; its partial velocity moments of the stage output are written per
+// (p-split, q-cell) and summed by the next stage's prologue (deterministic,
+// no atomics).
+#pragma once
+
+#include "fvm_common.cuh"
+#include "fvm_args.h"
+
+namespace bolt {
+
+// smem layout of the q-stage kernel
+template <typename T, int TQ1, int TQ2, bool Q2>
+struct QSmem {
+    static constexpr int HX = TQ1 + 2 * HALO;
+    static constexpr int HY = Q2 ? TQ2 + 2 * HALO : 1;
+    static constexpr int TILE = HY * HX * PW;          // elements per buffer
+    static constexpr int NQ = TQ1 * TQ2;               // q-cells per tile
+};
+
+// ---------------------------------------------------------------------------
+// moment contributions of one value (FP64), reference moments.py:6-24
+// ---------------------------------------------------------------------------
+struct PVel {
+    double v1, v2, v3, vsq;
+};
+
+__device__ __forceinline__ PVel lane_velocity(const SpeciesGrid& sg, int s, int ip1, int ip2,
+                                              int ip3) {
+    PVel v;
+    v.v1 = sg.p1_start[s] + (0.5 + ip1) * sg.dp1[s];
+    v.v2 = sg.p2_start[s] + (0.5 + ip2) * sg.dp2[s];
+    v.v3 = sg.p3_start[s] + (0.5 + ip3) * sg.dp3[s];
+    v.vsq = (v.v1 * v.v1 + v.v2 * v.v2) + v.v3 * v.v3;
+    return v;
+}
+
+// Periodic images of interior cell (ii, jj) in the ghost zones (any Ng/Nq).
+template <typename T>
+__device__ __forceinline__ void write_ghost_images(T* out, T v, int ii, int jj, int s, int p,
+                                                   int Ng, int Nq1, int Nq2, int Nq1g, int Nq2g,
+                                                   int per1, int per2, long long rowstride,
+                                                   long long colstride, int Np) {
+    const int n1 = per1 ? (Ng + Nq1 - 1) / Nq1 : 0;
+    const int n2 = per2 ? (Ng + Nq2 - 1) / Nq2 : 0;
+    for (int t1 = -n1; t1 <= n1; ++t1) {
+        const int g1 = ii + Ng + t1 * Nq1;
+        if (g1 < 0 || g1 >= Nq1g) continue;
+        for (int t2 = -n2; t2 <= n2; ++t2) {
+            const int g2 = jj + Ng + t2 * Nq2;
+            if (g2 < 0 || g2 >= Nq2g || (t1 == 0 && t2 == 0)) continue;
+            out[(long long)g2 * colstride + (long long)g1 * rowstride + (long long)s * Np + p] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// q-stage kernel
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT, int RECON, int TQ1, int TQ2, bool Q2, bool BGK>
+__global__ void __launch_bounds__(NTHREADS)
+qstage_kernel(const __grid_constant__ QStageArgs a) {
+    typedef QSmem<T, TQ1, TQ2, Q2> L;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* tile = reinterpret_cast<T*>(smem_raw);                        // [2][HY][HX][PW]
+    T* D1 = tile + 2 * L::TILE;                                       // [TQ2][TQ1][PW]
+    double* mom_acc = reinterpret_cast<double*>(D1 + L::NQ * PW);     // [NQ][5]
+    double* j_acc = mom_acc + L::NQ * kNumMom;                        // [NQ][3]
+    double* qc = j_acc + L::NQ * 3;                                   // [NQ][5] n*A,u1,u2,u3,2kT
+    double* tabs = qc + L::NQ * 5;                                    // [NQ][Np1+Np2+Np3]
+    const int ntab = a.Np1 + a.Np2 + a.Np3;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(
+        tabs + ((BGK && !a.bgk_direct) ? L::NQ * ntab : 0));
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
+    const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
+    const int i0 = tile1 * TQ1, j0 = tile2 * TQ2;                     // interior origin
+    const int nchunks = (a.Np + PW - 1) / PW;
+    const int k_begin = split * a.chunks_per_split;
+    const int k_end = min(nchunks, k_begin + a.chunks_per_split);
+    const long long rowstride = (long long)a.Ns * a.Np;               // per q1 step
+    const long long colstride = rowstride * a.Nq1g;                   // per q2 step
+    const T* fs = static_cast<const T*>(a.fs);
+
+    for (int c = tid; c < L::NQ * kNumMom; c += NTHREADS) mom_acc[c] = 0.0;
+    for (int c = tid; c < L::NQ * 3; c += NTHREADS) j_acc[c] = 0.0;
+    if (tid == 0 && a.use_tma) {
+        prefetch_tmap(&a.tmap);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_barrier_init();
+    }
+
+    // ---- BGK prologue: Maxwellian of the stage input per q-cell (FP64) ----
+    // collision_operator.py:102-118 and f0 :49-65
+    if (BGK) {
+        const double m = a.sg.mass[s];
+        const double kB = a.kB;
+        const double measure = (a.sg.dp3[s] * a.sg.dp2[s]) * a.sg.dp1[s];
+        const long long plane = (long long)a.Nq2 * a.Nq1;
+        for (int c = tid; c < L::NQ; c += NTHREADS) {
+            int ii = i0 + c % TQ1, jj = j0 + c / TQ1;
+            double mm[kNumMom] = {0, 0, 0, 0, 0};
+            if (ii < a.Nq1 && jj < a.Nq2) {
+                for (int sp = 0; sp < a.nsplit_in; ++sp)
+                    for (int q = 0; q < kNumMom; ++q)
+                        mm[q] += a.mom_in[(((long long)sp * kNumMom + q) * a.Ns + s) * plane
+                                          + (long long)jj * a.Nq1 + ii];
+            }
+            const double eps = 1e-30;
+            double n = mm[0] * measure;
+            double u1 = (mm[1] * measure) / (n + eps);
+            double u2 = (mm[2] * measure) / (n + eps);
+            double u3 = (mm[3] * measure) / (n + eps);
+            double E = mm[4] * measure;
+            double nm = n * m;
+            double Tt = (1.0 / a.p_dim) * ((((2.0 * (E * m) - nm * (u1 * u1)) - nm * (u2 * u2))
+                                            - nm * (u3 * u3))) / (n + eps) + eps;
+            double twokT = (2.0 * kB) * Tt;
+            double base = m / ((2.0 * 3.141592653589793 * kB) * Tt);
+            double A = a.p_dim == 3 ? pow(base, 1.5) : (a.p_dim == 2 ? base : sqrt(base));
+            qc[c * 5 + 0] = n * A;
+            qc[c * 5 + 1] = u1;
+            qc[c * 5 + 2] = u2;
+            qc[c * 5 + 3] = u3;
+            qc[c * 5 + 4] = twokT;
+            if (a.bgk_direct) continue;
+            double* tb = tabs + (long long)c * ntab;
+            for (int q = 0; q < a.Np1; ++q) {
+                double v = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
+                double dv = v - u1;
+                tb[q] = exp((-m * (dv * dv)) / twokT);
+            }
+            for (int q = 0; q < a.Np2; ++q) {
+                double v = a.sg.p2_start[s] + (0.5 + q) * a.sg.dp2[s];
+                double dv = v - u2;
+                tb[a.Np1 + q] = a.p_dim >= 2 ? exp((-m * (dv * dv)) / twokT) : 1.0;
+            }
+            for (int q = 0; q < a.Np3; ++q) {
+                double v = a.sg.p3_start[s] + (0.5 + q) * a.sg.dp3[s];
+                double dv = v - u3;
+                tb[a.Np1 + a.Np2 + q] = a.p_dim == 3 ? exp((-m * (dv * dv)) / twokT) : 1.0;
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- tile loader -------------------------------------------------------
+    bool failed = false;       // a bounded wait gave up: finish without TMA
+    const unsigned tile_bytes = L::TILE * sizeof(T);
+    auto issue = [&](int k, int buf) {
+        if (k >= k_end) return;
+        if (a.use_tma) {
+            if (tid == 0 && !failed) {
+                mbar_arrive_expect_tx(&bars[buf], tile_bytes);
+                tma_load_3d(tile + buf * L::TILE, &a.tmap, &bars[buf], s * a.Np + k * PW,
+                            i0 + a.Ng - HALO, Q2 ? j0 + a.Ng - HALO : j0 + a.Ng);
+            }
+        } else {
+            // coalesced loads with wrap-around (af.shift semantics) indexing
+            T* dst = tile + buf * L::TILE;
+            for (int r = warp; r < L::HY * L::HX; r += NTHREADS / 32) {
+                int hy = r / L::HX, hx = r % L::HX;
+                int g1 = i0 + a.Ng - HALO + hx;
+                int g2 = Q2 ? j0 + a.Ng - HALO + hy : j0 + a.Ng;
+                g1 = ((g1 % a.Nq1g) + a.Nq1g) % a.Nq1g;
+                g2 = ((g2 % a.Nq2g) + a.Nq2g) % a.Nq2g;
+                int p = k * PW + lane;
+                T v = T(0);
+                if (p < a.Np) v = fs[(long long)g2 * colstride + (long long)g1 * rowstride
+                                     + (long long)s * a.Np + p];
+                dst[r * PW + lane] = v;
+            }
+        }
+    };
+
+    unsigned phase[2] = {0u, 0u};
+    issue(k_begin, 0);
+    issue(k_begin + 1, 1);
+
+    T* out1 = static_cast<T*>(a.out1);
+    T* out2 = static_cast<T*>(a.out2);
+    const T* base1 = static_cast<const T*>(a.base1);
+    const T* base2 = static_cast<const T*>(a.base2);
+    const T* tau_arr = static_cast<const T*>(a.tau_arr);
+    const T c1 = T(a.c1), c2 = T(a.c2);
+
+    int buf = 0;
+    for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
+        if (a.use_tma && !failed) {
+            if (!mbar_wait_bounded(&bars[buf], phase[buf])) {
+                atomicExch(a.err, 4);
+                failed = true;
+            }
+            phase[buf] ^= 1u;
+        }
+        __syncthreads();   // plain-load path: tile visible; TMA path: harmless
+        const T* X = tile + buf * L::TILE;
+        const int p = k * PW + lane;
+        const bool pvalid = p < a.Np;
+        const int pc = pvalid ? p : a.Np - 1;
+        const int ip1 = pc % a.Np1, ip2 = (pc / a.Np1) % a.Np2, ip3 = pc / (a.Np1 * a.Np2);
+        const PVel V = lane_velocity(a.sg, s, ip1, ip2, ip3);
+        const T v1 = T(V.v1), v2 = T(V.v2);
+
+        // ---- phase A: q1 faces -> D1 = (-(F_R - F_L)) / dq1 ------------------
+        {
+            const bool right = v1 > T(0);
+            const int off = right ? 0 : 1;
+            Weno5Side<T> S; S.set(right);
+            constexpr int NSEG = (TQ2 >= 8) ? 1 : (8 / TQ2);
+            constexpr int SEG = (TQ1 + NSEG - 1) / NSEG;
+            for (int item = warp; item < TQ2 * NSEG; item += NTHREADS / 32) {
+                const int jr = item / NSEG, sg = item % NSEG;
+                const int cb = sg * SEG, ce = min(TQ1, cb + SEG);
+                if (cb >= ce) continue;
+                const T* row = X + ((Q2 ? jr + HALO : 0) * L::HX) * PW + lane;
+                // window for face f (between cells f-1 and f): cols f+off .. f+off+4
+                T y0 = row[(cb + off + 0) * PW], y1 = row[(cb + off + 1) * PW];
+                T y2 = row[(cb + off + 2) * PW], y3 = row[(cb + off + 3) * PW];
+                T y4 = row[(cb + off + 4) * PW];
+                T fv = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+                T Fprev = v1 * fv;
+                double jsum_prev = double(fv);
+                for (int cc = cb; cc < ce; ++cc) {
+                    // face cc+1
+                    y0 = y1; y1 = y2; y2 = y3; y3 = y4;
+                    y4 = row[(cc + 1 + off + 4) * PW];
+                    T fn = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+                    T Fn = v1 * fn;
+                    T d = (-(Fn - Fprev)) / T(a.dq1);
+                    D1[(jr * TQ1 + cc) * PW + lane] = d;
+                    if (a.want_j) {
+                        // J1 uses the state at each cell's left face (df_dt_fvm.py:214-216)
+                        double c = pvalid ? jsum_prev * V.v1 : 0.0;
+                        c = warp_sum(c);
+                        if (lane == 0) j_acc[(jr * TQ1 + cc) * 3 + 0] += c;
+                    }
+                    Fprev = Fn;
+                    jsum_prev = double(fn);
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- phase B: q2 faces, BGK, RK combine, outputs, moments -------------
+        {
+            const bool right = v2 > T(0);
+            const int off = right ? 0 : 1;
+            Weno5Side<T> S; S.set(right);
+            constexpr int NSEGB = (TQ1 >= 8) ? 1 : (8 / TQ1);
+            constexpr int SEGB = (TQ2 + NSEGB - 1) / NSEGB;
+            const int ntab_off2 = a.Np1 + ip2, ntab_off3 = a.Np1 + a.Np2 + ip3;
+            for (int item = warp; item < TQ1 * NSEGB; item += NTHREADS / 32) {
+                const int ic = item / NSEGB, sg = item % NSEGB;
+                const int rb = sg * SEGB, re = min(TQ2, rb + SEGB);
+                if (rb >= re) continue;
+                const T* col = X + (ic + HALO) * PW + lane;
+                T y0, y1, y2, y3, y4, Fprev = T(0), fprev = T(0);
+                if (Q2) {
+                    y0 = col[((rb + off + 0) * L::HX) * PW]; y1 = col[((rb + off + 1) * L::HX) * PW];
+                    y2 = col[((rb + off + 2) * L::HX) * PW]; y3 = col[((rb + off + 3) * L::HX) * PW];
+                    y4 = col[((rb + off + 4) * L::HX) * PW];
+                    fprev = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+                    Fprev = v2 * fprev;
+                }
+                for (int rr = rb; rr < re; ++rr) {
+                    const int ii = i0 + ic, jj = j0 + rr;
+                    const bool cvalid = pvalid && ii < a.Nq1 && jj < a.Nq2;
+                    const int cq = rr * TQ1 + ic;
+                    T kq = D1[cq * PW + lane];
+                    T fcell = col[((Q2 ? rr + HALO : 0) * L::HX) * PW];
+                    T fbot = fprev;
+                    if (Q2) {
+                        y0 = y1; y1 = y2; y2 = y3; y3 = y4;
+                        y4 = col[((rr + 1 + off + 4) * L::HX) * PW];
+                        T fn = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+                        T Fn = v2 * fn;
+                        kq = kq - (Fn - Fprev) / T(a.dq2);
+                        Fprev = Fn;
+                        fprev = fn;
+                    }
+                    T kk = kq;
+                    const long long gidx = (long long)(jj + a.Ng) * colstride
+                                         + (long long)(ii + a.Ng) * rowstride
+                                         + (long long)s * a.Np + p;
+                    if (BGK) {
+                        double fmb;
+                        if (a.bgk_direct) {
+                            // f0 of collision_operator.py:52-65 evaluated per cell
+                            const double* qq = qc + cq * 5;
+                            const double mneg = -a.sg.mass[s];
+                            double d1v = V.v1 - qq[1];
+                            fmb = qq[0] * exp((mneg * (d1v * d1v)) / qq[4]);
+                            if (a.p_dim >= 2) {
+                                double d2v = V.v2 - qq[2];
+                                fmb = fmb * exp((mneg * (d2v * d2v)) / qq[4]);
+                            }
+                            if (a.p_dim == 3) {
+                                double d3v = V.v3 - qq[3];
+                                fmb = fmb * exp((mneg * (d3v * d3v)) / qq[4]);
+                            }
+                        } else {
+                            const double* tb = tabs + (long long)cq * ntab;
+                            fmb = ((qc[cq * 5] * tb[ip1]) * tb[ntab_off2]) * tb[ntab_off3];
+                        }
+                        if (EXACT) {
+                            // (((n*A)*e1)*e2)*e3 with unit factors for absent dims
+                            double tauv = tau_arr ? double(tau_arr[cvalid ? gidx : 0]) : a.tau;
+                            kk = T(double(kk) + (-(double(fcell) - fmb) / tauv));
+                        } else {
+                            float tauv = tau_arr ? float(tau_arr[cvalid ? gidx : 0]) : float(a.tau);
+                            kk = kk + (-(fcell - T(fmb)) * fast_rcp(tauv));
+                        }
+                    }
+                    if (a.want_j) {
+                        double jc2 = cvalid ? double(fbot) * V.v2 : 0.0;
+                        double jc3 = cvalid ? double(fcell) * V.v3 : 0.0;
+                        jc2 = warp_sum(jc2);
+                        jc3 = warp_sum(jc3);
+                        if (lane == 0) { j_acc[cq * 3 + 1] += jc2; j_acc[cq * 3 + 2] += jc3; }
+                    }
+                    // RK stage combine (fvm_operator.py:26,33; integrators.py:18-25)
+                    T o1 = base1 ? base1[cvalid ? gidx : 0] + kk * c1 : kk;
+                    if (cvalid) {
+                        out1[gidx] = o1;
+                        if (out2) out2[gidx] = base2[gidx] + kk * c2;
+                        // wrap-around ghost copies (what the next halo refresh would do)
+                        if ((a.periodic1 && (ii < a.Ng || ii >= a.Nq1 - a.Ng)) ||
+                            (a.periodic2 && (jj < a.Ng || jj >= a.Nq2 - a.Ng)))
+                            write_ghost_images(out1, o1, ii, jj, s, p, a.Ng, a.Nq1, a.Nq2,
+                                               a.Nq1g, a.Nq2g, a.periodic1, a.periodic2,
+                                               rowstride, colstride, a.Np);
+                        if (a.flag && !isfinite(double(o1))) atomicOr(a.flag, 1);
+                    }
+                    if (a.mom_out) {
+                        double ov = cvalid ? double(o1) : 0.0;
+                        double m0 = warp_sum(ov);
+                        double m1 = warp_sum(ov * V.v1);
+                        double m2 = warp_sum(ov * V.v2);
+                        double m3 = warp_sum(ov * V.v3);
+                        double m4 = warp_sum((0.5 * ov) * V.vsq);
+                        if (lane == 0) {
+                            double* mp = mom_acc + cq * kNumMom;
+                            mp[0] += m0; mp[1] += m1; mp[2] += m2; mp[3] += m3; mp[4] += m4;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();   // buffer `buf` fully consumed
+        if (a.use_tma) fence_proxy_async();
+        issue(k + 2, buf);
+    }
+
+    // ---- epilogue: partial moments / currents of this split ------------------
+    const long long plane = (long long)a.Nq2 * a.Nq1;
+    if (a.mom_out) {
+        for (int c = tid; c < L::NQ * kNumMom; c += NTHREADS) {
+            int cq = c / kNumMom, q = c % kNumMom;
+            int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
+            if (ii < a.Nq1 && jj < a.Nq2)
+                a.mom_out[(((long long)split * kNumMom + q) * a.Ns + s) * plane
+                          + (long long)jj * a.Nq1 + ii] = mom_acc[c];
+        }
+    }
+    if (a.want_j && a.j_out) {
+        for (int c = tid; c < L::NQ * 3; c += NTHREADS) {
+            int cq = c / 3, q = c % 3;
+            int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
+            if (ii < a.Nq1 && jj < a.Nq2)
+                a.j_out[(((long long)split * 3 + q) * a.Ns + s) * plane
+                        + (long long)jj * a.Nq1 + ii] = j_acc[c];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// p-stage kernel (fields enabled): one CTA per (interior q-cell, species)
+// holds the whole p-block in shared memory.
+//   k = k_q + (-(d1 + d2 + d3)),  d_a = (F_a(right) - F_a(left)) * (1/dp_a)
+// (df_dt_fvm.py:245-323), with circular neighbours along each p axis, C_p
+// from the cell-centred fields (advection_terms.py:147-188), then the RK
+// combine and the FP64 moments of out1 (full sums: nsplit = 1).
+// ---------------------------------------------------------------------------
+
+template <int RECON, bool EXACT, typename T>
+__device__ __forceinline__ T p_face_flux(const T* fb, int c, int stride, int n, int pos,
+                                         T C, const Weno5Side<T>& Sr, const Weno5Side<T>& Sl) {
+    // flux at the left face of cell `c` along an axis with `n` cells; `pos` =
+    // the cell's index along that axis; neighbours wrap within the axis
+    const bool right = C > T(0);
+    const int off = right ? -3 : -2;          // window start relative to the cell
+    T y[5];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        int q = pos + off + t;
+        q = ((q % n) + n) % n;
+        y[t] = fb[c + (q - pos) * stride];
+    }
+    T fv = face_value<RECON, EXACT>(y[0], y[1], y[2], y[3], y[4], right, right ? Sr : Sl);
+    return C * fv;
+}
+
+template <typename T, bool EXACT, int RECON>
+__global__ void __launch_bounds__(PTHREADS)
+pstage_kernel(const __grid_constant__ PStageArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* fb = reinterpret_cast<T*>(smem_raw);      // [Np]
+    T* F = fb + a.Np;                            // [Np] face fluxes of one axis
+    T* d1 = F + a.Np;                            // [Np]
+    T* d2 = d1 + a.Np;                           // [Np]
+    __shared__ double red[PTHREADS / 32][kNumMom];
+
+    const int tid = threadIdx.x;
+    const int ii = blockIdx.x % a.Nq1, jj = blockIdx.x / a.Nq1, s = blockIdx.y;
+    const long long rowstride = (long long)a.Ns * a.Np;
+    const long long colstride = rowstride * a.Nq1g;
+    const long long cbase = (long long)(jj + a.Ng) * colstride + (long long)(ii + a.Ng) * rowstride
+                          + (long long)s * a.Np;
+    const T* fs = static_cast<const T*>(a.fs);
+    for (int c = tid; c < a.Np; c += PTHREADS) fb[c] = fs[cbase + c];
+    const long long plane_g = (long long)a.Nq2g * a.Nq1g;
+    const long long qg = (long long)(jj + a.Ng) * a.Nq1g + (ii + a.Ng);
+    const double E1 = a.cell[0 * plane_g + qg], E2 = a.cell[1 * plane_g + qg];
+    const double E3 = a.cell[2 * plane_g + qg], B1 = a.cell[3 * plane_g + qg];
+    const double B2 = a.cell[4 * plane_g + qg], B3 = a.cell[5 * plane_g + qg];
+    const double em = a.sg.charge[s] / a.sg.mass[s];
+    Weno5Side<T> Sr, Sl;
+    Sr.set(true);
+    Sl.set(false);
+    __syncthreads();
+
+    const int n1 = a.Np1, n2 = a.Np2, n3 = a.Np3;
+    // three axes; an axis with a single cell contributes exactly zero
+    for (int ax = 0; ax < 3; ++ax) {
+        const int n = ax == 0 ? n1 : (ax == 1 ? n2 : n3);
+        if (n == 1) continue;
+        const int stride = ax == 0 ? 1 : (ax == 1 ? n1 : n1 * n2);
+        for (int c = tid; c < a.Np; c += PTHREADS) {
+            const int i1 = c % n1, i2 = (c / n1) % n2, i3 = c / (n1 * n2);
+            const double v1 = a.sg.p1_start[s] + (0.5 + i1) * a.sg.dp1[s];
+            const double v2 = a.sg.p2_start[s] + (0.5 + i2) * a.sg.dp2[s];
+            const double v3 = a.sg.p3_start[s] + (0.5 + i3) * a.sg.dp3[s];
+            double C;
+            int pos;
+            if (ax == 0) { C = em * ((E1 + v2 * B3) - v3 * B2); pos = i1; }
+            else if (ax == 1) { C = em * ((E2 + v3 * B1) - v1 * B3); pos = i2; }
+            else { C = em * ((E3 + v1 * B2) - v2 * B1); pos = i3; }
+            F[c] = p_face_flux<RECON, EXACT>(fb, c, stride, n, pos, T(C), Sr, Sl);
+        }
+        __syncthreads();
+        const double dp = ax == 0 ? a.sg.dp1[s] : (ax == 1 ? a.sg.dp2[s] : a.sg.dp3[s]);
+        const T inv = T(1.0 / dp);
+        T* dst = ax == 0 ? d1 : (ax == 1 ? d2 : F + 0);
+        if (ax < 2) {
+            for (int c = tid; c < a.Np; c += PTHREADS) {
+                const int pos = ax == 0 ? c % n1 : (c / n1) % n2;
+                const int cn = pos + 1 < n ? c + stride : c - (n - 1) * stride;
+                dst[c] = (F[cn] - F[c]) * inv;
+            }
+        }
+        if (ax == 2) {
+            // keep d3 in F's slot: compute into d-registers below
+        }
+        __syncthreads();
+        if (ax == 2) break;
+    }
+    // final combine; d3 is computed from F when the p3 axis is active
+    T* out1 = static_cast<T*>(a.out1);
+    T* out2 = static_cast<T*>(a.out2);
+    const T* base1 = static_cast<const T*>(a.base1);
+    const T* base2 = static_cast<const T*>(a.base2);
+    const T* kq = static_cast<const T*>(a.kq);
+    double macc[kNumMom] = {0, 0, 0, 0, 0};
+    const T c1 = T(a.c1), c2 = T(a.c2);
+    for (int c = tid; c < a.Np; c += PTHREADS) {
+        const int i1 = c % n1, i2 = (c / n1) % n2, i3 = c / (n1 * n2);
+        T t1 = n1 > 1 ? d1[c] : T(0);
+        T t2 = n2 > 1 ? d2[c] : T(0);
+        T t3 = T(0);
+        if (n3 > 1) {
+            const int cn = i3 + 1 < n3 ? c + n1 * n2 : c - (n3 - 1) * n1 * n2;
+            t3 = (F[cn] - F[c]) * T(1.0 / a.sg.dp3[s]);
+        }
+        const long long g = cbase + c;
+        T kk = kq[g] + (-((t1 + t2) + t3));
+        T o1 = base1 ? base1[g] + kk * c1 : kk;
+        out1[g] = o1;
+        if (out2) out2[g] = base2[g] + kk * c2;
+        if ((a.periodic1 && (ii < a.Ng || ii >= a.Nq1 - a.Ng)) ||
+            (a.periodic2 && (jj < a.Ng || jj >= a.Nq2 - a.Ng)))
+            write_ghost_images(out1, o1, ii, jj, s, c, a.Ng, a.Nq1, a.Nq2, a.Nq1g, a.Nq2g,
+                               a.periodic1, a.periodic2, rowstride, colstride, a.Np);
+        if (a.flag && !isfinite(double(o1))) atomicOr(a.flag, 1);
+        if (a.mom_out) {
+            const PVel V = lane_velocity(a.sg, s, i1, i2, i3);
+            const double ov = double(o1);
+            macc[0] += ov; macc[1] += ov * V.v1; macc[2] += ov * V.v2; macc[3] += ov * V.v3;
+            macc[4] += (0.5 * ov) * V.vsq;
+        }
+    }
+    if (a.mom_out) {
+        const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+        for (int q = 0; q < kNumMom; ++q) {
+            double v = warp_sum(macc[q]);
+            if (lane == 0) red[warp][q] = v;
+        }
+        __syncthreads();
+        if (tid < kNumMom) {
+            double v = 0.0;
+            for (int w = 0; w < PTHREADS / 32; ++w) v += red[w][tid];
+            const long long plane = (long long)a.Nq2 * a.Nq1;
+            a.mom_out[((long long)tid * a.Ns + s) * plane + (long long)jj * a.Nq1 + ii] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// moments (compute_moments.py:7-59 with moments.py:6-58), FP64 output.
+// One CTA per (ghosted q-cell, species).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256)
+moment_kernel(const T* f, int mid, double* out, int Ns, int Np1, int Np2, int Np3, int Nq1g,
+              int Nq2g, SpeciesGrid sg) {
+    __shared__ double red[8];
+    const int q = blockIdx.x, s = blockIdx.y, tid = threadIdx.x;
+    const int Np = Np1 * Np2 * Np3;
+    const T* fp = f + ((long long)q * Ns + s) * Np;
+    double acc = 0.0;
+    for (int c = tid; c < Np; c += 256) {
+        const int i1 = c % Np1, i2 = (c / Np1) % Np2, i3 = c / (Np1 * Np2);
+        const PVel V = lane_velocity(sg, s, i1, i2, i3);
+        const double fv = double(fp[c]);
+        double g;
+        switch (mid) {
+            case 0: g = fv; break;
+            case 1: g = fv * V.v1; break;
+            case 2: g = fv * V.v2; break;
+            case 3: g = fv * V.v3; break;
+            case 4: g = (0.5 * fv) * V.vsq; break;
+            case 5: g = (0.5 * fv) * (V.v1 * V.v1); break;
+            case 6: g = (0.5 * fv) * (V.v2 * V.v2); break;
+            case 7: g = (0.5 * fv) * (V.v3 * V.v3); break;
+            case 8: g = (fv * V.v1) * V.vsq; break;
+            case 9: g = (fv * V.v2) * V.vsq; break;
+            default: g = (fv * V.v3) * V.vsq; break;
+        }
+        acc += g;
+    }
+    acc = warp_sum(acc);
+    if ((tid & 31) == 0) red[tid >> 5] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        double v = 0.0;
+        for (int w = 0; w < 8; ++w) v += red[w];
+        const double measure = (sg.dp3[s] * sg.dp2[s]) * sg.dp1[s];
+        out[(long long)q * Ns + s] = v * measure;
+    }
+}
+
+// The five BGK moments of the interior cells as one "split" of partial sums
+// ([1][5][Ns][Nq2][Nq1], sums without the measure factor).
+template <typename T>
+__global__ void __launch_bounds__(256)
+moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int Nq1, int Nq2,
+                int Ng, SpeciesGrid sg) {
+    __shared__ double red[8][kNumMom];
+    const int q = blockIdx.x, s = blockIdx.y, tid = threadIdx.x;
+    const int ii = q % Nq1, jj = q / Nq1;
+    const int Np = Np1 * Np2 * Np3;
+    const int Nq1g = Nq1 + 2 * Ng;
+    const T* fp = f + (((long long)(jj + Ng) * Nq1g + (ii + Ng)) * Ns + s) * Np;
+    double acc[kNumMom] = {0, 0, 0, 0, 0};
+    for (int c = tid; c < Np; c += 256) {
+        const int i1 = c % Np1, i2 = (c / Np1) % Np2, i3 = c / (Np1 * Np2);
+        const PVel V = lane_velocity(sg, s, i1, i2, i3);
+        const double fv = double(fp[c]);
+        acc[0] += fv; acc[1] += fv * V.v1; acc[2] += fv * V.v2; acc[3] += fv * V.v3;
+        acc[4] += (0.5 * fv) * V.vsq;
+    }
+#pragma unroll
+    for (int m = 0; m < kNumMom; ++m) {
+        double v = warp_sum(acc[m]);
+        if ((tid & 31) == 0) red[tid >> 5][m] = v;
+    }
+    __syncthreads();
+    if (tid < kNumMom) {
+        double v = 0.0;
+        for (int w = 0; w < 8; ++w) v += red[w][tid];
+        part[((long long)tid * Ns + s) * Nq2 * Nq1 + (long long)jj * Nq1 + ii] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// halo refresh: communicate_f (periodic wrap; ghosted halos are zero) then
+// apply_bcs_f's Dirichlet inflow selects in the order left, right, bottom,
+// top (boundaries.py:415-577, :147-225).  One thread per (ghost cell, s, p).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const T* dt,
+                             int Nq1, int Nq2, int Ng, int Ns, int Np, int Np1, int Np2,
+                             int per1, int per2, int dir1, int dir2, SpeciesGrid sg,
+                             long long nghost_cells) {
+    const int Nq1g = Nq1 + 2 * Ng;
+    const long long rowstride = (long long)Ns * Np;
+    const long long colstride = rowstride * Nq1g;
+    const long long total = nghost_cells * rowstride;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long gc = t / rowstride;
+        const int sp = int(t % rowstride);
+        const int s = sp / Np, p = sp % Np;
+        // enumerate ghost cells: rows [0,Ng) and [Nq2+Ng, Nq2g) full width, then
+        // the left/right ghost columns of the interior rows
+        int g1, g2;
+        const long long nrow = (long long)Ng * Nq1g;
+        if (gc < 2 * nrow) {
+            const int r = int(gc / Nq1g), c = int(gc % Nq1g);
+            g2 = r < Ng ? r : Nq2 + r;          // r in [Ng, 2Ng) -> Nq2+Ng .. Nq2+2Ng-1
+            g1 = c;
+        } else {
+            const long long rem = gc - 2 * nrow;
+            const int r = int(rem / (2 * Ng)), c = int(rem % (2 * Ng));
+            g2 = Ng + r;
+            g1 = c < Ng ? c : Nq1 + c;
+        }
+        const int i = g1 - Ng, j = g2 - Ng;
+        const bool in1 = i >= 0 && i < Nq1, in2 = j >= 0 && j < Nq2;
+        T v = T(0);
+        if ((in1 || per1) && (in2 || per2)) {
+            const int si = ((i % Nq1) + Nq1) % Nq1, sj = ((j % Nq2) + Nq2) % Nq2;
+            v = f[(long long)(sj + Ng) * colstride + (long long)(si + Ng) * rowstride + sp];
+        }
+        const long long g = (long long)g2 * colstride + (long long)g1 * rowstride + sp;
+        const int i1 = p % Np1, i2 = (p / Np1) % Np2;
+        const double v1 = sg.p1_start[s] + (0.5 + i1) * sg.dp1[s];
+        const double v2 = sg.p2_start[s] + (0.5 + i2) * sg.dp2[s];
+        if (dir1 && i < 0 && v1 > 0) v = dl[g];
+        if (dir1 && i >= Nq1 && v1 < 0) v = dr[g];
+        if (dir2 && j < 0 && v2 > 0) v = db[g];
+        if (dir2 && j >= Nq2 && v2 < 0) v = dt[g];
+        f[g] = v;
+    }
+}
+
+}  // namespace bolt

@@ -1,0 +1,65 @@
+// launch.h - host-side launchers of the FVM kernels, one set per dtype.
+// Implemented in kernels_f64.cu (FP64, reference operation order, no FMA
+// contraction) and kernels_f32.cu (FP32 fast path).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fvm_args.h"
+
+namespace bolt {
+
+enum Tiling { TILING_2D = 0, TILING_1D = 1, TILING_1D_Q2 = 2 };
+
+struct TileShape {
+    int tq1, tq2, q2;
+};
+
+inline TileShape tile_shape(int tiling) {
+    switch (tiling) {
+        case TILING_2D: return {8, 8, 1};
+        case TILING_1D: return {64, 1, 0};
+        default: return {64, 1, 1};
+    }
+}
+
+// bytes of dynamic shared memory of the q-stage kernel
+inline size_t qstage_smem(int tiling, size_t elem, int bgk, int bgk_direct, int ntab) {
+    TileShape t = tile_shape(tiling);
+    const size_t hx = t.tq1 + 2 * HALO, hy = t.q2 ? t.tq2 + 2 * HALO : 1;
+    const size_t tile = hy * hx * PW;
+    const size_t nq = (size_t)t.tq1 * t.tq2;
+    size_t b = 2 * tile * elem + nq * PW * elem;
+    b += nq * (kNumMom + 3 + 5) * sizeof(double);
+    if (bgk && !bgk_direct) b += nq * (size_t)ntab * sizeof(double);
+    b += 2 * sizeof(uint64_t);
+    return b;
+}
+
+inline size_t pstage_smem(int Np, size_t elem) { return 4 * (size_t)Np * elem; }
+
+#define BOLT_DECLARE_LAUNCHERS(SUFFIX, T)                                                   \
+    cudaError_t launch_qstage_##SUFFIX(const QStageArgs& a, int recon, int tiling, int bgk, \
+                                       dim3 grid, size_t smem, cudaStream_t st);            \
+    cudaError_t launch_pstage_##SUFFIX(const PStageArgs& a, int recon, dim3 grid,           \
+                                       size_t smem, cudaStream_t st);                       \
+    cudaError_t launch_moment_##SUFFIX(const void* f, int mid, double* out, int Ns,          \
+                                       int Np1, int Np2, int Np3, int Nq1g, int Nq2g,        \
+                                       const SpeciesGrid& sg, cudaStream_t st);             \
+    cudaError_t launch_moments5_##SUFFIX(const void* f, double* part, int Ns, int Np1,       \
+                                         int Np2, int Np3, int Nq1, int Nq2, int Ng,         \
+                                         const SpeciesGrid& sg, cudaStream_t st);           \
+    cudaError_t launch_ghost_##SUFFIX(void* f, const void* dl, const void* dr,               \
+                                      const void* db, const void* dt, int Nq1, int Nq2,      \
+                                      int Ng, int Ns, int Np, int Np1, int Np2, int per1,    \
+                                      int per2, int dir1, int dir2, const SpeciesGrid& sg,   \
+                                      cudaStream_t st);
+
+BOLT_DECLARE_LAUNCHERS(f64, double)
+BOLT_DECLARE_LAUNCHERS(f32, float)
+
+// FDTD sequence (FP64): prepare -> halo -> E -> halo -> B -> to_cell
+cudaError_t launch_fdtd(const FieldArgs& a, cudaStream_t st, long long* launches);
+cudaError_t launch_field_halo(const FieldArgs& a, cudaStream_t st);
+
+}  // namespace bolt

@@ -1,0 +1,174 @@
+/*
+ * bolt_b200.h - C ABI of the B200 (sm_100a) finite-volume kinetic update.
+ *
+ * One context per device per solver.  All device buffers passed in are owned
+ * by the caller (PyTorch tensors in the Python layer); the context owns its
+ * scratch (RK stage buffers, moment partial sums, Yee/cell field arrays).
+ * Every call is asynchronous on the CUDA stream it is given; nothing here
+ * synchronises the host except bolt_status_sync().
+ *
+ * Distribution-function layout (identical to Bolt's q-expanded array, which is
+ * column-major (N_p1*N_p2*N_p3, N_s, N_q1+2Ng, N_q2+2Ng)):
+ *     f[q2g][q1g][s][p3][p2][p1]   row-major, p1 fastest, ghost zones included
+ * Moments (FP64):  m[q2g][q1g][s]
+ * Fields  (FP64):  fld[c][q2g][q1g], c = E1,E2,E3,B1,B2,B3
+ *
+ * Reference interfaces replaced (paths within the Bolt project):
+ *   bolt_ctx_create      nonlinear_solver.__init__   bolt/lib/nonlinear/nonlinear_solver.py:67-413
+ *   bolt_fill_ghosts     communicate_f + apply_bcs_f bolt/lib/nonlinear/communicate.py:8-38,
+ *                                                    bolt/lib/nonlinear/boundaries.py:415-577
+ *   bolt_dfdt            df_dt_fvm                   bolt/lib/nonlinear/finite_volume/df_dt_fvm.py:33-339
+ *   bolt_step            op_fvm / timestep_fvm       bolt/lib/nonlinear/finite_volume/fvm_operator.py:6-50
+ *                        (RK4 stages: bolt/lib/nonlinear/temporal_evolution/integrators.py:15-28)
+ *   bolt_moments         compute_moments             bolt/lib/nonlinear/compute_moments.py:7-59
+ *   bolt_fields_set/get  fields_solver state         bolt/lib/nonlinear/fields/fields.py:421-495,649-690
+ *   bolt_divergence_flag check_divergence            bolt/lib/nonlinear/timestep.py:28-38
+ */
+#ifndef BOLT_B200_H
+#define BOLT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BOLT_MAX_SPECIES 8
+
+/* status codes */
+#define BOLT_OK                 0
+#define BOLT_ERR_ARG            1   /* bad argument / unsupported combination */
+#define BOLT_ERR_CUDA           2   /* a CUDA runtime/driver call failed        */
+#define BOLT_ERR_NONFINITE      3   /* Inf/NaN appeared in f ('Solver Diverging!') */
+#define BOLT_ERR_TIMEOUT        4   /* a bounded device-side wait gave up       */
+#define BOLT_ERR_UNSUPPORTED    5   /* shape/option outside this build's kernels */
+#define BOLT_ERR_NOMEM          6
+
+/* dtype of f */
+#define BOLT_F64 0
+#define BOLT_F32 1
+
+/* reconstruction (reconstruct.py:29-44) */
+#define BOLT_RECON_PC     0   /* 'piecewise-constant' */
+#define BOLT_RECON_MINMOD 1   /* 'minmod'             */
+#define BOLT_RECON_PPM    2   /* 'ppm'                */
+#define BOLT_RECON_WENO5  3   /* 'weno5'              */
+
+/* numerical flux (riemann.py:46-49; LLF as north-star extension) */
+#define BOLT_FLUX_UPWIND 0
+#define BOLT_FLUX_LLF    1
+
+/* boundary conditions along q1/q2 (boundaries.py:415-577) */
+#define BOLT_BC_PERIODIC  0
+#define BOLT_BC_DIRICHLET 1
+
+/* integrators */
+#define BOLT_RK2 2   /* fvm_operator.py:6-35 midpoint */
+#define BOLT_RK4 4   /* classic RK4 around df_dt_fvm  */
+
+/* moment ids (moments.py:6-58) */
+#define BOLT_MOM_DENSITY   0
+#define BOLT_MOM_V1        1
+#define BOLT_MOM_V2        2
+#define BOLT_MOM_V3        3
+#define BOLT_MOM_ENERGY    4
+#define BOLT_MOM_ENERGY_Q1 5
+#define BOLT_MOM_ENERGY_Q2 6
+#define BOLT_MOM_ENERGY_Q3 7
+#define BOLT_MOM_Q_Q1      8
+#define BOLT_MOM_Q_Q2      9
+#define BOLT_MOM_Q_Q3     10
+
+typedef struct BoltGrid {
+    int    N_q1, N_q2, N_ghost;
+    int    N_p1, N_p2, N_p3, N_s;
+    double q1_start, q2_start, dq1, dq2;
+    double p1_start[BOLT_MAX_SPECIES], p2_start[BOLT_MAX_SPECIES], p3_start[BOLT_MAX_SPECIES];
+    double dp1[BOLT_MAX_SPECIES], dp2[BOLT_MAX_SPECIES], dp3[BOLT_MAX_SPECIES];
+} BoltGrid;
+
+typedef struct BoltParams {
+    int    dtype;                 /* BOLT_F64 / BOLT_F32                       */
+    int    recon_q, recon_p;      /* BOLT_RECON_*                              */
+    int    flux_q, flux_p;        /* BOLT_FLUX_*                               */
+    int    bc_q1, bc_q2;          /* BOLT_BC_*                                 */
+    int    integrator;            /* BOLT_RK2 / BOLT_RK4                       */
+    int    source_enabled;        /* BGK relaxation on/off                     */
+    int    fields_enabled;        /* electrodynamic FDTD coupling on/off       */
+    int    p_dim;                 /* 1, 2 or 3                                 */
+    double mass[BOLT_MAX_SPECIES], charge[BOLT_MAX_SPECIES];
+    double boltzmann_constant;
+    double tau;                   /* constant BGK tau (see bolt_set_tau_array) */
+    double eps, mu;               /* FDTD permittivity / permeability          */
+} BoltParams;
+
+typedef struct BoltCtx BoltCtx;
+
+/* Context lifetime.  Allocates the RK scratch on the current device. */
+int  bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** out);
+void bolt_ctx_destroy(BoltCtx* ctx);
+
+/* Optional phase-space-dependent tau: f-shaped device array of the same dtype
+ * as f (caller-owned, must outlive the context).  NULL restores the constant. */
+int  bolt_set_tau_array(BoltCtx* ctx, const void* tau_dev);
+
+/* Dirichlet boundary values for side 0=left,1=right,2=bottom,3=top: an
+ * f-shaped device array of boundary-function values (caller-owned).  Ghost
+ * cells take these values where the q-velocity points into the domain and
+ * zero elsewhere (boundaries.py:147-225; PETSc ghosted halos stay zero). */
+int  bolt_set_dirichlet(BoltCtx* ctx, int side, const void* values_dev);
+
+/* Halo refresh of f in place (periodic wrap + Dirichlet inflow). */
+int  bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream);
+
+/* Forget cached halo/moment state (call after f was modified outside the
+ * library; bolt_step then refreshes halos and moments before stepping). */
+int  bolt_invalidate(BoltCtx* ctx);
+
+/* df/dt of f (ghosts must be current) into dfdt (interior cells written).
+ * With fields enabled, evolve_fields != 0 first advances the fields with the
+ * currents of this f (the reference's at_n == False branch). */
+int  bolt_dfdt(BoltCtx* ctx, const void* f_dev, void* dfdt_dev, int evolve_fields,
+               double dt, void* stream);
+
+/* One full RK step of f in place (ghosts refreshed by the call). */
+int  bolt_step(BoltCtx* ctx, void* f_dev, double dt, void* stream);
+
+/* n_steps RK steps, ghosts refreshed, launched back to back. */
+int  bolt_run(BoltCtx* ctx, void* f_dev, double dt, int n_steps, void* stream);
+
+/* One moment (BOLT_MOM_*) of f over the whole ghosted grid, FP64, written to
+ * out_dev[q2g][q1g][s] (moments.py definitions times dp1*dp2*dp3). */
+int  bolt_moments(BoltCtx* ctx, const void* f_dev, int moment_id, double* out_dev, void* stream);
+
+/* Fields state (FP64 device arrays of 6*Nq2g*Nq1g doubles). */
+int  bolt_fields_set(BoltCtx* ctx, const double* cell_dev, const double* yee_dev, void* stream);
+int  bolt_fields_get(BoltCtx* ctx, double* cell_dev, double* yee_dev, void* stream);
+
+/* FDTD time-level flag of the reference's fields solver (fields.py:271-273,
+ * 685-688): each df/dt evaluation flips it; a stage evolves the fields when it
+ * is 0 on entry (RK2).  RK4 evolves in stage 2 and leaves it unchanged. */
+int  bolt_get_at_n(BoltCtx* ctx);
+int  bolt_set_at_n(BoltCtx* ctx, int at_n);
+
+/* Divergence flag: device-side Inf/NaN detection on every step's output,
+ * written to pinned host memory.  Returns 1 once any step produced a
+ * non-finite value (no synchronisation), 0 otherwise. */
+int  bolt_divergence_flag(BoltCtx* ctx);
+int  bolt_clear_divergence_flag(BoltCtx* ctx);
+
+/* Synchronise the stream and return the first sticky error of the context. */
+int  bolt_status_sync(BoltCtx* ctx, void* stream);
+const char* bolt_strerror(int code);
+
+/* Number of kernels launched through this context so far. */
+long long bolt_launch_count(BoltCtx* ctx);
+
+/* Bytes of device scratch held by the context. */
+size_t bolt_scratch_bytes(BoltCtx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BOLT_B200_H */
