@@ -11,6 +11,35 @@ constexpr int PW = 32;          // p-cells per chunk (one per lane)
 constexpr int HALO = 3;         // q-stencil half width incl. face shift
 constexpr int NTHREADS = 256;   // q-stage CTA size (8 warps)
 constexpr int kNumMom = 5;      // n, mom_v1, mom_v2, mom_v3, energy
+constexpr int PWP = PW + 1;     // padded stage-buffer row (conflict-free column reads)
+
+// Shared-memory carve-up of the q-stage kernel (byte offsets), used by the
+// kernel and by the host to size the launch.
+struct QLayout {
+    unsigned tile, stage, vtab, jacc, qc, tabs, bars, total;
+};
+
+__host__ __device__ inline unsigned qalign(unsigned x, unsigned a) { return (x + a - 1) / a * a; }
+
+__host__ __device__ inline QLayout qstage_layout(int tq1, int tq2, int q2, int elem, int bgk,
+                                                 int bgk_direct, int ntab) {
+    QLayout L;
+    const unsigned hx = tq1 + 2 * HALO, hy = q2 ? tq2 + 2 * HALO : 1;
+    const unsigned nq = tq1 * tq2;
+    unsigned o = 0;
+    L.tile = o;  o += qalign(2u * hy * hx * PW * elem, 128);
+    // the epilogue reuses the tile region for the cross-thread moment reduction
+    const unsigned red = (unsigned)(NTHREADS * kNumMom * sizeof(double));
+    if (o < red) o = qalign(red, 128);
+    L.stage = o; o += qalign(nq * PWP * elem, 16);
+    L.vtab = o;  o += 4 * PW * sizeof(double);
+    L.jacc = o;  o += nq * 3 * sizeof(double);
+    L.qc = o;    o += nq * 5 * sizeof(double);
+    L.tabs = o;  o += (bgk && !bgk_direct) ? nq * ntab * sizeof(double) : 0;
+    L.bars = o;  o += 2 * sizeof(unsigned long long);
+    L.total = o;
+    return L;
+}
 
 struct SpeciesGrid {
     double p1_start[kMaxSpecies], p2_start[kMaxSpecies], p3_start[kMaxSpecies];

@@ -54,8 +54,12 @@ template <> struct Consts<float> {
 template <typename T>
 struct Weno5Side {
     T num1, den1, num2, den2, num3, den3;      // w_k = num_k / ((den_k*beta_k)*beta_k)
+    T cw1, cw2, cw3;                           // num_k / den_k (fast path)
     T a10, a11, a12, a20, a21, a22, a30, a31, a32;  // u_k = (a_k0 y + a_k1 y) + a_k2 y
     __device__ __forceinline__ void set(bool right) {
+        cw2 = T(0.625);
+        cw1 = right ? T(0.0625) : T(0.3125);
+        cw3 = right ? T(0.3125) : T(0.0625);
         if (right) {
             num1 = T(1); den1 = T(16); num2 = T(5); den2 = T(8); num3 = T(5); den3 = T(16);
             a10 = T(0.375);  a11 = T(-1.25); a12 = T(1.875);
@@ -108,10 +112,9 @@ __device__ __forceinline__ float weno5_fast(float y0, float y1, float y2, float 
     float r1 = fast_rcp(weno_beta_fast(y0, y1, y2));
     float r2 = fast_rcp(weno_beta_fast(y1, y2, y3));
     float r3 = fast_rcp(weno_beta_fast(y2, y3, y4));
-    // num/den folded into a single scale per weight
-    float w1 = (S.num1 / S.den1) * r1 * r1;
-    float w2 = (S.num2 / S.den2) * r2 * r2;
-    float w3 = (S.num3 / S.den3) * r3 * r3;
+    float w1 = S.cw1 * r1 * r1;
+    float w2 = S.cw2 * r2 * r2;
+    float w3 = S.cw3 * r3 * r3;
     float u1 = fmaf(S.a12, y2, fmaf(S.a11, y1, S.a10 * y0));
     float u2 = fmaf(S.a22, y3, fmaf(S.a21, y2, S.a20 * y1));
     float u3 = fmaf(S.a32, y4, fmaf(S.a31, y3, S.a30 * y2));

@@ -31,15 +31,6 @@
 
 namespace bolt {
 
-// smem layout of the q-stage kernel
-template <typename T, int TQ1, int TQ2, bool Q2>
-struct QSmem {
-    static constexpr int HX = TQ1 + 2 * HALO;
-    static constexpr int HY = Q2 ? TQ2 + 2 * HALO : 1;
-    static constexpr int TILE = HY * HX * PW;          // elements per buffer
-    static constexpr int NQ = TQ1 * TQ2;               // q-cells per tile
-};
-
 // ---------------------------------------------------------------------------
 // moment contributions of one value (FP64), reference moments.py:6-24
 // ---------------------------------------------------------------------------
@@ -78,21 +69,36 @@ __device__ __forceinline__ void write_ghost_images(T* out, T v, int ii, int jj, 
 
 // ---------------------------------------------------------------------------
 // q-stage kernel
+//
+// Per p-chunk (32 consecutive p of one species) and q-tile:
+//   phase A  q1 faces: one upwind face value per face, walking each tile row
+//            with a sliding window; D1 = (-(F_R - F_L)) / dq1 -> stage buffer
+//   phase B  q2 faces likewise, BGK, RK combine; writes out1/out2 to global
+//            and out1 back into the stage buffer
+//   phase C  FP64 moments of out1 from the stage buffer: each thread owns one
+//            q-cell and a quarter of the chunk's p values, accumulating in
+//            registers across all chunks of the CTA (reduced once at the end)
 // ---------------------------------------------------------------------------
 template <typename T, bool EXACT, int RECON, int TQ1, int TQ2, bool Q2, bool BGK>
-__global__ void __launch_bounds__(NTHREADS)
+__global__ void __launch_bounds__(NTHREADS, 2)
 qstage_kernel(const __grid_constant__ QStageArgs a) {
-    typedef QSmem<T, TQ1, TQ2, Q2> L;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    T* tile = reinterpret_cast<T*>(smem_raw);                        // [2][HY][HX][PW]
-    T* D1 = tile + 2 * L::TILE;                                       // [TQ2][TQ1][PW]
-    double* mom_acc = reinterpret_cast<double*>(D1 + L::NQ * PW);     // [NQ][5]
-    double* j_acc = mom_acc + L::NQ * kNumMom;                        // [NQ][3]
-    double* qc = j_acc + L::NQ * 3;                                   // [NQ][5] n*A,u1,u2,u3,2kT
-    double* tabs = qc + L::NQ * 5;                                    // [NQ][Np1+Np2+Np3]
+    constexpr int HX = TQ1 + 2 * HALO;
+    constexpr int HY = Q2 ? TQ2 + 2 * HALO : 1;
+    constexpr int NQ = TQ1 * TQ2;
+    constexpr int NQUART = NTHREADS / NQ;       // threads per q-cell in phase C
+    constexpr int PQ = PW / NQUART;             // p values per phase-C thread
+    static_assert(NTHREADS % NQ == 0 && PW % NQUART == 0, "phase C mapping");
     const int ntab = a.Np1 + a.Np2 + a.Np3;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(
-        tabs + ((BGK && !a.bgk_direct) ? L::NQ * ntab : 0));
+    const QLayout Lo = qstage_layout(TQ1, TQ2, Q2, sizeof(T), BGK, a.bgk_direct, ntab);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* tile = reinterpret_cast<T*>(smem_raw + Lo.tile);          // [2][HY][HX][PW]
+    T* stage = reinterpret_cast<T*>(smem_raw + Lo.stage);        // [NQ][PWP]
+    double* vtab = reinterpret_cast<double*>(smem_raw + Lo.vtab);   // [4][PW]
+    double* j_acc = reinterpret_cast<double*>(smem_raw + Lo.jacc);  // [NQ][3]
+    double* qc = reinterpret_cast<double*>(smem_raw + Lo.qc);       // [NQ][5]
+    double* tabs = reinterpret_cast<double*>(smem_raw + Lo.tabs);   // [NQ][ntab]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + Lo.bars);
+    constexpr int TILE = HY * HX * PW;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
@@ -105,8 +111,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     const long long colstride = rowstride * a.Nq1g;                   // per q2 step
     const T* fs = static_cast<const T*>(a.fs);
 
-    for (int c = tid; c < L::NQ * kNumMom; c += NTHREADS) mom_acc[c] = 0.0;
-    for (int c = tid; c < L::NQ * 3; c += NTHREADS) j_acc[c] = 0.0;
+    for (int c = tid; c < NQ * 3; c += NTHREADS) j_acc[c] = 0.0;
     if (tid == 0 && a.use_tma) {
         prefetch_tmap(&a.tmap);
         mbar_init(&bars[0], 1);
@@ -121,14 +126,17 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         const double kB = a.kB;
         const double measure = (a.sg.dp3[s] * a.sg.dp2[s]) * a.sg.dp1[s];
         const long long plane = (long long)a.Nq2 * a.Nq1;
-        for (int c = tid; c < L::NQ; c += NTHREADS) {
+        // moment sums of the stage input: 5 threads per q-cell
+        for (int c = tid; c < NQ; c += NTHREADS) {
             int ii = i0 + c % TQ1, jj = j0 + c / TQ1;
             double mm[kNumMom] = {0, 0, 0, 0, 0};
             if (ii < a.Nq1 && jj < a.Nq2) {
-                for (int sp = 0; sp < a.nsplit_in; ++sp)
+                for (int sp = 0; sp < a.nsplit_in; ++sp) {
+#pragma unroll
                     for (int q = 0; q < kNumMom; ++q)
                         mm[q] += a.mom_in[(((long long)sp * kNumMom + q) * a.Ns + s) * plane
                                           + (long long)jj * a.Nq1 + ii];
+                }
             }
             const double eps = 1e-30;
             double n = mm[0] * measure;
@@ -147,22 +155,26 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
             qc[c * 5 + 2] = u2;
             qc[c * 5 + 3] = u3;
             qc[c * 5 + 4] = twokT;
-            if (a.bgk_direct) continue;
-            double* tb = tabs + (long long)c * ntab;
-            for (int q = 0; q < a.Np1; ++q) {
-                double v = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
-                double dv = v - u1;
-                tb[q] = exp((-m * (dv * dv)) / twokT);
-            }
-            for (int q = 0; q < a.Np2; ++q) {
-                double v = a.sg.p2_start[s] + (0.5 + q) * a.sg.dp2[s];
-                double dv = v - u2;
-                tb[a.Np1 + q] = a.p_dim >= 2 ? exp((-m * (dv * dv)) / twokT) : 1.0;
-            }
-            for (int q = 0; q < a.Np3; ++q) {
-                double v = a.sg.p3_start[s] + (0.5 + q) * a.sg.dp3[s];
-                double dv = v - u3;
-                tb[a.Np1 + a.Np2 + q] = a.p_dim == 3 ? exp((-m * (dv * dv)) / twokT) : 1.0;
+        }
+        __syncthreads();
+        if (!a.bgk_direct) {
+            // exp tables: all threads over (q-cell, table entry)
+            for (int e = tid; e < NQ * ntab; e += NTHREADS) {
+                const int c = e / ntab, q = e % ntab;
+                const double* qq = qc + c * 5;
+                double v, u;
+                bool act;
+                if (q < a.Np1) {
+                    v = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s]; u = qq[1]; act = true;
+                } else if (q < a.Np1 + a.Np2) {
+                    int t = q - a.Np1;
+                    v = a.sg.p2_start[s] + (0.5 + t) * a.sg.dp2[s]; u = qq[2]; act = a.p_dim >= 2;
+                } else {
+                    int t = q - a.Np1 - a.Np2;
+                    v = a.sg.p3_start[s] + (0.5 + t) * a.sg.dp3[s]; u = qq[3]; act = a.p_dim == 3;
+                }
+                const double dv = v - u;
+                tabs[e] = act ? exp((-m * (dv * dv)) / qq[4]) : 1.0;
             }
         }
     }
@@ -170,20 +182,20 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
 
     // ---- tile loader -------------------------------------------------------
     bool failed = false;       // a bounded wait gave up: finish without TMA
-    const unsigned tile_bytes = L::TILE * sizeof(T);
+    const unsigned tile_bytes = TILE * sizeof(T);
     auto issue = [&](int k, int buf) {
         if (k >= k_end) return;
         if (a.use_tma) {
             if (tid == 0 && !failed) {
                 mbar_arrive_expect_tx(&bars[buf], tile_bytes);
-                tma_load_3d(tile + buf * L::TILE, &a.tmap, &bars[buf], s * a.Np + k * PW,
+                tma_load_3d(tile + buf * TILE, &a.tmap, &bars[buf], s * a.Np + k * PW,
                             i0 + a.Ng - HALO, Q2 ? j0 + a.Ng - HALO : j0 + a.Ng);
             }
         } else {
             // coalesced loads with wrap-around (af.shift semantics) indexing
-            T* dst = tile + buf * L::TILE;
-            for (int r = warp; r < L::HY * L::HX; r += NTHREADS / 32) {
-                int hy = r / L::HX, hx = r % L::HX;
+            T* dst = tile + buf * TILE;
+            for (int r = warp; r < HY * HX; r += NTHREADS / 32) {
+                int hy = r / HX, hx = r % HX;
                 int g1 = i0 + a.Ng - HALO + hx;
                 int g2 = Q2 ? j0 + a.Ng - HALO + hy : j0 + a.Ng;
                 g1 = ((g1 % a.Nq1g) + a.Nq1g) % a.Nq1g;
@@ -197,7 +209,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         }
     };
 
-    unsigned phase[2] = {0u, 0u};
+    unsigned phase0 = 0u, phase1 = 0u;
     issue(k_begin, 0);
     issue(k_begin + 1, 1);
 
@@ -207,24 +219,56 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     const T* base2 = static_cast<const T*>(a.base2);
     const T* tau_arr = static_cast<const T*>(a.tau_arr);
     const T c1 = T(a.c1), c2 = T(a.c2);
+    const T inv_tau = T(1.0 / a.tau);
+    const T inv_dq1 = T(1.0 / a.dq1), inv_dq2 = T(1.0 / a.dq2);
+    const bool want_mom = a.mom_out != nullptr;
+    // phase C ownership: q-cell pc_c, p values [pc_q*PQ, pc_q*PQ + PQ) of each chunk
+    const int pc_c = tid % NQ, pc_q = tid / NQ;
+    double macc[kNumMom] = {0, 0, 0, 0, 0};
 
     int buf = 0;
     for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
         if (a.use_tma && !failed) {
-            if (!mbar_wait_bounded(&bars[buf], phase[buf])) {
+            const unsigned ph = buf ? phase1 : phase0;
+            if (!mbar_wait_bounded(&bars[buf], ph)) {
                 atomicExch(a.err, 4);
                 failed = true;
             }
-            phase[buf] ^= 1u;
+            if (buf) phase1 ^= 1u; else phase0 ^= 1u;
         }
-        __syncthreads();   // plain-load path: tile visible; TMA path: harmless
-        const T* X = tile + buf * L::TILE;
+        __syncthreads();   // tile visible; previous chunk's phase C done with `stage`
+        const T* X = tile + buf * TILE;
         const int p = k * PW + lane;
         const bool pvalid = p < a.Np;
         const int pc = pvalid ? p : a.Np - 1;
         const int ip1 = pc % a.Np1, ip2 = (pc / a.Np1) % a.Np2, ip3 = pc / (a.Np1 * a.Np2);
         const PVel V = lane_velocity(a.sg, s, ip1, ip2, ip3);
         const T v1 = T(V.v1), v2 = T(V.v2);
+
+        // ---- prefetch the combine operands of this thread's phase-B cells -----
+        // (issued now so the HBM latency overlaps phase A)
+        constexpr int NSEGB = (TQ1 >= 8) ? 1 : (8 / TQ1);
+        constexpr int SEGB = (TQ2 + NSEGB - 1) / NSEGB;
+        constexpr int ITEMS = TQ1 * NSEGB / (NTHREADS / 32);
+        static_assert(TQ1 * NSEGB % (NTHREADS / 32) == 0, "phase B items per warp");
+        constexpr int NSLOT = ITEMS * SEGB;
+        T pre1[NSLOT], pre2[NSLOT];
+#pragma unroll
+        for (int it = 0; it < ITEMS; ++it) {
+            const int item = warp + it * (NTHREADS / 32);
+            const int ic = item / NSEGB, sgi = item % NSEGB;
+#pragma unroll
+            for (int r = 0; r < SEGB; ++r) {
+                const int rr = sgi * SEGB + r;
+                const int ii = i0 + ic, jj = j0 + rr;
+                const bool cvalid = pvalid && ii < a.Nq1 && jj < a.Nq2 && rr < TQ2;
+                const long long gidx = (long long)(jj + a.Ng) * colstride
+                                     + (long long)(ii + a.Ng) * rowstride
+                                     + (long long)s * a.Np + p;
+                pre1[it * SEGB + r] = (base1 && cvalid) ? base1[gidx] : T(0);
+                pre2[it * SEGB + r] = (base2 && cvalid) ? base2[gidx] : T(0);
+            }
+        }
 
         // ---- phase A: q1 faces -> D1 = (-(F_R - F_L)) / dq1 ------------------
         {
@@ -237,7 +281,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                 const int jr = item / NSEG, sg = item % NSEG;
                 const int cb = sg * SEG, ce = min(TQ1, cb + SEG);
                 if (cb >= ce) continue;
-                const T* row = X + ((Q2 ? jr + HALO : 0) * L::HX) * PW + lane;
+                const T* row = X + ((Q2 ? jr + HALO : 0) * HX) * PW + lane;
                 // window for face f (between cells f-1 and f): cols f+off .. f+off+4
                 T y0 = row[(cb + off + 0) * PW], y1 = row[(cb + off + 1) * PW];
                 T y2 = row[(cb + off + 2) * PW], y3 = row[(cb + off + 3) * PW];
@@ -245,14 +289,16 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                 T fv = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
                 T Fprev = v1 * fv;
                 double jsum_prev = double(fv);
+#pragma unroll 4
                 for (int cc = cb; cc < ce; ++cc) {
-                    // face cc+1
                     y0 = y1; y1 = y2; y2 = y3; y3 = y4;
                     y4 = row[(cc + 1 + off + 4) * PW];
                     T fn = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
                     T Fn = v1 * fn;
-                    T d = (-(Fn - Fprev)) / T(a.dq1);
-                    D1[(jr * TQ1 + cc) * PW + lane] = d;
+                    T d;
+                    if (EXACT) d = (-(Fn - Fprev)) / T(a.dq1);
+                    else d = (Fprev - Fn) * inv_dq1;
+                    stage[(jr * TQ1 + cc) * PWP + lane] = d;
                     if (a.want_j) {
                         // J1 uses the state at each cell's left face (df_dt_fvm.py:214-216)
                         double c = pvalid ? jsum_prev * V.v1 : 0.0;
@@ -266,40 +312,49 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         }
         __syncthreads();
 
-        // ---- phase B: q2 faces, BGK, RK combine, outputs, moments -------------
+        // ---- phase B: q2 faces, BGK, RK combine, outputs ---------------------
+        if (warp == 0) {
+            vtab[0 * PW + lane] = pvalid ? V.v1 : 0.0;
+            vtab[1 * PW + lane] = pvalid ? V.v2 : 0.0;
+            vtab[2 * PW + lane] = pvalid ? V.v3 : 0.0;
+            vtab[3 * PW + lane] = pvalid ? V.vsq : 0.0;
+        }
         {
             const bool right = v2 > T(0);
             const int off = right ? 0 : 1;
             Weno5Side<T> S; S.set(right);
-            constexpr int NSEGB = (TQ1 >= 8) ? 1 : (8 / TQ1);
-            constexpr int SEGB = (TQ2 + NSEGB - 1) / NSEGB;
             const int ntab_off2 = a.Np1 + ip2, ntab_off3 = a.Np1 + a.Np2 + ip3;
-            for (int item = warp; item < TQ1 * NSEGB; item += NTHREADS / 32) {
+#pragma unroll
+            for (int it = 0; it < ITEMS; ++it) {
+                const int item = warp + it * (NTHREADS / 32);
                 const int ic = item / NSEGB, sg = item % NSEGB;
-                const int rb = sg * SEGB, re = min(TQ2, rb + SEGB);
-                if (rb >= re) continue;
+                const int rb = sg * SEGB;
                 const T* col = X + (ic + HALO) * PW + lane;
                 T y0, y1, y2, y3, y4, Fprev = T(0), fprev = T(0);
                 if (Q2) {
-                    y0 = col[((rb + off + 0) * L::HX) * PW]; y1 = col[((rb + off + 1) * L::HX) * PW];
-                    y2 = col[((rb + off + 2) * L::HX) * PW]; y3 = col[((rb + off + 3) * L::HX) * PW];
-                    y4 = col[((rb + off + 4) * L::HX) * PW];
+                    y0 = col[((rb + off + 0) * HX) * PW]; y1 = col[((rb + off + 1) * HX) * PW];
+                    y2 = col[((rb + off + 2) * HX) * PW]; y3 = col[((rb + off + 3) * HX) * PW];
+                    y4 = col[((rb + off + 4) * HX) * PW];
                     fprev = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
                     Fprev = v2 * fprev;
                 }
-                for (int rr = rb; rr < re; ++rr) {
+#pragma unroll
+                for (int r = 0; r < SEGB; ++r) {
+                    const int rr = rb + r;
+                    if (rr >= TQ2) break;
                     const int ii = i0 + ic, jj = j0 + rr;
                     const bool cvalid = pvalid && ii < a.Nq1 && jj < a.Nq2;
                     const int cq = rr * TQ1 + ic;
-                    T kq = D1[cq * PW + lane];
-                    T fcell = col[((Q2 ? rr + HALO : 0) * L::HX) * PW];
+                    T kq = stage[cq * PWP + lane];
+                    T fcell = col[((Q2 ? rr + HALO : 0) * HX) * PW];
                     T fbot = fprev;
                     if (Q2) {
                         y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                        y4 = col[((rr + 1 + off + 4) * L::HX) * PW];
+                        y4 = col[((rr + 1 + off + 4) * HX) * PW];
                         T fn = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
                         T Fn = v2 * fn;
-                        kq = kq - (Fn - Fprev) / T(a.dq2);
+                        if (EXACT) kq = kq - (Fn - Fprev) / T(a.dq2);
+                        else kq = kq - (Fn - Fprev) * inv_dq2;
                         Fprev = Fn;
                         fprev = fn;
                     }
@@ -328,12 +383,11 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                             fmb = ((qc[cq * 5] * tb[ip1]) * tb[ntab_off2]) * tb[ntab_off3];
                         }
                         if (EXACT) {
-                            // (((n*A)*e1)*e2)*e3 with unit factors for absent dims
                             double tauv = tau_arr ? double(tau_arr[cvalid ? gidx : 0]) : a.tau;
                             kk = T(double(kk) + (-(double(fcell) - fmb) / tauv));
                         } else {
-                            float tauv = tau_arr ? float(tau_arr[cvalid ? gidx : 0]) : float(a.tau);
-                            kk = kk + (-(fcell - T(fmb)) * fast_rcp(tauv));
+                            T it = tau_arr ? T(1) / tau_arr[cvalid ? gidx : 0] : inv_tau;
+                            kk = kk + (T(fmb) - fcell) * it;
                         }
                     }
                     if (a.want_j) {
@@ -344,51 +398,63 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                         if (lane == 0) { j_acc[cq * 3 + 1] += jc2; j_acc[cq * 3 + 2] += jc3; }
                     }
                     // RK stage combine (fvm_operator.py:26,33; integrators.py:18-25)
-                    T o1 = base1 ? base1[cvalid ? gidx : 0] + kk * c1 : kk;
+                    T o1 = base1 ? pre1[it * SEGB + r] + kk * c1 : kk;
                     if (cvalid) {
                         out1[gidx] = o1;
-                        if (out2) out2[gidx] = base2[gidx] + kk * c2;
+                        if (out2) out2[gidx] = pre2[it * SEGB + r] + kk * c2;
                         // wrap-around ghost copies (what the next halo refresh would do)
                         if ((a.periodic1 && (ii < a.Ng || ii >= a.Nq1 - a.Ng)) ||
                             (a.periodic2 && (jj < a.Ng || jj >= a.Nq2 - a.Ng)))
                             write_ghost_images(out1, o1, ii, jj, s, p, a.Ng, a.Nq1, a.Nq2,
                                                a.Nq1g, a.Nq2g, a.periodic1, a.periodic2,
                                                rowstride, colstride, a.Np);
-                        if (a.flag && !isfinite(double(o1))) atomicOr(a.flag, 1);
+                        if (a.flag && !isfinite(o1)) atomicOr(a.flag, 1);
                     }
-                    if (a.mom_out) {
-                        double ov = cvalid ? double(o1) : 0.0;
-                        double m0 = warp_sum(ov);
-                        double m1 = warp_sum(ov * V.v1);
-                        double m2 = warp_sum(ov * V.v2);
-                        double m3 = warp_sum(ov * V.v3);
-                        double m4 = warp_sum((0.5 * ov) * V.vsq);
-                        if (lane == 0) {
-                            double* mp = mom_acc + cq * kNumMom;
-                            mp[0] += m0; mp[1] += m1; mp[2] += m2; mp[3] += m3; mp[4] += m4;
-                        }
-                    }
+                    stage[cq * PWP + lane] = cvalid ? o1 : T(0);
                 }
             }
         }
-        __syncthreads();   // buffer `buf` fully consumed
+        __syncthreads();   // tile `buf` consumed, stage holds out1 of the chunk
         if (a.use_tma) fence_proxy_async();
         issue(k + 2, buf);
+
+        // ---- phase C: FP64 moments of out1 (moments.py:6-24) ------------------
+        if (want_mom) {
+            const T* sp = stage + pc_c * PWP + pc_q * PQ;
+            const double* vt = vtab + pc_q * PQ;
+#pragma unroll
+            for (int t = 0; t < PQ; ++t) {
+                const double ov = double(sp[t]);
+                macc[0] += ov;
+                macc[1] += ov * vt[t];
+                macc[2] += ov * vt[PW + t];
+                macc[3] += ov * vt[2 * PW + t];
+                macc[4] += (0.5 * ov) * vt[3 * PW + t];
+            }
+        }
     }
+    __syncthreads();
 
     // ---- epilogue: partial moments / currents of this split ------------------
     const long long plane = (long long)a.Nq2 * a.Nq1;
-    if (a.mom_out) {
-        for (int c = tid; c < L::NQ * kNumMom; c += NTHREADS) {
+    if (want_mom) {
+        double* red = reinterpret_cast<double*>(smem_raw + Lo.tile);   // tile no longer used
+#pragma unroll
+        for (int q = 0; q < kNumMom; ++q) red[(pc_q * NQ + pc_c) * kNumMom + q] = macc[q];
+        __syncthreads();
+        for (int c = tid; c < NQ * kNumMom; c += NTHREADS) {
             int cq = c / kNumMom, q = c % kNumMom;
+            double v = 0.0;
+#pragma unroll
+            for (int h = 0; h < NQUART; ++h) v += red[(h * NQ + cq) * kNumMom + q];
             int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
             if (ii < a.Nq1 && jj < a.Nq2)
                 a.mom_out[(((long long)split * kNumMom + q) * a.Ns + s) * plane
-                          + (long long)jj * a.Nq1 + ii] = mom_acc[c];
+                          + (long long)jj * a.Nq1 + ii] = v;
         }
     }
     if (a.want_j && a.j_out) {
-        for (int c = tid; c < L::NQ * 3; c += NTHREADS) {
+        for (int c = tid; c < NQ * 3; c += NTHREADS) {
             int cq = c / 3, q = c % 3;
             int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
             if (ii < a.Nq1 && jj < a.Nq2)

@@ -26,14 +26,7 @@ inline TileShape tile_shape(int tiling) {
 // bytes of dynamic shared memory of the q-stage kernel
 inline size_t qstage_smem(int tiling, size_t elem, int bgk, int bgk_direct, int ntab) {
     TileShape t = tile_shape(tiling);
-    const size_t hx = t.tq1 + 2 * HALO, hy = t.q2 ? t.tq2 + 2 * HALO : 1;
-    const size_t tile = hy * hx * PW;
-    const size_t nq = (size_t)t.tq1 * t.tq2;
-    size_t b = 2 * tile * elem + nq * PW * elem;
-    b += nq * (kNumMom + 3 + 5) * sizeof(double);
-    if (bgk && !bgk_direct) b += nq * (size_t)ntab * sizeof(double);
-    b += 2 * sizeof(uint64_t);
-    return b;
+    return qstage_layout(t.tq1, t.tq2, t.q2, (int)elem, bgk, bgk_direct, ntab).total;
 }
 
 inline size_t pstage_smem(int Np, size_t elem) { return 4 * (size_t)Np * elem; }

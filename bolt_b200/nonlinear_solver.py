@@ -53,13 +53,31 @@ class _FieldsSolver(object):
         # (6, Nq2g, Nq1g) -> (6, 1, Nq1g, Nq2g)
         return a.permute(0, 2, 1).unsqueeze(1)
 
+    def _store(self, cell=None, yee=None):
+        nls = self._nls
+        conv = lambda a: None if a is None else \
+            torch.as_tensor(a, dtype=torch.float64, device=nls.device)[:, 0].permute(0, 2, 1).contiguous()
+        c, y = conv(cell), conv(yee)
+        self._keep = (c, y)
+        N.check(nls._lib.bolt_fields_set(nls._ctx, 0 if c is None else c.data_ptr(),
+                                         0 if y is None else y.data_ptr(), nls._stream()),
+                'bolt_fields_set')
+
     @property
     def cell_centered_EM_fields(self):
         return self._af(self._fetch()[0])
 
+    @cell_centered_EM_fields.setter
+    def cell_centered_EM_fields(self, value):
+        self._store(cell=value)
+
     @property
     def yee_grid_EM_fields(self):
         return self._af(self._fetch()[1])
+
+    @yee_grid_EM_fields.setter
+    def yee_grid_EM_fields(self, value):
+        self._store(yee=value)
 
     @property
     def at_n(self):
