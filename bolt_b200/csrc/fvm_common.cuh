@@ -103,7 +103,7 @@ __device__ __forceinline__ double weno5_exact(double y0, double y1, double y2, d
 __device__ __forceinline__ float weno_beta_fast(float a, float b, float c) {
     float d1 = fmaf(-2.0f, b, a + c);           // a - 2b + c
     float d2 = fmaf(3.0f, c, fmaf(-4.0f, b, a));  // a - 4b + 3c
-    float e = 1e-17f * (1.0f + fabsf(a) + fabsf(b) + fabsf(c));
+    float e = fmaf(1e-17f, fabsf(a) + fabsf(b) + fabsf(c), 1e-17f);
     return fmaf(13.0f / 12.0f * d1, d1, fmaf(0.25f * d2, d2, e));
 }
 
@@ -190,6 +190,93 @@ __device__ __forceinline__ T face_value(T y0, T y1, T y2, T y3, T y4, bool right
         }
     }
 }
+
+// ---------------------------------------------------------------------------
+// WENO5 along a sliding window.  Consecutive faces share two of their three
+// substencils: beta_1 of face f+1 is beta_2 of face f and beta_2 of face f+1
+// is beta_3 of face f, so each step computes one new smoothness indicator.
+// The exact flavour reuses the identical FP64 values (bit-for-bit the same
+// as recomputing them); the fast flavour carries 1/beta^2.
+// ---------------------------------------------------------------------------
+template <bool EXACT, typename T> struct Weno5Walker;
+
+template <> struct Weno5Walker<true, double> {
+    double b2, b3;
+    __device__ __forceinline__ double eval(double b1, double y0, double y1, double y2, double y3,
+                                           double y4, const Weno5Side<double>& S) {
+        double w1 = S.num1 / ((S.den1 * b1) * b1);
+        double w2 = S.num2 / ((S.den2 * b2) * b2);
+        double w3 = S.num3 / ((S.den3 * b3) * b3);
+        double den = (w1 + w2) + w3;
+        double u1 = (S.a10 * y0 + S.a11 * y1) + S.a12 * y2;
+        double u2 = (S.a20 * y1 + S.a21 * y2) + S.a22 * y3;
+        double u3 = (S.a30 * y2 + S.a31 * y3) + S.a32 * y4;
+        return ((w1 * u1 + w2 * u2) + w3 * u3) / den;
+    }
+    __device__ __forceinline__ double first(double y0, double y1, double y2, double y3, double y4,
+                                            const Weno5Side<double>& S) {
+        double b1 = weno_beta_exact(y0, y1, y2);
+        b2 = weno_beta_exact(y1, y2, y3);
+        b3 = weno_beta_exact(y2, y3, y4);
+        return eval(b1, y0, y1, y2, y3, y4, S);
+    }
+    // window shifted by one cell: y0..y3 are the previous y1..y4
+    __device__ __forceinline__ double next(double y0, double y1, double y2, double y3, double y4,
+                                           const Weno5Side<double>& S) {
+        double b1 = b2;
+        b2 = b3;
+        b3 = weno_beta_exact(y2, y3, y4);
+        return eval(b1, y0, y1, y2, y3, y4, S);
+    }
+};
+
+template <> struct Weno5Walker<false, float> {
+    float q2, q3;              // 1/beta^2 of substencils 2 and 3
+    __device__ __forceinline__ static float inv_sq(float b) {
+        float r = fast_rcp(b);
+        return r * r;
+    }
+    __device__ __forceinline__ float eval(float q1, float y0, float y1, float y2, float y3,
+                                          float y4, const Weno5Side<float>& S) {
+        float w1 = S.cw1 * q1, w2 = S.cw2 * q2, w3 = S.cw3 * q3;
+        float u1 = fmaf(S.a12, y2, fmaf(S.a11, y1, S.a10 * y0));
+        float u2 = fmaf(S.a22, y3, fmaf(S.a21, y2, S.a20 * y1));
+        float u3 = fmaf(S.a32, y4, fmaf(S.a31, y3, S.a30 * y2));
+        float num = fmaf(w3, u3, fmaf(w2, u2, w1 * u1));
+        return num * fast_rcp(w1 + w2 + w3);
+    }
+    __device__ __forceinline__ float first(float y0, float y1, float y2, float y3, float y4,
+                                           const Weno5Side<float>& S) {
+        float q1 = inv_sq(weno_beta_fast(y0, y1, y2));
+        q2 = inv_sq(weno_beta_fast(y1, y2, y3));
+        q3 = inv_sq(weno_beta_fast(y2, y3, y4));
+        return eval(q1, y0, y1, y2, y3, y4, S);
+    }
+    __device__ __forceinline__ float next(float y0, float y1, float y2, float y3, float y4,
+                                          const Weno5Side<float>& S) {
+        float q1 = q2;
+        q2 = q3;
+        q3 = inv_sq(weno_beta_fast(y2, y3, y4));
+        return eval(q1, y0, y1, y2, y3, y4, S);
+    }
+};
+
+// Face walker for any reconstruction: WENO5 carries state, the others are
+// evaluated from the window directly.
+template <int RECON, bool EXACT, typename T>
+struct FaceWalker {
+    Weno5Walker<EXACT, T> w;
+    __device__ __forceinline__ T first(T y0, T y1, T y2, T y3, T y4, bool right,
+                                       const Weno5Side<T>& S) {
+        if (RECON == BOLT_RECON_WENO5) return w.first(y0, y1, y2, y3, y4, S);
+        return face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+    }
+    __device__ __forceinline__ T next(T y0, T y1, T y2, T y3, T y4, bool right,
+                                      const Weno5Side<T>& S) {
+        if (RECON == BOLT_RECON_WENO5) return w.next(y0, y1, y2, y3, y4, S);
+        return face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+    }
+};
 
 // ---------------------------------------------------------------------------
 // mbarrier + TMA (cp.async.bulk.tensor) wrappers.  Waits are bounded: after

@@ -174,7 +174,9 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                     v = a.sg.p3_start[s] + (0.5 + t) * a.sg.dp3[s]; u = qq[3]; act = a.p_dim == 3;
                 }
                 const double dv = v - u;
-                tabs[e] = act ? exp((-m * (dv * dv)) / qq[4]) : 1.0;
+                const double ev = act ? exp((-m * (dv * dv)) / qq[4]) : 1.0;
+                // the p1 table holds (n*A)*e1, the first product of f0
+                tabs[e] = q < a.Np1 ? qq[0] * ev : ev;
             }
         }
     }
@@ -286,14 +288,15 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                 T y0 = row[(cb + off + 0) * PW], y1 = row[(cb + off + 1) * PW];
                 T y2 = row[(cb + off + 2) * PW], y3 = row[(cb + off + 3) * PW];
                 T y4 = row[(cb + off + 4) * PW];
-                T fv = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+                FaceWalker<RECON, EXACT, T> W;
+                T fv = W.first(y0, y1, y2, y3, y4, right, S);
                 T Fprev = v1 * fv;
                 double jsum_prev = double(fv);
 #pragma unroll 4
                 for (int cc = cb; cc < ce; ++cc) {
                     y0 = y1; y1 = y2; y2 = y3; y3 = y4;
                     y4 = row[(cc + 1 + off + 4) * PW];
-                    T fn = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+                    T fn = W.next(y0, y1, y2, y3, y4, right, S);
                     T Fn = v1 * fn;
                     T d;
                     if (EXACT) d = (-(Fn - Fprev)) / T(a.dq1);
@@ -331,11 +334,12 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                 const int rb = sg * SEGB;
                 const T* col = X + (ic + HALO) * PW + lane;
                 T y0, y1, y2, y3, y4, Fprev = T(0), fprev = T(0);
+                FaceWalker<RECON, EXACT, T> W;
                 if (Q2) {
                     y0 = col[((rb + off + 0) * HX) * PW]; y1 = col[((rb + off + 1) * HX) * PW];
                     y2 = col[((rb + off + 2) * HX) * PW]; y3 = col[((rb + off + 3) * HX) * PW];
                     y4 = col[((rb + off + 4) * HX) * PW];
-                    fprev = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+                    fprev = W.first(y0, y1, y2, y3, y4, right, S);
                     Fprev = v2 * fprev;
                 }
 #pragma unroll
@@ -351,7 +355,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                     if (Q2) {
                         y0 = y1; y1 = y2; y2 = y3; y3 = y4;
                         y4 = col[((rr + 1 + off + 4) * HX) * PW];
-                        T fn = face_value<RECON, EXACT>(y0, y1, y2, y3, y4, right, S);
+                        T fn = W.next(y0, y1, y2, y3, y4, right, S);
                         T Fn = v2 * fn;
                         if (EXACT) kq = kq - (Fn - Fprev) / T(a.dq2);
                         else kq = kq - (Fn - Fprev) * inv_dq2;
@@ -380,7 +384,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                             }
                         } else {
                             const double* tb = tabs + (long long)cq * ntab;
-                            fmb = ((qc[cq * 5] * tb[ip1]) * tb[ntab_off2]) * tb[ntab_off3];
+                            fmb = (tb[ip1] * tb[ntab_off2]) * tb[ntab_off3];
                         }
                         if (EXACT) {
                             double tauv = tau_arr ? double(tau_arr[cvalid ? gidx : 0]) : a.tau;
