@@ -402,6 +402,7 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     a.p_dim = ctx->p.p_dim;
     a.want_j = want_j;
     a.bgk_direct = ctx->bgk_direct;
+    a.full_chunks = (ctx->Np % PW) == 0;
     a.sg = ctx->sg;
     dim3 grid(ctx->ntiles1 * ctx->ntiles2, g.N_s * ctx->nsplit);
     const size_t smem = qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct, ctx->ntab);

@@ -16,7 +16,7 @@ constexpr int PWP = PW + 1;     // padded stage-buffer row (conflict-free column
 // Shared-memory carve-up of the q-stage kernel (byte offsets), used by the
 // kernel and by the host to size the launch.
 struct QLayout {
-    unsigned tile, stage, vtab, jacc, qc, tabs, bars, total;
+    unsigned tile, stage, vtab, jacc, qc, tabs, vgrid, bars, total;
 };
 
 __host__ __device__ inline unsigned qalign(unsigned x, unsigned a) { return (x + a - 1) / a * a; }
@@ -36,6 +36,7 @@ __host__ __device__ inline QLayout qstage_layout(int tq1, int tq2, int q2, int e
     L.jacc = o;  o += nq * 3 * sizeof(double);
     L.qc = o;    o += nq * 5 * sizeof(double);
     L.tabs = o;  o += (bgk && !bgk_direct) ? nq * ntab * sizeof(double) : 0;
+    L.vgrid = o; o += ntab * sizeof(double);      // p1, p2, p3 cell centres of the species
     L.bars = o;  o += 2 * sizeof(unsigned long long);
     L.total = o;
     return L;
@@ -67,6 +68,7 @@ struct QStageArgs {
     int nsplit_in, nsplit, chunks_per_split, ntiles1;
     int use_tma, p_dim, want_j;
     int bgk_direct;             // 1: exp per cell (no per-q-cell exp tables)
+    int full_chunks;            // Np % 32 == 0: every p-chunk is complete
     SpeciesGrid sg;
 };
 

@@ -85,39 +85,65 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     constexpr int HX = TQ1 + 2 * HALO;
     constexpr int HY = Q2 ? TQ2 + 2 * HALO : 1;
     constexpr int NQ = TQ1 * TQ2;
+    constexpr int NWARP = NTHREADS / 32;
     constexpr int NQUART = NTHREADS / NQ;       // threads per q-cell in phase C
     constexpr int PQ = PW / NQUART;             // p values per phase-C thread
     static_assert(NTHREADS % NQ == 0 && PW % NQUART == 0, "phase C mapping");
-    const int ntab = a.Np1 + a.Np2 + a.Np3;
+    constexpr int TILE = HY * HX * PW;
+    // phase A: rows split into NSEG segments; phase B: ITEMS (column, segment)
+    // items per warp of SEGB rows each -> NSLOT cells per thread
+    constexpr int NSEG = (TQ2 >= NWARP) ? 1 : (NWARP / TQ2);
+    constexpr int SEG = (TQ1 + NSEG - 1) / NSEG;
+    constexpr int NSEGB = (TQ1 >= NWARP) ? 1 : (NWARP / TQ1);
+    constexpr int SEGB = (TQ2 + NSEGB - 1) / NSEGB;
+    constexpr int ITEMS = TQ1 * NSEGB / NWARP;
+    static_assert(TQ1 * NSEGB % NWARP == 0, "phase B items per warp");
+    constexpr int NSLOT = ITEMS * SEGB;
+
+    const int Np1 = a.Np1, Np2 = a.Np2, Np3 = a.Np3, Np = a.Np, Ng = a.Ng;
+    const int Nq1 = a.Nq1, Nq2 = a.Nq2;
+    const int ntab = Np1 + Np2 + Np3;
     const QLayout Lo = qstage_layout(TQ1, TQ2, Q2, sizeof(T), BGK, a.bgk_direct, ntab);
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    T* tile = reinterpret_cast<T*>(smem_raw + Lo.tile);          // [2][HY][HX][PW]
-    T* stage = reinterpret_cast<T*>(smem_raw + Lo.stage);        // [NQ][PWP]
-    double* vtab = reinterpret_cast<double*>(smem_raw + Lo.vtab);   // [4][PW]
-    double* j_acc = reinterpret_cast<double*>(smem_raw + Lo.jacc);  // [NQ][3]
-    double* qc = reinterpret_cast<double*>(smem_raw + Lo.qc);       // [NQ][5]
-    double* tabs = reinterpret_cast<double*>(smem_raw + Lo.tabs);   // [NQ][ntab]
+    T* tile = reinterpret_cast<T*>(smem_raw + Lo.tile);              // [2][HY][HX][PW]
+    T* stage = reinterpret_cast<T*>(smem_raw + Lo.stage);            // [NQ][PWP]
+    double* vtab = reinterpret_cast<double*>(smem_raw + Lo.vtab);    // [4][PW]
+    double* j_acc = reinterpret_cast<double*>(smem_raw + Lo.jacc);   // [NQ][3]
+    double* qc = reinterpret_cast<double*>(smem_raw + Lo.qc);        // [NQ][5]
+    double* tabs = reinterpret_cast<double*>(smem_raw + Lo.tabs);    // [NQ][ntab]
+    double* vgrid = reinterpret_cast<double*>(smem_raw + Lo.vgrid);  // [ntab]
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + Lo.bars);
-    constexpr int TILE = HY * HX * PW;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
     const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
     const int i0 = tile1 * TQ1, j0 = tile2 * TQ2;                     // interior origin
-    const int nchunks = (a.Np + PW - 1) / PW;
+    const int nchunks = (Np + PW - 1) / PW;
     const int k_begin = split * a.chunks_per_split;
     const int k_end = min(nchunks, k_begin + a.chunks_per_split);
-    const long long rowstride = (long long)a.Ns * a.Np;               // per q1 step
+    const long long rowstride = (long long)a.Ns * Np;                 // per q1 step
     const long long colstride = rowstride * a.Nq1g;                   // per q2 step
     const T* fs = static_cast<const T*>(a.fs);
+    // CTA-uniform predicates: whole tile inside the domain and every chunk
+    // complete (no per-cell masks), tile within reach of a periodic border
+    const bool tile_full = (i0 + TQ1 <= Nq1) && (j0 + TQ2 <= Nq2);
+    const bool fast = tile_full && a.full_chunks;
+    const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ1 > Nq1 - Ng)) ||
+                        (a.periodic2 && (j0 < Ng || j0 + TQ2 > Nq2 - Ng));
 
     for (int c = tid; c < NQ * 3; c += NTHREADS) j_acc[c] = 0.0;
+    for (int q = tid; q < ntab; q += NTHREADS) {
+        if (q < Np1) vgrid[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
+        else if (q < Np1 + Np2) vgrid[q] = a.sg.p2_start[s] + (0.5 + (q - Np1)) * a.sg.dp2[s];
+        else vgrid[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
+    }
     if (tid == 0 && a.use_tma) {
         prefetch_tmap(&a.tmap);
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         fence_barrier_init();
     }
+    __syncthreads();
 
     // ---- BGK prologue: Maxwellian of the stage input per q-cell (FP64) ----
     // collision_operator.py:102-118 and f0 :49-65
@@ -125,17 +151,16 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         const double m = a.sg.mass[s];
         const double kB = a.kB;
         const double measure = (a.sg.dp3[s] * a.sg.dp2[s]) * a.sg.dp1[s];
-        const long long plane = (long long)a.Nq2 * a.Nq1;
-        // moment sums of the stage input: 5 threads per q-cell
+        const long long plane = (long long)Nq2 * Nq1;
         for (int c = tid; c < NQ; c += NTHREADS) {
             int ii = i0 + c % TQ1, jj = j0 + c / TQ1;
             double mm[kNumMom] = {0, 0, 0, 0, 0};
-            if (ii < a.Nq1 && jj < a.Nq2) {
+            if (ii < Nq1 && jj < Nq2) {
                 for (int sp = 0; sp < a.nsplit_in; ++sp) {
 #pragma unroll
                     for (int q = 0; q < kNumMom; ++q)
                         mm[q] += a.mom_in[(((long long)sp * kNumMom + q) * a.Ns + s) * plane
-                                          + (long long)jj * a.Nq1 + ii];
+                                          + (long long)jj * Nq1 + ii];
                 }
             }
             const double eps = 1e-30;
@@ -158,25 +183,15 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         }
         __syncthreads();
         if (!a.bgk_direct) {
-            // exp tables: all threads over (q-cell, table entry)
+            // exp tables over (q-cell, p1 | p2 | p3); the p1 entry carries n*A
             for (int e = tid; e < NQ * ntab; e += NTHREADS) {
                 const int c = e / ntab, q = e % ntab;
                 const double* qq = qc + c * 5;
-                double v, u;
-                bool act;
-                if (q < a.Np1) {
-                    v = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s]; u = qq[1]; act = true;
-                } else if (q < a.Np1 + a.Np2) {
-                    int t = q - a.Np1;
-                    v = a.sg.p2_start[s] + (0.5 + t) * a.sg.dp2[s]; u = qq[2]; act = a.p_dim >= 2;
-                } else {
-                    int t = q - a.Np1 - a.Np2;
-                    v = a.sg.p3_start[s] + (0.5 + t) * a.sg.dp3[s]; u = qq[3]; act = a.p_dim == 3;
-                }
-                const double dv = v - u;
+                const double u = q < Np1 ? qq[1] : (q < Np1 + Np2 ? qq[2] : qq[3]);
+                const bool act = q < Np1 || (q < Np1 + Np2 ? a.p_dim >= 2 : a.p_dim == 3);
+                const double dv = vgrid[q] - u;
                 const double ev = act ? exp((-m * (dv * dv)) / qq[4]) : 1.0;
-                // the p1 table holds (n*A)*e1, the first product of f0
-                tabs[e] = q < a.Np1 ? qq[0] * ev : ev;
+                tabs[e] = q < Np1 ? qq[0] * ev : ev;
             }
         }
     }
@@ -190,22 +205,22 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         if (a.use_tma) {
             if (tid == 0 && !failed) {
                 mbar_arrive_expect_tx(&bars[buf], tile_bytes);
-                tma_load_3d(tile + buf * TILE, &a.tmap, &bars[buf], s * a.Np + k * PW,
-                            i0 + a.Ng - HALO, Q2 ? j0 + a.Ng - HALO : j0 + a.Ng);
+                tma_load_3d(tile + buf * TILE, &a.tmap, &bars[buf], s * Np + k * PW,
+                            i0 + Ng - HALO, Q2 ? j0 + Ng - HALO : j0 + Ng);
             }
         } else {
             // coalesced loads with wrap-around (af.shift semantics) indexing
             T* dst = tile + buf * TILE;
-            for (int r = warp; r < HY * HX; r += NTHREADS / 32) {
+            for (int r = warp; r < HY * HX; r += NWARP) {
                 int hy = r / HX, hx = r % HX;
-                int g1 = i0 + a.Ng - HALO + hx;
-                int g2 = Q2 ? j0 + a.Ng - HALO + hy : j0 + a.Ng;
+                int g1 = i0 + Ng - HALO + hx;
+                int g2 = Q2 ? j0 + Ng - HALO + hy : j0 + Ng;
                 g1 = ((g1 % a.Nq1g) + a.Nq1g) % a.Nq1g;
                 g2 = ((g2 % a.Nq2g) + a.Nq2g) % a.Nq2g;
                 int p = k * PW + lane;
                 T v = T(0);
-                if (p < a.Np) v = fs[(long long)g2 * colstride + (long long)g1 * rowstride
-                                     + (long long)s * a.Np + p];
+                if (p < Np) v = fs[(long long)g2 * colstride + (long long)g1 * rowstride
+                                   + (long long)s * Np + p];
                 dst[r * PW + lane] = v;
             }
         }
@@ -223,10 +238,23 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     const T c1 = T(a.c1), c2 = T(a.c2);
     const T inv_tau = T(1.0 / a.tau);
     const T inv_dq1 = T(1.0 / a.dq1), inv_dq2 = T(1.0 / a.dq2);
+    const double mneg = -a.sg.mass[s];
     const bool want_mom = a.mom_out != nullptr;
+    const bool want_j = a.want_j != 0;
     // phase C ownership: q-cell pc_c, p values [pc_q*PQ, pc_q*PQ + PQ) of each chunk
     const int pc_c = tid % NQ, pc_q = tid / NQ;
     double macc[kNumMom] = {0, 0, 0, 0, 0};
+
+    // this lane's p index within the species, kept as (ip1, ip2, ip3) and
+    // advanced by PW per chunk without divisions
+    int p = k_begin * PW + lane;
+    int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
+    // element offset of this thread's first phase-B cell (q-cell (i0+ic0, j0+rb0))
+    // for item 0; other slots add compile-time multiples of the strides
+    const int ic0 = warp / NSEGB, rb0 = (warp % NSEGB) * SEGB;
+    const long long tbase = (long long)(j0 + rb0 + Ng) * colstride
+                          + (long long)(i0 + ic0 + Ng) * rowstride + (long long)s * Np;
+    const long long item_step = (long long)(NWARP / NSEGB) * rowstride;   // next item: columns
 
     int buf = 0;
     for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
@@ -240,35 +268,24 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         }
         __syncthreads();   // tile visible; previous chunk's phase C done with `stage`
         const T* X = tile + buf * TILE;
-        const int p = k * PW + lane;
-        const bool pvalid = p < a.Np;
-        const int pc = pvalid ? p : a.Np - 1;
-        const int ip1 = pc % a.Np1, ip2 = (pc / a.Np1) % a.Np2, ip3 = pc / (a.Np1 * a.Np2);
-        const PVel V = lane_velocity(a.sg, s, ip1, ip2, ip3);
-        const T v1 = T(V.v1), v2 = T(V.v2);
+        const bool pvalid = p < Np;
+        const int jp1 = pvalid ? ip1 : 0, jp2 = pvalid ? ip2 : 0, jp3 = pvalid ? ip3 : 0;
+        const double V1 = vgrid[jp1], V2 = vgrid[Np1 + jp2], V3 = vgrid[Np1 + Np2 + jp3];
+        const T v1 = T(V1), v2 = T(V2);
 
         // ---- prefetch the combine operands of this thread's phase-B cells -----
         // (issued now so the HBM latency overlaps phase A)
-        constexpr int NSEGB = (TQ1 >= 8) ? 1 : (8 / TQ1);
-        constexpr int SEGB = (TQ2 + NSEGB - 1) / NSEGB;
-        constexpr int ITEMS = TQ1 * NSEGB / (NTHREADS / 32);
-        static_assert(TQ1 * NSEGB % (NTHREADS / 32) == 0, "phase B items per warp");
-        constexpr int NSLOT = ITEMS * SEGB;
         T pre1[NSLOT], pre2[NSLOT];
 #pragma unroll
         for (int it = 0; it < ITEMS; ++it) {
-            const int item = warp + it * (NTHREADS / 32);
-            const int ic = item / NSEGB, sgi = item % NSEGB;
 #pragma unroll
             for (int r = 0; r < SEGB; ++r) {
-                const int rr = sgi * SEGB + r;
-                const int ii = i0 + ic, jj = j0 + rr;
-                const bool cvalid = pvalid && ii < a.Nq1 && jj < a.Nq2 && rr < TQ2;
-                const long long gidx = (long long)(jj + a.Ng) * colstride
-                                     + (long long)(ii + a.Ng) * rowstride
-                                     + (long long)s * a.Np + p;
-                pre1[it * SEGB + r] = (base1 && cvalid) ? base1[gidx] : T(0);
-                pre2[it * SEGB + r] = (base2 && cvalid) ? base2[gidx] : T(0);
+                const int ic = (warp + it * NWARP) / NSEGB;
+                const int rr = rb0 + r;
+                const bool cvalid = fast || (pvalid && i0 + ic < Nq1 && j0 + rr < Nq2 && rr < TQ2);
+                const long long g = tbase + it * item_step + r * colstride + p;
+                pre1[it * SEGB + r] = (base1 && cvalid) ? base1[g] : T(0);
+                pre2[it * SEGB + r] = (base2 && cvalid) ? base2[g] : T(0);
             }
         }
 
@@ -277,34 +294,32 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
             const bool right = v1 > T(0);
             const int off = right ? 0 : 1;
             Weno5Side<T> S; S.set(right);
-            constexpr int NSEG = (TQ2 >= 8) ? 1 : (8 / TQ2);
-            constexpr int SEG = (TQ1 + NSEG - 1) / NSEG;
-            for (int item = warp; item < TQ2 * NSEG; item += NTHREADS / 32) {
+            for (int item = warp; item < TQ2 * NSEG; item += NWARP) {
                 const int jr = item / NSEG, sg = item % NSEG;
                 const int cb = sg * SEG, ce = min(TQ1, cb + SEG);
                 if (cb >= ce) continue;
-                const T* row = X + ((Q2 ? jr + HALO : 0) * HX) * PW + lane;
+                const T* row = X + ((Q2 ? jr + HALO : 0) * HX) * PW + lane + off * PW;
                 // window for face f (between cells f-1 and f): cols f+off .. f+off+4
-                T y0 = row[(cb + off + 0) * PW], y1 = row[(cb + off + 1) * PW];
-                T y2 = row[(cb + off + 2) * PW], y3 = row[(cb + off + 3) * PW];
-                T y4 = row[(cb + off + 4) * PW];
+                T y0 = row[(cb + 0) * PW], y1 = row[(cb + 1) * PW];
+                T y2 = row[(cb + 2) * PW], y3 = row[(cb + 3) * PW];
+                T y4 = row[(cb + 4) * PW];
                 FaceWalker<RECON, EXACT, T> W;
                 T fv = W.first(y0, y1, y2, y3, y4, right, S);
                 T Fprev = v1 * fv;
                 double jsum_prev = double(fv);
-#pragma unroll 4
+#pragma unroll 2
                 for (int cc = cb; cc < ce; ++cc) {
                     y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                    y4 = row[(cc + 1 + off + 4) * PW];
+                    y4 = row[(cc + 5) * PW];
                     T fn = W.next(y0, y1, y2, y3, y4, right, S);
                     T Fn = v1 * fn;
                     T d;
                     if (EXACT) d = (-(Fn - Fprev)) / T(a.dq1);
                     else d = (Fprev - Fn) * inv_dq1;
                     stage[(jr * TQ1 + cc) * PWP + lane] = d;
-                    if (a.want_j) {
+                    if (want_j) {
                         // J1 uses the state at each cell's left face (df_dt_fvm.py:214-216)
-                        double c = pvalid ? jsum_prev * V.v1 : 0.0;
+                        double c = pvalid ? jsum_prev * V1 : 0.0;
                         c = warp_sum(c);
                         if (lane == 0) j_acc[(jr * TQ1 + cc) * 3 + 0] += c;
                     }
@@ -317,44 +332,43 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
 
         // ---- phase B: q2 faces, BGK, RK combine, outputs ---------------------
         if (warp == 0) {
-            vtab[0 * PW + lane] = pvalid ? V.v1 : 0.0;
-            vtab[1 * PW + lane] = pvalid ? V.v2 : 0.0;
-            vtab[2 * PW + lane] = pvalid ? V.v3 : 0.0;
-            vtab[3 * PW + lane] = pvalid ? V.vsq : 0.0;
+            vtab[0 * PW + lane] = pvalid ? V1 : 0.0;
+            vtab[1 * PW + lane] = pvalid ? V2 : 0.0;
+            vtab[2 * PW + lane] = pvalid ? V3 : 0.0;
+            vtab[3 * PW + lane] = pvalid ? (V1 * V1 + V2 * V2) + V3 * V3 : 0.0;
         }
         {
             const bool right = v2 > T(0);
             const int off = right ? 0 : 1;
             Weno5Side<T> S; S.set(right);
-            const int ntab_off2 = a.Np1 + ip2, ntab_off3 = a.Np1 + a.Np2 + ip3;
+            const int toff1 = jp1, toff2 = Np1 + jp2, toff3 = Np1 + Np2 + jp3;
 #pragma unroll
             for (int it = 0; it < ITEMS; ++it) {
-                const int item = warp + it * (NTHREADS / 32);
-                const int ic = item / NSEGB, sg = item % NSEGB;
-                const int rb = sg * SEGB;
+                const int item = warp + it * NWARP;
+                const int ic = item / NSEGB;
                 const T* col = X + (ic + HALO) * PW + lane;
+                const T* colw = col + (rb0 + off) * HX * PW;
                 T y0, y1, y2, y3, y4, Fprev = T(0), fprev = T(0);
                 FaceWalker<RECON, EXACT, T> W;
                 if (Q2) {
-                    y0 = col[((rb + off + 0) * HX) * PW]; y1 = col[((rb + off + 1) * HX) * PW];
-                    y2 = col[((rb + off + 2) * HX) * PW]; y3 = col[((rb + off + 3) * HX) * PW];
-                    y4 = col[((rb + off + 4) * HX) * PW];
+                    y0 = colw[0 * HX * PW]; y1 = colw[1 * HX * PW]; y2 = colw[2 * HX * PW];
+                    y3 = colw[3 * HX * PW]; y4 = colw[4 * HX * PW];
                     fprev = W.first(y0, y1, y2, y3, y4, right, S);
                     Fprev = v2 * fprev;
                 }
 #pragma unroll
                 for (int r = 0; r < SEGB; ++r) {
-                    const int rr = rb + r;
+                    const int rr = rb0 + r;
                     if (rr >= TQ2) break;
                     const int ii = i0 + ic, jj = j0 + rr;
-                    const bool cvalid = pvalid && ii < a.Nq1 && jj < a.Nq2;
+                    const bool cvalid = fast || (pvalid && ii < Nq1 && jj < Nq2);
                     const int cq = rr * TQ1 + ic;
                     T kq = stage[cq * PWP + lane];
                     T fcell = col[((Q2 ? rr + HALO : 0) * HX) * PW];
                     T fbot = fprev;
                     if (Q2) {
                         y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                        y4 = col[((rr + 1 + off + 4) * HX) * PW];
+                        y4 = colw[(r + 5) * HX * PW];
                         T fn = W.next(y0, y1, y2, y3, y4, right, S);
                         T Fn = v2 * fn;
                         if (EXACT) kq = kq - (Fn - Fprev) / T(a.dq2);
@@ -363,55 +377,52 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                         fprev = fn;
                     }
                     T kk = kq;
-                    const long long gidx = (long long)(jj + a.Ng) * colstride
-                                         + (long long)(ii + a.Ng) * rowstride
-                                         + (long long)s * a.Np + p;
+                    const long long gidx = tbase + it * item_step + r * colstride + p;
                     if (BGK) {
                         double fmb;
+                        const double* qq = qc + cq * 5;
                         if (a.bgk_direct) {
                             // f0 of collision_operator.py:52-65 evaluated per cell
-                            const double* qq = qc + cq * 5;
-                            const double mneg = -a.sg.mass[s];
-                            double d1v = V.v1 - qq[1];
+                            double d1v = V1 - qq[1];
                             fmb = qq[0] * exp((mneg * (d1v * d1v)) / qq[4]);
                             if (a.p_dim >= 2) {
-                                double d2v = V.v2 - qq[2];
+                                double d2v = V2 - qq[2];
                                 fmb = fmb * exp((mneg * (d2v * d2v)) / qq[4]);
                             }
                             if (a.p_dim == 3) {
-                                double d3v = V.v3 - qq[3];
+                                double d3v = V3 - qq[3];
                                 fmb = fmb * exp((mneg * (d3v * d3v)) / qq[4]);
                             }
                         } else {
-                            const double* tb = tabs + (long long)cq * ntab;
-                            fmb = (tb[ip1] * tb[ntab_off2]) * tb[ntab_off3];
+                            const double* tb = tabs + cq * ntab;
+                            fmb = (tb[toff1] * tb[toff2]) * tb[toff3];
                         }
                         if (EXACT) {
                             double tauv = tau_arr ? double(tau_arr[cvalid ? gidx : 0]) : a.tau;
                             kk = T(double(kk) + (-(double(fcell) - fmb) / tauv));
                         } else {
-                            T it = tau_arr ? T(1) / tau_arr[cvalid ? gidx : 0] : inv_tau;
-                            kk = kk + (T(fmb) - fcell) * it;
+                            T itau = tau_arr ? T(1) / tau_arr[cvalid ? gidx : 0] : inv_tau;
+                            kk = kk + (T(fmb) - fcell) * itau;
                         }
                     }
-                    if (a.want_j) {
-                        double jc2 = cvalid ? double(fbot) * V.v2 : 0.0;
-                        double jc3 = cvalid ? double(fcell) * V.v3 : 0.0;
+                    if (want_j) {
+                        double jc2 = cvalid ? double(fbot) * V2 : 0.0;
+                        double jc3 = cvalid ? double(fcell) * V3 : 0.0;
                         jc2 = warp_sum(jc2);
                         jc3 = warp_sum(jc3);
                         if (lane == 0) { j_acc[cq * 3 + 1] += jc2; j_acc[cq * 3 + 2] += jc3; }
                     }
                     // RK stage combine (fvm_operator.py:26,33; integrators.py:18-25)
-                    T o1 = base1 ? pre1[it * SEGB + r] + kk * c1 : kk;
+                    const T o1 = base1 ? pre1[it * SEGB + r] + kk * c1 : kk;
                     if (cvalid) {
                         out1[gidx] = o1;
                         if (out2) out2[gidx] = pre2[it * SEGB + r] + kk * c2;
                         // wrap-around ghost copies (what the next halo refresh would do)
-                        if ((a.periodic1 && (ii < a.Ng || ii >= a.Nq1 - a.Ng)) ||
-                            (a.periodic2 && (jj < a.Ng || jj >= a.Nq2 - a.Ng)))
-                            write_ghost_images(out1, o1, ii, jj, s, p, a.Ng, a.Nq1, a.Nq2,
+                        if (border && ((a.periodic1 && (ii < Ng || ii >= Nq1 - Ng)) ||
+                                       (a.periodic2 && (jj < Ng || jj >= Nq2 - Ng))))
+                            write_ghost_images(out1, o1, ii, jj, s, p, Ng, Nq1, Nq2,
                                                a.Nq1g, a.Nq2g, a.periodic1, a.periodic2,
-                                               rowstride, colstride, a.Np);
+                                               rowstride, colstride, Np);
                         if (a.flag && !isfinite(o1)) atomicOr(a.flag, 1);
                     }
                     stage[cq * PWP + lane] = cvalid ? o1 : T(0);
@@ -436,11 +447,18 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                 macc[4] += (0.5 * ov) * vt[3 * PW + t];
             }
         }
+        // advance this lane's p by one chunk
+        p += PW;
+        ip1 += PW;
+        while (ip1 >= Np1) {
+            ip1 -= Np1;
+            if (++ip2 == Np2) { ip2 = 0; ++ip3; }
+        }
     }
     __syncthreads();
 
     // ---- epilogue: partial moments / currents of this split ------------------
-    const long long plane = (long long)a.Nq2 * a.Nq1;
+    const long long plane = (long long)Nq2 * Nq1;
     if (want_mom) {
         double* red = reinterpret_cast<double*>(smem_raw + Lo.tile);   // tile no longer used
 #pragma unroll
@@ -452,18 +470,18 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
 #pragma unroll
             for (int h = 0; h < NQUART; ++h) v += red[(h * NQ + cq) * kNumMom + q];
             int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
-            if (ii < a.Nq1 && jj < a.Nq2)
+            if (ii < Nq1 && jj < Nq2)
                 a.mom_out[(((long long)split * kNumMom + q) * a.Ns + s) * plane
-                          + (long long)jj * a.Nq1 + ii] = v;
+                          + (long long)jj * Nq1 + ii] = v;
         }
     }
-    if (a.want_j && a.j_out) {
+    if (want_j && a.j_out) {
         for (int c = tid; c < NQ * 3; c += NTHREADS) {
             int cq = c / 3, q = c % 3;
             int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
-            if (ii < a.Nq1 && jj < a.Nq2)
+            if (ii < Nq1 && jj < Nq2)
                 a.j_out[(((long long)split * 3 + q) * a.Ns + s) * plane
-                        + (long long)jj * a.Nq1 + ii] = j_acc[c];
+                        + (long long)jj * Nq1 + ii] = j_acc[c];
         }
     }
 }
