@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -78,6 +79,7 @@ struct BoltCtx {
     size_t scratch_bytes;
     TmapEntry tmaps[4];
     int ntmaps;
+    int pair_enabled;       // paired FP32 kernel allowed (BOLT_NO_PAIR unset)
 };
 
 #define CK(x)                                             \
@@ -212,6 +214,7 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
     ctx->use_tma_ok = (g.N_ghost >= HALO) && (rowbytes % 16 == 0) &&
                       (((size_t)ctx->Np * ctx->elem) % 16 == 0) && get_encode_fn() != nullptr;
     ctx->at_n = 1;
+    ctx->pair_enabled = getenv("BOLT_NO_PAIR") == nullptr;
 
     int rc = BOLT_OK;
     const size_t fbytes = ctx->fcount * ctx->elem;
@@ -406,9 +409,16 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     a.sg = ctx->sg;
     dim3 grid(ctx->ntiles1 * ctx->ntiles2, g.N_s * ctx->nsplit);
     const size_t smem = qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct, ctx->ntab);
+    // the paired FP32 kernel covers the fused WENO5 2-D stage; everything
+    // else (FP64, other reconstructions, 1-D tilings, write-k mode, currents,
+    // no TMA) runs the scalar kernel
+    const bool pair = ctx->elem == 4 && ctx->recon_q == BOLT_RECON_WENO5 &&
+                      ctx->tiling == TILING_2D && !write_k && !want_j && a.use_tma &&
+                      a.base1 != nullptr && ctx->pair_enabled;
     cudaError_t e = ctx->elem == 8
         ? launch_qstage_f64(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st)
-        : launch_qstage_f32(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st);
+        : (pair ? launch_qpair_f32(a, ctx->bgk, grid, smem, st)
+                : launch_qstage_f32(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st));
     ctx->launches++;
     CK(e);
     return BOLT_OK;

@@ -279,6 +279,75 @@ struct FaceWalker {
 };
 
 // ---------------------------------------------------------------------------
+// Paired FP32 (two q-cells per thread, same p) WENO5 walker, using the
+// sm_100 f32x2 arithmetic.  Both components share the lane's upwind side, so
+// they share the coefficient set.  Smoothness indicators use a constant
+// 1e-17 floor (the reference's 1e-17*(1+|a|+|b|+|c|) differs from it only
+// where f varies by less than FP32 resolves).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(fast_rcp(a.x), fast_rcp(a.y)); }
+
+struct Weno5Pair {
+    float2 cw1, cw2, cw3;
+    float2 a10, a11, a12, a20, a21, a22, a30, a31, a32;
+    __device__ __forceinline__ void set(bool right) {
+        cw2 = f2(0.625f);
+        cw1 = f2(right ? 0.0625f : 0.3125f);
+        cw3 = f2(right ? 0.3125f : 0.0625f);
+        if (right) {
+            a10 = f2(0.375f);  a11 = f2(-1.25f); a12 = f2(1.875f);
+            a20 = f2(-0.125f); a21 = f2(0.75f);  a22 = f2(0.375f);
+            a30 = f2(0.375f);  a31 = f2(0.75f);  a32 = f2(-0.125f);
+        } else {
+            a10 = f2(-0.125f); a11 = f2(0.75f);  a12 = f2(0.375f);
+            a20 = f2(0.375f);  a21 = f2(0.75f);  a22 = f2(-0.125f);
+            a30 = f2(1.875f);  a31 = f2(-1.25f); a32 = f2(0.375f);
+        }
+    }
+};
+
+__device__ __forceinline__ float2 beta_pair(float2 a, float2 b, float2 c) {
+    const float2 d1 = fma2(f2(-2.0f), b, add2(a, c));            // a - 2b + c
+    const float2 d2 = fma2(f2(3.0f), c, fma2(f2(-4.0f), b, a));   // a - 4b + 3c
+    return fma2(mul2(f2(13.0f / 12.0f), d1), d1, fma2(mul2(f2(0.25f), d2), d2, f2(1e-17f)));
+}
+
+struct Weno5PairWalker {
+    float2 q2, q3;   // 1/beta^2 of substencils 2 and 3
+    __device__ __forceinline__ static float2 inv_sq(float2 b) {
+        const float2 r = rcp2(b);
+        return mul2(r, r);
+    }
+    __device__ __forceinline__ float2 eval(float2 q1, float2 y0, float2 y1, float2 y2, float2 y3,
+                                           float2 y4, const Weno5Pair& S) {
+        const float2 w1 = mul2(S.cw1, q1), w2 = mul2(S.cw2, q2), w3 = mul2(S.cw3, q3);
+        const float2 u1 = fma2(S.a12, y2, fma2(S.a11, y1, mul2(S.a10, y0)));
+        const float2 u2 = fma2(S.a22, y3, fma2(S.a21, y2, mul2(S.a20, y1)));
+        const float2 u3 = fma2(S.a32, y4, fma2(S.a31, y3, mul2(S.a30, y2)));
+        const float2 num = fma2(w3, u3, fma2(w2, u2, mul2(w1, u1)));
+        return mul2(num, rcp2(add2(add2(w1, w2), w3)));
+    }
+    __device__ __forceinline__ float2 first(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
+                                            const Weno5Pair& S) {
+        const float2 q1 = inv_sq(beta_pair(y0, y1, y2));
+        q2 = inv_sq(beta_pair(y1, y2, y3));
+        q3 = inv_sq(beta_pair(y2, y3, y4));
+        return eval(q1, y0, y1, y2, y3, y4, S);
+    }
+    __device__ __forceinline__ float2 next(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
+                                           const Weno5Pair& S) {
+        const float2 q1 = q2;
+        q2 = q3;
+        q3 = inv_sq(beta_pair(y2, y3, y4));
+        return eval(q1, y0, y1, y2, y3, y4, S);
+    }
+};
+
+// ---------------------------------------------------------------------------
 // mbarrier + TMA (cp.async.bulk.tensor) wrappers.  Waits are bounded: after
 // kWaitCycles clock cycles the wait reports failure and the caller records
 // BOLT_ERR_TIMEOUT instead of hanging.

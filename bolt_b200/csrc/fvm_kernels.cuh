@@ -68,69 +68,19 @@ __device__ __forceinline__ void write_ghost_images(T* out, T v, int ii, int jj, 
 }
 
 // ---------------------------------------------------------------------------
-// q-stage kernel
-//
-// Per p-chunk (32 consecutive p of one species) and q-tile:
-//   phase A  q1 faces: one upwind face value per face, walking each tile row
-//            with a sliding window; D1 = (-(F_R - F_L)) / dq1 -> stage buffer
-//   phase B  q2 faces likewise, BGK, RK combine; writes out1/out2 to global
-//            and out1 back into the stage buffer
-//   phase C  FP64 moments of out1 from the stage buffer: each thread owns one
-//            q-cell and a quarter of the chunk's p values, accumulating in
-//            registers across all chunks of the CTA (reduced once at the end)
+// q-stage prologue shared by the scalar and paired kernels: zero the current
+// accumulators, the species' p-cell centres, the TMA barriers, and for BGK the
+// Maxwellian of the stage input per q-cell (collision_operator.py:102-118,
+// f0 :49-65) with its per-q-cell exp tables (the p1 table carries n*A).
 // ---------------------------------------------------------------------------
-template <typename T, bool EXACT, int RECON, int TQ1, int TQ2, bool Q2, bool BGK>
-__global__ void __launch_bounds__(NTHREADS, 2)
-qstage_kernel(const __grid_constant__ QStageArgs a) {
-    constexpr int HX = TQ1 + 2 * HALO;
-    constexpr int HY = Q2 ? TQ2 + 2 * HALO : 1;
-    constexpr int NQ = TQ1 * TQ2;
-    constexpr int NWARP = NTHREADS / 32;
-    constexpr int NQUART = NTHREADS / NQ;       // threads per q-cell in phase C
-    constexpr int PQ = PW / NQUART;             // p values per phase-C thread
-    static_assert(NTHREADS % NQ == 0 && PW % NQUART == 0, "phase C mapping");
-    constexpr int TILE = HY * HX * PW;
-    // phase A: rows split into NSEG segments; phase B: ITEMS (column, segment)
-    // items per warp of SEGB rows each -> NSLOT cells per thread
-    constexpr int NSEG = (TQ2 >= NWARP) ? 1 : (NWARP / TQ2);
-    constexpr int SEG = (TQ1 + NSEG - 1) / NSEG;
-    constexpr int NSEGB = (TQ1 >= NWARP) ? 1 : (NWARP / TQ1);
-    constexpr int SEGB = (TQ2 + NSEGB - 1) / NSEGB;
-    constexpr int ITEMS = TQ1 * NSEGB / NWARP;
-    static_assert(TQ1 * NSEGB % NWARP == 0, "phase B items per warp");
-    constexpr int NSLOT = ITEMS * SEGB;
-
-    const int Np1 = a.Np1, Np2 = a.Np2, Np3 = a.Np3, Np = a.Np, Ng = a.Ng;
+template <int NQ, int TQ1, bool BGK>
+__device__ __forceinline__ void qstage_prologue(const QStageArgs& a, int s, int i0, int j0,
+                                                double* j_acc, double* vgrid, double* qc,
+                                                double* tabs, uint64_t* bars) {
+    const int tid = threadIdx.x;
+    const int Np1 = a.Np1, Np2 = a.Np2, Np3 = a.Np3;
     const int Nq1 = a.Nq1, Nq2 = a.Nq2;
     const int ntab = Np1 + Np2 + Np3;
-    const QLayout Lo = qstage_layout(TQ1, TQ2, Q2, sizeof(T), BGK, a.bgk_direct, ntab);
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    T* tile = reinterpret_cast<T*>(smem_raw + Lo.tile);              // [2][HY][HX][PW]
-    T* stage = reinterpret_cast<T*>(smem_raw + Lo.stage);            // [NQ][PWP]
-    double* vtab = reinterpret_cast<double*>(smem_raw + Lo.vtab);    // [4][PW]
-    double* j_acc = reinterpret_cast<double*>(smem_raw + Lo.jacc);   // [NQ][3]
-    double* qc = reinterpret_cast<double*>(smem_raw + Lo.qc);        // [NQ][5]
-    double* tabs = reinterpret_cast<double*>(smem_raw + Lo.tabs);    // [NQ][ntab]
-    double* vgrid = reinterpret_cast<double*>(smem_raw + Lo.vgrid);  // [ntab]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + Lo.bars);
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
-    const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
-    const int i0 = tile1 * TQ1, j0 = tile2 * TQ2;                     // interior origin
-    const int nchunks = (Np + PW - 1) / PW;
-    const int k_begin = split * a.chunks_per_split;
-    const int k_end = min(nchunks, k_begin + a.chunks_per_split);
-    const long long rowstride = (long long)a.Ns * Np;                 // per q1 step
-    const long long colstride = rowstride * a.Nq1g;                   // per q2 step
-    const T* fs = static_cast<const T*>(a.fs);
-    // CTA-uniform predicates: whole tile inside the domain and every chunk
-    // complete (no per-cell masks), tile within reach of a periodic border
-    const bool tile_full = (i0 + TQ1 <= Nq1) && (j0 + TQ2 <= Nq2);
-    const bool fast = tile_full && a.full_chunks;
-    const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ1 > Nq1 - Ng)) ||
-                        (a.periodic2 && (j0 < Ng || j0 + TQ2 > Nq2 - Ng));
-
     for (int c = tid; c < NQ * 3; c += NTHREADS) j_acc[c] = 0.0;
     for (int q = tid; q < ntab; q += NTHREADS) {
         if (q < Np1) vgrid[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
@@ -196,6 +146,74 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         }
     }
     __syncthreads();
+
+}
+
+// ---------------------------------------------------------------------------
+// q-stage kernel
+//
+// Per p-chunk (32 consecutive p of one species) and q-tile:
+//   phase A  q1 faces: one upwind face value per face, walking each tile row
+//            with a sliding window; D1 = (-(F_R - F_L)) / dq1 -> stage buffer
+//   phase B  q2 faces likewise, BGK, RK combine; writes out1/out2 to global
+//            and out1 back into the stage buffer
+//   phase C  FP64 moments of out1 from the stage buffer: each thread owns one
+//            q-cell and a quarter of the chunk's p values, accumulating in
+//            registers across all chunks of the CTA (reduced once at the end)
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT, int RECON, int TQ1, int TQ2, bool Q2, bool BGK>
+__global__ void __launch_bounds__(NTHREADS, 2)
+qstage_kernel(const __grid_constant__ QStageArgs a) {
+    constexpr int HX = TQ1 + 2 * HALO;
+    constexpr int HY = Q2 ? TQ2 + 2 * HALO : 1;
+    constexpr int NQ = TQ1 * TQ2;
+    constexpr int NWARP = NTHREADS / 32;
+    constexpr int NQUART = NTHREADS / NQ;       // threads per q-cell in phase C
+    constexpr int PQ = PW / NQUART;             // p values per phase-C thread
+    static_assert(NTHREADS % NQ == 0 && PW % NQUART == 0, "phase C mapping");
+    constexpr int TILE = HY * HX * PW;
+    // phase A: rows split into NSEG segments; phase B: ITEMS (column, segment)
+    // items per warp of SEGB rows each -> NSLOT cells per thread
+    constexpr int NSEG = (TQ2 >= NWARP) ? 1 : (NWARP / TQ2);
+    constexpr int SEG = (TQ1 + NSEG - 1) / NSEG;
+    constexpr int NSEGB = (TQ1 >= NWARP) ? 1 : (NWARP / TQ1);
+    constexpr int SEGB = (TQ2 + NSEGB - 1) / NSEGB;
+    constexpr int ITEMS = TQ1 * NSEGB / NWARP;
+    static_assert(TQ1 * NSEGB % NWARP == 0, "phase B items per warp");
+    constexpr int NSLOT = ITEMS * SEGB;
+
+    const int Np1 = a.Np1, Np2 = a.Np2, Np3 = a.Np3, Np = a.Np, Ng = a.Ng;
+    const int Nq1 = a.Nq1, Nq2 = a.Nq2;
+    const int ntab = Np1 + Np2 + Np3;
+    const QLayout Lo = qstage_layout(TQ1, TQ2, Q2, sizeof(T), BGK, a.bgk_direct, ntab);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* tile = reinterpret_cast<T*>(smem_raw + Lo.tile);              // [2][HY][HX][PW]
+    T* stage = reinterpret_cast<T*>(smem_raw + Lo.stage);            // [NQ][PWP]
+    double* vtab = reinterpret_cast<double*>(smem_raw + Lo.vtab);    // [4][PW]
+    double* j_acc = reinterpret_cast<double*>(smem_raw + Lo.jacc);   // [NQ][3]
+    double* qc = reinterpret_cast<double*>(smem_raw + Lo.qc);        // [NQ][5]
+    double* tabs = reinterpret_cast<double*>(smem_raw + Lo.tabs);    // [NQ][ntab]
+    double* vgrid = reinterpret_cast<double*>(smem_raw + Lo.vgrid);  // [ntab]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + Lo.bars);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
+    const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
+    const int i0 = tile1 * TQ1, j0 = tile2 * TQ2;                     // interior origin
+    const int nchunks = (Np + PW - 1) / PW;
+    const int k_begin = split * a.chunks_per_split;
+    const int k_end = min(nchunks, k_begin + a.chunks_per_split);
+    const long long rowstride = (long long)a.Ns * Np;                 // per q1 step
+    const long long colstride = rowstride * a.Nq1g;                   // per q2 step
+    const T* fs = static_cast<const T*>(a.fs);
+    // CTA-uniform predicates: whole tile inside the domain and every chunk
+    // complete (no per-cell masks), tile within reach of a periodic border
+    const bool tile_full = (i0 + TQ1 <= Nq1) && (j0 + TQ2 <= Nq2);
+    const bool fast = tile_full && a.full_chunks;
+    const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ1 > Nq1 - Ng)) ||
+                        (a.periodic2 && (j0 < Ng || j0 + TQ2 > Nq2 - Ng));
+
+    qstage_prologue<NQ, TQ1, BGK>(a, s, i0, j0, j_acc, vgrid, qc, tabs, bars);
 
     // ---- tile loader -------------------------------------------------------
     bool failed = false;       // a bounded wait gave up: finish without TMA
@@ -482,6 +500,279 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
             if (ii < Nq1 && jj < Nq2)
                 a.j_out[(((long long)split * 3 + q) * a.Ns + s) * plane
                         + (long long)jj * Nq1 + ii] = j_acc[c];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Paired FP32 WENO5 q-stage kernel (8x8 q-tile, fields off, fused combine).
+// Same stages as qstage_kernel, but every thread walks two adjacent q-rows
+// (phase A) or q-columns (phase B) of the same p at once with f32x2
+// arithmetic:
+//   phase A  warp w: rows 2(w%4), 2(w%4)+1, cells 4(w/4) .. +3 (5 faces)
+//   phase B  warp w: cols 2(w%4), 2(w%4)+1, rows  4(w/4) .. +3 (5 faces)
+// ---------------------------------------------------------------------------
+template <bool BGK>
+__global__ void __launch_bounds__(NTHREADS, 2)
+qpair_kernel(const __grid_constant__ QStageArgs a) {
+    constexpr int TQ1 = 8, TQ2 = 8;
+    constexpr int HX = TQ1 + 2 * HALO, HY = TQ2 + 2 * HALO;
+    constexpr int NQ = TQ1 * TQ2;
+    constexpr int NWARP = NTHREADS / 32;
+    constexpr int NQUART = NTHREADS / NQ;
+    constexpr int PQ = PW / NQUART;
+    constexpr int TILE = HY * HX * PW;
+    static_assert(NWARP == 8, "pair mapping assumes 8 warps");
+
+    const int Np1 = a.Np1, Np2 = a.Np2, Np = a.Np, Ng = a.Ng;
+    const int Nq1 = a.Nq1, Nq2 = a.Nq2;
+    const int ntab = Np1 + Np2 + a.Np3;
+    const QLayout Lo = qstage_layout(TQ1, TQ2, 1, sizeof(float), BGK, a.bgk_direct, ntab);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* tile = reinterpret_cast<float*>(smem_raw + Lo.tile);
+    float* stage = reinterpret_cast<float*>(smem_raw + Lo.stage);
+    double* vtab = reinterpret_cast<double*>(smem_raw + Lo.vtab);
+    double* j_acc = reinterpret_cast<double*>(smem_raw + Lo.jacc);
+    double* qc = reinterpret_cast<double*>(smem_raw + Lo.qc);
+    double* tabs = reinterpret_cast<double*>(smem_raw + Lo.tabs);
+    double* vgrid = reinterpret_cast<double*>(smem_raw + Lo.vgrid);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + Lo.bars);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
+    const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
+    const int i0 = tile1 * TQ1, j0 = tile2 * TQ2;
+    const int nchunks = (Np + PW - 1) / PW;
+    const int k_begin = split * a.chunks_per_split;
+    const int k_end = min(nchunks, k_begin + a.chunks_per_split);
+    const long long rowstride = (long long)a.Ns * Np;
+    const long long colstride = rowstride * a.Nq1g;
+    const bool tile_full = (i0 + TQ1 <= Nq1) && (j0 + TQ2 <= Nq2);
+    const bool fast = tile_full && a.full_chunks;
+    const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ1 > Nq1 - Ng)) ||
+                        (a.periodic2 && (j0 < Ng || j0 + TQ2 > Nq2 - Ng));
+
+    qstage_prologue<NQ, TQ1, BGK>(a, s, i0, j0, j_acc, vgrid, qc, tabs, bars);
+
+    bool failed = false;
+    const unsigned tile_bytes = TILE * sizeof(float);
+    auto issue = [&](int k, int buf) {
+        if (k >= k_end) return;
+        if (tid == 0 && !failed) {
+            mbar_arrive_expect_tx(&bars[buf], tile_bytes);
+            tma_load_3d(tile + buf * TILE, &a.tmap, &bars[buf], s * Np + k * PW,
+                        i0 + Ng - HALO, j0 + Ng - HALO);
+        }
+    };
+    unsigned phase0 = 0u, phase1 = 0u;
+    issue(k_begin, 0);
+    issue(k_begin + 1, 1);
+
+    float* out1 = static_cast<float*>(a.out1);
+    float* out2 = static_cast<float*>(a.out2);
+    const float* base1 = static_cast<const float*>(a.base1);
+    const float* base2 = static_cast<const float*>(a.base2);
+    const float* tau_arr = static_cast<const float*>(a.tau_arr);
+    const float c1 = float(a.c1), c2 = float(a.c2);
+    const float inv_tau = float(1.0 / a.tau);
+    const float2 inv_dq1 = f2(float(1.0 / a.dq1)), inv_dq2 = f2(float(1.0 / a.dq2));
+    const double mneg = -a.sg.mass[s];
+    const bool want_mom = a.mom_out != nullptr;
+    const int pc_c = tid % NQ, pc_q = tid / NQ;
+    double macc[kNumMom] = {0, 0, 0, 0, 0};
+
+    int p = k_begin * PW + lane;
+    int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
+    // phase A / B ownership
+    const int rp = warp & 3, seg = warp >> 2;          // row/column pair, segment
+    const int a_row = 2 * rp, a_c0 = 4 * seg;          // phase A: rows a_row, a_row+1
+    const int b_col = 2 * rp, b_r0 = 4 * seg;          // phase B: cols b_col, b_col+1
+    const long long tbase = (long long)(j0 + b_r0 + Ng) * colstride
+                          + (long long)(i0 + b_col + Ng) * rowstride + (long long)s * Np;
+
+    int buf = 0;
+    for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
+        if (!failed) {
+            const unsigned ph = buf ? phase1 : phase0;
+            if (!mbar_wait_bounded(&bars[buf], ph)) {
+                atomicExch(a.err, 4);
+                failed = true;
+            }
+            if (buf) phase1 ^= 1u; else phase0 ^= 1u;
+        }
+        __syncthreads();
+        const float* X = tile + buf * TILE;
+        const bool pvalid = p < Np;
+        const int jp1 = pvalid ? ip1 : 0, jp2 = pvalid ? ip2 : 0, jp3 = pvalid ? ip3 : 0;
+        const double V1 = vgrid[jp1], V2 = vgrid[Np1 + jp2], V3 = vgrid[Np1 + Np2 + jp3];
+
+        // prefetch combine operands of the 8 phase-B cells (col x, row r)
+        float pre1[2][4], pre2[2][4];
+#pragma unroll
+        for (int x = 0; x < 2; ++x)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const bool cvalid = fast || (pvalid && i0 + b_col + x < Nq1 && j0 + b_r0 + r < Nq2);
+                const long long g = tbase + x * rowstride + r * colstride + p;
+                pre1[x][r] = cvalid ? base1[g] : 0.0f;
+                pre2[x][r] = (base2 && cvalid) ? base2[g] : 0.0f;
+            }
+
+        // ---- phase A: q1 faces of rows a_row, a_row+1 -------------------------
+        {
+            const float v1 = float(V1);
+            const bool right = v1 > 0.0f;
+            const int off = right ? 0 : 1;
+            Weno5Pair S; S.set(right);
+            const float* ra = X + ((a_row + HALO) * HX + a_c0 + off) * PW + lane;
+            const float* rb = ra + HX * PW;
+            float2 y0 = make_float2(ra[0 * PW], rb[0 * PW]);
+            float2 y1 = make_float2(ra[1 * PW], rb[1 * PW]);
+            float2 y2 = make_float2(ra[2 * PW], rb[2 * PW]);
+            float2 y3 = make_float2(ra[3 * PW], rb[3 * PW]);
+            float2 y4 = make_float2(ra[4 * PW], rb[4 * PW]);
+            Weno5PairWalker W;
+            const float2 vv = f2(v1);
+            float2 Fprev = mul2(vv, W.first(y0, y1, y2, y3, y4, S));
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                y0 = y1; y1 = y2; y2 = y3; y3 = y4;
+                y4 = make_float2(ra[(c + 5) * PW], rb[(c + 5) * PW]);
+                const float2 Fn = mul2(vv, W.next(y0, y1, y2, y3, y4, S));
+                const float2 d = mul2(add2(Fprev, make_float2(-Fn.x, -Fn.y)), inv_dq1);
+                stage[(a_row * TQ1 + a_c0 + c) * PWP + lane] = d.x;
+                stage[((a_row + 1) * TQ1 + a_c0 + c) * PWP + lane] = d.y;
+                Fprev = Fn;
+            }
+        }
+        __syncthreads();
+
+        // ---- phase B: q2 faces of cols b_col, b_col+1, BGK, combine ------------
+        if (warp == 0) {
+            vtab[0 * PW + lane] = pvalid ? V1 : 0.0;
+            vtab[1 * PW + lane] = pvalid ? V2 : 0.0;
+            vtab[2 * PW + lane] = pvalid ? V3 : 0.0;
+            vtab[3 * PW + lane] = pvalid ? (V1 * V1 + V2 * V2) + V3 * V3 : 0.0;
+        }
+        {
+            const float v2 = float(V2);
+            const bool right = v2 > 0.0f;
+            const int off = right ? 0 : 1;
+            Weno5Pair S; S.set(right);
+            const float* ca = X + ((b_r0 + off) * HX + b_col + HALO) * PW + lane;
+            const float* cb = ca + PW;
+            const float* cella = X + ((b_r0 + HALO) * HX + b_col + HALO) * PW + lane;
+            float2 y0 = make_float2(ca[0 * HX * PW], cb[0 * HX * PW]);
+            float2 y1 = make_float2(ca[1 * HX * PW], cb[1 * HX * PW]);
+            float2 y2 = make_float2(ca[2 * HX * PW], cb[2 * HX * PW]);
+            float2 y3 = make_float2(ca[3 * HX * PW], cb[3 * HX * PW]);
+            float2 y4 = make_float2(ca[4 * HX * PW], cb[4 * HX * PW]);
+            Weno5PairWalker W;
+            const float2 vv = f2(v2);
+            float2 Fprev = mul2(vv, W.first(y0, y1, y2, y3, y4, S));
+            const int toff1 = jp1, toff2 = Np1 + jp2, toff3 = Np1 + Np2 + jp3;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int rr = b_r0 + r;
+                const int cq0 = rr * TQ1 + b_col;
+                y0 = y1; y1 = y2; y2 = y3; y3 = y4;
+                y4 = make_float2(ca[(r + 5) * HX * PW], cb[(r + 5) * HX * PW]);
+                const float2 Fn = mul2(vv, W.next(y0, y1, y2, y3, y4, S));
+                const float2 kq0 = make_float2(stage[cq0 * PWP + lane], stage[(cq0 + 1) * PWP + lane]);
+                float2 kk = fma2(make_float2(Fprev.x - Fn.x, Fprev.y - Fn.y), inv_dq2, kq0);
+                Fprev = Fn;
+                const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
+                const long long g0 = tbase + r * colstride + p;
+                if (BGK) {
+                    double fmb[2];
+#pragma unroll
+                    for (int x = 0; x < 2; ++x) {
+                        const int cq = cq0 + x;
+                        if (a.bgk_direct) {
+                            const double* qq = qc + cq * 5;
+                            double d1v = V1 - qq[1];
+                            double f0 = qq[0] * exp((mneg * (d1v * d1v)) / qq[4]);
+                            if (a.p_dim >= 2) { double d2v = V2 - qq[2]; f0 = f0 * exp((mneg * (d2v * d2v)) / qq[4]); }
+                            if (a.p_dim == 3) { double d3v = V3 - qq[3]; f0 = f0 * exp((mneg * (d3v * d3v)) / qq[4]); }
+                            fmb[x] = f0;
+                        } else {
+                            const double* tb = tabs + cq * ntab;
+                            fmb[x] = (tb[toff1] * tb[toff2]) * tb[toff3];
+                        }
+                    }
+                    float itx = inv_tau, ity = inv_tau;
+                    if (tau_arr) {
+                        const bool v0 = fast || (pvalid && i0 + b_col < Nq1 && j0 + rr < Nq2);
+                        const bool v1c = fast || (pvalid && i0 + b_col + 1 < Nq1 && j0 + rr < Nq2);
+                        itx = 1.0f / tau_arr[v0 ? g0 : 0];
+                        ity = 1.0f / tau_arr[v1c ? g0 + rowstride : 0];
+                    }
+                    kk = fma2(make_float2(float(fmb[0]) - fcell.x, float(fmb[1]) - fcell.y),
+                              make_float2(itx, ity), kk);
+                }
+                const float kkx[2] = {kk.x, kk.y};
+#pragma unroll
+                for (int x = 0; x < 2; ++x) {
+                    const int ii = i0 + b_col + x, jj = j0 + rr;
+                    const bool cvalid = fast || (pvalid && ii < Nq1 && jj < Nq2);
+                    const long long g = g0 + x * rowstride;
+                    const float o1 = fmaf(kkx[x], c1, pre1[x][r]);
+                    if (cvalid) {
+                        out1[g] = o1;
+                        if (out2) out2[g] = fmaf(kkx[x], c2, pre2[x][r]);
+                        if (border && ((a.periodic1 && (ii < Ng || ii >= Nq1 - Ng)) ||
+                                       (a.periodic2 && (jj < Ng || jj >= Nq2 - Ng))))
+                            write_ghost_images(out1, o1, ii, jj, s, p, Ng, Nq1, Nq2,
+                                               a.Nq1g, a.Nq2g, a.periodic1, a.periodic2,
+                                               rowstride, colstride, Np);
+                        if (a.flag && !isfinite(o1)) atomicOr(a.flag, 1);
+                    }
+                    stage[(cq0 + x) * PWP + lane] = cvalid ? o1 : 0.0f;
+                }
+            }
+        }
+        __syncthreads();
+        fence_proxy_async();
+        issue(k + 2, buf);
+
+        // ---- phase C: FP64 moments of out1 ------------------------------------
+        if (want_mom) {
+            const float* sp = stage + pc_c * PWP + pc_q * PQ;
+            const double* vt = vtab + pc_q * PQ;
+#pragma unroll
+            for (int t = 0; t < PQ; ++t) {
+                const double ov = double(sp[t]);
+                macc[0] += ov;
+                macc[1] += ov * vt[t];
+                macc[2] += ov * vt[PW + t];
+                macc[3] += ov * vt[2 * PW + t];
+                macc[4] += (0.5 * ov) * vt[3 * PW + t];
+            }
+        }
+        p += PW;
+        ip1 += PW;
+        while (ip1 >= Np1) {
+            ip1 -= Np1;
+            if (++ip2 == Np2) { ip2 = 0; ++ip3; }
+        }
+    }
+    __syncthreads();
+
+    const long long plane = (long long)Nq2 * Nq1;
+    if (want_mom) {
+        double* red = reinterpret_cast<double*>(smem_raw + Lo.tile);
+#pragma unroll
+        for (int q = 0; q < kNumMom; ++q) red[(pc_q * NQ + pc_c) * kNumMom + q] = macc[q];
+        __syncthreads();
+        for (int c = tid; c < NQ * kNumMom; c += NTHREADS) {
+            int cq = c / kNumMom, q = c % kNumMom;
+            double v = 0.0;
+#pragma unroll
+            for (int h = 0; h < NQUART; ++h) v += red[(h * NQ + cq) * kNumMom + q];
+            int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
+            if (ii < Nq1 && jj < Nq2)
+                a.mom_out[(((long long)split * kNumMom + q) * a.Ns + s) * plane
+                          + (long long)jj * Nq1 + ii] = v;
         }
     }
 }

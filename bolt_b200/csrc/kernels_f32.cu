@@ -4,3 +4,16 @@
 #define BOLT_EXACT false
 #define BOLT_SUFFIX f32
 #include "kernels_impl.cuh"
+
+namespace bolt {
+
+cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t smem,
+                             cudaStream_t st) {
+    auto k = bgk ? qpair_kernel<true> : qpair_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, NTHREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace bolt

@@ -51,6 +51,10 @@ inline size_t pstage_smem(int Np, size_t elem) { return 4 * (size_t)Np * elem; }
 BOLT_DECLARE_LAUNCHERS(f64, double)
 BOLT_DECLARE_LAUNCHERS(f32, float)
 
+// paired FP32 WENO5 q-stage (8x8 tiling, fields off, fused combine, TMA)
+cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t smem,
+                             cudaStream_t st);
+
 // FDTD sequence (FP64): prepare -> halo -> E -> halo -> B -> to_cell
 cudaError_t launch_fdtd(const FieldArgs& a, cudaStream_t st, long long* launches);
 cudaError_t launch_field_halo(const FieldArgs& a, cudaStream_t st);

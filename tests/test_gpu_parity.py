@@ -93,3 +93,29 @@ def test_fp64_matches_reference(name):
                                   'dirichlet_1d1v_weno5', 'two_species_2d2v_fields'])
 def test_fp32_close_to_reference(name):
     _check_case(name, 'fp32')
+
+
+PARTIAL = C.make(N_q1=12, N_q2=10, N_p1=8, N_p2=6, N_p3=4,
+                 p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+                 p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+                 tau=0.05, dt=1e-3, steps=3, integrator='RK4',
+                 riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                 init=dict(amp=0.1, k1=1, k2=1, u=[0.2, -0.1, 0.05]))
+
+
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-12), ('fp32', 2e-6)])
+def test_partial_tiles_and_chunks_vs_oracle(precision, tol):
+    """q-extents that are not multiples of the 8x8 tile and Np = 192 (six
+    full chunks of 32 for the FP32 paired kernel's fast path, partial tiles
+    at the right/top edges): CUDA vs the oracle from the same initial f."""
+    from oracle.bolt_oracle import Oracle
+    spec = PARTIAL
+    g = spec['N_ghost']
+    nls = make_solver(spec, precision)
+    f0 = to_layout(nls.f, spec)          # the state actually on the GPU
+    o = Oracle(spec, f0)
+    for _ in range(spec['steps']):
+        nls.strang_timestep(spec['dt'])
+        o.step(spec['dt'])
+    e = rel(interior(to_layout(nls.f, spec), g), interior(o.f, g))
+    assert e < tol, e
