@@ -79,7 +79,11 @@ SIGNATURES = {
     'bolt_strerror': (ctypes.c_char_p, [ctypes.c_int]),
     'bolt_launch_count': (ctypes.c_longlong, [_VP]),
     'bolt_scratch_bytes': (ctypes.c_size_t, [_VP]),
+    'bolt_dfdt_noalloc': (ctypes.c_int, [ctypes.POINTER(BoltGrid), ctypes.POINTER(BoltParams),
+                                         _VP, _VP, _VP]),
 }
+
+NOALLOC_MAX_QCELLS = 65536
 
 _lib = None
 

@@ -24,6 +24,7 @@ UNITS = [
     ('kernels_f64.cu', ['-fmad=false']),
     ('kernels_f32.cu', ['-prec-div=false', '-prec-sqrt=false', '-ftz=true']),
     ('bolt_capi.cu', []),
+    ('bolt_noalloc.cu', []),
 ]
 
 

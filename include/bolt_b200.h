@@ -158,6 +158,22 @@ int  bolt_set_at_n(BoltCtx* ctx, int at_n);
 int  bolt_divergence_flag(BoltCtx* ctx);
 int  bolt_clear_divergence_flag(BoltCtx* ctx);
 
+/* Allocation-free df/dt, for callers that cannot allocate device memory when
+ * they need an evaluation (fixed-budget memory pools, code that must not
+ * trigger the implicit synchronisation of cudaMalloc/cudaFree, embedders
+ * that own all device memory).  No reference counterpart: Bolt's df_dt_fvm
+ * always allocates its temporaries.  Same result as bolt_dfdt for
+ * fields-disabled problems: writes df/dt of f (ghost cells current) into the
+ * interior cells of dfdt.  Its only scratch (FP64 moment sums and an error
+ * word) is a fixed device array of this library holding
+ * BOLT_NOALLOC_MAX_QCELLS (N_s*N_q1*N_q2) q-cells; larger grids and fields
+ * return BOLT_ERR_UNSUPPORTED.  The first call on a device looks up that
+ * array's address (make it before any stream capture); calls that overlap on
+ * the GPU share the array and race. */
+#define BOLT_NOALLOC_MAX_QCELLS 65536
+int  bolt_dfdt_noalloc(const BoltGrid* grid, const BoltParams* params, const void* f_dev,
+                       void* dfdt_dev, void* stream);
+
 /* Synchronise the stream and return the first sticky error of the context. */
 int  bolt_status_sync(BoltCtx* ctx, void* stream);
 const char* bolt_strerror(int code);
