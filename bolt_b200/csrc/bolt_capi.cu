@@ -414,7 +414,9 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     // no TMA) runs the scalar kernel
     const bool pair = ctx->elem == 4 && ctx->recon_q == BOLT_RECON_WENO5 &&
                       ctx->tiling == TILING_2D && !write_k && !want_j && a.use_tma &&
-                      a.base1 != nullptr && ctx->pair_enabled;
+                      a.base1 != nullptr && ctx->pair_enabled && ctx->tau_arr == nullptr &&
+                      g.N_q1 % 8 == 0 && g.N_q2 % 8 == 0 && ctx->Np % PW == 0 &&
+                      ctx->fcount < (1ull << 31);
     cudaError_t e = ctx->elem == 8
         ? launch_qstage_f64(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st)
         : (pair ? launch_qpair_f32(a, ctx->bgk, grid, smem, st)

@@ -511,8 +511,13 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
 // arithmetic:
 //   phase A  warp w: rows 2(w%4), 2(w%4)+1, cells 4(w/4) .. +3 (5 faces)
 //   phase B  warp w: cols 2(w%4), 2(w%4)+1, rows  4(w/4) .. +3 (5 faces)
+// Launched only when every tile and p-chunk is complete (N_q1, N_q2
+// multiples of 8, N_p multiple of 32) and f has fewer than 2^31 elements, so
+// it carries no masks and addresses with 32-bit offsets.  Periodic ghost
+// images are written from shared memory by the border CTAs after phase B, and
+// the divergence check runs on the staged outputs in phase C.
 // ---------------------------------------------------------------------------
-template <bool BGK>
+template <bool BGK, bool HAS2>
 __global__ void __launch_bounds__(NTHREADS, 2)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
     constexpr int TQ1 = 8, TQ2 = 8;
@@ -542,13 +547,11 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
     const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
     const int i0 = tile1 * TQ1, j0 = tile2 * TQ2;
-    const int nchunks = (Np + PW - 1) / PW;
+    const int nchunks = Np / PW;
     const int k_begin = split * a.chunks_per_split;
     const int k_end = min(nchunks, k_begin + a.chunks_per_split);
-    const long long rowstride = (long long)a.Ns * Np;
-    const long long colstride = rowstride * a.Nq1g;
-    const bool tile_full = (i0 + TQ1 <= Nq1) && (j0 + TQ2 <= Nq2);
-    const bool fast = tile_full && a.full_chunks;
+    const unsigned rowstride = (unsigned)(a.Ns * Np);
+    const unsigned colstride = rowstride * (unsigned)a.Nq1g;
     const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ1 > Nq1 - Ng)) ||
                         (a.periodic2 && (j0 < Ng || j0 + TQ2 > Nq2 - Ng));
 
@@ -568,27 +571,27 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     issue(k_begin, 0);
     issue(k_begin + 1, 1);
 
-    float* out1 = static_cast<float*>(a.out1);
-    float* out2 = static_cast<float*>(a.out2);
-    const float* base1 = static_cast<const float*>(a.base1);
-    const float* base2 = static_cast<const float*>(a.base2);
-    const float* tau_arr = static_cast<const float*>(a.tau_arr);
+    float* __restrict__ out1 = static_cast<float*>(a.out1);
+    float* __restrict__ out2 = static_cast<float*>(a.out2);
+    const float* __restrict__ base1 = static_cast<const float*>(a.base1);
+    const float* __restrict__ base2 = static_cast<const float*>(a.base2);
     const float c1 = float(a.c1), c2 = float(a.c2);
-    const float inv_tau = float(1.0 / a.tau);
     const float2 inv_dq1 = f2(float(1.0 / a.dq1)), inv_dq2 = f2(float(1.0 / a.dq2));
-    const double mneg = -a.sg.mass[s];
+    const float inv_tau = float(1.0 / a.tau);
     const bool want_mom = a.mom_out != nullptr;
+    const bool check = a.flag != nullptr;
+    bool nonfinite = false;
     const int pc_c = tid % NQ, pc_q = tid / NQ;
     double macc[kNumMom] = {0, 0, 0, 0, 0};
 
     int p = k_begin * PW + lane;
     int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
-    // phase A / B ownership
-    const int rp = warp & 3, seg = warp >> 2;          // row/column pair, segment
+    const int rp = warp & 3, seg = warp >> 2;
     const int a_row = 2 * rp, a_c0 = 4 * seg;          // phase A: rows a_row, a_row+1
     const int b_col = 2 * rp, b_r0 = 4 * seg;          // phase B: cols b_col, b_col+1
-    const long long tbase = (long long)(j0 + b_r0 + Ng) * colstride
-                          + (long long)(i0 + b_col + Ng) * rowstride + (long long)s * Np;
+    // element offset of phase-B cell (b_col, b_r0) for p = lane of chunk 0
+    unsigned toff = (unsigned)(j0 + b_r0 + Ng) * colstride + (unsigned)(i0 + b_col + Ng) * rowstride
+                  + (unsigned)(s * Np) + (unsigned)p;
 
     int buf = 0;
     for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
@@ -602,9 +605,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         }
         __syncthreads();
         const float* X = tile + buf * TILE;
-        const bool pvalid = p < Np;
-        const int jp1 = pvalid ? ip1 : 0, jp2 = pvalid ? ip2 : 0, jp3 = pvalid ? ip3 : 0;
-        const double V1 = vgrid[jp1], V2 = vgrid[Np1 + jp2], V3 = vgrid[Np1 + Np2 + jp3];
+        const double V1 = vgrid[ip1], V2 = vgrid[Np1 + ip2], V3 = vgrid[Np1 + Np2 + ip3];
 
         // prefetch combine operands of the 8 phase-B cells (col x, row r)
         float pre1[2][4], pre2[2][4];
@@ -612,10 +613,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         for (int x = 0; x < 2; ++x)
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                const bool cvalid = fast || (pvalid && i0 + b_col + x < Nq1 && j0 + b_r0 + r < Nq2);
-                const long long g = tbase + x * rowstride + r * colstride + p;
-                pre1[x][r] = cvalid ? base1[g] : 0.0f;
-                pre2[x][r] = (base2 && cvalid) ? base2[g] : 0.0f;
+                const unsigned o = toff + x * rowstride + r * colstride;
+                pre1[x][r] = base1[o];
+                if (HAS2) pre2[x][r] = base2[o];
             }
 
         // ---- phase A: q1 faces of rows a_row, a_row+1 -------------------------
@@ -639,7 +639,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
                 y4 = make_float2(ra[(c + 5) * PW], rb[(c + 5) * PW]);
                 const float2 Fn = mul2(vv, W.next(y0, y1, y2, y3, y4, S));
-                const float2 d = mul2(add2(Fprev, make_float2(-Fn.x, -Fn.y)), inv_dq1);
+                const float2 d = mul2(make_float2(Fprev.x - Fn.x, Fprev.y - Fn.y), inv_dq1);
                 stage[(a_row * TQ1 + a_c0 + c) * PWP + lane] = d.x;
                 stage[((a_row + 1) * TQ1 + a_c0 + c) * PWP + lane] = d.y;
                 Fprev = Fn;
@@ -649,10 +649,10 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
 
         // ---- phase B: q2 faces of cols b_col, b_col+1, BGK, combine ------------
         if (warp == 0) {
-            vtab[0 * PW + lane] = pvalid ? V1 : 0.0;
-            vtab[1 * PW + lane] = pvalid ? V2 : 0.0;
-            vtab[2 * PW + lane] = pvalid ? V3 : 0.0;
-            vtab[3 * PW + lane] = pvalid ? (V1 * V1 + V2 * V2) + V3 * V3 : 0.0;
+            vtab[0 * PW + lane] = V1;
+            vtab[1 * PW + lane] = V2;
+            vtab[2 * PW + lane] = V3;
+            vtab[3 * PW + lane] = (V1 * V1 + V2 * V2) + V3 * V3;
         }
         {
             const float v2 = float(V2);
@@ -670,78 +670,76 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             Weno5PairWalker W;
             const float2 vv = f2(v2);
             float2 Fprev = mul2(vv, W.first(y0, y1, y2, y3, y4, S));
-            const int toff1 = jp1, toff2 = Np1 + jp2, toff3 = Np1 + Np2 + jp3;
+            const double* tb0 = tabs + (b_r0 * TQ1 + b_col) * ntab;
+            const int toff1 = ip1, toff2 = Np1 + ip2, toff3 = Np1 + Np2 + ip3;
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                const int rr = b_r0 + r;
-                const int cq0 = rr * TQ1 + b_col;
+                const int cq0 = (b_r0 + r) * TQ1 + b_col;
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
                 y4 = make_float2(ca[(r + 5) * HX * PW], cb[(r + 5) * HX * PW]);
                 const float2 Fn = mul2(vv, W.next(y0, y1, y2, y3, y4, S));
                 const float2 kq0 = make_float2(stage[cq0 * PWP + lane], stage[(cq0 + 1) * PWP + lane]);
                 float2 kk = fma2(make_float2(Fprev.x - Fn.x, Fprev.y - Fn.y), inv_dq2, kq0);
                 Fprev = Fn;
-                const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
-                const long long g0 = tbase + r * colstride + p;
                 if (BGK) {
+                    const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
                     double fmb[2];
 #pragma unroll
                     for (int x = 0; x < 2; ++x) {
-                        const int cq = cq0 + x;
                         if (a.bgk_direct) {
-                            const double* qq = qc + cq * 5;
+                            const double* qq = qc + (cq0 + x) * 5;
+                            const double mneg = -a.sg.mass[s];
                             double d1v = V1 - qq[1];
                             double f0 = qq[0] * exp((mneg * (d1v * d1v)) / qq[4]);
                             if (a.p_dim >= 2) { double d2v = V2 - qq[2]; f0 = f0 * exp((mneg * (d2v * d2v)) / qq[4]); }
                             if (a.p_dim == 3) { double d3v = V3 - qq[3]; f0 = f0 * exp((mneg * (d3v * d3v)) / qq[4]); }
                             fmb[x] = f0;
                         } else {
-                            const double* tb = tabs + cq * ntab;
+                            const double* tb = tb0 + (r * TQ1 + x) * ntab;
                             fmb[x] = (tb[toff1] * tb[toff2]) * tb[toff3];
                         }
                     }
-                    float itx = inv_tau, ity = inv_tau;
-                    if (tau_arr) {
-                        const bool v0 = fast || (pvalid && i0 + b_col < Nq1 && j0 + rr < Nq2);
-                        const bool v1c = fast || (pvalid && i0 + b_col + 1 < Nq1 && j0 + rr < Nq2);
-                        itx = 1.0f / tau_arr[v0 ? g0 : 0];
-                        ity = 1.0f / tau_arr[v1c ? g0 + rowstride : 0];
-                    }
                     kk = fma2(make_float2(float(fmb[0]) - fcell.x, float(fmb[1]) - fcell.y),
-                              make_float2(itx, ity), kk);
+                              f2(inv_tau), kk);
                 }
-                const float kkx[2] = {kk.x, kk.y};
-#pragma unroll
-                for (int x = 0; x < 2; ++x) {
-                    const int ii = i0 + b_col + x, jj = j0 + rr;
-                    const bool cvalid = fast || (pvalid && ii < Nq1 && jj < Nq2);
-                    const long long g = g0 + x * rowstride;
-                    const float o1 = fmaf(kkx[x], c1, pre1[x][r]);
-                    if (cvalid) {
-                        out1[g] = o1;
-                        if (out2) out2[g] = fmaf(kkx[x], c2, pre2[x][r]);
-                        if (border && ((a.periodic1 && (ii < Ng || ii >= Nq1 - Ng)) ||
-                                       (a.periodic2 && (jj < Ng || jj >= Nq2 - Ng))))
-                            write_ghost_images(out1, o1, ii, jj, s, p, Ng, Nq1, Nq2,
-                                               a.Nq1g, a.Nq2g, a.periodic1, a.periodic2,
-                                               rowstride, colstride, Np);
-                        if (a.flag && !isfinite(o1)) atomicOr(a.flag, 1);
-                    }
-                    stage[(cq0 + x) * PWP + lane] = cvalid ? o1 : 0.0f;
+                const unsigned o0 = toff + r * colstride;
+                const float o1a = fmaf(kk.x, c1, pre1[0][r]);
+                const float o1b = fmaf(kk.y, c1, pre1[1][r]);
+                out1[o0] = o1a;
+                out1[o0 + rowstride] = o1b;
+                if (HAS2) {
+                    out2[o0] = fmaf(kk.x, c2, pre2[0][r]);
+                    out2[o0 + rowstride] = fmaf(kk.y, c2, pre2[1][r]);
                 }
+                stage[cq0 * PWP + lane] = o1a;
+                stage[(cq0 + 1) * PWP + lane] = o1b;
             }
         }
         __syncthreads();
         fence_proxy_async();
         issue(k + 2, buf);
 
-        // ---- phase C: FP64 moments of out1 ------------------------------------
-        if (want_mom) {
+        // ---- periodic ghost images of border cells, from the staged outputs ---
+        if (border) {
+            for (int c = warp; c < NQ; c += NWARP) {
+                const int ii = i0 + c % TQ1, jj = j0 + c / TQ1;
+                if ((a.periodic1 && (ii < Ng || ii >= Nq1 - Ng)) ||
+                    (a.periodic2 && (jj < Ng || jj >= Nq2 - Ng)))
+                    write_ghost_images(out1, stage[c * PWP + lane], ii, jj, s, p, Ng, Nq1, Nq2,
+                                       a.Nq1g, a.Nq2g, a.periodic1, a.periodic2,
+                                       (long long)rowstride, (long long)colstride, Np);
+            }
+        }
+
+        // ---- phase C: FP64 moments of out1, divergence check ------------------
+        if (want_mom || check) {
             const float* sp = stage + pc_c * PWP + pc_q * PQ;
             const double* vt = vtab + pc_q * PQ;
 #pragma unroll
             for (int t = 0; t < PQ; ++t) {
-                const double ov = double(sp[t]);
+                const float o = sp[t];
+                nonfinite |= !isfinite(o);
+                const double ov = double(o);
                 macc[0] += ov;
                 macc[1] += ov * vt[t];
                 macc[2] += ov * vt[PW + t];
@@ -750,12 +748,14 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             }
         }
         p += PW;
+        toff += PW;
         ip1 += PW;
         while (ip1 >= Np1) {
             ip1 -= Np1;
             if (++ip2 == Np2) { ip2 = 0; ++ip3; }
         }
     }
+    if (check && nonfinite) atomicOr(a.flag, 1);
     __syncthreads();
 
     const long long plane = (long long)Nq2 * Nq1;
@@ -770,9 +770,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
 #pragma unroll
             for (int h = 0; h < NQUART; ++h) v += red[(h * NQ + cq) * kNumMom + q];
             int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
-            if (ii < Nq1 && jj < Nq2)
-                a.mom_out[(((long long)split * kNumMom + q) * a.Ns + s) * plane
-                          + (long long)jj * Nq1 + ii] = v;
+            a.mom_out[(((long long)split * kNumMom + q) * a.Ns + s) * plane
+                      + (long long)jj * Nq1 + ii] = v;
         }
     }
 }

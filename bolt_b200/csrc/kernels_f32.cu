@@ -9,7 +9,9 @@ namespace bolt {
 
 cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t smem,
                              cudaStream_t st) {
-    auto k = bgk ? qpair_kernel<true> : qpair_kernel<false>;
+    const bool has2 = a.out2 != nullptr;
+    auto k = bgk ? (has2 ? qpair_kernel<true, true> : qpair_kernel<true, false>)
+                 : (has2 ? qpair_kernel<false, true> : qpair_kernel<false, false>);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, NTHREADS, smem, st>>>(a);
