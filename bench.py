@@ -312,7 +312,8 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg_bytes_per_update * cells / (ms * 1e-3) / 1e9
     roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                 'frac': achieved / peak, 'traffic': args.traffic,
-                'peak_kind': peak_kind, 'kernel': 'qstage_kernel (WENO5, 8x8 q-tile)',
+                'peak_kind': peak_kind, 'kernel': 'qpair_kernel (paired FP32 WENO5 stage, 8x8 q-tile)' if args.precision == 'fp32'
+                else 'qstage_kernel (WENO5, 8x8 q-tile)',
                 'alg_bytes_per_launch': alg_bytes_per_update * cells / qstage_per_step,
                 'avg_launch_ms': ms / qstage_per_step}
     cpu = None

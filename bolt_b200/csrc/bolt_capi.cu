@@ -38,8 +38,14 @@ EncodeTiledFn get_encode_fn() {
     return fn;
 }
 
+// tensor-map kinds: the stage input's halo box, and the paired kernel's
+// 8x8x32 interior boxes (plain, or 128-byte swizzled for the out1 staging tile)
+enum TmapKind { TMAP_HALO = 0, TMAP_TILE = 1, TMAP_TILE_SWZ = 2 };
+constexpr int kTmapSlots = 16;
+
 struct TmapEntry {
     const void* ptr;
+    int kind;
     CUtensorMap map;
 };
 
@@ -77,9 +83,10 @@ struct BoltCtx {
     int sticky;
     long long launches;
     size_t scratch_bytes;
-    TmapEntry tmaps[4];
-    int ntmaps;
+    TmapEntry tmaps[kTmapSlots];
+    int ntmaps, next_tmap;
     int pair_enabled;       // paired FP32 kernel allowed (BOLT_NO_PAIR unset)
+    int pair_shape_ok;      // grid/method meet the paired kernel's shape conditions
 };
 
 #define CK(x)                                             \
@@ -104,9 +111,9 @@ static int dev_alloc(BoltCtx* ctx, void** p, size_t bytes) {
     return BOLT_OK;
 }
 
-static const CUtensorMap* get_tmap(BoltCtx* ctx, const void* ptr) {
+static const CUtensorMap* get_tmap(BoltCtx* ctx, const void* ptr, int kind) {
     for (int i = 0; i < ctx->ntmaps; ++i)
-        if (ctx->tmaps[i].ptr == ptr) return &ctx->tmaps[i].map;
+        if (ctx->tmaps[i].ptr == ptr && ctx->tmaps[i].kind == kind) return &ctx->tmaps[i].map;
     EncodeTiledFn enc = get_encode_fn();
     if (!enc) return nullptr;
     TileShape t = tile_shape(ctx->tiling);
@@ -116,16 +123,28 @@ static const CUtensorMap* get_tmap(BoltCtx* ctx, const void* ptr) {
                              (cuuint64_t)ctx->g.N_s * ctx->Np * ctx->elem * ctx->Nq1g};
     cuuint32_t box[3] = {(cuuint32_t)PW, (cuuint32_t)(t.tq1 + 2 * HALO),
                          (cuuint32_t)(t.q2 ? t.tq2 + 2 * HALO : 1)};
+    if (kind != TMAP_HALO) {
+        box[1] = 8;
+        box[2] = 8;
+    }
     cuuint32_t estr[3] = {1, 1, 1};
     CUtensorMap m;
     CUresult r = enc(&m, ctx->elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                      3, const_cast<void*>(ptr), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     kind == TMAP_TILE_SWZ ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return nullptr;
-    int slot = ctx->ntmaps < 4 ? ctx->ntmaps++ : 0;
+    int slot;
+    if (ctx->ntmaps < kTmapSlots) {
+        slot = ctx->ntmaps++;
+    } else {
+        slot = ctx->next_tmap;
+        ctx->next_tmap = (ctx->next_tmap + 1) % kTmapSlots;
+    }
     ctx->tmaps[slot].ptr = ptr;
+    ctx->tmaps[slot].kind = kind;
     ctx->tmaps[slot].map = m;
     return &ctx->tmaps[slot].map;
 }
@@ -202,14 +221,42 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
     ctx->ntab = g.N_p1 + g.N_p2 + g.N_p3;
     ctx->bgk_direct = (p.p_dim == 1 ||
                        (size_t)t.tq1 * t.tq2 * ctx->ntab * sizeof(double) > 64 * 1024) ? 1 : 0;
-    // p-splits: enough CTAs for several waves on 148 SMs
-    const int nchunks = (ctx->Np + PW - 1) / PW;
-    const long long base_ctas = (long long)ctx->ntiles1 * ctx->ntiles2 * g.N_s;
-    long long want = (148LL * 8 + base_ctas - 1) / base_ctas;
-    if (want < 1) want = 1;
-    if (want > nchunks) want = nchunks;
-    ctx->chunks_per_split = (int)((nchunks + want - 1) / want);
-    ctx->nsplit = (nchunks + ctx->chunks_per_split - 1) / ctx->chunks_per_split;
+    // the paired FP32 kernel's shape conditions (the per-call ones are checked at launch)
+    ctx->pair_shape_ok = ctx->elem == 4 && p.recon_q == BOLT_RECON_WENO5 &&
+                         ctx->tiling == TILING_2D && !(ctx->bgk && ctx->bgk_direct) &&
+                         g.N_q1 % 8 == 0 && g.N_q2 % 8 == 0 && ctx->Np % PW == 0 &&
+                         g.N_p1 % 8 == 0 && 2 * g.N_ghost <= g.N_q1 &&
+                         2 * g.N_ghost <= g.N_q2 && ctx->fcount < (1ull << 31);
+    // p-splits: the grid is (q-tiles, species x splits); choose the split that
+    // minimises (waves, rounded up) x (chunks per CTA + ~2 chunks of prologue),
+    // a wave being SMs x resident CTAs per SM of the q-stage kernel
+    {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const size_t smem_est = ctx->pair_shape_ok
+            ? qpair_smem(ctx->ntab, ctx->bgk)
+            : qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct, ctx->ntab);
+        long long per_sm = 233472LL / (long long)(smem_est + 1024);
+        per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
+        const long long wave = (long long)sms * per_sm;
+        const int nchunks = (ctx->Np + PW - 1) / PW;
+        const long long base_ctas = (long long)ctx->ntiles1 * ctx->ntiles2 * g.N_s;
+        double best = 1e300;
+        int best_cps = nchunks;
+        for (int n = 1; n <= nchunks && n <= 64; ++n) {
+            const int cps = (nchunks + n - 1) / n;
+            const int ne = (nchunks + cps - 1) / cps;
+            const long long waves = (base_ctas * ne + wave - 1) / wave;
+            const double cost = (double)waves * (cps + 2.0);
+            if (cost < best - 1e-9) {
+                best = cost;
+                best_cps = cps;
+            }
+        }
+        ctx->chunks_per_split = best_cps;
+        ctx->nsplit = (nchunks + best_cps - 1) / best_cps;
+    }
     const size_t rowbytes = (size_t)g.N_s * ctx->Np * ctx->elem;
     ctx->use_tma_ok = (g.N_ghost >= HALO) && (rowbytes % 16 == 0) &&
                       (((size_t)ctx->Np * ctx->elem) % 16 == 0) && get_encode_fn() != nullptr;
@@ -369,7 +416,7 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     memset(&a, 0, sizeof(a));
     a.use_tma = 0;
     if (ctx->use_tma_ok && (((uintptr_t)io.fs) % 16 == 0)) {
-        const CUtensorMap* m = get_tmap(ctx, io.fs);
+        const CUtensorMap* m = get_tmap(ctx, io.fs, TMAP_HALO);
         if (m) {
             a.tmap = *m;
             a.use_tma = 1;
@@ -408,15 +455,32 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     a.full_chunks = (ctx->Np % PW) == 0;
     a.sg = ctx->sg;
     dim3 grid(ctx->ntiles1 * ctx->ntiles2, g.N_s * ctx->nsplit);
-    const size_t smem = qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct, ctx->ntab);
-    // the paired FP32 kernel covers the fused WENO5 2-D stage; everything
-    // else (FP64, other reconstructions, 1-D tilings, write-k mode, currents,
-    // no TMA) runs the scalar kernel
-    const bool pair = ctx->elem == 4 && ctx->recon_q == BOLT_RECON_WENO5 &&
-                      ctx->tiling == TILING_2D && !write_k && !want_j && a.use_tma &&
-                      a.base1 != nullptr && ctx->pair_enabled && ctx->tau_arr == nullptr &&
-                      g.N_q1 % 8 == 0 && g.N_q2 % 8 == 0 && ctx->Np % PW == 0 &&
-                      ctx->fcount < (1ull << 31);
+    // the paired FP32 kernel covers the fused WENO5 2-D stage with every
+    // buffer reachable by TMA; everything else (FP64, other reconstructions,
+    // 1-D tilings, write-k mode, currents, tau arrays) runs the scalar kernel
+    bool pair = ctx->pair_shape_ok && ctx->pair_enabled && !write_k && !want_j && a.use_tma &&
+                a.base1 != nullptr && ctx->tau_arr == nullptr;
+    if (pair) {
+        const void* ptrs[4] = {a.base1, a.out1, a.base2, a.out2};
+        for (int i = 0; i < 4; ++i)
+            if (ptrs[i] && ((uintptr_t)ptrs[i]) % 16 != 0) pair = false;
+        if ((a.base2 == nullptr) != (a.out2 == nullptr)) pair = false;
+    }
+    if (pair) {
+        // copy each map out at once: a later lookup may recycle its cache slot
+        const CUtensorMap* m;
+        if ((m = get_tmap(ctx, a.base1, TMAP_TILE))) a.tm_b1 = *m; else pair = false;
+        if (pair && (m = get_tmap(ctx, a.out1, TMAP_TILE_SWZ))) a.tm_o1 = *m; else pair = false;
+        a.tm_b2 = a.tm_b1;
+        a.tm_o2 = a.tm_o1;
+        if (pair && a.base2) {
+            if ((m = get_tmap(ctx, a.base2, TMAP_TILE))) a.tm_b2 = *m; else pair = false;
+            if (pair && (m = get_tmap(ctx, a.out2, TMAP_TILE))) a.tm_o2 = *m; else pair = false;
+        }
+    }
+    const size_t smem = pair ? qpair_smem(ctx->ntab, ctx->bgk)
+                             : qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct,
+                                           ctx->ntab);
     cudaError_t e = ctx->elem == 8
         ? launch_qstage_f64(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st)
         : (pair ? launch_qpair_f32(a, ctx->bgk, grid, smem, st)

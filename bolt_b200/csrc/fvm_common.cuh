@@ -283,29 +283,32 @@ struct FaceWalker {
 // sm_100 f32x2 arithmetic.  Both components share the lane's upwind side, so
 // they share the coefficient set.  Smoothness indicators use a constant
 // 1e-17 floor (the reference's 1e-17*(1+|a|+|b|+|c|) differs from it only
-// where f varies by less than FP32 resolves).
+// where f varies by less than FP32 resolves).  The linear weights are folded
+// into the substencil interpolants: value = sum q_k U_k / sum c_k q_k with
+// q_k = 1/beta_k^2 and U_k = c_k u_k, which is the reference's
+// sum w_k u_k / sum w_k (w_k = c_k q_k) reassociated.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
 __device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(fast_rcp(a.x), fast_rcp(a.y)); }
 
 struct Weno5Pair {
     float2 cw1, cw2, cw3;
-    float2 a10, a11, a12, a20, a21, a22, a30, a31, a32;
+    float2 a10, a11, a12, a20, a21, a22, a30, a31, a32;   // c_k * interpolant coefficients
     __device__ __forceinline__ void set(bool right) {
-        cw2 = f2(0.625f);
-        cw1 = f2(right ? 0.0625f : 0.3125f);
-        cw3 = f2(right ? 0.3125f : 0.0625f);
+        const float c1 = right ? 0.0625f : 0.3125f, c2 = 0.625f, c3 = right ? 0.3125f : 0.0625f;
+        cw1 = f2(c1); cw2 = f2(c2); cw3 = f2(c3);
         if (right) {
-            a10 = f2(0.375f);  a11 = f2(-1.25f); a12 = f2(1.875f);
-            a20 = f2(-0.125f); a21 = f2(0.75f);  a22 = f2(0.375f);
-            a30 = f2(0.375f);  a31 = f2(0.75f);  a32 = f2(-0.125f);
+            a10 = f2(c1 * 0.375f);  a11 = f2(c1 * -1.25f); a12 = f2(c1 * 1.875f);
+            a20 = f2(c2 * -0.125f); a21 = f2(c2 * 0.75f);  a22 = f2(c2 * 0.375f);
+            a30 = f2(c3 * 0.375f);  a31 = f2(c3 * 0.75f);  a32 = f2(c3 * -0.125f);
         } else {
-            a10 = f2(-0.125f); a11 = f2(0.75f);  a12 = f2(0.375f);
-            a20 = f2(0.375f);  a21 = f2(0.75f);  a22 = f2(-0.125f);
-            a30 = f2(1.875f);  a31 = f2(-1.25f); a32 = f2(0.375f);
+            a10 = f2(c1 * -0.125f); a11 = f2(c1 * 0.75f);  a12 = f2(c1 * 0.375f);
+            a20 = f2(c2 * 0.375f);  a21 = f2(c2 * 0.75f);  a22 = f2(c2 * -0.125f);
+            a30 = f2(c3 * 1.875f);  a31 = f2(c3 * -1.25f); a32 = f2(c3 * 0.375f);
         }
     }
 };
@@ -324,12 +327,12 @@ struct Weno5PairWalker {
     }
     __device__ __forceinline__ float2 eval(float2 q1, float2 y0, float2 y1, float2 y2, float2 y3,
                                            float2 y4, const Weno5Pair& S) {
-        const float2 w1 = mul2(S.cw1, q1), w2 = mul2(S.cw2, q2), w3 = mul2(S.cw3, q3);
         const float2 u1 = fma2(S.a12, y2, fma2(S.a11, y1, mul2(S.a10, y0)));
         const float2 u2 = fma2(S.a22, y3, fma2(S.a21, y2, mul2(S.a20, y1)));
         const float2 u3 = fma2(S.a32, y4, fma2(S.a31, y3, mul2(S.a30, y2)));
-        const float2 num = fma2(w3, u3, fma2(w2, u2, mul2(w1, u1)));
-        return mul2(num, rcp2(add2(add2(w1, w2), w3)));
+        const float2 num = fma2(q3, u3, fma2(q2, u2, mul2(q1, u1)));
+        const float2 den = fma2(S.cw3, q3, fma2(S.cw2, q2, mul2(S.cw1, q1)));
+        return mul2(num, rcp2(den));
     }
     __device__ __forceinline__ float2 first(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
                                             const Weno5Pair& S) {
@@ -404,6 +407,29 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
         ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)),
           "r"(x), "r"(y), "r"(z)
         : "memory");
+}
+
+// shared -> global box store; completion tracked by bulk groups of the issuing thread
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x,
+                                             int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+        ::"l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// the committed stores no longer read shared memory
+__device__ __forceinline__ void bulk_wait_read_all() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// the committed stores are complete
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {

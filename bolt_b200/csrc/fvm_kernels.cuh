@@ -68,6 +68,58 @@ __device__ __forceinline__ void write_ghost_images(T* out, T v, int ii, int jj, 
 }
 
 // ---------------------------------------------------------------------------
+// Maxwellian parameters of q-cell (ii, jj) from the stage input's partial
+// moments (collision_operator.py:102-118, f0 :49-65), FP64:
+// qq = {n*A, u1, u2, u3, 2 kB T} with A the normalisation of the p_dim-D
+// Maxwellian.  Cells outside the grid get the parameters of zero moments.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void bgk_cell_params(const QStageArgs& a, int s, int ii, int jj,
+                                                double* qq) {
+    const int Nq1 = a.Nq1, Nq2 = a.Nq2;
+    const double m = a.sg.mass[s];
+    const double kB = a.kB;
+    const double measure = (a.sg.dp3[s] * a.sg.dp2[s]) * a.sg.dp1[s];
+    const long long plane = (long long)Nq2 * Nq1;
+    double mm[kNumMom] = {0, 0, 0, 0, 0};
+    if (ii < Nq1 && jj < Nq2) {
+        for (int sp = 0; sp < a.nsplit_in; ++sp) {
+#pragma unroll
+            for (int q = 0; q < kNumMom; ++q)
+                mm[q] += a.mom_in[(((long long)sp * kNumMom + q) * a.Ns + s) * plane
+                                  + (long long)jj * Nq1 + ii];
+        }
+    }
+    const double eps = 1e-30;
+    double n = mm[0] * measure;
+    double u1 = (mm[1] * measure) / (n + eps);
+    double u2 = (mm[2] * measure) / (n + eps);
+    double u3 = (mm[3] * measure) / (n + eps);
+    double E = mm[4] * measure;
+    double nm = n * m;
+    double Tt = (1.0 / a.p_dim) * ((((2.0 * (E * m) - nm * (u1 * u1)) - nm * (u2 * u2))
+                                    - nm * (u3 * u3))) / (n + eps) + eps;
+    double twokT = (2.0 * kB) * Tt;
+    double base = m / ((2.0 * 3.141592653589793 * kB) * Tt);
+    double A = a.p_dim == 3 ? pow(base, 1.5) : (a.p_dim == 2 ? base : sqrt(base));
+    qq[0] = n * A;
+    qq[1] = u1;
+    qq[2] = u2;
+    qq[3] = u3;
+    qq[4] = twokT;
+}
+
+// exp table entry q of a q-cell: p1 entries carry n*A, inactive axes are 1
+__device__ __forceinline__ double bgk_table_entry(const QStageArgs& a, const double* qq,
+                                                  const double* vgrid, int q, double m) {
+    const int Np1 = a.Np1, Np2 = a.Np2;
+    const double u = q < Np1 ? qq[1] : (q < Np1 + Np2 ? qq[2] : qq[3]);
+    const bool act = q < Np1 || (q < Np1 + Np2 ? a.p_dim >= 2 : a.p_dim == 3);
+    const double dv = vgrid[q] - u;
+    const double ev = act ? exp((-m * (dv * dv)) / qq[4]) : 1.0;
+    return q < Np1 ? qq[0] * ev : ev;
+}
+
+// ---------------------------------------------------------------------------
 // q-stage prologue shared by the scalar and paired kernels: zero the current
 // accumulators, the species' p-cell centres, the TMA barriers, and for BGK the
 // Maxwellian of the stage input per q-cell (collision_operator.py:102-118,
@@ -79,7 +131,6 @@ __device__ __forceinline__ void qstage_prologue(const QStageArgs& a, int s, int 
                                                 double* tabs, uint64_t* bars) {
     const int tid = threadIdx.x;
     const int Np1 = a.Np1, Np2 = a.Np2, Np3 = a.Np3;
-    const int Nq1 = a.Nq1, Nq2 = a.Nq2;
     const int ntab = Np1 + Np2 + Np3;
     for (int c = tid; c < NQ * 3; c += NTHREADS) j_acc[c] = 0.0;
     for (int q = tid; q < ntab; q += NTHREADS) {
@@ -98,50 +149,15 @@ __device__ __forceinline__ void qstage_prologue(const QStageArgs& a, int s, int 
     // ---- BGK prologue: Maxwellian of the stage input per q-cell (FP64) ----
     // collision_operator.py:102-118 and f0 :49-65
     if (BGK) {
-        const double m = a.sg.mass[s];
-        const double kB = a.kB;
-        const double measure = (a.sg.dp3[s] * a.sg.dp2[s]) * a.sg.dp1[s];
-        const long long plane = (long long)Nq2 * Nq1;
-        for (int c = tid; c < NQ; c += NTHREADS) {
-            int ii = i0 + c % TQ1, jj = j0 + c / TQ1;
-            double mm[kNumMom] = {0, 0, 0, 0, 0};
-            if (ii < Nq1 && jj < Nq2) {
-                for (int sp = 0; sp < a.nsplit_in; ++sp) {
-#pragma unroll
-                    for (int q = 0; q < kNumMom; ++q)
-                        mm[q] += a.mom_in[(((long long)sp * kNumMom + q) * a.Ns + s) * plane
-                                          + (long long)jj * Nq1 + ii];
-                }
-            }
-            const double eps = 1e-30;
-            double n = mm[0] * measure;
-            double u1 = (mm[1] * measure) / (n + eps);
-            double u2 = (mm[2] * measure) / (n + eps);
-            double u3 = (mm[3] * measure) / (n + eps);
-            double E = mm[4] * measure;
-            double nm = n * m;
-            double Tt = (1.0 / a.p_dim) * ((((2.0 * (E * m) - nm * (u1 * u1)) - nm * (u2 * u2))
-                                            - nm * (u3 * u3))) / (n + eps) + eps;
-            double twokT = (2.0 * kB) * Tt;
-            double base = m / ((2.0 * 3.141592653589793 * kB) * Tt);
-            double A = a.p_dim == 3 ? pow(base, 1.5) : (a.p_dim == 2 ? base : sqrt(base));
-            qc[c * 5 + 0] = n * A;
-            qc[c * 5 + 1] = u1;
-            qc[c * 5 + 2] = u2;
-            qc[c * 5 + 3] = u3;
-            qc[c * 5 + 4] = twokT;
-        }
+        for (int c = tid; c < NQ; c += NTHREADS)
+            bgk_cell_params(a, s, i0 + c % TQ1, j0 + c / TQ1, qc + c * 5);
         __syncthreads();
         if (!a.bgk_direct) {
             // exp tables over (q-cell, p1 | p2 | p3); the p1 entry carries n*A
+            const double m = a.sg.mass[s];
             for (int e = tid; e < NQ * ntab; e += NTHREADS) {
                 const int c = e / ntab, q = e % ntab;
-                const double* qq = qc + c * 5;
-                const double u = q < Np1 ? qq[1] : (q < Np1 + Np2 ? qq[2] : qq[3]);
-                const bool act = q < Np1 || (q < Np1 + Np2 ? a.p_dim >= 2 : a.p_dim == 3);
-                const double dv = vgrid[q] - u;
-                const double ev = act ? exp((-m * (dv * dv)) / qq[4]) : 1.0;
-                tabs[e] = q < Np1 ? qq[0] * ev : ev;
+                tabs[e] = bgk_table_entry(a, qc + c * 5, vgrid, q, m);
             }
         }
     }
@@ -500,278 +516,6 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
             if (ii < Nq1 && jj < Nq2)
                 a.j_out[(((long long)split * 3 + q) * a.Ns + s) * plane
                         + (long long)jj * Nq1 + ii] = j_acc[c];
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Paired FP32 WENO5 q-stage kernel (8x8 q-tile, fields off, fused combine).
-// Same stages as qstage_kernel, but every thread walks two adjacent q-rows
-// (phase A) or q-columns (phase B) of the same p at once with f32x2
-// arithmetic:
-//   phase A  warp w: rows 2(w%4), 2(w%4)+1, cells 4(w/4) .. +3 (5 faces)
-//   phase B  warp w: cols 2(w%4), 2(w%4)+1, rows  4(w/4) .. +3 (5 faces)
-// Launched only when every tile and p-chunk is complete (N_q1, N_q2
-// multiples of 8, N_p multiple of 32) and f has fewer than 2^31 elements, so
-// it carries no masks and addresses with 32-bit offsets.  Periodic ghost
-// images are written from shared memory by the border CTAs after phase B, and
-// the divergence check runs on the staged outputs in phase C.
-// ---------------------------------------------------------------------------
-template <bool BGK, bool HAS2>
-__global__ void __launch_bounds__(NTHREADS, 2)
-qpair_kernel(const __grid_constant__ QStageArgs a) {
-    constexpr int TQ1 = 8, TQ2 = 8;
-    constexpr int HX = TQ1 + 2 * HALO, HY = TQ2 + 2 * HALO;
-    constexpr int NQ = TQ1 * TQ2;
-    constexpr int NWARP = NTHREADS / 32;
-    constexpr int NQUART = NTHREADS / NQ;
-    constexpr int PQ = PW / NQUART;
-    constexpr int TILE = HY * HX * PW;
-    static_assert(NWARP == 8, "pair mapping assumes 8 warps");
-
-    const int Np1 = a.Np1, Np2 = a.Np2, Np = a.Np, Ng = a.Ng;
-    const int Nq1 = a.Nq1, Nq2 = a.Nq2;
-    const int ntab = Np1 + Np2 + a.Np3;
-    const QLayout Lo = qstage_layout(TQ1, TQ2, 1, sizeof(float), BGK, a.bgk_direct, ntab);
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float* tile = reinterpret_cast<float*>(smem_raw + Lo.tile);
-    float* stage = reinterpret_cast<float*>(smem_raw + Lo.stage);
-    double* vtab = reinterpret_cast<double*>(smem_raw + Lo.vtab);
-    double* j_acc = reinterpret_cast<double*>(smem_raw + Lo.jacc);
-    double* qc = reinterpret_cast<double*>(smem_raw + Lo.qc);
-    double* tabs = reinterpret_cast<double*>(smem_raw + Lo.tabs);
-    double* vgrid = reinterpret_cast<double*>(smem_raw + Lo.vgrid);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + Lo.bars);
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
-    const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
-    const int i0 = tile1 * TQ1, j0 = tile2 * TQ2;
-    const int nchunks = Np / PW;
-    const int k_begin = split * a.chunks_per_split;
-    const int k_end = min(nchunks, k_begin + a.chunks_per_split);
-    const unsigned rowstride = (unsigned)(a.Ns * Np);
-    const unsigned colstride = rowstride * (unsigned)a.Nq1g;
-    const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ1 > Nq1 - Ng)) ||
-                        (a.periodic2 && (j0 < Ng || j0 + TQ2 > Nq2 - Ng));
-
-    qstage_prologue<NQ, TQ1, BGK>(a, s, i0, j0, j_acc, vgrid, qc, tabs, bars);
-
-    bool failed = false;
-    const unsigned tile_bytes = TILE * sizeof(float);
-    auto issue = [&](int k, int buf) {
-        if (k >= k_end) return;
-        if (tid == 0 && !failed) {
-            mbar_arrive_expect_tx(&bars[buf], tile_bytes);
-            tma_load_3d(tile + buf * TILE, &a.tmap, &bars[buf], s * Np + k * PW,
-                        i0 + Ng - HALO, j0 + Ng - HALO);
-        }
-    };
-    unsigned phase0 = 0u, phase1 = 0u;
-    issue(k_begin, 0);
-    issue(k_begin + 1, 1);
-
-    float* __restrict__ out1 = static_cast<float*>(a.out1);
-    float* __restrict__ out2 = static_cast<float*>(a.out2);
-    const float* __restrict__ base1 = static_cast<const float*>(a.base1);
-    const float* __restrict__ base2 = static_cast<const float*>(a.base2);
-    const float c1 = float(a.c1), c2 = float(a.c2);
-    const float2 inv_dq1 = f2(float(1.0 / a.dq1)), inv_dq2 = f2(float(1.0 / a.dq2));
-    const float inv_tau = float(1.0 / a.tau);
-    const bool want_mom = a.mom_out != nullptr;
-    const bool check = a.flag != nullptr;
-    bool nonfinite = false;
-    const int pc_c = tid % NQ, pc_q = tid / NQ;
-    double macc[kNumMom] = {0, 0, 0, 0, 0};
-
-    int p = k_begin * PW + lane;
-    int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
-    const int rp = warp & 3, seg = warp >> 2;
-    const int a_row = 2 * rp, a_c0 = 4 * seg;          // phase A: rows a_row, a_row+1
-    const int b_col = 2 * rp, b_r0 = 4 * seg;          // phase B: cols b_col, b_col+1
-    // element offset of phase-B cell (b_col, b_r0) for p = lane of chunk 0
-    unsigned toff = (unsigned)(j0 + b_r0 + Ng) * colstride + (unsigned)(i0 + b_col + Ng) * rowstride
-                  + (unsigned)(s * Np) + (unsigned)p;
-
-    int buf = 0;
-    for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
-        if (!failed) {
-            const unsigned ph = buf ? phase1 : phase0;
-            if (!mbar_wait_bounded(&bars[buf], ph)) {
-                atomicExch(a.err, 4);
-                failed = true;
-            }
-            if (buf) phase1 ^= 1u; else phase0 ^= 1u;
-        }
-        __syncthreads();
-        const float* X = tile + buf * TILE;
-        const double V1 = vgrid[ip1], V2 = vgrid[Np1 + ip2], V3 = vgrid[Np1 + Np2 + ip3];
-
-        // prefetch combine operands of the 8 phase-B cells (col x, row r)
-        float pre1[2][4], pre2[2][4];
-#pragma unroll
-        for (int x = 0; x < 2; ++x)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const unsigned o = toff + x * rowstride + r * colstride;
-                pre1[x][r] = base1[o];
-                if (HAS2) pre2[x][r] = base2[o];
-            }
-
-        // ---- phase A: q1 faces of rows a_row, a_row+1 -------------------------
-        {
-            const float v1 = float(V1);
-            const bool right = v1 > 0.0f;
-            const int off = right ? 0 : 1;
-            Weno5Pair S; S.set(right);
-            const float* ra = X + ((a_row + HALO) * HX + a_c0 + off) * PW + lane;
-            const float* rb = ra + HX * PW;
-            float2 y0 = make_float2(ra[0 * PW], rb[0 * PW]);
-            float2 y1 = make_float2(ra[1 * PW], rb[1 * PW]);
-            float2 y2 = make_float2(ra[2 * PW], rb[2 * PW]);
-            float2 y3 = make_float2(ra[3 * PW], rb[3 * PW]);
-            float2 y4 = make_float2(ra[4 * PW], rb[4 * PW]);
-            Weno5PairWalker W;
-            const float2 vv = f2(v1);
-            float2 Fprev = mul2(vv, W.first(y0, y1, y2, y3, y4, S));
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                y4 = make_float2(ra[(c + 5) * PW], rb[(c + 5) * PW]);
-                const float2 Fn = mul2(vv, W.next(y0, y1, y2, y3, y4, S));
-                const float2 d = mul2(make_float2(Fprev.x - Fn.x, Fprev.y - Fn.y), inv_dq1);
-                stage[(a_row * TQ1 + a_c0 + c) * PWP + lane] = d.x;
-                stage[((a_row + 1) * TQ1 + a_c0 + c) * PWP + lane] = d.y;
-                Fprev = Fn;
-            }
-        }
-        __syncthreads();
-
-        // ---- phase B: q2 faces of cols b_col, b_col+1, BGK, combine ------------
-        if (warp == 0) {
-            vtab[0 * PW + lane] = V1;
-            vtab[1 * PW + lane] = V2;
-            vtab[2 * PW + lane] = V3;
-            vtab[3 * PW + lane] = (V1 * V1 + V2 * V2) + V3 * V3;
-        }
-        {
-            const float v2 = float(V2);
-            const bool right = v2 > 0.0f;
-            const int off = right ? 0 : 1;
-            Weno5Pair S; S.set(right);
-            const float* ca = X + ((b_r0 + off) * HX + b_col + HALO) * PW + lane;
-            const float* cb = ca + PW;
-            const float* cella = X + ((b_r0 + HALO) * HX + b_col + HALO) * PW + lane;
-            float2 y0 = make_float2(ca[0 * HX * PW], cb[0 * HX * PW]);
-            float2 y1 = make_float2(ca[1 * HX * PW], cb[1 * HX * PW]);
-            float2 y2 = make_float2(ca[2 * HX * PW], cb[2 * HX * PW]);
-            float2 y3 = make_float2(ca[3 * HX * PW], cb[3 * HX * PW]);
-            float2 y4 = make_float2(ca[4 * HX * PW], cb[4 * HX * PW]);
-            Weno5PairWalker W;
-            const float2 vv = f2(v2);
-            float2 Fprev = mul2(vv, W.first(y0, y1, y2, y3, y4, S));
-            const double* tb0 = tabs + (b_r0 * TQ1 + b_col) * ntab;
-            const int toff1 = ip1, toff2 = Np1 + ip2, toff3 = Np1 + Np2 + ip3;
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int cq0 = (b_r0 + r) * TQ1 + b_col;
-                y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                y4 = make_float2(ca[(r + 5) * HX * PW], cb[(r + 5) * HX * PW]);
-                const float2 Fn = mul2(vv, W.next(y0, y1, y2, y3, y4, S));
-                const float2 kq0 = make_float2(stage[cq0 * PWP + lane], stage[(cq0 + 1) * PWP + lane]);
-                float2 kk = fma2(make_float2(Fprev.x - Fn.x, Fprev.y - Fn.y), inv_dq2, kq0);
-                Fprev = Fn;
-                if (BGK) {
-                    const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
-                    double fmb[2];
-#pragma unroll
-                    for (int x = 0; x < 2; ++x) {
-                        if (a.bgk_direct) {
-                            const double* qq = qc + (cq0 + x) * 5;
-                            const double mneg = -a.sg.mass[s];
-                            double d1v = V1 - qq[1];
-                            double f0 = qq[0] * exp((mneg * (d1v * d1v)) / qq[4]);
-                            if (a.p_dim >= 2) { double d2v = V2 - qq[2]; f0 = f0 * exp((mneg * (d2v * d2v)) / qq[4]); }
-                            if (a.p_dim == 3) { double d3v = V3 - qq[3]; f0 = f0 * exp((mneg * (d3v * d3v)) / qq[4]); }
-                            fmb[x] = f0;
-                        } else {
-                            const double* tb = tb0 + (r * TQ1 + x) * ntab;
-                            fmb[x] = (tb[toff1] * tb[toff2]) * tb[toff3];
-                        }
-                    }
-                    kk = fma2(make_float2(float(fmb[0]) - fcell.x, float(fmb[1]) - fcell.y),
-                              f2(inv_tau), kk);
-                }
-                const unsigned o0 = toff + r * colstride;
-                const float o1a = fmaf(kk.x, c1, pre1[0][r]);
-                const float o1b = fmaf(kk.y, c1, pre1[1][r]);
-                out1[o0] = o1a;
-                out1[o0 + rowstride] = o1b;
-                if (HAS2) {
-                    out2[o0] = fmaf(kk.x, c2, pre2[0][r]);
-                    out2[o0 + rowstride] = fmaf(kk.y, c2, pre2[1][r]);
-                }
-                stage[cq0 * PWP + lane] = o1a;
-                stage[(cq0 + 1) * PWP + lane] = o1b;
-            }
-        }
-        __syncthreads();
-        fence_proxy_async();
-        issue(k + 2, buf);
-
-        // ---- periodic ghost images of border cells, from the staged outputs ---
-        if (border) {
-            for (int c = warp; c < NQ; c += NWARP) {
-                const int ii = i0 + c % TQ1, jj = j0 + c / TQ1;
-                if ((a.periodic1 && (ii < Ng || ii >= Nq1 - Ng)) ||
-                    (a.periodic2 && (jj < Ng || jj >= Nq2 - Ng)))
-                    write_ghost_images(out1, stage[c * PWP + lane], ii, jj, s, p, Ng, Nq1, Nq2,
-                                       a.Nq1g, a.Nq2g, a.periodic1, a.periodic2,
-                                       (long long)rowstride, (long long)colstride, Np);
-            }
-        }
-
-        // ---- phase C: FP64 moments of out1, divergence check ------------------
-        if (want_mom || check) {
-            const float* sp = stage + pc_c * PWP + pc_q * PQ;
-            const double* vt = vtab + pc_q * PQ;
-#pragma unroll
-            for (int t = 0; t < PQ; ++t) {
-                const float o = sp[t];
-                nonfinite |= !isfinite(o);
-                const double ov = double(o);
-                macc[0] += ov;
-                macc[1] += ov * vt[t];
-                macc[2] += ov * vt[PW + t];
-                macc[3] += ov * vt[2 * PW + t];
-                macc[4] += (0.5 * ov) * vt[3 * PW + t];
-            }
-        }
-        p += PW;
-        toff += PW;
-        ip1 += PW;
-        while (ip1 >= Np1) {
-            ip1 -= Np1;
-            if (++ip2 == Np2) { ip2 = 0; ++ip3; }
-        }
-    }
-    if (check && nonfinite) atomicOr(a.flag, 1);
-    __syncthreads();
-
-    const long long plane = (long long)Nq2 * Nq1;
-    if (want_mom) {
-        double* red = reinterpret_cast<double*>(smem_raw + Lo.tile);
-#pragma unroll
-        for (int q = 0; q < kNumMom; ++q) red[(pc_q * NQ + pc_c) * kNumMom + q] = macc[q];
-        __syncthreads();
-        for (int c = tid; c < NQ * kNumMom; c += NTHREADS) {
-            int cq = c / kNumMom, q = c % kNumMom;
-            double v = 0.0;
-#pragma unroll
-            for (int h = 0; h < NQUART; ++h) v += red[(h * NQ + cq) * kNumMom + q];
-            int ii = i0 + cq % TQ1, jj = j0 + cq / TQ1;
-            a.mom_out[(((long long)split * kNumMom + q) * a.Ns + s) * plane
-                      + (long long)jj * Nq1 + ii] = v;
         }
     }
 }

@@ -4,6 +4,7 @@
 #define BOLT_EXACT false
 #define BOLT_SUFFIX f32
 #include "kernels_impl.cuh"
+#include "qpair_kernel.cuh"
 
 namespace bolt {
 

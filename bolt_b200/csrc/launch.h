@@ -29,6 +29,9 @@ inline size_t qstage_smem(int tiling, size_t elem, int bgk, int bgk_direct, int 
     return qstage_layout(t.tq1, t.tq2, t.q2, (int)elem, bgk, bgk_direct, ntab).total;
 }
 
+// bytes of dynamic shared memory of the paired FP32 kernel
+inline size_t qpair_smem(int ntab, int bgk) { return qpair_layout(ntab, bgk).total; }
+
 inline size_t pstage_smem(int Np, size_t elem) { return 4 * (size_t)Np * elem; }
 
 #define BOLT_DECLARE_LAUNCHERS(SUFFIX, T)                                                   \
@@ -51,7 +54,7 @@ inline size_t pstage_smem(int Np, size_t elem) { return 4 * (size_t)Np * elem; }
 BOLT_DECLARE_LAUNCHERS(f64, double)
 BOLT_DECLARE_LAUNCHERS(f32, float)
 
-// paired FP32 WENO5 q-stage (8x8 tiling, fields off, fused combine, TMA)
+// paired FP32 WENO5 q-stage (8x8 tiling, fields off, fused combine, TMA in and out)
 cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t smem,
                              cudaStream_t st);
 

@@ -1,0 +1,372 @@
+// qpair_kernel.cuh - paired FP32 WENO5 q-stage kernel (sm_100a).
+//
+// The fused RK stage of the 2D3V FVM update with fields off
+// (df_dt_fvm.py:56-97 q-part + BGK source, combined with the stage update of
+// integrators.py:15-28 / fvm_operator.py:26,33) for an 8x8 q-tile and 32
+// consecutive p-cells of one species per chunk.  Every thread walks two
+// adjacent q-rows (phase A) or q-columns (phase B) of the same p at once with
+// f32x2 arithmetic:
+//
+//   phase A  warp w: rows 2(w%4), 2(w%4)+1, cells 4(w/4)..+3 (5 faces each);
+//            q1 part of df/dt -> D1 tile
+//   phase B  warp w: cols 2(w%4), 2(w%4)+1, rows 4(w/4)..+3 (5 faces each);
+//            q2 part + D1 + BGK, then out1 = base1 + c1 k, out2 = base2 + c2 k
+//            into shared staging tiles
+//   phase C  FP64 velocity moments of out1 and the divergence check
+//
+// All global traffic is TMA: the halo tile of the stage input (14x14x32,
+// double-buffered), the base1/base2 tiles (8x8x32) and the out1/out2 tiles
+// (stores from shared memory, bulk-group completion).  out1 is staged with
+// the 128-byte swizzle so that phase C reads 8 consecutive p of one q-cell as
+// two conflict-free 16-byte loads.  Barrier waits are time-bounded and a
+// failure is made CTA-uniform, recorded in the error word, and ends the work.
+//
+// Launch conditions (checked by the host): FP32, WENO5 in q, 8x8 tiling,
+// N_q1, N_q2 multiples of 8 and at least 2 N_g, N_p multiple of 32, N_p1
+// multiple of 8, BGK by exp tables, all five buffers 16-byte aligned, f with
+// fewer than 2^31 elements (32-bit offsets).
+#pragma once
+
+#include "fvm_kernels.cuh"
+
+namespace bolt {
+
+// Swizzled position of element p (0..31) of q-cell row c in a 128-byte
+// swizzled tile: 16-byte chunk index XOR (c mod 8).
+__device__ __forceinline__ int swz(int c, int p) {
+    return c * PW + ((((p >> 2) ^ (c & 7)) << 2) | (p & 3));
+}
+
+// Prologue: p-cell centres of the species, barriers, and for BGK the
+// Maxwellian of the stage input per q-cell with exp tables stored as float2
+// over q-cell pairs (cells 2j, 2j+1 of one tile row): tab[(row*4 + j)*ntab + q].
+template <bool BGK>
+__device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i0, int j0,
+                                               double* vgrid, double* qc, float2* tabs,
+                                               uint64_t* bars) {
+    const int tid = threadIdx.x;
+    const int Np1 = a.Np1, Np2 = a.Np2;
+    const int ntab = Np1 + Np2 + a.Np3;
+    for (int q = tid; q < ntab; q += NTHREADS) {
+        if (q < Np1) vgrid[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
+        else if (q < Np1 + Np2) vgrid[q] = a.sg.p2_start[s] + (0.5 + (q - Np1)) * a.sg.dp2[s];
+        else vgrid[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
+    }
+    if (tid == 0) {
+        prefetch_tmap(&a.tmap);
+        prefetch_tmap(&a.tm_b1);
+        prefetch_tmap(&a.tm_b2);
+        prefetch_tmap(&a.tm_o1);
+        prefetch_tmap(&a.tm_o2);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
+        fence_barrier_init();
+    }
+    if (BGK) {
+        for (int c = tid; c < 64; c += NTHREADS)
+            bgk_cell_params(a, s, i0 + (c & 7), j0 + (c >> 3), qc + c * 5);
+    }
+    __syncthreads();
+    if (BGK) {
+        const double m = a.sg.mass[s];
+        for (int e = tid; e < 32 * ntab; e += NTHREADS) {
+            const int P = e / ntab, q = e - P * ntab;
+            const int c0 = (P >> 2) * 8 + 2 * (P & 3);
+            tabs[e] = make_float2(float(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
+                                  float(bgk_table_entry(a, qc + (c0 + 1) * 5, vgrid, q, m)));
+        }
+    }
+    __syncthreads();
+}
+
+template <bool BGK, bool HAS2>
+__global__ void __launch_bounds__(NTHREADS, 2)
+qpair_kernel(const __grid_constant__ QStageArgs a) {
+    constexpr int TQ = 8, HX = TQ + 2 * HALO, NQ = TQ * TQ, NWARP = NTHREADS / 32;
+    constexpr int XT = HX * HX * PW;                 // floats of one halo tile
+    constexpr int NQUART = NTHREADS / NQ;            // phase C: threads per q-cell
+    static_assert(NWARP == 8 && NQUART == 4, "pair mapping assumes 8 warps");
+
+    const int Np1 = a.Np1, Np2 = a.Np2, Np = a.Np, Ng = a.Ng;
+    const int Nq1 = a.Nq1, Nq2 = a.Nq2;
+    const int ntab = Np1 + Np2 + a.Np3;
+    const PLayout Lo = qpair_layout(ntab, BGK);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* sm = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    float* X = reinterpret_cast<float*>(sm + Lo.x);
+    float* o1s = reinterpret_cast<float*>(sm + Lo.o1);
+    float* o2s = reinterpret_cast<float*>(sm + Lo.o2);
+    float* b1s = reinterpret_cast<float*>(sm + Lo.b1);
+    float* b2s = reinterpret_cast<float*>(sm + Lo.b2);
+    float* d1s = reinterpret_cast<float*>(sm + Lo.d1);
+    float2* tabs = reinterpret_cast<float2*>(sm + Lo.tabs);
+    double* vgrid = reinterpret_cast<double*>(sm + Lo.vgrid);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + Lo.bars);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
+    const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
+    const int i0 = tile1 * TQ, j0 = tile2 * TQ;
+    const int k_begin = split * a.chunks_per_split;
+    const int k_end = min(Np / PW, k_begin + a.chunks_per_split);
+    const int xs = s * Np;                           // TMA x coordinate of the species
+    const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ > Nq1 - Ng)) ||
+                        (a.periodic2 && (j0 < Ng || j0 + TQ > Nq2 - Ng));
+
+    qpair_prologue<BGK>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, bars);
+
+    bool failed = false;
+    unsigned pend = 0u;        // thread 0: barriers with a load in flight
+    auto load_x = [&](int k, int b) {
+        if (k < k_end) {
+            pend |= 1u << b;
+            mbar_arrive_expect_tx(&bars[b], XT * 4);
+            tma_load_3d(X + b * XT, &a.tmap, &bars[b], xs + k * PW, i0 + Ng - HALO,
+                        j0 + Ng - HALO);
+        }
+    };
+    auto load_b = [&](int k) {
+        if (k < k_end) {
+            pend |= 4u;
+            mbar_arrive_expect_tx(&bars[2], (HAS2 ? 2 : 1) * kPairTile);
+            tma_load_3d(b1s, &a.tm_b1, &bars[2], xs + k * PW, i0 + Ng, j0 + Ng);
+            if (HAS2) tma_load_3d(b2s, &a.tm_b2, &bars[2], xs + k * PW, i0 + Ng, j0 + Ng);
+        }
+    };
+    if (tid == 0) {
+        load_x(k_begin, 0);
+        load_x(k_begin + 1, 1);
+        load_b(k_begin);
+    }
+
+    float* __restrict__ out1 = static_cast<float*>(a.out1);
+    const float2 c1 = f2(float(a.c1)), c2 = f2(float(a.c2));
+    const float inv_dq1 = float(1.0 / a.dq1), inv_dq2 = float(1.0 / a.dq2);
+    const float2 inv_tau = f2(float(1.0 / a.tau));
+    const bool want_mom = a.mom_out != nullptr;
+    const bool check = a.flag != nullptr;
+    const unsigned rowstride = (unsigned)(a.Ns * Np);
+    const unsigned colstride = rowstride * (unsigned)a.Nq1g;
+    bool nonfinite = false;
+
+    // phase A / B lane: p = k*32 + lane
+    int ip1, ip2, ip3;
+    {
+        const int p = k_begin * PW + lane;
+        ip1 = p % Np1; ip2 = (p / Np1) % Np2; ip3 = p / (Np1 * Np2);
+    }
+    // phase C: q-cell pc_c, p = k*32 + 8*pc_q .. +7 (one p1 row: N_p1 % 8 == 0)
+    const int pc_c = tid % NQ, pc_q = tid / NQ;
+    int g1, g2, g3;
+    {
+        const int p = k_begin * PW + 8 * pc_q;
+        g1 = p % Np1; g2 = (p / Np1) % Np2; g3 = p / (Np1 * Np2);
+    }
+    const double dp1 = a.sg.dp1[s];
+    double macc[kNumMom] = {0, 0, 0, 0, 0};
+
+    const int rp = warp & 3, seg = warp >> 2;
+    const int a_row = 2 * rp, a_c0 = 4 * seg;        // phase A: rows a_row, a_row+1
+    const int b_col = 2 * rp, b_r0 = 4 * seg;        // phase B: cols b_col, b_col+1
+    const int sw0 = swz(b_col, lane) - b_col * PW;   // swizzled lane slot, column b_col
+    const int sw1 = swz(b_col + 1, lane) - (b_col + 1) * PW;
+    const float4* c_src0 = reinterpret_cast<const float4*>(o1s + pc_c * PW) + ((2 * pc_q) ^ (pc_c & 7));
+    const float4* c_src1 = reinterpret_cast<const float4*>(o1s + pc_c * PW) + ((2 * pc_q + 1) ^ (pc_c & 7));
+    const float2* tb_row = tabs + (b_r0 * 4 + rp) * ntab;
+
+    unsigned phx0 = 0u, phx1 = 0u, phb = 0u;
+    int buf = 0;
+    for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
+        if (!failed && !mbar_wait_bounded(&bars[buf], buf ? phx1 : phx0)) failed = true;
+        if (buf) phx1 ^= 1u; else phx0 ^= 1u;
+        pend &= ~(1u << buf);
+        failed = __syncthreads_or(failed);                        // S1
+        if (failed) break;
+        const float* Xb = X + buf * XT;
+        const double V1 = vgrid[ip1], V2 = vgrid[Np1 + ip2];
+
+        // ---- phase A: q1 faces of rows a_row, a_row+1 -> D1 -------------------
+        {
+            const float v1 = float(V1);
+            const bool right = v1 > 0.0f;
+            Weno5Pair S; S.set(right);
+            const float* ra = Xb + ((a_row + HALO) * HX + a_c0 + (right ? 0 : 1)) * PW + lane;
+            const float* rb = ra + HX * PW;
+            float2 y0 = make_float2(ra[0 * PW], rb[0 * PW]);
+            float2 y1 = make_float2(ra[1 * PW], rb[1 * PW]);
+            float2 y2 = make_float2(ra[2 * PW], rb[2 * PW]);
+            float2 y3 = make_float2(ra[3 * PW], rb[3 * PW]);
+            float2 y4 = make_float2(ra[4 * PW], rb[4 * PW]);
+            Weno5PairWalker W;
+            const float2 vq = f2(v1 * inv_dq1);
+            float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
+            float* da = d1s + (a_row * TQ + a_c0) * PW + lane;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                y0 = y1; y1 = y2; y2 = y3; y3 = y4;
+                y4 = make_float2(ra[(c + 5) * PW], rb[(c + 5) * PW]);
+                const float2 Fn = W.next(y0, y1, y2, y3, y4, S);
+                const float2 d = mul2(sub2(Fprev, Fn), vq);
+                da[c * PW] = d.x;
+                da[(TQ + c) * PW] = d.y;
+                Fprev = Fn;
+            }
+        }
+        // the store of chunk k-1 must be done reading the staging tiles, and
+        // the base tiles of chunk k must have landed, before phase B
+        if (tid == 0) bulk_wait_read_all();
+        if (!failed && !mbar_wait_bounded(&bars[2], phb)) failed = true;
+        phb ^= 1u;
+        pend &= ~4u;
+        failed = __syncthreads_or(failed);                        // S2
+        if (failed) break;
+
+        // ---- phase B: q2 faces of cols b_col, b_col+1, BGK, combine ------------
+        {
+            const float v2 = float(V2);
+            const bool right = v2 > 0.0f;
+            Weno5Pair S; S.set(right);
+            const float* ca = Xb + ((b_r0 + (right ? 0 : 1)) * HX + b_col + HALO) * PW + lane;
+            const float* cb = ca + PW;
+            const float* cella = Xb + ((b_r0 + HALO) * HX + b_col + HALO) * PW + lane;
+            float2 y0 = make_float2(ca[0 * HX * PW], cb[0 * HX * PW]);
+            float2 y1 = make_float2(ca[1 * HX * PW], cb[1 * HX * PW]);
+            float2 y2 = make_float2(ca[2 * HX * PW], cb[2 * HX * PW]);
+            float2 y3 = make_float2(ca[3 * HX * PW], cb[3 * HX * PW]);
+            float2 y4 = make_float2(ca[4 * HX * PW], cb[4 * HX * PW]);
+            Weno5PairWalker W;
+            const float2 vq = f2(v2 * inv_dq2);
+            float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
+            const int cb0 = b_r0 * TQ + b_col;                   // q-cell of row 0, col b_col
+            const float* dk = d1s + cb0 * PW + lane;
+            const float* bb1 = b1s + cb0 * PW + lane;
+            const float* bb2 = b2s + cb0 * PW + lane;
+            float* ob1 = o1s + cb0 * PW;
+            float* ob2 = o2s + cb0 * PW + lane;
+            const float2* t1 = tb_row + ip1;
+            const float2* t2 = tb_row + Np1 + ip2;
+            const float2* t3 = tb_row + Np1 + Np2 + ip3;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                y0 = y1; y1 = y2; y2 = y3; y3 = y4;
+                y4 = make_float2(ca[(r + 5) * HX * PW], cb[(r + 5) * HX * PW]);
+                const float2 Fn = W.next(y0, y1, y2, y3, y4, S);
+                const float2 kq = make_float2(dk[r * TQ * PW], dk[r * TQ * PW + PW]);
+                float2 kk = fma2(sub2(Fprev, Fn), vq, kq);
+                Fprev = Fn;
+                if (BGK) {
+                    const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
+                    const float2 f0 = mul2(mul2(t1[r * 4 * ntab], t2[r * 4 * ntab]),
+                                           t3[r * 4 * ntab]);
+                    kk = fma2(sub2(f0, fcell), inv_tau, kk);
+                }
+                const float2 o1 = fma2(kk, c1, make_float2(bb1[r * TQ * PW], bb1[r * TQ * PW + PW]));
+                ob1[r * TQ * PW + sw0] = o1.x;
+                ob1[r * TQ * PW + PW + sw1] = o1.y;
+                if (HAS2) {
+                    const float2 o2 = fma2(kk, c2, make_float2(bb2[r * TQ * PW], bb2[r * TQ * PW + PW]));
+                    ob2[r * TQ * PW] = o2.x;
+                    ob2[r * TQ * PW + PW] = o2.y;
+                }
+            }
+        }
+        fence_proxy_async();       // staging writes -> visible to the bulk-copy proxy
+        __syncthreads();                                          // S3
+        if (tid == 0) {
+            tma_store_3d(&a.tm_o1, o1s, xs + k * PW, i0 + Ng, j0 + Ng);
+            if (HAS2) tma_store_3d(&a.tm_o2, o2s, xs + k * PW, i0 + Ng, j0 + Ng);
+            bulk_commit();
+            load_x(k + 2, buf);
+            load_b(k + 1);
+        }
+
+        // ---- periodic ghost images of border cells, from the staged out1 -------
+        // (2 N_g <= N_q on both axes: at most one image per axis and a corner)
+        if (border) {
+            const int ii = i0 + warp;                              // warp w owns column w
+            const int d1 = !a.periodic1 ? 0 : (ii < Ng ? Nq1 : (ii >= Nq1 - Ng ? -Nq1 : 0));
+            const int base_c = (Ng * (int)colstride) + (ii + Ng) * (int)rowstride + xs + k * PW + lane;
+#pragma unroll 1
+            for (int r = 0; r < TQ; ++r) {
+                const int jj = j0 + r;
+                const int d2 = !a.periodic2 ? 0 : (jj < Ng ? Nq2 : (jj >= Nq2 - Ng ? -Nq2 : 0));
+                if ((d1 | d2) == 0) continue;
+                const float v = o1s[swz(r * TQ + warp, lane)];
+                const int o = base_c + jj * (int)colstride;
+                if (d1) out1[o + d1 * (int)rowstride] = v;
+                if (d2) out1[o + d2 * (int)colstride] = v;
+                if (d1 && d2) out1[o + d1 * (int)rowstride + d2 * (int)colstride] = v;
+            }
+        }
+
+        // ---- phase C: FP64 moments of out1, divergence check ------------------
+        // 8 consecutive p of one p1 row: v1 = V1_0 + t dp1 (t = 0..7), v2, v3
+        // fixed, so every moment follows from S0 = sum o_t, S1 = sum t o_t and
+        // S2 = sum t^2 o_t (moments.py:6-24 / compute_moments.py:7-59)
+        if (want_mom || check) {
+            const float4 u = *c_src0, w = *c_src1;
+            const double o0 = u.x, o1 = u.y, o2 = u.z, o3 = u.w;
+            const double o4 = w.x, o5 = w.y, o6 = w.z, o7 = w.w;
+            const double S0 = ((o0 + o1) + (o2 + o3)) + ((o4 + o5) + (o6 + o7));
+            const double S1 = fma(7.0, o7, fma(6.0, o6, fma(5.0, o5, fma(4.0, o4,
+                              fma(3.0, o3, fma(2.0, o2, o1))))));
+            const double S2 = fma(49.0, o7, fma(36.0, o6, fma(25.0, o5, fma(16.0, o4,
+                              fma(9.0, o3, fma(4.0, o2, o1))))));
+            nonfinite |= !isfinite(S0);
+            const double W1 = vgrid[g1], W2 = vgrid[Np1 + g2], W3 = vgrid[Np1 + Np2 + g3];
+            macc[0] += S0;
+            macc[1] = fma(W1, S0, fma(dp1, S1, macc[1]));
+            macc[2] = fma(W2, S0, macc[2]);
+            macc[3] = fma(W3, S0, macc[3]);
+            // 0.5 sum o_t (v1_t^2 + v2^2 + v3^2)
+            const double e0 = fma(W1, W1, fma(W2, W2, W3 * W3));
+            const double q = fma(e0, S0, fma(2.0 * W1 * dp1, S1, (dp1 * dp1) * S2));
+            macc[4] = fma(0.5, q, macc[4]);
+        }
+        ip1 += PW;
+        while (ip1 >= Np1) {
+            ip1 -= Np1;
+            if (++ip2 == Np2) { ip2 = 0; ++ip3; }
+        }
+        g1 += PW;
+        while (g1 >= Np1) {
+            g1 -= Np1;
+            if (++g2 == Np2) { g2 = 0; ++g3; }
+        }
+    }
+    if (failed) {
+        // a barrier wait ran out: record it, then let the copies still in
+        // flight land (bounded) before the CTA releases its shared memory
+        if (tid == 0) {
+            atomicExch(a.err, 4);
+            bulk_wait_all();
+            if (pend & 1u) mbar_wait_bounded(&bars[0], phx0);
+            if (pend & 2u) mbar_wait_bounded(&bars[1], phx1);
+            if (pend & 4u) mbar_wait_bounded(&bars[2], phb);
+        }
+        return;
+    }
+    if (check && nonfinite) atomicOr(a.flag, 1);
+    if (tid == 0) bulk_wait_all();
+    __syncthreads();
+
+    const long long plane = (long long)Nq2 * Nq1;
+    if (want_mom) {
+        double* red = reinterpret_cast<double*>(sm + Lo.x);
+#pragma unroll
+        for (int q = 0; q < kNumMom; ++q) red[(pc_q * NQ + pc_c) * kNumMom + q] = macc[q];
+        __syncthreads();
+        for (int c = tid; c < NQ * kNumMom; c += NTHREADS) {
+            const int cq = c / kNumMom, q = c % kNumMom;
+            double v = 0.0;
+#pragma unroll
+            for (int h = 0; h < NQUART; ++h) v += red[(h * NQ + cq) * kNumMom + q];
+            const int ii = i0 + (cq & 7), jj = j0 + (cq >> 3);
+            a.mom_out[(((long long)split * kNumMom + q) * a.Ns + s) * plane
+                      + (long long)jj * Nq1 + ii] = v;
+        }
+    }
+}
+
+}  // namespace bolt
