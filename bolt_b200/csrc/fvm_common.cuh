@@ -295,58 +295,74 @@ __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
 __device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(fast_rcp(a.x), fast_rcp(a.y)); }
 
+// Per-lane coefficients of the upwind side.  With D2_k the second difference
+// and D3 the third difference of the window, the reference's weighted value
+// sum w_k u_k / sum w_k equals u2 + (w1 (u1 - u2) + w3 (u3 - u2)) / sum w_k,
+// where u1 - u2 and u3 - u2 are multiples of the third differences
+// D3a = y0 - 3y1 + 3y2 - y3 = D2_1 - D2_2 and D3b = y1 - 3y2 + 3y3 - y4 = D2_2 - D2_3
+// (right face: 0.375 D3a, 0.125 D3b; left face: -0.125 D3a, -0.375 D3b).
+// The weights are scaled by 16 (w = (1, 10, 5) / 16 right, (5, 10, 1) / 16 left).
 struct Weno5Pair {
-    float2 cw1, cw2, cw3;
-    float2 a10, a11, a12, a20, a21, a22, a30, a31, a32;   // c_k * interpolant coefficients
+    float2 w1, w3, k1, k3, ua, uc;
     __device__ __forceinline__ void set(bool right) {
-        const float c1 = right ? 0.0625f : 0.3125f, c2 = 0.625f, c3 = right ? 0.3125f : 0.0625f;
-        cw1 = f2(c1); cw2 = f2(c2); cw3 = f2(c3);
-        if (right) {
-            a10 = f2(c1 * 0.375f);  a11 = f2(c1 * -1.25f); a12 = f2(c1 * 1.875f);
-            a20 = f2(c2 * -0.125f); a21 = f2(c2 * 0.75f);  a22 = f2(c2 * 0.375f);
-            a30 = f2(c3 * 0.375f);  a31 = f2(c3 * 0.75f);  a32 = f2(c3 * -0.125f);
-        } else {
-            a10 = f2(c1 * -0.125f); a11 = f2(c1 * 0.75f);  a12 = f2(c1 * 0.375f);
-            a20 = f2(c2 * 0.375f);  a21 = f2(c2 * 0.75f);  a22 = f2(c2 * -0.125f);
-            a30 = f2(c3 * 1.875f);  a31 = f2(c3 * -1.25f); a32 = f2(c3 * 0.375f);
-        }
+        w1 = f2(right ? 1.0f : 5.0f);
+        w3 = f2(right ? 5.0f : 1.0f);
+        k1 = f2(right ? 0.375f : -0.625f);     // 16 c1 (u1 - u2) / D3a
+        k3 = f2(right ? 0.625f : -0.375f);     // 16 c3 (u3 - u2) / D3b
+        ua = f2(right ? -0.125f : 0.375f);     // u2 = ua y1 + 0.75 y2 + uc y3
+        uc = f2(right ? 0.375f : -0.125f);
     }
 };
 
-__device__ __forceinline__ float2 beta_pair(float2 a, float2 b, float2 c) {
-    const float2 d1 = fma2(f2(-2.0f), b, add2(a, c));            // a - 2b + c
-    const float2 d2 = fma2(f2(3.0f), c, fma2(f2(-4.0f), b, a));   // a - 4b + 3c
-    return fma2(mul2(f2(13.0f / 12.0f), d1), d1, fma2(mul2(f2(0.25f), d2), d2, f2(1e-17f)));
+// smoothness indicator of substencil (a, b, c) given its second difference
+// D2 = a - 2b + c: 13/12 D2^2 + 1/4 (a - 4b + 3c)^2 + 1e-17, a - 4b + 3c = D2 + 2 (c - b)
+__device__ __forceinline__ float2 beta_pair(float2 D2, float2 b, float2 c) {
+    const float2 e = fma2(f2(2.0f), sub2(c, b), D2);
+    return fma2(mul2(f2(13.0f / 12.0f), D2), D2, fma2(mul2(f2(0.25f), e), e, f2(1e-17f)));
 }
 
+__device__ __forceinline__ float2 second_diff(float2 a, float2 b, float2 c) {
+    return fma2(f2(-2.0f), b, add2(a, c));
+}
+
+// Sliding walker: carries 1/beta^2 of substencils 2 and 3, the second
+// difference of substencil 3 and the third difference D3b of the last face.
 struct Weno5PairWalker {
-    float2 q2, q3;   // 1/beta^2 of substencils 2 and 3
+    float2 q2, q3, d23, d3b;
     __device__ __forceinline__ static float2 inv_sq(float2 b) {
         const float2 r = rcp2(b);
         return mul2(r, r);
     }
-    __device__ __forceinline__ float2 eval(float2 q1, float2 y0, float2 y1, float2 y2, float2 y3,
-                                           float2 y4, const Weno5Pair& S) {
-        const float2 u1 = fma2(S.a12, y2, fma2(S.a11, y1, mul2(S.a10, y0)));
-        const float2 u2 = fma2(S.a22, y3, fma2(S.a21, y2, mul2(S.a20, y1)));
-        const float2 u3 = fma2(S.a32, y4, fma2(S.a31, y3, mul2(S.a30, y2)));
-        const float2 num = fma2(q3, u3, fma2(q2, u2, mul2(q1, u1)));
-        const float2 den = fma2(S.cw3, q3, fma2(S.cw2, q2, mul2(S.cw1, q1)));
-        return mul2(num, rcp2(den));
+    __device__ __forceinline__ float2 eval(float2 q1, float2 d3a, float2 y1, float2 y2, float2 y3,
+                                           const Weno5Pair& S) const {
+        const float2 u2 = fma2(S.ua, y1, fma2(f2(0.75f), y2, mul2(S.uc, y3)));
+        const float2 num = fma2(mul2(S.k3, q3), d3b, mul2(mul2(S.k1, q1), d3a));
+        const float2 den = fma2(S.w3, q3, fma2(f2(10.0f), q2, mul2(S.w1, q1)));
+        return fma2(num, rcp2(den), u2);
     }
     __device__ __forceinline__ float2 first(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
                                             const Weno5Pair& S) {
-        const float2 q1 = inv_sq(beta_pair(y0, y1, y2));
-        q2 = inv_sq(beta_pair(y1, y2, y3));
-        q3 = inv_sq(beta_pair(y2, y3, y4));
-        return eval(q1, y0, y1, y2, y3, y4, S);
+        const float2 d21 = second_diff(y0, y1, y2);
+        const float2 d22 = second_diff(y1, y2, y3);
+        d23 = second_diff(y2, y3, y4);
+        const float2 q1 = inv_sq(beta_pair(d21, y1, y2));
+        q2 = inv_sq(beta_pair(d22, y2, y3));
+        q3 = inv_sq(beta_pair(d23, y3, y4));
+        const float2 d3a = sub2(d21, d22);
+        d3b = sub2(d22, d23);
+        return eval(q1, d3a, y1, y2, y3, S);
     }
+    // window advanced by one cell: y0..y4 are the new window's values
     __device__ __forceinline__ float2 next(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
                                            const Weno5Pair& S) {
         const float2 q1 = q2;
+        const float2 d3a = d3b;
+        const float2 d22 = d23;
         q2 = q3;
-        q3 = inv_sq(beta_pair(y2, y3, y4));
-        return eval(q1, y0, y1, y2, y3, y4, S);
+        d23 = second_diff(y2, y3, y4);
+        q3 = inv_sq(beta_pair(d23, y3, y4));
+        d3b = sub2(d22, d23);
+        return eval(q1, d3a, y1, y2, y3, S);
     }
 };
 

@@ -15,7 +15,8 @@
 //   phase C  FP64 velocity moments of out1 and the divergence check
 //
 // All global traffic is TMA: the halo tile of the stage input (14x14x32,
-// double-buffered), the base1/base2 tiles (8x8x32) and the out1/out2 tiles
+// double-buffered), the base1/base2 tiles (8x8x32; taken from the halo tile
+// when they are the stage input itself) and the out1/out2 tiles
 // (stores from shared memory, bulk-group completion).  out1 is staged with
 // the 128-byte swizzle so that phase C reads 8 consecutive p of one q-cell as
 // two conflict-free 16-byte loads.  Barrier waits are time-bounded and a
@@ -80,7 +81,9 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
     __syncthreads();
 }
 
-template <bool BGK, bool HAS2>
+// BX: base1 (and base2) are the stage input itself (the first RK4 stage), so
+// the base values come from the halo tile and no base tiles are loaded.
+template <bool BGK, bool HAS2, bool BX>
 __global__ void __launch_bounds__(NTHREADS, 2)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
     constexpr int TQ = 8, HX = TQ + 2 * HALO, NQ = TQ * TQ, NWARP = NTHREADS / 32;
@@ -127,7 +130,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         }
     };
     auto load_b = [&](int k) {
-        if (k < k_end) {
+        if (!BX && k < k_end) {
             pend |= 4u;
             mbar_arrive_expect_tx(&bars[2], (HAS2 ? 2 : 1) * kPairTile);
             tma_load_3d(b1s, &a.tm_b1, &bars[2], xs + k * PW, i0 + Ng, j0 + Ng);
@@ -181,8 +184,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         if (!failed && !mbar_wait_bounded(&bars[buf], buf ? phx1 : phx0)) failed = true;
         if (buf) phx1 ^= 1u; else phx0 ^= 1u;
         pend &= ~(1u << buf);
-        failed = __syncthreads_or(failed);                        // S1
-        if (failed) break;
+        // no CTA barrier here: each thread has waited for the halo tile itself,
+        // D1 was last read before the previous chunk's third barrier, and a
+        // failed wait reaches every thread through the next barrier
         const float* Xb = X + buf * XT;
         const double V1 = vgrid[ip1], V2 = vgrid[Np1 + ip2];
 
@@ -216,10 +220,12 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         // the store of chunk k-1 must be done reading the staging tiles, and
         // the base tiles of chunk k must have landed, before phase B
         if (tid == 0) bulk_wait_read_all();
-        if (!failed && !mbar_wait_bounded(&bars[2], phb)) failed = true;
-        phb ^= 1u;
-        pend &= ~4u;
-        failed = __syncthreads_or(failed);                        // S2
+        if (!BX) {
+            if (!failed && !mbar_wait_bounded(&bars[2], phb)) failed = true;
+            phb ^= 1u;
+            pend &= ~4u;
+        }
+        failed = __syncthreads_or(failed);                        // barrier 1
         if (failed) break;
 
         // ---- phase B: q2 faces of cols b_col, b_col+1, BGK, combine ------------
@@ -255,24 +261,26 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
                 const float2 kq = make_float2(dk[r * TQ * PW], dk[r * TQ * PW + PW]);
                 float2 kk = fma2(sub2(Fprev, Fn), vq, kq);
                 Fprev = Fn;
+                const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
                 if (BGK) {
-                    const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
                     const float2 f0 = mul2(mul2(t1[r * 4 * ntab], t2[r * 4 * ntab]),
                                            t3[r * 4 * ntab]);
                     kk = fma2(sub2(f0, fcell), inv_tau, kk);
                 }
-                const float2 o1 = fma2(kk, c1, make_float2(bb1[r * TQ * PW], bb1[r * TQ * PW + PW]));
+                const float2 o1 = fma2(kk, c1, BX ? fcell : make_float2(bb1[r * TQ * PW],
+                                                                         bb1[r * TQ * PW + PW]));
                 ob1[r * TQ * PW + sw0] = o1.x;
                 ob1[r * TQ * PW + PW + sw1] = o1.y;
                 if (HAS2) {
-                    const float2 o2 = fma2(kk, c2, make_float2(bb2[r * TQ * PW], bb2[r * TQ * PW + PW]));
+                    const float2 o2 = fma2(kk, c2, BX ? fcell : make_float2(bb2[r * TQ * PW],
+                                                                             bb2[r * TQ * PW + PW]));
                     ob2[r * TQ * PW] = o2.x;
                     ob2[r * TQ * PW + PW] = o2.y;
                 }
             }
         }
         fence_proxy_async();       // staging writes -> visible to the bulk-copy proxy
-        __syncthreads();                                          // S3
+        __syncthreads();                                          // barrier 2
         if (tid == 0) {
             tma_store_3d(&a.tm_o1, o1s, xs + k * PW, i0 + Ng, j0 + Ng);
             if (HAS2) tma_store_3d(&a.tm_o2, o2s, xs + k * PW, i0 + Ng, j0 + Ng);
