@@ -465,17 +465,19 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
         for (int i = 0; i < 4; ++i)
             if (ptrs[i] && ((uintptr_t)ptrs[i]) % 16 != 0) pair = false;
         if ((a.base2 == nullptr) != (a.out2 == nullptr)) pair = false;
+        // stage shapes of the paired kernel: bases = stage input, or out2 is
+        // its own base (accumulated in place), or no out2
+        const bool bx = a.base1 == a.fs && (!a.base2 || a.base2 == a.fs);
+        if (a.base2 && !bx && a.base2 != a.out2) pair = false;
     }
     if (pair) {
         // copy each map out at once: a later lookup may recycle its cache slot
         const CUtensorMap* m;
         if ((m = get_tmap(ctx, a.base1, TMAP_TILE))) a.tm_b1 = *m; else pair = false;
         if (pair && (m = get_tmap(ctx, a.out1, TMAP_TILE_SWZ))) a.tm_o1 = *m; else pair = false;
-        a.tm_b2 = a.tm_b1;
         a.tm_o2 = a.tm_o1;
-        if (pair && a.base2) {
-            if ((m = get_tmap(ctx, a.base2, TMAP_TILE))) a.tm_b2 = *m; else pair = false;
-            if (pair && (m = get_tmap(ctx, a.out2, TMAP_TILE))) a.tm_o2 = *m; else pair = false;
+        if (pair && a.out2) {
+            if ((m = get_tmap(ctx, a.out2, TMAP_TILE))) a.tm_o2 = *m; else pair = false;
         }
     }
     const size_t smem = pair ? qpair_smem(ctx->ntab, ctx->bgk)

@@ -46,7 +46,7 @@ __host__ __device__ inline QLayout qstage_layout(int tq1, int tq2, int q2, int e
 // a 1024-byte aligned base (the 128-byte swizzled output tile needs it; the
 // kernel aligns the dynamic base itself, hence the 1 KB of slack in total).
 struct PLayout {
-    unsigned x, o1, o2, b1, b2, d1, tabs, vgrid, bars, total;
+    unsigned x, o1, o2, b1, d1, tabs, vgrid, bars, total;
 };
 
 constexpr unsigned kPairTile = 8 * 8 * PW * 4;                       // 8 KB
@@ -59,13 +59,12 @@ __host__ __device__ inline PLayout qpair_layout(int ntab, int bgk) {
     o = qalign(o, 1024);
     L.o1 = o; o += kPairTile;                     // out1 staging (128B swizzle)
     L.o2 = o; o += kPairTile;                     // out2 staging
-    L.b1 = o; o += kPairTile;                     // base1 tile
-    L.b2 = o; o += kPairTile;                     // base2 tile
+    L.b1 = o; o += 2 * kPairTile;                 // base1 tile, double-buffered
     L.d1 = o; o += kPairTile;                     // q1 part of df/dt (prologue: Maxwellian
                                                   // parameters of the 64 q-cells)
     L.tabs = o; o += bgk ? 32u * ntab * 8u : 0u;  // exp tables, one float2 per q-cell pair
     L.vgrid = o; o += ntab * sizeof(double);
-    L.bars = qalign(o, 8); o = L.bars + 3 * sizeof(unsigned long long);
+    L.bars = qalign(o, 8); o = L.bars + 4 * sizeof(unsigned long long);
     L.total = o + 1024;
     return L;
 }
@@ -98,8 +97,8 @@ struct QStageArgs {
     int bgk_direct;             // 1: exp per cell (no per-q-cell exp tables)
     int full_chunks;            // Np % 32 == 0: every p-chunk is complete
     SpeciesGrid sg;
-    // paired kernel only: 8x8x32 boxes over base1, base2, out1 (128B swizzle), out2
-    CUtensorMap tm_b1, tm_b2, tm_o1, tm_o2;
+    // paired kernel only: 8x8x32 boxes over base1, out1 (128B swizzle), out2
+    CUtensorMap tm_b1, tm_o1, tm_o2;
 };
 
 struct PStageArgs {

@@ -434,6 +434,16 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void*
         : "memory");
 }
 
+// shared -> global box reduction: global += shared, element type of the map
+__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap* map, const void* src, int x,
+                                                  int y, int z) {
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group"
+        " [%0, {%2, %3, %4}], [%1];"
+        ::"l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
 __device__ __forceinline__ void bulk_commit() {
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }

@@ -11,15 +11,20 @@ namespace bolt {
 cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t smem,
                              cudaStream_t st) {
     const bool has2 = a.out2 != nullptr;
-    // first RK4 stage: base1 (and base2) are the stage input
+    // first RK4 / RK2 stage: the bases are the stage input
     const bool bx = a.base1 == a.fs && (!has2 || a.base2 == a.fs);
+    int mode;
+    if (bx) mode = has2 ? QP_X2 : QP_X1;
+    else if (!has2) mode = QP_B1;
+    else if (a.base2 == a.out2) mode = QP_B1R2;
+    else return cudaErrorInvalidValue;        // excluded by the host's dispatch
     void (*k)(QStageArgs);
-    if (bx)
-        k = bgk ? (has2 ? qpair_kernel<true, true, true> : qpair_kernel<true, false, true>)
-                : (has2 ? qpair_kernel<false, true, true> : qpair_kernel<false, false, true>);
-    else
-        k = bgk ? (has2 ? qpair_kernel<true, true, false> : qpair_kernel<true, false, false>)
-                : (has2 ? qpair_kernel<false, true, false> : qpair_kernel<false, false, false>);
+    switch (mode) {
+        case QP_X1: k = bgk ? qpair_kernel<true, QP_X1> : qpair_kernel<false, QP_X1>; break;
+        case QP_X2: k = bgk ? qpair_kernel<true, QP_X2> : qpair_kernel<false, QP_X2>; break;
+        case QP_B1: k = bgk ? qpair_kernel<true, QP_B1> : qpair_kernel<false, QP_B1>; break;
+        default: k = bgk ? qpair_kernel<true, QP_B1R2> : qpair_kernel<false, QP_B1R2>; break;
+    }
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, NTHREADS, smem, st>>>(a);

@@ -15,8 +15,9 @@
 //   phase C  FP64 velocity moments of out1 and the divergence check
 //
 // All global traffic is TMA: the halo tile of the stage input (14x14x32,
-// double-buffered), the base1/base2 tiles (8x8x32; taken from the halo tile
-// when they are the stage input itself) and the out1/out2 tiles
+// double-buffered), the base1 tile (8x8x32, double-buffered; taken from the
+// halo tile when it is the stage input itself) and the out1/out2 tiles; an
+// out2 that is its own base (the RK4 accumulator) gets c2 k by TMA reduce-add
 // (stores from shared memory, bulk-group completion).  out1 is staged with
 // the 128-byte swizzle so that phase C reads 8 consecutive p of one q-cell as
 // two conflict-free 16-byte loads.  Barrier waits are time-bounded and a
@@ -56,12 +57,12 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
     if (tid == 0) {
         prefetch_tmap(&a.tmap);
         prefetch_tmap(&a.tm_b1);
-        prefetch_tmap(&a.tm_b2);
         prefetch_tmap(&a.tm_o1);
         prefetch_tmap(&a.tm_o2);
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_init(&bars[2], 1);
+        mbar_init(&bars[3], 1);
         fence_barrier_init();
     }
     if (BGK) {
@@ -81,11 +82,21 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
     __syncthreads();
 }
 
-// BX: base1 (and base2) are the stage input itself (the first RK4 stage), so
-// the base values come from the halo tile and no base tiles are loaded.
-template <bool BGK, bool HAS2, bool BX>
+// Stage modes (which of out1 = base1 + c1 k, out2 = base2 + c2 k exist and
+// where their bases come from):
+//   QP_X1   base1 = stage input (from the halo tile), out1 only
+//   QP_X2   base1 = base2 = stage input, out1 and out2 stored
+//   QP_B1   base1 tiles loaded (double-buffered), out1 only
+//   QP_B1R2 base1 tiles loaded, out2 = base2 in place: c2 k is added to it by
+//           a TMA reduce-add (no base2 load)
+enum QPairMode { QP_X1 = 0, QP_X2 = 1, QP_B1 = 2, QP_B1R2 = 3 };
+
+template <bool BGK, int MODE>
 __global__ void __launch_bounds__(NTHREADS, 2)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
+    constexpr bool BX = MODE == QP_X1 || MODE == QP_X2;
+    constexpr bool HAS2 = MODE == QP_X2 || MODE == QP_B1R2;
+    constexpr bool RED2 = MODE == QP_B1R2;
     constexpr int TQ = 8, HX = TQ + 2 * HALO, NQ = TQ * TQ, NWARP = NTHREADS / 32;
     constexpr int XT = HX * HX * PW;                 // floats of one halo tile
     constexpr int NQUART = NTHREADS / NQ;            // phase C: threads per q-cell
@@ -101,7 +112,6 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     float* o1s = reinterpret_cast<float*>(sm + Lo.o1);
     float* o2s = reinterpret_cast<float*>(sm + Lo.o2);
     float* b1s = reinterpret_cast<float*>(sm + Lo.b1);
-    float* b2s = reinterpret_cast<float*>(sm + Lo.b2);
     float* d1s = reinterpret_cast<float*>(sm + Lo.d1);
     float2* tabs = reinterpret_cast<float2*>(sm + Lo.tabs);
     double* vgrid = reinterpret_cast<double*>(sm + Lo.vgrid);
@@ -129,18 +139,19 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
                         j0 + Ng - HALO);
         }
     };
-    auto load_b = [&](int k) {
+    auto load_b = [&](int k, int b) {          // base1 tile of chunk k -> buffer b
         if (!BX && k < k_end) {
-            pend |= 4u;
-            mbar_arrive_expect_tx(&bars[2], (HAS2 ? 2 : 1) * kPairTile);
-            tma_load_3d(b1s, &a.tm_b1, &bars[2], xs + k * PW, i0 + Ng, j0 + Ng);
-            if (HAS2) tma_load_3d(b2s, &a.tm_b2, &bars[2], xs + k * PW, i0 + Ng, j0 + Ng);
+            pend |= 4u << b;
+            mbar_arrive_expect_tx(&bars[2 + b], kPairTile);
+            tma_load_3d(b1s + b * (kPairTile / 4), &a.tm_b1, &bars[2 + b], xs + k * PW, i0 + Ng,
+                        j0 + Ng);
         }
     };
     if (tid == 0) {
         load_x(k_begin, 0);
         load_x(k_begin + 1, 1);
-        load_b(k_begin);
+        load_b(k_begin, 0);
+        load_b(k_begin + 1, 1);
     }
 
     float* __restrict__ out1 = static_cast<float*>(a.out1);
@@ -178,7 +189,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const float4* c_src1 = reinterpret_cast<const float4*>(o1s + pc_c * PW) + ((2 * pc_q + 1) ^ (pc_c & 7));
     const float2* tb_row = tabs + (b_r0 * 4 + rp) * ntab;
 
-    unsigned phx0 = 0u, phx1 = 0u, phb = 0u;
+    unsigned phx0 = 0u, phx1 = 0u, phb0 = 0u, phb1 = 0u;
     int buf = 0;
     for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
         if (!failed && !mbar_wait_bounded(&bars[buf], buf ? phx1 : phx0)) failed = true;
@@ -221,9 +232,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         // the base tiles of chunk k must have landed, before phase B
         if (tid == 0) bulk_wait_read_all();
         if (!BX) {
-            if (!failed && !mbar_wait_bounded(&bars[2], phb)) failed = true;
-            phb ^= 1u;
-            pend &= ~4u;
+            if (!failed && !mbar_wait_bounded(&bars[2 + buf], buf ? phb1 : phb0)) failed = true;
+            if (buf) phb1 ^= 1u; else phb0 ^= 1u;
+            pend &= ~(4u << buf);
         }
         failed = __syncthreads_or(failed);                        // barrier 1
         if (failed) break;
@@ -246,8 +257,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
             const int cb0 = b_r0 * TQ + b_col;                   // q-cell of row 0, col b_col
             const float* dk = d1s + cb0 * PW + lane;
-            const float* bb1 = b1s + cb0 * PW + lane;
-            const float* bb2 = b2s + cb0 * PW + lane;
+            const float* bb1 = b1s + buf * (kPairTile / 4) + cb0 * PW + lane;
             float* ob1 = o1s + cb0 * PW;
             float* ob2 = o2s + cb0 * PW + lane;
             const float2* t1 = tb_row + ip1;
@@ -272,8 +282,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
                 ob1[r * TQ * PW + sw0] = o1.x;
                 ob1[r * TQ * PW + PW + sw1] = o1.y;
                 if (HAS2) {
-                    const float2 o2 = fma2(kk, c2, BX ? fcell : make_float2(bb2[r * TQ * PW],
-                                                                             bb2[r * TQ * PW + PW]));
+                    // QP_X2: the full out2; QP_B1R2: the increment c2 k
+                    const float2 o2 = RED2 ? mul2(kk, c2) : fma2(kk, c2, fcell);
                     ob2[r * TQ * PW] = o2.x;
                     ob2[r * TQ * PW + PW] = o2.y;
                 }
@@ -283,10 +293,11 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         __syncthreads();                                          // barrier 2
         if (tid == 0) {
             tma_store_3d(&a.tm_o1, o1s, xs + k * PW, i0 + Ng, j0 + Ng);
-            if (HAS2) tma_store_3d(&a.tm_o2, o2s, xs + k * PW, i0 + Ng, j0 + Ng);
+            if (MODE == QP_X2) tma_store_3d(&a.tm_o2, o2s, xs + k * PW, i0 + Ng, j0 + Ng);
+            if (RED2) tma_reduce_add_3d(&a.tm_o2, o2s, xs + k * PW, i0 + Ng, j0 + Ng);
             bulk_commit();
             load_x(k + 2, buf);
-            load_b(k + 1);
+            load_b(k + 2, buf);
         }
 
         // ---- periodic ghost images of border cells, from the staged out1 -------
@@ -351,7 +362,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             bulk_wait_all();
             if (pend & 1u) mbar_wait_bounded(&bars[0], phx0);
             if (pend & 2u) mbar_wait_bounded(&bars[1], phx1);
-            if (pend & 4u) mbar_wait_bounded(&bars[2], phb);
+            if (pend & 4u) mbar_wait_bounded(&bars[2], phb0);
+            if (pend & 8u) mbar_wait_bounded(&bars[3], phb1);
         }
         return;
     }
