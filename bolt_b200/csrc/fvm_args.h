@@ -51,6 +51,7 @@ struct PLayout {
 
 constexpr unsigned kPairTile = 8 * 8 * PW * 4;                       // 8 KB
 constexpr unsigned kPairHalo = (8 + 2 * HALO) * (8 + 2 * HALO) * PW * 4;  // 24.5 KB
+constexpr unsigned kTabPitch = 33;       // exp-table row: 32 q-cell pairs + 1 pad
 
 __host__ __device__ inline PLayout qpair_layout(int ntab, int bgk) {
     PLayout L;
@@ -62,7 +63,7 @@ __host__ __device__ inline PLayout qpair_layout(int ntab, int bgk) {
     L.b1 = o; o += 2 * kPairTile;                 // base1 tile, double-buffered
     L.d1 = o; o += kPairTile;                     // q1 part of df/dt (prologue: Maxwellian
                                                   // parameters of the 64 q-cells)
-    L.tabs = o; o += bgk ? 32u * ntab * 8u : 0u;  // exp tables, one float2 per q-cell pair
+    L.tabs = o; o += bgk ? kTabPitch * ntab * 8u : 0u;  // exp tables, float2 per q-cell pair
     L.vgrid = o; o += ntab * sizeof(double);
     L.bars = qalign(o, 8); o = L.bars + 4 * sizeof(unsigned long long);
     L.total = o + 1024;

@@ -41,7 +41,9 @@ __device__ __forceinline__ int swz(int c, int p) {
 
 // Prologue: p-cell centres of the species, barriers, and for BGK the
 // Maxwellian of the stage input per q-cell with exp tables stored as float2
-// over q-cell pairs (cells 2j, 2j+1 of one tile row): tab[(row*4 + j)*ntab + q].
+// over q-cell pairs P = row*4 + j (cells 2j, 2j+1 of one tile row):
+// tab[q*kTabPitch + P], the pitch of 33 pairs keeping a warp's reads of
+// different q (one per lane) on distinct banks.
 template <bool BGK>
 __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i0, int j0,
                                                double* vgrid, double* qc, float2* tabs,
@@ -73,9 +75,9 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
     if (BGK) {
         const double m = a.sg.mass[s];
         for (int e = tid; e < 32 * ntab; e += NTHREADS) {
-            const int P = e / ntab, q = e - P * ntab;
+            const int q = e >> 5, P = e & 31;
             const int c0 = (P >> 2) * 8 + 2 * (P & 3);
-            tabs[e] = make_float2(float(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
+            tabs[q * kTabPitch + P] = make_float2(float(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
                                   float(bgk_table_entry(a, qc + (c0 + 1) * 5, vgrid, q, m)));
         }
     }
@@ -187,7 +189,24 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const int sw1 = swz(b_col + 1, lane) - (b_col + 1) * PW;
     const float4* c_src0 = reinterpret_cast<const float4*>(o1s + pc_c * PW) + ((2 * pc_q) ^ (pc_c & 7));
     const float4* c_src1 = reinterpret_cast<const float4*>(o1s + pc_c * PW) + ((2 * pc_q + 1) ^ (pc_c & 7));
-    const float2* tb_row = tabs + (b_r0 * 4 + rp) * ntab;
+    const float2* tb_row = tabs + b_r0 * 4 + rp;           // pair of row b_r0, cols b_col..+1
+
+    // periodic ghost images (border CTAs): offsets of column `warp` of the
+    // tile, the q1 image shift g_d1, and the rows [0, g_bot) with a q2 image
+    // at +N_q2 and [g_top, TQ) with one at -N_q2 (element offsets)
+    int g_src = 0, g_dst = 0, g_d1 = 0, g_d2 = 0, g_bot = 0, g_top = TQ;
+    if (border) {
+        const int ii = i0 + warp;
+        g_src = swz(warp, lane);                           // row r adds r*TQ*PW
+        g_dst = (j0 + Ng) * (int)colstride + (ii + Ng) * (int)rowstride + xs + lane;
+        if (a.periodic1)
+            g_d1 = ii < Ng ? Nq1 * (int)rowstride : (ii >= Nq1 - Ng ? -Nq1 * (int)rowstride : 0);
+        if (a.periodic2) {
+            g_d2 = Nq2 * (int)colstride;
+            g_bot = max(0, min(TQ, Ng - j0));
+            g_top = min(TQ, max(0, Nq2 - Ng - j0));
+        }
+    }
 
     unsigned phx0 = 0u, phx1 = 0u, phb0 = 0u, phb1 = 0u;
     int buf = 0;
@@ -260,9 +279,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             const float* bb1 = b1s + buf * (kPairTile / 4) + cb0 * PW + lane;
             float* ob1 = o1s + cb0 * PW;
             float* ob2 = o2s + cb0 * PW + lane;
-            const float2* t1 = tb_row + ip1;
-            const float2* t2 = tb_row + Np1 + ip2;
-            const float2* t3 = tb_row + Np1 + Np2 + ip3;
+            const float2* t1 = tb_row + ip1 * kTabPitch;
+            const float2* t2 = tb_row + (Np1 + ip2) * kTabPitch;
+            const float2* t3 = tb_row + (Np1 + Np2 + ip3) * kTabPitch;
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
@@ -273,8 +292,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
                 Fprev = Fn;
                 const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
                 if (BGK) {
-                    const float2 f0 = mul2(mul2(t1[r * 4 * ntab], t2[r * 4 * ntab]),
-                                           t3[r * 4 * ntab]);
+                    const float2 f0 = mul2(mul2(t1[r * 4], t2[r * 4]), t3[r * 4]);
                     kk = fma2(sub2(f0, fcell), inv_tau, kk);
                 }
                 const float2 o1 = fma2(kk, c1, BX ? fcell : make_float2(bb1[r * TQ * PW],
@@ -301,21 +319,25 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         }
 
         // ---- periodic ghost images of border cells, from the staged out1 -------
-        // (2 N_g <= N_q on both axes: at most one image per axis and a corner)
+        // warp w owns tile column w; images along q1 (whole column), along q2
+        // (rows below g_bot and from g_top) and at the corners (2 N_g <= N_q)
         if (border) {
-            const int ii = i0 + warp;                              // warp w owns column w
-            const int d1 = !a.periodic1 ? 0 : (ii < Ng ? Nq1 : (ii >= Nq1 - Ng ? -Nq1 : 0));
-            const int base_c = (Ng * (int)colstride) + (ii + Ng) * (int)rowstride + xs + k * PW + lane;
-#pragma unroll 1
-            for (int r = 0; r < TQ; ++r) {
-                const int jj = j0 + r;
-                const int d2 = !a.periodic2 ? 0 : (jj < Ng ? Nq2 : (jj >= Nq2 - Ng ? -Nq2 : 0));
-                if ((d1 | d2) == 0) continue;
-                const float v = o1s[swz(r * TQ + warp, lane)];
-                const int o = base_c + jj * (int)colstride;
-                if (d1) out1[o + d1 * (int)rowstride] = v;
-                if (d2) out1[o + d2 * (int)colstride] = v;
-                if (d1 && d2) out1[o + d1 * (int)rowstride + d2 * (int)colstride] = v;
+            const float* src = o1s + g_src;
+            float* dst = out1 + (g_dst + k * PW);
+            if (g_d1) {
+#pragma unroll
+                for (int r = 0; r < TQ; ++r)
+                    dst[r * (int)colstride + g_d1] = src[r * TQ * PW];
+            }
+            for (int r = 0; r < g_bot; ++r) {
+                const float v = src[r * TQ * PW];
+                dst[r * (int)colstride + g_d2] = v;
+                if (g_d1) dst[r * (int)colstride + g_d1 + g_d2] = v;
+            }
+            for (int r = g_top; r < TQ; ++r) {
+                const float v = src[r * TQ * PW];
+                dst[r * (int)colstride - g_d2] = v;
+                if (g_d1) dst[r * (int)colstride + g_d1 - g_d2] = v;
             }
         }
 
@@ -367,9 +389,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         }
         return;
     }
-    if (check && nonfinite) atomicOr(a.flag, 1);
     if (tid == 0) bulk_wait_all();
-    __syncthreads();
+    // one flag write per CTA (the flag may live in host memory)
+    if (__syncthreads_or(check && nonfinite) && tid == 0) atomicOr(a.flag, 1);
 
     const long long plane = (long long)Nq2 * Nq1;
     if (want_mom) {
