@@ -296,29 +296,33 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b
 __device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(fast_rcp(a.x), fast_rcp(a.y)); }
 
 // Per-lane coefficients of the upwind side.  With D2_k the second difference
-// and D3 the third difference of the window, the reference's weighted value
-// sum w_k u_k / sum w_k equals u2 + (w1 (u1 - u2) + w3 (u3 - u2)) / sum w_k,
-// where u1 - u2 and u3 - u2 are multiples of the third differences
-// D3a = y0 - 3y1 + 3y2 - y3 = D2_1 - D2_2 and D3b = y1 - 3y2 + 3y3 - y4 = D2_2 - D2_3
-// (right face: 0.375 D3a, 0.125 D3b; left face: -0.125 D3a, -0.375 D3b).
-// The weights are scaled by 16 (w = (1, 10, 5) / 16 right, (5, 10, 1) / 16 left).
+// of substencil k and the third differences D3a = y0 - 3y1 + 3y2 - y3 =
+// D2_1 - D2_2, D3b = y1 - 3y2 + 3y3 - y4 = D2_2 - D2_3, the reference's weighted
+// value sum w_k u_k / sum w_k equals u2 + (w1 (u1 - u2) + w3 (u3 - u2)) / sum w_k
+// with u1 - u2 = k1 D3a, u3 - u2 = k3 D3b (right face: k = 0.375, 0.125;
+// left face: -0.125, -0.375) and u2 = (y2 + ys)/2 - D2_2/8, ys = y3 (right) or
+// y1 (left).  With q_k = 1/beta_k^2 and the weights (1, 10, 5)/16 (right) or
+// (5, 10, 1)/16 (left), the walker returns TWICE the face value as
+//   (y2 + ys - D2_2/4) + (q3 D3b + r q1 D3a) / (a1 q1 + a2 q2 + a3 q3),
+// r = (w1 k1)/(w3 k3) and a_k = w_k / (2 w3 k3); callers halve the flux factor.
 struct Weno5Pair {
-    float2 w1, w3, k1, k3, ua, uc;
-    __device__ __forceinline__ void set(bool right) {
-        w1 = f2(right ? 1.0f : 5.0f);
-        w3 = f2(right ? 5.0f : 1.0f);
-        k1 = f2(right ? 0.375f : -0.625f);     // 16 c1 (u1 - u2) / D3a
-        k3 = f2(right ? 0.625f : -0.375f);     // 16 c3 (u3 - u2) / D3b
-        ua = f2(right ? -0.125f : 0.375f);     // u2 = ua y1 + 0.75 y2 + uc y3
-        uc = f2(right ? 0.375f : -0.125f);
+    float2 r, a1, a2, a3;
+    bool right;
+    __device__ __forceinline__ void set(bool rt) {
+        right = rt;
+        r = f2(rt ? 0.6f : 5.0f / 3.0f);
+        a1 = f2(rt ? 0.8f : -20.0f / 3.0f);
+        a2 = f2(rt ? 8.0f : -40.0f / 3.0f);
+        a3 = f2(rt ? 4.0f : -4.0f / 3.0f);
     }
 };
 
 // smoothness indicator of substencil (a, b, c) given its second difference
-// D2 = a - 2b + c: 13/12 D2^2 + 1/4 (a - 4b + 3c)^2 + 1e-17, a - 4b + 3c = D2 + 2 (c - b)
+// D2 = a - 2b + c: 13/12 D2^2 + 1/4 (a - 4b + 3c)^2 + 1e-17, where
+// (a - 4b + 3c)/2 = D2/2 + (c - b)
 __device__ __forceinline__ float2 beta_pair(float2 D2, float2 b, float2 c) {
-    const float2 e = fma2(f2(2.0f), sub2(c, b), D2);
-    return fma2(mul2(f2(13.0f / 12.0f), D2), D2, fma2(mul2(f2(0.25f), e), e, f2(1e-17f)));
+    const float2 e = fma2(f2(0.5f), D2, sub2(c, b));
+    return fma2(mul2(f2(13.0f / 12.0f), D2), D2, fma2(e, e, f2(1e-17f)));
 }
 
 __device__ __forceinline__ float2 second_diff(float2 a, float2 b, float2 c) {
@@ -333,12 +337,13 @@ struct Weno5PairWalker {
         const float2 r = rcp2(b);
         return mul2(r, r);
     }
-    __device__ __forceinline__ float2 eval(float2 q1, float2 d3a, float2 y1, float2 y2, float2 y3,
-                                           const Weno5Pair& S) const {
-        const float2 u2 = fma2(S.ua, y1, fma2(f2(0.75f), y2, mul2(S.uc, y3)));
-        const float2 num = fma2(mul2(S.k3, q3), d3b, mul2(mul2(S.k1, q1), d3a));
-        const float2 den = fma2(S.w3, q3, fma2(f2(10.0f), q2, mul2(S.w1, q1)));
-        return fma2(num, rcp2(den), u2);
+    __device__ __forceinline__ float2 eval(float2 q1, float2 d3a, float2 d22, float2 y1, float2 y2,
+                                           float2 y3, const Weno5Pair& S) const {
+        const float2 ys = S.right ? y3 : y1;
+        const float2 base = fma2(f2(-0.25f), d22, add2(y2, ys));
+        const float2 num = fma2(q3, d3b, mul2(mul2(S.r, q1), d3a));
+        const float2 den = fma2(S.a3, q3, fma2(S.a2, q2, mul2(S.a1, q1)));
+        return fma2(num, rcp2(den), base);
     }
     __device__ __forceinline__ float2 first(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
                                             const Weno5Pair& S) {
@@ -350,7 +355,7 @@ struct Weno5PairWalker {
         q3 = inv_sq(beta_pair(d23, y3, y4));
         const float2 d3a = sub2(d21, d22);
         d3b = sub2(d22, d23);
-        return eval(q1, d3a, y1, y2, y3, S);
+        return eval(q1, d3a, d22, y1, y2, y3, S);
     }
     // window advanced by one cell: y0..y4 are the new window's values
     __device__ __forceinline__ float2 next(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
@@ -362,7 +367,7 @@ struct Weno5PairWalker {
         d23 = second_diff(y2, y3, y4);
         q3 = inv_sq(beta_pair(d23, y3, y4));
         d3b = sub2(d22, d23);
-        return eval(q1, d3a, y1, y2, y3, S);
+        return eval(q1, d3a, d22, y1, y2, y3, S);
     }
 };
 

@@ -172,14 +172,12 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         const int p = k_begin * PW + lane;
         ip1 = p % Np1; ip2 = (p / Np1) % Np2; ip3 = p / (Np1 * Np2);
     }
-    // phase C: q-cell pc_c, p = k*32 + 8*pc_q .. +7 (one p1 row: N_p1 % 8 == 0)
-    const int pc_c = tid % NQ, pc_q = tid / NQ;
-    int g1, g2, g3;
-    {
-        const int p = k_begin * PW + 8 * pc_q;
-        g1 = p % Np1; g2 = (p / Np1) % Np2; g3 = p / (Np1 * Np2);
-    }
+    // phase C: q-cell pc_c = (row warp, col lane%8), p = k*32 + 8*pc_q .. +7
+    // with pc_q = lane/8: the group holds the lane's own p and lies in one p1
+    // row (N_p1 % 8 == 0), so its velocities follow from the lane's
+    const int pc_c = warp * TQ + (lane & 7), pc_q = lane >> 3;
     const double dp1 = a.sg.dp1[s];
+    const double t_own = double(lane & 7);
     double macc[kNumMom] = {0, 0, 0, 0, 0};
 
     const int rp = warp & 3, seg = warp >> 2;
@@ -233,7 +231,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             float2 y3 = make_float2(ra[3 * PW], rb[3 * PW]);
             float2 y4 = make_float2(ra[4 * PW], rb[4 * PW]);
             Weno5PairWalker W;
-            const float2 vq = f2(v1 * inv_dq1);
+            const float2 vq = f2(0.5f * v1 * inv_dq1);   // walker returns 2x face value
             float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
             float* da = d1s + (a_row * TQ + a_c0) * PW + lane;
 #pragma unroll
@@ -272,7 +270,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             float2 y3 = make_float2(ca[3 * HX * PW], cb[3 * HX * PW]);
             float2 y4 = make_float2(ca[4 * HX * PW], cb[4 * HX * PW]);
             Weno5PairWalker W;
-            const float2 vq = f2(v2 * inv_dq2);
+            const float2 vq = f2(0.5f * v2 * inv_dq2);   // walker returns 2x face value
             float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
             const int cb0 = b_r0 * TQ + b_col;                   // q-cell of row 0, col b_col
             const float* dk = d1s + cb0 * PW + lane;
@@ -355,7 +353,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             const double S2 = fma(49.0, o7, fma(36.0, o6, fma(25.0, o5, fma(16.0, o4,
                               fma(9.0, o3, fma(4.0, o2, o1))))));
             nonfinite |= !isfinite(S0);
-            const double W1 = vgrid[g1], W2 = vgrid[Np1 + g2], W3 = vgrid[Np1 + Np2 + g3];
+            const double W1 = fma(-t_own, dp1, V1), W2 = V2, W3 = vgrid[Np1 + Np2 + ip3];
             macc[0] += S0;
             macc[1] = fma(W1, S0, fma(dp1, S1, macc[1]));
             macc[2] = fma(W2, S0, macc[2]);
@@ -369,11 +367,6 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         while (ip1 >= Np1) {
             ip1 -= Np1;
             if (++ip2 == Np2) { ip2 = 0; ++ip3; }
-        }
-        g1 += PW;
-        while (g1 >= Np1) {
-            g1 -= Np1;
-            if (++g2 == Np2) { g2 = 0; ++g3; }
         }
     }
     if (failed) {
