@@ -37,6 +37,11 @@ sys.path.insert(0, ROOT)
 METRIC = 'cell-updates/s WENO5+LLF RK4: FP64 plain vs FP32/batched/adjoint; % HBM roofline'
 UNIT = 'cell-updates/s'
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per stage launch of
+# the FP32 workload, averaged over the four RK4 stage kernels of one step:
+# measured by ncu on the 64x64 x 24^3 case (959.0 MB per launch) and scaled by
+# the 4x cells of 128x128 x 24^3
+TRAFFIC_FP32_PER_LAUNCH = 3.836e9
 
 
 def workload_spec(small=False):
@@ -215,6 +220,26 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x, world):
+    """The maximum of a per-rank float over all ranks (every rank gets it).
+    NCCL reduces on the device, gloo (CPU tests of the multi-rank path) on the
+    host."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = 'cuda' if dist.get_backend() == 'nccl' else 'cpu'
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(cells_per_rank, world, ms_max):
+    """Whole-job cell-updates/s: every rank advances its own replica of the
+    workload, the slowest rank's time per step bounds the job."""
+    return cells_per_rank * world / (ms_max * 1e-3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -243,12 +268,10 @@ def run_ours(args, rank, world, local_rank):
     ms = ev0.elapsed_time(ev1) / args.steps
     launches = nls.launch_count() - launches0
     torch.cuda.synchronize()
+    ms = max_over_ranks(ms, world)
     if world > 1:
-        t = torch.tensor([ms], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = cells * world / (ms * 1e-3)
+    value = job_value(cells, world, ms)
 
     # end-to-end through the public API with host buffers: every step copies
     # f from pinned host memory, steps, and copies the result back
@@ -269,12 +292,9 @@ def run_ours(args, rank, world, local_rank):
     e1.record()
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, world)
     fbytes = host_in.numel() * host_in.element_size()
-    e2e = {'value': cells * world / (e2e_ms * 1e-3), 'unit': UNIT,
+    e2e = {'value': job_value(cells, world, e2e_ms), 'unit': UNIT,
            'h2d_bytes_per_step': fbytes, 'd2h_bytes_per_step': fbytes}
 
     # FP64 plain form of the same workload (reported beside the FP32 number)
@@ -293,27 +313,32 @@ def run_ours(args, rank, world, local_rank):
             nls64.strang_timestep(dt)
         a1.record()
         a1.synchronize()
-        ms64 = a0.elapsed_time(a1) / n64
-        if world > 1:
-            t = torch.tensor([ms64], device='cuda')
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms64 = float(t.item())
-        fp64 = {'value': cells * world / (ms64 * 1e-3), 'ms_per_step': ms64,
-                'bytes_per_cell_update': 128}
+        ms64 = max_over_ranks(a0.elapsed_time(a1) / n64, world)
+        fp64 = {'value': job_value(cells, world, ms64), 'ms_per_step': ms64,
+                'bytes_per_cell_update': 136}
         del nls64
 
     if rank != 0:
         return
     word = 4 if args.precision == 'fp32' else 8
-    alg_bytes_per_update = 16 * word          # RK4, accumulator form, moments fused
+    # algorithmic bytes per cell-update of classic RK4 with the combine and the
+    # moments fused: 3 + 5 + 5 + 4 = 17 words (the stages read/write f, k-stage
+    # inputs and the accumulator); this implementation moves 16 (the last stage
+    # reads the accumulator as its only base)
+    alg_bytes_per_update = 17 * word
     peak, peak_kind = measured_peak()
     launches_per_step = launches / args.steps
-    qstage_per_step = 4.0
+    qstage_per_step = 4.0                      # one fused stage kernel per RK4 stage
     achieved = alg_bytes_per_update * cells / (ms * 1e-3) / 1e9
+    traffic = args.traffic
+    if traffic is None and args.precision == 'fp32' and not args.small:
+        traffic = TRAFFIC_FP32_PER_LAUNCH
     roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                'frac': achieved / peak, 'traffic': args.traffic,
-                'peak_kind': peak_kind, 'kernel': 'qpair_kernel (paired FP32 WENO5 stage, 8x8 q-tile)' if args.precision == 'fp32'
-                else 'qstage_kernel (WENO5, 8x8 q-tile)',
+                'frac': achieved / peak, 'traffic': traffic,
+                'peak_kind': peak_kind,
+                'kernel': 'qpair_kernel (paired FP32 WENO5 RK stage, 8x8 q-tile)'
+                if args.precision == 'fp32' else 'qstage_kernel (WENO5, 8x8 q-tile)',
+                'alg_bytes_per_update': alg_bytes_per_update,
                 'alg_bytes_per_launch': alg_bytes_per_update * cells / qstage_per_step,
                 'avg_launch_ms': ms / qstage_per_step}
     cpu = None
