@@ -101,6 +101,51 @@ def make_solver(spec, precision):
     return nonlinear_solver(physical_system(dom, bc, params, ini, adv, col.BGK, mom))
 
 
+def ragged_sweep(nruns=256, seed=0):
+    """The ragged 1D1V sweep (seed 0, numpy PCG64): N_q1 uniform over
+    {32, 48, ..., 256}, N_p1 over {64, 96, ..., 512}, p1 in [-10, 10],
+    tau and the density amplitude log-uniform in [1e-3, 1e-1], wavenumber
+    k in {1, 2, 3, 4}; dt = 0.5 dq1 / 10 (CFL 0.5 at |p1| = 10)."""
+    rng = np.random.default_rng(seed)
+    runs = []
+    for _ in range(nruns):
+        nq = int(rng.choice(np.arange(32, 257, 16)))
+        npp = int(rng.choice(np.arange(64, 513, 32)))
+        tau = float(10 ** rng.uniform(-3, -1))
+        amp = float(10 ** rng.uniform(-3, -1))
+        k = int(rng.integers(1, 5))
+        runs.append(dict(N_q1=nq, N_p1=npp, tau=tau, amp=amp, k=k, dt=0.5 * (1.0 / nq) / 10.0))
+    return runs
+
+
+def ragged_system(run, precision='fp32', source=True):
+    """Bolt physical_system of one ragged-sweep run: 1D1V, q1 in [0, 1]
+    periodic, p1 in [-10, 10], p2 = p3 = [-0.5, 0.5] with one cell, BGK with
+    the run's tau, f0 = Maxwellian(T = 1) (1 + A cos(2 pi k q1)), WENO5 + LLF,
+    RK4."""
+    import torch
+    from bolt_b200.physical_system import physical_system
+    import bolt_b200.src.nonrelativistic_boltzmann.advection_terms as adv
+    import bolt_b200.src.nonrelativistic_boltzmann.collision_operator as col
+    import bolt_b200.src.nonrelativistic_boltzmann.moments as mom
+    spec = dict(q1_start=0.0, q1_end=1.0, q2_start=0.0, q2_end=1.0, N_q1=run['N_q1'], N_q2=1,
+                N_p1=run['N_p1'], N_p2=1, N_p3=1, N_ghost=3, p1_start=[-10.0], p1_end=[10.0],
+                p2_start=[-0.5], p2_end=[0.5], p3_start=[-0.5], p3_end=[0.5], tau=run['tau'],
+                amp=0.0)
+    dom, bc, params, ini = config_modules(spec, precision)
+    params.p_dim = 1
+    params.source_enabled = source
+    amp, k = run['amp'], run['k']
+
+    def initialize_f(q1, q2, p1, p2, p3, params):
+        m, kB = params.mass, params.boltzmann_constant
+        m = m[0] if isinstance(m, list) else m
+        n = 1 + amp * torch.cos(2 * np.pi * k * q1)
+        return n * (m / (2 * np.pi * kB)) ** 0.5 * torch.exp(-m * p1 ** 2 / (2 * kB))
+    ini.initialize_f = initialize_f
+    return physical_system(dom, bc, params, ini, adv, col.BGK, mom)
+
+
 def interior_cells(spec):
     return spec['N_q1'] * spec['N_q2'] * spec['N_p1'] * spec['N_p2'] * spec['N_p3'] * len(spec['mass'])
 
@@ -370,6 +415,65 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, rank, world, local_rank):
+    """The ragged 1D1V sweep: all runs advanced by BatchSolver (one launch per
+    RK stage over the packed runs, the steps replayed as one CUDA graph)
+    against the same runs advanced one after another by nonlinear_solver
+    (sequential plain runs, same FP32 f + FP64 moments), both timed with CUDA
+    events; value = total cell-updates/s of the batch."""
+    import torch
+    from bolt_b200.batch import BatchSolver
+    from bolt_b200.nonlinear_solver import nonlinear_solver
+    torch.cuda.set_device(local_rank)
+    runs = ragged_sweep(args.batch_runs)
+    nsteps = args.batch_steps
+    cells = sum(r['N_q1'] * r['N_p1'] for r in runs)
+    bs = BatchSolver([ragged_system(r) for r in runs], [r['dt'] for r in runs])
+    bs.run(nsteps)                       # warm-up: captures and instantiates the graph
+    bs.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    bs.run(nsteps)
+    e1.record()
+    e1.synchronize()
+    t_batch = e0.elapsed_time(e1) * 1e-3
+    bs.synchronize()
+    del bs
+    # sequential plain runs: each run constructed, then nsteps strang_timestep calls timed
+    t_seq = 0.0
+    for r in runs:
+        nls = nonlinear_solver(ragged_system(r))
+        for _ in range(2):
+            nls.strang_timestep(r['dt'])
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(nsteps):
+            nls.strang_timestep(r['dt'])
+        e1.record()
+        e1.synchronize()
+        t_seq += e0.elapsed_time(e1) * 1e-3
+        del nls
+    t_batch = max_over_ranks(t_batch, world)
+    t_seq = max_over_ranks(t_seq, world)
+    if rank != 0:
+        return
+    value = job_value(cells * nsteps, world, t_batch * 1e3)
+    seq = job_value(cells * nsteps, world, t_seq * 1e3)
+    line = {
+        'metric': 'cell-updates/s ragged 1D1V batch (one launch per RK stage, CUDA graph) '
+                  'vs sequential plain runs', 'value': value, 'unit': UNIT,
+        'n_gpus': world, 'steps': nsteps, 'higher_is_better': True, 'scaling': 'weak',
+        'dtype': 'f32', 'data': 'synthetic',
+        'config': {'workload': '%d ragged 1D1V runs (seed 0): N_q1 in {32..256}, N_p1 in '
+                               '{64..512}, tau, amplitude log-uniform [1e-3, 1e-1], k in 1..4, '
+                               'WENO5+LLF, RK4, dt = 0.5 dq1/10, FP32 f + FP64 moments'
+                               % len(runs), 'cells': cells, 'runs': len(runs)},
+        'batch_s': t_batch, 'sequential_s': t_seq, 'sequential_value': seq,
+        'speedup_vs_sequential': t_seq / t_batch,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -380,6 +484,10 @@ def main():
     ap.add_argument('--small', action='store_true', help='64x64 x 24^3 (profiling size)')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-fp64', action='store_true')
+    ap.add_argument('--workload', default='c3', choices=['c3', 'ragged-batch'],
+                    help='c3: the 128^2 x 24^3 headline; ragged-batch: the 1D1V sweep')
+    ap.add_argument('--batch-runs', type=int, default=256)
+    ap.add_argument('--batch-steps', type=int, default=200)
     ap.add_argument('--traffic', type=float, default=None,
                     help='ncu dram bytes per launch of the dominant kernel (recorded in roofline)')
     args = ap.parse_args()
@@ -396,7 +504,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == 'ragged-batch':
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -55,6 +55,16 @@ class BoltParams(ctypes.Structure):
                 ('eps', ctypes.c_double), ('mu', ctypes.c_double)]
 
 
+class BoltBatchRun(ctypes.Structure):
+    _fields_ = [('N_q1', ctypes.c_int), ('N_p1', ctypes.c_int),
+                ('q1_start', ctypes.c_double), ('q1_end', ctypes.c_double),
+                ('p1_start', ctypes.c_double), ('p1_end', ctypes.c_double),
+                ('p2_center', ctypes.c_double), ('p3_center', ctypes.c_double),
+                ('dp2', ctypes.c_double), ('dp3', ctypes.c_double),
+                ('mass', ctypes.c_double), ('boltzmann_constant', ctypes.c_double),
+                ('tau', ctypes.c_double), ('dt', ctypes.c_double)]
+
+
 # exported symbol -> (restype, argtypes); every function of include/bolt_b200.h
 _VP = ctypes.c_void_p
 SIGNATURES = {
@@ -81,6 +91,18 @@ SIGNATURES = {
     'bolt_scratch_bytes': (ctypes.c_size_t, [_VP]),
     'bolt_dfdt_noalloc': (ctypes.c_int, [ctypes.POINTER(BoltGrid), ctypes.POINTER(BoltParams),
                                          _VP, _VP, _VP]),
+    'bolt_batch_create': (ctypes.c_int, [ctypes.POINTER(BoltBatchRun), ctypes.c_int,
+                                         ctypes.c_int, ctypes.POINTER(_VP)]),
+    'bolt_batch_destroy': (None, [_VP]),
+    'bolt_batch_f': (_VP, [_VP]),
+    'bolt_batch_f_count': (ctypes.c_longlong, [_VP]),
+    'bolt_batch_f_offset': (ctypes.c_longlong, [_VP, ctypes.c_int]),
+    'bolt_batch_q_offset': (ctypes.c_int, [_VP, ctypes.c_int]),
+    'bolt_batch_q_count': (ctypes.c_int, [_VP]),
+    'bolt_batch_prepare': (ctypes.c_int, [_VP, _VP]),
+    'bolt_batch_run': (ctypes.c_int, [_VP, ctypes.c_int, _VP]),
+    'bolt_batch_moments': (ctypes.c_int, [_VP, _VP, _VP]),
+    'bolt_batch_divergence_flag': (ctypes.c_int, [_VP]),
 }
 
 NOALLOC_MAX_QCELLS = 65536

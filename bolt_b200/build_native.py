@@ -25,6 +25,7 @@ UNITS = [
     ('kernels_f32.cu', ['-prec-div=false', '-prec-sqrt=false', '-ftz=true']),
     ('bolt_capi.cu', []),
     ('bolt_noalloc.cu', []),
+    ('bolt_batch.cu', ['-prec-div=false', '-prec-sqrt=false', '-ftz=true']),
 ]
 
 

@@ -184,6 +184,53 @@ long long bolt_launch_count(BoltCtx* ctx);
 /* Bytes of device scratch held by the context. */
 size_t bolt_scratch_bytes(BoltCtx* ctx);
 
+/* ------------------------------------------------------------------------
+ * Ragged batch of independent 1D1V runs.  No reference counterpart: Bolt
+ * advances one system per nonlinear_solver (nonlinear_solver.py:67,
+ * timestep.py:101-160); a sweep is a loop of such runs.  Here every run keeps
+ * Bolt's 1D1V setup (q1 periodic, N_q2 = N_p2 = N_p3 = 1, p_dim = 1, one
+ * species, fields off, WENO5 + upwind/LLF in q1, BGK with a constant tau,
+ * RK4 as in bolt_step) with its own N_q1, N_p1, ranges, tau and dt, and all
+ * runs advance together: FP32 f with FP64 moments, one launch per RK stage
+ * over the packed runs, nsteps steps replayed as one CUDA graph.
+ * Layout: run r's ghosted f is N_q1 + 6 rows (q1, N_ghost = 3) of N_p1 FP32
+ * values (p1 fastest) at element bolt_batch_f_offset(r) of bolt_batch_f();
+ * moment sums are 5 doubles (n, mom_v1..3, energy, raw sums over p without
+ * the p-cell measure) per q-cell at q-cell bolt_batch_q_offset(r).
+ * ------------------------------------------------------------------------ */
+typedef struct BoltBatchRun {
+    int N_q1, N_p1;               /* N_q1 % 4 == 0 and >= 6; N_p1 % 32 == 0 */
+    double q1_start, q1_end;      /* periodic q1 domain (domain.q1_start/_end) */
+    double p1_start, p1_end;      /* domain.p1_start/_end */
+    double p2_center, p3_center;  /* centre of the single p2 / p3 cell */
+    double dp2, dp3;              /* width of that cell (the p-cell measure) */
+    double mass, boltzmann_constant, tau, dt;
+} BoltBatchRun;
+
+typedef struct BoltBatch BoltBatch;
+
+/* Allocate the packed buffers and the work queue.  BOLT_ERR_UNSUPPORTED for
+ * shapes outside the batch kernel (N_q1 % 4, N_p1 % 32), BOLT_ERR_ARG for
+ * invalid ranges or constants. */
+int  bolt_batch_create(const BoltBatchRun* runs, int nruns, int source_enabled,
+                       BoltBatch** out);
+void bolt_batch_destroy(BoltBatch* b);
+void* bolt_batch_f(BoltBatch* b);                          /* packed f, device */
+long long bolt_batch_f_count(const BoltBatch* b);          /* elements of packed f */
+long long bolt_batch_f_offset(const BoltBatch* b, int run);
+int  bolt_batch_q_offset(const BoltBatch* b, int run);
+int  bolt_batch_q_count(const BoltBatch* b);
+/* After f is written: periodic ghosts of every run (communicate_f +
+ * apply_bcs_f) and the moments of f. */
+int  bolt_batch_prepare(BoltBatch* b, void* stream);
+/* nsteps RK4 steps of every run on the stream (a CUDA graph of 4 stage
+ * launches per step, captured on first use for this nsteps). */
+int  bolt_batch_run(BoltBatch* b, int nsteps, void* stream);
+/* Copy the moment sums of the current f ([q-cell][5] doubles) to out_dev. */
+int  bolt_batch_moments(BoltBatch* b, double* out_dev, void* stream);
+/* 1 once a stage produced a non-finite value (cleared by the call). */
+int  bolt_batch_divergence_flag(BoltBatch* b);
+
 #ifdef __cplusplus
 }
 #endif

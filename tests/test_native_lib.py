@@ -48,3 +48,29 @@ def test_ctx_create_rejects_bad_grids_without_gpu():
     g.N_q1 = 0          # invalid
     ctx = ctypes.c_void_p()
     assert lib.bolt_ctx_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(ctx)) == N.BOLT_ERR_ARG
+
+
+def test_batch_run_layout_and_validation_without_gpu():
+    lib = N.load()
+    # BoltBatchRun: 2 ints, 12 doubles
+    assert ctypes.sizeof(N.BoltBatchRun) == 2 * 4 + 12 * 8
+    runs = (N.BoltBatchRun * 1)()
+    R = runs[0]
+    R.N_q1, R.N_p1 = 32, 64
+    R.q1_start, R.q1_end, R.p1_start, R.p1_end = 0.0, 1.0, -10.0, 10.0
+    R.dp2 = R.dp3 = 1.0
+    R.mass = R.boltzmann_constant = 1.0
+    R.tau, R.dt = 0.01, 1e-3
+    b = ctypes.c_void_p()
+    # shapes outside the batch kernel and invalid constants are refused before any CUDA call
+    R.N_q1 = 30
+    assert lib.bolt_batch_create(runs, 1, 1, ctypes.byref(b)) == N.BOLT_ERR_UNSUPPORTED
+    R.N_q1, R.N_p1 = 32, 48
+    assert lib.bolt_batch_create(runs, 1, 1, ctypes.byref(b)) == N.BOLT_ERR_UNSUPPORTED
+    R.N_p1, R.dt = 64, 0.0
+    assert lib.bolt_batch_create(runs, 1, 1, ctypes.byref(b)) == N.BOLT_ERR_ARG
+    R.dt, R.tau = 1e-3, 0.0
+    assert lib.bolt_batch_create(runs, 1, 1, ctypes.byref(b)) == N.BOLT_ERR_ARG
+    assert lib.bolt_batch_create(runs, 0, 1, ctypes.byref(b)) == N.BOLT_ERR_ARG
+    assert lib.bolt_batch_run(None, 1, None) == N.BOLT_ERR_ARG
+    assert lib.bolt_batch_f_offset(None, 0) == -1
