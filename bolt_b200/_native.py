@@ -65,6 +65,15 @@ class BoltBatchRun(ctypes.Structure):
                 ('tau', ctypes.c_double), ('dt', ctypes.c_double)]
 
 
+class BoltAdj1DSpec(ctypes.Structure):
+    _fields_ = [('N_q1', ctypes.c_int), ('N_p1', ctypes.c_int),
+                ('q1_start', ctypes.c_double), ('q1_end', ctypes.c_double),
+                ('p1_start', ctypes.c_double), ('p1_end', ctypes.c_double),
+                ('dp2', ctypes.c_double), ('dp3', ctypes.c_double),
+                ('mass', ctypes.c_double), ('boltzmann_constant', ctypes.c_double),
+                ('tau', ctypes.c_double), ('dt', ctypes.c_double)]
+
+
 # exported symbol -> (restype, argtypes); every function of include/bolt_b200.h
 _VP = ctypes.c_void_p
 SIGNATURES = {
@@ -103,6 +112,13 @@ SIGNATURES = {
     'bolt_batch_run': (ctypes.c_int, [_VP, ctypes.c_int, _VP]),
     'bolt_batch_moments': (ctypes.c_int, [_VP, _VP, _VP]),
     'bolt_batch_divergence_flag': (ctypes.c_int, [_VP]),
+    'bolt_adj1d_create': (ctypes.c_int, [ctypes.POINTER(BoltAdj1DSpec), ctypes.c_int,
+                                         ctypes.POINTER(_VP)]),
+    'bolt_adj1d_destroy': (None, [_VP]),
+    'bolt_adj1d_set_tau': (ctypes.c_int, [_VP, ctypes.c_double]),
+    'bolt_adj1d_step': (ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    'bolt_adj1d_step_adjoint': (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, _VP, _VP]),
+    'bolt_adj1d_objective': (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
 }
 
 NOALLOC_MAX_QCELLS = 65536

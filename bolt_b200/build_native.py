@@ -26,6 +26,7 @@ UNITS = [
     ('bolt_capi.cu', []),
     ('bolt_noalloc.cu', []),
     ('bolt_batch.cu', ['-prec-div=false', '-prec-sqrt=false', '-ftz=true']),
+    ('bolt_adjoint.cu', []),
 ]
 
 

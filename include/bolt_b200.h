@@ -231,6 +231,45 @@ int  bolt_batch_moments(BoltBatch* b, double* out_dev, void* stream);
 /* 1 once a stage produced a non-finite value (cleared by the call). */
 int  bolt_batch_divergence_flag(BoltBatch* b);
 
+/* ------------------------------------------------------------------------
+ * Adjoint of the 1D1V update.  No reference counterpart: Bolt has no
+ * differentiation.  The forward step is the same scheme as bolt_step for a
+ * 1D1V system (df_dt_fvm.py:56-97 with the WENO5 of weno5.py:4-98 including
+ * its eps (1 + |a| + |b| + |c|), upwind/LLF faces, BGK with p_dim = 1,
+ * RK4 of integrators.py:15-28), on f[N_q1][N_p1] (p1 fastest) with periodic
+ * q1 and no ghost storage.  The adjoint step is hand-written: exact
+ * derivatives of the WENO5 nonlinear weights, of the Maxwellian through the
+ * velocity moments and of tau (see bolt_adj1d_step_adjoint).  Objective:
+ * J = sum over steps n >= 1 of dt |nhat_1(f_n)|^2, nhat_1 the k = 1 Fourier
+ * coefficient (1/N_q1) sum_i n_i exp(-2 pi i x_i / L) of the density.
+ * ------------------------------------------------------------------------ */
+typedef struct BoltAdj1DSpec {
+    int N_q1, N_p1;                /* N_q1 >= 6, N_p1 <= 2048 */
+    double q1_start, q1_end;       /* periodic q1 */
+    double p1_start, p1_end;
+    double dp2, dp3;               /* the single p2 / p3 cell (centred at 0) */
+    double mass, boltzmann_constant;
+    double tau;                    /* BGK collision time; 0 = collisionless */
+    double dt;
+} BoltAdj1DSpec;
+
+typedef struct BoltAdj1D BoltAdj1D;
+
+int  bolt_adj1d_create(const BoltAdj1DSpec* spec, int dtype, BoltAdj1D** out);
+void bolt_adj1d_destroy(BoltAdj1D* c);
+int  bolt_adj1d_set_tau(BoltAdj1D* c, double tau);
+/* One RK4 step of f (device, in place); J_dev (device double, may be null)
+ * += dt |nhat_1(f_new)|^2. */
+int  bolt_adj1d_step(BoltAdj1D* c, void* f, double* J_dev, void* stream);
+/* Adjoint of the step that starts from f_n: lam holds the adjoint of
+ * f_{n+1} on entry and of f_n on return; with objective_at_start != 0 the
+ * objective's term of f_n is added; dtau_dev (device double, may be null)
+ * += this step's contribution to dJ/dtau. */
+int  bolt_adj1d_step_adjoint(BoltAdj1D* c, const void* f_n, void* lam, int objective_at_start,
+                             double* dtau_dev, void* stream);
+/* J_dev += dt |nhat_1(f)|^2; lam (may be null) += its gradient. */
+int  bolt_adj1d_objective(BoltAdj1D* c, const void* f, double* J_dev, void* lam, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
