@@ -474,6 +474,87 @@ def run_batch(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args, rank, world, local_rank):
+    """Config 5: gradients of J = sum_n dt |nhat_1(n)|^2 for 1D1V 128 x 256,
+    p1 in [-10, 10], n = 1 + a cos(2 pi q1) (a = 0.01), Maxwellian T = 1,
+    tau = 0.02, RK4, dt = 2e-4, 2000 steps, binomial checkpointing with 20
+    snapshots; FP32 f with FP64 moments.  Reports the forward and gradient
+    wall times (CUDA events), and checks dJ/dtau and dJ/da against central
+    differences (h = 1e-4, FP64 forward) and dJ/d(f0, tau, a) against FP64
+    autograd of the PyTorch transcription of the reference scheme."""
+    import math
+    import torch
+    from bolt_b200.adjoint import Rollout1D1V, rollout
+    torch.cuda.set_device(local_rank)
+    NQ, NP, P0, P1, TAU, DT, STEPS, AMP = 128, 256, -10.0, 10.0, 0.02, 2e-4, args.adj_steps, 0.01
+    dev = torch.device('cuda', local_rank)
+    x = ((0.5 + torch.arange(NQ, dtype=torch.float64, device=dev)) / NQ)[:, None]
+    v = (P0 + (0.5 + torch.arange(NP, dtype=torch.float64, device=dev)) * (P1 - P0) / NP)[None, :]
+    maxw = torch.exp(-v ** 2 / 2) / math.sqrt(2 * math.pi)
+    f_of = lambda a: (1 + a * torch.cos(2 * math.pi * x)) * maxw
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    out = {}
+    for prec in ('fp32', 'fp64'):
+        r = Rollout1D1V(NQ, NP, P0, P1, DT, TAU, STEPS, snapshots=20, precision=prec)
+        a = torch.tensor(AMP, dtype=torch.float64, device=dev, requires_grad=True)
+        tau = torch.tensor(TAU, dtype=torch.float64, device=dev, requires_grad=True)
+        r.forward(f_of(AMP))                             # warm-up
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record()
+        J = rollout(f_of(a), tau, r)
+        e1.record()
+        J.backward()
+        e2.record()
+        e2.synchronize()
+        gf, _ = r.gradient(f_of(AMP))
+        out[prec] = dict(J=float(J), da=float(a.grad), dtau=float(tau.grad), gf=gf.double(),
+                         fwd_s=e0.elapsed_time(e1) * 1e-3, grad_s=e1.elapsed_time(e2) * 1e-3,
+                         recomputed_steps=r.forward_steps)
+        if prec == 'fp64':
+            h = 1e-4
+            Jf = lambda aa, tt: float(r.forward(f_of(aa), tt)[0])
+            out['fd_da'] = (Jf(AMP * (1 + h), TAU) - Jf(AMP * (1 - h), TAU)) / (2 * AMP * h)
+            out['fd_dtau'] = (Jf(AMP, TAU * (1 + h)) - Jf(AMP, TAU * (1 - h))) / (2 * TAU * h)
+    # FP64 autograd of the transcription (checkpointed every 50 steps)
+    sys.path.insert(0, ROOT)
+    from oracle.bolt_torch import Problem1D1V
+    pr = Problem1D1V(NQ, NP, P0, P1, DT, TAU, device=dev)
+    a = torch.tensor(AMP, dtype=torch.float64, device=dev, requires_grad=True)
+    tau = torch.tensor(TAU, dtype=torch.float64, device=dev, requires_grad=True)
+    f0 = f_of(a)
+    f0.retain_grad()
+    Jt, _ = pr.objective(f0, tau, STEPS, checkpoint_every=50)
+    Jt.backward()
+    rel = lambda x, y: abs(x - y) / abs(y)
+    o32, o64 = out['fp32'], out['fp64']
+    if rank != 0:
+        return
+    line = {
+        'metric': 'adjoint of the 1D1V WENO5+LLF RK4 BGK update: gradient wall time',
+        'value': o32['grad_s'], 'unit': 's', 'higher_is_better': False, 'n_gpus': 1,
+        'steps': STEPS, 'dtype': 'f32', 'data': 'synthetic',
+        'config': {'workload': '1D1V 128 x 256, p1 in [-10, 10], n = 1 + 0.01 cos(2 pi q1), '
+                               'tau = 0.02, dt = 2e-4, %d RK4 steps, J = sum dt |nhat_1|^2, '
+                               '20 snapshots (binomial checkpointing)' % STEPS},
+        'J': o32['J'], 'forward_s': o32['fwd_s'], 'forward_to_gradient': o32['grad_s'] / o32['fwd_s'],
+        'recomputed_steps': o32['recomputed_steps'],
+        'fp64': {'J': o64['J'], 'forward_s': o64['fwd_s'], 'gradient_s': o64['grad_s']},
+        'check': {
+            'dJ_da': {'fp64_adjoint': o64['da'], 'central_difference': out['fd_da'],
+                      'autograd_fp64': float(a.grad), 'fp32_adjoint': o32['da']},
+            'dJ_dtau': {'fp64_adjoint': o64['dtau'], 'central_difference': out['fd_dtau'],
+                        'autograd_fp64': float(tau.grad), 'fp32_adjoint': o32['dtau']},
+            'rel_fp64_vs_fd': {'a': rel(o64['da'], out['fd_da']), 'tau': rel(o64['dtau'], out['fd_dtau'])},
+            'rel_fp64_vs_autograd': {'a': rel(o64['da'], float(a.grad)),
+                                     'tau': rel(o64['dtau'], float(tau.grad)),
+                                     'f0': float((o64['gf'] - f0.grad).norm() / f0.grad.norm())},
+            'rel_fp32_vs_fp64': {'a': rel(o32['da'], o64['da']), 'tau': rel(o32['dtau'], o64['dtau']),
+                                 'f0': float((o32['gf'] - o64['gf']).norm() / o64['gf'].norm())},
+        },
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -484,8 +565,10 @@ def main():
     ap.add_argument('--small', action='store_true', help='64x64 x 24^3 (profiling size)')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-fp64', action='store_true')
-    ap.add_argument('--workload', default='c3', choices=['c3', 'ragged-batch'],
-                    help='c3: the 128^2 x 24^3 headline; ragged-batch: the 1D1V sweep')
+    ap.add_argument('--workload', default='c3', choices=['c3', 'ragged-batch', 'adjoint'],
+                    help='c3: the 128^2 x 24^3 headline; ragged-batch: the 1D1V sweep; '
+                         'adjoint: gradients of the 1D1V density-mode functional')
+    ap.add_argument('--adj-steps', type=int, default=2000)
     ap.add_argument('--batch-runs', type=int, default=256)
     ap.add_argument('--batch-steps', type=int, default=200)
     ap.add_argument('--traffic', type=float, default=None,
@@ -506,6 +589,8 @@ def main():
     try:
         if args.workload == 'ragged-batch':
             run_batch(args, rank, world, local_rank)
+        elif args.workload == 'adjoint':
+            run_adjoint(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:
