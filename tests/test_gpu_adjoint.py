@@ -84,7 +84,7 @@ def test_gradients_match_autograd_of_transcription():
     f02.retain_grad()
     Jt, _ = transcription().objective(f02, tau2, STEPS)
     Jt.backward()
-    assert abs(float(J) - float(Jt.detach())) < 1e-12 * abs(float(Jt.detach()))
+    assert abs(float(J.detach()) - float(Jt.detach())) < 1e-12 * abs(float(Jt.detach()))
     assert abs(g_a - float(a2.grad)) < 1e-9 * abs(float(a2.grad))
     assert abs(g_tau - float(tau2.grad)) < 1e-9 * abs(float(tau2.grad))
     assert float((gf - f02.grad).norm() / f02.grad.norm()) < 1e-9
