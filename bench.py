@@ -555,6 +555,74 @@ def run_adjoint(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def c2_spec():
+    """Config 2: 2D2V on [0,1]^2 periodic, 64 x 64 q, p1, p2 in [-8, 8] with
+    32 x 32, p3 one cell in [-0.5, 0.5], p_dim 2; f0 = n_q exp(-p1^2/4 - p2^2/2)
+    / (2 pi sqrt 2), n_q = 1 + 1e-3 xi_q with xi ~ N(0, 1) per q-cell from
+    numpy.random.default_rng(0); collisionless, electrodynamic FDTD with the
+    fields of the FFT solve of the noise density, charge -1, m = eps = mu =
+    k = 1, WENO5 + LLF, RK4, dt = 5e-4."""
+    sys.path.insert(0, os.path.join(ROOT, 'tests'))
+    sys.path.insert(0, os.path.join(ROOT, 'tests', 'golden'))
+    import cases as C
+    return C.make(N_q1=64, N_q2=64, N_p1=32, N_p2=32, N_p3=1,
+                  p1_start=[-8.0], p1_end=[8.0], p2_start=[-8.0], p2_end=[8.0],
+                  p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0], p_dim=2,
+                  source_enabled=False, fields_enabled=True, dt=5e-4, integrator='RK4',
+                  riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                  init=dict(amp=0.0, noise=1e-3, seed=0, T=[2.0, 1.0, 1.0]))
+
+
+def run_c2(args, rank, world, local_rank):
+    """Config 2, FP64 and FP32 f (FP64 moments): cell-updates/s over the timed
+    steps (CUDA events) and, after all steps, the FP32 error in density,
+    energy and the cell-centred fields against the FP64 run."""
+    import torch
+    spec = c2_spec()                     # also puts the case builders on sys.path
+    from _modules import make_solver as make_case_solver, moments_layout
+    torch.cuda.set_device(local_rank)
+    cells = spec['N_q1'] * spec['N_q2'] * spec['N_p1'] * spec['N_p2']
+    res, state = {}, {}
+    for prec in ('fp64', 'fp32'):
+        nls = make_case_solver(spec, prec)
+        for _ in range(args.warmup):
+            nls.strang_timestep(spec['dt'])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.c2_steps - args.warmup):
+            nls.strang_timestep(spec['dt'])
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / (args.c2_steps - args.warmup)
+        res[prec] = {'value': cells / (ms * 1e-3), 'ms_per_step': ms,
+                     'launches_per_step': None}
+        g = spec['N_ghost']
+        state[prec] = {k: moments_layout(nls.compute_moments(k))[g:-g, g:-g]
+                       for k in ('density', 'energy')}
+        state[prec]['fields'] = nls.fields_solver.cell_centered_EM_fields[:, 0, g:-g, g:-g] \
+            .detach().cpu().numpy()
+        del nls
+        torch.cuda.empty_cache()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    if rank != 0:
+        return
+    line = {
+        'metric': 'cell-updates/s 2D2V FDTD-coupled WENO5+LLF RK4 (config 2), FP32 vs FP64',
+        'value': res['fp32']['value'], 'unit': UNIT, 'n_gpus': 1, 'steps': args.c2_steps,
+        'higher_is_better': True, 'dtype': 'f32', 'data': 'synthetic (seed 0 noise)',
+        'config': {'workload': '2D2V 64^2 x 32^2, FDTD fields, collisionless, dt = 5e-4',
+                   'cells': cells},
+        'fp32': res['fp32'], 'fp64': res['fp64'],
+        'fp32_over_fp64': res['fp32']['value'] / res['fp64']['value'],
+        'fp32_vs_fp64_after_steps': {
+            'density': rel(state['fp32']['density'], state['fp64']['density']),
+            'energy': rel(state['fp32']['energy'], state['fp64']['energy']),
+            'fields': rel(state['fp32']['fields'], state['fp64']['fields'])},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -565,10 +633,11 @@ def main():
     ap.add_argument('--small', action='store_true', help='64x64 x 24^3 (profiling size)')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-fp64', action='store_true')
-    ap.add_argument('--workload', default='c3', choices=['c3', 'ragged-batch', 'adjoint'],
+    ap.add_argument('--workload', default='c3', choices=['c3', 'c2', 'ragged-batch', 'adjoint'],
                     help='c3: the 128^2 x 24^3 headline; ragged-batch: the 1D1V sweep; '
                          'adjoint: gradients of the 1D1V density-mode functional')
     ap.add_argument('--adj-steps', type=int, default=2000)
+    ap.add_argument('--c2-steps', type=int, default=500)
     ap.add_argument('--batch-runs', type=int, default=256)
     ap.add_argument('--batch-steps', type=int, default=200)
     ap.add_argument('--traffic', type=float, default=None,
@@ -591,6 +660,8 @@ def main():
             run_batch(args, rank, world, local_rank)
         elif args.workload == 'adjoint':
             run_adjoint(args, rank, world, local_rank)
+        elif args.workload == 'c2':
+            run_c2(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:
