@@ -283,10 +283,7 @@ struct FaceWalker {
 // sm_100 f32x2 arithmetic.  Both components share the lane's upwind side, so
 // they share the coefficient set.  Smoothness indicators use a constant
 // 1e-17 floor (the reference's 1e-17*(1+|a|+|b|+|c|) differs from it only
-// where f varies by less than FP32 resolves).  The linear weights are folded
-// into the substencil interpolants: value = sum q_k U_k / sum c_k q_k with
-// q_k = 1/beta_k^2 and U_k = c_k u_k, which is the reference's
-// sum w_k u_k / sum w_k (w_k = c_k q_k) reassociated.
+// where f varies by less than FP32 resolves).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
