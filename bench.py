@@ -596,6 +596,70 @@ def c2_spec():
                   init=dict(amp=0.0, noise=1e-3, seed=0, T=[2.0, 1.0, 1.0]))
 
 
+def run_c1(args, rank, world, local_rank):
+    """Config 1 (1D1V 64 x 128, WENO5, RK2, dt = 1e-4, 100 steps, FP64): 8,192
+    cells, so a step is launch-latency bound.  Times 100 steps three ways:
+    Python strang_timestep calls, nls.run(dt, 100) (the C loop of bolt_run),
+    and one replay of a CUDA graph captured around nls.run."""
+    import torch
+    c2_spec()                            # puts the case builders on sys.path
+    import cases as C
+    from _modules import make_solver as make_case_solver
+    torch.cuda.set_device(local_rank)
+    spec = C.CASES['c1_1d1v_weno5_rk2']
+    cells = spec['N_q1'] * spec['N_p1']
+    n, dt = spec['steps'], spec['dt']
+    nls = make_case_solver(spec, 'fp64')
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    res = {}
+    for _ in range(3):
+        nls.strang_timestep(dt)
+    e0, e1 = ev(), ev()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(n):
+        nls.strang_timestep(dt)
+    e1.record()
+    e1.synchronize()
+    res['python_loop_ms_per_step'] = e0.elapsed_time(e1) / n
+    nls.run(dt, n)
+    torch.cuda.synchronize()
+    e0.record()
+    nls.run(dt, n)
+    e1.record()
+    e1.synchronize()
+    res['bolt_run_ms_per_step'] = e0.elapsed_time(e1) / n
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        nls.run(dt, n)                    # warm-up on the capture stream
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g):
+        nls.run(dt, n)
+    g.replay()
+    torch.cuda.synchronize()
+    e0.record()
+    g.replay()
+    e1.record()
+    e1.synchronize()
+    res['cuda_graph_ms_per_step'] = e0.elapsed_time(e1) / n
+    del g
+    if rank != 0:
+        return
+    line = {'metric': 'cell-updates/s 1D1V 64x128 WENO5 RK2 FP64 (config 1), launch-bound',
+            'value': cells / (res['cuda_graph_ms_per_step'] * 1e-3), 'unit': UNIT, 'n_gpus': 1,
+            'steps': n, 'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': 'config 1: 1D1V 64 x 128, n = 1 + 0.01 cos(2 pi q1), tau = '
+                                   '0.01, WENO5, RK2, dt = 1e-4', 'cells': cells},
+            }
+    line.update({k: v for k, v in res.items()})
+    line['python_loop_value'] = cells / (res['python_loop_ms_per_step'] * 1e-3)
+    line['bolt_run_value'] = cells / (res['bolt_run_ms_per_step'] * 1e-3)
+    print(json.dumps(line), flush=True)
+
+
 def run_c2(args, rank, world, local_rank):
     """Config 2, FP64 and FP32 f (FP64 moments): cell-updates/s over the timed
     steps (CUDA events) and, after all steps, the FP32 error in density,
@@ -656,7 +720,7 @@ def main():
     ap.add_argument('--small', action='store_true', help='64x64 x 24^3 (profiling size)')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-fp64', action='store_true')
-    ap.add_argument('--workload', default='c3', choices=['c3', 'c2', 'ragged-batch', 'adjoint'],
+    ap.add_argument('--workload', default='c3', choices=['c3', 'c1', 'c2', 'ragged-batch', 'adjoint'],
                     help='c3: the 128^2 x 24^3 headline; ragged-batch: the 1D1V sweep; '
                          'adjoint: gradients of the 1D1V density-mode functional')
     ap.add_argument('--adj-steps', type=int, default=2000)
@@ -685,6 +749,8 @@ def main():
             run_adjoint(args, rank, world, local_rank)
         elif args.workload == 'c2':
             run_c2(args, rank, world, local_rank)
+        elif args.workload == 'c1':
+            run_c1(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:
