@@ -25,7 +25,7 @@ F64, F32 = 0, 1
 RECON = {'piecewise-constant': 0, 'minmod': 1, 'ppm': 2, 'weno5': 3}
 FLUX = {'upwind-flux': 0, 'upwind': 0, 'lax-friedrichs': 1, 'llf': 1,
         'local-lax-friedrichs': 1}
-BC = {'periodic': 0, 'dirichlet': 1}
+BC = {'periodic': 0, 'dirichlet': 1, 'external': 2}
 RK = {'RK2': 2, 'RK4': 4}
 MOMENT_IDS = {'density': 0, 'mom_v1_bulk': 1, 'mom_v2_bulk': 2, 'mom_v3_bulk': 3,
               'energy': 4, 'energy_q1': 5, 'energy_q2': 6, 'energy_q3': 7,
@@ -87,6 +87,9 @@ SIGNATURES = {
     'bolt_dfdt': (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_double, _VP]),
     'bolt_step': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),
     'bolt_run': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
+    'bolt_stage_count': (ctypes.c_int, [_VP]),
+    'bolt_stage_input': (_VP, [_VP, _VP, ctypes.c_int]),
+    'bolt_stage': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
     'bolt_moments': (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
     'bolt_fields_set': (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     'bolt_fields_get': (ctypes.c_int, [_VP, _VP, _VP, _VP]),
@@ -124,6 +127,16 @@ SIGNATURES = {
 NOALLOC_MAX_QCELLS = 65536
 
 _lib = None
+
+
+class DeviceArray(object):
+    """A device allocation of the library exposed to torch without a copy
+    (torch.as_tensor(DeviceArray(ptr, count, '<f4'), device='cuda'))."""
+
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = {'shape': (int(count),), 'typestr': typestr,
+                                         'data': (int(ptr), False), 'version': 3,
+                                         'strides': None}
 
 
 class BoltError(RuntimeError):

@@ -23,15 +23,6 @@ from .nonlinear_solver import nonlinear_solver, _plugin_ok
 BATCH_MOMENTS = ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy')
 
 
-class _DeviceArray(object):
-    """A device allocation of the library exposed to torch without a copy."""
-
-    def __init__(self, ptr, count, typestr):
-        self.__cuda_array_interface__ = {'shape': (int(count),), 'typestr': typestr,
-                                         'data': (int(ptr), False), 'version': 3,
-                                         'strides': None}
-
-
 class _RunGrid(object):
     """The attributes nonlinear_solver._build_grids reads, for one run."""
 
@@ -125,7 +116,7 @@ class BatchSolver(object):
         self._b = b
         self._runs = runs
         count = self._lib.bolt_batch_f_count(b)
-        self._flat = torch.as_tensor(_DeviceArray(self._lib.bolt_batch_f(b), count, '<f4'),
+        self._flat = torch.as_tensor(N.DeviceArray(self._lib.bolt_batch_f(b), count, '<f4'),
                                      device=self.device)
         self._f_off = [int(self._lib.bolt_batch_f_offset(b, r)) for r in range(self.nruns)]
         self._q_off = [int(self._lib.bolt_batch_q_offset(b, r)) for r in range(self.nruns)]

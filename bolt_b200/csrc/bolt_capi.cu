@@ -177,7 +177,8 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
     if (p.integrator != BOLT_RK2 && p.integrator != BOLT_RK4) return BOLT_ERR_ARG;
     if (p.p_dim < 1 || p.p_dim > 3) return BOLT_ERR_ARG;
     if ((p.bc_q1 != BOLT_BC_PERIODIC && p.bc_q1 != BOLT_BC_DIRICHLET) ||
-        (p.bc_q2 != BOLT_BC_PERIODIC && p.bc_q2 != BOLT_BC_DIRICHLET))
+        (p.bc_q2 != BOLT_BC_PERIODIC && p.bc_q2 != BOLT_BC_DIRICHLET &&
+         p.bc_q2 != BOLT_BC_EXTERNAL))
         return BOLT_ERR_ARG;
     if (p.fields_enabled && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
         return BOLT_ERR_UNSUPPORTED;
@@ -364,6 +365,8 @@ int bolt_status_sync(BoltCtx* ctx, void* stream) {
 static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
     const BoltGrid& g = ctx->g;
     const int dir1 = ctx->p.bc_q1 == BOLT_BC_DIRICHLET, dir2 = ctx->p.bc_q2 == BOLT_BC_DIRICHLET;
+    const int ext2 = ctx->p.bc_q2 == BOLT_BC_EXTERNAL;
+    const int per2 = !dir2 && !ext2;
     if (g.N_ghost == 0) return BOLT_OK;
     if ((dir1 && (!ctx->dirichlet[0] || !ctx->dirichlet[1])) ||
         (dir2 && (!ctx->dirichlet[2] || !ctx->dirichlet[3])))
@@ -372,11 +375,11 @@ static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
     if (ctx->elem == 8)
         e = launch_ghost_f64(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
                              ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
-                             g.N_p1, g.N_p2, !dir1, !dir2, dir1, dir2, ctx->sg, st);
+                             g.N_p1, g.N_p2, !dir1, per2, dir1, dir2, ext2, ctx->sg, st);
     else
         e = launch_ghost_f32(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
                              ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
-                             g.N_p1, g.N_p2, !dir1, !dir2, dir1, dir2, ctx->sg, st);
+                             g.N_p1, g.N_p2, !dir1, per2, dir1, dir2, ext2, ctx->sg, st);
     ctx->launches++;
     CK(e);
     return BOLT_OK;
@@ -577,36 +580,49 @@ static int ensure_state(BoltCtx* ctx, void* f, cudaStream_t st) {
     return rc;
 }
 
-static int step_once(BoltCtx* ctx, void* f, double dt, cudaStream_t st) {
-    int rc = ensure_state(ctx, f, st);
-    if (rc) return rc;
+// Stage k of one step of f (RK2: k = 0, 1; RK4: k = 0..3, in order).  Stage
+// k reads the moments written by stage k-1 (the ping-pong pair momP flips
+// every stage, so after a whole step the moments of the new f are back in
+// momP[cur_mom]); the last stage finalises the bookkeeping.
+static int stage_count(const BoltCtx* ctx) { return ctx->p.integrator == BOLT_RK2 ? 2 : 4; }
+
+static void* stage_input(BoltCtx* ctx, void* f, int k) {
+    if (k == 0) return f;
+    if (ctx->p.integrator == BOLT_RK2) return ctx->buf[0];
+    return k == 2 ? ctx->buf[1] : ctx->buf[0];
+}
+
+static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st) {
+    int rc = BOLT_OK;
+    if (k == 0) {
+        rc = ensure_state(ctx, f, st);
+        if (rc) return rc;
+    }
     const int dir = ctx->p.bc_q1 == BOLT_BC_DIRICHLET || ctx->p.bc_q2 == BOLT_BC_DIRICHLET;
     const int fe = ctx->p.fields_enabled;
     const int mo_split = fe ? 1 : ctx->nsplit;     // nsplit of partials written by a stage
-    double* mcur = ctx->momP[ctx->cur_mom];
-    double* mnxt = ctx->momP[ctx->cur_mom ^ 1];
-    int nin = ctx->cur_nsplit;
+    double* m_in = ctx->momP[ctx->cur_mom ^ (k & 1)];
+    double* m_out = ctx->momP[ctx->cur_mom ^ (k & 1) ^ 1];
+    const int nin = k == 0 ? ctx->cur_nsplit : mo_split;
     StageIO io;
     memset(&io, 0, sizeof(io));
+    io.mom_in = m_in;
+    io.nsplit_in = nin;
+    io.mom_out = ctx->bgk ? m_out : nullptr;
+    const int last = k == stage_count(ctx) - 1;
+    io.flag = last ? ctx->dflag : nullptr;
+    void* out1;
+    int ev;
     if (ctx->p.integrator == BOLT_RK2) {
         // fvm_operator.py:22-33: f_half = f + k1*(dt/2); f = f_initial + k2*dt
         void* A = ctx->buf[0];
-        io.fs = f; io.base1 = f; io.c1 = dt / 2; io.out1 = A;
-        io.mom_in = mcur; io.nsplit_in = nin; io.mom_out = ctx->bgk ? mnxt : nullptr;
-        int ev = fe && !ctx->at_n;
-        rc = run_stage(ctx, io, ev, dt, st);
-        if (fe) ctx->at_n ^= 1;
-        if (!rc && dir) rc = launch_ghosts(ctx, A, st);
-        if (rc) return rc;
-        memset(&io, 0, sizeof(io));
-        io.fs = A; io.base1 = f; io.c1 = dt; io.out1 = f;
-        io.mom_in = mnxt; io.nsplit_in = mo_split; io.mom_out = ctx->bgk ? mcur : nullptr;
-        io.flag = ctx->dflag;
+        io.fs = k == 0 ? f : A;
+        io.base1 = f;
+        io.c1 = k == 0 ? dt / 2 : dt;
+        io.out1 = out1 = k == 0 ? A : f;
         ev = fe && !ctx->at_n;
         rc = run_stage(ctx, io, ev, dt, st);
         if (fe) ctx->at_n ^= 1;
-        if (!rc && dir) rc = launch_ghosts(ctx, f, st);
-        if (rc) return rc;
     } else {
         // classic RK4 (integrators.py:15-28) in accumulator form:
         //   f1 = f + (dt/2) k1, acc = f + (dt/6) k1
@@ -627,26 +643,26 @@ static int step_once(BoltCtx* ctx, void* f, double dt, cudaStream_t st) {
             {B, f, dt, A, C, c_three, C, 0},
             {A, C, c_six, f, nullptr, 0.0, nullptr, 0},
         };
-        double* m_in = mcur;
-        double* m_out = mnxt;
-        for (int k = 0; k < 4; ++k) {
-            memset(&io, 0, sizeof(io));
-            io.fs = stages[k].fs; io.base1 = stages[k].b1; io.c1 = stages[k].c1;
-            io.out1 = stages[k].o1; io.base2 = stages[k].b2; io.c2 = stages[k].c2;
-            io.out2 = stages[k].o2;
-            io.mom_in = m_in; io.nsplit_in = k == 0 ? nin : mo_split;
-            io.mom_out = ctx->bgk ? m_out : nullptr;
-            io.flag = k == 3 ? ctx->dflag : nullptr;
-            rc = run_stage(ctx, io, fe && stages[k].ev, dt, st);
-            if (!rc && dir) rc = launch_ghosts(ctx, stages[k].o1, st);
-            if (rc) return rc;
-            double* tmp = m_in; m_in = m_out; m_out = tmp;
-        }
-        // after 4 swaps m_in (== mcur) holds the moments of the new f
+        io.fs = stages[k].fs; io.base1 = stages[k].b1; io.c1 = stages[k].c1;
+        io.out1 = out1 = stages[k].o1; io.base2 = stages[k].b2; io.c2 = stages[k].c2;
+        io.out2 = stages[k].o2;
+        rc = run_stage(ctx, io, fe && stages[k].ev, dt, st);
     }
-    ctx->cur_nsplit = mo_split;
-    ctx->ghost_owner = f;
-    ctx->mom_owner = ctx->bgk ? f : nullptr;
+    if (!rc && dir) rc = launch_ghosts(ctx, out1, st);
+    if (rc) return rc;
+    if (last) {
+        ctx->cur_nsplit = mo_split;
+        ctx->ghost_owner = f;
+        ctx->mom_owner = ctx->bgk ? f : nullptr;
+    }
+    return BOLT_OK;
+}
+
+static int step_once(BoltCtx* ctx, void* f, double dt, cudaStream_t st) {
+    for (int k = 0; k < stage_count(ctx); ++k) {
+        const int rc = run_rk_stage(ctx, f, dt, k, st);
+        if (rc) return rc;
+    }
     return BOLT_OK;
 }
 
@@ -671,6 +687,18 @@ int bolt_invalidate(BoltCtx* ctx) {
 int bolt_step(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
     if (!ctx || !f_dev) return BOLT_ERR_ARG;
     return step_once(ctx, f_dev, dt, (cudaStream_t)stream);
+}
+
+int bolt_stage_count(BoltCtx* ctx) { return ctx ? stage_count(ctx) : -1; }
+
+void* bolt_stage_input(BoltCtx* ctx, void* f_dev, int k) {
+    if (!ctx || k < 0 || k >= stage_count(ctx)) return nullptr;
+    return stage_input(ctx, f_dev, k);
+}
+
+int bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream) {
+    if (!ctx || !f_dev || k < 0 || k >= stage_count(ctx)) return BOLT_ERR_ARG;
+    return run_rk_stage(ctx, f_dev, dt, k, (cudaStream_t)stream);
 }
 
 int bolt_run(BoltCtx* ctx, void* f_dev, double dt, int n_steps, void* stream) {

@@ -747,7 +747,7 @@ moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int
 template <typename T>
 __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const T* dt,
                              int Nq1, int Nq2, int Ng, int Ns, int Np, int Np1, int Np2,
-                             int per1, int per2, int dir1, int dir2, SpeciesGrid sg,
+                             int per1, int per2, int dir1, int dir2, int ext2, SpeciesGrid sg,
                              long long nghost_cells) {
     const int Nq1g = Nq1 + 2 * Ng;
     const long long rowstride = (long long)Ns * Np;
@@ -774,6 +774,7 @@ __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const 
         }
         const int i = g1 - Ng, j = g2 - Ng;
         const bool in1 = i >= 0 && i < Nq1, in2 = j >= 0 && j < Nq2;
+        if (ext2 && !in2) continue;            // q2 ghost rows belong to the caller
         T v = T(0);
         if ((in1 || per1) && (in2 || per2)) {
             const int si = ((i % Nq1) + Nq1) % Nq1, sj = ((j % Nq2) + Nq2) % Nq2;

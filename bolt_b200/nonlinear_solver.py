@@ -463,6 +463,32 @@ class nonlinear_solver(object):
         self.check_divergence()
         self.time_elapsed += dt * n_steps
 
+    # ---- stage-level stepping (q2 slabs exchange halos between stages) ----------------
+    def stage_count(self):
+        return int(self._lib.bolt_stage_count(self._ctx))
+
+    def stage_input(self, k):
+        """The buffer RK stage k of the next step reads, as a tensor of the
+        storage shape (N_q2 + 2N_g, N_q1 + 2N_g, N_s, N_p) (its ghost rows must
+        be current before stage k runs)."""
+        if k == 0:
+            return self._fstore
+        ptr = self._lib.bolt_stage_input(self._ctx, self._fstore.data_ptr(), int(k))
+        if not ptr:
+            raise ValueError('stage %d of %d' % (k, self.stage_count()))
+        flat = torch.as_tensor(N.DeviceArray(ptr, self._fstore.numel(),
+                                             '<f4' if self.dtype == torch.float32 else '<f8'),
+                               device=self.device)
+        return flat.view(self._store_shape())
+
+    def stage(self, k, dt):
+        """Run RK stage k of the step of f (stages 0 .. stage_count()-1 in
+        order make one strang_timestep, without its time bookkeeping)."""
+        self.dt = dt
+        N.check(self._lib.bolt_stage(self._ctx, self._fstore.data_ptr(), float(dt), int(k),
+                                     self._stream()), 'bolt_stage')
+        self._seen_version = self._fstore._version
+
     def df_dt(self, f=None, evolve_fields=None):
         """df/dt of f (df_dt_fvm.py:33-339) as an AF-ordered tensor.  Ghost
         cells of f are refreshed first (as fvm_operator.py does before every

@@ -62,6 +62,10 @@ extern "C" {
 /* boundary conditions along q1/q2 (boundaries.py:415-577) */
 #define BOLT_BC_PERIODIC  0
 #define BOLT_BC_DIRICHLET 1
+/* q2 only: the ghost rows are supplied by the caller before every stage (a
+ * q2 slab of a larger domain whose neighbours own those rows); the library
+ * reads them and never writes them. */
+#define BOLT_BC_EXTERNAL  2
 
 /* integrators */
 #define BOLT_RK2 2   /* fvm_operator.py:6-35 midpoint */
@@ -137,6 +141,18 @@ int  bolt_step(BoltCtx* ctx, void* f_dev, double dt, void* stream);
 
 /* n_steps RK steps, ghosts refreshed, launched back to back. */
 int  bolt_run(BoltCtx* ctx, void* f_dev, double dt, int n_steps, void* stream);
+
+/* One RK step as separate stages, for callers that must act between stages
+ * (a q2 slab exchanging its BOLT_BC_EXTERNAL ghost rows with the neighbouring
+ * slabs before each stage; fvm_operator.py:22-33 refreshes halos at the same
+ * points).  bolt_stage_count gives 2 (RK2) or 4 (RK4); bolt_stage_input the
+ * device buffer that stage k reads (f for k = 0, a context stage buffer
+ * otherwise; its ghost rows must be current when stage k is launched);
+ * bolt_stage runs stage k of the step of f.  Stages 0..count-1 in order are
+ * one bolt_step. */
+int   bolt_stage_count(BoltCtx* ctx);
+void* bolt_stage_input(BoltCtx* ctx, void* f_dev, int k);
+int   bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream);
 
 /* One moment (BOLT_MOM_*) of f over the whole ghosted grid, FP64, written to
  * out_dev[q2g][q1g][s] (moments.py definitions times dp1*dp2*dp3). */

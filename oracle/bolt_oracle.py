@@ -439,6 +439,9 @@ class Oracle(object):
         self.g = Grid(spec)
         self.f = np.array(f0, dtype=np.float64).reshape(self.g.fshape)
         self.tau = spec.get('tau', 1.0) if tau is None else tau
+        # bc_q2 == 'external': called on every stage input before its halo
+        # refresh, to fill the q2 ghost rows from the neighbouring slabs
+        self.exchange = None
         self.time_elapsed = 0.0
         self.fields = None
         self.dirichlet = {}
@@ -471,6 +474,10 @@ class Oracle(object):
         filled = inner[src2][:, src1]
         mask = ok2[:, None] & ok1[None, :]
         out[mask] = filled[mask]
+        if sp['bc_q2'] == 'external':
+            # a q2 slab: its ghost rows were supplied by the neighbouring slabs
+            out[:Ng] = f[:Ng]
+            out[g.Nq2g - Ng:] = f[g.Nq2g - Ng:]
         # Dirichlet inflow (boundaries.py:147-225): ghost = user value where
         # the q-velocity points into the domain, else keep
         for side in ('left', 'right', 'bottom', 'top'):
@@ -570,12 +577,15 @@ class Oracle(object):
         """One strang_timestep with the FVM in q and p (timestep.py:101-160)."""
         self.dt = dt
         integ = self.spec.get('integrator', 'RK2')
+
+        def refresh(x):
+            return self.refresh(self.exchange(x) if self.exchange else x)
         if integ == 'RK2':
             # fvm_operator.py:6-35
-            self.f = self.refresh(self.f)
+            self.f = refresh(self.f)
             f_initial = self.f
             self.f = self.f + self.dfdt(self.f) * (dt / 2)
-            self.f = self.refresh(self.f)
+            self.f = refresh(self.f)
             self.f = f_initial + self.dfdt(self.f) * dt
         elif integ == 'RK4':
             # integrators.py:15-28 with the refresh of fvm_operator.py before
@@ -583,14 +593,14 @@ class Oracle(object):
             # stage whose input is the first midpoint state (stage 2), with
             # the currents of that state.
             fe = self.fields is not None
-            self.f = self.refresh(self.f)
+            self.f = refresh(self.f)
             f_initial = self.f
             k1 = self.dfdt(self.f, evolve_fields=False if fe else None)
-            x = self.refresh(f_initial + 0.5 * k1 * dt)
+            x = refresh(f_initial + 0.5 * k1 * dt)
             k2 = self.dfdt(x, evolve_fields=True if fe else None)
-            x = self.refresh(f_initial + 0.5 * k2 * dt)
+            x = refresh(f_initial + 0.5 * k2 * dt)
             k3 = self.dfdt(x, evolve_fields=False if fe else None)
-            x = self.refresh(f_initial + k3 * dt)
+            x = refresh(f_initial + k3 * dt)
             k4 = self.dfdt(x, evolve_fields=False if fe else None)
             self.f = f_initial + ((k1 + 2 * k2 + 2 * k3 + k4) / 6) * dt
         else:

@@ -30,7 +30,8 @@ def build_modules(spec, precision='fp64', integrator=None):
             n = ini.get('base', 1.0) * (1 + ini.get('amp', 0.0)
                                         * torch.cos(2 * np.pi * ini.get('k1', 1) * q1)
                                         * torch.cos(2 * np.pi * ini.get('k2', 0) * q2))
-            n = n * (1 + ini.get('noise', 0.0) * noise.to(q1.device))
+            if ini.get('noise', 0.0):
+                n = n * (1 + ini['noise'] * noise.to(q1.device))
             T = ini.get('T', [1.0, 1.0, 1.0])
             u = ini.get('u', [0.0, 0.0, 0.0])
             out = 1.0

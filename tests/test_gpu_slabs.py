@@ -1,0 +1,93 @@
+"""q2 slabs on one GPU: bolt_b200.distributed.SlabSolver against the
+periodic nonlinear_solver on the whole domain.
+
+(a) One slab (world 1, no process group): the halo exchange wraps the slab onto
+itself, so the run is the periodic run with the q2 ghost rows supplied by a
+host-side copy instead of the kernels' periodic images -- equal to the bit.
+(b) Two and four slabs in one process, stepped in lockstep with the halo rows
+copied between their stage buffers before every RK stage (what the send/recv
+exchange does between ranks): interior cells equal the whole-domain run to a
+few ulps (the slabs' FP64 moment partial sums may be split differently over
+p).  The slabs are 8 rows, so FP32 runs the paired kernel with external q2
+ghosts."""
+
+import pytest
+import torch
+
+import cases as C
+from _modules import make_solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _spec(N_q2, integrator):
+    return C.make(N_q1=24, N_q2=N_q2, N_p1=8, N_p2=8, N_p3=4,
+                  p1_start=[-5.0, -3.0], p1_end=[5.0, 3.0], p2_start=[-5.0, -3.0],
+                  p2_end=[5.0, 3.0], p3_start=[-5.0, -3.0], p3_end=[5.0, 3.0],
+                  mass=[1.0, 4.0], charge=[0.0, 0.0], p_dim=3, tau=0.01, dt=1e-3,
+                  steps=4, integrator=integrator,
+                  riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                  init=dict(amp=0.1, k1=1, k2=2, u=[0.2, -0.1, 0.05], T=[1.0, 1.5, 0.8]))
+
+
+def _interior(f, Ng):
+    return f[:, :, Ng:-Ng, Ng:-Ng]
+
+
+def _exchange(slabs, k):
+    """Halo rows between slabs held in one process (periodic over the slabs)."""
+    Ng = slabs[0].Ng
+    xs = [s.stage_input(k) for s in slabs]
+    W, n = len(xs), xs[0].shape[0]
+    bot = [xs[(r - 1) % W][n - 2 * Ng:n - Ng].clone() for r in range(W)]
+    top = [xs[(r + 1) % W][Ng:2 * Ng].clone() for r in range(W)]
+    for r in range(W):
+        xs[r][:Ng].copy_(bot[r])
+        xs[r][n - Ng:].copy_(top[r])
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+@pytest.mark.parametrize('integrator', ['RK4', 'RK2'])
+def test_single_slab_equals_periodic_run(precision, integrator):
+    from bolt_b200.distributed import SlabSolver
+    spec = _spec(16, integrator)
+    whole = make_solver(spec, precision)
+    slab = SlabSolver(whole.physical_system)
+    slab.local.f = whole.f.clone()
+    for _ in range(spec['steps']):
+        whole.strang_timestep(spec['dt'])
+        slab.strang_timestep(spec['dt'])
+    Ng = spec['N_ghost']
+    assert torch.equal(_interior(slab.local.f, Ng), _interior(whole.f, Ng))
+    assert slab.time_elapsed == pytest.approx(whole.time_elapsed)
+
+
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-13), ('fp32', 2e-6)])
+@pytest.mark.parametrize('world,integrator', [(2, 'RK4'), (4, 'RK4'), (2, 'RK2')])
+def test_slabs_in_lockstep_equal_whole_domain(world, integrator, precision, tol):
+    from bolt_b200.distributed import SlabSolver
+    spec = _spec(8 * world, integrator)
+    whole = make_solver(spec, precision)
+    slabs = [SlabSolver(whole.physical_system, slab=(r, world)) for r in range(world)]
+    Ng, n = spec['N_ghost'], 8
+    for r, s in enumerate(slabs):
+        s.local.f = whole.f[:, :, :, r * n:r * n + n + 2 * Ng].clone()
+    dt = spec['dt']
+    for _ in range(spec['steps']):
+        whole.strang_timestep(dt)
+        for s in slabs:
+            s.begin_step()
+        for k in range(slabs[0].stage_count()):
+            _exchange(slabs, k)
+            for s in slabs:
+                s.stage(k, dt)
+        for s in slabs:
+            s.end_step(dt)
+    got = torch.cat([_interior(s.local.f, Ng) for s in slabs], dim=3).double()
+    ref = _interior(whole.f, Ng).double()
+    err = float((got - ref).abs().max() / ref.abs().max())
+    assert err < tol, err
+    # the moments of the slabs, stitched, are the whole domain's
+    m = torch.cat([_interior(s.local.compute_moments('density'), Ng) for s in slabs], dim=3)
+    mref = _interior(whole.compute_moments('density'), Ng)
+    assert float(((m - mref).abs().max() / mref.abs().max())) < tol

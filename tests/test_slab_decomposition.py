@@ -1,0 +1,101 @@
+"""q2-slab decomposition on the CPU with two gloo ranks (127.0.0.1):
+bolt_b200.distributed.exchange_q2_halos fills each slab's ghost rows from the
+neighbouring slabs (periodic over the ranks), and the oracle advanced slab by
+slab -- q2 as 'external', halos exchanged before every RK stage exactly where
+SlabSolver exchanges them -- equals the oracle advanced on the whole domain."""
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(('127.0.0.1', 0))
+        return s.getsockname()[1]
+
+
+def _spec():
+    import cases as C
+    return C.make(N_q1=8, N_q2=16, N_p1=8, N_p2=4, N_p3=4,
+                  p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+                  p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+                  tau=0.05, dt=1e-3, steps=3, integrator='RK4',
+                  riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                  init=dict(amp=0.1, k1=1, k2=2, noise=1e-3, seed=3, u=[0.2, -0.1, 0.05]))
+
+
+def _rank_main(rank, world, port, out):
+    import datetime
+    import sys
+    sys.path[:0] = [ROOT, HERE, os.path.join(HERE, 'golden')]
+    import torch
+    import torch.distributed as dist
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        from bolt_b200.distributed import exchange_q2_halos, slab_of
+        # 1) the exchange itself: rows hold (rank, row) labels
+        Ng, n = 3, 4
+        t = torch.zeros((n + 2 * Ng, 5), dtype=torch.float64)
+        for j in range(n):
+            t[Ng + j] = 100 * rank + j
+        exchange_q2_halos(t, Ng)
+        down, up = (rank - 1) % world, (rank + 1) % world
+        ok_ex = all(float(t[g, 0]) == 100 * down + (n - Ng + g) for g in range(Ng)) and \
+            all(float(t[n + Ng + g, 0]) == 100 * up + g for g in range(Ng))
+        # 2) the oracle advanced slab by slab
+        import cases as C
+        from oracle.bolt_oracle import Oracle
+        spec = _spec()
+        fg = C.initial_f(spec)
+        nloc, lo, hi = slab_of(spec['N_q2'], spec['q2_start'], spec['q2_end'], rank, world)
+        local = dict(spec, N_q2=nloc, q2_start=lo, q2_end=hi, bc_q2='external')
+        f0 = fg[rank * nloc: rank * nloc + nloc + 2 * Ng].copy()
+        o = Oracle(local, f0)
+
+        def exchange(x):
+            x = np.ascontiguousarray(x)
+            exchange_q2_halos(torch.from_numpy(x), Ng)
+            return x
+        o.exchange = exchange
+        for _ in range(spec['steps']):
+            o.step(spec['dt'])
+        out.put((rank, ok_ex, o.f[Ng:Ng + nloc, Ng:-Ng].copy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_slabs_over_two_gloo_ranks_equal_the_whole_domain():
+    import sys
+    sys.path[:0] = [ROOT, HERE, os.path.join(HERE, 'golden')]
+    import cases as C
+    from oracle.bolt_oracle import Oracle
+    world = 2
+    ctx = mp.get_context('spawn')
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted((out.get(timeout=300) for _ in range(world)), key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(r[1] for r in res), 'halo rows'
+    spec = _spec()
+    o = Oracle(spec, C.initial_f(spec))
+    for _ in range(spec['steps']):
+        o.step(spec['dt'])
+    Ng = spec['N_ghost']
+    whole = o.f[Ng:Ng + spec['N_q2'], Ng:-Ng]     # interior cells
+    slabs = np.concatenate([r[2] for r in res], axis=0)
+    assert np.max(np.abs(slabs - whole)) <= 1e-15 * np.max(np.abs(whole))
