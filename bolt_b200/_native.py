@@ -25,7 +25,7 @@ F64, F32 = 0, 1
 RECON = {'piecewise-constant': 0, 'minmod': 1, 'ppm': 2, 'weno5': 3}
 FLUX = {'upwind-flux': 0, 'upwind': 0, 'lax-friedrichs': 1, 'llf': 1,
         'local-lax-friedrichs': 1}
-BC = {'periodic': 0, 'dirichlet': 1, 'external': 2}
+BC = {'periodic': 0, 'dirichlet': 1, 'external': 2, 'mirror': 3, 'mirror+dirichlet': 4}
 RK = {'RK2': 2, 'RK4': 4}
 MOMENT_IDS = {'density': 0, 'mom_v1_bulk': 1, 'mom_v2_bulk': 2, 'mom_v3_bulk': 3,
               'energy': 4, 'energy_q1': 5, 'energy_q2': 6, 'energy_q3': 7,

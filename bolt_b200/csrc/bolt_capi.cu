@@ -98,6 +98,11 @@ struct BoltCtx {
         }                                                 \
     } while (0)
 
+static inline int bc_dirichlet(int bc) {
+    return bc == BOLT_BC_DIRICHLET || bc == BOLT_BC_MIRROR_DIRICHLET;
+}
+static inline int bc_mirror(int bc) { return bc == BOLT_BC_MIRROR || bc == BOLT_BC_MIRROR_DIRICHLET; }
+
 static int dev_alloc(BoltCtx* ctx, void** p, size_t bytes) {
     if (bytes == 0) {
         *p = nullptr;
@@ -176,13 +181,16 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
     if (p.recon_q < 0 || p.recon_q > 3 || p.recon_p < 0 || p.recon_p > 3) return BOLT_ERR_ARG;
     if (p.integrator != BOLT_RK2 && p.integrator != BOLT_RK4) return BOLT_ERR_ARG;
     if (p.p_dim < 1 || p.p_dim > 3) return BOLT_ERR_ARG;
-    if ((p.bc_q1 != BOLT_BC_PERIODIC && p.bc_q1 != BOLT_BC_DIRICHLET) ||
-        (p.bc_q2 != BOLT_BC_PERIODIC && p.bc_q2 != BOLT_BC_DIRICHLET &&
-         p.bc_q2 != BOLT_BC_EXTERNAL))
+    if (p.bc_q1 < BOLT_BC_PERIODIC || p.bc_q1 > BOLT_BC_MIRROR_DIRICHLET ||
+        p.bc_q1 == BOLT_BC_EXTERNAL || p.bc_q2 < BOLT_BC_PERIODIC ||
+        p.bc_q2 > BOLT_BC_MIRROR_DIRICHLET)
         return BOLT_ERR_ARG;
     if (p.fields_enabled && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
         return BOLT_ERR_UNSUPPORTED;
-    if (g.N_ghost == 0 && (p.bc_q1 == BOLT_BC_DIRICHLET || p.bc_q2 == BOLT_BC_DIRICHLET))
+    if (g.N_ghost == 0 && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
+        return BOLT_ERR_UNSUPPORTED;
+    // a mirror image of the ghost zone must lie inside the grid
+    if ((bc_mirror(p.bc_q1) && g.N_ghost > g.N_q1) || (bc_mirror(p.bc_q2) && g.N_ghost > g.N_q2))
         return BOLT_ERR_UNSUPPORTED;
 
     BoltCtx* ctx = new (std::nothrow) BoltCtx;
@@ -364,9 +372,10 @@ int bolt_status_sync(BoltCtx* ctx, void* stream) {
 // ---------------------------------------------------------------------------
 static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
     const BoltGrid& g = ctx->g;
-    const int dir1 = ctx->p.bc_q1 == BOLT_BC_DIRICHLET, dir2 = ctx->p.bc_q2 == BOLT_BC_DIRICHLET;
+    const int dir1 = bc_dirichlet(ctx->p.bc_q1), dir2 = bc_dirichlet(ctx->p.bc_q2);
+    const int mir1 = bc_mirror(ctx->p.bc_q1), mir2 = bc_mirror(ctx->p.bc_q2);
     const int ext2 = ctx->p.bc_q2 == BOLT_BC_EXTERNAL;
-    const int per2 = !dir2 && !ext2;
+    const int per1 = ctx->p.bc_q1 == BOLT_BC_PERIODIC, per2 = ctx->p.bc_q2 == BOLT_BC_PERIODIC;
     if (g.N_ghost == 0) return BOLT_OK;
     if ((dir1 && (!ctx->dirichlet[0] || !ctx->dirichlet[1])) ||
         (dir2 && (!ctx->dirichlet[2] || !ctx->dirichlet[3])))
@@ -375,11 +384,11 @@ static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
     if (ctx->elem == 8)
         e = launch_ghost_f64(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
                              ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
-                             g.N_p1, g.N_p2, !dir1, per2, dir1, dir2, ext2, ctx->sg, st);
+                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext2, ctx->sg, st);
     else
         e = launch_ghost_f32(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
                              ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
-                             g.N_p1, g.N_p2, !dir1, per2, dir1, dir2, ext2, ctx->sg, st);
+                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext2, ctx->sg, st);
     ctx->launches++;
     CK(e);
     return BOLT_OK;
@@ -598,7 +607,10 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         rc = ensure_state(ctx, f, st);
         if (rc) return rc;
     }
-    const int dir = ctx->p.bc_q1 == BOLT_BC_DIRICHLET || ctx->p.bc_q2 == BOLT_BC_DIRICHLET;
+    // the stage kernels write periodic images only; any other q1 / q2
+    // condition (an external q2 excepted) needs the ghost pass after the stage
+    const int dir = ctx->p.bc_q1 != BOLT_BC_PERIODIC ||
+                    (ctx->p.bc_q2 != BOLT_BC_PERIODIC && ctx->p.bc_q2 != BOLT_BC_EXTERNAL);
     const int fe = ctx->p.fields_enabled;
     const int mo_split = fe ? 1 : ctx->nsplit;     // nsplit of partials written by a stage
     double* m_in = ctx->momP[ctx->cur_mom ^ (k & 1)];

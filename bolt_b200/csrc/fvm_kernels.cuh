@@ -11,8 +11,8 @@
 //                   (df_dt_fvm.py:245-323), added to the q-part, then the RK
 //                   combine (used only when fields are enabled).
 //   moments_kernel  compute_moments.py:7-59 for any moment of moments.py.
-//   ghost_kernel    communicate_f + apply_bcs_f (periodic wrap, Dirichlet
-//                   inflow, zero for ghosted outflow cells).
+//   ghost_kernel    communicate_f + apply_bcs_f (periodic wrap, mirror,
+//                   Dirichlet inflow, zero for ghosted outflow cells).
 //   fdtd kernels    fields.py:568-647 / fdtd_explicit.py:9-177 on the Yee grid.
 //
 // Layout: f[q2g][q1g][s][p] with p = (p3, p2, p1) flattened, p1 fastest.
@@ -740,15 +740,20 @@ moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int
 }
 
 // ---------------------------------------------------------------------------
-// halo refresh: communicate_f (periodic wrap; ghosted halos are zero) then
-// apply_bcs_f's Dirichlet inflow selects in the order left, right, bottom,
-// top (boundaries.py:415-577, :147-225).  One thread per (ghost cell, s, p).
+// halo refresh: communicate_f (periodic wrap; ghosted halos are zero), then
+// apply_bcs_f per axis (boundaries.py:415-577): the mirror image
+// (boundaries.py:226-301, cartesian p-grid) and/or the Dirichlet inflow
+// select (:147-225).  One thread per (ghost cell, s, p); every value is read
+// from an interior cell, so one pass gives the reference's sequential
+// left, right, bottom, top result everywhere except in the corner cells
+// (ghost in both q1 and q2) of mixed mirror / Dirichlet axes, which no
+// interior update reads (the q1 and q2 stencils are separate).
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const T* dt,
                              int Nq1, int Nq2, int Ng, int Ns, int Np, int Np1, int Np2,
-                             int per1, int per2, int dir1, int dir2, int ext2, SpeciesGrid sg,
-                             long long nghost_cells) {
+                             int per1, int per2, int dir1, int dir2, int mir1, int mir2,
+                             int ext2, SpeciesGrid sg, long long nghost_cells) {
     const int Nq1g = Nq1 + 2 * Ng;
     const long long rowstride = (long long)Ns * Np;
     const long long colstride = rowstride * Nq1g;
@@ -775,13 +780,37 @@ __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const 
         const int i = g1 - Ng, j = g2 - Ng;
         const bool in1 = i >= 0 && i < Nq1, in2 = j >= 0 && j < Nq2;
         if (ext2 && !in2) continue;            // q2 ghost rows belong to the caller
-        T v = T(0);
-        if ((in1 || per1) && (in2 || per2)) {
-            const int si = ((i % Nq1) + Nq1) % Nq1, sj = ((j % Nq2) + Nq2) % Nq2;
-            v = f[(long long)(sj + Ng) * colstride + (long long)(si + Ng) * rowstride + sp];
-        }
-        const long long g = (long long)g2 * colstride + (long long)g1 * rowstride + sp;
         const int i1 = p % Np1, i2 = (p / Np1) % Np2;
+        // source cell and p index: periodic wrap, or the mirror image across
+        // the edge (ghost i < 0 <- interior -1-i, i >= N <- 2N-1-i) with the
+        // normal velocity index reversed (boundaries.py:226-301)
+        int si = i, sj = j, ps = p;
+        bool have = true;
+        if (!in1) {
+            if (per1) {
+                si = ((i % Nq1) + Nq1) % Nq1;
+            } else if (mir1) {
+                si = i < 0 ? -1 - i : 2 * Nq1 - 1 - i;
+                ps += Np1 - 1 - 2 * i1;
+            } else {
+                have = false;
+            }
+        }
+        if (!in2) {
+            if (per2) {
+                sj = ((j % Nq2) + Nq2) % Nq2;
+            } else if (mir2) {
+                sj = j < 0 ? -1 - j : 2 * Nq2 - 1 - j;
+                ps += Np1 * (Np2 - 1 - 2 * i2);
+            } else {
+                have = false;
+            }
+        }
+        T v = T(0);
+        if (have)
+            v = f[(long long)(sj + Ng) * colstride + (long long)(si + Ng) * rowstride +
+                  (long long)s * Np + ps];
+        const long long g = (long long)g2 * colstride + (long long)g1 * rowstride + sp;
         const double v1 = sg.p1_start[s] + (0.5 + i1) * sg.dp1[s];
         const double v2 = sg.p2_start[s] + (0.5 + i2) * sg.dp2[s];
         if (dir1 && i < 0 && v1 > 0) v = dl[g];

@@ -48,8 +48,8 @@ inline size_t pstage_smem(int Np, size_t elem) { return 4 * (size_t)Np * elem; }
     cudaError_t launch_ghost_##SUFFIX(void* f, const void* dl, const void* dr,               \
                                       const void* db, const void* dt, int Nq1, int Nq2,      \
                                       int Ng, int Ns, int Np, int Np1, int Np2, int per1,    \
-                                      int per2, int dir1, int dir2, int ext2,                \
-                                      const SpeciesGrid& sg,                                 \
+                                      int per2, int dir1, int dir2, int mir1, int mir2,      \
+                                      int ext2, const SpeciesGrid& sg,                       \
                                       cudaStream_t st);
 
 BOLT_DECLARE_LAUNCHERS(f64, double)

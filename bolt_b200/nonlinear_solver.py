@@ -26,6 +26,8 @@ import torch
 from . import _native as N
 
 _PLUGIN_SUFFIX = 'nonrelativistic_boltzmann'
+# conditions whose ghost values take the user's f_left / f_right / f_bottom / f_top
+_DIRICHLET_BCS = ('dirichlet', 'mirror+dirichlet')
 
 
 def _plugin_ok(fn, module_tail, name):
@@ -323,16 +325,19 @@ class nonlinear_solver(object):
             self._refresh_boundaries()
             self._seen_version = v
 
+    def _has_dirichlet(self):
+        return any(b in _DIRICHLET_BCS for b in (self._bc_q1, self._bc_q2))
+
     def _refresh_boundaries(self):
         """Evaluate the Dirichlet boundary functions (boundaries.py:147-225)."""
-        if 'dirichlet' not in (self._bc_q1, self._bc_q2):
+        if not self._has_dirichlet():
             return
         bc = self.boundary_conditions
         args = (self.f, self.time_elapsed, self.q1_center, self.q2_center,
                 self.p1_center, self.p2_center, self.p3_center, self.physical_system.params)
         self._dirichlet = {}
-        sides = ['left', 'right'] if self._bc_q1 == 'dirichlet' else []
-        sides += ['bottom', 'top'] if self._bc_q2 == 'dirichlet' else []
+        sides = ['left', 'right'] if self._bc_q1 in _DIRICHLET_BCS else []
+        sides += ['bottom', 'top'] if self._bc_q2 in _DIRICHLET_BCS else []
         for k, side in enumerate(('left', 'right', 'bottom', 'top')):
             if side not in sides:
                 continue
@@ -415,7 +420,7 @@ class nonlinear_solver(object):
             t0 = torch.cuda.Event(enable_timing=True)
             t1 = torch.cuda.Event(enable_timing=True)
             t0.record()
-        if 'dirichlet' in (self._bc_q1, self._bc_q2):
+        if self._has_dirichlet():
             self._refresh_boundaries()
         N.check(self._lib.bolt_step(self._ctx, self._fstore.data_ptr(), float(dt), self._stream()),
                 'bolt_step')
@@ -453,7 +458,7 @@ class nonlinear_solver(object):
         """n_steps strang steps launched back to back (no per-step host work)."""
         self.dt = dt
         self._sync_external_edits()
-        if 'dirichlet' in (self._bc_q1, self._bc_q2):
+        if self._has_dirichlet():
             for _ in range(n_steps):
                 self._step(dt)
             return

@@ -66,6 +66,13 @@ extern "C" {
  * q2 slab of a larger domain whose neighbours own those rows); the library
  * reads them and never writes them. */
 #define BOLT_BC_EXTERNAL  2
+/* mirror (boundaries.py:226-301, cartesian p-grid): ghost cell i < 0 holds
+ * interior cell -1-i (i >= N: 2N-1-i) with the p-index normal to the edge
+ * reversed (p1 for q1, p2 for q2); needs N_ghost <= N_q along the axis */
+#define BOLT_BC_MIRROR    3
+/* mirror, then the Dirichlet inflow values where the velocity normal to the
+ * edge points into the domain (apply_bcs_f's 'mirror+dirichlet') */
+#define BOLT_BC_MIRROR_DIRICHLET 4
 
 /* integrators */
 #define BOLT_RK2 2   /* fvm_operator.py:6-35 midpoint */

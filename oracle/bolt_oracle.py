@@ -478,12 +478,27 @@ class Oracle(object):
             # a q2 slab: its ghost rows were supplied by the neighbouring slabs
             out[:Ng] = f[:Ng]
             out[g.Nq2g - Ng:] = f[g.Nq2g - Ng:]
-        # Dirichlet inflow (boundaries.py:147-225): ghost = user value where
-        # the q-velocity points into the domain, else keep
+        # apply_bcs_f (boundaries.py:415-577): side by side in the order left,
+        # right, bottom, top, the mirror image (boundaries.py:226-301) and/or
+        # the Dirichlet inflow values (boundaries.py:147-225)
         for side in ('left', 'right', 'bottom', 'top'):
             axis_bc = sp['bc_q1'] if side in ('left', 'right') else sp['bc_q2']
-            if axis_bc != 'dirichlet':
+            if axis_bc in ('mirror', 'mirror+dirichlet'):
+                # ghost cells take the interior cells mirrored across the edge,
+                # with the p-index normal to the edge reversed (p1 for q1 edges,
+                # p2 for q2 edges; axes -1 / -2 of (q2, q1, s, p3, p2, p1))
+                if side == 'left':
+                    out[:, :Ng] = out[:, Ng:2 * Ng][:, ::-1][..., ::-1]
+                elif side == 'right':
+                    out[:, -Ng:] = out[:, -2 * Ng:-Ng][:, ::-1][..., ::-1]
+                elif side == 'bottom':
+                    out[:Ng] = out[Ng:2 * Ng][::-1][..., ::-1, :]
+                else:
+                    out[-Ng:] = out[-2 * Ng:-Ng][::-1][..., ::-1, :]
+            if axis_bc not in ('dirichlet', 'mirror+dirichlet'):
                 continue
+            # Dirichlet inflow: ghost = user value where the q-velocity points
+            # into the domain, else keep
             val = self.dirichlet[side]          # full f-shaped array
             v = g.p1c if side in ('left', 'right') else g.p2c
             v = np.broadcast_to(v[None, None], out.shape)

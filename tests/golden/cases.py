@@ -122,6 +122,24 @@ CASES = {
                        bottom=dict(base=1.1, T=[1.0, 1.0, 1.0], u=[0.0, 0.4, 0]),
                        top=dict(base=0.9, T=[1.0, 1.0, 1.0], u=[0.0, -0.4, 0])),
         init=dict(amp=0.1, k1=1, k2=1)),
+    # mirror walls on both q axes (boundaries.py:226-301), a drifting,
+    # anisotropic 2D2V gas reflecting off them, WENO5, BGK, RK2
+    'mirror_2d2v_weno5': make(
+        N_q1=8, N_q2=8, N_p1=8, N_p2=8, N_p3=1,
+        p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=2,
+        bc_q1='mirror', bc_q2='mirror', tau=0.05, dt=2e-3, steps=4,
+        init=dict(amp=0.1, k1=1, k2=1, u=[0.4, -0.3, 0.0], T=[1.0, 1.5, 1.0])),
+    # mirror + Dirichlet inflow along q1, periodic q2, 2D3V, LLF, RK4
+    'mirror_dirichlet_2d3v_rk4': make(
+        N_q1=8, N_q2=8, N_p1=8, N_p2=4, N_p3=4,
+        p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+        p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+        bc_q1='mirror+dirichlet', tau=0.05, dt=2e-3, steps=3, integrator='RK4',
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+        dirichlet=dict(left=dict(base=1.3, T=[1.0, 1.0, 1.0], u=[0.5, 0.1, 0]),
+                       right=dict(base=0.7, T=[1.5, 1.0, 1.0], u=[-0.4, 0, 0])),
+        init=dict(amp=0.1, k1=1, k2=2, u=[-0.2, 0.3, 0.1])),
     # two species with different masses, charges and p-ranges, fields + BGK
     'two_species_2d2v_fields': make(
         N_q1=6, N_q2=4, N_p1=8, N_p2=6, N_p3=1,

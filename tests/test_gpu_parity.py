@@ -90,7 +90,8 @@ def test_fp64_matches_reference(name):
 @pytest.mark.parametrize('name', ['c1_1d1v_weno5_rk2', 'c1_1d1v_weno5_rk4_llf',
                                   'c3_2d3v_weno5_rk4_small', 'c2_2d2v_fdtd_rk4_small',
                                   'minmod_2d2v_fields_bgk', 'ppm_2d2v_fields_bgk',
-                                  'dirichlet_1d1v_weno5', 'two_species_2d2v_fields'])
+                                  'dirichlet_1d1v_weno5', 'two_species_2d2v_fields',
+                                  'mirror_2d2v_weno5', 'mirror_dirichlet_2d3v_rk4'])
 def test_fp32_close_to_reference(name):
     _check_case(name, 'fp32')
 
@@ -142,6 +143,13 @@ PAIR_CASES = {
                        bottom=dict(base=1.1, T=[1.0, 1.0, 1.0], u=[0.0, 0.4, 0]),
                        top=dict(base=0.9, T=[1.0, 1.0, 1.0], u=[0.0, -0.4, 0])),
         init=dict(amp=0.1, k1=1, k2=1)),
+    'pair_mirror_rk4': C.make(
+        N_q1=16, N_q2=24, N_p1=8, N_p2=4, N_p3=4,
+        p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+        p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+        bc_q1='mirror', bc_q2='mirror', tau=0.02, dt=1e-3, steps=3, integrator='RK4',
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+        init=dict(amp=0.1, k1=1, k2=1, u=[0.5, -0.4, 0.1], T=[1.0, 1.3, 0.9])),
 }
 
 

@@ -50,6 +50,27 @@ def test_ctx_create_rejects_bad_grids_without_gpu():
     assert lib.bolt_ctx_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(ctx)) == N.BOLT_ERR_ARG
 
 
+def test_ctx_create_checks_boundary_conditions_without_gpu():
+    """Boundary codes are validated before any device work: an unknown code or
+    an external q1 is an argument error; a mirror whose ghost zone is deeper
+    than the grid, or a non-periodic axis without ghost cells, is unsupported."""
+    lib = N.load()
+
+    def create(bc_q1, bc_q2, N_q1=8, N_ghost=3):
+        g = N.BoltGrid()
+        g.N_q1, g.N_q2, g.N_ghost, g.N_p1, g.N_p2, g.N_p3, g.N_s = N_q1, 8, N_ghost, 8, 8, 1, 1
+        p = N.BoltParams()
+        p.dtype, p.recon_q, p.recon_p = N.F64, N.RECON['weno5'], N.RECON['weno5']
+        p.integrator, p.p_dim = N.RK['RK2'], 2
+        p.bc_q1, p.bc_q2 = N.BC[bc_q1] if bc_q1 in N.BC else bc_q1, N.BC[bc_q2]
+        ctx = ctypes.c_void_p()
+        return lib.bolt_ctx_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(ctx))
+    assert create(7, 'periodic') == N.BOLT_ERR_ARG
+    assert create('external', 'periodic') == N.BOLT_ERR_ARG
+    assert create('mirror', 'periodic', N_q1=2) == N.BOLT_ERR_UNSUPPORTED
+    assert create('periodic', 'mirror+dirichlet', N_ghost=0) == N.BOLT_ERR_UNSUPPORTED
+
+
 def test_batch_run_layout_and_validation_without_gpu():
     lib = N.load()
     # BoltBatchRun: 2 ints, 12 doubles
