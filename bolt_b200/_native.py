@@ -27,6 +27,7 @@ FLUX = {'upwind-flux': 0, 'upwind': 0, 'lax-friedrichs': 1, 'llf': 1,
         'local-lax-friedrichs': 1}
 BC = {'periodic': 0, 'dirichlet': 1, 'external': 2, 'mirror': 3, 'mirror+dirichlet': 4}
 RK = {'RK2': 2, 'RK4': 4}
+FIELDS = {'electrodynamic': 0, 'electrostatic': 1}
 MOMENT_IDS = {'density': 0, 'mom_v1_bulk': 1, 'mom_v2_bulk': 2, 'mom_v3_bulk': 3,
               'energy': 4, 'energy_q1': 5, 'energy_q2': 6, 'energy_q3': 7,
               'q_q1': 8, 'q_q2': 9, 'q_q3': 10}
@@ -50,6 +51,7 @@ class BoltParams(ctypes.Structure):
                 ('bc_q1', ctypes.c_int), ('bc_q2', ctypes.c_int),
                 ('integrator', ctypes.c_int), ('source_enabled', ctypes.c_int),
                 ('fields_enabled', ctypes.c_int), ('p_dim', ctypes.c_int),
+                ('fields_type', ctypes.c_int),
                 ('mass', _D8), ('charge', _D8),
                 ('boltzmann_constant', ctypes.c_double), ('tau', ctypes.c_double),
                 ('eps', ctypes.c_double), ('mu', ctypes.c_double)]

@@ -27,6 +27,7 @@ UNITS = [
     ('bolt_noalloc.cu', []),
     ('bolt_batch.cu', ['-prec-div=false', '-prec-sqrt=false', '-ftz=true']),
     ('bolt_adjoint.cu', []),
+    ('poisson.cu', ['-fmad=false']),
 ]
 
 
@@ -64,7 +65,7 @@ def build(force=False, verbose=False, ptxas_v=False):
             print(' '.join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [nvcc()] + ARCH + ['-shared', '-o', LIB] + objs
+    cmd = [nvcc()] + ARCH + ['-shared', '-o', LIB] + objs + ['-lcufft']
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)

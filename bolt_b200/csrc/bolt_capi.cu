@@ -74,6 +74,11 @@ struct BoltCtx {
     // fields
     double *cell, *yee, *ebefore, *J;
     int at_n;
+    // electrostatic fields: density partials of the df/dt argument, FFT work
+    // arrays and the cuFFT plans (0 when unused)
+    double* es_part;
+    double2 *es_rho, *es_e;
+    int es_fwd, es_inv;
     // misc
     const void* tau_arr;
     const void* dirichlet[4];
@@ -187,6 +192,9 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
         return BOLT_ERR_ARG;
     if (p.fields_enabled && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
         return BOLT_ERR_UNSUPPORTED;
+    if (p.fields_enabled && p.fields_type != BOLT_FIELDS_ELECTRODYNAMIC &&
+        p.fields_type != BOLT_FIELDS_ELECTROSTATIC)
+        return BOLT_ERR_ARG;
     if (g.N_ghost == 0 && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
         return BOLT_ERR_UNSUPPORTED;
     // a mirror image of the ghost zone must lie inside the grid
@@ -292,6 +300,14 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
             cudaMemset(ctx->cell, 0, 6 * fp * sizeof(double));
             cudaMemset(ctx->yee, 0, 6 * fp * sizeof(double));
         }
+        if (rc == BOLT_OK && p.fields_type == BOLT_FIELDS_ELECTROSTATIC) {
+            const size_t nq = (size_t)g.N_q1 * g.N_q2;
+            rc = dev_alloc(ctx, (void**)&ctx->es_part, kNumMom * plane * sizeof(double));
+            if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->es_rho, nq * sizeof(double2));
+            if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->es_e, 2 * nq * sizeof(double2));
+            if (rc == BOLT_OK && poisson_plans_create(g.N_q1, g.N_q2, &ctx->es_fwd, &ctx->es_inv))
+                rc = BOLT_ERR_CUDA;
+        }
     }
     if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->derr, sizeof(int));
     if (rc == BOLT_OK && cudaMemset(ctx->derr, 0, sizeof(int)) != cudaSuccess) rc = BOLT_ERR_CUDA;
@@ -323,6 +339,10 @@ void bolt_ctx_destroy(BoltCtx* ctx) {
     cudaFree(ctx->ebefore);
     cudaFree(ctx->J);
     cudaFree(ctx->derr);
+    cudaFree(ctx->es_part);
+    cudaFree(ctx->es_rho);
+    cudaFree(ctx->es_e);
+    poisson_plans_destroy(ctx->es_fwd, ctx->es_inv);
     if (ctx->hflag) cudaFreeHost(ctx->hflag);
     delete ctx;
 }
@@ -556,12 +576,44 @@ static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st)
     return BOLT_OK;
 }
 
+static int electrostatic(const BoltCtx* ctx) {
+    return ctx->p.fields_enabled && ctx->p.fields_type == BOLT_FIELDS_ELECTROSTATIC;
+}
+
+// electrostatic fields of the df/dt argument f (df_dt_fvm.py:234-242): its
+// species densities, then the FFT Poisson solve into the cell-centred E1, E2
+static int launch_electrostatic(BoltCtx* ctx, const void* f, cudaStream_t st) {
+    const BoltGrid& g = ctx->g;
+    int rc = launch_moments5(ctx, f, ctx->es_part, st);
+    if (rc) return rc;
+    PoissonArgs a;
+    memset(&a, 0, sizeof(a));
+    a.part = ctx->es_part;
+    a.rho_hat = ctx->es_rho;
+    a.e_hat = ctx->es_e;
+    a.cell = ctx->cell;
+    a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost; a.Ns = g.N_s;
+    a.dq1 = g.dq1; a.dq2 = g.dq2; a.eps = ctx->p.eps;
+    for (int s = 0; s < g.N_s; ++s) {
+        a.charge[s] = ctx->p.charge[s];
+        a.measure[s] = (g.dp3[s] * g.dp2[s]) * g.dp1[s];
+    }
+    CK(launch_poisson(a, ctx->es_fwd, ctx->es_inv, st, &ctx->launches));
+    return BOLT_OK;
+}
+
 // one df/dt evaluation + stage update: q-part (fused combine when there is no
 // p-advection), then p-part when fields are enabled
 static int run_stage(BoltCtx* ctx, StageIO io, int evolve, double dt, cudaStream_t st) {
     int rc;
     if (!ctx->p.fields_enabled) {
         rc = launch_qstage(ctx, io, 0, 0, st);
+    } else if (electrostatic(ctx)) {
+        rc = launch_electrostatic(ctx, io.fs, st);
+        StageIO qio = io;
+        qio.out1 = ctx->kbuf;
+        if (rc == BOLT_OK) rc = launch_qstage(ctx, qio, 1, 0, st);
+        if (rc == BOLT_OK) rc = launch_pstage(ctx, io, ctx->kbuf, st);
     } else {
         StageIO qio = io;
         qio.out1 = ctx->kbuf;
@@ -739,6 +791,11 @@ int bolt_dfdt(BoltCtx* ctx, const void* f_dev, void* dfdt_dev, int evolve_fields
         io.out1 = dfdt_dev;
         return launch_qstage(ctx, io, 1, 0, st);
     }
+    if (electrostatic(ctx)) {
+        rc = launch_electrostatic(ctx, f_dev, st);
+        evolve_fields = 0;
+    }
+    if (rc) return rc;
     StageIO qio = io;
     qio.out1 = ctx->kbuf;
     rc = launch_qstage(ctx, qio, 1, evolve_fields, st);

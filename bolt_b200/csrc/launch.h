@@ -52,6 +52,21 @@ inline size_t pstage_smem(int Np, size_t elem) { return 4 * (size_t)Np * elem; }
                                       int ext2, const SpeciesGrid& sg,                       \
                                       cudaStream_t st);
 
+// electrostatic field solve of one df/dt argument (poisson.cu)
+struct PoissonArgs {
+    const double* part;       // density partial sums [Ns][Nq2][Nq1] (moments5 split 0)
+    double2* rho_hat;         // Nq2 x Nq1 complex work
+    double2* e_hat;           // 2 x Nq2 x Nq1 complex work (E1, E2)
+    double* cell;             // (6, Nq2g, Nq1g) cell-centred fields; E1, E2 written
+    int Nq1, Nq2, Ng, Ns;
+    double dq1, dq2, eps;
+    double charge[kMaxSpecies], measure[kMaxSpecies];
+};
+int poisson_plans_create(int Nq1, int Nq2, int* fwd, int* inv);
+void poisson_plans_destroy(int fwd, int inv);
+cudaError_t launch_poisson(const PoissonArgs& a, int fwd, int inv, cudaStream_t st,
+                           long long* launches);
+
 BOLT_DECLARE_LAUNCHERS(f64, double)
 BOLT_DECLARE_LAUNCHERS(f32, float)
 

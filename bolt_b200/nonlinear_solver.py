@@ -124,8 +124,14 @@ class nonlinear_solver(object):
         if getattr(params, 'p_space_grid', 'cartesian') != 'cartesian':
             raise NotImplementedError('only the cartesian p-space grid is implemented')
         self.fields_enabled = bool(getattr(params, 'fields_enabled', False))
-        if self.fields_enabled and params.fields_type != 'electrodynamic':
-            raise NotImplementedError('only electrodynamic (FDTD) fields are implemented')
+        self.fields_type = getattr(params, 'fields_type', 'electrodynamic')
+        if self.fields_enabled:
+            ok = (self.fields_type == 'electrodynamic' and
+                  getattr(params, 'fields_solver', 'fdtd') == 'fdtd') or \
+                (self.fields_type == 'electrostatic' and
+                 getattr(params, 'fields_solver', 'fft') == 'fft')
+            if not ok:
+                raise NotImplementedError('fields: electrodynamic FDTD or electrostatic FFT only')
 
         # ---- domain ---------------------------------------------------------------
         self.q1_start, self.q1_end = ps.q1_start, ps.q1_end
@@ -255,6 +261,7 @@ class nonlinear_solver(object):
         p.integrator = N.RK[self.time_integrator]
         p.source_enabled = 1 if getattr(params, 'source_enabled', False) else 0
         p.fields_enabled = 1 if self.fields_enabled else 0
+        p.fields_type = N.FIELDS[self.fields_type] if self.fields_enabled else 0
         p.p_dim = int(params.p_dim)
         for s in range(self.N_species):
             p.mass[s], p.charge[s] = self._mass[s], self._charge[s]

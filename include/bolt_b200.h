@@ -74,6 +74,13 @@ extern "C" {
  * edge points into the domain (apply_bcs_f's 'mirror+dirichlet') */
 #define BOLT_BC_MIRROR_DIRICHLET 4
 
+/* field models (fields.py:559-690): electrodynamic fields advanced by FDTD
+ * once per step, or electrostatic fields re-solved from the charge density of
+ * every df/dt argument by the periodic FFT Poisson solve (fft.py:9-78,
+ * df_dt_fvm.py:234-242) */
+#define BOLT_FIELDS_ELECTRODYNAMIC 0
+#define BOLT_FIELDS_ELECTROSTATIC  1
+
 /* integrators */
 #define BOLT_RK2 2   /* fvm_operator.py:6-35 midpoint */
 #define BOLT_RK4 4   /* classic RK4 around df_dt_fvm  */
@@ -106,8 +113,9 @@ typedef struct BoltParams {
     int    bc_q1, bc_q2;          /* BOLT_BC_*                                 */
     int    integrator;            /* BOLT_RK2 / BOLT_RK4                       */
     int    source_enabled;        /* BGK relaxation on/off                     */
-    int    fields_enabled;        /* electrodynamic FDTD coupling on/off       */
+    int    fields_enabled;        /* field coupling on/off                     */
     int    p_dim;                 /* 1, 2 or 3                                 */
+    int    fields_type;           /* BOLT_FIELDS_* (when fields_enabled)       */
     double mass[BOLT_MAX_SPECIES], charge[BOLT_MAX_SPECIES];
     double boltzmann_constant;
     double tau;                   /* constant BGK tau (see bolt_set_tau_array) */

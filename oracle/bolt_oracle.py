@@ -542,6 +542,13 @@ class Oracle(object):
             fs = self.fields
             if evolve_fields is None:
                 evolve_fields = not self.at_n
+            if sp.get('fields_type', 'electrodynamic') == 'electrostatic':
+                # df_dt_fvm.py:234-242 + fields.py:559-566: the fields of this
+                # df/dt argument from its charge density, by the FFT solve,
+                # then the periodic halo refresh
+                evolve_fields = False
+                fs._fft_poisson(initial_rho(g, f))
+                fs.cell = _periodic_fill(g, fs.cell)
             if evolve_fields:
                 f_left = np.where(v1 > 0, lm, lp)
                 f_bot = np.where(v2 > 0, bm, bp)

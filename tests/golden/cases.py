@@ -140,6 +140,25 @@ CASES = {
         dirichlet=dict(left=dict(base=1.3, T=[1.0, 1.0, 1.0], u=[0.5, 0.1, 0]),
                        right=dict(base=0.7, T=[1.5, 1.0, 1.0], u=[-0.4, 0, 0])),
         init=dict(amp=0.1, k1=1, k2=2, u=[-0.2, 0.3, 0.1])),
+    # electrostatic fields re-solved by FFT at every df/dt (Vlasov-Poisson):
+    # Landau damping as the reference's landau_damping/linear example sets it
+    # up (uniform along a 3-cell q2, minmod, upwind, collisionless), RK2
+    'es_1d1v_landau_rk2': make(
+        N_q1=32, N_q2=3, N_p1=48, N_p2=1, N_p3=1, recon_q='minmod', recon_p='minmod',
+        p1_start=[-6.0], p1_end=[6.0], p2_start=[-0.5], p2_end=[0.5],
+        p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0], p_dim=1,
+        source_enabled=False, fields_enabled=True,
+        fields_type='electrostatic', fields_solver='fft', dt=2e-3, steps=5,
+        init=dict(amp=0.05, k1=1, k2=0)),
+    # 2D2V electrostatic with BGK, two species, LLF, RK4
+    'es_2d2v_two_species_rk4': make(
+        N_q1=8, N_q2=6, N_p1=8, N_p2=8, N_p3=1,
+        p1_start=[-5.0, -2.0], p1_end=[5.0, 2.0], p2_start=[-5.0, -2.0], p2_end=[5.0, 2.0],
+        p3_start=[-0.5, -0.5], p3_end=[0.5, 0.5], mass=[1.0, 6.0], charge=[-1.0, 0.5],
+        p_dim=2, fields_enabled=True, fields_type='electrostatic', fields_solver='fft',
+        tau=0.1, dt=1e-3, steps=3, integrator='RK4',
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+        init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=11, u=[0.2, -0.1, 0.0])),
     # two species with different masses, charges and p-ranges, fields + BGK
     'two_species_2d2v_fields': make(
         N_q1=6, N_q2=4, N_p1=8, N_p2=6, N_p3=1,

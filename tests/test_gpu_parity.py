@@ -91,7 +91,8 @@ def test_fp64_matches_reference(name):
                                   'c3_2d3v_weno5_rk4_small', 'c2_2d2v_fdtd_rk4_small',
                                   'minmod_2d2v_fields_bgk', 'ppm_2d2v_fields_bgk',
                                   'dirichlet_1d1v_weno5', 'two_species_2d2v_fields',
-                                  'mirror_2d2v_weno5', 'mirror_dirichlet_2d3v_rk4'])
+                                  'mirror_2d2v_weno5', 'mirror_dirichlet_2d3v_rk4',
+                                  'es_1d1v_landau_rk2', 'es_2d2v_two_species_rk4'])
 def test_fp32_close_to_reference(name):
     _check_case(name, 'fp32')
 

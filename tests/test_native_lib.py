@@ -28,7 +28,7 @@ def test_library_exports_all_declared_symbols():
 def test_struct_layouts_match_header():
     # BoltGrid: 7 ints, 4 doubles, 6 x 8 doubles (with alignment padding)
     assert ctypes.sizeof(N.BoltGrid) == 7 * 4 + 4 + 4 * 8 + 6 * 8 * 8
-    assert ctypes.sizeof(N.BoltParams) == 11 * 4 + 4 + 2 * 8 * 8 + 4 * 8
+    assert ctypes.sizeof(N.BoltParams) == 12 * 4 + 2 * 8 * 8 + 4 * 8
 
 
 def test_strerror_and_null_args():
