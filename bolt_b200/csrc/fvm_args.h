@@ -17,17 +17,23 @@ constexpr int PWP = PW + 1;     // padded stage-buffer row (conflict-free column
 // kernel and by the host to size the launch.
 struct QLayout {
     unsigned tile, stage, vtab, jacc, qc, tabs, vgrid, bars, total;
+    int nbuf;               // halo tiles in flight (2: double-buffered)
 };
+
+// dynamic shared memory per CTA that still lets two CTAs share an SM
+// (228 KB per SM, 1 KB reserved per CTA)
+constexpr unsigned kTwoCtaSmem = 113u * 1024u;
 
 __host__ __device__ inline unsigned qalign(unsigned x, unsigned a) { return (x + a - 1) / a * a; }
 
-__host__ __device__ inline QLayout qstage_layout(int tq1, int tq2, int q2, int elem, int bgk,
-                                                 int bgk_direct, int ntab) {
+__host__ __device__ inline QLayout qstage_layout_n(int tq1, int tq2, int q2, int elem, int bgk,
+                                                   int bgk_direct, int ntab, int nbuf) {
     QLayout L;
+    L.nbuf = nbuf;
     const unsigned hx = tq1 + 2 * HALO, hy = q2 ? tq2 + 2 * HALO : 1;
     const unsigned nq = tq1 * tq2;
     unsigned o = 0;
-    L.tile = o;  o += qalign(2u * hy * hx * PW * elem, 128);
+    L.tile = o;  o += qalign((unsigned)nbuf * hy * hx * PW * elem, 128);
     // the epilogue reuses the tile region for the cross-thread moment reduction
     const unsigned red = (unsigned)(NTHREADS * kNumMom * sizeof(double));
     if (o < red) o = qalign(red, 128);
@@ -40,6 +46,16 @@ __host__ __device__ inline QLayout qstage_layout(int tq1, int tq2, int q2, int e
     L.bars = o;  o += 2 * sizeof(unsigned long long);
     L.total = o;
     return L;
+}
+
+// Double-buffered halo tiles when two CTAs per SM still fit, else one (the
+// FP64 8x8 tile with exp tables: 160 KB double-buffered, 110 KB single) --
+// the co-resident CTA then hides the load that double-buffering would.
+__host__ __device__ inline QLayout qstage_layout(int tq1, int tq2, int q2, int elem, int bgk,
+                                                 int bgk_direct, int ntab) {
+    const QLayout L2 = qstage_layout_n(tq1, tq2, q2, elem, bgk, bgk_direct, ntab, 2);
+    if (L2.total <= kTwoCtaSmem) return L2;
+    return qstage_layout_n(tq1, tq2, q2, elem, bgk, bgk_direct, ntab, 1);
 }
 
 // Shared-memory carve-up of the paired FP32 kernel (8x8 q-tile), offsets from

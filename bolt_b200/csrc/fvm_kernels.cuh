@@ -203,7 +203,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     const int ntab = Np1 + Np2 + Np3;
     const QLayout Lo = qstage_layout(TQ1, TQ2, Q2, sizeof(T), BGK, a.bgk_direct, ntab);
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    T* tile = reinterpret_cast<T*>(smem_raw + Lo.tile);              // [2][HY][HX][PW]
+    T* tile = reinterpret_cast<T*>(smem_raw + Lo.tile);              // [NB][HY][HX][PW]
     T* stage = reinterpret_cast<T*>(smem_raw + Lo.stage);            // [NQ][PWP]
     double* vtab = reinterpret_cast<double*>(smem_raw + Lo.vtab);    // [4][PW]
     double* j_acc = reinterpret_cast<double*>(smem_raw + Lo.jacc);   // [NQ][3]
@@ -232,12 +232,12 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     qstage_prologue<NQ, TQ1, BGK>(a, s, i0, j0, j_acc, vgrid, qc, tabs, bars);
 
     // ---- tile loader -------------------------------------------------------
-    bool failed = false;       // a bounded wait gave up: finish without TMA
+    bool failed = false;       // a bounded wait gave up
     const unsigned tile_bytes = TILE * sizeof(T);
     auto issue = [&](int k, int buf) {
         if (k >= k_end) return;
         if (a.use_tma) {
-            if (tid == 0 && !failed) {
+            if (tid == 0) {
                 mbar_arrive_expect_tx(&bars[buf], tile_bytes);
                 tma_load_3d(tile + buf * TILE, &a.tmap, &bars[buf], s * Np + k * PW,
                             i0 + Ng - HALO, Q2 ? j0 + Ng - HALO : j0 + Ng);
@@ -261,8 +261,9 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     };
 
     unsigned phase0 = 0u, phase1 = 0u;
+    const int NB = Lo.nbuf;                     // 1 or 2 halo tiles
     issue(k_begin, 0);
-    issue(k_begin + 1, 1);
+    if (NB == 2) issue(k_begin + 1, 1);
 
     T* out1 = static_cast<T*>(a.out1);
     T* out2 = static_cast<T*>(a.out2);
@@ -291,16 +292,27 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     const long long item_step = (long long)(NWARP / NSEGB) * rowstride;   // next item: columns
 
     int buf = 0;
-    for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
-        if (a.use_tma && !failed) {
+    for (int k = k_begin; k < k_end; ++k, buf ^= (NB - 1)) {
+        if (a.use_tma) {
             const unsigned ph = buf ? phase1 : phase0;
-            if (!mbar_wait_bounded(&bars[buf], ph)) {
-                atomicExch(a.err, 4);
-                failed = true;
-            }
+            if (!mbar_wait_bounded(&bars[buf], ph)) failed = true;
             if (buf) phase1 ^= 1u; else phase0 ^= 1u;
         }
-        __syncthreads();   // tile visible; previous chunk's phase C done with `stage`
+        // tile visible; previous chunk's phase C done with `stage`.  A wait
+        // that ran out ends the CTA: record it and let the copies still in
+        // flight (chunks k .. k+NB-1) land, bounded, before returning.
+        if (__syncthreads_or(failed)) {
+            if (tid == 0) {
+                atomicExch(a.err, 4);
+                // chunk k's parity was already flipped above; chunk k+1's not
+                for (int j = 0; j < NB && k + j < k_end; ++j) {
+                    const int b = (buf + j) % NB;
+                    const unsigned ph = (b ? phase1 : phase0) ^ (j == 0 ? 1u : 0u);
+                    mbar_wait_bounded(&bars[b], ph);
+                }
+            }
+            return;
+        }
         const T* X = tile + buf * TILE;
         const bool pvalid = p < Np;
         const int jp1 = pvalid ? ip1 : 0, jp2 = pvalid ? ip2 : 0, jp3 = pvalid ? ip3 : 0;
@@ -465,7 +477,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
         }
         __syncthreads();   // tile `buf` consumed, stage holds out1 of the chunk
         if (a.use_tma) fence_proxy_async();
-        issue(k + 2, buf);
+        issue(k + NB, buf);
 
         // ---- phase C: FP64 moments of out1 (moments.py:6-24) ------------------
         if (want_mom) {
