@@ -360,10 +360,32 @@ def run_ours(args, rank, world, local_rank):
     e1.record(main)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    # the copies alone, both directions at once on the same pinned buffers:
+    # the PCIe floor of one end-to-end step
+    torch.cuda.synchronize()
+    e0.record(main)
+    s_in.wait_stream(main)
+    s_out.wait_stream(main)
+    for _ in range(e2e_steps):
+        with torch.cuda.stream(s_in):
+            stage_in.copy_(host_in, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            host_out.copy_(stage_out, non_blocking=True)
+    main.wait_stream(s_in)
+    main.wait_stream(s_out)
+    e1.record(main)
+    e1.synchronize()
+    copy_ms = e0.elapsed_time(e1) / e2e_steps
     e2e_ms = max_over_ranks(e2e_ms, world)
+    copy_ms = max_over_ranks(copy_ms, world)
     fbytes = host_in.numel() * host_in.element_size()
     e2e = {'value': job_value(cells, world, e2e_ms), 'unit': UNIT,
-           'h2d_bytes_per_step': fbytes, 'd2h_bytes_per_step': fbytes}
+           'h2d_bytes_per_step': fbytes, 'd2h_bytes_per_step': fbytes,
+           'ms_per_step': e2e_ms,
+           # floor: the same host<->device bytes copied with nothing else running
+           'copy_floor_ms_per_step': copy_ms,
+           'frac_of_copy_floor': copy_ms / e2e_ms,
+           'pcie_gbs_per_direction': fbytes / (copy_ms * 1e-3) / 1e9}
 
     # FP64 plain form of the same workload (reported beside the FP32 number)
     fp64 = None

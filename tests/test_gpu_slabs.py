@@ -9,7 +9,8 @@ copied between their stage buffers before every RK stage (what the send/recv
 exchange does between ranks): interior cells equal the whole-domain run to a
 few ulps (the slabs' FP64 moment partial sums may be split differently over
 p).  The slabs are 8 rows, so FP32 runs the paired kernel with external q2
-ghosts."""
+ghosts.  Mirror walls along q1 (filled by the ghost pass after every stage)
+are covered as well."""
 
 import pytest
 import torch
@@ -20,8 +21,8 @@ from _modules import make_solver
 pytestmark = pytest.mark.gpu
 
 
-def _spec(N_q2, integrator):
-    return C.make(N_q1=24, N_q2=N_q2, N_p1=8, N_p2=8, N_p3=4,
+def _spec(N_q2, integrator, bc_q1='periodic'):
+    return C.make(N_q1=24, N_q2=N_q2, N_p1=8, N_p2=8, N_p3=4, bc_q1=bc_q1,
                   p1_start=[-5.0, -3.0], p1_end=[5.0, 3.0], p2_start=[-5.0, -3.0],
                   p2_end=[5.0, 3.0], p3_start=[-5.0, -3.0], p3_end=[5.0, 3.0],
                   mass=[1.0, 4.0], charge=[0.0, 0.0], p_dim=3, tau=0.01, dt=1e-3,
@@ -47,10 +48,11 @@ def _exchange(slabs, k):
 
 
 @pytest.mark.parametrize('precision', ['fp64', 'fp32'])
-@pytest.mark.parametrize('integrator', ['RK4', 'RK2'])
-def test_single_slab_equals_periodic_run(precision, integrator):
+@pytest.mark.parametrize('integrator,bc_q1', [('RK4', 'periodic'), ('RK2', 'periodic'),
+                                              ('RK4', 'mirror')])
+def test_single_slab_equals_periodic_run(precision, integrator, bc_q1):
     from bolt_b200.distributed import SlabSolver
-    spec = _spec(16, integrator)
+    spec = _spec(16, integrator, bc_q1)
     whole = make_solver(spec, precision)
     slab = SlabSolver(whole.physical_system)
     slab.local.f = whole.f.clone()
@@ -63,10 +65,11 @@ def test_single_slab_equals_periodic_run(precision, integrator):
 
 
 @pytest.mark.parametrize('precision,tol', [('fp64', 1e-13), ('fp32', 2e-6)])
-@pytest.mark.parametrize('world,integrator', [(2, 'RK4'), (4, 'RK4'), (2, 'RK2')])
-def test_slabs_in_lockstep_equal_whole_domain(world, integrator, precision, tol):
+@pytest.mark.parametrize('world,integrator,bc_q1', [(2, 'RK4', 'periodic'), (4, 'RK4', 'periodic'),
+                                                    (2, 'RK2', 'periodic'), (2, 'RK4', 'mirror')])
+def test_slabs_in_lockstep_equal_whole_domain(world, integrator, bc_q1, precision, tol):
     from bolt_b200.distributed import SlabSolver
-    spec = _spec(8 * world, integrator)
+    spec = _spec(8 * world, integrator, bc_q1)
     whole = make_solver(spec, precision)
     slabs = [SlabSolver(whole.physical_system, slab=(r, world)) for r in range(world)]
     Ng, n = spec['N_ghost'], 8
