@@ -117,6 +117,10 @@ SIGNATURES = {
     'bolt_batch_run': (ctypes.c_int, [_VP, ctypes.c_int, _VP]),
     'bolt_batch_moments': (ctypes.c_int, [_VP, _VP, _VP]),
     'bolt_batch_divergence_flag': (ctypes.c_int, [_VP]),
+    'bolt_batch_set_schedule': (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    'bolt_batch_get_schedule': (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int)]),
     'bolt_adj1d_create': (ctypes.c_int, [ctypes.POINTER(BoltAdj1DSpec), ctypes.c_int,
                                          ctypes.POINTER(_VP)]),
     'bolt_adj1d_destroy': (None, [_VP]),

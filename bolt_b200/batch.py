@@ -13,6 +13,14 @@ replayed as one CUDA graph.  Grids, ranges, tau and dt may differ per run.
 Per run, ``f(r)`` is a torch view of the run's f in Bolt's layout
 (N_p1, 1, N_q1 + 2 N_g, 1) and ``compute_moments(name, r)`` returns the
 moment over the interior q-cells, shape (1, 1, N_q1, 1), FP64.
+
+The launch schedule is chosen by an autotuner (``autotune``).  It covers the
+q-cells per work item (the pencil-to-block tile), the persistent CTAs per SM
+and the queue order. Before the first ``run``, each candidate is timed on
+the batch itself, a few steps from its current state with CUDA events, and
+the state is restored afterwards. The fastest is kept, and it is remembered
+for batches with the same run shapes in this process.  Every schedule gives
+bit-identical results.
 """
 
 import torch
@@ -21,6 +29,11 @@ from . import _native as N
 from .nonlinear_solver import nonlinear_solver, _plugin_ok
 
 BATCH_MOMENTS = ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy')
+
+# schedules the autotuner times: (q-cells per work item, CTAs per SM, queue
+# order 1 = longest items first / 0 = run by run)
+TUNE_CANDIDATES = tuple((tq, c, o) for tq in (16, 32, 64) for c in (1, 2, 4, 8) for o in (1, 0))
+_TUNED = {}    # (collisional, run shapes) -> schedule chosen in this process
 
 
 class _RunGrid(object):
@@ -62,7 +75,7 @@ def _check_system(ps, r):
 
 class BatchSolver(object):
 
-    def __init__(self, systems, dts):
+    def __init__(self, systems, dts, autotune=True):
         if not torch.cuda.is_available():
             raise RuntimeError('bolt_b200 runs on a CUDA device (sm_100a); no CUDA device '
                                'is available and there is no CPU fallback')
@@ -134,6 +147,12 @@ class BatchSolver(object):
             self.f(r).copy_(torch.broadcast_to(f0, self.f(r).shape))
         self._prepared = False
         self._seen = self._flat._version
+        self._key = (self.source_enabled, tuple((R.N_q1, R.N_p1) for R in runs))
+        self.tuning = None
+        self._tune_pending = bool(autotune)
+        if autotune and self._key in _TUNED:
+            self.set_schedule(*_TUNED[self._key])
+            self._tune_pending = False
 
     def __del__(self):
         try:
@@ -154,8 +173,62 @@ class BatchSolver(object):
         store = self._flat[self._f_off[r]:self._f_off[r] + n].view(R.N_q1 + 6, R.N_p1)
         return store.permute(1, 0).unsqueeze(1).unsqueeze(3)
 
+    # ---- launch schedule ------------------------------------------------------------
+    def set_schedule(self, tile_cells, ctas_per_sm, lpt_order):
+        N.check(self._lib.bolt_batch_set_schedule(self._b, int(tile_cells), int(ctas_per_sm),
+                                                  int(lpt_order)), 'bolt_batch_set_schedule')
+
+    def schedule(self):
+        """(q-cells per work item, CTAs launched, queue order)."""
+        v = [N.ctypes.c_int() for _ in range(3)]
+        N.check(self._lib.bolt_batch_get_schedule(self._b, *[N.ctypes.byref(x) for x in v]),
+                'bolt_batch_get_schedule')
+        return tuple(x.value for x in v)
+
+    def autotune(self, steps=4, repeats=2, candidates=TUNE_CANDIDATES):
+        """Time every candidate schedule over ``steps`` RK4 steps of this batch
+        (best of ``repeats`` CUDA-event timings, after one untimed replay that
+        also captures the graph) from the current f, then restore f and keep
+        the fastest.  Returns [((tile_cells, ctas, order), ms per step), ...]."""
+        saved = self._flat.clone()
+        stream = self._stream()
+        results, seen = [], set()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for tq, cps, order in candidates:
+            self.set_schedule(tq, cps, order)
+            eff = self.schedule()
+            if eff in seen:
+                continue
+            seen.add(eff)
+            self._flat.copy_(saved)
+            N.check(self._lib.bolt_batch_prepare(self._b, stream), 'bolt_batch_prepare')
+            N.check(self._lib.bolt_batch_run(self._b, steps, stream), 'bolt_batch_run')
+            best = float('inf')
+            for _ in range(repeats):
+                e0.record()
+                N.check(self._lib.bolt_batch_run(self._b, steps, stream), 'bolt_batch_run')
+                e1.record()
+                e1.synchronize()
+                best = min(best, e0.elapsed_time(e1) / steps)
+            results.append(((tq, cps, order), eff, best))
+        (tq, cps, order), eff, ms = min(results, key=lambda x: x[2])
+        self.set_schedule(tq, cps, order)
+        self._flat.copy_(saved)
+        self._prepared = False
+        self._seen = -1
+        self._lib.bolt_batch_divergence_flag(self._b)       # tuning steps leave no flag
+        _TUNED[self._key] = (tq, cps, order)
+        self.tuning = {'chosen': {'tile_cells': eff[0], 'ctas': eff[1], 'lpt_order': eff[2],
+                                  'ms_per_step': ms},
+                       'candidates': [{'tile_cells': e[0], 'ctas': e[1], 'lpt_order': e[2],
+                                       'ms_per_step': t} for _, e, t in results]}
+        self._tune_pending = False
+        return results
+
     def run(self, nsteps):
         """Advance every run by nsteps RK4 steps of its own dt."""
+        if self._tune_pending:
+            self.autotune()
         if not self._prepared or self._flat._version != self._seen:
             N.check(self._lib.bolt_batch_prepare(self._b, self._stream()), 'bolt_batch_prepare')
             self._prepared = True

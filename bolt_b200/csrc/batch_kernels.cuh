@@ -4,10 +4,12 @@
 // Every run r keeps its own ghosted distribution f_r[q1g][p1] (N_g = 3,
 // periodic in q1, p1 fastest) at element offset f_off in one packed buffer;
 // the RK stage buffers use the same packing.  A stage is ONE launch over all
-// runs: persistent CTAs take work items (run, 32-cell q-tile) from a queue
-// ordered by decreasing cost, and each item walks all p-chunks of its tile,
-// so its q-cells' velocity moments are complete when the item ends (no
-// partial sums, no atomics on data).
+// runs: persistent CTAs take work items (run, q-tile of 4 cells per warp)
+// from a queue, and each item walks all p-chunks of its tile, so its
+// q-cells' velocity moments are complete when the item ends (no partial sums,
+// no atomics on data).  The tile height (warps per CTA), the CTAs per SM and
+// the queue order are the schedule the batch's autotuner chooses; every
+// schedule computes each cell with the same operations in the same order.
 //
 // Per item and 32-wide p-chunk (one p per lane):
 //   * the tile's rows plus 3 halo rows each side are staged in shared memory
@@ -27,9 +29,9 @@
 
 namespace bolt {
 
-constexpr int kBatchTQ = 32;         // q-cells per work item
-constexpr int kBatchThreads = 256;   // 8 warps x 4 q-cells
 constexpr int kBatchNg = 3;          // ghost width (WENO5 stencil +-2 and the face shift)
+// a work item is a q-tile of 4 cells per warp; CTAs of 4, 8 or 16 warps
+constexpr int kBatchCellsPerWarp = 4;
 
 struct BatchRunDev {
     long long f_off;       // element offset of the run's ghosted f in every packed buffer
@@ -44,7 +46,7 @@ struct BatchRunDev {
 
 struct BatchStageArgs {
     const BatchRunDev* runs;
-    const int2* items;     // (run, tile), decreasing cost
+    const int2* items;     // (run, tile) in queue order
     int nitems;
     int* counter;          // work-queue head (zeroed before the launch)
     const float* fs;       // stage input (ghosted)
@@ -105,11 +107,13 @@ __device__ __forceinline__ void batch_moments_out(const BatchRunDev& R, double m
     dst[4] = e1 + 0.5 * (R.v2c * R.v2c + R.v3c * R.v3c) * m0;
 }
 
-__global__ void __launch_bounds__(kBatchThreads)
+template <int NW>
+__global__ void __launch_bounds__(NW * 32)
 batch_stage_kernel(const BatchStageArgs a) {
-    constexpr int ROWS = kBatchTQ + 2 * kBatchNg;
+    constexpr int TQ = NW * kBatchCellsPerWarp;
+    constexpr int ROWS = TQ + 2 * kBatchNg;
     __shared__ float X[ROWS][PW];
-    __shared__ double par[kBatchTQ][3];
+    __shared__ double par[TQ][3];
     __shared__ int item_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     bool nonfinite = false;
@@ -122,8 +126,8 @@ batch_stage_kernel(const BatchStageArgs a) {
         const int2 rt = a.items[it];
         const BatchRunDev& R = a.runs[rt.x];
         const int Nq1 = R.Nq1, Np1 = R.Np1;
-        const int i0 = rt.y * kBatchTQ;
-        const int ncell = min(kBatchTQ, Nq1 - i0);
+        const int i0 = rt.y * TQ;
+        const int ncell = min(TQ, Nq1 - i0);
         const float* fs = a.fs + R.f_off;
 
         // Maxwellian parameters of the tile's cells (stage input's moments)
@@ -142,7 +146,7 @@ batch_stage_kernel(const BatchStageArgs a) {
         for (int c = 0; c < Np1 / PW; ++c) {
             const int p = c * PW + lane;
             __syncthreads();                      // previous chunk's X reads are done
-            for (int row = warp; row < ncell + 2 * kBatchNg; row += kBatchThreads / 32)
+            for (int row = warp; row < ncell + 2 * kBatchNg; row += NW)
                 X[row][lane] = fs[(long long)(i0 + row) * Np1 + p];
             __syncthreads();
             if (!active) continue;
@@ -203,9 +207,11 @@ batch_stage_kernel(const BatchStageArgs a) {
 }
 
 // velocity moments of f for every run (the first stage after f is set)
-__global__ void __launch_bounds__(kBatchThreads)
+template <int NW>
+__global__ void __launch_bounds__(NW * 32)
 batch_moments_kernel(const BatchRunDev* runs, const int2* items, int nitems, int* counter,
                      const float* f, double* mom) {
+    constexpr int TQ = NW * kBatchCellsPerWarp;
     __shared__ int item_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (;;) {
@@ -215,7 +221,7 @@ batch_moments_kernel(const BatchRunDev* runs, const int2* items, int nitems, int
         if (it >= nitems) break;
         const int2 rt = items[it];
         const BatchRunDev& R = runs[rt.x];
-        const int i0 = rt.y * kBatchTQ, ncell = min(kBatchTQ, R.Nq1 - i0);
+        const int i0 = rt.y * TQ, ncell = min(TQ, R.Nq1 - i0);
         const int j0 = 4 * warp;
         if (j0 < ncell) {
             double acc[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};

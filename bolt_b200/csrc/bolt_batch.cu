@@ -4,10 +4,13 @@
 // Packing: run r's ghosted f (N_q1 + 6 rows of N_p1 FP32 values, periodic q1)
 // starts at an element offset that is a multiple of 32 (128 bytes) in each of
 // the four f-sized buffers (f, RK4 stage buffers A, B and the accumulator C);
-// FP64 moment sums are packed by q-cell, [cell][5].  Work items (run, 32-cell
-// q-tile) are sorted by decreasing cost (cells x p-chunks) and consumed by
-// persistent CTAs through an atomic queue that a memset node resets before
-// every stage.  bolt_batch_run captures nsteps RK4 steps of all runs (4 stage
+// FP64 moment sums are packed by q-cell, [cell][5].  Work items (run, q-tile)
+// are consumed by persistent CTAs through an atomic queue that a memset node
+// resets before every stage.  The schedule -- q-cells per tile (16, 32 or 64:
+// CTAs of 4, 8 or 16 warps), CTAs per SM and the queue order (decreasing cost
+// = cells x p-chunks, or run by run) -- is set by bolt_batch_set_schedule; the
+// batch's autotuner (bolt_b200.batch) times the candidates on the batch
+// itself.  bolt_batch_run captures nsteps RK4 steps of all runs (4 stage
 // launches each) into one CUDA graph on the batch's own stream and launches
 // it on the caller's stream.
 #include <cuda_runtime.h>
@@ -38,6 +41,10 @@ struct BoltBatch {
     int* hflag;             // non-finite flag, host-mapped
     int* dflag;
     int nctas;
+    int tile_warps;         // schedule: warps per CTA (4 q-cells each)
+    int ctas_per_sm;        //           persistent CTAs per SM (clamped to occupancy)
+    int lpt;                //           1: items by decreasing cost, 0: run by run
+    int sms;
     cudaStream_t cap;       // capture stream
     cudaGraphExec_t exec;
     int exec_steps;
@@ -47,6 +54,85 @@ struct BoltBatch {
 namespace {
 
 int batch_ck(cudaError_t e) { return e == cudaSuccess ? BOLT_OK : BOLT_ERR_CUDA; }
+
+template <int NW>
+int stage_occupancy() {
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_stage_kernel<NW>, NW * 32, 0);
+    return std::max(1, per_sm);
+}
+
+int occupancy(int tile_warps) {
+    switch (tile_warps) {
+        case 4: return stage_occupancy<4>();
+        case 8: return stage_occupancy<8>();
+        default: return stage_occupancy<16>();
+    }
+}
+
+// work items of the current schedule -> d_items, nitems, nctas (drops the
+// captured graph: its launches carry the old grid and item list)
+int build_schedule(BoltBatch* b) {
+    const int tq = b->tile_warps * kBatchCellsPerWarp;
+    std::vector<int2> items;
+    std::vector<long long> cost;
+    for (int r = 0; r < b->nruns; ++r) {
+        const BatchRunDev& R = b->runs[r];
+        for (int t = 0; t * tq < R.Nq1; ++t) {
+            items.push_back(make_int2(r, t));
+            cost.push_back((long long)std::min(tq, R.Nq1 - t * tq) * (R.Np1 / PW));
+        }
+    }
+    std::vector<int> order(items.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    if (b->lpt)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return cost[x] > cost[y]; });
+    std::vector<int2> sorted(items.size());
+    for (size_t i = 0; i < order.size(); ++i) sorted[i] = items[order[i]];
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+        b->exec_steps = 0;
+    }
+    if ((int)sorted.size() != b->nitems || !b->d_items) {
+        cudaFree(b->d_items);
+        b->d_items = nullptr;
+        if (cudaMalloc((void**)&b->d_items, sorted.size() * sizeof(int2)) != cudaSuccess)
+            return BOLT_ERR_NOMEM;
+    }
+    b->nitems = (int)sorted.size();
+    int rc = batch_ck(cudaMemcpy(b->d_items, sorted.data(), sorted.size() * sizeof(int2),
+                                 cudaMemcpyHostToDevice));
+    const int per_sm = std::min(b->ctas_per_sm, occupancy(b->tile_warps));
+    b->nctas = std::max(1, std::min(b->nitems, b->sms * per_sm));
+    return rc;
+}
+
+void launch_stage(const BoltBatch* b, const BatchStageArgs& a, cudaStream_t st) {
+    switch (b->tile_warps) {
+        case 4: batch_stage_kernel<4><<<b->nctas, 4 * 32, 0, st>>>(a); break;
+        case 8: batch_stage_kernel<8><<<b->nctas, 8 * 32, 0, st>>>(a); break;
+        default: batch_stage_kernel<16><<<b->nctas, 16 * 32, 0, st>>>(a); break;
+    }
+}
+
+void launch_moments(const BoltBatch* b, cudaStream_t st) {
+    switch (b->tile_warps) {
+        case 4:
+            batch_moments_kernel<4><<<b->nctas, 4 * 32, 0, st>>>(
+                b->d_runs, b->d_items, b->nitems, b->counters, b->buf[0], b->mom[0]);
+            break;
+        case 8:
+            batch_moments_kernel<8><<<b->nctas, 8 * 32, 0, st>>>(
+                b->d_runs, b->d_items, b->nitems, b->counters, b->buf[0], b->mom[0]);
+            break;
+        default:
+            batch_moments_kernel<16><<<b->nctas, 16 * 32, 0, st>>>(
+                b->d_runs, b->d_items, b->nitems, b->counters, b->buf[0], b->mom[0]);
+            break;
+    }
+}
 
 void batch_free(BoltBatch* b) {
     if (!b) return;
@@ -93,7 +179,7 @@ int enqueue_step(BoltBatch* b, cudaStream_t st) {
         a.a1 = stages[s].a1;
         a.a2 = stages[s].a2;
         a.source = b->source;
-        batch_stage_kernel<<<b->nctas, kBatchThreads, 0, st>>>(a);
+        launch_stage(b, a, st);
         if (cudaGetLastError() != cudaSuccess) return BOLT_ERR_CUDA;
     }
     return BOLT_OK;
@@ -122,8 +208,6 @@ int bolt_batch_create(const BoltBatchRun* runs, int nruns, int source_enabled, B
     b->runs.resize(nruns);
     long long off = 0;
     int qoff = 0;
-    std::vector<int2> items;
-    std::vector<long long> cost;
     for (int r = 0; r < nruns; ++r) {
         const BoltBatchRun& R = runs[r];
         BatchRunDev& D = b->runs[r];
@@ -143,19 +227,13 @@ int bolt_batch_create(const BoltBatchRun* runs, int nruns, int source_enabled, B
         D.inv_tau = source_enabled ? 1.0 / R.tau : 0.0;
         off += ((long long)(R.N_q1 + 2 * kBatchNg) * R.N_p1 + 31) / 32 * 32;
         qoff += R.N_q1;
-        for (int t = 0; t * kBatchTQ < R.N_q1; ++t) {
-            items.push_back(make_int2(r, t));
-            cost.push_back((long long)std::min(kBatchTQ, R.N_q1 - t * kBatchTQ) * (R.N_p1 / PW));
-        }
     }
     b->fcount = (size_t)off;
     b->nq_total = qoff;
-    b->nitems = (int)items.size();
-    std::vector<int> order(items.size());
-    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
-    std::vector<int2> sorted(items.size());
-    for (size_t i = 0; i < order.size(); ++i) sorted[i] = items[order[i]];
+    // default schedule: 32-cell tiles, as many CTAs as fit, longest items first
+    b->tile_warps = 8;
+    b->ctas_per_sm = 64;
+    b->lpt = 1;
 
     int rc = BOLT_OK;
     auto alloc = [&](void** p, size_t bytes) {
@@ -166,7 +244,6 @@ int bolt_batch_create(const BoltBatchRun* runs, int nruns, int source_enabled, B
     alloc((void**)&b->mom[1], (size_t)qoff * kNumMom * sizeof(double));
     alloc((void**)&b->counters, 4 * sizeof(int));
     alloc((void**)&b->d_runs, nruns * sizeof(BatchRunDev));
-    alloc((void**)&b->d_items, sorted.size() * sizeof(int2));
     if (rc == BOLT_OK && cudaHostAlloc((void**)&b->hflag, sizeof(int), cudaHostAllocMapped) !=
                              cudaSuccess)
         rc = BOLT_ERR_NOMEM;
@@ -177,19 +254,15 @@ int bolt_batch_create(const BoltBatchRun* runs, int nruns, int source_enabled, B
     if (rc == BOLT_OK)
         rc = batch_ck(cudaMemcpy(b->d_runs, b->runs.data(), nruns * sizeof(BatchRunDev),
                                  cudaMemcpyHostToDevice));
-    if (rc == BOLT_OK)
-        rc = batch_ck(cudaMemcpy(b->d_items, sorted.data(), sorted.size() * sizeof(int2),
-                                 cudaMemcpyHostToDevice));
     for (int i = 0; i < 4 && rc == BOLT_OK; ++i)
         rc = batch_ck(cudaMemset(b->buf[i], 0, b->fcount * sizeof(float)));
     if (rc == BOLT_OK) rc = batch_ck(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
     if (rc == BOLT_OK) {
-        int dev = 0, sms = 148, per_sm = 1;
+        int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_stage_kernel,
-                                                      kBatchThreads, 0);
-        b->nctas = std::max(1, std::min(b->nitems, sms * std::max(1, per_sm)));
+        b->sms = sms;
+        rc = build_schedule(b);
     }
     if (rc != BOLT_OK) {
         batch_free(b);
@@ -224,10 +297,27 @@ int bolt_batch_prepare(BoltBatch* b, void* stream) {
     batch_ghost_kernel<<<g, 256, 0, st>>>(b->d_runs, b->nruns, b->buf[0]);
     if (cudaGetLastError() != cudaSuccess) return BOLT_ERR_CUDA;
     if (cudaMemsetAsync(b->counters, 0, sizeof(int), st) != cudaSuccess) return BOLT_ERR_CUDA;
-    batch_moments_kernel<<<b->nctas, kBatchThreads, 0, st>>>(b->d_runs, b->d_items, b->nitems,
-                                                             b->counters, b->buf[0], b->mom[0]);
+    launch_moments(b, st);
     if (cudaGetLastError() != cudaSuccess) return BOLT_ERR_CUDA;
     b->prepared = 1;
+    return BOLT_OK;
+}
+
+int bolt_batch_set_schedule(BoltBatch* b, int tile_cells, int ctas_per_sm, int lpt_order) {
+    if (!b || ctas_per_sm < 1) return BOLT_ERR_ARG;
+    if (tile_cells != 16 && tile_cells != 32 && tile_cells != 64) return BOLT_ERR_ARG;
+    if (cudaDeviceSynchronize() != cudaSuccess) return BOLT_ERR_CUDA;  // no launch uses the items
+    b->tile_warps = tile_cells / kBatchCellsPerWarp;
+    b->ctas_per_sm = ctas_per_sm;
+    b->lpt = lpt_order ? 1 : 0;
+    return build_schedule(b);
+}
+
+int bolt_batch_get_schedule(const BoltBatch* b, int* tile_cells, int* ctas, int* lpt_order) {
+    if (!b) return BOLT_ERR_ARG;
+    if (tile_cells) *tile_cells = b->tile_warps * kBatchCellsPerWarp;
+    if (ctas) *ctas = b->nctas;
+    if (lpt_order) *lpt_order = b->lpt;
     return BOLT_OK;
 }
 

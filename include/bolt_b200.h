@@ -261,6 +261,15 @@ int  bolt_batch_run(BoltBatch* b, int nsteps, void* stream);
 int  bolt_batch_moments(BoltBatch* b, double* out_dev, void* stream);
 /* 1 once a stage produced a non-finite value (cleared by the call). */
 int  bolt_batch_divergence_flag(BoltBatch* b);
+/* The launch schedule: q-cells per work item (16, 32 or 64: CTAs of 4, 8 or
+ * 16 warps), persistent CTAs per SM (clamped to what fits), and the queue
+ * order (1: items by decreasing cells x p-chunks, 0: run by run).  Every
+ * schedule gives bit-identical results; it changes only the speed.  The
+ * default is (32, all that fit, 1).  Setting it synchronises the device and
+ * drops the captured graph.  bolt_batch_get_schedule reports the CTA count
+ * actually launched. */
+int  bolt_batch_set_schedule(BoltBatch* b, int tile_cells, int ctas_per_sm, int lpt_order);
+int  bolt_batch_get_schedule(const BoltBatch* b, int* tile_cells, int* ctas, int* lpt_order);
 
 /* ------------------------------------------------------------------------
  * Adjoint of the 1D1V update.  No reference counterpart: Bolt has no

@@ -109,3 +109,34 @@ def test_collisionless_batch_conserves_mass():
     for i in range(len(runs)):
         m1 = float(bs.compute_moments('density', i).sum())
         assert abs(m1 - m0[i]) < 2e-6 * abs(m0[i]), (i, m0[i], m1)
+
+
+def test_every_schedule_gives_identical_results_and_autotune_keeps_the_state():
+    """The autotuner's candidate schedules (tile height 16/32/64 q-cells,
+    CTAs per SM, queue order) compute every cell the same way: f and the
+    moments after the steps are bit-identical.  autotune() times them from
+    the current f and leaves f unchanged."""
+    from bolt_b200.batch import BatchSolver
+    systems = [bench.ragged_system(r) for r in RUNS]
+    dts = [r['dt'] for r in RUNS]
+    ref = None
+    for sched in [(32, 2, 1), (16, 4, 0), (64, 1, 1), (16, 1, 1)]:
+        bs = BatchSolver(systems, dts, autotune=False)
+        bs.set_schedule(*sched)
+        assert bs.schedule()[0] == sched[0]
+        bs.run(STEPS)
+        bs.synchronize()
+        out = (bs._flat.clone(), [bs.compute_moments('energy', r) for r in range(len(RUNS))])
+        if ref is None:
+            ref = out
+        else:
+            assert torch.equal(out[0], ref[0]), sched
+            assert all(torch.equal(a, b) for a, b in zip(out[1], ref[1])), sched
+    bs = BatchSolver(systems, dts, autotune=False)
+    before = bs._flat.clone()
+    res = bs.autotune(steps=2, repeats=1)
+    assert torch.equal(bs._flat, before)
+    assert len(res) >= 6 and bs.tuning['chosen']['ms_per_step'] > 0
+    bs.run(STEPS)
+    bs.synchronize()
+    assert torch.equal(bs._flat, ref[0])
