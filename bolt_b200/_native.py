@@ -73,7 +73,7 @@ class BoltAdj1DSpec(ctypes.Structure):
                 ('p1_start', ctypes.c_double), ('p1_end', ctypes.c_double),
                 ('dp2', ctypes.c_double), ('dp3', ctypes.c_double),
                 ('mass', ctypes.c_double), ('boltzmann_constant', ctypes.c_double),
-                ('tau', ctypes.c_double), ('dt', ctypes.c_double)]
+                ('tau', ctypes.c_double), ('dt', ctypes.c_double), ('recon', ctypes.c_int)]
 
 
 # exported symbol -> (restype, argtypes); every function of include/bolt_b200.h

@@ -11,8 +11,9 @@ system) with the adjoint kernels of libbolt_b200.so (include/bolt_b200.h,
 the time-integrated squared k = 1 Fourier amplitude of the density.  Its
 gradient with respect to the initial f (every cell) and to the BGK collision
 time tau comes from the hand-written adjoint of the RK4 step (exact
-derivatives of the WENO5 nonlinear weights and of the Maxwellian through the
-moments), run backwards over the trajectory with binomial checkpointing: at
+derivatives of the WENO5 nonlinear weights -- or, with
+``reconstruction='minmod'``, a subgradient of the minmod limiter -- and of
+the Maxwellian through the moments), run backwards over the trajectory with binomial checkpointing: at
 most ``snapshots`` copies of f are held, and the forward steps are recomputed
 in the recursive schedule of Griewank's treeverse (the left segment of n
 steps with c snapshots and t sweeps holds at most C(c + t - 1, c) steps).
@@ -38,7 +39,7 @@ class Rollout1D1V(object):
 
     def __init__(self, N_q1, N_p1, p1_start, p1_end, dt, tau, nsteps, snapshots=20,
                  precision='fp64', q1_start=0.0, q1_end=1.0, dp2=1.0, dp3=1.0, mass=1.0,
-                 boltzmann_constant=1.0):
+                 boltzmann_constant=1.0, reconstruction='weno5'):
         if not torch.cuda.is_available():
             raise RuntimeError('bolt_b200 runs on a CUDA device (sm_100a); no CUDA device '
                                'is available and there is no CPU fallback')
@@ -53,6 +54,10 @@ class Rollout1D1V(object):
         s.q1_start, s.q1_end, s.p1_start, s.p1_end = q1_start, q1_end, p1_start, p1_end
         s.dp2, s.dp3, s.mass, s.boltzmann_constant = dp2, dp3, mass, boltzmann_constant
         s.tau, s.dt = float(tau), float(dt)
+        if reconstruction not in ('weno5', 'minmod'):
+            raise NotImplementedError('adjoint reconstruction: weno5 or minmod')
+        s.recon = N.RECON[reconstruction]
+        self.reconstruction = reconstruction
         self.spec = s
         self.dt = float(dt)
         c = N.ctypes.c_void_p()

@@ -11,6 +11,13 @@
 // RK4 (integrators.py:15-28): k1 = L(f), k2 = L(f + dt/2 k1),
 // k3 = L(f + dt/2 k2), k4 = L(f + dt k3), f' = f + dt/6 (k1 + 2k2 + 2k3 + k4).
 //
+// phi may also be the reference's minmod face (minmod.py:4-71: the theta = 2
+// limited slope of the upwind cell, sign(0) = +1), differentiated by a
+// subgradient: where the limiter's three arguments share a sign it passes the
+// smallest magnitude and that argument (the first of equal magnitudes) gets
+// derivative 1, elsewhere the slope is 0 and so is its derivative -- the
+// one-sided derivative at every kink, hence an element of the Clarke
+// subdifferential.
 // The adjoint of a stage applies L'(g)^T to an adjoint field a:
 //   * advection: phi_F enters L_F with -v/dq and L_F+1 with +v/dq, so
 //     phibar_F = -(v/dq)(a_F - a_F+1); cell j receives phibar_F dphi_F/dy_j
@@ -31,6 +38,9 @@ namespace bolt {
 
 constexpr int kAdjThreads = 256;
 constexpr int kAdjMaxNp = 2048;
+// face reconstructions of the adjoint (the BOLT_RECON_* values)
+constexpr int kAdjMinmod = 1;
+constexpr int kAdjWeno5 = 3;
 
 struct Adj1DArgs {
     int Nq1, Np1;
@@ -124,6 +134,40 @@ __device__ __forceinline__ T adj_weno(const T* y, bool right, T* d) {
     return phi;
 }
 
+// minmod face of the window y[0..4] (the upwind cell is y[2], its neighbours
+// y[1], y[3]; y[0], y[4] unused) on the given side, and optionally its
+// subgradient d[0..4] (minmod.py:4-71)
+template <typename T>
+__device__ __forceinline__ T adj_minmod(const T* y, bool right, T* d) {
+    const T bwd = y[2] - y[1], fwd = y[3] - y[2];
+    const T cen = bwd + fwd;
+    const T x[3] = {T(2) * bwd, T(0.5) * cen, T(2) * fwd};
+    const T sx = x[0] < T(0) ? T(-1) : T(1);
+    const T sy = x[1] < T(0) ? T(-1) : T(1);
+    const T sz = x[2] < T(0) ? T(-1) : T(1);
+    const T m = fmin(fmin(fabs(x[0]), fabs(x[1])), fabs(x[2]));
+    const T slope = T(0.25) * fabs(sx + sy) * (sx + sz) * m;
+    const T half = right ? T(0.5) : T(-0.5);
+    if (d) {
+        for (int j = 0; j < 5; ++j) d[j] = T(0);
+        d[2] = T(1);
+        if (sx == sy && sx == sz) {
+            // d slope / d x_k = 1 for the passed argument k; dx_k / dy
+            const int k = fabs(x[0]) == m ? 0 : (fabs(x[1]) == m ? 1 : 2);
+            if (k == 0) { d[1] -= half * T(2); d[2] += half * T(2); }
+            else if (k == 1) { d[1] -= half * T(0.5); d[3] += half * T(0.5); }
+            else { d[2] -= half * T(2); d[3] += half * T(2); }
+        }
+    }
+    return y[2] + half * slope;
+}
+
+template <typename T, int RECON>
+__device__ __forceinline__ T adj_face(const T* y, bool right, T* d) {
+    if (RECON == kAdjMinmod) return adj_minmod<T>(y, right, d);
+    return adj_weno<T>(y, right, d);
+}
+
 // FP64 block sum over the CTA (kAdjThreads threads)
 __device__ __forceinline__ double adj_block_sum(double v, double* red) {
     v = warp_sum(v);
@@ -164,7 +208,7 @@ __device__ __forceinline__ double adj_f0(const Adj1DArgs& P, const AdjMaxwell& M
 __device__ __forceinline__ int adj_wrap(int i, int n) { return ((i % n) + n) % n; }
 
 // k_out = L(f + c k_in) (k_in may be null), one CTA per q-cell
-template <typename T>
+template <typename T, int RECON>
 __global__ void __launch_bounds__(kAdjThreads)
 adj_stage_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, T* k_out) {
     __shared__ double red[kAdjThreads / 32];
@@ -193,9 +237,9 @@ adj_stage_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, T* k_out) {
         T y[5];
         // face i+1/2 (between i and i+1) and face i-1/2
         for (int t = 0; t < 5; ++t) y[t] = g(i - 2 + off + t, p);
-        const T phr = adj_weno<T>(y, right, nullptr);
+        const T phr = adj_face<T, RECON>(y, right, nullptr);
         for (int t = 0; t < 5; ++t) y[t] = g(i - 3 + off + t, p);
-        const T phl = adj_weno<T>(y, right, nullptr);
+        const T phl = adj_face<T, RECON>(y, right, nullptr);
         const T gi = g(i, p);
         T k = -(v * T(P.inv_dq)) * (phr - phl);
         if (P.tau > 0) k += (T(adj_f0(P, M, vd)) - gi) / T(P.tau);
@@ -257,7 +301,7 @@ __global__ void adj_mode_adjoint_kernel(const Adj1DArgs P, const double* reim, d
 }
 
 // out = L'(g)^T a at g = f + c k_in; dtau_part[i] = sum_p a (-(f0 - g)/tau^2)
-template <typename T>
+template <typename T, int RECON>
 __global__ void __launch_bounds__(kAdjThreads)
 adj_vjp_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, const T* a, T* out,
                double* dtau_part) {
@@ -330,7 +374,7 @@ adj_vjp_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, const T* a, T*
             if (pos < 0 || pos > 4) continue;
             T y[5], d[5];
             for (int t = 0; t < 5; ++t) y[t] = g(s0 + t, p);
-            adj_weno<T>(y, right, d);
+            adj_face<T, RECON>(y, right, d);
             const T phibar = k * (ad(F, p) - ad(F + 1, p));
             acc += phibar * d[pos];
         }

@@ -21,6 +21,7 @@ using namespace bolt;
 
 struct BoltAdj1D {
     int dtype;
+    int recon;               // kAdjWeno5 or kAdjMinmod
     Adj1DArgs P;
     double dt;
     long long n;             // N_q1 * N_p1
@@ -55,15 +56,15 @@ int ew_blocks(long long n) {
     return (int)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
 }
 
-template <typename T>
+template <typename T, int R>
 int step_impl(BoltAdj1D* c, T* f, double* J, cudaStream_t st) {
     const Adj1DArgs& P = c->P;
     const T dt = T(c->dt);
     T* k1 = (T*)c->k[0]; T* k2 = (T*)c->k[1]; T* k3 = (T*)c->k[2]; T* k4 = (T*)c->k[3];
-    adj_stage_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, (const T*)nullptr, T(0), k1);
-    adj_stage_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k1, dt / T(2), k2);
-    adj_stage_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k2, dt / T(2), k3);
-    adj_stage_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k3, dt, k4);
+    adj_stage_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, (const T*)nullptr, T(0), k1);
+    adj_stage_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k1, dt / T(2), k2);
+    adj_stage_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k2, dt / T(2), k3);
+    adj_stage_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k3, dt, k4);
     adj_combine_kernel<T><<<ew_blocks(c->n), 256, 0, st>>>(c->n, f, k1, k2, k3, k4, dt / T(6));
     if (J) {
         adj_density_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, c->dens);
@@ -72,7 +73,7 @@ int step_impl(BoltAdj1D* c, T* f, double* J, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? BOLT_OK : BOLT_ERR_CUDA;
 }
 
-template <typename T>
+template <typename T, int R>
 int adjoint_impl(BoltAdj1D* c, const T* f, T* lam, int obj_at_start, double* dtau,
                  cudaStream_t st) {
     const Adj1DArgs& P = c->P;
@@ -82,27 +83,27 @@ int adjoint_impl(BoltAdj1D* c, const T* f, T* lam, int obj_at_start, double* dta
     T* k1 = (T*)c->k[0]; T* k2 = (T*)c->k[1]; T* k3 = (T*)c->k[2];
     T* a = (T*)c->a; T* gacc = (T*)c->gacc; T* gs = (T*)c->gs;
     // recompute the stages from f
-    adj_stage_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, (const T*)nullptr, T(0), k1);
-    adj_stage_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k1, dt / T(2), k2);
-    adj_stage_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k2, dt / T(2), k3);
+    adj_stage_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, (const T*)nullptr, T(0), k1);
+    adj_stage_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k1, dt / T(2), k2);
+    adj_stage_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k2, dt / T(2), k3);
     // stage 4 (state f + dt k3)
     adj_axpby_kernel<T><<<eb, 256, 0, st>>>(n, a, dt / T(6), lam, T(0), (const T*)nullptr);
-    adj_vjp_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k3, dt, a, gs, c->dtau_part);
+    adj_vjp_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k3, dt, a, gs, c->dtau_part);
     if (dtau) adj_sum_kernel<<<1, kAdjThreads, 0, st>>>(c->dtau_part, P.Nq1, dtau);
     adj_axpby_kernel<T><<<eb, 256, 0, st>>>(n, gacc, T(1), lam, T(1), gs);
     // stage 3 (state f + dt/2 k2)
     adj_axpby_kernel<T><<<eb, 256, 0, st>>>(n, a, dt / T(3), lam, dt, gs);
-    adj_vjp_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k2, dt / T(2), a, gs, c->dtau_part);
+    adj_vjp_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k2, dt / T(2), a, gs, c->dtau_part);
     if (dtau) adj_sum_kernel<<<1, kAdjThreads, 0, st>>>(c->dtau_part, P.Nq1, dtau);
     adj_axpby_kernel<T><<<eb, 256, 0, st>>>(n, gacc, T(1), gacc, T(1), gs);
     // stage 2 (state f + dt/2 k1)
     adj_axpby_kernel<T><<<eb, 256, 0, st>>>(n, a, dt / T(3), lam, dt / T(2), gs);
-    adj_vjp_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k1, dt / T(2), a, gs, c->dtau_part);
+    adj_vjp_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, k1, dt / T(2), a, gs, c->dtau_part);
     if (dtau) adj_sum_kernel<<<1, kAdjThreads, 0, st>>>(c->dtau_part, P.Nq1, dtau);
     adj_axpby_kernel<T><<<eb, 256, 0, st>>>(n, gacc, T(1), gacc, T(1), gs);
     // stage 1 (state f)
     adj_axpby_kernel<T><<<eb, 256, 0, st>>>(n, a, dt / T(6), lam, dt / T(2), gs);
-    adj_vjp_kernel<T><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, (const T*)nullptr, T(0), a, gs,
+    adj_vjp_kernel<T, R><<<P.Nq1, kAdjThreads, 0, st>>>(P, f, (const T*)nullptr, T(0), a, gs,
                                                      c->dtau_part);
     if (dtau) adj_sum_kernel<<<1, kAdjThreads, 0, st>>>(c->dtau_part, P.Nq1, dtau);
     adj_axpby_kernel<T><<<eb, 256, 0, st>>>(n, lam, T(1), gacc, T(1), gs);
@@ -138,9 +139,11 @@ int bolt_adj1d_create(const BoltAdj1DSpec* s, int dtype, BoltAdj1D** out) {
         !(s->p1_end > s->p1_start) || !(s->dp2 > 0) || !(s->dp3 > 0) || !(s->mass > 0) ||
         !(s->boltzmann_constant > 0) || !(s->dt > 0) || s->tau < 0)
         return BOLT_ERR_ARG;
+    if (s->recon != BOLT_RECON_WENO5 && s->recon != BOLT_RECON_MINMOD) return BOLT_ERR_UNSUPPORTED;
     BoltAdj1D* c = new (std::nothrow) BoltAdj1D();
     if (!c) return BOLT_ERR_NOMEM;
     c->dtype = dtype;
+    c->recon = s->recon == BOLT_RECON_MINMOD ? kAdjMinmod : kAdjWeno5;
     c->dt = s->dt;
     c->n = (long long)s->N_q1 * s->N_p1;
     Adj1DArgs& P = c->P;
@@ -185,17 +188,28 @@ int bolt_adj1d_set_tau(BoltAdj1D* c, double tau) {
 int bolt_adj1d_step(BoltAdj1D* c, void* f, double* J_dev, void* stream) {
     if (!c || !f) return BOLT_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    return c->dtype == BOLT_F64 ? step_impl<double>(c, (double*)f, J_dev, st)
-                                : step_impl<float>(c, (float*)f, J_dev, st);
+    if (c->recon == kAdjMinmod)
+        return c->dtype == BOLT_F64 ? step_impl<double, kAdjMinmod>(c, (double*)f, J_dev, st)
+                                    : step_impl<float, kAdjMinmod>(c, (float*)f, J_dev, st);
+    return c->dtype == BOLT_F64 ? step_impl<double, kAdjWeno5>(c, (double*)f, J_dev, st)
+                                : step_impl<float, kAdjWeno5>(c, (float*)f, J_dev, st);
 }
 
 int bolt_adj1d_step_adjoint(BoltAdj1D* c, const void* f_n, void* lam, int objective_at_start,
                             double* dtau_dev, void* stream) {
     if (!c || !f_n || !lam) return BOLT_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
+    if (c->recon == kAdjMinmod)
+        return c->dtype == BOLT_F64
+            ? adjoint_impl<double, kAdjMinmod>(c, (const double*)f_n, (double*)lam,
+                                               objective_at_start, dtau_dev, st)
+            : adjoint_impl<float, kAdjMinmod>(c, (const float*)f_n, (float*)lam,
+                                              objective_at_start, dtau_dev, st);
     return c->dtype == BOLT_F64
-        ? adjoint_impl<double>(c, (const double*)f_n, (double*)lam, objective_at_start, dtau_dev, st)
-        : adjoint_impl<float>(c, (const float*)f_n, (float*)lam, objective_at_start, dtau_dev, st);
+        ? adjoint_impl<double, kAdjWeno5>(c, (const double*)f_n, (double*)lam,
+                                          objective_at_start, dtau_dev, st)
+        : adjoint_impl<float, kAdjWeno5>(c, (const float*)f_n, (float*)lam,
+                                         objective_at_start, dtau_dev, st);
 }
 
 int bolt_adj1d_objective(BoltAdj1D* c, const void* f, double* J_dev, void* lam, void* stream) {

@@ -275,11 +275,13 @@ int  bolt_batch_get_schedule(const BoltBatch* b, int* tile_cells, int* ctas, int
  * Adjoint of the 1D1V update.  No reference counterpart: Bolt has no
  * differentiation.  The forward step is the same scheme as bolt_step for a
  * 1D1V system (df_dt_fvm.py:56-97 with the WENO5 of weno5.py:4-98 including
- * its eps (1 + |a| + |b| + |c|), upwind/LLF faces, BGK with p_dim = 1,
- * RK4 of integrators.py:15-28), on f[N_q1][N_p1] (p1 fastest) with periodic
- * q1 and no ghost storage.  The adjoint step is hand-written: exact
- * derivatives of the WENO5 nonlinear weights, of the Maxwellian through the
- * velocity moments and of tau (see bolt_adj1d_step_adjoint).  Objective:
+ * its eps (1 + |a| + |b| + |c|) or the minmod of minmod.py:4-71, upwind/LLF
+ * faces, BGK with p_dim = 1, RK4 of integrators.py:15-28), on f[N_q1][N_p1]
+ * (p1 fastest) with periodic q1 and no ghost storage.  The adjoint step is
+ * hand-written: exact derivatives of the WENO5 nonlinear weights (a
+ * subgradient of the minmod limiter: the passed argument gets derivative 1),
+ * of the Maxwellian through the velocity moments and of tau (see
+ * bolt_adj1d_step_adjoint).  Objective:
  * J = sum over steps n >= 1 of dt |nhat_1(f_n)|^2, nhat_1 the k = 1 Fourier
  * coefficient (1/N_q1) sum_i n_i exp(-2 pi i x_i / L) of the density.
  * ------------------------------------------------------------------------ */
@@ -291,6 +293,8 @@ typedef struct BoltAdj1DSpec {
     double mass, boltzmann_constant;
     double tau;                    /* BGK collision time; 0 = collisionless */
     double dt;
+    int recon;                     /* BOLT_RECON_WENO5, or BOLT_RECON_MINMOD
+                                      (differentiated by a subgradient)   */
 } BoltAdj1DSpec;
 
 typedef struct BoltAdj1D BoltAdj1D;

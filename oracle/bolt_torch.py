@@ -7,6 +7,7 @@ p_dim = 1, one species, fields off):
   * reconstruct_weno5 (bolt/lib/nonlinear/finite_volume/reconstruction/
     weno5.py:17-96): circular shifts along q, smoothness indicators with
     eps * (1 + |a| + |b| + |c|), weights c/(16 beta^2) style, normalised sums;
+    or reconstruct_minmod (minmod.py:4-71);
   * riemann_solver (riemann.py:46-49): left state where the velocity is
     positive, right state otherwise (the LLF flux with alpha = |v| equals it);
   * the q-flux divergence of df_dt_fvm.py:56-89, -(F_i+1/2 - F_i-1/2)/dq1;
@@ -53,11 +54,33 @@ def weno5_faces(f):
     return left, right
 
 
+def minmod_faces(f):
+    """(left_value, right_value) of every cell along dim 0 with the minmod
+    limited slope of minmod.py:4-71 (theta = 2, sign(0) = +1).  The slope is
+    written as the passed argument itself (the first of equal magnitudes)
+    where the three arguments share a sign, else 0 -- the same values as the
+    reference's 0.25 |sx + sy| (sx + sz) min|.|, and the subgradient autograd
+    takes through it is the hand-written adjoint's."""
+    bwd = f - torch.roll(f, 1, 0)
+    fwd = torch.roll(f, -1, 0) - f
+    cen = bwd + fwd
+    x0, x1, x2 = 2 * bwd, 0.5 * cen, 2 * fwd
+    a0, a1, a2 = x0.abs().detach(), x1.abs().detach(), x2.abs().detach()
+    m = torch.minimum(torch.minimum(a0, a1), a2)
+    sel = torch.where(a0 == m, x0, torch.where(a1 == m, x1, x2))
+    neg0, neg1, neg2 = x0.detach() < 0, x1.detach() < 0, x2.detach() < 0
+    agree = (neg0 == neg1) & (neg0 == neg2)
+    slope = torch.where(agree, sel, torch.zeros_like(sel))
+    return f - 0.5 * slope, f + 0.5 * slope
+
+
 class Problem1D1V(object):
     """Grid and constants of one 1D1V run (p1 centres v, dp2 = dp3 given)."""
 
     def __init__(self, N_q1, N_p1, p1_start, p1_end, dt, tau, mass=1.0, kB=1.0,
-                 q1_start=0.0, q1_end=1.0, dp2=1.0, dp3=1.0, device='cpu'):
+                 q1_start=0.0, q1_end=1.0, dp2=1.0, dp3=1.0, device='cpu',
+                 reconstruction='weno5'):
+        self.faces = minmod_faces if reconstruction == 'minmod' else weno5_faces
         self.N_q1, self.N_p1 = N_q1, N_p1
         self.dq1 = (q1_end - q1_start) / N_q1
         self.dp1 = (p1_end - p1_start) / N_p1
@@ -70,7 +93,7 @@ class Problem1D1V(object):
 
     def dfdt(self, f, tau):
         v = self.v[None, :]
-        left, right = weno5_faces(f)
+        left, right = self.faces(f)
         # state at face i+1/2: right value of cell i (v > 0) or left value of cell i+1
         face = torch.where(v > 0, right, torch.roll(left, -1, 0))
         F = v * face

@@ -139,3 +139,42 @@ def test_fp32_gradient_close_to_fp64():
     g32, t32 = roll('fp32').gradient(f0)
     assert float((g32.double() - g64).norm() / g64.norm()) < 1e-3
     assert abs(float(t32) - float(t64)) < 2e-2 * abs(float(t64))
+
+
+def test_minmod_adjoint_subgradient():
+    """reconstruction='minmod': the forward equals the transcription's (1e-12),
+    the hand-written subgradient equals autograd of the transcription, whose
+    minmod routes the derivative through the same passed argument (1e-9 for
+    dJ/da, dJ/dtau and dJ/df0), and the derivatives in a and tau match
+    central differences to 1e-3 (J is only piecewise smooth: a kink of the
+    limiter inside the +-h interval costs O(h))."""
+    from bolt_b200.adjoint import Rollout1D1V, rollout
+    from oracle.bolt_torch import Problem1D1V
+    r = Rollout1D1V(NQ, NP, P0, P1, DT, TAU, STEPS, snapshots=4, precision='fp64',
+                    reconstruction='minmod')
+    pr = Problem1D1V(NQ, NP, P0, P1, DT, TAU, device='cuda', reconstruction='minmod')
+    f0 = f_init(AMP, 'cuda')
+    J, fN = r.forward(f0)
+    Jt, ft = pr.objective(f0, torch.tensor(TAU, dtype=torch.float64, device='cuda'), STEPS)
+    assert abs(float(J) - float(Jt)) < 1e-12 * abs(float(Jt))
+    assert float((fN - ft).norm() / ft.norm()) < 1e-12
+
+    a = torch.tensor(AMP, dtype=torch.float64, device='cuda', requires_grad=True)
+    tau = torch.tensor(TAU, dtype=torch.float64, device='cuda', requires_grad=True)
+    rollout(f_init(a, 'cuda'), tau, r).backward()
+    gf, _ = r.gradient(f0)
+    a2 = torch.tensor(AMP, dtype=torch.float64, device='cuda', requires_grad=True)
+    tau2 = torch.tensor(TAU, dtype=torch.float64, device='cuda', requires_grad=True)
+    f02 = f_init(a2, 'cuda')
+    f02.retain_grad()
+    pr.objective(f02, tau2, STEPS)[0].backward()
+    assert abs(float(a.grad) - float(a2.grad)) < 1e-9 * abs(float(a2.grad))
+    assert abs(float(tau.grad) - float(tau2.grad)) < 1e-9 * abs(float(tau2.grad))
+    assert float((gf - f02.grad).norm() / f02.grad.norm()) < 1e-9
+
+    h = 1e-4
+    Jf = lambda amp, t: float(r.forward(f_init(amp, 'cuda'), t)[0])
+    fd_a = (Jf(AMP * (1 + h), TAU) - Jf(AMP * (1 - h), TAU)) / (2 * AMP * h)
+    fd_tau = (Jf(AMP, TAU * (1 + h)) - Jf(AMP, TAU * (1 - h))) / (2 * TAU * h)
+    assert abs(float(a.grad) - fd_a) < 1e-3 * abs(fd_a)
+    assert abs(float(tau.grad) - fd_tau) < 1e-3 * abs(fd_tau)
