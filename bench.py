@@ -313,6 +313,9 @@ def run_ours(args, rank, world, local_rank):
     ms = ev0.elapsed_time(ev1) / args.steps
     launches = nls.launch_count() - launches0
     torch.cuda.synchronize()
+    # density and energy after warmup + steps, for the FP32-vs-FP64 check
+    g = spec['N_ghost']
+    mom32 = {k: nls.compute_moments(k)[..., g:-g, g:-g].clone() for k in ('density', 'energy')}
     ms = max_over_ranks(ms, world)
     if world > 1:
         dist.barrier()
@@ -404,8 +407,18 @@ def run_ours(args, rank, world, local_rank):
         a1.record()
         a1.synchronize()
         ms64 = max_over_ranks(a0.elapsed_time(a1) / n64, world)
+        # untimed steps up to the FP32 run's count, then the relative L2
+        # error of the FP32 result's density and energy against FP64
+        for _ in range(args.steps - n64):
+            nls64.strang_timestep(dt)
+        err = {}
+        for k, v32 in mom32.items():
+            v64 = nls64.compute_moments(k)[..., g:-g, g:-g]
+            err[k] = float((v32 - v64).norm() / v64.norm())
         fp64 = {'value': job_value(cells, world, ms64), 'ms_per_step': ms64,
-                'bytes_per_cell_update': 136}
+                'bytes_per_cell_update': 136,
+                'fp32_rel_l2_error_vs_fp64': err,
+                'error_after_steps': args.warmup + args.steps}
         del nls64
 
     if rank != 0:
