@@ -32,6 +32,8 @@
 // One CTA per q-cell, threads over p (block reductions in FP64).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "fvm_common.cuh"
 
 namespace bolt {
@@ -207,12 +209,11 @@ __device__ __forceinline__ double adj_f0(const Adj1DArgs& P, const AdjMaxwell& M
 // periodic q-neighbour row
 __device__ __forceinline__ int adj_wrap(int i, int n) { return ((i % n) + n) % n; }
 
-// k_out = L(f + c k_in) (k_in may be null), one CTA per q-cell
+// row i of k_out = L(f + c k_in) (k_in may be null), by one CTA
 template <typename T, int RECON>
-__global__ void __launch_bounds__(kAdjThreads)
-adj_stage_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, T* k_out) {
-    __shared__ double red[kAdjThreads / 32];
-    const int i = blockIdx.x, Np = P.Np1, Nq = P.Nq1;
+__device__ __forceinline__ void adj_stage_cell(const Adj1DArgs& P, const T* f, const T* k_in,
+                                               T c, T* k_out, int i, double* red) {
+    const int Np = P.Np1, Nq = P.Nq1;
     auto g = [&](int q, int p) -> T {
         const long long o = (long long)adj_wrap(q, Nq) * Np + p;
         return k_in ? f[o] + c * k_in[o] : f[o];
@@ -247,6 +248,14 @@ adj_stage_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, T* k_out) {
     }
 }
 
+// k_out = L(f + c k_in), one CTA per q-cell
+template <typename T, int RECON>
+__global__ void __launch_bounds__(kAdjThreads)
+adj_stage_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, T* k_out) {
+    __shared__ double red[kAdjThreads / 32];
+    adj_stage_cell<T, RECON>(P, f, k_in, c, k_out, blockIdx.x, red);
+}
+
 // f <- f + dt/6 (k1 + 2 k2 + 2 k3 + k4)
 template <typename T>
 __global__ void adj_combine_kernel(long long n, T* f, const T* k1, const T* k2, const T* k3,
@@ -258,21 +267,25 @@ __global__ void adj_combine_kernel(long long n, T* f, const T* k1, const T* k2, 
 
 // density n_i = dp sum_p f (FP64), one CTA per q-cell
 template <typename T>
-__global__ void __launch_bounds__(kAdjThreads)
-adj_density_kernel(const Adj1DArgs P, const T* f, double* dens) {
-    __shared__ double red[kAdjThreads / 32];
-    const int i = blockIdx.x;
+__device__ __forceinline__ void adj_density_cell(const Adj1DArgs& P, const T* f, double* dens,
+                                                 int i, double* red) {
     double s = 0;
     for (int p = threadIdx.x; p < P.Np1; p += kAdjThreads) s += f[(long long)i * P.Np1 + p];
     s = adj_block_sum(s, red);
     if (threadIdx.x == 0) dens[i] = s * P.measure;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kAdjThreads)
+adj_density_kernel(const Adj1DArgs P, const T* f, double* dens) {
+    __shared__ double red[kAdjThreads / 32];
+    adj_density_cell<T>(P, f, dens, blockIdx.x, red);
+}
+
 // J += w |nhat_1|^2, nhat_1 = (1/N_q1) sum_i n_i exp(-2 pi i x_i / L) over the
 // cell centres; also stores (Re, Im) for the adjoint.  One CTA.
-__global__ void __launch_bounds__(kAdjThreads)
-adj_mode_kernel(const Adj1DArgs P, const double* dens, double w, double* J, double* reim) {
-    __shared__ double red[kAdjThreads / 32];
+__device__ __forceinline__ void adj_mode_block(const Adj1DArgs& P, const double* dens, double w,
+                                               double* J, double* reim, double* red) {
     double re = 0, im = 0;
     for (int i = threadIdx.x; i < P.Nq1; i += kAdjThreads) {
         const double th = 2.0 * 3.141592653589793 * (i + 0.5) / P.Nq1;
@@ -287,26 +300,36 @@ adj_mode_kernel(const Adj1DArgs P, const double* dens, double w, double* J, doub
     }
 }
 
+__global__ void __launch_bounds__(kAdjThreads)
+adj_mode_kernel(const Adj1DArgs P, const double* dens, double w, double* J, double* reim) {
+    __shared__ double red[kAdjThreads / 32];
+    adj_mode_block(P, dens, w, J, reim, red);
+}
+
 // lam += w d|nhat_1|^2 / df (reim from adj_mode_kernel on the same f)
+template <typename T>
+__device__ __forceinline__ void adj_mode_adjoint_at(const Adj1DArgs& P, const double* reim,
+                                                    double w, T* lam, long long e) {
+    const int i = int(e / P.Np1);
+    const double th = 2.0 * 3.141592653589793 * (i + 0.5) / P.Nq1;
+    const double dn = (2.0 / P.Nq1) * (reim[0] * cos(th) - reim[1] * sin(th));
+    lam[e] = lam[e] + T(w * dn * P.measure);
+}
+
 template <typename T>
 __global__ void adj_mode_adjoint_kernel(const Adj1DArgs P, const double* reim, double w, T* lam) {
     const long long n = (long long)P.Nq1 * P.Np1;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int i = int(e / P.Np1);
-        const double th = 2.0 * 3.141592653589793 * (i + 0.5) / P.Nq1;
-        const double dn = (2.0 / P.Nq1) * (reim[0] * cos(th) - reim[1] * sin(th));
-        lam[e] = lam[e] + T(w * dn * P.measure);
-    }
+         e += (long long)gridDim.x * blockDim.x)
+        adj_mode_adjoint_at<T>(P, reim, w, lam, e);
 }
 
-// out = L'(g)^T a at g = f + c k_in; dtau_part[i] = sum_p a (-(f0 - g)/tau^2)
-template <typename T, int RECON>
-__global__ void __launch_bounds__(kAdjThreads)
-adj_vjp_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, const T* a, T* out,
-               double* dtau_part) {
-    __shared__ double red[kAdjThreads / 32];
-    const int j = blockIdx.x, Np = P.Np1, Nq = P.Nq1;
+// Row j of L'(g)^T a at g = f + c k_in: epi(o, value) receives every element
+// (o its offset); returns sum_p a (-(f0 - g)/tau^2) of the row (thread 0)
+template <typename T, int RECON, typename Epi>
+__device__ __forceinline__ double adj_vjp_cell(const Adj1DArgs& P, const T* f, const T* k_in, T c,
+                                               const T* a, int j, double* red, Epi epi) {
+    const int Np = P.Np1, Nq = P.Nq1;
     auto g = [&](int q, int p) -> T {
         const long long o = (long long)adj_wrap(q, Nq) * Np + p;
         return k_in ? f[o] + c * k_in[o] : f[o];
@@ -344,9 +367,6 @@ adj_vjp_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, const T* a, T*
         Su = adj_block_sum(Su, red);
         ST = adj_block_sum(ST, red);
         St = adj_block_sum(St, red);
-        if (threadIdx.x == 0) dtau_part[j] = St;
-    } else if (threadIdx.x == 0) {
-        dtau_part[j] = 0.0;
     }
     // (n, u, T) as functions of the raw sums (m0, m1, m2)
     const double meas = P.measure, m = P.mass, N = M.N;
@@ -381,7 +401,148 @@ adj_vjp_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, const T* a, T*
         double r = double(acc);
         if (bgk)
             r += (-double(ad(j, p)) + (G0 + G1 * vd + G2 * 0.5 * vd * vd)) / P.tau;
-        out[(long long)j * Np + p] = T(r);
+        epi((long long)j * Np + p, T(r));
+    }
+    return St;
+}
+
+// out = L'(g)^T a at g = f + c k_in; dtau_part[j] = sum_p a (-(f0 - g)/tau^2)
+template <typename T, int RECON>
+__global__ void __launch_bounds__(kAdjThreads)
+adj_vjp_kernel(const Adj1DArgs P, const T* f, const T* k_in, T c, const T* a, T* out,
+               double* dtau_part) {
+    __shared__ double red[kAdjThreads / 32];
+    const double St = adj_vjp_cell<T, RECON>(P, f, k_in, c, a, blockIdx.x, red,
+                                             [&](long long o, T v) { out[o] = v; });
+    if (threadIdx.x == 0) dtau_part[blockIdx.x] = St;
+}
+
+// ---------------------------------------------------------------------------
+// Whole steps as single cooperative launches.  A 1D1V step is a chain of
+// small dependent passes (4 stages and the combine forward; 3 stages, 4 VJPs
+// and their combines backward), each a few microseconds of work over
+// N_q1 x N_p1 cells; one launch per step, with grid-wide barriers between the
+// passes, removes the launch gaps between them.  The grid never exceeds the
+// co-resident CTAs (cudaLaunchCooperativeKernel refuses otherwise) and CTAs
+// take q-rows by a grid-stride loop.  The passes are the per-row functions of
+// the separate kernels above, in the same order, so the results are the same.
+// ---------------------------------------------------------------------------
+template <typename T, int RECON>
+__global__ void __launch_bounds__(kAdjThreads)
+adj_step_coop_kernel(const Adj1DArgs P, T* f, T* k1, T* k2, T* k3, T* k4, T dt, double* J,
+                     double* dens, double Jw) {
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    __shared__ double red[kAdjThreads / 32];
+    const int Nq = P.Nq1, Np = P.Np1;
+    for (int i = blockIdx.x; i < Nq; i += gridDim.x)
+        adj_stage_cell<T, RECON>(P, f, (const T*)nullptr, T(0), k1, i, red);
+    grid.sync();
+    for (int i = blockIdx.x; i < Nq; i += gridDim.x)
+        adj_stage_cell<T, RECON>(P, f, k1, dt / T(2), k2, i, red);
+    grid.sync();
+    for (int i = blockIdx.x; i < Nq; i += gridDim.x)
+        adj_stage_cell<T, RECON>(P, f, k2, dt / T(2), k3, i, red);
+    grid.sync();
+    for (int i = blockIdx.x; i < Nq; i += gridDim.x)
+        adj_stage_cell<T, RECON>(P, f, k3, dt, k4, i, red);
+    grid.sync();
+    const T dt6 = dt / T(6);
+    for (int i = blockIdx.x; i < Nq; i += gridDim.x)
+        for (int p = threadIdx.x; p < Np; p += kAdjThreads) {
+            const long long e = (long long)i * Np + p;
+            f[e] = f[e] + dt6 * (((k1[e] + T(2) * k2[e]) + T(2) * k3[e]) + k4[e]);
+        }
+    if (J) {
+        grid.sync();
+        for (int i = blockIdx.x; i < Nq; i += gridDim.x) adj_density_cell<T>(P, f, dens, i, red);
+        grid.sync();
+        if (blockIdx.x == 0) adj_mode_block(P, dens, Jw, J, nullptr, red);
+    }
+}
+
+// adjoint of one step (the order of bolt_adj1d_step_adjoint's separate
+// launches): A and B alternate as the stage adjoint fields a_s; part holds
+// the four stages' per-row dJ/dtau terms, summed in stage order at the end
+template <typename T, int RECON>
+__global__ void __launch_bounds__(kAdjThreads)
+adj_step_adjoint_coop_kernel(const Adj1DArgs P, const T* f, T* lam, T* k1, T* k2, T* k3, T* A,
+                             T* B, T* gacc, T dt, double* part, double* dtau, int obj_at_start,
+                             double* dens, double* reim, double wobj) {
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    __shared__ double red[kAdjThreads / 32];
+    const int Nq = P.Nq1, Np = P.Np1;
+    // recompute the stages from f
+    for (int i = blockIdx.x; i < Nq; i += gridDim.x)
+        adj_stage_cell<T, RECON>(P, f, (const T*)nullptr, T(0), k1, i, red);
+    grid.sync();
+    for (int i = blockIdx.x; i < Nq; i += gridDim.x)
+        adj_stage_cell<T, RECON>(P, f, k1, dt / T(2), k2, i, red);
+    grid.sync();
+    for (int i = blockIdx.x; i < Nq; i += gridDim.x) {
+        adj_stage_cell<T, RECON>(P, f, k2, dt / T(2), k3, i, red);
+        for (int p = threadIdx.x; p < Np; p += kAdjThreads) {     // a4 = dt/6 lam
+            const long long e = (long long)i * Np + p;
+            A[e] = (dt / T(6)) * lam[e];
+        }
+    }
+    grid.sync();
+    // stage 4 (state f + dt k3): gacc = lam + g4, a3 = dt/3 lam + dt g4
+    for (int j = blockIdx.x; j < Nq; j += gridDim.x) {
+        const double St = adj_vjp_cell<T, RECON>(P, f, k3, dt, A, j, red, [&](long long e, T g) {
+            gacc[e] = T(1) * lam[e] + T(1) * g;
+            B[e] = (dt / T(3)) * lam[e] + dt * g;
+        });
+        if (threadIdx.x == 0) part[j] = St;
+    }
+    grid.sync();
+    // stage 3 (state f + dt/2 k2): gacc += g3, a2 = dt/3 lam + dt/2 g3
+    for (int j = blockIdx.x; j < Nq; j += gridDim.x) {
+        const double St = adj_vjp_cell<T, RECON>(P, f, k2, dt / T(2), B, j, red,
+                                                 [&](long long e, T g) {
+            gacc[e] = T(1) * gacc[e] + T(1) * g;
+            A[e] = (dt / T(3)) * lam[e] + (dt / T(2)) * g;
+        });
+        if (threadIdx.x == 0) part[Nq + j] = St;
+    }
+    grid.sync();
+    // stage 2 (state f + dt/2 k1): gacc += g2, a1 = dt/6 lam + dt/2 g2
+    for (int j = blockIdx.x; j < Nq; j += gridDim.x) {
+        const double St = adj_vjp_cell<T, RECON>(P, f, k1, dt / T(2), A, j, red,
+                                                 [&](long long e, T g) {
+            gacc[e] = T(1) * gacc[e] + T(1) * g;
+            B[e] = (dt / T(6)) * lam[e] + (dt / T(2)) * g;
+        });
+        if (threadIdx.x == 0) part[2 * Nq + j] = St;
+    }
+    grid.sync();
+    // stage 1 (state f): lam = gacc + g1
+    for (int j = blockIdx.x; j < Nq; j += gridDim.x) {
+        const double St = adj_vjp_cell<T, RECON>(P, f, (const T*)nullptr, T(0), B, j, red,
+                                                 [&](long long e, T g) {
+            lam[e] = T(1) * gacc[e] + T(1) * g;
+        });
+        if (threadIdx.x == 0) part[3 * Nq + j] = St;
+    }
+    if (dtau || obj_at_start) grid.sync();
+    if (dtau && blockIdx.x == 0) {
+        for (int s = 0; s < 4; ++s) {
+            double v = 0;
+            for (int i = threadIdx.x; i < Nq; i += kAdjThreads) v += part[s * Nq + i];
+            v = adj_block_sum(v, red);
+            if (threadIdx.x == 0) *dtau += v;
+        }
+    }
+    if (obj_at_start) {
+        for (int i = blockIdx.x; i < Nq; i += gridDim.x) adj_density_cell<T>(P, f, dens, i, red);
+        grid.sync();
+        if (blockIdx.x == 0) adj_mode_block(P, dens, 0.0, reim + 2, reim, red);
+        grid.sync();
+        const long long n = (long long)Nq * Np;
+        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+             e += (long long)gridDim.x * blockDim.x)
+            adj_mode_adjoint_at<T>(P, reim, wobj, lam, e);
     }
 }
 

@@ -12,6 +12,7 @@
 // lam at every step boundary it sees.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <new>
 
 #include "../../include/bolt_b200.h"
@@ -28,10 +29,12 @@ struct BoltAdj1D {
     void* k[4];
     void* a;
     void* gacc;              // running lam + sum g
-    void* gs;                // one stage's g
-    double* dtau_part;       // [N_q1]
+    void* gs;                // one stage's g (the second stage adjoint field of the
+                             // cooperative step)
+    double* dtau_part;       // [4][N_q1]
     double* dens;            // [N_q1]
-    double* reim;            // [2]
+    double* reim;            // [3]
+    int coop_grid;           // CTAs of the cooperative whole-step launches (0: separate launches)
 };
 
 namespace {
@@ -56,8 +59,58 @@ int ew_blocks(long long n) {
     return (int)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
 }
 
+// CTAs the cooperative step kernels may use (every one co-resident), or 0
+// when the device has no cooperative launch
+template <typename T, int R>
+int coop_grid_for(int Nq1) {
+    int dev = 0, coop = 0, sms = 0, per_a = 0, per_b = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (!coop || sms <= 0) return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_a, adj_step_coop_kernel<T, R>,
+                                                  kAdjThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_b, adj_step_adjoint_coop_kernel<T, R>,
+                                                  kAdjThreads, 0);
+    const int per = per_a < per_b ? per_a : per_b;
+    if (per <= 0) return 0;
+    return Nq1 < sms * per ? Nq1 : sms * per;
+}
+
+template <typename T, int R>
+int step_coop(BoltAdj1D* c, T* f, double* J, cudaStream_t st) {
+    Adj1DArgs P = c->P;
+    T* k1 = (T*)c->k[0]; T* k2 = (T*)c->k[1]; T* k3 = (T*)c->k[2]; T* k4 = (T*)c->k[3];
+    T dt = T(c->dt);
+    double* dens = c->dens;
+    double Jw = c->dt;
+    void* args[] = {&P, &f, &k1, &k2, &k3, &k4, &dt, &J, &dens, &Jw};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)adj_step_coop_kernel<T, R>,
+                                                dim3(c->coop_grid), dim3(kAdjThreads), args, 0, st);
+    return e == cudaSuccess ? BOLT_OK : BOLT_ERR_CUDA;
+}
+
+template <typename T, int R>
+int adjoint_coop(BoltAdj1D* c, const T* f, T* lam, int obj_at_start, double* dtau,
+                 cudaStream_t st) {
+    Adj1DArgs P = c->P;
+    T* k1 = (T*)c->k[0]; T* k2 = (T*)c->k[1]; T* k3 = (T*)c->k[2];
+    T* A = (T*)c->a; T* B = (T*)c->gs; T* gacc = (T*)c->gacc;
+    T dt = T(c->dt);
+    double* part = c->dtau_part;
+    double* dens = c->dens;
+    double* reim = c->reim;
+    double wobj = c->dt;
+    void* args[] = {&P, &f, &lam, &k1, &k2, &k3, &A, &B, &gacc, &dt, &part, &dtau,
+                    &obj_at_start, &dens, &reim, &wobj};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)adj_step_adjoint_coop_kernel<T, R>,
+                                                dim3(c->coop_grid), dim3(kAdjThreads), args, 0, st);
+    return e == cudaSuccess ? BOLT_OK : BOLT_ERR_CUDA;
+}
+
 template <typename T, int R>
 int step_impl(BoltAdj1D* c, T* f, double* J, cudaStream_t st) {
+    if (c->coop_grid > 0) return step_coop<T, R>(c, f, J, st);
     const Adj1DArgs& P = c->P;
     const T dt = T(c->dt);
     T* k1 = (T*)c->k[0]; T* k2 = (T*)c->k[1]; T* k3 = (T*)c->k[2]; T* k4 = (T*)c->k[3];
@@ -76,6 +129,7 @@ int step_impl(BoltAdj1D* c, T* f, double* J, cudaStream_t st) {
 template <typename T, int R>
 int adjoint_impl(BoltAdj1D* c, const T* f, T* lam, int obj_at_start, double* dtau,
                  cudaStream_t st) {
+    if (c->coop_grid > 0) return adjoint_coop<T, R>(c, f, lam, obj_at_start, dtau, st);
     const Adj1DArgs& P = c->P;
     const T dt = T(c->dt);
     const long long n = c->n;
@@ -166,12 +220,21 @@ int bolt_adj1d_create(const BoltAdj1DSpec* s, int dtype, BoltAdj1D** out) {
     alloc(&c->a, c->n * eb);
     alloc(&c->gacc, c->n * eb);
     alloc(&c->gs, c->n * eb);
-    alloc((void**)&c->dtau_part, s->N_q1 * sizeof(double));
+    alloc((void**)&c->dtau_part, 4 * (size_t)s->N_q1 * sizeof(double));
     alloc((void**)&c->dens, s->N_q1 * sizeof(double));
     alloc((void**)&c->reim, 3 * sizeof(double));
     if (rc != BOLT_OK) {
         adj_free(c);
         return rc;
+    }
+    // whole steps as cooperative launches unless BOLT_ADJ_SEPARATE is set
+    if (!getenv("BOLT_ADJ_SEPARATE")) {
+        if (dtype == BOLT_F64)
+            c->coop_grid = c->recon == kAdjMinmod ? coop_grid_for<double, kAdjMinmod>(P.Nq1)
+                                                  : coop_grid_for<double, kAdjWeno5>(P.Nq1);
+        else
+            c->coop_grid = c->recon == kAdjMinmod ? coop_grid_for<float, kAdjMinmod>(P.Nq1)
+                                                  : coop_grid_for<float, kAdjWeno5>(P.Nq1);
     }
     *out = c;
     return BOLT_OK;

@@ -178,3 +178,26 @@ def test_minmod_adjoint_subgradient():
     fd_tau = (Jf(AMP, TAU * (1 + h)) - Jf(AMP, TAU * (1 - h))) / (2 * TAU * h)
     assert abs(float(a.grad) - fd_a) < 1e-3 * abs(fd_a)
     assert abs(float(tau.grad) - fd_tau) < 1e-3 * abs(fd_tau)
+
+
+@pytest.mark.parametrize('precision,tol,tol_tau', [('fp64', 1e-10, 1e-9), ('fp32', 1e-5, 2e-2)])
+def test_cooperative_steps_match_separate_launches(monkeypatch, precision, tol, tol_tau):
+    """Whole RK4 steps and step adjoints as single cooperative launches
+    (the default) against the same passes as separate launches
+    (BOLT_ADJ_SEPARATE): J, f_N and the gradients agree to rounding (the
+    fused epilogues may contract the elementwise combines into FMAs where the
+    separate axpby launches do not; 60 adjoint steps through the WENO weight
+    derivatives amplify that to ~1e-11 in FP64; dJ/dtau in FP32 is a strongly
+    cancelled sum, see test_fp32_gradient_close_to_fp64)."""
+    f0 = f_init(AMP, 'cuda')
+    coop = roll(precision)
+    Jc, fc = coop.forward(f0)
+    gc, tc = coop.gradient(f0)
+    monkeypatch.setenv('BOLT_ADJ_SEPARATE', '1')
+    sep = roll(precision)
+    Js, fs = sep.forward(f0)
+    gs, ts = sep.gradient(f0)
+    assert abs(float(Jc) - float(Js)) <= tol * abs(float(Js))
+    assert float((fc - fs).norm() / fs.norm()) <= tol
+    assert float((gc - gs).norm() / gs.norm()) <= tol
+    assert abs(float(tc) - float(ts)) <= tol_tau * abs(float(ts))
