@@ -545,7 +545,7 @@ static int launch_pstage(BoltCtx* ctx, const StageIO& io, const void* kq, cudaSt
     a.periodic1 = io.base1 != nullptr && ctx->p.bc_q1 == BOLT_BC_PERIODIC && g.N_ghost > 0;
     a.periodic2 = io.base1 != nullptr && ctx->p.bc_q2 == BOLT_BC_PERIODIC && g.N_ghost > 0;
     a.sg = ctx->sg;
-    const size_t smem = pstage_smem(ctx->Np, ctx->elem);
+    const size_t smem = pstage_smem(ctx->Np, ctx->elem, g.N_p1 + g.N_p2 + g.N_p3);
     if (smem > 200 * 1024) return BOLT_ERR_UNSUPPORTED;
     dim3 grid(g.N_q1 * g.N_q2, g.N_s);
     cudaError_t e = ctx->elem == 8 ? launch_pstage_f64(a, ctx->recon_p, grid, smem, st)

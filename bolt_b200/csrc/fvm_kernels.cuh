@@ -541,18 +541,39 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
 // combine and the FP64 moments of out1 (full sums: nsplit = 1).
 // ---------------------------------------------------------------------------
 
+// q / n and q % n for 0 <= q < 2^24 with n >= 1, from a float reciprocal
+// and one correction step
+struct PDiv {
+    int n;
+    float inv;
+    __device__ __forceinline__ void set(int nn) { n = nn; inv = 1.0f / float(nn); }
+    __device__ __forceinline__ int div(int q, int* rem) const {
+        int d = __float2int_rz(float(q) * inv);
+        int r = q - d * n;
+        if (r < 0) { --d; r += n; }
+        else if (r >= n) { ++d; r -= n; }
+        *rem = r;
+        return d;
+    }
+};
+
+// flux at the left face of element c along an axis with n cells (n >= 3: a
+// window position pos-3 .. pos+2 wraps at most once), pos its index along
+// the axis, neighbours circular within the axis
 template <int RECON, bool EXACT, typename T>
 __device__ __forceinline__ T p_face_flux(const T* fb, int c, int stride, int n, int pos,
                                          T C, const Weno5Side<T>& Sr, const Weno5Side<T>& Sl) {
-    // flux at the left face of cell `c` along an axis with `n` cells; `pos` =
-    // the cell's index along that axis; neighbours wrap within the axis
     const bool right = C > T(0);
     const int off = right ? -3 : -2;          // window start relative to the cell
     T y[5];
 #pragma unroll
     for (int t = 0; t < 5; ++t) {
         int q = pos + off + t;
-        q = ((q % n) + n) % n;
+        if (n >= 3) {
+            q = q < 0 ? q + n : (q >= n ? q - n : q);
+        } else {
+            q = ((q % n) + n) % n;
+        }
         y[t] = fb[c + (q - pos) * stride];
     }
     T fv = face_value<RECON, EXACT>(y[0], y[1], y[2], y[3], y[4], right, right ? Sr : Sl);
@@ -564,9 +585,10 @@ __global__ void __launch_bounds__(PTHREADS)
 pstage_kernel(const __grid_constant__ PStageArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T* fb = reinterpret_cast<T*>(smem_raw);      // [Np]
-    T* F = fb + a.Np;                            // [Np] face fluxes of one axis
-    T* d1 = F + a.Np;                            // [Np]
-    T* d2 = d1 + a.Np;                           // [Np]
+    T* Fx[3] = {fb + a.Np, fb + 2 * a.Np, fb + 3 * a.Np};   // left-face fluxes per p axis
+    // p-cell centres of the species along p1, p2, p3 (after the four arrays,
+    // 8-byte aligned)
+    double* vg = reinterpret_cast<double*>(smem_raw + ((4 * (size_t)a.Np * sizeof(T) + 7) & ~(size_t)7));
     __shared__ double red[PTHREADS / 32][kNumMom];
 
     const int tid = threadIdx.x;
@@ -576,7 +598,13 @@ pstage_kernel(const __grid_constant__ PStageArgs a) {
     const long long cbase = (long long)(jj + a.Ng) * colstride + (long long)(ii + a.Ng) * rowstride
                           + (long long)s * a.Np;
     const T* fs = static_cast<const T*>(a.fs);
+    const int n1 = a.Np1, n2 = a.Np2, n3 = a.Np3;
     for (int c = tid; c < a.Np; c += PTHREADS) fb[c] = fs[cbase + c];
+    for (int q = tid; q < n1 + n2 + n3; q += PTHREADS) {
+        if (q < n1) vg[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
+        else if (q < n1 + n2) vg[q] = a.sg.p2_start[s] + (0.5 + (q - n1)) * a.sg.dp2[s];
+        else vg[q] = a.sg.p3_start[s] + (0.5 + (q - n1 - n2)) * a.sg.dp3[s];
+    }
     const long long plane_g = (long long)a.Nq2g * a.Nq1g;
     const long long qg = (long long)(jj + a.Ng) * a.Nq1g + (ii + a.Ng);
     const double E1 = a.cell[0 * plane_g + qg], E2 = a.cell[1 * plane_g + qg];
@@ -586,44 +614,34 @@ pstage_kernel(const __grid_constant__ PStageArgs a) {
     Weno5Side<T> Sr, Sl;
     Sr.set(true);
     Sl.set(false);
+    PDiv D1, D2;
+    D1.set(n1);
+    D2.set(n2);
     __syncthreads();
 
-    const int n1 = a.Np1, n2 = a.Np2, n3 = a.Np3;
-    // three axes; an axis with a single cell contributes exactly zero
-    for (int ax = 0; ax < 3; ++ax) {
-        const int n = ax == 0 ? n1 : (ax == 1 ? n2 : n3);
-        if (n == 1) continue;
-        const int stride = ax == 0 ? 1 : (ax == 1 ? n1 : n1 * n2);
-        for (int c = tid; c < a.Np; c += PTHREADS) {
-            const int i1 = c % n1, i2 = (c / n1) % n2, i3 = c / (n1 * n2);
-            const double v1 = a.sg.p1_start[s] + (0.5 + i1) * a.sg.dp1[s];
-            const double v2 = a.sg.p2_start[s] + (0.5 + i2) * a.sg.dp2[s];
-            const double v3 = a.sg.p3_start[s] + (0.5 + i3) * a.sg.dp3[s];
-            double C;
-            int pos;
-            if (ax == 0) { C = em * ((E1 + v2 * B3) - v3 * B2); pos = i1; }
-            else if (ax == 1) { C = em * ((E2 + v3 * B1) - v1 * B3); pos = i2; }
-            else { C = em * ((E3 + v1 * B2) - v2 * B1); pos = i3; }
-            F[c] = p_face_flux<RECON, EXACT>(fb, c, stride, n, pos, T(C), Sr, Sl);
-        }
-        __syncthreads();
-        const double dp = ax == 0 ? a.sg.dp1[s] : (ax == 1 ? a.sg.dp2[s] : a.sg.dp3[s]);
-        const T inv = T(1.0 / dp);
-        T* dst = ax == 0 ? d1 : (ax == 1 ? d2 : F + 0);
-        if (ax < 2) {
-            for (int c = tid; c < a.Np; c += PTHREADS) {
-                const int pos = ax == 0 ? c % n1 : (c / n1) % n2;
-                const int cn = pos + 1 < n ? c + stride : c - (n - 1) * stride;
-                dst[c] = (F[cn] - F[c]) * inv;
-            }
-        }
-        if (ax == 2) {
-            // keep d3 in F's slot: compute into d-registers below
-        }
-        __syncthreads();
-        if (ax == 2) break;
+    // element c -> (i1, i2, i3)
+    auto split = [&](int c, int& i1, int& i2, int& i3) {
+        const int r12 = D1.div(c, &i1);
+        i3 = D2.div(r12, &i2);
+    };
+    // left-face fluxes of every element along each p axis with more than one
+    // cell (a single-cell axis contributes exactly zero), one pass
+    for (int c = tid; c < a.Np; c += PTHREADS) {
+        int i1, i2, i3;
+        split(c, i1, i2, i3);
+        const double v1 = vg[i1], v2 = vg[n1 + i2], v3 = vg[n1 + n2 + i3];
+        if (n1 > 1)
+            Fx[0][c] = p_face_flux<RECON, EXACT>(fb, c, 1, n1, i1,
+                                                 T(em * ((E1 + v2 * B3) - v3 * B2)), Sr, Sl);
+        if (n2 > 1)
+            Fx[1][c] = p_face_flux<RECON, EXACT>(fb, c, n1, n2, i2,
+                                                 T(em * ((E2 + v3 * B1) - v1 * B3)), Sr, Sl);
+        if (n3 > 1)
+            Fx[2][c] = p_face_flux<RECON, EXACT>(fb, c, n1 * n2, n3, i3,
+                                                 T(em * ((E3 + v1 * B2) - v2 * B1)), Sr, Sl);
     }
-    // final combine; d3 is computed from F when the p3 axis is active
+    __syncthreads();
+    // final combine
     T* out1 = static_cast<T*>(a.out1);
     T* out2 = static_cast<T*>(a.out2);
     const T* base1 = static_cast<const T*>(a.base1);
@@ -631,30 +649,42 @@ pstage_kernel(const __grid_constant__ PStageArgs a) {
     const T* kq = static_cast<const T*>(a.kq);
     double macc[kNumMom] = {0, 0, 0, 0, 0};
     const T c1 = T(a.c1), c2 = T(a.c2);
+    const bool ghost_cell = (a.periodic1 && (ii < a.Ng || ii >= a.Nq1 - a.Ng)) ||
+                            (a.periodic2 && (jj < a.Ng || jj >= a.Nq2 - a.Ng));
+    const T inv1 = T(1.0 / a.sg.dp1[s]), inv2 = T(1.0 / a.sg.dp2[s]);
+    const T inv3 = T(1.0 / a.sg.dp3[s]);
     for (int c = tid; c < a.Np; c += PTHREADS) {
-        const int i1 = c % n1, i2 = (c / n1) % n2, i3 = c / (n1 * n2);
-        T t1 = n1 > 1 ? d1[c] : T(0);
-        T t2 = n2 > 1 ? d2[c] : T(0);
-        T t3 = T(0);
+        int i1, i2, i3;
+        split(c, i1, i2, i3);
+        // d_a = (F_a(right face) - F_a(left face)) / dp_a, circular along the axis
+        T t1 = T(0), t2 = T(0), t3 = T(0);
+        if (n1 > 1) {
+            const int cn = i1 + 1 < n1 ? c + 1 : c - (n1 - 1);
+            t1 = (Fx[0][cn] - Fx[0][c]) * inv1;
+        }
+        if (n2 > 1) {
+            const int cn = i2 + 1 < n2 ? c + n1 : c - (n2 - 1) * n1;
+            t2 = (Fx[1][cn] - Fx[1][c]) * inv2;
+        }
         if (n3 > 1) {
             const int cn = i3 + 1 < n3 ? c + n1 * n2 : c - (n3 - 1) * n1 * n2;
-            t3 = (F[cn] - F[c]) * T(1.0 / a.sg.dp3[s]);
+            t3 = (Fx[2][cn] - Fx[2][c]) * inv3;
         }
         const long long g = cbase + c;
         T kk = kq[g] + (-((t1 + t2) + t3));
         T o1 = base1 ? base1[g] + kk * c1 : kk;
         out1[g] = o1;
         if (out2) out2[g] = base2[g] + kk * c2;
-        if ((a.periodic1 && (ii < a.Ng || ii >= a.Nq1 - a.Ng)) ||
-            (a.periodic2 && (jj < a.Ng || jj >= a.Nq2 - a.Ng)))
+        if (ghost_cell)
             write_ghost_images(out1, o1, ii, jj, s, c, a.Ng, a.Nq1, a.Nq2, a.Nq1g, a.Nq2g,
                                a.periodic1, a.periodic2, rowstride, colstride, a.Np);
         if (a.flag && !isfinite(double(o1))) atomicOr(a.flag, 1);
         if (a.mom_out) {
-            const PVel V = lane_velocity(a.sg, s, i1, i2, i3);
+            const double w1 = vg[i1], w2 = vg[n1 + i2], w3 = vg[n1 + n2 + i3];
+            const double vsq = (w1 * w1 + w2 * w2) + w3 * w3;
             const double ov = double(o1);
-            macc[0] += ov; macc[1] += ov * V.v1; macc[2] += ov * V.v2; macc[3] += ov * V.v3;
-            macc[4] += (0.5 * ov) * V.vsq;
+            macc[0] += ov; macc[1] += ov * w1; macc[2] += ov * w2; macc[3] += ov * w3;
+            macc[4] += (0.5 * ov) * vsq;
         }
     }
     if (a.mom_out) {

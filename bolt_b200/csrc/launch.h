@@ -32,7 +32,10 @@ inline size_t qstage_smem(int tiling, size_t elem, int bgk, int bgk_direct, int 
 // bytes of dynamic shared memory of the paired FP32 kernel
 inline size_t qpair_smem(int ntab, int bgk) { return qpair_layout(ntab, bgk).total; }
 
-inline size_t pstage_smem(int Np, size_t elem) { return 4 * (size_t)Np * elem; }
+// the f, flux and two divergence arrays, then the p-cell centres (doubles)
+inline size_t pstage_smem(int Np, size_t elem, int ntab) {
+    return ((4 * (size_t)Np * elem + 7) & ~(size_t)7) + (size_t)ntab * sizeof(double);
+}
 
 #define BOLT_DECLARE_LAUNCHERS(SUFFIX, T)                                                   \
     cudaError_t launch_qstage_##SUFFIX(const QStageArgs& a, int recon, int tiling, int bgk, \
