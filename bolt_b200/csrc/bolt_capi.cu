@@ -490,8 +490,10 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     // the paired FP32 kernel covers the fused WENO5 2-D stage with every
     // buffer reachable by TMA; everything else (FP64, other reconstructions,
     // 1-D tilings, write-k mode, currents, tau arrays) runs the scalar kernel
-    bool pair = ctx->pair_shape_ok && ctx->pair_enabled && !write_k && !want_j && a.use_tma &&
-                a.base1 != nullptr && ctx->tau_arr == nullptr;
+    // (write-k stages -- fields enabled -- use it too, unless they also
+    // accumulate currents)
+    bool pair = ctx->pair_shape_ok && ctx->pair_enabled && !want_j && a.use_tma &&
+                (a.base1 != nullptr || write_k) && ctx->tau_arr == nullptr;
     if (pair) {
         const void* ptrs[4] = {a.base1, a.out1, a.base2, a.out2};
         for (int i = 0; i < 4; ++i)
@@ -505,8 +507,11 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     if (pair) {
         // copy each map out at once: a later lookup may recycle its cache slot
         const CUtensorMap* m;
-        if ((m = get_tmap(ctx, a.base1, TMAP_TILE))) a.tm_b1 = *m; else pair = false;
+        if (a.base1) {
+            if ((m = get_tmap(ctx, a.base1, TMAP_TILE))) a.tm_b1 = *m; else pair = false;
+        }
         if (pair && (m = get_tmap(ctx, a.out1, TMAP_TILE_SWZ))) a.tm_o1 = *m; else pair = false;
+        if (!a.base1) a.tm_b1 = a.tm_o1;            // unused (no base tiles): a valid map
         a.tm_o2 = a.tm_o1;
         if (pair && a.out2) {
             if ((m = get_tmap(ctx, a.out2, TMAP_TILE))) a.tm_o2 = *m; else pair = false;

@@ -14,7 +14,8 @@ cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t sme
     // first RK4 / RK2 stage: the bases are the stage input
     const bool bx = a.base1 == a.fs && (!has2 || a.base2 == a.fs);
     int mode;
-    if (bx) mode = has2 ? QP_X2 : QP_X1;
+    if (a.base1 == nullptr && !has2) mode = QP_K;
+    else if (bx) mode = has2 ? QP_X2 : QP_X1;
     else if (!has2) mode = QP_B1;
     else if (a.base2 == a.out2) mode = QP_B1R2;
     else return cudaErrorInvalidValue;        // excluded by the host's dispatch
@@ -23,6 +24,7 @@ cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t sme
         case QP_X1: k = bgk ? qpair_kernel<true, QP_X1> : qpair_kernel<false, QP_X1>; break;
         case QP_X2: k = bgk ? qpair_kernel<true, QP_X2> : qpair_kernel<false, QP_X2>; break;
         case QP_B1: k = bgk ? qpair_kernel<true, QP_B1> : qpair_kernel<false, QP_B1>; break;
+        case QP_K: k = bgk ? qpair_kernel<true, QP_K> : qpair_kernel<false, QP_K>; break;
         default: k = bgk ? qpair_kernel<true, QP_B1R2> : qpair_kernel<false, QP_B1R2>; break;
     }
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -91,12 +91,15 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
 //   QP_B1   base1 tiles loaded (double-buffered), out1 only
 //   QP_B1R2 base1 tiles loaded, out2 = base2 in place: c2 k is added to it by
 //           a TMA reduce-add (no base2 load)
-enum QPairMode { QP_X1 = 0, QP_X2 = 1, QP_B1 = 2, QP_B1R2 = 3 };
+//   QP_K    out1 = k itself (the q-part of df/dt when a p-stage follows: fields
+//           enabled), no base, no moments
+enum QPairMode { QP_X1 = 0, QP_X2 = 1, QP_B1 = 2, QP_B1R2 = 3, QP_K = 4 };
 
 template <bool BGK, int MODE>
 __global__ void __launch_bounds__(NTHREADS, 2)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
-    constexpr bool BX = MODE == QP_X1 || MODE == QP_X2;
+    constexpr bool BX = MODE == QP_X1 || MODE == QP_X2 || MODE == QP_K;   // no base tiles
+    constexpr bool KOUT = MODE == QP_K;
     constexpr bool HAS2 = MODE == QP_X2 || MODE == QP_B1R2;
     constexpr bool RED2 = MODE == QP_B1R2;
     constexpr int TQ = 8, HX = TQ + 2 * HALO, NQ = TQ * TQ, NWARP = NTHREADS / 32;
@@ -293,8 +296,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
                     const float2 f0 = mul2(mul2(t1[r * 4], t2[r * 4]), t3[r * 4]);
                     kk = fma2(sub2(f0, fcell), inv_tau, kk);
                 }
-                const float2 o1 = fma2(kk, c1, BX ? fcell : make_float2(bb1[r * TQ * PW],
-                                                                         bb1[r * TQ * PW + PW]));
+                const float2 o1 = KOUT ? kk
+                                       : fma2(kk, c1, BX ? fcell : make_float2(bb1[r * TQ * PW],
+                                                                               bb1[r * TQ * PW + PW]));
                 ob1[r * TQ * PW + sw0] = o1.x;
                 ob1[r * TQ * PW + PW + sw1] = o1.y;
                 if (HAS2) {
