@@ -490,10 +490,12 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     // the paired FP32 kernel covers the fused WENO5 2-D stage with every
     // buffer reachable by TMA; everything else (FP64, other reconstructions,
     // 1-D tilings, write-k mode, currents, tau arrays) runs the scalar kernel
-    // (write-k stages -- fields enabled -- use it too, unless they also
-    // accumulate currents)
+    // (so do the write-k stages of field-coupled steps, unless they also
+    // accumulate currents; bolt_dfdt without fields keeps the scalar kernel,
+    // the one bolt_dfdt_noalloc runs, so the two agree to the bit)
     bool pair = ctx->pair_shape_ok && ctx->pair_enabled && !want_j && a.use_tma &&
-                (a.base1 != nullptr || write_k) && ctx->tau_arr == nullptr;
+                (write_k ? ctx->p.fields_enabled != 0 : a.base1 != nullptr) &&
+                ctx->tau_arr == nullptr;
     if (pair) {
         const void* ptrs[4] = {a.base1, a.out1, a.base2, a.out2};
         for (int i = 0; i < 4; ++i)
