@@ -550,7 +550,7 @@ def run_batch(args, rank, world, local_rank):
 
 
 def run_adjoint(args, rank, world, local_rank):
-    """Config 5: gradients of J = sum_n dt |nhat_1(n)|^2 for 1D1V 128 x 256,
+    """Adjoint workload: gradients of J = sum_n dt |nhat_1(n)|^2 for 1D1V 128 x 256,
     p1 in [-10, 10], n = 1 + a cos(2 pi q1) (a = 0.01), Maxwellian T = 1,
     tau = 0.02, RK4, dt = 2e-4, 2000 steps, binomial checkpointing with 20
     snapshots; FP32 f with FP64 moments.  Reports the forward and gradient
@@ -631,7 +631,7 @@ def run_adjoint(args, rank, world, local_rank):
 
 
 def c2_spec():
-    """Config 2: 2D2V on [0,1]^2 periodic, 64 x 64 q, p1, p2 in [-8, 8] with
+    """2D2V FDTD-coupled workload: [0,1]^2 periodic, 64 x 64 q, p1, p2 in [-8, 8] with
     32 x 32, p3 one cell in [-0.5, 0.5], p_dim 2; f0 = n_q exp(-p1^2/4 - p2^2/2)
     / (2 pi sqrt 2), n_q = 1 + 1e-3 xi_q with xi ~ N(0, 1) per q-cell from
     numpy.random.default_rng(0); collisionless, electrodynamic FDTD with the
@@ -649,7 +649,7 @@ def c2_spec():
 
 
 def run_c1(args, rank, world, local_rank):
-    """Config 1 (1D1V 64 x 128, WENO5, RK2, dt = 1e-4, 100 steps, FP64): 8,192
+    """1D1V BGK relaxation (64 x 128, WENO5, RK2, dt = 1e-4, 100 steps, FP64): 8,192
     cells, so a step is launch-latency bound.  Times 100 steps three ways:
     Python strang_timestep calls, nls.run(dt, 100) (the C loop of bolt_run),
     and one replay of a CUDA graph captured around nls.run."""
@@ -700,10 +700,10 @@ def run_c1(args, rank, world, local_rank):
     del g
     if rank != 0:
         return
-    line = {'metric': 'cell-updates/s 1D1V 64x128 WENO5 RK2 FP64 (config 1), launch-bound',
+    line = {'metric': 'cell-updates/s 1D1V 64x128 WENO5 RK2 FP64, launch-bound',
             'value': cells / (res['cuda_graph_ms_per_step'] * 1e-3), 'unit': UNIT, 'n_gpus': 1,
             'steps': n, 'higher_is_better': True, 'dtype': 'f64', 'data': 'synthetic',
-            'config': {'workload': 'config 1: 1D1V 64 x 128, n = 1 + 0.01 cos(2 pi q1), tau = '
+            'config': {'workload': '1D1V 64 x 128, n = 1 + 0.01 cos(2 pi q1), tau = '
                                    '0.01, WENO5, RK2, dt = 1e-4', 'cells': cells},
             }
     line.update({k: v for k, v in res.items()})
@@ -713,7 +713,7 @@ def run_c1(args, rank, world, local_rank):
 
 
 def run_c2(args, rank, world, local_rank):
-    """Config 2, FP64 and FP32 f (FP64 moments): cell-updates/s over the timed
+    """2D2V FDTD-coupled workload, FP64 and FP32 f (FP64 moments): cell-updates/s over the timed
     steps (CUDA events) and, after all steps, the FP32 error in density,
     energy and the cell-centred fields against the FP64 run."""
     import torch
@@ -747,7 +747,7 @@ def run_c2(args, rank, world, local_rank):
     if rank != 0:
         return
     line = {
-        'metric': 'cell-updates/s 2D2V FDTD-coupled WENO5+LLF RK4 (config 2), FP32 vs FP64',
+        'metric': 'cell-updates/s 2D2V FDTD-coupled WENO5+LLF RK4, FP32 vs FP64',
         'value': res['fp32']['value'], 'unit': UNIT, 'n_gpus': 1, 'steps': args.c2_steps,
         'higher_is_better': True, 'dtype': 'f32', 'data': 'synthetic (seed 0 noise)',
         'config': {'workload': '2D2V 64^2 x 32^2, FDTD fields, collisionless, dt = 5e-4',
@@ -772,11 +772,16 @@ def main():
     ap.add_argument('--small', action='store_true', help='64x64 x 24^3 (profiling size)')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-fp64', action='store_true')
-    ap.add_argument('--workload', default='c3', choices=['c3', 'c1', 'c2', 'ragged-batch', 'adjoint'],
-                    help='c3: the 128^2 x 24^3 headline; ragged-batch: the 1D1V sweep; '
-                         'adjoint: gradients of the 1D1V density-mode functional')
+    ap.add_argument('--workload', default='2d3v',
+                    choices=['2d3v', '1d1v-relax', '2d2v-fdtd', 'ragged-batch', 'adjoint',
+                             'c3', 'c1', 'c2'],
+                    help='2d3v: the 128^2 x 24^3 BGK throughput headline; 1d1v-relax: the '
+                         '64 x 128 FP64 relaxation (launch-bound); 2d2v-fdtd: the 64^2 x 32^2 '
+                         'FDTD-coupled run, FP32 vs FP64; ragged-batch: the 1D1V sweep; adjoint: '
+                         'gradients of the 1D1V density-mode functional (c3, c1, c2: short names '
+                         'of the first three)')
     ap.add_argument('--adj-steps', type=int, default=2000)
-    ap.add_argument('--c2-steps', type=int, default=500)
+    ap.add_argument('--c2-steps', type=int, default=500, help='steps of the 2d2v-fdtd workload')
     ap.add_argument('--batch-runs', type=int, default=256)
     ap.add_argument('--batch-steps', type=int, default=200)
     ap.add_argument('--traffic', type=float, default=None,
@@ -799,9 +804,9 @@ def main():
             run_batch(args, rank, world, local_rank)
         elif args.workload == 'adjoint':
             run_adjoint(args, rank, world, local_rank)
-        elif args.workload == 'c2':
+        elif args.workload in ('2d2v-fdtd', 'c2'):
             run_c2(args, rank, world, local_rank)
-        elif args.workload == 'c1':
+        elif args.workload in ('1d1v-relax', 'c1'):
             run_c1(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)

@@ -55,7 +55,8 @@ extern "C" {
 #define BOLT_RECON_PPM    2   /* 'ppm'                */
 #define BOLT_RECON_WENO5  3   /* 'weno5'              */
 
-/* numerical flux (riemann.py:46-49; LLF as north-star extension) */
+/* numerical flux (riemann.py:46-49 upwind; LLF, the local Lax-Friedrichs flux, has no
+ * counterpart in riemann.py) */
 #define BOLT_FLUX_UPWIND 0
 #define BOLT_FLUX_LLF    1
 

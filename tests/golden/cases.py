@@ -39,7 +39,7 @@ def make(**kw):
 
 
 CASES = {
-    # 1D1V BGK relaxation, WENO5, RK2, dt=1e-4, 100 steps
+    # 1D1V BGK relaxation 64 x 128, WENO5, RK2, dt=1e-4, 100 steps
     'c1_1d1v_weno5_rk2': make(
         N_q1=64, N_q2=1, N_p1=128, N_p2=1, N_p3=1,
         p1_start=[-10.0], p1_end=[10.0], p2_start=[-0.5], p2_end=[0.5],
@@ -54,7 +54,7 @@ CASES = {
         tau=0.01, dt=1e-4, steps=20, integrator='RK4',
         riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
         init=dict(amp=0.01, k1=1, k2=0)),
-    # reduced config 3: 2D3V, BGK tau=0.05, WENO5, RK4
+    # reduced 2D3V throughput case: BGK tau=0.05, WENO5, RK4
     'c3_2d3v_weno5_rk4_small': make(
         N_q1=8, N_q2=8, N_p1=8, N_p2=8, N_p3=8,
         p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0], p2_end=[6.0],
@@ -62,7 +62,7 @@ CASES = {
         tau=0.05, dt=1e-3, steps=3, integrator='RK4',
         riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
         init=dict(amp=0.05, k1=1, k2=1)),
-    # reduced config 2: 2D2V electromagnetic FDTD, collisionless, RK2 (reference scheme)
+    # reduced 2D2V electromagnetic FDTD case, collisionless, RK2 (reference scheme)
     'c2_2d2v_fdtd_rk2_small': make(
         N_q1=8, N_q2=8, N_p1=16, N_p2=16, N_p3=1,
         p1_start=[-8.0], p1_end=[8.0], p2_start=[-8.0], p2_end=[8.0],
