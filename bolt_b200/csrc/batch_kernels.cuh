@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(NW * 32)
 batch_stage_kernel(const BatchStageArgs a) {
     constexpr int TQ = NW * kBatchCellsPerWarp;
     constexpr int ROWS = TQ + 2 * kBatchNg;
-    __shared__ float X[ROWS][PW];
+    __shared__ float X[2][ROWS][PW];      // chunk c in X[c & 1]; chunk c+1 loads meanwhile
     __shared__ double par[TQ][3];
     __shared__ int item_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -143,53 +143,69 @@ batch_stage_kernel(const BatchStageArgs a) {
         const float c1 = float(a.a1 * R.dt), c2 = float(a.a2 * R.dt);
         double acc[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 
-        for (int c = 0; c < Np1 / PW; ++c) {
-            const int p = c * PW + lane;
-            __syncthreads();                      // previous chunk's X reads are done
+        // the tile's rows of one p-chunk -> X[b], asynchronously (one group)
+        auto issue = [&](int c, int b) {
             for (int row = warp; row < ncell + 2 * kBatchNg; row += NW)
-                X[row][lane] = fs[(long long)(i0 + row) * Np1 + p];
-            __syncthreads();
-            if (!active) continue;
-
-            const double V = R.p1_start + (0.5 + p) * R.dp1;
-            const float v = float(V);
-            const bool right = v > 0.0f;
-            Weno5Side<float> S;
-            S.set(right);
-            Weno5Walker<false, float> W;
-            // face between local cells f and f+1 reads rows f+1+off .. f+5+off
-            const int r0 = j0 + (right ? 0 : 1);
-            float y0 = X[r0][lane], y1 = X[r0 + 1][lane], y2 = X[r0 + 2][lane];
-            float y3 = X[r0 + 3][lane], y4 = X[r0 + 4][lane];
-            float Fprev = v * W.first(y0, y1, y2, y3, y4, S);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int j = j0 + q;             // local cell
-                y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                y4 = X[r0 + 5 + q][lane];
-                const float Fn = v * W.next(y0, y1, y2, y3, y4, S);
-                float k = (Fprev - Fn) * inv_dq;
-                Fprev = Fn;
-                const float fc = X[j + kBatchNg][lane];
-                if (a.source) {
-                    const double dv = V - par[j][1];
-                    const float f0 = float(par[j][0]) * batch_exp(par[j][2] * (dv * dv));
-                    k = fmaf(f0 - fc, inv_tau, k);
-                }
-                const long long o = R.f_off + (long long)(i0 + j + kBatchNg) * Np1 + p;
-                const float o1 = fmaf(k, c1, a.base1[o]);
-                a.out1[o] = o1;
-                if (a.out2) a.out2[o] = fmaf(k, c2, a.base2[o]);
-                // periodic images of the border cells (2 N_g <= N_q1)
-                const int ii = i0 + j;
-                if (ii < kBatchNg) a.out1[o + (long long)Nq1 * Np1] = o1;
-                else if (ii >= Nq1 - kBatchNg) a.out1[o - (long long)Nq1 * Np1] = o1;
-                nonfinite |= !isfinite(o1);
-                const double od = o1;
-                acc[q][0] += od;
-                acc[q][1] = fma(od, V, acc[q][1]);
-                acc[q][2] = fma(0.5 * od, V * V, acc[q][2]);
+                cp_async4(&X[b][row][lane], fs + (long long)(i0 + row) * Np1 + c * PW + lane);
+            cp_async_commit();
+        };
+        const int nch = Np1 / PW;
+        __syncthreads();                          // the previous item is done with X
+        issue(0, 0);
+        for (int c = 0; c < nch; ++c) {
+            const int p = c * PW + lane;
+            const int b = c & 1;
+            // X[b ^ 1] was last read in chunk c-1, before its closing barrier
+            if (c + 1 < nch) {
+                issue(c + 1, b ^ 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
             }
+            __syncthreads();                      // chunk c's rows landed for every thread
+            if (active) {
+                const double V = R.p1_start + (0.5 + p) * R.dp1;
+                const float v = float(V);
+                const bool right = v > 0.0f;
+                Weno5Side<float> S;
+                S.set(right);
+                Weno5Walker<false, float> W;
+                const float (*Xb)[PW] = X[b];
+                // face between local cells f and f+1 reads rows f+1+off .. f+5+off
+                const int r0 = j0 + (right ? 0 : 1);
+                float y0 = Xb[r0][lane], y1 = Xb[r0 + 1][lane], y2 = Xb[r0 + 2][lane];
+                float y3 = Xb[r0 + 3][lane], y4 = Xb[r0 + 4][lane];
+                float Fprev = v * W.first(y0, y1, y2, y3, y4, S);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int j = j0 + q;             // local cell
+                    y0 = y1; y1 = y2; y2 = y3; y3 = y4;
+                    y4 = Xb[r0 + 5 + q][lane];
+                    const float Fn = v * W.next(y0, y1, y2, y3, y4, S);
+                    float k = (Fprev - Fn) * inv_dq;
+                    Fprev = Fn;
+                    const float fc = Xb[j + kBatchNg][lane];
+                    if (a.source) {
+                        const double dv = V - par[j][1];
+                        const float f0 = float(par[j][0]) * batch_exp(par[j][2] * (dv * dv));
+                        k = fmaf(f0 - fc, inv_tau, k);
+                    }
+                    const long long o = R.f_off + (long long)(i0 + j + kBatchNg) * Np1 + p;
+                    const float o1 = fmaf(k, c1, a.base1[o]);
+                    a.out1[o] = o1;
+                    if (a.out2) a.out2[o] = fmaf(k, c2, a.base2[o]);
+                    // periodic images of the border cells (2 N_g <= N_q1)
+                    const int ii = i0 + j;
+                    if (ii < kBatchNg) a.out1[o + (long long)Nq1 * Np1] = o1;
+                    else if (ii >= Nq1 - kBatchNg) a.out1[o - (long long)Nq1 * Np1] = o1;
+                    nonfinite |= !isfinite(o1);
+                    const double od = o1;
+                    acc[q][0] += od;
+                    acc[q][1] = fma(od, V, acc[q][1]);
+                    acc[q][2] = fma(0.5 * od, V * V, acc[q][2]);
+                }
+            }
+            __syncthreads();                      // X[b] reads done before it is refilled
         }
         if (active) {
 #pragma unroll

@@ -369,6 +369,26 @@ struct Weno5PairWalker {
 };
 
 // ---------------------------------------------------------------------------
+// Per-thread asynchronous global -> shared copies (cp.async, 4 bytes, cached
+// in L1), committed in groups; wait_group<N> returns once at most N of this
+// thread's groups are still in flight (always completes: no timeout needed).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;"
+                 ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst))),
+                   "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// ---------------------------------------------------------------------------
 // mbarrier + TMA (cp.async.bulk.tensor) wrappers.  Waits are bounded: after
 // kWaitCycles clock cycles the wait reports failure and the caller records
 // BOLT_ERR_TIMEOUT instead of hanging.
