@@ -402,7 +402,9 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                     fprev = W.first(y0, y1, y2, y3, y4, right, S);
                     Fprev = v2 * fprev;
                 }
-#pragma unroll
+                // the FP64 reference-order body is long (divisions in the WENO
+                // weights): rolled, it stays in the instruction cache
+#pragma unroll (EXACT ? 1 : SEGB)
                 for (int r = 0; r < SEGB; ++r) {
                     const int rr = rb0 + r;
                     if (rr >= TQ2) break;
