@@ -368,6 +368,26 @@ struct Weno5PairWalker {
     }
 };
 
+// Minmod faces for the paired kernel, same interface as Weno5PairWalker:
+// twice the face value of the window's centre cell y2 (its right face for
+// right-moving lanes, its left face otherwise), 2 y2 +- the limited slope of
+// (y1, y2, y3) (minmod.py:4-71).  No state is carried between faces.
+struct MinmodPairWalker {
+    __device__ __forceinline__ static float2 face(float2 y1, float2 y2, float2 y3, bool right) {
+        float2 sl = make_float2(minmod_slope(y1.x, y2.x, y3.x), minmod_slope(y1.y, y2.y, y3.y));
+        if (!right) sl = make_float2(-sl.x, -sl.y);
+        return fma2(f2(2.0f), y2, sl);
+    }
+    __device__ __forceinline__ float2 first(float2, float2 y1, float2 y2, float2 y3, float2,
+                                            const Weno5Pair& S) {
+        return face(y1, y2, y3, S.right);
+    }
+    __device__ __forceinline__ float2 next(float2, float2 y1, float2 y2, float2 y3, float2,
+                                           const Weno5Pair& S) {
+        return face(y1, y2, y3, S.right);
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Per-thread asynchronous global -> shared copies (cp.async, 4 bytes, cached
 // in L1), committed in groups; wait_group<N> returns once at most N of this

@@ -8,7 +8,18 @@
 
 namespace bolt {
 
-cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t smem,
+template <int R>
+static void (*pick_qpair(int bgk, int mode))(QStageArgs) {
+    switch (mode) {
+        case QP_X1: return bgk ? qpair_kernel<true, QP_X1, R> : qpair_kernel<false, QP_X1, R>;
+        case QP_X2: return bgk ? qpair_kernel<true, QP_X2, R> : qpair_kernel<false, QP_X2, R>;
+        case QP_B1: return bgk ? qpair_kernel<true, QP_B1, R> : qpair_kernel<false, QP_B1, R>;
+        case QP_K: return bgk ? qpair_kernel<true, QP_K, R> : qpair_kernel<false, QP_K, R>;
+        default: return bgk ? qpair_kernel<true, QP_B1R2, R> : qpair_kernel<false, QP_B1R2, R>;
+    }
+}
+
+cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, int recon, dim3 grid, size_t smem,
                              cudaStream_t st) {
     const bool has2 = a.out2 != nullptr;
     // first RK4 / RK2 stage: the bases are the stage input
@@ -19,14 +30,8 @@ cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t sme
     else if (!has2) mode = QP_B1;
     else if (a.base2 == a.out2) mode = QP_B1R2;
     else return cudaErrorInvalidValue;        // excluded by the host's dispatch
-    void (*k)(QStageArgs);
-    switch (mode) {
-        case QP_X1: k = bgk ? qpair_kernel<true, QP_X1> : qpair_kernel<false, QP_X1>; break;
-        case QP_X2: k = bgk ? qpair_kernel<true, QP_X2> : qpair_kernel<false, QP_X2>; break;
-        case QP_B1: k = bgk ? qpair_kernel<true, QP_B1> : qpair_kernel<false, QP_B1>; break;
-        case QP_K: k = bgk ? qpair_kernel<true, QP_K> : qpair_kernel<false, QP_K>; break;
-        default: k = bgk ? qpair_kernel<true, QP_B1R2> : qpair_kernel<false, QP_B1R2>; break;
-    }
+    void (*k)(QStageArgs) = recon == BOLT_RECON_MINMOD ? pick_qpair<BOLT_RECON_MINMOD>(bgk, mode)
+                                                      : pick_qpair<BOLT_RECON_WENO5>(bgk, mode);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, NTHREADS, smem, st>>>(a);

@@ -74,7 +74,7 @@ BOLT_DECLARE_LAUNCHERS(f64, double)
 BOLT_DECLARE_LAUNCHERS(f32, float)
 
 // paired FP32 WENO5 q-stage (8x8 tiling, fields off, fused combine, TMA in and out)
-cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, dim3 grid, size_t smem,
+cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, int recon, dim3 grid, size_t smem,
                              cudaStream_t st);
 
 // FDTD sequence (FP64): prepare -> halo -> E -> halo -> B -> to_cell

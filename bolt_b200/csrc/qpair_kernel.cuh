@@ -23,11 +23,13 @@
 // two conflict-free 16-byte loads.  Barrier waits are time-bounded and a
 // failure is made CTA-uniform, recorded in the error word, and ends the work.
 //
-// Launch conditions (checked by the host): FP32, WENO5 in q, 8x8 tiling,
+// Launch conditions (checked by the host): FP32, WENO5 or minmod in q, 8x8 tiling,
 // N_q1, N_q2 multiples of 8 and at least 2 N_g, N_p multiple of 32, N_p1
 // multiple of 8, BGK by exp tables, all five buffers 16-byte aligned, f with
 // fewer than 2^31 elements (32-bit offsets).
 #pragma once
+
+#include <type_traits>
 
 #include "fvm_kernels.cuh"
 
@@ -95,9 +97,12 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
 //           enabled), no base, no moments
 enum QPairMode { QP_X1 = 0, QP_X2 = 1, QP_B1 = 2, QP_B1R2 = 3, QP_K = 4 };
 
-template <bool BGK, int MODE>
+template <bool BGK, int MODE, int RECON>
 __global__ void __launch_bounds__(NTHREADS, 2)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
+    // WENO5 faces with the sliding walker, or minmod faces
+    using Walker = typename std::conditional<RECON == BOLT_RECON_MINMOD, MinmodPairWalker,
+                                             Weno5PairWalker>::type;
     constexpr bool BX = MODE == QP_X1 || MODE == QP_X2 || MODE == QP_K;   // no base tiles
     constexpr bool KOUT = MODE == QP_K;
     constexpr bool HAS2 = MODE == QP_X2 || MODE == QP_B1R2;
@@ -233,7 +238,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             float2 y2 = make_float2(ra[2 * PW], rb[2 * PW]);
             float2 y3 = make_float2(ra[3 * PW], rb[3 * PW]);
             float2 y4 = make_float2(ra[4 * PW], rb[4 * PW]);
-            Weno5PairWalker W;
+            Walker W;
             const float2 vq = f2(0.5f * v1 * inv_dq1);   // walker returns 2x face value
             float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
             float* da = d1s + (a_row * TQ + a_c0) * PW + lane;
@@ -272,7 +277,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             float2 y2 = make_float2(ca[2 * HX * PW], cb[2 * HX * PW]);
             float2 y3 = make_float2(ca[3 * HX * PW], cb[3 * HX * PW]);
             float2 y4 = make_float2(ca[4 * HX * PW], cb[4 * HX * PW]);
-            Weno5PairWalker W;
+            Walker W;
             const float2 vq = f2(0.5f * v2 * inv_dq2);   // walker returns 2x face value
             float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
             const int cb0 = b_r0 * TQ + b_col;                   // q-cell of row 0, col b_col

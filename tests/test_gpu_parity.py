@@ -92,6 +92,7 @@ def test_fp64_matches_reference(name):
                                   'minmod_2d2v_fields_bgk', 'ppm_2d2v_fields_bgk',
                                   'dirichlet_1d1v_weno5', 'two_species_2d2v_fields',
                                   'mirror_2d2v_weno5', 'mirror_dirichlet_2d3v_rk4',
+                                  'dirichlet_2d2v_minmod',
                                   'es_1d1v_landau_rk2', 'es_2d2v_two_species_rk4'])
 def test_fp32_close_to_reference(name):
     _check_case(name, 'fp32')
@@ -144,6 +145,13 @@ PAIR_CASES = {
                        bottom=dict(base=1.1, T=[1.0, 1.0, 1.0], u=[0.0, 0.4, 0]),
                        top=dict(base=0.9, T=[1.0, 1.0, 1.0], u=[0.0, -0.4, 0])),
         init=dict(amp=0.1, k1=1, k2=1)),
+    'pair_minmod_rk4': C.make(
+        N_q1=24, N_q2=16, N_p1=8, N_p2=8, N_p3=4, recon_q='minmod', recon_p='minmod',
+        p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+        p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+        tau=0.02, dt=1e-3, steps=3, integrator='RK4',
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+        init=dict(amp=0.1, k1=1, k2=2, u=[0.3, -0.2, 0.05], T=[1.0, 1.4, 0.8])),
     'pair_mirror_rk4': C.make(
         N_q1=16, N_q2=24, N_p1=8, N_p2=4, N_p3=4,
         p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
@@ -180,12 +188,13 @@ def test_paired_kernel_cases_vs_oracle(name, precision, tol):
     assert max(errs.values()) < tol, errs
 
 
-def test_paired_kernel_matches_scalar_kernel(monkeypatch):
+@pytest.mark.parametrize('recon', ['weno5', 'minmod'])
+def test_paired_kernel_matches_scalar_kernel(monkeypatch, recon):
     """The paired FP32 kernel against the scalar FP32 kernel (BOLT_NO_PAIR) on
     a 32x32 x 24^3 Maxwellian with a density wave, two RK4 steps: same
     arithmetic type, different operation order, so they agree to a few FP32
     ulps."""
-    spec = C.make(N_q1=32, N_q2=32, N_p1=24, N_p2=24, N_p3=24,
+    spec = C.make(N_q1=32, N_q2=32, N_p1=24, N_p2=24, N_p3=24, recon_q=recon, recon_p=recon,
                   p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0], p2_end=[6.0],
                   p3_start=[-6.0], p3_end=[6.0], mass=[1.0], charge=[0.0], p_dim=3,
                   tau=0.05, dt=1e-3, steps=2, integrator='RK4',
