@@ -240,7 +240,6 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
                        (size_t)t.tq1 * t.tq2 * ctx->ntab * sizeof(double) > 64 * 1024) ? 1 : 0;
     // the paired FP32 kernel's shape conditions (the per-call ones are checked at launch)
     ctx->pair_shape_ok = ctx->elem == 4 &&
-                         (p.recon_q == BOLT_RECON_WENO5 || p.recon_q == BOLT_RECON_MINMOD) &&
                          ctx->tiling == TILING_2D && !(ctx->bgk && ctx->bgk_direct) &&
                          g.N_q1 % 8 == 0 && g.N_q2 % 8 == 0 && ctx->Np % PW == 0 &&
                          g.N_p1 % 8 == 0 && 2 * g.N_ghost <= g.N_q1 &&

@@ -388,6 +388,31 @@ struct MinmodPairWalker {
     }
 };
 
+// PPM (ppm.py:4-100) and piecewise-constant faces for the paired kernel:
+// twice the face value of the window's centre cell y2, per element
+struct PpmPairWalker {
+    __device__ __forceinline__ float2 first(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
+                                            const Weno5Pair& S) {
+        return next(y0, y1, y2, y3, y4, S);
+    }
+    __device__ __forceinline__ float2 next(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
+                                           const Weno5Pair& S) {
+        return make_float2(2.0f * ppm_face(y0.x, y1.x, y2.x, y3.x, y4.x, S.right),
+                           2.0f * ppm_face(y0.y, y1.y, y2.y, y3.y, y4.y, S.right));
+    }
+};
+
+struct ConstPairWalker {
+    __device__ __forceinline__ float2 first(float2, float2, float2 y2, float2, float2,
+                                            const Weno5Pair&) {
+        return add2(y2, y2);
+    }
+    __device__ __forceinline__ float2 next(float2, float2, float2 y2, float2, float2,
+                                           const Weno5Pair&) {
+        return add2(y2, y2);
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Per-thread asynchronous global -> shared copies (cp.async, 4 bytes, cached
 // in L1), committed in groups; wait_group<N> returns once at most N of this

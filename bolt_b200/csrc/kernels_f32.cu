@@ -30,8 +30,13 @@ cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, int recon, dim3 grid,
     else if (!has2) mode = QP_B1;
     else if (a.base2 == a.out2) mode = QP_B1R2;
     else return cudaErrorInvalidValue;        // excluded by the host's dispatch
-    void (*k)(QStageArgs) = recon == BOLT_RECON_MINMOD ? pick_qpair<BOLT_RECON_MINMOD>(bgk, mode)
-                                                      : pick_qpair<BOLT_RECON_WENO5>(bgk, mode);
+    void (*k)(QStageArgs);
+    switch (recon) {
+        case BOLT_RECON_MINMOD: k = pick_qpair<BOLT_RECON_MINMOD>(bgk, mode); break;
+        case BOLT_RECON_PPM: k = pick_qpair<BOLT_RECON_PPM>(bgk, mode); break;
+        case BOLT_RECON_PC: k = pick_qpair<BOLT_RECON_PC>(bgk, mode); break;
+        default: k = pick_qpair<BOLT_RECON_WENO5>(bgk, mode); break;
+    }
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, NTHREADS, smem, st>>>(a);

@@ -23,7 +23,7 @@
 // two conflict-free 16-byte loads.  Barrier waits are time-bounded and a
 // failure is made CTA-uniform, recorded in the error word, and ends the work.
 //
-// Launch conditions (checked by the host): FP32, WENO5 or minmod in q, 8x8 tiling,
+// Launch conditions (checked by the host): FP32, any reconstruction in q, 8x8 tiling,
 // N_q1, N_q2 multiples of 8 and at least 2 N_g, N_p multiple of 32, N_p1
 // multiple of 8, BGK by exp tables, all five buffers 16-byte aligned, f with
 // fewer than 2^31 elements (32-bit offsets).
@@ -100,9 +100,13 @@ enum QPairMode { QP_X1 = 0, QP_X2 = 1, QP_B1 = 2, QP_B1R2 = 3, QP_K = 4 };
 template <bool BGK, int MODE, int RECON>
 __global__ void __launch_bounds__(NTHREADS, 2)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
-    // WENO5 faces with the sliding walker, or minmod faces
-    using Walker = typename std::conditional<RECON == BOLT_RECON_MINMOD, MinmodPairWalker,
-                                             Weno5PairWalker>::type;
+    // WENO5 faces with the sliding walker, or minmod / PPM / piecewise-constant faces
+    using Walker = typename std::conditional<
+        RECON == BOLT_RECON_MINMOD, MinmodPairWalker,
+        typename std::conditional<
+            RECON == BOLT_RECON_PPM, PpmPairWalker,
+            typename std::conditional<RECON == BOLT_RECON_PC, ConstPairWalker,
+                                      Weno5PairWalker>::type>::type>::type;
     constexpr bool BX = MODE == QP_X1 || MODE == QP_X2 || MODE == QP_K;   // no base tiles
     constexpr bool KOUT = MODE == QP_K;
     constexpr bool HAS2 = MODE == QP_X2 || MODE == QP_B1R2;

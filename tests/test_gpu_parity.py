@@ -92,7 +92,7 @@ def test_fp64_matches_reference(name):
                                   'minmod_2d2v_fields_bgk', 'ppm_2d2v_fields_bgk',
                                   'dirichlet_1d1v_weno5', 'two_species_2d2v_fields',
                                   'mirror_2d2v_weno5', 'mirror_dirichlet_2d3v_rk4',
-                                  'dirichlet_2d2v_minmod',
+                                  'dirichlet_2d2v_minmod', 'pc_2d3v_fields',
                                   'es_1d1v_landau_rk2', 'es_2d2v_two_species_rk4'])
 def test_fp32_close_to_reference(name):
     _check_case(name, 'fp32')
@@ -152,6 +152,12 @@ PAIR_CASES = {
         tau=0.02, dt=1e-3, steps=3, integrator='RK4',
         riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
         init=dict(amp=0.1, k1=1, k2=2, u=[0.3, -0.2, 0.05], T=[1.0, 1.4, 0.8])),
+    'pair_ppm_rk2': C.make(
+        N_q1=16, N_q2=24, N_p1=8, N_p2=4, N_p3=4, recon_q='ppm', recon_p='ppm',
+        p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+        p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+        tau=0.03, dt=1e-3, steps=3, integrator='RK2',
+        init=dict(amp=0.1, k1=2, k2=1, u=[-0.3, 0.2, 0.1])),
     'pair_mirror_rk4': C.make(
         N_q1=16, N_q2=24, N_p1=8, N_p2=4, N_p3=4,
         p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
@@ -188,7 +194,7 @@ def test_paired_kernel_cases_vs_oracle(name, precision, tol):
     assert max(errs.values()) < tol, errs
 
 
-@pytest.mark.parametrize('recon', ['weno5', 'minmod'])
+@pytest.mark.parametrize('recon', ['weno5', 'minmod', 'ppm', 'piecewise-constant'])
 def test_paired_kernel_matches_scalar_kernel(monkeypatch, recon):
     """The paired FP32 kernel against the scalar FP32 kernel (BOLT_NO_PAIR) on
     a 32x32 x 24^3 Maxwellian with a density wave, two RK4 steps: same
