@@ -187,8 +187,7 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
     if (p.integrator != BOLT_RK2 && p.integrator != BOLT_RK4) return BOLT_ERR_ARG;
     if (p.p_dim < 1 || p.p_dim > 3) return BOLT_ERR_ARG;
     if (p.bc_q1 < BOLT_BC_PERIODIC || p.bc_q1 > BOLT_BC_MIRROR_DIRICHLET ||
-        p.bc_q1 == BOLT_BC_EXTERNAL || p.bc_q2 < BOLT_BC_PERIODIC ||
-        p.bc_q2 > BOLT_BC_MIRROR_DIRICHLET)
+        p.bc_q2 < BOLT_BC_PERIODIC || p.bc_q2 > BOLT_BC_MIRROR_DIRICHLET)
         return BOLT_ERR_ARG;
     if (p.fields_enabled && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
         return BOLT_ERR_UNSUPPORTED;
@@ -394,7 +393,7 @@ static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
     const BoltGrid& g = ctx->g;
     const int dir1 = bc_dirichlet(ctx->p.bc_q1), dir2 = bc_dirichlet(ctx->p.bc_q2);
     const int mir1 = bc_mirror(ctx->p.bc_q1), mir2 = bc_mirror(ctx->p.bc_q2);
-    const int ext2 = ctx->p.bc_q2 == BOLT_BC_EXTERNAL;
+    const int ext1 = ctx->p.bc_q1 == BOLT_BC_EXTERNAL, ext2 = ctx->p.bc_q2 == BOLT_BC_EXTERNAL;
     const int per1 = ctx->p.bc_q1 == BOLT_BC_PERIODIC, per2 = ctx->p.bc_q2 == BOLT_BC_PERIODIC;
     if (g.N_ghost == 0) return BOLT_OK;
     if ((dir1 && (!ctx->dirichlet[0] || !ctx->dirichlet[1])) ||
@@ -404,11 +403,11 @@ static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
     if (ctx->elem == 8)
         e = launch_ghost_f64(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
                              ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
-                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext2, ctx->sg, st);
+                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, ctx->sg, st);
     else
         e = launch_ghost_f32(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
                              ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
-                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext2, ctx->sg, st);
+                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, ctx->sg, st);
     ctx->launches++;
     CK(e);
     return BOLT_OK;
@@ -667,8 +666,8 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         if (rc) return rc;
     }
     // the stage kernels write periodic images only; any other q1 / q2
-    // condition (an external q2 excepted) needs the ghost pass after the stage
-    const int dir = ctx->p.bc_q1 != BOLT_BC_PERIODIC ||
+    // condition (external axes excepted) needs the ghost pass after the stage
+    const int dir = (ctx->p.bc_q1 != BOLT_BC_PERIODIC && ctx->p.bc_q1 != BOLT_BC_EXTERNAL) ||
                     (ctx->p.bc_q2 != BOLT_BC_PERIODIC && ctx->p.bc_q2 != BOLT_BC_EXTERNAL);
     const int fe = ctx->p.fields_enabled;
     const int mo_split = fe ? 1 : ctx->nsplit;     // nsplit of partials written by a stage

@@ -797,7 +797,7 @@ template <typename T>
 __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const T* dt,
                              int Nq1, int Nq2, int Ng, int Ns, int Np, int Np1, int Np2,
                              int per1, int per2, int dir1, int dir2, int mir1, int mir2,
-                             int ext2, SpeciesGrid sg, long long nghost_cells) {
+                             int ext1, int ext2, SpeciesGrid sg, long long nghost_cells) {
     const int Nq1g = Nq1 + 2 * Ng;
     const long long rowstride = (long long)Ns * Np;
     const long long colstride = rowstride * Nq1g;
@@ -823,7 +823,8 @@ __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const 
         }
         const int i = g1 - Ng, j = g2 - Ng;
         const bool in1 = i >= 0 && i < Nq1, in2 = j >= 0 && j < Nq2;
-        if (ext2 && !in2) continue;            // q2 ghost rows belong to the caller
+        // ghost rows / columns of an external axis belong to the caller
+        if ((ext1 && !in1) || (ext2 && !in2)) continue;
         const int i1 = p % Np1, i2 = (p / Np1) % Np2;
         // source cell and p index: periodic wrap, or the mirror image across
         // the edge (ghost i < 0 <- interior -1-i, i >= N <- 2N-1-i) with the

@@ -52,7 +52,7 @@ inline size_t pstage_smem(int Np, size_t elem, int ntab) {
                                       const void* db, const void* dt, int Nq1, int Nq2,      \
                                       int Ng, int Ns, int Np, int Np1, int Np2, int per1,    \
                                       int per2, int dir1, int dir2, int mir1, int mir2,      \
-                                      int ext2, const SpeciesGrid& sg,                       \
+                                      int ext1, int ext2, const SpeciesGrid& sg,             \
                                       cudaStream_t st);
 
 // electrostatic field solve of one df/dt argument (poisson.cu)

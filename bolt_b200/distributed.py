@@ -1,17 +1,25 @@
-"""q2-slab decomposition of one run over the ranks of a torch.distributed group.
+"""q-block decomposition of one run over the ranks of a torch.distributed group.
 
-Bolt distributes a run over MPI ranks with a PETSc DMDA whose halos are
-exchanged by ``communicate_f`` before every df/dt evaluation
-(nonlinear_solver.py:251-280, communicate.py:8-38).  Here the q2 axis is cut
-into equal slabs, one per rank (one process per GPU); each rank's solver sees
-q2 as ``BOLT_BC_EXTERNAL`` and, before every RK stage, the N_g ghost rows of
-the stage input are exchanged with the neighbouring slabs (periodic over the
-ranks) by point-to-point sends and receives -- NCCL over NVLink between GPUs,
-gloo between CPU processes.  Rows are the slowest axis of the layout, so every
-message is one contiguous block of N_g (N_q1 + 2 N_g) N_s N_p values sent from
-and received into the stage buffer itself.  q1 stays whole and periodic on
-every rank; fields are not distributed (the reference's FFT initial solve is
-serial too, fft.py:26-27).
+Bolt distributes a run over MPI ranks with a PETSc DMDA that cuts the q-grid
+along q1 and q2, and refreshes the halos with communicate_f before every df/dt
+evaluation (nonlinear_solver.py:251-280, communicate.py:8-38).  Here the
+ranks form a P1 x P2 grid (rank = r1 + P1 r2, one process per GPU) and each
+owns an equal block of the q-grid.  An axis cut into several blocks must be
+periodic in the global problem; in the block's own solver it is
+``BOLT_BC_EXTERNAL``.  Before every RK stage the N_g halo layers of the stage
+input are exchanged with the neighbouring blocks (periodic over the grid), by
+point-to-point sends and receives -- NCCL over NVLink between GPUs, gloo
+between CPU processes:
+
+* q2 rows, the slowest axis of the layout: each message is one contiguous
+  block of N_g (N_q1 + 2 N_g) N_s N_p values, sent from and received into the
+  stage buffer itself;
+* q1 columns: packed into a contiguous buffer, then unpacked.
+
+Corner cells (ghost in both q1 and q2) are not exchanged: no interior update
+reads them, because the q1 and q2 stencils are separate.  An axis kept whole
+(P = 1) keeps the global problem's boundary condition.  Fields are not
+distributed: the reference's FFT initial solve is serial too (fft.py:26-27).
 """
 
 import types
@@ -25,69 +33,124 @@ def _group_info(group):
     return dist.get_rank(group), dist.get_world_size(group)
 
 
-def exchange_q2_halos(store, Ng, group=None):
-    """Fill the N_g ghost rows at both ends of dim 0 of ``store`` (this rank's
-    slab, (N_q2 + 2 N_g, ...)) with the boundary rows of the neighbouring
-    ranks' slabs; with one rank the slab wraps onto itself (periodic q2)."""
-    rank, world = _group_info(group)
-    n2g = store.shape[0]
-    bot_ghost, top_ghost = store[:Ng], store[n2g - Ng:]
-    bot_inner, top_inner = store[Ng:2 * Ng], store[n2g - 2 * Ng:n2g - Ng]
-    if world == 1:
-        bot_ghost.copy_(top_inner)
-        top_ghost.copy_(bot_inner)
-        return
-    up = dist.get_global_rank(group, (rank + 1) % world) if group is not None else (rank + 1) % world
-    down = dist.get_global_rank(group, (rank - 1) % world) if group is not None else (rank - 1) % world
-    ops = [dist.P2POp(dist.isend, top_inner.contiguous(), up, group),
-           dist.P2POp(dist.irecv, bot_ghost, down, group),
-           dist.P2POp(dist.isend, bot_inner.contiguous(), down, group),
-           dist.P2POp(dist.irecv, top_ghost, up, group)]
+def _global_rank(group, r):
+    return dist.get_global_rank(group, r) if group is not None else r
+
+
+def _swap(send_lo, send_hi, recv_lo, recv_hi, lo_rank, hi_rank, group):
+    """send_hi -> the hi neighbour, send_lo -> the lo neighbour; recv_lo <- the
+    lo neighbour's send_hi, recv_hi <- the hi neighbour's send_lo."""
+    ops = [dist.P2POp(dist.isend, send_hi, _global_rank(group, hi_rank), group),
+           dist.P2POp(dist.irecv, recv_lo, _global_rank(group, lo_rank), group),
+           dist.P2POp(dist.isend, send_lo, _global_rank(group, lo_rank), group),
+           dist.P2POp(dist.irecv, recv_hi, _global_rank(group, hi_rank), group)]
     for req in dist.batch_isend_irecv(ops):
         req.wait()
 
 
-def slab_of(N_q2, q2_start, q2_end, rank, world):
-    """(local N_q2, local q2_start, local q2_end) of rank's slab."""
-    if N_q2 % world:
-        raise ValueError('N_q2 = %d is not divisible by %d ranks' % (N_q2, world))
-    n = N_q2 // world
-    dq2 = (q2_end - q2_start) / N_q2
-    return n, q2_start + rank * n * dq2, q2_start + (rank + 1) * n * dq2
+def exchange_q2_halos(store, Ng, group=None, neighbours=None):
+    """Fill the N_g ghost rows at both ends of dim 0 of ``store`` (this rank's
+    block, (N_q2 + 2 N_g, ...)) with the boundary rows of the blocks below and
+    above (``neighbours`` = (down, up) ranks, default the ranks before and
+    after this one, periodically); with one rank the block wraps onto itself."""
+    rank, world = _group_info(group)
+    n2g = store.shape[0]
+    bot_ghost, top_ghost = store[:Ng], store[n2g - Ng:]
+    bot_inner, top_inner = store[Ng:2 * Ng], store[n2g - 2 * Ng:n2g - Ng]
+    down, up = neighbours if neighbours is not None else \
+        ((rank - 1) % world, (rank + 1) % world)
+    if down == rank and up == rank:
+        bot_ghost.copy_(top_inner)
+        top_ghost.copy_(bot_inner)
+        return
+    _swap(bot_inner.contiguous(), top_inner.contiguous(), bot_ghost, top_ghost, down, up, group)
 
 
-class SlabSolver(object):
-    """nonlinear_solver of this rank's q2 slab of ``physical_system``'s domain
-    (q2 periodic in the global problem), stepped stage by stage with halo
-    exchanges.  Exposes the local solver as ``.local``.  ``slab=(rank, world)``
-    builds that slab without a process group (several slabs in one process,
-    stepped in lockstep through begin_step / stage_input / stage / end_step)."""
+def exchange_q1_halos(store, Ng, group=None, neighbours=None):
+    """The same along dim 1 (q1 columns of (N_q2g, N_q1 + 2 N_g, ...);
+    ``neighbours`` = (left, right) ranks): the columns travel packed in
+    contiguous buffers."""
+    rank, world = _group_info(group)
+    n1g = store.shape[1]
+    left, right = neighbours if neighbours is not None else \
+        ((rank - 1) % world, (rank + 1) % world)
+    lo_inner, hi_inner = store[:, Ng:2 * Ng], store[:, n1g - 2 * Ng:n1g - Ng]
+    if left == rank and right == rank:
+        store[:, :Ng].copy_(hi_inner)
+        store[:, n1g - Ng:].copy_(lo_inner)
+        return
+    recv_lo = hi_inner.contiguous().clone()
+    recv_hi = lo_inner.contiguous().clone()
+    _swap(lo_inner.contiguous(), hi_inner.contiguous(), recv_lo, recv_hi, left, right, group)
+    store[:, :Ng].copy_(recv_lo)
+    store[:, n1g - Ng:].copy_(recv_hi)
 
-    def __init__(self, physical_system, group=None, slab=None):
+
+def slab_of(N_q, q_start, q_end, rank, world):
+    """(local N_q, local q_start, local q_end) of block ``rank`` of ``world``
+    equal blocks along one axis."""
+    if N_q % world:
+        raise ValueError('N_q = %d is not divisible by %d blocks' % (N_q, world))
+    n = N_q // world
+    dq = (q_end - q_start) / N_q
+    return n, q_start + rank * n * dq, q_start + (rank + 1) * n * dq
+
+
+class BlockSolver(object):
+    """nonlinear_solver of this rank's q-block of ``physical_system``'s domain,
+    on a ``dims`` = (P1, P2) grid of ranks (rank = r1 + P1 r2), stepped stage by
+    stage with halo exchanges.  Exposes the local solver as ``.local``.
+    ``block=(r1, r2)`` builds that block without a process group (several
+    blocks in one process, stepped in lockstep through begin_step /
+    stage_input / stage / end_step)."""
+
+    def __init__(self, physical_system, dims, group=None, block=None, external=None):
         from .physical_system import physical_system as PS
         from .nonlinear_solver import nonlinear_solver
         ps = physical_system
         bc = ps.boundary_conditions
-        if bc.in_q2_bottom != 'periodic' or bc.in_q2_top != 'periodic':
-            raise NotImplementedError('the q2 slabs split a periodic q2 axis')
+        P1, P2 = int(dims[0]), int(dims[1])
+        self.dims = (P1, P2)
+        # axes whose halos come from exchange(): every cut axis, or as given
+        ext1, ext2 = external if external is not None else (P1 > 1, P2 > 1)
+        self.external = (bool(ext1), bool(ext2))
+        self.group = group
+        if block is not None:
+            r1, r2 = block
+            self.rank = r1 + P1 * r2
+        else:
+            self.rank, world = _group_info(group)
+            if world != P1 * P2:
+                raise ValueError('%d ranks for a %d x %d block grid' % (world, P1, P2))
+            r1, r2 = self.rank % P1, self.rank // P1
+        self.coords = (r1, r2)
+        if ext1 and (bc.in_q1_left != 'periodic' or bc.in_q1_right != 'periodic'):
+            raise NotImplementedError('a q1 cut into blocks must be periodic')
+        if ext2 and (bc.in_q2_bottom != 'periodic' or bc.in_q2_top != 'periodic'):
+            raise NotImplementedError('a q2 cut into blocks must be periodic')
         if getattr(ps.params, 'fields_enabled', False):
             raise NotImplementedError('fields are not distributed')
-        self.group = group
-        self.rank, self.world = slab if slab is not None else _group_info(group)
         dom = types.ModuleType('domain')
-        for k in ('N_q1', 'q1_start', 'q1_end', 'N_p1', 'N_p2', 'N_p3', 'N_ghost'):
+        for k in ('N_p1', 'N_p2', 'N_p3', 'N_ghost'):
             setattr(dom, k, getattr(ps, k))
         for k in ('p1_start', 'p1_end', 'p2_start', 'p2_end', 'p3_start', 'p3_end'):
             setattr(dom, k, list(getattr(ps, k)))
-        n, lo, hi = slab_of(ps.N_q2, ps.q2_start, ps.q2_end, self.rank, self.world)
-        if n < ps.N_ghost:
-            raise ValueError('a slab of %d rows is thinner than N_ghost = %d' % (n, ps.N_ghost))
-        dom.N_q2, dom.q2_start, dom.q2_end = n, lo, hi
+        n1, lo1, hi1 = slab_of(ps.N_q1, ps.q1_start, ps.q1_end, r1, P1)
+        n2, lo2, hi2 = slab_of(ps.N_q2, ps.q2_start, ps.q2_end, r2, P2)
+        for n, e in ((n1, ext1), (n2, ext2)):
+            if e and n < ps.N_ghost:
+                raise ValueError('a block of %d cells is thinner than N_ghost = %d'
+                                 % (n, ps.N_ghost))
+        dom.N_q1, dom.q1_start, dom.q1_end = n1, lo1, hi1
+        dom.N_q2, dom.q2_start, dom.q2_end = n2, lo2, hi2
         lbc = types.ModuleType('boundary_conditions')
         lbc.__dict__.update({k: v for k, v in vars(bc).items() if not k.startswith('__')})
-        lbc.in_q2_bottom = lbc.in_q2_top = 'external'
+        if ext1:
+            lbc.in_q1_left = lbc.in_q1_right = 'external'
+        if ext2:
+            lbc.in_q2_bottom = lbc.in_q2_top = 'external'
         # a solver built on ps.params has turned mass and charge into (1, N_s)
-        # arrays (as the reference's does); the slab's solver starts from lists
+        # arrays (as the reference's does); the block's solver starts from lists
         lp = types.ModuleType('params')
         lp.__dict__.update({k: v for k, v in vars(ps.params).items() if not k.startswith('__')})
         for k in ('mass', 'charge'):
@@ -99,6 +162,10 @@ class SlabSolver(object):
         self.local = nonlinear_solver(local)
         self.Ng = self.local.N_ghost
         self.time_elapsed = 0.0
+        # neighbour ranks: (left, right) along q1, (down, up) along q2
+        at = lambda a, b: (a % P1) + P1 * (b % P2)
+        self.q1_neighbours = (at(r1 - 1, r2), at(r1 + 1, r2))
+        self.q2_neighbours = (at(r1, r2 - 1), at(r1, r2 + 1))
 
     def stage_count(self):
         return self.local.stage_count()
@@ -117,12 +184,36 @@ class SlabSolver(object):
         self.time_elapsed += dt
         self.local.check_divergence()
 
+    def exchange(self, store):
+        """The halo exchanges of one stage input (every rank calls it)."""
+        if self.external[1]:
+            exchange_q2_halos(store, self.Ng, self.group, self.q2_neighbours)
+        if self.external[0]:
+            exchange_q1_halos(store, self.Ng, self.group, self.q1_neighbours)
+
     def strang_timestep(self, dt):
         """One step of the whole distributed run (every rank calls it)."""
         self.begin_step()
         for k in range(self.stage_count()):
-            exchange_q2_halos(self.stage_input(k), self.Ng, self.group)
+            self.exchange(self.stage_input(k))
             self.stage(k, dt)
         self.end_step(dt)
 
     lie_timestep = swss_timestep = jia_timestep = strang_timestep
+
+
+class SlabSolver(BlockSolver):
+    """BlockSolver cutting q2 only, one slab per rank (``slab=(rank, world)``
+    builds that slab without a process group).  With one rank the slab is the
+    whole domain and its q2 halo wraps onto itself."""
+
+    def __init__(self, physical_system, group=None, slab=None):
+        if slab is not None:
+            rank, world = slab
+            super(SlabSolver, self).__init__(physical_system, (1, world), group,
+                                             block=(0, rank), external=(False, True))
+        else:
+            _, world = _group_info(group)
+            super(SlabSolver, self).__init__(physical_system, (1, world), group,
+                                             external=(False, True))
+        self.world = world

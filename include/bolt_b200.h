@@ -63,9 +63,9 @@ extern "C" {
 /* boundary conditions along q1/q2 (boundaries.py:415-577) */
 #define BOLT_BC_PERIODIC  0
 #define BOLT_BC_DIRICHLET 1
-/* q2 only: the ghost rows are supplied by the caller before every stage (a
- * q2 slab of a larger domain whose neighbours own those rows); the library
- * reads them and never writes them. */
+/* the ghost rows (q2) / columns (q1) are supplied by the caller before every
+ * stage (a block of a larger domain whose neighbours own those cells); the
+ * library reads them and never writes them. */
 #define BOLT_BC_EXTERNAL  2
 /* mirror (boundaries.py:226-301, cartesian p-grid): ghost cell i < 0 holds
  * interior cell -1-i (i >= N: 2N-1-i) with the p-index normal to the edge

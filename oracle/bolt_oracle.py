@@ -439,8 +439,8 @@ class Oracle(object):
         self.g = Grid(spec)
         self.f = np.array(f0, dtype=np.float64).reshape(self.g.fshape)
         self.tau = spec.get('tau', 1.0) if tau is None else tau
-        # bc_q2 == 'external': called on every stage input before its halo
-        # refresh, to fill the q2 ghost rows from the neighbouring slabs
+        # an 'external' axis: called on every stage input before its halo
+        # refresh, to fill the ghost rows / columns from the neighbouring blocks
         self.exchange = None
         self.time_elapsed = 0.0
         self.fields = None
@@ -478,6 +478,10 @@ class Oracle(object):
             # a q2 slab: its ghost rows were supplied by the neighbouring slabs
             out[:Ng] = f[:Ng]
             out[g.Nq2g - Ng:] = f[g.Nq2g - Ng:]
+        if sp['bc_q1'] == 'external':
+            # a q1 block: its ghost columns were supplied by the neighbours
+            out[:, :Ng] = f[:, :Ng]
+            out[:, g.Nq1g - Ng:] = f[:, g.Nq1g - Ng:]
         # apply_bcs_f (boundaries.py:415-577): side by side in the order left,
         # right, bottom, top, the mirror image (boundaries.py:226-301) and/or
         # the Dirichlet inflow values (boundaries.py:147-225)

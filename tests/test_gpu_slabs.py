@@ -94,3 +94,64 @@ def test_slabs_in_lockstep_equal_whole_domain(world, integrator, bc_q1, precisio
     m = torch.cat([_interior(s.local.compute_moments('density'), Ng) for s in slabs], dim=3)
     mref = _interior(whole.compute_moments('density'), Ng)
     assert float(((m - mref).abs().max() / mref.abs().max())) < tol
+
+
+def _exchange_blocks(blocks, dims, k):
+    """Halo rows, then halo columns, between blocks held in one process."""
+    P1, P2 = dims
+    Ng = blocks[0].Ng
+    xs = [b.stage_input(k) for b in blocks]
+    at = lambda a, c: (a % P1) + P1 * (c % P2)
+    if P2 > 1:
+        n = xs[0].shape[0]
+        bot = [xs[at(i % P1, i // P1 - 1)][n - 2 * Ng:n - Ng].clone() for i in range(len(xs))]
+        top = [xs[at(i % P1, i // P1 + 1)][Ng:2 * Ng].clone() for i in range(len(xs))]
+        for i, x in enumerate(xs):
+            x[:Ng].copy_(bot[i])
+            x[n - Ng:].copy_(top[i])
+    if P1 > 1:
+        n = xs[0].shape[1]
+        lft = [xs[at(i % P1 - 1, i // P1)][:, n - 2 * Ng:n - Ng].clone() for i in range(len(xs))]
+        rgt = [xs[at(i % P1 + 1, i // P1)][:, Ng:2 * Ng].clone() for i in range(len(xs))]
+        for i, x in enumerate(xs):
+            x[:, :Ng].copy_(lft[i])
+            x[:, n - Ng:].copy_(rgt[i])
+
+
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-13), ('fp32', 2e-6)])
+@pytest.mark.parametrize('dims', [(2, 2), (3, 1)])
+def test_blocks_in_lockstep_equal_whole_domain(dims, precision, tol):
+    """A P1 x P2 grid of q-blocks (external q1 columns and q2 rows) stepped in
+    lockstep on one GPU equals the whole-domain run."""
+    from bolt_b200.distributed import BlockSolver
+    P1, P2 = dims
+    spec = C.make(N_q1=8 * P1, N_q2=8 * P2, N_p1=8, N_p2=8, N_p3=4,
+                  p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+                  p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+                  tau=0.02, dt=1e-3, steps=4, integrator='RK4',
+                  riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                  init=dict(amp=0.1, k1=1, k2=2, u=[0.3, -0.2, 0.05], T=[1.0, 1.4, 0.8]))
+    whole = make_solver(spec, precision)
+    blocks = [BlockSolver(whole.physical_system, dims, block=(i % P1, i // P1))
+              for i in range(P1 * P2)]
+    Ng, n = spec['N_ghost'], 8
+    for i, b in enumerate(blocks):
+        r1, r2 = i % P1, i // P1
+        b.local.f = whole.f[:, :, r1 * n:r1 * n + n + 2 * Ng, r2 * n:r2 * n + n + 2 * Ng].clone()
+    dt = spec['dt']
+    for _ in range(spec['steps']):
+        whole.strang_timestep(dt)
+        for b in blocks:
+            b.begin_step()
+        for k in range(blocks[0].stage_count()):
+            _exchange_blocks(blocks, dims, k)
+            for b in blocks:
+                b.stage(k, dt)
+        for b in blocks:
+            b.end_step(dt)
+    cols = [torch.cat([_interior(blocks[r1 + P1 * r2].local.f, Ng) for r2 in range(P2)], dim=3)
+            for r1 in range(P1)]
+    got = torch.cat(cols, dim=2).double()
+    ref = _interior(whole.f, Ng).double()
+    err = float((got - ref).abs().max() / ref.abs().max())
+    assert err < tol, err

@@ -51,9 +51,9 @@ def test_ctx_create_rejects_bad_grids_without_gpu():
 
 
 def test_ctx_create_checks_boundary_conditions_without_gpu():
-    """Boundary codes are validated before any device work: an unknown code or
-    an external q1 is an argument error; a mirror whose ghost zone is deeper
-    than the grid, or a non-periodic axis without ghost cells, is unsupported."""
+    """Boundary codes are validated before any device work: an unknown code is
+    an argument error; a mirror whose ghost zone is deeper than the grid, or a
+    non-periodic axis without ghost cells, is unsupported."""
     lib = N.load()
 
     def create(bc_q1, bc_q2, N_q1=8, N_ghost=3):
@@ -66,7 +66,7 @@ def test_ctx_create_checks_boundary_conditions_without_gpu():
         ctx = ctypes.c_void_p()
         return lib.bolt_ctx_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(ctx))
     assert create(7, 'periodic') == N.BOLT_ERR_ARG
-    assert create('external', 'periodic') == N.BOLT_ERR_ARG
+    assert create(-1, 'periodic') == N.BOLT_ERR_ARG
     assert create('mirror', 'periodic', N_q1=2) == N.BOLT_ERR_UNSUPPORTED
     assert create('periodic', 'mirror+dirichlet', N_ghost=0) == N.BOLT_ERR_UNSUPPORTED
 

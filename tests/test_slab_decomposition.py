@@ -99,3 +99,81 @@ def test_slabs_over_two_gloo_ranks_equal_the_whole_domain():
     whole = o.f[Ng:Ng + spec['N_q2'], Ng:-Ng]     # interior cells
     slabs = np.concatenate([r[2] for r in res], axis=0)
     assert np.max(np.abs(slabs - whole)) <= 1e-15 * np.max(np.abs(whole))
+
+
+def _block_rank_main(rank, dims, port, out):
+    import datetime
+    import sys
+    sys.path[:0] = [ROOT, HERE, os.path.join(HERE, 'golden')]
+    import torch
+    import torch.distributed as dist
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    P1, P2 = dims
+    dist.init_process_group('gloo', rank=rank, world_size=P1 * P2,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        from bolt_b200.distributed import exchange_q1_halos, exchange_q2_halos, slab_of
+        import cases as C
+        from oracle.bolt_oracle import Oracle
+        spec = _spec()
+        Ng = spec['N_ghost']
+        r1, r2 = rank % P1, rank // P1
+        at = lambda a, b: (a % P1) + P1 * (b % P2)
+        n1, lo1, hi1 = slab_of(spec['N_q1'], spec['q1_start'], spec['q1_end'], r1, P1)
+        n2, lo2, hi2 = slab_of(spec['N_q2'], spec['q2_start'], spec['q2_end'], r2, P2)
+        local = dict(spec, N_q1=n1, q1_start=lo1, q1_end=hi1, N_q2=n2, q2_start=lo2,
+                     q2_end=hi2)
+        if P1 > 1:
+            local['bc_q1'] = 'external'
+        if P2 > 1:
+            local['bc_q2'] = 'external'
+        fg = C.initial_f(spec)
+        f0 = fg[r2 * n2:r2 * n2 + n2 + 2 * Ng, r1 * n1:r1 * n1 + n1 + 2 * Ng].copy()
+        o = Oracle(local, f0)
+
+        def exchange(x):
+            x = np.ascontiguousarray(x)
+            t = torch.from_numpy(x)
+            if P2 > 1:
+                exchange_q2_halos(t, Ng, None, (at(r1, r2 - 1), at(r1, r2 + 1)))
+            if P1 > 1:
+                exchange_q1_halos(t, Ng, None, (at(r1 - 1, r2), at(r1 + 1, r2)))
+            return x
+        o.exchange = exchange
+        for _ in range(spec['steps']):
+            o.step(spec['dt'])
+        out.put((rank, o.f[Ng:Ng + n2, Ng:Ng + n1].copy()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('dims', [(2, 2), (2, 1)])
+def test_blocks_over_gloo_ranks_equal_the_whole_domain(dims):
+    """A P1 x P2 grid of q-blocks (q1 columns exchanged packed, q2 rows in
+    place), the oracle advanced block by block equals the whole domain."""
+    import sys
+    sys.path[:0] = [ROOT, HERE, os.path.join(HERE, 'golden')]
+    import cases as C
+    from oracle.bolt_oracle import Oracle
+    P1, P2 = dims
+    world = P1 * P2
+    ctx = mp.get_context('spawn')
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_block_rank_main, args=(r, dims, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(out.get(timeout=300) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    spec = _spec()
+    o = Oracle(spec, C.initial_f(spec))
+    for _ in range(spec['steps']):
+        o.step(spec['dt'])
+    Ng = spec['N_ghost']
+    whole = o.f[Ng:Ng + spec['N_q2'], Ng:Ng + spec['N_q1']]
+    rows = [np.concatenate([res[r1 + P1 * r2] for r1 in range(P1)], axis=1) for r2 in range(P2)]
+    blocks = np.concatenate(rows, axis=0)
+    assert np.max(np.abs(blocks - whole)) <= 1e-15 * np.max(np.abs(whole))
