@@ -92,6 +92,8 @@ SIGNATURES = {
     'bolt_stage_count': (ctypes.c_int, [_VP]),
     'bolt_stage_input': (_VP, [_VP, _VP, ctypes.c_int]),
     'bolt_stage': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
+    'bolt_set_peer_halos': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
+    'bolt_stage_buffer': (_VP, [_VP, ctypes.c_int]),
     'bolt_moments': (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
     'bolt_fields_set': (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     'bolt_fields_get': (ctypes.c_int, [_VP, _VP, _VP, _VP]),

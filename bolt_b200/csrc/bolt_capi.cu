@@ -79,6 +79,9 @@ struct BoltCtx {
     double* es_part;
     double2 *es_rho, *es_e;
     int es_fwd, es_inv;
+    // q2 slab neighbours' copies of (f, buf[0], buf[1]): [0] below, [1] above
+    void* peer[2][3];
+    int peer_on;
     // misc
     const void* tau_arr;
     const void* dirichlet[4];
@@ -359,6 +362,29 @@ int bolt_set_dirichlet(BoltCtx* ctx, int side, const void* values_dev) {
     return BOLT_OK;
 }
 
+int bolt_set_peer_halos(BoltCtx* ctx, const void* const* below, const void* const* above) {
+    if (!ctx) return BOLT_ERR_ARG;
+    if (!below || !above) {
+        ctx->peer_on = 0;
+        memset(ctx->peer, 0, sizeof(ctx->peer));
+        return BOLT_OK;
+    }
+    if (ctx->p.bc_q2 != BOLT_BC_EXTERNAL || ctx->p.fields_enabled) return BOLT_ERR_UNSUPPORTED;
+    const int nb = ctx->p.integrator == BOLT_RK4 ? 3 : 2;   // f and the stage inputs
+    for (int i = 0; i < 3; ++i) {
+        if (i < nb && (!below[i] || !above[i])) return BOLT_ERR_ARG;
+        ctx->peer[0][i] = i < nb ? const_cast<void*>(below[i]) : nullptr;
+        ctx->peer[1][i] = i < nb ? const_cast<void*>(above[i]) : nullptr;
+    }
+    ctx->peer_on = 1;
+    return BOLT_OK;
+}
+
+void* bolt_stage_buffer(BoltCtx* ctx, int i) {
+    if (!ctx || i < 0 || i > 1) return nullptr;
+    return ctx->buf[i];
+}
+
 long long bolt_launch_count(BoltCtx* ctx) { return ctx ? ctx->launches : 0; }
 size_t bolt_scratch_bytes(BoltCtx* ctx) { return ctx ? ctx->scratch_bytes : 0; }
 
@@ -426,6 +452,8 @@ static int launch_moments5(BoltCtx* ctx, const void* f, double* part, cudaStream
 }
 
 struct StageIO {
+    void* peer_lo;          // neighbours' copies of out1 (q2 slab) or null
+    void* peer_hi;
     const void* fs;
     const void* base1;
     double c1;
@@ -458,6 +486,8 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     a.base2 = write_k ? nullptr : io.base2;
     a.out1 = io.out1;
     a.out2 = write_k ? nullptr : io.out2;
+    a.peer_lo = write_k ? nullptr : io.peer_lo;
+    a.peer_hi = write_k ? nullptr : io.peer_hi;
     a.tau_arr = ctx->tau_arr;
     a.mom_in = io.mom_in;
     a.mom_out = write_k ? nullptr : io.mom_out;
@@ -683,6 +713,16 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
     io.flag = last ? ctx->dflag : nullptr;
     void* out1;
     int ev;
+    // a q2 slab with peers: the stage also stores its boundary rows into the
+    // neighbours' copy of out1 (f, buf[0] or buf[1])
+    auto peers_of = [&](void* out) {
+        io.peer_lo = io.peer_hi = nullptr;
+        if (!ctx->peer_on) return;
+        const int idx = out == f ? 0 : (out == ctx->buf[0] ? 1 : (out == ctx->buf[1] ? 2 : -1));
+        if (idx < 0) return;
+        io.peer_lo = ctx->peer[0][idx];
+        io.peer_hi = ctx->peer[1][idx];
+    };
     if (ctx->p.integrator == BOLT_RK2) {
         // fvm_operator.py:22-33: f_half = f + k1*(dt/2); f = f_initial + k2*dt
         void* A = ctx->buf[0];
@@ -690,6 +730,7 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         io.base1 = f;
         io.c1 = k == 0 ? dt / 2 : dt;
         io.out1 = out1 = k == 0 ? A : f;
+        peers_of(out1);
         ev = fe && !ctx->at_n;
         rc = run_stage(ctx, io, ev, dt, st);
         if (fe) ctx->at_n ^= 1;
@@ -716,6 +757,7 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         io.fs = stages[k].fs; io.base1 = stages[k].b1; io.c1 = stages[k].c1;
         io.out1 = out1 = stages[k].o1; io.base2 = stages[k].b2; io.c2 = stages[k].c2;
         io.out2 = stages[k].o2;
+        peers_of(out1);
         rc = run_stage(ctx, io, fe && stages[k].ev, dt, st);
     }
     if (!rc && dir) rc = launch_ghosts(ctx, out1, st);

@@ -471,6 +471,11 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                             write_ghost_images(out1, o1, ii, jj, s, p, Ng, Nq1, Nq2,
                                                a.Nq1g, a.Nq2g, a.periodic1, a.periodic2,
                                                rowstride, colstride, Np);
+                        // a q2 slab: the neighbours' ghost rows of the same buffer
+                        if (a.peer_lo && jj < Ng)
+                            static_cast<T*>(a.peer_lo)[gidx + (long long)Nq2 * colstride] = o1;
+                        if (a.peer_hi && jj >= Nq2 - Ng)
+                            static_cast<T*>(a.peer_hi)[gidx - (long long)Nq2 * colstride] = o1;
                         if (a.flag && !isfinite(o1)) atomicOr(a.flag, 1);
                     }
                     stage[cq * PWP + lane] = cvalid ? o1 : T(0);

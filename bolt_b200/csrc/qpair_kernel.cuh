@@ -138,8 +138,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const int k_begin = split * a.chunks_per_split;
     const int k_end = min(Np / PW, k_begin + a.chunks_per_split);
     const int xs = s * Np;                           // TMA x coordinate of the species
+    const bool peer2 = a.peer_lo != nullptr;          // q2 images go to the neighbours
     const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ > Nq1 - Ng)) ||
-                        (a.periodic2 && (j0 < Ng || j0 + TQ > Nq2 - Ng));
+                        ((a.periodic2 || peer2) && (j0 < Ng || j0 + TQ > Nq2 - Ng));
 
     qpair_prologue<BGK>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, bars);
 
@@ -211,7 +212,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         g_dst = (j0 + Ng) * (int)colstride + (ii + Ng) * (int)rowstride + xs + lane;
         if (a.periodic1)
             g_d1 = ii < Ng ? Nq1 * (int)rowstride : (ii >= Nq1 - Ng ? -Nq1 * (int)rowstride : 0);
-        if (a.periodic2) {
+        if (a.periodic2 || peer2) {
             g_d2 = Nq2 * (int)colstride;
             g_bot = max(0, min(TQ, Ng - j0));
             g_top = min(TQ, max(0, Nq2 - Ng - j0));
@@ -335,6 +336,11 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         if (border) {
             const float* src = o1s + g_src;
             float* dst = out1 + (g_dst + k * PW);
+            // q2 images: this buffer (periodic q2) or the neighbours' copies
+            // (a q2 slab; their corner cells are not needed)
+            float* dlo = peer2 ? static_cast<float*>(a.peer_lo) + (g_dst + k * PW) : dst;
+            float* dhi = peer2 ? static_cast<float*>(a.peer_hi) + (g_dst + k * PW) : dst;
+            const int gc1 = peer2 ? 0 : g_d1;
             if (g_d1) {
 #pragma unroll
                 for (int r = 0; r < TQ; ++r)
@@ -342,13 +348,13 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             }
             for (int r = 0; r < g_bot; ++r) {
                 const float v = src[r * TQ * PW];
-                dst[r * (int)colstride + g_d2] = v;
-                if (g_d1) dst[r * (int)colstride + g_d1 + g_d2] = v;
+                dlo[r * (int)colstride + g_d2] = v;
+                if (gc1) dst[r * (int)colstride + gc1 + g_d2] = v;
             }
             for (int r = g_top; r < TQ; ++r) {
                 const float v = src[r * TQ * PW];
-                dst[r * (int)colstride - g_d2] = v;
-                if (g_d1) dst[r * (int)colstride + g_d1 - g_d2] = v;
+                dhi[r * (int)colstride - g_d2] = v;
+                if (gc1) dst[r * (int)colstride + gc1 - g_d2] = v;
             }
         }
 

@@ -162,10 +162,39 @@ class BlockSolver(object):
         self.local = nonlinear_solver(local)
         self.Ng = self.local.N_ghost
         self.time_elapsed = 0.0
+        self._peer = False          # peer halos off: exchange before every stage
+        self._halos_ready = False
         # neighbour ranks: (left, right) along q1, (down, up) along q2
         at = lambda a, b: (a % P1) + P1 * (b % P2)
         self.q1_neighbours = (at(r1 - 1, r2), at(r1 + 1, r2))
         self.q2_neighbours = (at(r1, r2 - 1), at(r1, r2 + 1))
+
+    # ---- peer halos: the stage kernels write the neighbours' ghost rows ------
+    def peer_buffers(self):
+        """Device pointers of this block's f store and RK stage buffers 0, 1
+        (what a neighbour passes to bolt_set_peer_halos)."""
+        lib, ctx = self.local._lib, self.local._ctx
+        return (self.local._fstore.data_ptr(), lib.bolt_stage_buffer(ctx, 0) or 0,
+                lib.bolt_stage_buffer(ctx, 1) or 0)
+
+    def set_peer_halos(self, below, above):
+        """q2 slabs only: the stage kernels store their boundary rows straight
+        into the lower / upper neighbours' buffers (``below`` / ``above`` =
+        their peer_buffers(), mapped into this process), so a stage needs no
+        exchange beforehand -- only an ordering between the blocks' stages.
+        None switches it off."""
+        from . import _native as N
+        if self.dims[0] > 1 or not self.external[1]:
+            raise NotImplementedError('peer halos: q2 slabs (P1 = 1) only')
+        lib, ctx = self.local._lib, self.local._ctx
+        if below is None:
+            N.check(lib.bolt_set_peer_halos(ctx, None, None), 'bolt_set_peer_halos')
+            self._peer = False
+            return
+        arr = N.ctypes.c_void_p * 3
+        N.check(lib.bolt_set_peer_halos(ctx, arr(*below), arr(*above)), 'bolt_set_peer_halos')
+        self._peer = True
+        self._halos_ready = False
 
     def stage_count(self):
         return self.local.stage_count()
@@ -184,19 +213,45 @@ class BlockSolver(object):
         self.time_elapsed += dt
         self.local.check_divergence()
 
+    def needs_exchange(self, k):
+        """Whether stage k's input needs exchange() first: always, unless peer
+        halos are on and the halos of f were made current once (the stages
+        then keep them current themselves)."""
+        return not (self._peer and (k > 0 or self._halos_ready))
+
     def exchange(self, store):
         """The halo exchanges of one stage input (every rank calls it)."""
         if self.external[1]:
             exchange_q2_halos(store, self.Ng, self.group, self.q2_neighbours)
         if self.external[0]:
             exchange_q1_halos(store, self.Ng, self.group, self.q1_neighbours)
+        if self._peer:
+            self._halos_ready = True
+
+    def refresh_halos(self):
+        """Make the halos of f current (collective): after f was written by
+        anything other than the stages."""
+        self._halos_ready = False
+
+    def _stage_barrier(self):
+        # every rank's stage k has finished (and written the neighbours'
+        # ghost rows) before any rank's stage k+1 reads them: a one-element
+        # all-reduce ordered on the stream after the stage kernel
+        if self.group is not None or (dist.is_available() and dist.is_initialized()):
+            import torch
+            if getattr(self, '_token', None) is None:
+                self._token = torch.zeros(1, device=self.local.device)
+            dist.all_reduce(self._token, group=self.group)
 
     def strang_timestep(self, dt):
         """One step of the whole distributed run (every rank calls it)."""
         self.begin_step()
         for k in range(self.stage_count()):
-            self.exchange(self.stage_input(k))
+            if self.needs_exchange(k):
+                self.exchange(self.stage_input(k))
             self.stage(k, dt)
+            if self._peer:
+                self._stage_barrier()
         self.end_step(dt)
 
     lie_timestep = swss_timestep = jia_timestep = strang_timestep

@@ -170,6 +170,20 @@ int   bolt_stage_count(BoltCtx* ctx);
 void* bolt_stage_input(BoltCtx* ctx, void* f_dev, int k);
 int   bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream);
 
+/* Peer halos of a q2 slab (bc_q2 = BOLT_BC_EXTERNAL, fields off): below[] and
+ * above[] are the lower and upper neighbours' device copies of
+ * (f, bolt_stage_buffer(0), bolt_stage_buffer(1)) -- on another GPU, its
+ * memory mapped into this process (CUDA IPC or symmetric memory).  Every stage
+ * then also stores its bottom / top N_g interior rows into the matching
+ * buffer's top / bottom ghost rows at the neighbours, from the stage kernel
+ * itself, so no exchange precedes the next stage.  The caller must order the
+ * slabs' stages: every slab's stage k completes before any slab's stage k+1
+ * (one bolt_stage per slab, then a barrier between the ranks).  Null arrays
+ * switch it off.  RK2 needs the first two entries. */
+int   bolt_set_peer_halos(BoltCtx* ctx, const void* const* below, const void* const* above);
+/* The context's RK stage buffers 0 and 1 (their neighbours' peer pointers). */
+void* bolt_stage_buffer(BoltCtx* ctx, int i);
+
 /* One moment (BOLT_MOM_*) of f over the whole ghosted grid, FP64, written to
  * out_dev[q2g][q1g][s] (moments.py definitions times dp1*dp2*dp3). */
 int  bolt_moments(BoltCtx* ctx, const void* f_dev, int moment_id, double* out_dev, void* stream);

@@ -155,3 +155,45 @@ def test_blocks_in_lockstep_equal_whole_domain(dims, precision, tol):
     ref = _interior(whole.f, Ng).double()
     err = float((got - ref).abs().max() / ref.abs().max())
     assert err < tol, err
+
+
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-13), ('fp32', 2e-6)])
+@pytest.mark.parametrize('world,integrator', [(2, 'RK4'), (3, 'RK4'), (2, 'RK2')])
+def test_peer_halo_slabs_equal_whole_domain(world, integrator, precision, tol):
+    """Slabs whose stage kernels store their boundary rows straight into the
+    neighbours' buffers (bolt_set_peer_halos; the neighbours are other
+    contexts on the same GPU here, their buffers at plain device pointers):
+    only the first stage input is exchanged, and the run equals the whole
+    domain.  FP32 runs the paired kernel's peer images, FP64 the scalar
+    kernel's."""
+    from bolt_b200.distributed import SlabSolver
+    spec = _spec(8 * world, integrator)
+    whole = make_solver(spec, precision)
+    slabs = [SlabSolver(whole.physical_system, slab=(r, world)) for r in range(world)]
+    Ng, n = spec['N_ghost'], 8
+    for r, s in enumerate(slabs):
+        s.local.f = whole.f[:, :, :, r * n:r * n + n + 2 * Ng].clone()
+    for r, s in enumerate(slabs):
+        s.set_peer_halos(slabs[(r - 1) % world].peer_buffers(),
+                         slabs[(r + 1) % world].peer_buffers())
+    dt = spec['dt']
+    exchanges = 0
+    for _ in range(spec['steps']):
+        whole.strang_timestep(dt)
+        for s in slabs:
+            s.begin_step()
+        for k in range(slabs[0].stage_count()):
+            if slabs[0].needs_exchange(k):
+                _exchange(slabs, k)
+                exchanges += 1
+                for s in slabs:
+                    s._halos_ready = True
+            for s in slabs:
+                s.stage(k, dt)
+        for s in slabs:
+            s.end_step(dt)
+    assert exchanges == 1
+    got = torch.cat([_interior(s.local.f, Ng) for s in slabs], dim=3).double()
+    ref = _interior(whole.f, Ng).double()
+    err = float((got - ref).abs().max() / ref.abs().max())
+    assert err < tol, err
