@@ -94,6 +94,9 @@ SIGNATURES = {
     'bolt_stage': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
     'bolt_set_peer_halos': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     'bolt_stage_buffer': (_VP, [_VP, ctypes.c_int]),
+    'bolt_ipc_get': (ctypes.c_int, [_VP, ctypes.c_char_p]),
+    'bolt_ipc_open': (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
+    'bolt_ipc_close': (ctypes.c_int, [_VP]),
     'bolt_moments': (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
     'bolt_fields_set': (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     'bolt_fields_get': (ctypes.c_int, [_VP, _VP, _VP, _VP]),

@@ -380,6 +380,29 @@ int bolt_set_peer_halos(BoltCtx* ctx, const void* const* below, const void* cons
     return BOLT_OK;
 }
 
+int bolt_ipc_get(const void* dev_ptr, unsigned char* handle64) {
+    if (!dev_ptr || !handle64) return BOLT_ERR_ARG;
+    cudaIpcMemHandle_t h;
+    if (cudaIpcGetMemHandle(&h, const_cast<void*>(dev_ptr)) != cudaSuccess) return BOLT_ERR_CUDA;
+    static_assert(sizeof(h) == 64, "CUDA IPC handles are 64 bytes");
+    memcpy(handle64, &h, sizeof(h));
+    return BOLT_OK;
+}
+
+int bolt_ipc_open(const unsigned char* handle64, void** dev_ptr) {
+    if (!handle64 || !dev_ptr) return BOLT_ERR_ARG;
+    cudaIpcMemHandle_t h;
+    memcpy(&h, handle64, sizeof(h));
+    if (cudaIpcOpenMemHandle(dev_ptr, h, cudaIpcMemLazyEnablePeerAccess) != cudaSuccess)
+        return BOLT_ERR_CUDA;
+    return BOLT_OK;
+}
+
+int bolt_ipc_close(void* dev_ptr) {
+    if (!dev_ptr) return BOLT_ERR_ARG;
+    return cudaIpcCloseMemHandle(dev_ptr) == cudaSuccess ? BOLT_OK : BOLT_ERR_CUDA;
+}
+
 void* bolt_stage_buffer(BoltCtx* ctx, int i) {
     if (!ctx || i < 0 || i > 1) return nullptr;
     return ctx->buf[i];

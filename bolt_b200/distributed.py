@@ -196,6 +196,50 @@ class BlockSolver(object):
         self._peer = True
         self._halos_ready = False
 
+    def enable_peer_halos(self):
+        """Collective: map the neighbouring ranks' f and stage buffers into
+        this process (CUDA IPC: torch's for f, bolt_ipc_* for the library's
+        stage buffers) and switch the peer halos on.  One process per GPU,
+        peer access between the GPUs (NVLink)."""
+        import ctypes
+        from torch.multiprocessing.reductions import reduce_tensor
+        from . import _native as N
+        lib, ctx = self.local._lib, self.local._ctx
+        handles = []
+        for i in range(2):
+            h = ctypes.create_string_buffer(64)
+            N.check(lib.bolt_ipc_get(lib.bolt_stage_buffer(ctx, i), h), 'bolt_ipc_get')
+            handles.append(h.raw)
+        mine = (reduce_tensor(self.local._fstore), handles)
+        _, world = _group_info(self.group)
+        every = [None] * world
+        dist.all_gather_object(every, mine, group=self.group)
+        self._mapped = getattr(self, '_mapped', {})
+
+        def mapped(r):
+            if r == self.rank:                              # one slab: its own buffers
+                return self.peer_buffers()
+            if r not in self._mapped:
+                (fn, args), hs = every[r]
+                ft = fn(*args)                              # keeps the mapping alive
+                ptrs = []
+                for h in hs:
+                    p = ctypes.c_void_p()
+                    N.check(lib.bolt_ipc_open(h, ctypes.byref(p)), 'bolt_ipc_open')
+                    ptrs.append(p.value)
+                self._mapped[r] = (ft, ptrs)
+            ft, ptrs = self._mapped[r]
+            return (ft.data_ptr(), ptrs[0], ptrs[1])
+        down, up = self.q2_neighbours
+        self.set_peer_halos(mapped(down), mapped(up))
+
+    def disable_peer_halos(self):
+        self.set_peer_halos(None, None)
+        for _, ptrs in getattr(self, '_mapped', {}).values():
+            for p in ptrs:
+                self.local._lib.bolt_ipc_close(p)
+        self._mapped = {}
+
     def stage_count(self):
         return self.local.stage_count()
 

@@ -183,6 +183,12 @@ int   bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream);
 int   bolt_set_peer_halos(BoltCtx* ctx, const void* const* below, const void* const* above);
 /* The context's RK stage buffers 0 and 1 (their neighbours' peer pointers). */
 void* bolt_stage_buffer(BoltCtx* ctx, int i);
+/* CUDA IPC of a whole device allocation (the stage buffers are): a 64-byte
+ * handle another process maps with bolt_ipc_open and releases with
+ * bolt_ipc_close. */
+int   bolt_ipc_get(const void* dev_ptr, unsigned char* handle64);
+int   bolt_ipc_open(const unsigned char* handle64, void** dev_ptr);
+int   bolt_ipc_close(void* dev_ptr);
 
 /* One moment (BOLT_MOM_*) of f over the whole ghosted grid, FP64, written to
  * out_dev[q2g][q1g][s] (moments.py definitions times dp1*dp2*dp3). */
