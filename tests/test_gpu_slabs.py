@@ -197,3 +197,33 @@ def test_peer_halo_slabs_equal_whole_domain(world, integrator, precision, tol):
     ref = _interior(whole.f, Ng).double()
     err = float((got - ref).abs().max() / ref.abs().max())
     assert err < tol, err
+
+
+def test_peer_halos_through_a_process_group(monkeypatch):
+    """The collective set-up and the per-stage ordering of the peer halos on a
+    one-rank NCCL group (the single slab is its own neighbour): the IPC handle
+    export, all_gather_object, the stage-ordering all-reduce -- equal to the
+    periodic run.  (Mapping another process's buffers needs a second GPU.)"""
+    import socket
+    import torch.distributed as dist
+    from bolt_b200.distributed import SlabSolver
+    with socket.socket() as sk:
+        sk.bind(('127.0.0.1', 0))
+        port = sk.getsockname()[1]
+    monkeypatch.setenv('MASTER_ADDR', '127.0.0.1')
+    monkeypatch.setenv('MASTER_PORT', str(port))
+    dist.init_process_group('nccl', rank=0, world_size=1)
+    try:
+        spec = _spec(16, 'RK4')
+        whole = make_solver(spec, 'fp32')
+        slab = SlabSolver(whole.physical_system)
+        slab.local.f = whole.f.clone()
+        slab.enable_peer_halos()
+        for _ in range(spec['steps']):
+            whole.strang_timestep(spec['dt'])
+            slab.strang_timestep(spec['dt'])
+        Ng = spec['N_ghost']
+        assert torch.equal(_interior(slab.local.f, Ng), _interior(whole.f, Ng))
+        slab.disable_peer_halos()
+    finally:
+        dist.destroy_process_group()
