@@ -32,7 +32,8 @@ BATCH_MOMENTS = ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy
 
 # schedules the autotuner times: (q-cells per work item, CTAs per SM, queue
 # order 1 = longest items first / 0 = run by run)
-TUNE_CANDIDATES = tuple((tq, c, o) for tq in (16, 32, 64) for c in (1, 2, 4, 8) for o in (1, 0))
+TUNE_CANDIDATES = tuple((tq, c, o) for tq in (8, 16, 32, 64) for c in (1, 2, 4, 8, 16)
+                        for o in (1, 0))
 _TUNED = {}    # (collisional, run shapes) -> schedule chosen in this process
 
 

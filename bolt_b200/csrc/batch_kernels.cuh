@@ -30,7 +30,7 @@
 namespace bolt {
 
 constexpr int kBatchNg = 3;          // ghost width (WENO5 stencil +-2 and the face shift)
-// a work item is a q-tile of 4 cells per warp; CTAs of 4, 8 or 16 warps
+// a work item is a q-tile of 4 cells per warp; CTAs of 2, 4, 8 or 16 warps
 constexpr int kBatchCellsPerWarp = 4;
 
 struct BatchRunDev {

@@ -6,8 +6,8 @@
 // the four f-sized buffers (f, RK4 stage buffers A, B and the accumulator C);
 // FP64 moment sums are packed by q-cell, [cell][5].  Work items (run, q-tile)
 // are consumed by persistent CTAs through an atomic queue that a memset node
-// resets before every stage.  The schedule -- q-cells per tile (16, 32 or 64:
-// CTAs of 4, 8 or 16 warps), CTAs per SM and the queue order (decreasing cost
+// resets before every stage.  The schedule -- q-cells per tile (8, 16, 32 or 64:
+// CTAs of 2, 4, 8 or 16 warps), CTAs per SM and the queue order (decreasing cost
 // = cells x p-chunks, or run by run) -- is set by bolt_batch_set_schedule; the
 // batch's autotuner (bolt_b200.batch) times the candidates on the batch
 // itself.  bolt_batch_run captures nsteps RK4 steps of all runs (4 stage
@@ -64,6 +64,7 @@ int stage_occupancy() {
 
 int occupancy(int tile_warps) {
     switch (tile_warps) {
+        case 2: return stage_occupancy<2>();
         case 4: return stage_occupancy<4>();
         case 8: return stage_occupancy<8>();
         default: return stage_occupancy<16>();
@@ -111,6 +112,7 @@ int build_schedule(BoltBatch* b) {
 
 void launch_stage(const BoltBatch* b, const BatchStageArgs& a, cudaStream_t st) {
     switch (b->tile_warps) {
+        case 2: batch_stage_kernel<2><<<b->nctas, 2 * 32, 0, st>>>(a); break;
         case 4: batch_stage_kernel<4><<<b->nctas, 4 * 32, 0, st>>>(a); break;
         case 8: batch_stage_kernel<8><<<b->nctas, 8 * 32, 0, st>>>(a); break;
         default: batch_stage_kernel<16><<<b->nctas, 16 * 32, 0, st>>>(a); break;
@@ -119,6 +121,10 @@ void launch_stage(const BoltBatch* b, const BatchStageArgs& a, cudaStream_t st) 
 
 void launch_moments(const BoltBatch* b, cudaStream_t st) {
     switch (b->tile_warps) {
+        case 2:
+            batch_moments_kernel<2><<<b->nctas, 2 * 32, 0, st>>>(
+                b->d_runs, b->d_items, b->nitems, b->counters, b->buf[0], b->mom[0]);
+            break;
         case 4:
             batch_moments_kernel<4><<<b->nctas, 4 * 32, 0, st>>>(
                 b->d_runs, b->d_items, b->nitems, b->counters, b->buf[0], b->mom[0]);
@@ -305,7 +311,8 @@ int bolt_batch_prepare(BoltBatch* b, void* stream) {
 
 int bolt_batch_set_schedule(BoltBatch* b, int tile_cells, int ctas_per_sm, int lpt_order) {
     if (!b || ctas_per_sm < 1) return BOLT_ERR_ARG;
-    if (tile_cells != 16 && tile_cells != 32 && tile_cells != 64) return BOLT_ERR_ARG;
+    if (tile_cells != 8 && tile_cells != 16 && tile_cells != 32 && tile_cells != 64)
+        return BOLT_ERR_ARG;
     if (cudaDeviceSynchronize() != cudaSuccess) return BOLT_ERR_CUDA;  // no launch uses the items
     b->tile_warps = tile_cells / kBatchCellsPerWarp;
     b->ctas_per_sm = ctas_per_sm;

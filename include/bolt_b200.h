@@ -282,8 +282,8 @@ int  bolt_batch_run(BoltBatch* b, int nsteps, void* stream);
 int  bolt_batch_moments(BoltBatch* b, double* out_dev, void* stream);
 /* 1 once a stage produced a non-finite value (cleared by the call). */
 int  bolt_batch_divergence_flag(BoltBatch* b);
-/* The launch schedule: q-cells per work item (16, 32 or 64: CTAs of 4, 8 or
- * 16 warps), persistent CTAs per SM (clamped to what fits), and the queue
+/* The launch schedule: q-cells per work item (8, 16, 32 or 64: CTAs of 2, 4,
+ * 8 or 16 warps), persistent CTAs per SM (clamped to what fits), and the queue
  * order (1: items by decreasing cells x p-chunks, 0: run by run).  Every
  * schedule gives bit-identical results; it changes only the speed.  The
  * default is (32, all that fit, 1).  Setting it synchronises the device and

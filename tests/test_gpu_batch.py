@@ -120,7 +120,7 @@ def test_every_schedule_gives_identical_results_and_autotune_keeps_the_state():
     systems = [bench.ragged_system(r) for r in RUNS]
     dts = [r['dt'] for r in RUNS]
     ref = None
-    for sched in [(32, 2, 1), (16, 4, 0), (64, 1, 1), (16, 1, 1)]:
+    for sched in [(32, 2, 1), (16, 4, 0), (64, 1, 1), (16, 1, 1), (8, 8, 1)]:
         bs = BatchSolver(systems, dts, autotune=False)
         bs.set_schedule(*sched)
         assert bs.schedule()[0] == sched[0]
