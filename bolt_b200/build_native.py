@@ -55,7 +55,7 @@ def build(force=False, verbose=False, ptxas_v=False):
     if not force and up_to_date():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src, extra in UNITS:
         obj = os.path.join(OUT_DIR, src.replace('.cu', '.o'))
         cmd = [nvcc()] + ARCH + COMMON + extra + ['-c', os.path.join(CSRC, src), '-o', obj]
@@ -63,8 +63,16 @@ def build(force=False, verbose=False, ptxas_v=False):
             cmd += ['-Xptxas', '-v']
         if verbose:
             print(' '.join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # the units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for res in list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            sys.stdout.write(res.stdout)
+            sys.stderr.write(res.stderr)
+            if res.returncode != 0:
+                raise subprocess.CalledProcessError(res.returncode, res.args)
     cmd = [nvcc()] + ARCH + ['-shared', '-o', LIB] + objs + ['-lcufft']
     subprocess.run(cmd, check=True)
     for o in objs:
