@@ -171,6 +171,15 @@ batch_stage_kernel(const BatchStageArgs a) {
                 S.set(right);
                 Weno5Walker<false, float> W;
                 const float (*Xb)[PW] = X[b];
+                // the combine bases of this warp's 4 cells, loaded before the
+                // stencil so that their latency overlaps it
+                float b1v[4], b2v[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const long long o = R.f_off + (long long)(i0 + j0 + q + kBatchNg) * Np1 + p;
+                    b1v[q] = a.base1[o];
+                    b2v[q] = a.out2 ? a.base2[o] : 0.0f;
+                }
                 // face between local cells f and f+1 reads rows f+1+off .. f+5+off
                 const int r0 = j0 + (right ? 0 : 1);
                 float y0 = Xb[r0][lane], y1 = Xb[r0 + 1][lane], y2 = Xb[r0 + 2][lane];
@@ -191,9 +200,9 @@ batch_stage_kernel(const BatchStageArgs a) {
                         k = fmaf(f0 - fc, inv_tau, k);
                     }
                     const long long o = R.f_off + (long long)(i0 + j + kBatchNg) * Np1 + p;
-                    const float o1 = fmaf(k, c1, a.base1[o]);
+                    const float o1 = fmaf(k, c1, b1v[q]);
                     a.out1[o] = o1;
-                    if (a.out2) a.out2[o] = fmaf(k, c2, a.base2[o]);
+                    if (a.out2) a.out2[o] = fmaf(k, c2, b2v[q]);
                     // periodic images of the border cells (2 N_g <= N_q1)
                     const int ii = i0 + j;
                     if (ii < kBatchNg) a.out1[o + (long long)Nq1 * Np1] = o1;
