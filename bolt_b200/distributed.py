@@ -20,10 +20,18 @@ Corner cells (ghost in both q1 and q2) are not exchanged: no interior update
 reads them, because the q1 and q2 stencils are separate.  An axis kept whole
 (P = 1) keeps the global problem's boundary condition.  Fields are not
 distributed: the reference's FFT initial solve is serial too (fft.py:26-27).
+
+Restart files stay those of a single-process run: PETSc writes a DMDA
+vector in the natural (q2, q1, dof) order whatever the process grid
+(dump.py:121-168, load.py:10-43), so each rank stores and reads its own rows
+of the one shared file (write_block_vec, read_block_vec).  The conserved
+totals of the whole run are one FP64 all-reduce of the blocks' sums.
 """
 
 import types
 
+import numpy as np
+import torch
 import torch.distributed as dist
 
 
@@ -86,6 +94,66 @@ def exchange_q1_halos(store, Ng, group=None, neighbours=None):
     store[:, n1g - Ng:].copy_(recv_hi)
 
 
+def _barrier(group):
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier(group=group)
+
+
+def write_block_vec(path, block, corner, shape, group=None, create=True, block_size=None):
+    """Collective write of one PETSc binary Vec holding a whole q-grid array in
+    natural order (q2, q1, dof), dof fastest -- what PETSc's VecView writes for
+    a DMDA global vector whatever the process grid (dump.py:121-168).
+
+    ``block`` is this rank's interior part, (n2, n1, dof) FP64, starting at
+    global interior cell ``corner`` = (j0, i0); ``shape`` = (N_q2, N_q1, dof).
+    The creating rank (rank 0 of ``group``; without a process group the caller
+    says which call creates, and calls the creating one first) writes the
+    header (int32 class id 1211214, int32 length, big-endian) and sizes the
+    file; after a barrier every rank stores its rows at their offsets."""
+    rank, _ = _group_info(group)
+    N2, N1, dof = (int(x) for x in shape)
+    n2, n1 = block.shape[0], block.shape[1]
+    j0, i0 = int(corner[0]), int(corner[1])
+    if block.shape[2] != dof or j0 < 0 or i0 < 0 or j0 + n2 > N2 or i0 + n1 > N1:
+        raise ValueError('block %s at %s does not fit %s' % (block.shape, corner, shape))
+    total = N2 * N1 * dof
+    if total >= 2 ** 31:
+        raise ValueError('a PETSc binary Vec holds fewer than 2^31 values')
+    collective = dist.is_available() and dist.is_initialized()
+    if (rank == 0) if collective else create:
+        with open(path, 'wb') as fh:
+            np.array([1211214, total], dtype='>i4').tofile(fh)
+            fh.truncate(8 + 8 * total)
+        with open(path + '.info', 'w') as fh:
+            fh.write('-vecload_block_size %d\n' % (block_size or dof))
+    _barrier(group)
+    mm = np.memmap(path, dtype='>f8', mode='r+', offset=8, shape=(N2, N1, dof))
+    mm[j0:j0 + n2, i0:i0 + n1] = block
+    mm.flush()
+    del mm
+    _barrier(group)
+
+
+def read_block_vec(path, corner, block_shape, shape):
+    """This rank's (n2, n1, dof) FP64 part, starting at global interior cell
+    ``corner``, of a PETSc binary Vec holding a (N_q2, N_q1, dof) q-grid array
+    in natural order (load.py:10-43: PETSc's VecLoad scatters the file to the
+    DMDA's ranks; each rank here reads its own rows)."""
+    N2, N1, dof = (int(x) for x in shape)
+    n2, n1 = int(block_shape[0]), int(block_shape[1])
+    j0, i0 = int(corner[0]), int(corner[1])
+    with open(path, 'rb') as fh:
+        hdr = np.fromfile(fh, dtype='>i4', count=2)
+    if hdr.size != 2 or int(hdr[0]) != 1211214:
+        raise IOError('%s is not a PETSc binary Vec' % path)
+    if int(hdr[1]) != N2 * N1 * dof:
+        raise IOError('%s holds %d values, the grid %d' % (path, int(hdr[1]), N2 * N1 * dof))
+    mm = np.memmap(path, dtype='>f8', mode='r', offset=8, shape=(N2, N1, dof))
+    out = np.array(mm[j0:j0 + n2, i0:i0 + n1], dtype=np.float64)
+    del mm
+    return out
+
+
 def slab_of(N_q, q_start, q_end, rank, world):
     """(local N_q, local q_start, local q_end) of block ``rank`` of ``world``
     equal blocks along one axis."""
@@ -124,6 +192,7 @@ class BlockSolver(object):
                 raise ValueError('%d ranks for a %d x %d block grid' % (world, P1, P2))
             r1, r2 = self.rank % P1, self.rank // P1
         self.coords = (r1, r2)
+        self._collective = block is None and dist.is_available() and dist.is_initialized()
         if ext1 and (bc.in_q1_left != 'periodic' or bc.in_q1_right != 'periodic'):
             raise NotImplementedError('a q1 cut into blocks must be periodic')
         if ext2 and (bc.in_q2_bottom != 'periodic' or bc.in_q2_top != 'periodic'):
@@ -282,7 +351,6 @@ class BlockSolver(object):
         # ghost rows) before any rank's stage k+1 reads them: a one-element
         # all-reduce ordered on the stream after the stage kernel
         if self.group is not None or (dist.is_available() and dist.is_initialized()):
-            import torch
             if getattr(self, '_token', None) is None:
                 self._token = torch.zeros(1, device=self.local.device)
             dist.all_reduce(self._token, group=self.group)
@@ -299,6 +367,60 @@ class BlockSolver(object):
         self.end_step(dt)
 
     lie_timestep = swss_timestep = jia_timestep = strang_timestep
+
+    # ---- the whole run's restart files and totals ----------------------------
+    def _grid(self, dof):
+        loc = self.local
+        corner = (self.coords[1] * loc.N_q2, self.coords[0] * loc.N_q1)
+        shape = (self.dims[1] * loc.N_q2, self.dims[0] * loc.N_q1, dof)
+        return corner, shape
+
+    def _dof(self):
+        loc = self.local
+        return loc.N_species * loc.N_p1 * loc.N_p2 * loc.N_p3
+
+    def dump_distribution_function(self, file_name):
+        """The whole run's interior f as one PETSc binary Vec, the file a
+        single-process run writes (collective; without a process group call
+        the blocks in rank order)."""
+        data = self.local._interior_store().to(torch.float64).cpu().numpy()
+        corner, shape = self._grid(self._dof())
+        write_block_vec(file_name + '.bin', data.reshape(data.shape[0], data.shape[1], -1),
+                        corner, shape, self.group if self._collective else None,
+                        create=self.rank == 0)
+
+    def load_distribution_function(self, file_name):
+        """This block's part of a whole-run f file (dump_distribution_function,
+        or a single-process run's); the halos are refreshed before the next
+        stage."""
+        loc = self.local
+        corner, shape = self._grid(self._dof())
+        vals = read_block_vec(file_name + '.bin', corner, (loc.N_q2, loc.N_q1), shape)
+        loc._load_interior(vals)
+        self.refresh_halos()
+
+    def dump_moments(self, file_name):
+        """The whole run's dump_moments file (collective, as
+        dump_distribution_function)."""
+        arr = self.local._moments_interior()
+        corner, shape = self._grid(arr.shape[2])
+        write_block_vec(file_name + '.bin', arr, corner, shape,
+                        self.group if self._collective else None, create=self.rank == 0)
+
+    def conserved_totals(self):
+        """Integrals over the whole q-domain of each species' density, bulk
+        momenta (v1, v2, v3) and energy, FP64 (5, N_s): this block's interior
+        sums, all-reduced over the group (collective; without a process group
+        the block's own share)."""
+        loc, g = self.local, self.Ng
+        rows = []
+        for name in ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy'):
+            m = loc._moment_store(name)
+            rows.append(m[g:m.shape[0] - g, g:m.shape[1] - g].sum(dim=(0, 1)))
+        t = torch.stack(rows) * (float(loc.dq1) * float(loc.dq2))
+        if self._collective:
+            dist.all_reduce(t, group=self.group)
+        return t
 
 
 class SlabSolver(BlockSolver):

@@ -559,10 +559,12 @@ class nonlinear_solver(object):
 
     def load_distribution_function(self, file_name):
         """load.py:10-43: read the Vec, copy to the interior, refresh halos."""
-        vals = _read_petsc_vec(file_name + '.bin')
-        g = self.N_ghost
-        inner = torch.from_numpy(vals).to(self.device, self.dtype).reshape(self._interior_store().shape)
-        self._interior_store().copy_(inner)
+        self._load_interior(_read_petsc_vec(file_name + '.bin'))
+
+    def _load_interior(self, vals):
+        """FP64 interior values in natural order (q2, q1, s, p) -> f, ghosts refilled."""
+        inner = torch.from_numpy(np.ascontiguousarray(vals)).to(self.device, self.dtype)
+        self._interior_store().copy_(inner.reshape(self._interior_store().shape))
         self._invalidate()
         N.check(self._lib.bolt_fill_ghosts(self._ctx, self._fstore.data_ptr(), self._stream()),
                 'bolt_fill_ghosts')
@@ -571,6 +573,11 @@ class nonlinear_solver(object):
     def dump_moments(self, file_name):
         """dump.py:41-119: all moments of the moments module, alphabetical,
         joined along the species axis, interior cells, PETSc binary Vec."""
+        arr = self._moments_interior()
+        _write_petsc_vec(file_name + '.bin', arr.reshape(-1), block=arr.shape[2])
+
+    def _moments_interior(self):
+        """(N_q2, N_q1, N_moments N_s) FP64 numpy array of dump_moments."""
         attrs = [a for a in dir(self.physical_system.moments) if not a.startswith('_')]
         if 'integral_over_v' in attrs:
             attrs.remove('integral_over_v')
@@ -579,8 +586,7 @@ class nonlinear_solver(object):
         for a in attrs:
             m = self._moment_store(a)
             parts.append(m[g:m.shape[0] - g, g:m.shape[1] - g])
-        arr = torch.cat(parts, dim=2).cpu().numpy()
-        _write_petsc_vec(file_name + '.bin', arr.reshape(-1), block=arr.shape[2])
+        return torch.cat(parts, dim=2).cpu().numpy()
 
     def dump_EM_fields(self, file_name):
         """dump.py:170-207: interior Yee-grid fields (q2, q1, component)."""

@@ -12,6 +12,7 @@ p).  The slabs are 8 rows, so FP32 runs the paired kernel with external q2
 ghosts.  Mirror walls along q1 (filled by the ghost pass after every stage)
 are covered as well."""
 
+import numpy as np
 import pytest
 import torch
 
@@ -157,6 +158,98 @@ def test_blocks_in_lockstep_equal_whole_domain(dims, precision, tol):
     assert err < tol, err
 
 
+def _read_vec(path):
+    from bolt_b200.nonlinear_solver import _read_petsc_vec
+    return _read_petsc_vec(path)
+
+
+def _raw(path):
+    with open(path, 'rb') as fh:
+        return fh.read()
+
+
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-13), ('fp32', 2e-6)])
+def test_block_grid_restart_files_and_totals(precision, tol, tmp_path):
+    """A 2 x 2 block grid writes one whole-run f file and one moments file
+    (each block its own rows; blocks called in rank order), loads a
+    whole-domain run's f file back block by block, and all-reduces the
+    conserved totals: the files hold the blocks' interiors in natural order
+    to the bit and equal the whole-domain run's files to the run's
+    tolerance; the loaded blocks continue the whole-domain run."""
+    from bolt_b200.distributed import BlockSolver
+    dims, (P1, P2) = (2, 2), (2, 2)
+    spec = C.make(N_q1=16, N_q2=16, N_p1=8, N_p2=8, N_p3=4,
+                  p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+                  p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+                  tau=0.02, dt=1e-3, steps=2, integrator='RK4',
+                  riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                  init=dict(amp=0.1, k1=1, k2=2, u=[0.3, -0.2, 0.05], T=[1.0, 1.4, 0.8]))
+    whole = make_solver(spec, precision)
+    mk = lambda: [BlockSolver(whole.physical_system, dims, block=(i % P1, i // P1))
+                  for i in range(P1 * P2)]
+    blocks = mk()
+    Ng, n = spec['N_ghost'], 8
+    for i, b in enumerate(blocks):
+        r1, r2 = i % P1, i // P1
+        b.local.f = whole.f[:, :, r1 * n:r1 * n + n + 2 * Ng, r2 * n:r2 * n + n + 2 * Ng].clone()
+
+    def step(bs):
+        for b in bs:
+            b.begin_step()
+        for k in range(bs[0].stage_count()):
+            _exchange_blocks(bs, dims, k)
+            for b in bs:
+                b.stage(k, spec['dt'])
+        for b in bs:
+            b.end_step(spec['dt'])
+
+    for _ in range(spec['steps']):
+        whole.strang_timestep(spec['dt'])
+        step(blocks)
+    for b in blocks:
+        b.dump_distribution_function(str(tmp_path / 'bf'))
+        b.dump_moments(str(tmp_path / 'bm'))
+    whole.dump_distribution_function(str(tmp_path / 'wf'))
+    whole.dump_moments(str(tmp_path / 'wm'))
+    # the file holds the blocks' own interiors, natural order, to the bit
+    got = _read_vec(str(tmp_path / 'bf.bin')).reshape(16, 16, -1)
+    for b in blocks:
+        r1, r2 = b.coords
+        mine = b.local._interior_store().double().cpu().numpy()
+        assert np.array_equal(got[r2 * n:r2 * n + n, r1 * n:r1 * n + n],
+                              mine.reshape(n, n, -1))
+    assert _raw(str(tmp_path / 'bf.bin'))[:8] == _raw(str(tmp_path / 'wf.bin'))[:8]
+    for a, c in (('bf', 'wf'), ('bm', 'wm')):
+        x, y = _read_vec(str(tmp_path / (a + '.bin'))), _read_vec(str(tmp_path / (c + '.bin')))
+        assert x.shape == y.shape
+        assert np.abs(x - y).max() <= tol * np.abs(y).max()
+    # conserved totals: the blocks' shares add up to the whole domain's
+    one = BlockSolver(whole.physical_system, (1, 1), block=(0, 0))
+    one.local.f = whole.f.clone()
+    tot = sum(b.conserved_totals() for b in blocks)
+    ref = one.conserved_totals()
+    assert tot.shape == (5, 1)
+    assert float((tot - ref).abs().max()) <= tol * float(ref.abs().max())
+    dens = _interior(whole.compute_moments('density'), Ng).sum() * whole.dq1 * whole.dq2
+    assert abs(float(ref[0, 0]) - float(dens)) <= 1e-12 * abs(float(dens))
+    # load the whole-domain file into fresh blocks and continue together
+    fresh = mk()
+    for b in fresh:
+        b.load_distribution_function(str(tmp_path / 'wf'))
+    wf = _interior(whole.f, Ng)
+    for b in fresh:
+        r1, r2 = b.coords
+        assert torch.equal(_interior(b.local.f, Ng),
+                           wf[:, :, r1 * n:r1 * n + n, r2 * n:r2 * n + n])
+    whole.strang_timestep(spec['dt'])
+    step(fresh)
+    cols = [torch.cat([_interior(fresh[r1 + P1 * r2].local.f, Ng) for r2 in range(P2)], dim=3)
+            for r1 in range(P1)]
+    err = float((torch.cat(cols, dim=2).double() - _interior(whole.f, Ng).double()).abs().max()
+                / _interior(whole.f, Ng).double().abs().max())
+    assert err < tol, err
+
+
 @pytest.mark.parametrize('precision,tol', [('fp64', 1e-13), ('fp32', 2e-6)])
 @pytest.mark.parametrize('world,integrator', [(2, 'RK4'), (3, 'RK4'), (2, 'RK2')])
 def test_peer_halo_slabs_equal_whole_domain(world, integrator, precision, tol):
@@ -199,7 +292,7 @@ def test_peer_halo_slabs_equal_whole_domain(world, integrator, precision, tol):
     assert err < tol, err
 
 
-def test_peer_halos_through_a_process_group(monkeypatch):
+def test_peer_halos_through_a_process_group(monkeypatch, tmp_path):
     """The collective set-up and the per-stage ordering of the peer halos on a
     one-rank NCCL group (the single slab is its own neighbour): the IPC handle
     export, all_gather_object, the stage-ordering all-reduce -- equal to the
@@ -223,6 +316,16 @@ def test_peer_halos_through_a_process_group(monkeypatch):
             whole.strang_timestep(spec['dt'])
             slab.strang_timestep(spec['dt'])
         Ng = spec['N_ghost']
+        assert torch.equal(_interior(slab.local.f, Ng), _interior(whole.f, Ng))
+        # the collective restart file (barriers over NCCL) and totals
+        slab.dump_distribution_function(str(tmp_path / 's'))
+        whole.dump_distribution_function(str(tmp_path / 'w'))
+        assert _raw(str(tmp_path / 's.bin')) == _raw(str(tmp_path / 'w.bin'))
+        tot = slab.conserved_totals()
+        assert tot.device.type == 'cuda' and tot.shape == (5, 2)
+        slab.load_distribution_function(str(tmp_path / 'w'))
+        slab.strang_timestep(spec['dt'])
+        whole.strang_timestep(spec['dt'])
         assert torch.equal(_interior(slab.local.f, Ng), _interior(whole.f, Ng))
         slab.disable_peer_halos()
     finally:
