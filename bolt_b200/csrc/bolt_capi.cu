@@ -79,8 +79,9 @@ struct BoltCtx {
     double* es_part;
     double2 *es_rho, *es_e;
     int es_fwd, es_inv;
-    // q2 slab neighbours' copies of (f, buf[0], buf[1]): [0] below, [1] above
-    void* peer[2][3];
+    // block neighbours' copies of (f, buf[0], buf[1]): [0] below, [1] above
+    // (q2), [2] left, [3] right (q1); peer_on bit 1: q2 on, bit 2: q1 on
+    void* peer[4][3];
     int peer_on;
     // misc
     const void* tau_arr;
@@ -362,22 +363,34 @@ int bolt_set_dirichlet(BoltCtx* ctx, int side, const void* values_dev) {
     return BOLT_OK;
 }
 
-int bolt_set_peer_halos(BoltCtx* ctx, const void* const* below, const void* const* above) {
+// neighbours lo / hi along one axis (side 0: q2, 1: q1) of an external axis
+static int set_peers(BoltCtx* ctx, int side, int bc, const void* const* lo,
+                     const void* const* hi) {
     if (!ctx) return BOLT_ERR_ARG;
-    if (!below || !above) {
-        ctx->peer_on = 0;
-        memset(ctx->peer, 0, sizeof(ctx->peer));
+    const int bit = 1 << side;
+    if (!lo || !hi) {
+        ctx->peer_on &= ~bit;
+        for (int i = 0; i < 3; ++i) ctx->peer[2 * side][i] = ctx->peer[2 * side + 1][i] = nullptr;
         return BOLT_OK;
     }
-    if (ctx->p.bc_q2 != BOLT_BC_EXTERNAL || ctx->p.fields_enabled) return BOLT_ERR_UNSUPPORTED;
+    if (bc != BOLT_BC_EXTERNAL || ctx->p.fields_enabled) return BOLT_ERR_UNSUPPORTED;
     const int nb = ctx->p.integrator == BOLT_RK4 ? 3 : 2;   // f and the stage inputs
+    for (int i = 0; i < nb; ++i)
+        if (!lo[i] || !hi[i]) return BOLT_ERR_ARG;
     for (int i = 0; i < 3; ++i) {
-        if (i < nb && (!below[i] || !above[i])) return BOLT_ERR_ARG;
-        ctx->peer[0][i] = i < nb ? const_cast<void*>(below[i]) : nullptr;
-        ctx->peer[1][i] = i < nb ? const_cast<void*>(above[i]) : nullptr;
+        ctx->peer[2 * side][i] = i < nb ? const_cast<void*>(lo[i]) : nullptr;
+        ctx->peer[2 * side + 1][i] = i < nb ? const_cast<void*>(hi[i]) : nullptr;
     }
-    ctx->peer_on = 1;
+    ctx->peer_on |= bit;
     return BOLT_OK;
+}
+
+int bolt_set_peer_halos(BoltCtx* ctx, const void* const* below, const void* const* above) {
+    return set_peers(ctx, 0, ctx ? ctx->p.bc_q2 : 0, below, above);
+}
+
+int bolt_set_peer_halos_q1(BoltCtx* ctx, const void* const* left, const void* const* right) {
+    return set_peers(ctx, 1, ctx ? ctx->p.bc_q1 : 0, left, right);
 }
 
 int bolt_ipc_get(const void* dev_ptr, unsigned char* handle64) {
@@ -475,8 +488,10 @@ static int launch_moments5(BoltCtx* ctx, const void* f, double* part, cudaStream
 }
 
 struct StageIO {
-    void* peer_lo;          // neighbours' copies of out1 (q2 slab) or null
+    void* peer_lo;          // neighbours' copies of out1 (q2 cut) or null
     void* peer_hi;
+    void* peer_left;        // neighbours' copies of out1 (q1 cut) or null
+    void* peer_right;
     const void* fs;
     const void* base1;
     double c1;
@@ -511,6 +526,8 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     a.out2 = write_k ? nullptr : io.out2;
     a.peer_lo = write_k ? nullptr : io.peer_lo;
     a.peer_hi = write_k ? nullptr : io.peer_hi;
+    a.peer_left = write_k ? nullptr : io.peer_left;
+    a.peer_right = write_k ? nullptr : io.peer_right;
     a.tau_arr = ctx->tau_arr;
     a.mom_in = io.mom_in;
     a.mom_out = write_k ? nullptr : io.mom_out;
@@ -736,15 +753,21 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
     io.flag = last ? ctx->dflag : nullptr;
     void* out1;
     int ev;
-    // a q2 slab with peers: the stage also stores its boundary rows into the
-    // neighbours' copy of out1 (f, buf[0] or buf[1])
+    // a block with peers: the stage also stores its boundary rows (q2) and
+    // columns (q1) into the neighbours' copy of out1 (f, buf[0] or buf[1])
     auto peers_of = [&](void* out) {
-        io.peer_lo = io.peer_hi = nullptr;
+        io.peer_lo = io.peer_hi = io.peer_left = io.peer_right = nullptr;
         if (!ctx->peer_on) return;
         const int idx = out == f ? 0 : (out == ctx->buf[0] ? 1 : (out == ctx->buf[1] ? 2 : -1));
         if (idx < 0) return;
-        io.peer_lo = ctx->peer[0][idx];
-        io.peer_hi = ctx->peer[1][idx];
+        if (ctx->peer_on & 1) {
+            io.peer_lo = ctx->peer[0][idx];
+            io.peer_hi = ctx->peer[1][idx];
+        }
+        if (ctx->peer_on & 2) {
+            io.peer_left = ctx->peer[2][idx];
+            io.peer_right = ctx->peer[3][idx];
+        }
     };
     if (ctx->p.integrator == BOLT_RK2) {
         // fvm_operator.py:22-33: f_half = f + k1*(dt/2); f = f_initial + k2*dt

@@ -121,6 +121,12 @@ struct QStageArgs {
     // top ghost rows), the top N_g rows N_q2 rows lower in peer_hi
     void* peer_lo;
     void* peer_hi;
+    // q1 block neighbours' copies of out1 (or null): the left N_g interior
+    // columns are also stored N_q1 columns further right in peer_left (the
+    // left neighbour's right ghost columns), the right N_g columns N_q1
+    // columns further left in peer_right
+    void* peer_left;
+    void* peer_right;
 };
 
 struct PStageArgs {

@@ -476,6 +476,11 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
                             static_cast<T*>(a.peer_lo)[gidx + (long long)Nq2 * colstride] = o1;
                         if (a.peer_hi && jj >= Nq2 - Ng)
                             static_cast<T*>(a.peer_hi)[gidx - (long long)Nq2 * colstride] = o1;
+                        // a q1 block: the neighbours' ghost columns
+                        if (a.peer_left && ii < Ng)
+                            static_cast<T*>(a.peer_left)[gidx + (long long)Nq1 * rowstride] = o1;
+                        if (a.peer_right && ii >= Nq1 - Ng)
+                            static_cast<T*>(a.peer_right)[gidx - (long long)Nq1 * rowstride] = o1;
                         if (a.flag && !isfinite(o1)) atomicOr(a.flag, 1);
                     }
                     stage[cq * PWP + lane] = cvalid ? o1 : T(0);

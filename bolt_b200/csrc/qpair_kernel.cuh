@@ -139,7 +139,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const int k_end = min(Np / PW, k_begin + a.chunks_per_split);
     const int xs = s * Np;                           // TMA x coordinate of the species
     const bool peer2 = a.peer_lo != nullptr;          // q2 images go to the neighbours
-    const bool border = (a.periodic1 && (i0 < Ng || i0 + TQ > Nq1 - Ng)) ||
+    const bool peer1 = a.peer_left != nullptr;        // q1 images go to the neighbours
+    const bool border = ((a.periodic1 || peer1) && (i0 < Ng || i0 + TQ > Nq1 - Ng)) ||
                         ((a.periodic2 || peer2) && (j0 < Ng || j0 + TQ > Nq2 - Ng));
 
     qpair_prologue<BGK>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, bars);
@@ -210,7 +211,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         const int ii = i0 + warp;
         g_src = swz(warp, lane);                           // row r adds r*TQ*PW
         g_dst = (j0 + Ng) * (int)colstride + (ii + Ng) * (int)rowstride + xs + lane;
-        if (a.periodic1)
+        if (a.periodic1 || peer1)
             g_d1 = ii < Ng ? Nq1 * (int)rowstride : (ii >= Nq1 - Ng ? -Nq1 * (int)rowstride : 0);
         if (a.periodic2 || peer2) {
             g_d2 = Nq2 * (int)colstride;
@@ -336,15 +337,18 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         if (border) {
             const float* src = o1s + g_src;
             float* dst = out1 + (g_dst + k * PW);
-            // q2 images: this buffer (periodic q2) or the neighbours' copies
-            // (a q2 slab; their corner cells are not needed)
+            // q1 / q2 images: this buffer (periodic axis) or the neighbours'
+            // copies (a cut axis; then no corner cell is needed)
             float* dlo = peer2 ? static_cast<float*>(a.peer_lo) + (g_dst + k * PW) : dst;
             float* dhi = peer2 ? static_cast<float*>(a.peer_hi) + (g_dst + k * PW) : dst;
-            const int gc1 = peer2 ? 0 : g_d1;
+            const int gc1 = (peer1 || peer2) ? 0 : g_d1;
             if (g_d1) {
+                float* d1 = peer1 ? static_cast<float*>(g_d1 > 0 ? a.peer_left : a.peer_right) +
+                                        (g_dst + k * PW)
+                                  : dst;
 #pragma unroll
                 for (int r = 0; r < TQ; ++r)
-                    dst[r * (int)colstride + g_d1] = src[r * TQ * PW];
+                    d1[r * (int)colstride + g_d1] = src[r * TQ * PW];
             }
             for (int r = 0; r < g_bot; ++r) {
                 const float v = src[r * TQ * PW];

@@ -238,7 +238,7 @@ class BlockSolver(object):
         self.q1_neighbours = (at(r1 - 1, r2), at(r1 + 1, r2))
         self.q2_neighbours = (at(r1, r2 - 1), at(r1, r2 + 1))
 
-    # ---- peer halos: the stage kernels write the neighbours' ghost rows ------
+    # ---- peer halos: the stage kernels write the neighbours' ghost cells -----
     def peer_buffers(self):
         """Device pointers of this block's f store and RK stage buffers 0, 1
         (what a neighbour passes to bolt_set_peer_halos)."""
@@ -246,22 +246,30 @@ class BlockSolver(object):
         return (self.local._fstore.data_ptr(), lib.bolt_stage_buffer(ctx, 0) or 0,
                 lib.bolt_stage_buffer(ctx, 1) or 0)
 
-    def set_peer_halos(self, below, above):
-        """q2 slabs only: the stage kernels store their boundary rows straight
-        into the lower / upper neighbours' buffers (``below`` / ``above`` =
-        their peer_buffers(), mapped into this process), so a stage needs no
-        exchange beforehand -- only an ordering between the blocks' stages.
-        None switches it off."""
+    def set_peer_halos(self, below, above, left=None, right=None):
+        """The stage kernels store their boundary rows straight into the lower
+        / upper neighbours' buffers (``below`` / ``above``) and their boundary
+        columns into the left / right neighbours' (``left`` / ``right``): each
+        the neighbour's peer_buffers(), mapped into this process.  Every cut
+        axis needs its pair, so that a stage needs no exchange beforehand --
+        only an ordering between the blocks' stages.  ``below=None`` switches
+        it off."""
         from . import _native as N
-        if self.dims[0] > 1 or not self.external[1]:
-            raise NotImplementedError('peer halos: q2 slabs (P1 = 1) only')
         lib, ctx = self.local._lib, self.local._ctx
-        if below is None:
+        if below is None and left is None:
             N.check(lib.bolt_set_peer_halos(ctx, None, None), 'bolt_set_peer_halos')
+            N.check(lib.bolt_set_peer_halos_q1(ctx, None, None), 'bolt_set_peer_halos_q1')
             self._peer = False
             return
+        if (below is not None) != self.external[1] or (left is not None) != self.external[0]:
+            raise ValueError('peer halos: one pair of neighbours per cut axis, none for the others')
         arr = N.ctypes.c_void_p * 3
-        N.check(lib.bolt_set_peer_halos(ctx, arr(*below), arr(*above)), 'bolt_set_peer_halos')
+        if below is not None:
+            N.check(lib.bolt_set_peer_halos(ctx, arr(*below), arr(*above)),
+                    'bolt_set_peer_halos')
+        if left is not None:
+            N.check(lib.bolt_set_peer_halos_q1(ctx, arr(*left), arr(*right)),
+                    'bolt_set_peer_halos_q1')
         self._peer = True
         self._halos_ready = False
 
@@ -300,7 +308,11 @@ class BlockSolver(object):
             ft, ptrs = self._mapped[r]
             return (ft.data_ptr(), ptrs[0], ptrs[1])
         down, up = self.q2_neighbours
-        self.set_peer_halos(mapped(down), mapped(up))
+        lft, rgt = self.q1_neighbours
+        self.set_peer_halos(mapped(down) if self.external[1] else None,
+                            mapped(up) if self.external[1] else None,
+                            mapped(lft) if self.external[0] else None,
+                            mapped(rgt) if self.external[0] else None)
 
     def disable_peer_halos(self):
         self.set_peer_halos(None, None)

@@ -181,6 +181,14 @@ int   bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream);
  * (one bolt_stage per slab, then a barrier between the ranks).  Null arrays
  * switch it off.  RK2 needs the first two entries. */
 int   bolt_set_peer_halos(BoltCtx* ctx, const void* const* below, const void* const* above);
+/* The same along q1 for a block of a P1 x P2 grid (bc_q1 = BOLT_BC_EXTERNAL):
+ * left[] and right[] are the q1 neighbours' copies; every stage also stores
+ * its left / right N_g interior columns into their right / left ghost
+ * columns.  Corner ghost cells are written by neither call: no interior
+ * update reads them.  Replaces the q1 part of the DMDA halo refresh
+ * (communicate.py:8-38, nonlinear_solver.py:251-280).  Null arrays switch
+ * it off. */
+int   bolt_set_peer_halos_q1(BoltCtx* ctx, const void* const* left, const void* const* right);
 /* The context's RK stage buffers 0 and 1 (their neighbours' peer pointers). */
 void* bolt_stage_buffer(BoltCtx* ctx, int i);
 /* CUDA IPC of a whole device allocation (the stage buffers are): a 64-byte

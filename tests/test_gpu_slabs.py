@@ -292,6 +292,66 @@ def test_peer_halo_slabs_equal_whole_domain(world, integrator, precision, tol):
     assert err < tol, err
 
 
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-13), ('fp32', 2e-6)])
+@pytest.mark.parametrize('dims,integrator', [((2, 2), 'RK4'), ((3, 1), 'RK4'), ((2, 2), 'RK2')])
+def test_peer_halo_blocks_equal_whole_domain(dims, integrator, precision, tol):
+    """A P1 x P2 block grid whose stage kernels store their boundary rows and
+    columns straight into the neighbours' buffers (bolt_set_peer_halos and
+    bolt_set_peer_halos_q1; the neighbours are other contexts on the same
+    GPU): only the first stage input is exchanged, and the run equals the
+    whole domain.  With P2 = 1 the q2 axis stays periodic inside each block."""
+    from bolt_b200.distributed import BlockSolver
+    P1, P2 = dims
+    spec = C.make(N_q1=8 * P1, N_q2=8 * P2, N_p1=8, N_p2=8, N_p3=4,
+                  p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+                  p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+                  tau=0.02, dt=1e-3, steps=4, integrator=integrator,
+                  riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                  init=dict(amp=0.1, k1=1, k2=2, u=[0.3, -0.2, 0.05], T=[1.0, 1.4, 0.8]))
+    whole = make_solver(spec, precision)
+    blocks = [BlockSolver(whole.physical_system, dims, block=(i % P1, i // P1))
+              for i in range(P1 * P2)]
+    Ng, n = spec['N_ghost'], 8
+    for i, b in enumerate(blocks):
+        r1, r2 = i % P1, i // P1
+        b.local.f = whole.f[:, :, r1 * n:r1 * n + n + 2 * Ng, r2 * n:r2 * n + n + 2 * Ng].clone()
+    if P2 > 1:
+        with pytest.raises(ValueError):          # a cut axis without its neighbours
+            blocks[0].set_peer_halos(None, None, blocks[1].peer_buffers(),
+                                     blocks[1].peer_buffers())
+    for b in blocks:
+        nb = lambda r: blocks[r].peer_buffers()
+        (lft, rgt), (dn, up) = b.q1_neighbours, b.q2_neighbours
+        b.set_peer_halos(nb(dn) if P2 > 1 else None, nb(up) if P2 > 1 else None,
+                         nb(lft), nb(rgt))
+    dt = spec['dt']
+    exchanges = 0
+    for _ in range(spec['steps']):
+        whole.strang_timestep(dt)
+        for b in blocks:
+            b.begin_step()
+        for k in range(blocks[0].stage_count()):
+            if blocks[0].needs_exchange(k):
+                _exchange_blocks(blocks, dims, k)
+                exchanges += 1
+                for b in blocks:
+                    b._halos_ready = True
+            for b in blocks:
+                b.stage(k, dt)
+        for b in blocks:
+            b.end_step(dt)
+    assert exchanges == 1
+    cols = [torch.cat([_interior(blocks[r1 + P1 * r2].local.f, Ng) for r2 in range(P2)], dim=3)
+            for r1 in range(P1)]
+    got = torch.cat(cols, dim=2).double()
+    ref = _interior(whole.f, Ng).double()
+    err = float((got - ref).abs().max() / ref.abs().max())
+    assert err < tol, err
+    for b in blocks:
+        b.set_peer_halos(None, None)
+        assert b.needs_exchange(1)
+
+
 def test_peer_halos_through_a_process_group(monkeypatch, tmp_path):
     """The collective set-up and the per-stage ordering of the peer halos on a
     one-rank NCCL group (the single slab is its own neighbour): the IPC handle
