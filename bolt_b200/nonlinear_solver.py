@@ -210,8 +210,10 @@ class nonlinear_solver(object):
         self.q2_left_bot = q2_lb.expand(shape).contiguous()
         self.q1_center_bot = self.q1_left_bot + 0.5 * self.dq1
         self.q2_center_bot = self.q2_left_bot
+        # calculate_q.py:35-38 returns (q1_left_center, q2_center_bot) as the
+        # left-centre grid: its q2 is the cell's bottom face, as here
         self.q1_left_center = self.q1_left_bot
-        self.q2_left_center = self.q2_left_bot + 0.5 * self.dq2
+        self.q2_left_center = self.q2_center_bot
         self.q1_center = self.q1_left_bot + 0.5 * self.dq1
         self.q2_center = self.q2_left_bot + 0.5 * self.dq2
         ps = self.physical_system
@@ -368,6 +370,69 @@ class nonlinear_solver(object):
             self._init_fields(params)
 
     # ---- fields initialisation (fields.py:421-495, fft.py:9-78) -------------------------
+    def _user_field(self, fn, k, q1, q2, params):
+        """Component k of a user field function on one of the staggered q-grids,
+        as a (N_q2 + 2N_g, N_q1 + 2N_g) FP64 tensor."""
+        Nq1g, Nq2g = self.N_q1_local_with_Ng, self.N_q2_local_with_Ng
+        a = torch.as_tensor(fn(q1, q2, params)[k], dtype=torch.float64, device=self.device)
+        return a.expand(1, 1, Nq1g, Nq2g).reshape(Nq1g, Nq2g).T
+
+    def _user_E(self, params):
+        """fields.py:280-337: E1 on the left-centre grid (q2 at the bottom face,
+        see _build_grids), E2 at (centre, bottom), E3 at the centre, from
+        initialize_E; or from initialize_A_phi by the reference's one-sided
+        differences of A and phi."""
+        ini = self.physical_system.initial_conditions
+        u = lambda fn, k, at: self._user_field(fn, k, *at, params)
+        lc = (self.q1_left_center, self.q2_left_center)
+        cb = (self.q1_center_bot, self.q2_center_bot)
+        cc = (self.q1_center, self.q2_center)
+        lb = (self.q1_left_bot, self.q2_left_bot)
+        if hasattr(ini, 'initialize_E'):
+            E = ini.initialize_E
+            return torch.stack([u(E, 0, lc), u(E, 1, cb), u(E, 2, cc)])
+        if hasattr(ini, 'initialize_A_phi'):
+            F = ini.initialize_A_phi
+            A1, A2, A3, phi = u(F, 0, cb), u(F, 1, lc), u(F, 2, lb), u(F, 3, cc)
+            dA3_dq2 = (_shift(A3, 0, -1) - A3) / self.dq2
+            dA3_dq1 = (_shift(A3, -1, 0) - A3) / self.dq1
+            dA2_dq1 = (_shift(A2, -1, 0) - A2) / self.dq1
+            dA1_dq2 = (_shift(A1, 0, -1) - A1) / self.dq2
+            dphi_dq1 = -(_shift(phi, 1, 0) - phi) / self.dq1
+            dphi_dq2 = -(_shift(phi, 0, 1) - phi) / self.dq2
+            return torch.stack([dA3_dq2 - dphi_dq1, -dA3_dq1 - dphi_dq2, dA2_dq1 - dA1_dq2])
+        raise NotImplementedError('Initialization method for electric fields not valid/found')
+
+    def _user_B(self, params):
+        """fields.py:339-410: B1 at (centre, bottom), B2 on the left-centre
+        grid, B3 at (left, bottom), from initialize_B; or from initialize_A, or
+        from initialize_A3_B3 (B1, B2 as backward differences of A3)."""
+        ini = self.physical_system.initial_conditions
+        u = lambda fn, k, at: self._user_field(fn, k, *at, params)
+        lc = (self.q1_left_center, self.q2_left_center)
+        cb = (self.q1_center_bot, self.q2_center_bot)
+        cc = (self.q1_center, self.q2_center)
+        lb = (self.q1_left_bot, self.q2_left_bot)
+        if hasattr(ini, 'initialize_B') and hasattr(ini, 'initialize_A3_B3'):
+            raise Exception('Can\'t use both initialize_B and initialize_A3_B3!')
+        if hasattr(ini, 'initialize_B'):
+            B = ini.initialize_B
+            return torch.stack([u(B, 0, cb), u(B, 1, lc), u(B, 2, lb)])
+        if hasattr(ini, 'initialize_A'):
+            F = ini.initialize_A
+            A1, A2, A3 = u(F, 0, lc), u(F, 1, cb), u(F, 2, cc)
+            B1 = (_shift(A3, 0, -1) - A3) / self.dq2
+            B2 = -(_shift(A3, -1, 0) - A3) / self.dq1
+            B3 = (_shift(A2, -1, 0) - A2) / self.dq1 - (_shift(A1, 0, -1) - A1) / self.dq2
+            return torch.stack([B1, B2, B3])
+        if hasattr(ini, 'initialize_A3_B3'):
+            F = ini.initialize_A3_B3
+            A3 = u(F, 0, cc)
+            B1 = (A3 - _shift(A3, 0, 1)) / self.dq2
+            B2 = -(A3 - _shift(A3, 1, 0)) / self.dq1
+            return torch.stack([B1, B2, u(F, 1, lb)])
+        raise NotImplementedError('Initialization method for magnetic fields not valid/found')
+
     def _init_fields(self, params):
         dev, Ng = self.device, self.N_ghost
         Nq1g, Nq2g = self.N_q1_local_with_Ng, self.N_q2_local_with_Ng
@@ -375,7 +440,7 @@ class nonlinear_solver(object):
         yee = torch.zeros_like(cell)
         eps = float(getattr(params, 'eps', 1.0))
         init = params.fields_initialize
-        if init == 'fft':
+        if init in ('fft', 'fft + user-defined magnetic fields'):
             dens = self._moment_store('density')                       # (Nq2g, Nq1g, Ns)
             q = torch.tensor(self._charge, dtype=torch.float64, device=dev)
             rho = (dens * q).sum(dim=2)
@@ -397,19 +462,16 @@ class nonlinear_solver(object):
             yee[0] = 0.5 * (cell[0] + torch.roll(cell[0], 1, dims=1))
             yee[1] = 0.5 * (cell[1] + torch.roll(cell[1], 1, dims=0))
             yee[2] = cell[2]
+            if init != 'fft':
+                # fields.py:477-482: user B on the Yee grid, then its cell values
+                yee[3:6] = self._user_B(params)
+                cell[3:6] = _yee_to_cell(yee)[3:6]
             yee = _periodic_fill_fields(yee, Ng, self.N_q1, self.N_q2)
         elif init == 'user-defined':
-            ini = self.physical_system.initial_conditions
-            st = lambda a: a.reshape(self.N_q1_local_with_Ng, self.N_q2_local_with_Ng).T \
-                if torch.is_tensor(a) else torch.full((Nq2g, Nq1g), float(a), dtype=torch.float64, device=dev)
-            E = ini.initialize_E
-            B = ini.initialize_B
-            yee[0] = st(torch.as_tensor(E(self.q1_left_center, self.q2_left_center, params)[0], device=dev).expand(1, 1, Nq1g, Nq2g))
-            yee[1] = st(torch.as_tensor(E(self.q1_center_bot, self.q2_center_bot, params)[1], device=dev).expand(1, 1, Nq1g, Nq2g))
-            yee[2] = st(torch.as_tensor(E(self.q1_center, self.q2_center, params)[2], device=dev).expand(1, 1, Nq1g, Nq2g))
-            yee[3] = st(torch.as_tensor(B(self.q1_center_bot, self.q2_center_bot, params)[0], device=dev).expand(1, 1, Nq1g, Nq2g))
-            yee[4] = st(torch.as_tensor(B(self.q1_left_center, self.q2_left_center, params)[1], device=dev).expand(1, 1, Nq1g, Nq2g))
-            yee[5] = st(torch.as_tensor(B(self.q1_left_bot, self.q2_left_bot, params)[2], device=dev).expand(1, 1, Nq1g, Nq2g))
+            # fields.py:472-475: Yee E and B from the user's functions, then
+            # every cell-centred field from the (not yet refreshed) Yee grid
+            yee[0:3] = self._user_E(params)
+            yee[3:6] = self._user_B(params)
             cell = _yee_to_cell(yee)
             yee = _periodic_fill_fields(yee, Ng, self.N_q1, self.N_q2)
         else:
@@ -632,6 +694,16 @@ def _as_list(v, n):
     if torch.is_tensor(v):
         return [float(x) for x in v.reshape(-1)[:n].tolist()]
     return list(v)
+
+
+def _shift(a, s1, s2):
+    """af.shift(a, 0, 0, s1, s2) of Bolt's (..., q1, q2) arrays on this
+    module's (..., N_q2g, N_q1g) arrays: circular, out[i] = a[i - s]."""
+    if s1:
+        a = torch.roll(a, s1, dims=-1)
+    if s2:
+        a = torch.roll(a, s2, dims=-2)
+    return a
 
 
 def _periodic_fill_fields(a, Ng, N1, N2):

@@ -331,7 +331,10 @@ class FieldState(object):
     three always hold the same values; get_fields therefore returns that array
     whichever time level its toggle selects (fields.py:649-690)."""
 
-    def __init__(self, grid, rho_total):
+    def __init__(self, grid, rho_total, user=None):
+        """``user``: the initialize module's field functions by name
+        (initialize_E / initialize_A_phi, initialize_B / initialize_A /
+        initialize_A3_B3) as numpy callables of (q1, q2, params)."""
         self.g = grid
         sp = grid.spec
         self.eps = sp.get('eps', 1.0)
@@ -340,15 +343,79 @@ class FieldState(object):
         self.cell = np.zeros((6, Nq2g, Nq1g))
         self.yee = np.zeros((6, Nq2g, Nq1g))
         init = sp.get('fields_initialize', 'fft')
-        if init != 'fft':
+        user = user or {}
+        if init == 'user-defined':
+            # fields.py:472-475: Yee E and B from the user's functions, then
+            # every cell-centred field from the (not yet refreshed) Yee grid
+            self.yee[0:3] = self._user_E(user)
+            self.yee[3:6] = self._user_B(user)
+            self.cell = self._yee_to_cell()
+            self.yee = _periodic_fill(grid, self.yee)
+            self.J = None
+            return
+        if init not in ('fft', 'fft + user-defined magnetic fields'):
             raise NotImplementedError(init)
         self._fft_poisson(rho_total)
         self.cell = _periodic_fill(grid, self.cell)
         self._cell_to_yee_E()
+        if init != 'fft':
+            # fields.py:477-482: user B on the Yee grid, then its cell values
+            self.yee[3:6] = self._user_B(user)
+            self.cell[3:6] = self._yee_to_cell()[3:6]
         # the constructor's constraint check calls compute_divE, which
         # refreshes the Yee-grid halos (fields.py:37, 278)
         self.yee = _periodic_fill(grid, self.yee)
         self.J = None
+
+    def _user_E(self, user):
+        """fields.py:280-337: E1 on the 'left-centre' grid, E2 at (centre,
+        bottom), E3 at the centre; or from A and phi by one-sided differences.
+        The reference's left-centre grid is (q1 left, q2 BOTTOM):
+        calculate_q.py:35-38 pairs q1_left_center with q2_center_bot."""
+        g, dq1, dq2 = self.g, self.g.dq1, self.g.dq2
+        q1l, q2b, q1c, q2c = g.q1_left, g.q2_bot, g.q1_center, g.q2_center
+        if 'initialize_E' in user:
+            E = user['initialize_E']
+            return np.stack([E(q1l, q2b, None)[0], E(q1c, q2b, None)[1], E(q1c, q2c, None)[2]])
+        if 'initialize_A_phi' in user:
+            F = user['initialize_A_phi']
+            A1, A2 = F(q1c, q2b, None)[0], F(q1l, q2b, None)[1]
+            A3, phi = F(q1l, q2b, None)[2], F(q1c, q2c, None)[3]
+            dA3_dq2 = (_sh(A3, 0, -1) - A3) / dq2
+            dA3_dq1 = (_sh(A3, -1, 0) - A3) / dq1
+            dA2_dq1 = (_sh(A2, -1, 0) - A2) / dq1
+            dA1_dq2 = (_sh(A1, 0, -1) - A1) / dq2
+            dphi_dq1 = -(_sh(phi, 1, 0) - phi) / dq1
+            dphi_dq2 = -(_sh(phi, 0, 1) - phi) / dq2
+            return np.stack([dA3_dq2 - dphi_dq1, -dA3_dq1 - dphi_dq2, dA2_dq1 - dA1_dq2])
+        raise NotImplementedError('initial electric fields')
+
+    def _user_B(self, user):
+        """fields.py:339-410: B1 at (centre, bottom), B2 on the 'left-centre'
+        grid (q1 left, q2 bottom, as above), B3 at (left, bottom); or from A,
+        or from A3 and B3."""
+        g, dq1, dq2 = self.g, self.g.dq1, self.g.dq2
+        q1l, q2b, q1c, q2c = g.q1_left, g.q2_bot, g.q1_center, g.q2_center
+        if 'initialize_B' in user and 'initialize_A3_B3' in user:
+            raise ValueError('initialize_B and initialize_A3_B3 together')
+        if 'initialize_B' in user:
+            B = user['initialize_B']
+            return np.stack([B(q1c, q2b, None)[0], B(q1l, q2b, None)[1], B(q1l, q2b, None)[2]])
+        if 'initialize_A' in user:
+            F = user['initialize_A']
+            A1, A2, A3 = F(q1l, q2b, None)[0], F(q1c, q2b, None)[1], F(q1c, q2c, None)[2]
+            B1 = (_sh(A3, 0, -1) - A3) / dq2
+            B2 = -(_sh(A3, -1, 0) - A3) / dq1
+            B3 = (_sh(A2, -1, 0) - A2) / dq1 - (_sh(A1, 0, -1) - A1) / dq2
+            return np.stack([B1, B2, B3])
+        if 'initialize_A3_B3' in user:
+            F = user['initialize_A3_B3']
+            A3 = F(q1c, q2c, None)[0]
+            # backward differences (np.roll by +1 along q2 and q1)
+            B1 = (A3 - _sh(A3, 0, 1)) / dq2
+            B2 = -(A3 - _sh(A3, 1, 0)) / dq1
+            return np.stack([B1, B2, F(q1l, q2b, None)[1]])
+        raise NotImplementedError('initial magnetic fields')
 
     def _fft_poisson(self, rho):
         """fft.py:9-78 (serial). rho: (Nq2g, Nq1g) total charge density."""
@@ -434,7 +501,7 @@ class Oracle(object):
     """Holds grid, tau, optional fields, and evaluates df/dt and RK steps the
     way Bolt's nonlinear_solver does for the FVM path."""
 
-    def __init__(self, spec, f0, tau=None):
+    def __init__(self, spec, f0, tau=None, field_functions=None):
         self.spec = spec
         self.g = Grid(spec)
         self.f = np.array(f0, dtype=np.float64).reshape(self.g.fshape)
@@ -447,7 +514,7 @@ class Oracle(object):
         self.dirichlet = {}
         if spec.get('fields_enabled', False):
             rho = initial_rho(self.g, self.f)
-            self.fields = FieldState(self.g, rho)
+            self.fields = FieldState(self.g, rho, field_functions)
             self.at_n = True
 
     # ghost refresh: communicate_f + apply_bcs_f -----------------------------

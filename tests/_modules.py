@@ -46,6 +46,9 @@ def build_modules(spec, precision='fp64', integrator=None):
     ini.update(spec['init'])
     initialize = types.ModuleType('initialize')
     initialize.initialize_f = make_f(ini)
+    if spec.get('field_init'):
+        for k, fn in C.field_functions(spec['field_init'], torch.sin, torch.cos).items():
+            setattr(initialize, k, fn)
 
     bc = types.ModuleType('boundary_conditions')
     bc.in_q1_left = bc.in_q1_right = spec['bc_q1']

@@ -168,6 +168,52 @@ CASES = {
         init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=6, T=[1.0, 1.5, 1.0])),
 }
 
+# user-defined initial fields (fields.py:280-420): each form of the initialize
+# module's field functions, FDTD-coupled 2D2V, reference scheme (RK2)
+_FIELD_INIT_BASE = dict(
+    N_q1=8, N_q2=6, N_p1=8, N_p2=6, N_p3=1,
+    p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+    p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0],
+    p_dim=2, fields_enabled=True, tau=0.1, dt=1e-3, steps=2,
+    init=dict(amp=0.05, k1=1, k2=1, T=[1.0, 1.2, 1.0]))
+for _name, _init, _form in (
+        ('fields_user_E_B', 'user-defined', 'E_B'),
+        ('fields_user_Aphi_A', 'user-defined', 'Aphi_A'),
+        ('fields_user_E_A3B3', 'user-defined', 'E_A3B3'),
+        ('fields_fft_user_B', 'fft + user-defined magnetic fields', 'B')):
+    CASES[_name] = make(fields_initialize=_init, field_init=_form,
+                        **copy.deepcopy(_FIELD_INIT_BASE))
+
+
+def field_functions(form, sin, cos):
+    """The initialize-module field functions of the 'field_init' cases, written
+    against a math namespace (numpy, torch, or the ArrayFire stand-in):
+    E_B -> initialize_E, initialize_B; Aphi_A -> initialize_A_phi,
+    initialize_A; E_A3B3 -> initialize_E, initialize_A3_B3; B -> initialize_B."""
+    tp = 2 * np.pi
+
+    def initialize_E(q1, q2, params):
+        return (0.1 * sin(tp * q2), 0.05 * cos(tp * q1), 0.02 * sin(tp * (q1 + q2)))
+
+    def initialize_B(q1, q2, params):
+        return (0.03 * cos(tp * q2), 0.04 * sin(tp * q1), 0.5 + 0.02 * cos(tp * (q1 - q2)))
+
+    def initialize_A_phi(q1, q2, params):
+        return (0.02 * cos(tp * q2), 0.02 * sin(tp * q1), 0.03 * sin(tp * (q1 + q2)),
+                0.01 * cos(tp * q1) * cos(tp * q2))
+
+    def initialize_A(q1, q2, params):
+        return (0.015 * sin(tp * q2), 0.025 * cos(tp * q1), 0.03 * cos(tp * (q1 + 2 * q2)))
+
+    def initialize_A3_B3(q1, q2, params):
+        return (0.03 * sin(tp * (q1 + 2 * q2)), 0.4 + 0.01 * cos(tp * q1))
+
+    table = {'E_B': (initialize_E, initialize_B),
+             'Aphi_A': (initialize_A_phi, initialize_A),
+             'E_A3B3': (initialize_E, initialize_A3_B3),
+             'B': (initialize_B,)}
+    return {fn.__name__: fn for fn in table[form]}
+
 
 # ---------------------------------------------------------------------------
 def _noise(spec, Nq1g, Nq2g):

@@ -46,6 +46,10 @@ def cell_of(nls):
     return nls.fields_solver.cell_centered_EM_fields[:, 0].permute(0, 2, 1).cpu().numpy()
 
 
+def yee_of(nls):
+    return nls.fields_solver.yee_grid_EM_fields[:, 0].permute(0, 2, 1).cpu().numpy()
+
+
 def _check_case(name, precision):
     tol = TOL[precision]
     spec = C.CASES[name]
@@ -56,6 +60,7 @@ def _check_case(name, precision):
     assert rel(interior(to_layout(nls.f, spec), g), G['f0']) < tol['f0']
     if spec['fields_enabled']:
         assert rel(cell_of(nls), G['fields_cell0']) < tol['fields0']
+        assert rel(yee_of(nls), G['fields_yee0']) < tol['fields0']
     # drive from the fixture's state
     nls.f = af_from_layout(G['f0_refreshed']).to('cuda')
     if spec['fields_enabled']:
@@ -93,7 +98,8 @@ def test_fp64_matches_reference(name):
                                   'dirichlet_1d1v_weno5', 'two_species_2d2v_fields',
                                   'mirror_2d2v_weno5', 'mirror_dirichlet_2d3v_rk4',
                                   'dirichlet_2d2v_minmod', 'pc_2d3v_fields',
-                                  'es_1d1v_landau_rk2', 'es_2d2v_two_species_rk4'])
+                                  'es_1d1v_landau_rk2', 'es_2d2v_two_species_rk4',
+                                  'fields_user_Aphi_A', 'fields_fft_user_B'])
 def test_fp32_close_to_reference(name):
     _check_case(name, 'fp32')
 

@@ -19,7 +19,9 @@ def test_oracle_matches_reference(name):
     g = spec['N_ghost']
     f0 = C.initial_f(spec)
     assert rel(interior(f0, g), G['f0']) < 1e-14
-    o = Oracle(spec, f0)
+    user = C.field_functions(spec['field_init'], np.sin, np.cos) \
+        if spec.get('field_init') else None
+    o = Oracle(spec, f0, field_functions=user)
     o.dirichlet = C.dirichlet_values(spec)
     fr = o.refresh(o.f)
     assert rel(fr, G['f0_refreshed']) < 1e-14
