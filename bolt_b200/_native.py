@@ -94,6 +94,7 @@ SIGNATURES = {
     'bolt_stage': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
     'bolt_set_peer_halos': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     'bolt_set_peer_halos_q1': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
+    'bolt_fields_evolve': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),
     'bolt_stage_buffer': (_VP, [_VP, ctypes.c_int]),
     'bolt_ipc_get': (ctypes.c_int, [_VP, ctypes.c_char_p]),
     'bolt_ipc_open': (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_VP)]),

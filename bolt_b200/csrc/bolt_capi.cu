@@ -631,7 +631,8 @@ static int launch_pstage(BoltCtx* ctx, const StageIO& io, const void* kq, cudaSt
     return BOLT_OK;
 }
 
-static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st) {
+static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st,
+                         const double* j_given = nullptr) {
     const BoltGrid& g = ctx->g;
     FieldArgs a;
     memset(&a, 0, sizeof(a));
@@ -640,6 +641,7 @@ static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st)
     a.ebefore = ctx->ebefore;
     a.J = ctx->J;
     a.jpart = ctx->jpart;
+    a.j_given = j_given;
     a.nsplit = nsplit_j;
     a.Ns = g.N_s; a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost;
     a.Nq1g = ctx->Nq1g; a.Nq2g = ctx->Nq2g;
@@ -932,6 +934,13 @@ int bolt_fields_get(BoltCtx* ctx, double* cell_dev, double* yee_dev, void* strea
     if (cell_dev) CK(cudaMemcpyAsync(cell_dev, ctx->cell, bytes, cudaMemcpyDeviceToDevice, st));
     if (yee_dev) CK(cudaMemcpyAsync(yee_dev, ctx->yee, bytes, cudaMemcpyDeviceToDevice, st));
     return BOLT_OK;
+}
+
+int bolt_fields_evolve(BoltCtx* ctx, const double* J_dev, double dt, void* stream) {
+    if (!ctx || !J_dev || !ctx->p.fields_enabled ||
+        ctx->p.fields_type != BOLT_FIELDS_ELECTRODYNAMIC)
+        return BOLT_ERR_ARG;
+    return launch_fields(ctx, dt, 0, (cudaStream_t)stream, J_dev);
 }
 
 int bolt_get_at_n(BoltCtx* ctx) { return ctx ? ctx->at_n : -1; }

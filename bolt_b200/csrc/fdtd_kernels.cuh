@@ -13,7 +13,7 @@ namespace bolt {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int wrapi(int x, int n) { return ((x % n) + n) % n; }
 
-// J from partial sums; copy of the cell-centred E before the update
+// J from partial sums (or the caller's J); copy of the cell-centred E before the update
 __global__ void fdtd_prepare_kernel(FieldArgs a) {
     const int n = a.Nq1g * a.Nq2g;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
@@ -21,7 +21,9 @@ __global__ void fdtd_prepare_kernel(FieldArgs a) {
         const int i = g1 - a.Ng, j = g2 - a.Ng;
         for (int c = 0; c < 3; ++c) {
             double v = 0.0;
-            if (i >= 0 && i < a.Nq1 && j >= 0 && j < a.Nq2) {
+            if (a.j_given) {
+                v = a.j_given[c * n + t];
+            } else if (i >= 0 && i < a.Nq1 && j >= 0 && j < a.Nq2) {
                 // per species: charge * (sum * measure); then the species sum
                 for (int s = 0; s < a.Ns; ++s) {
                     double sum = 0.0;

@@ -153,6 +153,7 @@ struct FieldArgs {
     double* ebefore;        // [3][Nq2g][Nq1g]
     double* J;              // [3][Nq2g][Nq1g]
     const double* jpart;    // [nsplit][3][Ns][Nq2][Nq1]
+    const double* j_given;  // [3][Nq2g][Nq1g] species-summed currents from the caller, or null
     int nsplit, Ns, Nq1, Nq2, Ng, Nq1g, Nq2g;
     double dq1, dq2, dt, eps, mu;
     double charge[kMaxSpecies], measure[kMaxSpecies];

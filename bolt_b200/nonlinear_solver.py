@@ -40,6 +40,14 @@ class _FieldsSolver(object):
 
     def __init__(self, nls):
         self._nls = nls
+        self.time_elapsed = 0.0          # advanced by evolve_electrodynamic_fields
+
+    # the grid attributes the reference's fields_solver carries (fields.py:200-240)
+    N_g = property(lambda self: self._nls.N_ghost)
+    dq1 = property(lambda self: self._nls.dq1)
+    dq2 = property(lambda self: self._nls.dq2)
+    q1_center = property(lambda self: self._nls.q1_center)
+    q2_center = property(lambda self: self._nls.q2_center)
 
     def _fetch(self):
         nls = self._nls
@@ -95,6 +103,50 @@ class _FieldsSolver(object):
         out = tuple(c[i:i + 1] for i in range(6))
         self.at_n = not self.at_n
         return out
+
+    def evolve_electrodynamic_fields(self, J1, J2, J3, dt):
+        """fields.py:568-647: one FDTD update with the caller's currents, each
+        (1, N_s, Nq1g, Nq2g) (summed over species, as af.sum(J, 1)),
+        (1, 1, Nq1g, Nq2g) or a scalar, on the E components' Yee positions."""
+        nls = self._nls
+        Nq1g, Nq2g = nls.N_q1_local_with_Ng, nls.N_q2_local_with_Ng
+
+        def yee_layout(J):
+            J = torch.as_tensor(J, dtype=torch.float64, device=nls.device)
+            if J.dim() == 4:
+                J = J.sum(dim=1, keepdim=True)
+            return J.expand(1, 1, Nq1g, Nq2g).reshape(Nq1g, Nq2g).T
+        J = torch.stack([yee_layout(J1), yee_layout(J2), yee_layout(J3)]).contiguous()
+        self._keep_j = J                     # alive until the stream has used it
+        N.check(nls._lib.bolt_fields_evolve(nls._ctx, J.data_ptr(), float(dt), nls._stream()),
+                'bolt_fields_evolve')
+        self.time_elapsed += dt
+
+    def compute_divB(self):
+        """fields.py:22-32: (B1 - B1 one cell back in q1) / dq1 + (B2 - B2 one
+        cell back in q2) / dq2 at the cell's left-bottom corner, (1, 1, Nq1g, Nq2g)."""
+        y = self._fetch()[1]
+        d = (y[3] - _shift(y[3], 1, 0)) / self.dq1 + (y[4] - _shift(y[4], 0, 1)) / self.dq2
+        return self._af(d.unsqueeze(0))
+
+    def compute_divE(self):
+        """fields.py:35-46: the divergence of E at the cell centre, after the
+        periodic refresh of the Yee-grid halos, (1, 1, Nq1g, Nq2g)."""
+        nls = self._nls
+        y = _periodic_fill_fields(self._fetch()[1], nls.N_ghost, nls.N_q1, nls.N_q2)
+        d = (_shift(y[0], -1, 0) - y[0]) / self.dq1 + (_shift(y[1], 0, -1) - y[1]) / self.dq2
+        return self._af(d.unsqueeze(0))
+
+    def check_maxwells_contraint_equations(self, rho):
+        """fields.py:48-75: prints max |div B| and max |div E - rho + mean(rho)|
+        over the interior cells."""
+        g = self.N_g
+        inner = lambda a: a[..., g:a.shape[-2] - g, g:a.shape[-1] - g]
+        rho = torch.as_tensor(rho, dtype=torch.float64, device=self._nls.device)
+        print("Initial Maxwell's Constraints:")
+        print('MAX(|divB|) =', float(inner(self.compute_divB()).abs().max()))
+        print('MAX(|divE-rho|) =',
+              float(inner(self.compute_divE() - rho + rho.mean()).abs().max()))
 
 
 class nonlinear_solver(object):

@@ -205,6 +205,12 @@ int  bolt_moments(BoltCtx* ctx, const void* f_dev, int moment_id, double* out_de
 /* Fields state (FP64 device arrays of 6*Nq2g*Nq1g doubles). */
 int  bolt_fields_set(BoltCtx* ctx, const double* cell_dev, const double* yee_dev, void* stream);
 int  bolt_fields_get(BoltCtx* ctx, double* cell_dev, double* yee_dev, void* stream);
+/* One FDTD update of the context's fields with the caller's currents:
+ * J_dev = [3][N_q2+2N_g][N_q1+2N_g] FP64 (J1, J2, J3 summed over species, on
+ * the E components' Yee positions), as fields_solver.evolve_electrodynamic_fields
+ * (fields.py:568-647): E += dt curl B / (mu eps) - J dt / eps, then
+ * B -= dt curl E, then the cell-centred fields.  Electrodynamic contexts only. */
+int  bolt_fields_evolve(BoltCtx* ctx, const double* J_dev, double dt, void* stream);
 
 /* FDTD time-level flag of the reference's fields solver (fields.py:271-273,
  * 685-688): each df/dt evaluation flips it; a stage evolves the fields when it

@@ -171,6 +171,8 @@ def test_div_b_vanishes():
         y = _yee(nls)
         B1, B2 = y[3], y[4]                # (Nq1g, Nq2g): q1 is dim 0 here
         d = (B1 - torch.roll(B1, 1, dims=0)) / dq1 + (B2 - torch.roll(B2, 1, dims=1)) / dq2
+        api = nls.fields_solver.compute_divB()[0, 0]
+        assert torch.equal(api, d)
         return float(torch.mean(torch.abs(_interior_q(d, g))))
     assert div_b() < 1e-14 * (4 * math.pi / dq1)
     for _ in range(20):

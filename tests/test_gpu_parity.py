@@ -104,6 +104,38 @@ def test_fp32_close_to_reference(name):
     _check_case(name, 'fp32')
 
 
+def test_evolve_electrodynamic_fields_matches_oracle():
+    """fields_solver.evolve_electrodynamic_fields with the caller's currents
+    (per species, summed as af.sum(J, 1)) against the oracle's restatement of
+    fields.py:568-647, three updates from the fixture's fields; compute_divE
+    against its definition (fields.py:35-46)."""
+    from oracle.bolt_oracle import Oracle, _periodic_fill, _sh
+    name = 'fields_user_E_B'
+    spec = C.CASES[name]
+    G = load_golden(name)
+    nls = make_solver(spec, 'fp64')
+    o = Oracle(spec, C.initial_f(spec),
+               field_functions=C.field_functions(spec['field_init'], np.sin, np.cos))
+    nls.fields_solver.cell_centered_EM_fields = fields_af(G['fields_cell0'])
+    nls.fields_solver.yee_grid_EM_fields = fields_af(G['fields_yee0'])
+    o.fields.cell, o.fields.yee = G['fields_cell0'].copy(), G['fields_yee0'].copy()
+    rng = np.random.default_rng(5)
+    shape = o.fields.yee.shape[1:]                              # (Nq2g, Nq1g)
+    for _ in range(3):
+        J = rng.standard_normal((3, 2) + shape) * 0.1          # 2 per-species parts
+        Jaf = [torch.from_numpy(np.ascontiguousarray(J[c].transpose(0, 2, 1)))[None]
+               for c in range(3)]                               # (1, 2, Nq1g, Nq2g)
+        nls.fields_solver.evolve_electrodynamic_fields(*Jaf, 2e-3)
+        o.fields.evolve(J[0].sum(0), J[1].sum(0), J[2].sum(0), 2e-3)
+    assert rel(yee_of(nls), o.fields.yee) < 1e-13
+    assert rel(cell_of(nls), o.fields.cell) < 1e-13
+    assert nls.fields_solver.time_elapsed == pytest.approx(6e-3)
+    y = _periodic_fill(o.g, o.fields.yee)
+    divE = (_sh(y[0], -1, 0) - y[0]) / o.g.dq1 + (_sh(y[1], 0, -1) - y[1]) / o.g.dq2
+    got = nls.fields_solver.compute_divE()[0, 0].T.cpu().numpy()
+    assert rel(got, divE) < 1e-12
+
+
 PARTIAL = C.make(N_q1=12, N_q2=10, N_p1=8, N_p2=6, N_p3=4,
                  p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
                  p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
