@@ -554,6 +554,21 @@ class nonlinear_solver(object):
         self.check_divergence()
         self.time_elapsed += dt
 
+    def _communicate_f(self):
+        """communicate.py:8-38 with apply_bcs_f (boundaries.py:415-577): one
+        pass of the ghost kernel fills every ghost cell of f -- periodic
+        images, mirror images, Dirichlet inflow -- from the interior."""
+        self._sync_external_edits()
+        if self._has_dirichlet():
+            self._refresh_boundaries()
+        N.check(self._lib.bolt_fill_ghosts(self._ctx, self._fstore.data_ptr(), self._stream()),
+                'bolt_fill_ghosts')
+        self._seen_version = self._fstore._version
+
+    # the ghost pass applies the boundary conditions too; calling it again is
+    # harmless (every ghost is a function of the interior)
+    _apply_bcs_f = _communicate_f
+
     def check_divergence(self):
         """timestep.py:28-38 -- the device flags any non-finite f value written
         by a step; the flag is read from pinned host memory without
