@@ -13,7 +13,13 @@ path (the oracle versions of the first three are in test_oracle_golden.py):
   initialize_A3_B3 (test_fdtd_explicit.py:120-220, mode 1: slope within 0.2
   of -2), over exactly one period;
 * the discrete divergence of B from initialize_A3_B3 vanishes
-  (test_check_maxwells_contraints.py:96) and stays zero under the FDTD update.
+  (test_check_maxwells_contraints.py:96) and stays zero under the FDTD update;
+* the TM mode driven by a current J3, through evolve_electrodynamic_fields
+  (test_fdtd_explicit_with_currents.py:97-159: slope within 0.25 of -2), set
+  up on the Yee positions of fields.py's initialisation;
+* the FFT Poisson solve of rho = -sin(2 pi q1 + 4 pi q2) on 1024^2 cells
+  against its closed form to 1e-14 (test_fft_poisson.py:55-80), both the
+  initial solve and the per-df/dt solve of the electrostatic path.
 """
 
 import math
@@ -99,7 +105,7 @@ def test_rk_temporal_order(integrator, order):
     assert abs(slope - order) < 0.3, (errs, slope)
 
 
-def _fdtd_mode1_solver(N, dt, a3b3):
+def _fdtd_mode1_solver(N, dt, a3b3, init_E=None):
     """2D2V with charge 0 (vacuum Maxwell), fields from initialize_E and
     initialize_A3_B3."""
     spec = C.make(N_q1=N, N_q2=N, N_p1=4, N_p2=4, N_p3=1,
@@ -115,7 +121,9 @@ def _fdtd_mode1_solver(N, dt, a3b3):
     dom, bc, params, initialize = build_modules(spec, 'fp64', None)
     params.dt = dt
     initialize.initialize_A3_B3 = a3b3
-    if a3b3 is _mode1_A3_B3:
+    if init_E is not None:
+        initialize.initialize_E = init_E
+    elif a3b3 is _mode1_A3_B3:
         initialize.initialize_E = _mode1_E
     else:
         initialize.initialize_E = lambda q1, q2, p: (0 * q1, 0 * q1, 0 * q1)
@@ -178,3 +186,76 @@ def test_div_b_vanishes():
     for _ in range(20):
         nls.strang_timestep(1 / (2 * N))
     assert div_b() < 1e-14 * (4 * math.pi / dq1)
+
+
+def test_fdtd_tm_mode_with_currents_converges_second_order():
+    """The driven TM mode of test_fdtd_explicit_with_currents.py:97-159:
+    A3 = sin(phi), B1 = dA3/dq2, B2 = -dA3/dq1, E3 = 6 pi cos(phi),
+    J3 = -16 pi^2 sin(phi), phi = 2 pi q1 + 4 pi q2 - 6 pi t, one drive period.
+    The fields sit on the Yee positions of fields.py's initialisation (E3 and
+    A3 at the cell centre, J3 with E3); the reference's test file places every
+    component at the left-bottom corner instead, and imports a module path
+    (bolt.lib.nonlinear_solver) absent from its tree."""
+    Ns = [32, 64, 128]
+    errs = {3: [], 4: [], 2: []}
+    for N in Ns:
+        dt = (1.0 / N) / 2
+        tm_E = lambda q1, q2, p: (0 * q1, 0 * q1,
+                                  6 * math.pi * torch.cos(2 * math.pi * q1 + 4 * math.pi * q2))
+        # B half a step ahead of E (B^{n+1/2} with E^n)
+        tm_A3_B3 = lambda q1, q2, p: (torch.sin(2 * math.pi * (q1 - 0.5 * dt)
+                                                + 4 * math.pi * (q2 - 0.5 * dt)), 0 * q1)
+        nls = _fdtd_mode1_solver(N, dt, tm_A3_B3, tm_E)
+        q1, q2 = nls.q1_center, nls.q2_center
+        y0 = _yee(nls).clone()
+        n = 2 * N                                               # t = 1: one drive period
+        for k in range(1, n + 1):
+            t = k * dt - 0.5 * dt                               # currents at n + 1/2
+            J3 = -16 * math.pi ** 2 * torch.sin(2 * math.pi * (q1 - t) + 4 * math.pi * (q2 - t))
+            nls.fields_solver.evolve_electrodynamic_fields(0, 0, J3, dt)
+        y1 = _yee(nls)
+        g = nls.N_ghost
+        for c in errs:
+            errs[c].append(float(torch.mean(torch.abs(_interior_q(y1[c] - y0[c], g)))))
+    for c, e in errs.items():
+        slope = np.polyfit(np.log10(Ns), np.log10(e), 1)[0]
+        assert abs(slope + 2) < 0.25, (c, e, slope)
+
+
+def test_fft_poisson_kat():
+    """One p-cell of width 1, so the density is f itself; charge 1 and
+    n = 2 - sin(2 pi q1 + 4 pi q2) give rho - mean(rho) = -sin(...)."""
+    N = 1024
+    spec = C.make(N_q1=N, N_q2=N, N_p1=1, N_p2=1, N_p3=1,
+                  p1_start=[-0.5], p1_end=[0.5], p2_start=[-0.5], p2_end=[0.5],
+                  p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[1.0], p_dim=1,
+                  source_enabled=False, fields_enabled=True, fields_type='electrostatic',
+                  fields_solver='fft', fields_initialize='fft')
+    nls = make_solver(spec, 'fp64')
+    q1, q2 = nls.q1_center, nls.q2_center
+    theta = 2 * math.pi * q1 + 4 * math.pi * q2
+    g = spec['N_ghost']
+    E1x = (0.1 / math.pi) * torch.cos(theta)
+    E2x = (0.2 / math.pi) * torch.cos(theta)
+
+    def errors():
+        c = nls.fields_solver.cell_centered_EM_fields
+        return (float(torch.mean(torch.abs(_interior_q(c[0:1] - E1x, g)))),
+                float(torch.mean(torch.abs(_interior_q(c[1:2] - E2x, g)))))
+    nls.f = (2 - torch.sin(theta)).expand_as(nls.f)
+    nls.df_dt()                                  # the electrostatic solve of the CUDA path
+    e1, e2 = errors()
+    assert e1 < 1e-14 and e2 < 1e-14, (e1, e2)
+    # the solve at construction, from the initial f of the same density
+    def init_f(q1, q2, p1, p2, p3, params):
+        return (2 - torch.sin(2 * math.pi * q1 + 4 * math.pi * q2)) * p1 ** 0
+    from bolt_b200.physical_system import physical_system
+    from bolt_b200.nonlinear_solver import nonlinear_solver
+    import bolt_b200.src.nonrelativistic_boltzmann.advection_terms as adv
+    import bolt_b200.src.nonrelativistic_boltzmann.collision_operator as col
+    import bolt_b200.src.nonrelativistic_boltzmann.moments as mom
+    dom, bc, params, initialize = build_modules(spec, 'fp64', None)
+    initialize.initialize_f = init_f
+    nls = nonlinear_solver(physical_system(dom, bc, params, initialize, adv, col.BGK, mom))
+    e1, e2 = errors()
+    assert e1 < 1e-14 and e2 < 1e-14, (e1, e2)
