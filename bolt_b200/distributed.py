@@ -99,17 +99,20 @@ def _barrier(group):
         dist.barrier(group=group)
 
 
-def write_block_vec(path, block, corner, shape, group=None, create=True, block_size=None):
+def write_block_vec(path, block, corner, shape, group=None, create=True, block_size=None,
+                    collective=None):
     """Collective write of one PETSc binary Vec holding a whole q-grid array in
     natural order (q2, q1, dof), dof fastest -- what PETSc's VecView writes for
     a DMDA global vector whatever the process grid (dump.py:121-168).
 
     ``block`` is this rank's interior part, (n2, n1, dof) FP64, starting at
     global interior cell ``corner`` = (j0, i0); ``shape`` = (N_q2, N_q1, dof).
-    The creating rank (rank 0 of ``group``; without a process group the caller
-    says which call creates, and calls the creating one first) writes the
-    header (int32 class id 1211214, int32 length, big-endian) and sizes the
-    file; after a barrier every rank stores its rows at their offsets."""
+    The creating rank (rank 0 of ``group``) writes the header (int32 class id
+    1211214, int32 length, big-endian) and sizes the file; after a barrier
+    every rank stores its rows at their offsets.  ``collective=False`` (several
+    blocks written from one process; default: whether torch.distributed is
+    initialised) skips the barriers: ``create`` then says which call makes the
+    file, and that call must come first."""
     rank, _ = _group_info(group)
     N2, N1, dof = (int(x) for x in shape)
     n2, n1 = block.shape[0], block.shape[1]
@@ -119,19 +122,22 @@ def write_block_vec(path, block, corner, shape, group=None, create=True, block_s
     total = N2 * N1 * dof
     if total >= 2 ** 31:
         raise ValueError('a PETSc binary Vec holds fewer than 2^31 values')
-    collective = dist.is_available() and dist.is_initialized()
+    if collective is None:
+        collective = dist.is_available() and dist.is_initialized()
     if (rank == 0) if collective else create:
         with open(path, 'wb') as fh:
             np.array([1211214, total], dtype='>i4').tofile(fh)
             fh.truncate(8 + 8 * total)
         with open(path + '.info', 'w') as fh:
             fh.write('-vecload_block_size %d\n' % (block_size or dof))
-    _barrier(group)
+    if collective:
+        _barrier(group)
     mm = np.memmap(path, dtype='>f8', mode='r+', offset=8, shape=(N2, N1, dof))
     mm[j0:j0 + n2, i0:i0 + n1] = block
     mm.flush()
     del mm
-    _barrier(group)
+    if collective:
+        _barrier(group)
 
 
 def read_block_vec(path, corner, block_shape, shape):
@@ -398,8 +404,8 @@ class BlockSolver(object):
         data = self.local._interior_store().to(torch.float64).cpu().numpy()
         corner, shape = self._grid(self._dof())
         write_block_vec(file_name + '.bin', data.reshape(data.shape[0], data.shape[1], -1),
-                        corner, shape, self.group if self._collective else None,
-                        create=self.rank == 0)
+                        corner, shape, self.group, create=self.rank == 0,
+                        collective=self._collective)
 
     def load_distribution_function(self, file_name):
         """This block's part of a whole-run f file (dump_distribution_function,
@@ -416,8 +422,8 @@ class BlockSolver(object):
         dump_distribution_function)."""
         arr = self.local._moments_interior()
         corner, shape = self._grid(arr.shape[2])
-        write_block_vec(file_name + '.bin', arr, corner, shape,
-                        self.group if self._collective else None, create=self.rank == 0)
+        write_block_vec(file_name + '.bin', arr, corner, shape, self.group,
+                        create=self.rank == 0, collective=self._collective)
 
     def conserved_totals(self):
         """Integrals over the whole q-domain of each species' density, bulk

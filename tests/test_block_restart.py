@@ -98,8 +98,42 @@ def test_blocks_written_in_rank_order_without_a_group(tmp_path):
     for r in range(4):
         corner = ((r // 2) * 4, (r % 2) * 4)
         write_block_vec(out_path, read_block_vec(src, corner, (4, 4), (N2, N1, dof)),
-                        corner, (N2, N1, dof), create=r == 0)
+                        corner, (N2, N1, dof), create=r == 0, collective=False)
     assert _raw(out_path) == _raw(src)
+
+
+def test_blocks_of_one_process_inside_a_process_group(tmp_path):
+    """Blocks written one after another by a process that has a process group
+    (collective=False): the creating call does not erase the others' rows."""
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    p = ctx.Process(target=_one_process_blocks, args=(_free_port(), str(tmp_path / 'o.bin'), q))
+    p.start()
+    ok = q.get(timeout=300)
+    p.join(timeout=60)
+    assert p.exitcode == 0 and ok
+
+
+def _one_process_blocks(port, out_path, q):
+    import datetime
+    import sys
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        from bolt_b200.distributed import read_block_vec, write_block_vec
+        name, N2, N1, dof = FILES[0]
+        src = os.path.join(DUMPS, name)
+        for r in range(4):
+            corner = ((r // 2) * 4, (r % 2) * 4)
+            write_block_vec(out_path, read_block_vec(src, corner, (4, 4), (N2, N1, dof)),
+                            corner, (N2, N1, dof), create=r == 0, collective=False)
+        q.put(_raw(out_path) == _raw(src))
+    finally:
+        dist.destroy_process_group()
 
 
 def test_block_vec_errors(tmp_path):
