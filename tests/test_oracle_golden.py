@@ -121,3 +121,37 @@ def test_reference_restart_files_parse():
         a = open(os.path.join(t, 'x.bin'), 'rb').read()
         b = open(os.path.join(d, 'c3_2d3v_weno5_rk4_small_f.bin'), 'rb').read()
         assert a == b
+
+
+def test_fdtd_tm_mode_with_currents_second_order():
+    """test_fdtd_explicit_with_currents.py:97-159 on the oracle's FDTD: the TM
+    mode driven by J3 = -16 pi^2 sin(phi), set up on the Yee positions of
+    fields.py's initialisation (E3, A3 and J3 at the cell centre, B from A3
+    by backward differences), returns to its initial state after one drive
+    period with error O(N^-2) (slope within 0.25 of -2)."""
+    import math
+    Ns = [32, 64, 128]
+    errs = {2: [], 3: [], 4: []}
+    for N in Ns:
+        dt = 0.5 / N
+        spec = C.make(N_q1=N, N_q2=N, N_p1=4, N_p2=4, N_p3=1, p1_start=[-1.0], p1_end=[1.0],
+                      p2_start=[-1.0], p2_end=[1.0], p3_start=[-0.5], p3_end=[0.5],
+                      mass=[1.0], charge=[0.0], p_dim=2, source_enabled=False,
+                      fields_enabled=True, fields_initialize='user-defined')
+        tp = 2 * math.pi
+        user = {'initialize_E': lambda q1, q2, p: (0 * q1, 0 * q1,
+                                                   3 * tp * np.cos(tp * q1 + 2 * tp * q2)),
+                'initialize_A3_B3': lambda q1, q2, p: (
+                    np.sin(tp * (q1 - 0.5 * dt) + 2 * tp * (q2 - 0.5 * dt)), 0 * q1)}
+        o = Oracle(spec, np.ones(Grid(spec).fshape), field_functions=user)
+        y0 = o.fields.yee.copy()
+        q1, q2 = o.g.q1_center, o.g.q2_center
+        for k in range(1, 2 * N + 1):
+            t = (k - 0.5) * dt
+            J3 = -4 * tp ** 2 * np.sin(tp * (q1 - t) + 2 * tp * (q2 - t))
+            o.fields.evolve(0 * q1, 0 * q1, J3, dt)
+        for c in errs:
+            errs[c].append(np.mean(np.abs(interior(o.fields.yee[c] - y0[c], 3))))
+    for c, e in errs.items():
+        slope = np.polyfit(np.log10(Ns), np.log10(e), 1)[0]
+        assert abs(slope + 2) < 0.25, (c, e, slope)
