@@ -168,6 +168,16 @@ CASES = {
         init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=6, T=[1.0, 1.5, 1.0])),
 }
 
+# a wider ghost zone than the stencil needs (the reference's halo tests draw
+# N_ghost from 3..4: test_communicate.py, test_apply_boundary_conditions.py)
+CASES['c3_2d3v_weno5_rk4_ghost4'] = make(
+    N_q1=8, N_q2=8, N_p1=8, N_p2=8, N_p3=8, N_ghost=4,
+    p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0], p2_end=[6.0],
+    p3_start=[-6.0], p3_end=[6.0], mass=[1.0], charge=[0.0], p_dim=3,
+    tau=0.05, dt=1e-3, steps=3, integrator='RK4',
+    riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+    init=dict(amp=0.05, k1=1, k2=1, noise=1e-3, seed=4, u=[0.1, -0.2, 0.05]))
+
 # user-defined initial fields (fields.py:280-420): each form of the initialize
 # module's field functions, FDTD-coupled 2D2V, reference scheme (RK2)
 _FIELD_INIT_BASE = dict(

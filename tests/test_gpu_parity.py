@@ -99,7 +99,8 @@ def test_fp64_matches_reference(name):
                                   'mirror_2d2v_weno5', 'mirror_dirichlet_2d3v_rk4',
                                   'dirichlet_2d2v_minmod', 'pc_2d3v_fields',
                                   'es_1d1v_landau_rk2', 'es_2d2v_two_species_rk4',
-                                  'fields_user_Aphi_A', 'fields_fft_user_B'])
+                                  'fields_user_Aphi_A', 'fields_fft_user_B',
+                                  'c3_2d3v_weno5_rk4_ghost4'])
 def test_fp32_close_to_reference(name):
     _check_case(name, 'fp32')
 
