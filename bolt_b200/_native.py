@@ -107,11 +107,19 @@ SIGNATURES = {
     'bolt_divergence_flag': (ctypes.c_int, [_VP]),
     'bolt_clear_divergence_flag': (ctypes.c_int, [_VP]),
     'bolt_status_sync': (ctypes.c_int, [_VP, _VP]),
+    'bolt_error_flag': (ctypes.c_int, [_VP]),
+    'bolt_clear_error': (ctypes.c_int, [_VP]),
+    'bolt_set_wait_budget': (ctypes.c_int, [_VP, ctypes.c_longlong]),
+    'bolt_test_stall_waits': (ctypes.c_int, [_VP, ctypes.c_int]),
     'bolt_strerror': (ctypes.c_char_p, [ctypes.c_int]),
     'bolt_launch_count': (ctypes.c_longlong, [_VP]),
+    'bolt_paired_launch_count': (ctypes.c_longlong, [_VP]),
+    'bolt_split_info': (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
     'bolt_scratch_bytes': (ctypes.c_size_t, [_VP]),
     'bolt_dfdt_noalloc': (ctypes.c_int, [ctypes.POINTER(BoltGrid), ctypes.POINTER(BoltParams),
                                          _VP, _VP, _VP]),
+    'bolt_noalloc_status': (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
     'bolt_batch_create': (ctypes.c_int, [ctypes.POINTER(BoltBatchRun), ctypes.c_int,
                                          ctypes.c_int, ctypes.POINTER(_VP)]),
     'bolt_batch_destroy': (None, [_VP]),

@@ -14,6 +14,7 @@
 
 #include "../../include/bolt_b200.h"
 #include "launch.h"
+#include "validate.h"
 
 using namespace bolt;
 
@@ -24,17 +25,19 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+EncodeTiledFn lookup_encode_fn() {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+        return reinterpret_cast<EncodeTiledFn>(p);
+    return nullptr;
+}
+
+// looked up once per process (a function-local static is initialised once,
+// even when several host threads make their first call together)
 EncodeTiledFn get_encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess && q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
+    static const EncodeTiledFn fn = lookup_encode_fn();
     return fn;
 }
 
@@ -88,9 +91,13 @@ struct BoltCtx {
     const void* dirichlet[4];
     int* hflag;             // pinned, mapped
     int* dflag;
-    int* derr;
+    int* herr;              // device error word: pinned, mapped (host view)
+    int* derr;              // (device view)
+    long long wait_cycles;  // budget of the stage kernels' tile waits
+    int stall_test;         // test hook: the stage kernels issue no tile copies
     int sticky;
     long long launches;
+    long long pair_launches;    // of which the paired FP32 stage kernel
     size_t scratch_bytes;
     TmapEntry tmaps[kTmapSlots];
     int ntmaps, next_tmap;
@@ -110,7 +117,7 @@ struct BoltCtx {
 static inline int bc_dirichlet(int bc) {
     return bc == BOLT_BC_DIRICHLET || bc == BOLT_BC_MIRROR_DIRICHLET;
 }
-static inline int bc_mirror(int bc) { return bc == BOLT_BC_MIRROR || bc == BOLT_BC_MIRROR_DIRICHLET; }
+static inline int bc_mirror(int bc) { return bc_is_mirror(bc) ? 1 : 0; }
 
 static int dev_alloc(BoltCtx* ctx, void** p, size_t bytes) {
     if (bytes == 0) {
@@ -183,26 +190,8 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
     *out = nullptr;
     const BoltGrid& g = *grid;
     const BoltParams& p = *params;
-    if (g.N_q1 < 1 || g.N_q2 < 1 || g.N_p1 < 1 || g.N_p2 < 1 || g.N_p3 < 1 || g.N_ghost < 0 ||
-        g.N_s < 1 || g.N_s > BOLT_MAX_SPECIES)
-        return BOLT_ERR_ARG;
-    if (p.dtype != BOLT_F64 && p.dtype != BOLT_F32) return BOLT_ERR_ARG;
-    if (p.recon_q < 0 || p.recon_q > 3 || p.recon_p < 0 || p.recon_p > 3) return BOLT_ERR_ARG;
-    if (p.integrator != BOLT_RK2 && p.integrator != BOLT_RK4) return BOLT_ERR_ARG;
-    if (p.p_dim < 1 || p.p_dim > 3) return BOLT_ERR_ARG;
-    if (p.bc_q1 < BOLT_BC_PERIODIC || p.bc_q1 > BOLT_BC_MIRROR_DIRICHLET ||
-        p.bc_q2 < BOLT_BC_PERIODIC || p.bc_q2 > BOLT_BC_MIRROR_DIRICHLET)
-        return BOLT_ERR_ARG;
-    if (p.fields_enabled && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
-        return BOLT_ERR_UNSUPPORTED;
-    if (p.fields_enabled && p.fields_type != BOLT_FIELDS_ELECTRODYNAMIC &&
-        p.fields_type != BOLT_FIELDS_ELECTROSTATIC)
-        return BOLT_ERR_ARG;
-    if (g.N_ghost == 0 && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
-        return BOLT_ERR_UNSUPPORTED;
-    // a mirror image of the ghost zone must lie inside the grid
-    if ((bc_mirror(p.bc_q1) && g.N_ghost > g.N_q1) || (bc_mirror(p.bc_q2) && g.N_ghost > g.N_q2))
-        return BOLT_ERR_UNSUPPORTED;
+    const int vrc = check_grid_params(g, p);
+    if (vrc) return vrc;
 
     BoltCtx* ctx = new (std::nothrow) BoltCtx;
     if (!ctx) return BOLT_ERR_NOMEM;
@@ -247,35 +236,26 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
                          g.N_q1 % 8 == 0 && g.N_q2 % 8 == 0 && ctx->Np % PW == 0 &&
                          g.N_p1 % 8 == 0 && 2 * g.N_ghost <= g.N_q1 &&
                          2 * g.N_ghost <= g.N_q2 && ctx->fcount < (1ull << 31);
-    // p-splits: the grid is (q-tiles, species x splits); choose the split that
-    // minimises (waves, rounded up) x (chunks per CTA + ~2 chunks of prologue),
-    // a wave being SMs x resident CTAs per SM of the q-stage kernel
+    // p-splits: the grid is (q-tiles, species x splits)
     {
-        int dev = 0, sms = 148;
-        if (cudaGetDevice(&dev) == cudaSuccess)
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const size_t smem_est = ctx->pair_shape_ok
             ? qpair_smem(ctx->ntab, ctx->bgk)
             : qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct, ctx->ntab);
-        long long per_sm = 233472LL / (long long)(smem_est + 1024);
-        per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
-        const long long wave = (long long)sms * per_sm;
         const int nchunks = (ctx->Np + PW - 1) / PW;
         const long long base_ctas = (long long)ctx->ntiles1 * ctx->ntiles2 * g.N_s;
-        double best = 1e300;
-        int best_cps = nchunks;
-        for (int n = 1; n <= nchunks && n <= 64; ++n) {
-            const int cps = (nchunks + n - 1) / n;
-            const int ne = (nchunks + cps - 1) / cps;
-            const long long waves = (base_ctas * ne + wave - 1) / wave;
-            const double cost = (double)waves * (cps + 2.0);
-            if (cost < best - 1e-9) {
-                best = cost;
-                best_cps = cps;
+        PSplit sp = choose_psplit(nchunks, base_ctas, current_sm_count(), smem_est);
+        // BOLT_CHUNKS_PER_SPLIT fixes the split instead (tests run one problem
+        // under several splits; results differ only in the order of the FP64
+        // moment partial sums)
+        if (const char* env = getenv("BOLT_CHUNKS_PER_SPLIT")) {
+            const int c = atoi(env);
+            if (c >= 1) {
+                sp.chunks_per_split = c < nchunks ? c : nchunks;
+                sp.nsplit = (nchunks + sp.chunks_per_split - 1) / sp.chunks_per_split;
             }
         }
-        ctx->chunks_per_split = best_cps;
-        ctx->nsplit = (nchunks + best_cps - 1) / best_cps;
+        ctx->chunks_per_split = sp.chunks_per_split;
+        ctx->nsplit = sp.nsplit;
     }
     const size_t rowbytes = (size_t)g.N_s * ctx->Np * ctx->elem;
     ctx->use_tma_ok = (g.N_ghost >= HALO) && (rowbytes % 16 == 0) &&
@@ -312,15 +292,21 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
                 rc = BOLT_ERR_CUDA;
         }
     }
-    if (rc == BOLT_OK) rc = dev_alloc(ctx, (void**)&ctx->derr, sizeof(int));
-    if (rc == BOLT_OK && cudaMemset(ctx->derr, 0, sizeof(int)) != cudaSuccess) rc = BOLT_ERR_CUDA;
+    // the divergence flag and the error word live in pinned host memory the
+    // kernels write through its device mapping, so the host reads either
+    // without synchronising
     if (rc == BOLT_OK) {
-        if (cudaHostAlloc((void**)&ctx->hflag, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
-            cudaHostGetDevicePointer((void**)&ctx->dflag, ctx->hflag, 0) != cudaSuccess)
+        if (cudaHostAlloc((void**)&ctx->hflag, 2 * sizeof(int), cudaHostAllocMapped) !=
+                cudaSuccess ||
+            cudaHostGetDevicePointer((void**)&ctx->dflag, ctx->hflag, 0) != cudaSuccess) {
             rc = BOLT_ERR_CUDA;
-        else
-            *ctx->hflag = 0;
+        } else {
+            ctx->hflag[0] = ctx->hflag[1] = 0;
+            ctx->herr = ctx->hflag + 1;
+            ctx->derr = ctx->dflag + 1;
+        }
     }
+    ctx->wait_cycles = kDefaultWaitCycles;
     if (rc == BOLT_OK && cudaDeviceSynchronize() != cudaSuccess) rc = BOLT_ERR_CUDA;
     if (rc != BOLT_OK) {
         bolt_ctx_destroy(ctx);
@@ -341,7 +327,6 @@ void bolt_ctx_destroy(BoltCtx* ctx) {
     cudaFree(ctx->yee);
     cudaFree(ctx->ebefore);
     cudaFree(ctx->J);
-    cudaFree(ctx->derr);
     cudaFree(ctx->es_part);
     cudaFree(ctx->es_rho);
     cudaFree(ctx->es_e);
@@ -422,6 +407,13 @@ void* bolt_stage_buffer(BoltCtx* ctx, int i) {
 }
 
 long long bolt_launch_count(BoltCtx* ctx) { return ctx ? ctx->launches : 0; }
+long long bolt_paired_launch_count(BoltCtx* ctx) { return ctx ? ctx->pair_launches : 0; }
+int bolt_split_info(BoltCtx* ctx, int* nsplit, int* chunks_per_split) {
+    if (!ctx || !nsplit || !chunks_per_split) return BOLT_ERR_ARG;
+    *nsplit = ctx->nsplit;
+    *chunks_per_split = ctx->chunks_per_split;
+    return BOLT_OK;
+}
 size_t bolt_scratch_bytes(BoltCtx* ctx) { return ctx ? ctx->scratch_bytes : 0; }
 
 int bolt_divergence_flag(BoltCtx* ctx) {
@@ -438,11 +430,32 @@ int bolt_clear_divergence_flag(BoltCtx* ctx) {
 int bolt_status_sync(BoltCtx* ctx, void* stream) {
     if (!ctx) return BOLT_ERR_ARG;
     if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return BOLT_ERR_CUDA;
-    int e = 0;
-    if (cudaMemcpy(&e, ctx->derr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-        return BOLT_ERR_CUDA;
+    const int e = *(volatile int*)ctx->herr;
     if (e) return e;
     if (ctx->sticky) return ctx->sticky;
+    return BOLT_OK;
+}
+
+int bolt_error_flag(BoltCtx* ctx) {
+    if (!ctx || !ctx->herr) return BOLT_ERR_ARG;
+    return *(volatile int*)ctx->herr;
+}
+
+int bolt_clear_error(BoltCtx* ctx) {
+    if (!ctx || !ctx->herr) return BOLT_ERR_ARG;
+    *(volatile int*)ctx->herr = 0;
+    return BOLT_OK;
+}
+
+int bolt_set_wait_budget(BoltCtx* ctx, long long cycles) {
+    if (!ctx) return BOLT_ERR_ARG;
+    ctx->wait_cycles = cycles > 0 ? cycles : kDefaultWaitCycles;
+    return BOLT_OK;
+}
+
+int bolt_test_stall_waits(BoltCtx* ctx, int on) {
+    if (!ctx) return BOLT_ERR_ARG;
+    ctx->stall_test = on ? 1 : 0;
     return BOLT_OK;
 }
 
@@ -534,6 +547,8 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     a.j_out = want_j ? ctx->jpart : nullptr;
     a.flag = write_k ? nullptr : io.flag;
     a.err = ctx->derr;
+    a.wait_cycles = ctx->wait_cycles;
+    a.stall_test = ctx->stall_test;
     a.c1 = io.c1;
     a.c2 = io.c2;
     a.tau = ctx->p.tau;
@@ -596,6 +611,7 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
         : (pair ? launch_qpair_f32(a, ctx->bgk, ctx->recon_q, grid, smem, st)
                 : launch_qstage_f32(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st));
     ctx->launches++;
+    if (pair) ctx->pair_launches++;
     CK(e);
     return BOLT_OK;
 }

@@ -6,8 +6,8 @@
 // cudaMalloc/cudaFree may), and embedders that own all device memory
 // themselves.  bolt_dfdt_noalloc serves them: the caller passes f and the
 // output buffer, and the only scratch the evaluation needs -- the FP64 velocity
-// moment sums per q-cell that the BGK term reads, and an error word -- lives in
-// a fixed array in this library's device memory.
+// moment sums per q-cell that the BGK term reads, an error word and a
+// non-finite flag -- lives in a fixed array in this library's device memory.
 //
 // Limits and behaviour (also stated in include/bolt_b200.h):
 //   * the moment scratch holds BOLT_NOALLOC_MAX_QCELLS q-cells x species
@@ -17,19 +17,25 @@
 //     exits;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture;
+//     before any stream capture.  The address is cached per device for the
+//     life of the process and does not survive a cudaDeviceReset;
 //   * all calls share the array, which keeps the last call's contents; the
-//     moment sums are fully overwritten by each call and the error word is
-//     cleared at the start of each call, so calls that overlap on the GPU
-//     (different streams, or different host threads) race and must not;
-//   * fields must be disabled and the ghost cells of f must be current.
+//     moment sums are fully overwritten by each call and the error word and
+//     flag are cleared at the start of each call, so calls that overlap on the
+//     GPU (different streams, or different host threads) race and must not;
+//   * bolt_noalloc_status reads (and clears) the error word and flag of the
+//     last call, a bounded-wait timeout or a non-finite df/dt;
+//   * fields must be disabled, tau is the constant params->tau, and the ghost
+//     cells of f must be current.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <mutex>
 
 #include "../../include/bolt_b200.h"
 #include "launch.h"
+#include "validate.h"
 
 using namespace bolt;
 
@@ -38,42 +44,51 @@ namespace {
 constexpr int kMaxDevices = 64;
 constexpr size_t kMomDoubles = (size_t)kNumMom * BOLT_NOALLOC_MAX_QCELLS;
 
-// moment sums [5][Ns][Nq2][Nq1] followed by the device error word
+// moment sums [5][Ns][Nq2][Nq1], then the error word and the non-finite flag
 static __device__ __align__(256) double g_noalloc_scratch[kMomDoubles + 32];
 
-double* g_scratch_ptr[kMaxDevices];   // device address of g_noalloc_scratch, per device
+double* g_scratch_ptr[kMaxDevices];          // device address of g_noalloc_scratch
+int g_scratch_rc[kMaxDevices];               // result of its lookup
+std::once_flag g_scratch_once[kMaxDevices];  // one lookup per device
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+EncodeTiledFn lookup_encode_fn() {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+        return reinterpret_cast<EncodeTiledFn>(p);
+    return nullptr;
+}
+
+// looked up once per process, thread-safely (function-local static)
 EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess && q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
+    static const EncodeTiledFn fn = lookup_encode_fn();
     return fn;
 }
 
 int scratch_for_current_device(double** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BOLT_ERR_CUDA;
-    if (!g_scratch_ptr[dev]) {
+    std::call_once(g_scratch_once[dev], [dev] {
         void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
-            return BOLT_ERR_CUDA;
-        g_scratch_ptr[dev] = static_cast<double*>(p);
-    }
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            g_scratch_rc[dev] = BOLT_ERR_CUDA;
+        } else {
+            g_scratch_ptr[dev] = static_cast<double*>(p);
+            g_scratch_rc[dev] = BOLT_OK;
+        }
+    });
+    if (g_scratch_rc[dev]) return g_scratch_rc[dev];
     *out = g_scratch_ptr[dev];
     return BOLT_OK;
 }
+
+int* error_words(double* scratch) { return reinterpret_cast<int*>(scratch + kMomDoubles); }
 
 }  // namespace
 
@@ -82,20 +97,18 @@ extern "C" int bolt_dfdt_noalloc(const BoltGrid* grid, const BoltParams* params,
     if (!grid || !params || !f_dev || !dfdt_dev) return BOLT_ERR_ARG;
     const BoltGrid& g = *grid;
     const BoltParams& p = *params;
-    if (g.N_q1 < 1 || g.N_q2 < 1 || g.N_p1 < 1 || g.N_p2 < 1 || g.N_p3 < 1 || g.N_ghost < 0 ||
-        g.N_s < 1 || g.N_s > BOLT_MAX_SPECIES)
-        return BOLT_ERR_ARG;
-    if (p.dtype != BOLT_F64 && p.dtype != BOLT_F32) return BOLT_ERR_ARG;
-    if (p.recon_q < 0 || p.recon_q > 3 || p.p_dim < 1 || p.p_dim > 3) return BOLT_ERR_ARG;
+    const int vrc = check_grid_params(g, p);
+    if (vrc) return vrc;
     if (p.fields_enabled) return BOLT_ERR_UNSUPPORTED;
+    if (p.source_enabled && !(p.tau > 0.0)) return BOLT_ERR_ARG;
     if ((long long)g.N_s * g.N_q1 * g.N_q2 > BOLT_NOALLOC_MAX_QCELLS) return BOLT_ERR_UNSUPPORTED;
 
     double* scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
     if (rc) return rc;
-    int* err = reinterpret_cast<int*>(scratch + kMomDoubles);
+    int* err = error_words(scratch);            // [0] error word, [1] non-finite flag
     cudaStream_t st = (cudaStream_t)stream;
-    if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return BOLT_ERR_CUDA;
+    if (cudaMemsetAsync(err, 0, 2 * sizeof(int), st) != cudaSuccess) return BOLT_ERR_CUDA;
 
     const int Np = g.N_p1 * g.N_p2 * g.N_p3;
     const int Nq1g = g.N_q1 + 2 * g.N_ghost, Nq2g = g.N_q2 + 2 * g.N_ghost;
@@ -117,7 +130,8 @@ extern "C" int bolt_dfdt_noalloc(const BoltGrid* grid, const BoltParams* params,
         if (e != cudaSuccess) return BOLT_ERR_CUDA;
     }
 
-    // same tiling and p-split rules as the context path
+    // the context path's tiling and p-split rules (the split is chosen for the
+    // current device's SM count; the result does not depend on it)
     const bool q2_needed = g.N_q2 > 1 || p.bc_q2 != BOLT_BC_PERIODIC;
     const int tiling = g.N_q2 == 1 ? (q2_needed ? TILING_1D_Q2 : TILING_1D) : TILING_2D;
     const TileShape t = tile_shape(tiling);
@@ -126,12 +140,9 @@ extern "C" int bolt_dfdt_noalloc(const BoltGrid* grid, const BoltParams* params,
     const int bgk_direct = (p.p_dim == 1 ||
                             (size_t)t.tq1 * t.tq2 * ntab * sizeof(double) > 64 * 1024) ? 1 : 0;
     const int nchunks = (Np + PW - 1) / PW;
-    const long long base_ctas = (long long)ntiles1 * ntiles2 * g.N_s;
-    long long want = (148LL * 8 + base_ctas - 1) / base_ctas;
-    if (want < 1) want = 1;
-    if (want > nchunks) want = nchunks;
-    const int cps = (int)((nchunks + want - 1) / want);
-    const int nsplit = (nchunks + cps - 1) / cps;
+    const size_t smem = qstage_smem(tiling, elem, bgk, bgk_direct, ntab);
+    const PSplit sp = choose_psplit(nchunks, (long long)ntiles1 * ntiles2 * g.N_s,
+                                    current_sm_count(), smem);
 
     QStageArgs a;
     memset(&a, 0, sizeof(a));
@@ -155,22 +166,40 @@ extern "C" int bolt_dfdt_noalloc(const BoltGrid* grid, const BoltParams* params,
     a.mom_in = scratch;
     a.nsplit_in = 1;
     a.err = err;
+    a.flag = err + 1;
+    a.wait_cycles = kDefaultWaitCycles;
     a.tau = p.tau;
     a.dq1 = g.dq1; a.dq2 = g.dq2; a.kB = p.boltzmann_constant;
     a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost; a.Ns = g.N_s;
     a.Np1 = g.N_p1; a.Np2 = g.N_p2; a.Np3 = g.N_p3; a.Np = Np;
     a.Nq1g = Nq1g; a.Nq2g = Nq2g;
-    a.nsplit = nsplit;
-    a.chunks_per_split = cps;
+    a.nsplit = sp.nsplit;
+    a.chunks_per_split = sp.chunks_per_split;
     a.ntiles1 = ntiles1;
     a.p_dim = p.p_dim;
     a.bgk_direct = bgk_direct;
     a.full_chunks = (Np % PW) == 0;
     a.sg = sg;
-    dim3 grid_dim(ntiles1 * ntiles2, g.N_s * nsplit);
-    const size_t smem = qstage_smem(tiling, elem, bgk, bgk_direct, ntab);
+    dim3 grid_dim(ntiles1 * ntiles2, g.N_s * sp.nsplit);
     cudaError_t e = elem == 8
         ? launch_qstage_f64(a, p.recon_q, tiling, bgk, grid_dim, smem, st)
         : launch_qstage_f32(a, p.recon_q, tiling, bgk, grid_dim, smem, st);
     return e == cudaSuccess ? BOLT_OK : BOLT_ERR_CUDA;
+}
+
+extern "C" int bolt_noalloc_status(void* stream, int* status) {
+    if (!status) return BOLT_ERR_ARG;
+    *status = BOLT_OK;
+    double* scratch = nullptr;
+    int rc = scratch_for_current_device(&scratch);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    int w[2] = {0, 0};
+    int* err = error_words(scratch);
+    if (cudaMemcpyAsync(w, err, sizeof(w), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemsetAsync(err, 0, sizeof(w), st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return BOLT_ERR_CUDA;
+    *status = w[0] ? w[0] : (w[1] ? BOLT_ERR_NONFINITE : BOLT_OK);
+    return BOLT_OK;
 }

@@ -12,6 +12,10 @@ constexpr int HALO = 3;         // q-stencil half width incl. face shift
 constexpr int NTHREADS = 256;   // q-stage CTA size (8 warps)
 constexpr int kNumMom = 5;      // n, mom_v1, mom_v2, mom_v3, energy
 constexpr int PWP = PW + 1;     // padded stage-buffer row (conflict-free column reads)
+// default budget of a bounded mbarrier wait, in SM clock cycles (~2 s at the
+// boost clock); after it the wait reports failure and the kernel records
+// BOLT_ERR_TIMEOUT in its error word instead of hanging
+constexpr long long kDefaultWaitCycles = 4000000000LL;
 
 // Shared-memory carve-up of the q-stage kernel (byte offsets), used by the
 // kernel and by the host to size the launch.
@@ -113,6 +117,10 @@ struct QStageArgs {
     int use_tma, p_dim, want_j;
     int bgk_direct;             // 1: exp per cell (no per-q-cell exp tables)
     int full_chunks;            // Np % 32 == 0: every p-chunk is complete
+    // budget of the tile waits (cycles); stall_test != 0 (a test hook) issues
+    // no tile copies, so the first wait runs out with nothing in flight
+    long long wait_cycles;
+    int stall_test;
     SpeciesGrid sg;
     // paired kernel only: 8x8x32 boxes over base1, out1 (128B swizzle), out2
     CUtensorMap tm_b1, tm_o1, tm_o2;

@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "fvm_args.h"
+
 #define BOLT_RECON_PC     0
 #define BOLT_RECON_MINMOD 1
 #define BOLT_RECON_PPM    2
@@ -435,10 +437,10 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // ---------------------------------------------------------------------------
 // mbarrier + TMA (cp.async.bulk.tensor) wrappers.  Waits are bounded: after
-// kWaitCycles clock cycles the wait reports failure and the caller records
-// BOLT_ERR_TIMEOUT instead of hanging.
+// a budget of clock cycles (the launch's wait_cycles for the tile waits,
+// kDefaultWaitCycles for the clean-up of a failed CTA) the wait reports
+// failure and the caller records BOLT_ERR_TIMEOUT instead of hanging.
 // ---------------------------------------------------------------------------
-constexpr long long kWaitCycles = 4000000000LL;   // ~2 s at the boost clock
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -471,14 +473,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
-// returns false if the barrier did not complete within the time budget
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+// returns false if the barrier did not complete within `budget` clock cycles
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity,
+                                                  long long budget = kDefaultWaitCycles) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     for (;;) {
         for (int it = 0; it < 256; ++it)
             if (mbar_try_wait(bar, parity)) return true;
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > budget) return false;
     }
 }
 

@@ -237,6 +237,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     auto issue = [&](int k, int buf) {
         if (k >= k_end) return;
         if (a.use_tma) {
+            if (a.stall_test) return;           // test hook: the wait below runs out
             if (tid == 0) {
                 mbar_arrive_expect_tx(&bars[buf], tile_bytes);
                 tma_load_3d(tile + buf * TILE, &a.tmap, &bars[buf], s * Np + k * PW,
@@ -295,7 +296,7 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
     for (int k = k_begin; k < k_end; ++k, buf ^= (NB - 1)) {
         if (a.use_tma) {
             const unsigned ph = buf ? phase1 : phase0;
-            if (!mbar_wait_bounded(&bars[buf], ph)) failed = true;
+            if (!mbar_wait_bounded(&bars[buf], ph, a.wait_cycles)) failed = true;
             if (buf) phase1 ^= 1u; else phase0 ^= 1u;
         }
         // tile visible; previous chunk's phase C done with `stage`.  A wait
@@ -305,7 +306,8 @@ qstage_kernel(const __grid_constant__ QStageArgs a) {
             if (tid == 0) {
                 atomicExch(a.err, 4);
                 // chunk k's parity was already flipped above; chunk k+1's not
-                for (int j = 0; j < NB && k + j < k_end; ++j) {
+                // (under the stall hook no copy was issued)
+                for (int j = 0; j < NB && k + j < k_end && !a.stall_test; ++j) {
                     const int b = (buf + j) % NB;
                     const unsigned ph = (b ? phase1 : phase0) ^ (j == 0 ? 1u : 0u);
                     mbar_wait_bounded(&bars[b], ph);

@@ -32,6 +32,42 @@ inline size_t qstage_smem(int tiling, size_t elem, int bgk, int bgk_direct, int 
 // bytes of dynamic shared memory of the paired FP32 kernel
 inline size_t qpair_smem(int ntab, int bgk) { return qpair_layout(ntab, bgk).total; }
 
+// p-split of the q-stage grid (q-tiles x species x splits): the split that
+// minimises (waves, rounded up) x (chunks per CTA + ~2 chunks of prologue), a
+// wave being the GPU's SMs x the stage kernel's resident CTAs per SM (from its
+// shared memory, at most 2).  Shared by the context and the allocation-free
+// entry point.
+struct PSplit {
+    int nsplit, chunks_per_split;
+};
+
+inline PSplit choose_psplit(int nchunks, long long base_ctas, int sms, size_t smem_per_cta) {
+    long long per_sm = 233472LL / (long long)(smem_per_cta + 1024);
+    per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
+    const long long wave = (long long)(sms > 0 ? sms : 1) * per_sm;
+    double best = 1e300;
+    int best_cps = nchunks;
+    for (int n = 1; n <= nchunks && n <= 64; ++n) {
+        const int cps = (nchunks + n - 1) / n;
+        const int ne = (nchunks + cps - 1) / cps;
+        const long long waves = (base_ctas * ne + wave - 1) / wave;
+        const double cost = (double)waves * (cps + 2.0);
+        if (cost < best - 1e-9) {
+            best = cost;
+            best_cps = cps;
+        }
+    }
+    return PSplit{(nchunks + best_cps - 1) / best_cps, best_cps};
+}
+
+// SM count of the current device (148 on B200 if the query fails)
+inline int current_sm_count() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
 // the f, flux and two divergence arrays, then the p-cell centres (doubles)
 inline size_t pstage_smem(int Np, size_t elem, int ntab) {
     return ((4 * (size_t)Np * elem + 7) & ~(size_t)7) + (size_t)ntab * sizeof(double);

@@ -148,7 +148,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     bool failed = false;
     unsigned pend = 0u;        // thread 0: barriers with a load in flight
     auto load_x = [&](int k, int b) {
-        if (k < k_end) {
+        if (k < k_end && !a.stall_test) {       // test hook: no copy, the wait runs out
             pend |= 1u << b;
             mbar_arrive_expect_tx(&bars[b], XT * 4);
             tma_load_3d(X + b * XT, &a.tmap, &bars[b], xs + k * PW, i0 + Ng - HALO,
@@ -156,7 +156,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         }
     };
     auto load_b = [&](int k, int b) {          // base1 tile of chunk k -> buffer b
-        if (!BX && k < k_end) {
+        if (!BX && k < k_end && !a.stall_test) {
             pend |= 4u << b;
             mbar_arrive_expect_tx(&bars[2 + b], kPairTile);
             tma_load_3d(b1s + b * (kPairTile / 4), &a.tm_b1, &bars[2 + b], xs + k * PW, i0 + Ng,
@@ -223,7 +223,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     unsigned phx0 = 0u, phx1 = 0u, phb0 = 0u, phb1 = 0u;
     int buf = 0;
     for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
-        if (!failed && !mbar_wait_bounded(&bars[buf], buf ? phx1 : phx0)) failed = true;
+        if (!failed && !mbar_wait_bounded(&bars[buf], buf ? phx1 : phx0, a.wait_cycles))
+            failed = true;
         if (buf) phx1 ^= 1u; else phx0 ^= 1u;
         pend &= ~(1u << buf);
         // no CTA barrier here: each thread has waited for the halo tile itself,
@@ -263,7 +264,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         // the base tiles of chunk k must have landed, before phase B
         if (tid == 0) bulk_wait_read_all();
         if (!BX) {
-            if (!failed && !mbar_wait_bounded(&bars[2 + buf], buf ? phb1 : phb0)) failed = true;
+            if (!failed && !mbar_wait_bounded(&bars[2 + buf], buf ? phb1 : phb0, a.wait_cycles))
+                failed = true;
             if (buf) phb1 ^= 1u; else phb0 ^= 1u;
             pend &= ~(4u << buf);
         }

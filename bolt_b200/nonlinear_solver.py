@@ -572,9 +572,22 @@ class nonlinear_solver(object):
     def check_divergence(self):
         """timestep.py:28-38 -- the device flags any non-finite f value written
         by a step; the flag is read from pinned host memory without
-        synchronising, so it reports steps whose kernels have completed."""
+        synchronising, so it reports steps whose kernels have completed (the
+        reference's check is synchronous; here a non-finite step raises at the
+        first step boundary after its kernels finished).  A stage whose
+        bounded tile wait ran out left part of f unwritten: its error word is
+        read the same way and raised as a BoltError (BOLT_ERR_TIMEOUT)."""
+        err = self._lib.bolt_error_flag(self._ctx)
+        if err:
+            raise N.BoltError(err, 'stage kernel')
         if self._lib.bolt_divergence_flag(self._ctx):
             raise SystemExit('Solver Diverging!')
+
+    def set_wait_budget(self, cycles):
+        """Budget of the stage kernels' bounded tile waits in SM clock cycles
+        (None or <= 0: the default, about 2 s)."""
+        N.check(self._lib.bolt_set_wait_budget(self._ctx, int(cycles or 0)),
+                'bolt_set_wait_budget')
 
     # with the FVM in both q and p every splitting scheme is the same step
     # (timestep.py:13-15)
@@ -750,6 +763,18 @@ class nonlinear_solver(object):
 
     def launch_count(self):
         return int(self._lib.bolt_launch_count(self._ctx))
+
+    def paired_launch_count(self):
+        """Launches of the paired FP32 stage kernel among launch_count()."""
+        return int(self._lib.bolt_paired_launch_count(self._ctx))
+
+    def split_info(self):
+        """(nsplit, chunks_per_split) of the q-stage grid's p-split."""
+        import ctypes
+        n, c = ctypes.c_int(), ctypes.c_int()
+        N.check(self._lib.bolt_split_info(self._ctx, ctypes.byref(n), ctypes.byref(c)),
+                'bolt_split_info')
+        return n.value, c.value
 
     def synchronize(self):
         rc = self._lib.bolt_status_sync(self._ctx, self._stream())

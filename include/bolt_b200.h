@@ -229,23 +229,62 @@ int  bolt_clear_divergence_flag(BoltCtx* ctx);
  * trigger the implicit synchronisation of cudaMalloc/cudaFree, embedders
  * that own all device memory).  No reference counterpart: Bolt's df_dt_fvm
  * always allocates its temporaries.  Same result as bolt_dfdt for
- * fields-disabled problems: writes df/dt of f (ghost cells current) into the
- * interior cells of dfdt.  Its only scratch (FP64 moment sums and an error
- * word) is a fixed device array of this library holding
- * BOLT_NOALLOC_MAX_QCELLS (N_s*N_q1*N_q2) q-cells; larger grids and fields
- * return BOLT_ERR_UNSUPPORTED.  The first call on a device looks up that
+ * fields-disabled problems with a constant tau (params->tau; a phase-space
+ * tau array is not available here): writes df/dt of f (ghost cells current)
+ * into the interior cells of dfdt.  Its only scratch (FP64 moment sums, an
+ * error word and a non-finite flag) is a fixed device array of this library
+ * holding BOLT_NOALLOC_MAX_QCELLS (N_s*N_q1*N_q2) q-cells; larger grids and
+ * fields return BOLT_ERR_UNSUPPORTED, and grids or parameters bolt_ctx_create
+ * would refuse are refused alike.  The first call on a device looks up that
  * array's address (make it before any stream capture); calls that overlap on
  * the GPU share the array and race. */
 #define BOLT_NOALLOC_MAX_QCELLS 65536
 int  bolt_dfdt_noalloc(const BoltGrid* grid, const BoltParams* params, const void* f_dev,
                        void* dfdt_dev, void* stream);
+/* Status of the last bolt_dfdt_noalloc on the current device, read after the
+ * stream has synchronised and then cleared: *status = BOLT_OK,
+ * BOLT_ERR_TIMEOUT (a bounded tile wait ran out and part of dfdt is
+ * unwritten) or BOLT_ERR_NONFINITE (df/dt holds Inf/NaN).  Allocates nothing;
+ * returns BOLT_ERR_CUDA if the copy or the synchronisation failed. */
+int  bolt_noalloc_status(void* stream, int* status);
 
-/* Synchronise the stream and return the first sticky error of the context. */
+/* Synchronise the stream and return the first sticky error of the context:
+ * the device error word (BOLT_ERR_TIMEOUT once a stage kernel's bounded wait
+ * ran out), else the first failed CUDA call. */
 int  bolt_status_sync(BoltCtx* ctx, void* stream);
+
+/* The device error word without synchronising (it lives in pinned host
+ * memory): BOLT_OK, or BOLT_ERR_TIMEOUT once a stage kernel whose bounded
+ * tile wait ran out has finished; that stage left part of its output
+ * unwritten.  Like bolt_divergence_flag it reports kernels that have
+ * completed; bolt_clear_error resets it.  Extends check_divergence
+ * (timestep.py:28-38), which has no timeout to report. */
+int  bolt_error_flag(BoltCtx* ctx);
+int  bolt_clear_error(BoltCtx* ctx);
+
+/* Budget of the stage kernels' bounded tile waits, in SM clock cycles; the
+ * default (<= 0 restores it) is 4e9, about 2 s at the boost clock. */
+int  bolt_set_wait_budget(BoltCtx* ctx, long long cycles);
+
+/* Test hook: with on != 0 the TMA stage kernels issue no tile copies, so the
+ * first bounded tile wait of every CTA runs out (after the budget above) with
+ * nothing in flight; the CTAs record BOLT_ERR_TIMEOUT and return without
+ * writing their outputs.  It makes the timeout path testable without a fault
+ * or a hang.  No reference counterpart. */
+int  bolt_test_stall_waits(BoltCtx* ctx, int on);
 const char* bolt_strerror(int code);
 
-/* Number of kernels launched through this context so far. */
+/* Number of kernels launched through this context so far, and how many of
+ * them were the paired FP32 stage kernel (the fused q-stage taken for FP32
+ * 8x8-tiled grids; every other stage runs the one-cell-per-thread kernel).
+ * Diagnostics: the reference has no counterpart. */
 long long bolt_launch_count(BoltCtx* ctx);
+long long bolt_paired_launch_count(BoltCtx* ctx);
+
+/* The context's p-split of the q-stage grid: nsplit CTAs per q-tile and
+ * species, each over chunks_per_split chunks of 32 p-cells (chosen to fill
+ * the GPU's SMs; $BOLT_CHUNKS_PER_SPLIT at context creation fixes it). */
+int  bolt_split_info(BoltCtx* ctx, int* nsplit, int* chunks_per_split);
 
 /* Bytes of device scratch held by the context. */
 size_t bolt_scratch_bytes(BoltCtx* ctx);

@@ -178,6 +178,59 @@ CASES['c3_2d3v_weno5_rk4_ghost4'] = make(
     riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
     init=dict(amp=0.05, k1=1, k2=1, noise=1e-3, seed=4, u=[0.1, -0.2, 0.05]))
 
+# The headline velocity grid, 24^3 p-cells per q-cell, on one 8x8 q-tile (the
+# smallest grid the paired FP32 kernel takes): 13,824 p-cells are 432 chunks
+# of 32, so most chunks start inside a p1 row and a p-split's first chunk at
+# any p1 offset that is a multiple of 8.  Its f (0.9M cells) is too large to
+# store whole, so make_golden.py writes a compact fixture (see compact()).
+COMPACT_CASES = {
+    'c3_2d3v_weno5_rk4_p24': make(
+        N_q1=8, N_q2=8, N_p1=24, N_p2=24, N_p3=24,
+        p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0], p2_end=[6.0],
+        p3_start=[-6.0], p3_end=[6.0], mass=[1.0], charge=[0.0], p_dim=3,
+        tau=0.05, dt=1e-3, steps=3, integrator='RK4', compact=True,
+        riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+        init=dict(amp=0.05, k1=1, k2=1)),
+}
+# interior (q2, q1) cells whose df/dt and f_final a compact fixture holds in full
+COMPACT_SEL = ((0, 0), (7, 7), (2, 5), (5, 2))
+
+
+def compact_f0(fx):
+    """f0 with ghost cells from a compact fixture's factors: n_q[q2, q1] times
+    v_p[p3, p2, p1], the single multiplication initialize_f ends with."""
+    n, v = fx['n_q'], fx['v_p']
+    return n[:, :, None, None, None, None] * v[None, None, None]
+
+
+def periodic_wrap(a, spec):
+    """The interior of a (Nq2g, Nq1g, ...) array with its ghost cells refilled
+    periodically (communicate_f on a periodic grid)."""
+    g = spec['N_ghost']
+    inner = a[g:a.shape[0] - g, g:a.shape[1] - g]
+    j = (np.arange(a.shape[0]) - g) % inner.shape[0]
+    i = (np.arange(a.shape[1]) - g) % inner.shape[1]
+    return inner[j][:, i]
+
+
+def qcell_sums(spec, a):
+    """Per q-cell and species velocity sums of an interior (Nq2, Nq1, Ns, Np3,
+    Np2, Np1) array x: [sum x, sum v1 x, sum v2 x, sum v3 x, sum |v|^2 x,
+    sum x^2] over p (no p-cell measure), shape (Nq2, Nq1, Ns, 6)."""
+    out = np.empty(a.shape[:3] + (6,))
+    for s in range(a.shape[2]):
+        p1, p2, p3 = _pgrid(spec, s)
+        x = a[:, :, s]
+        sm = lambda y: y.sum(axis=(2, 3, 4))
+        out[:, :, s, 0] = sm(x)
+        out[:, :, s, 1] = sm(x * p1)
+        out[:, :, s, 2] = sm(x * p2)
+        out[:, :, s, 3] = sm(x * p3)
+        out[:, :, s, 4] = sm(x * (p1 ** 2 + p2 ** 2 + p3 ** 2))
+        out[:, :, s, 5] = sm(x * x)
+    return out
+
+
 # user-defined initial fields (fields.py:280-420): each form of the initialize
 # module's field functions, FDTD-coupled 2D2V, reference scheme (RK2)
 _FIELD_INIT_BASE = dict(

@@ -6,7 +6,8 @@ The PETSc binary Vec format of those files is the stand-in viewer's: the
 big-endian int32 Vec class id 1211214, the int32 length, then big-endian
 float64 values.  Test infrastructure, run in the container with the reference:
 
-    python tests/golden/make_dump_golden.py [/path/to/reference] [case ...]
+    python tests/golden/make_dump_golden.py /path/to/reference [case ...]
+    (or the reference root in $BOLT_REFERENCE_DIR)
 
 writes tests/golden/dumps/<case>_{f,moments,fields}.bin and <case>_state.npz
 (the interior f the dumps were made from, in (q2, q1, s, p3, p2, p1) order).
@@ -57,13 +58,7 @@ def dump_case(name):
 
 
 def main(argv):
-    ref = '/root/reference'
-    names = []
-    for a in argv:
-        if os.path.isdir(a):
-            ref = a
-        else:
-            names.append(a)
+    ref, names = G.reference_dir(argv)
     sys.path.insert(1, ref)
     for name in names or CASES:
         dump_case(name)

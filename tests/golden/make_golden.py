@@ -1,7 +1,8 @@
 """Generate golden fixtures by running the UNMODIFIED Bolt reference source.
 
-Usage (in a container where the reference is present, read-only):
-    python tests/golden/make_golden.py [/path/to/reference] [case ...]
+Usage (where a read-only copy of the reference project is present):
+    python tests/golden/make_golden.py /path/to/reference [case ...]
+    BOLT_REFERENCE_DIR=/path/to/reference python tests/golden/make_golden.py [case ...]
 
 The reference's runtime stack (arrayfire, petsc4py, mpi4py, prettytable) is not
 installable offline, so single-process numpy stand-ins from tests/golden/refshim
@@ -53,7 +54,10 @@ def q_to_layout(a):
     return np.transpose(arr[0], (2, 1, 0)).copy()
 
 
-def build_modules(spec, af):
+def build_modules(spec, af, record=None):
+    """Config modules of a case; with a dict `record`, initialize_f also leaves
+    its q-factor n and p-factor out there (f0 = n * out, one multiplication
+    per cell)."""
     dom = types.ModuleType('domain')
     for k in ('q1_start', 'q1_end', 'q2_start', 'q2_end', 'N_q1', 'N_q2',
               'N_p1', 'N_p2', 'N_p3', 'N_ghost'):
@@ -66,7 +70,7 @@ def build_modules(spec, af):
     noise = C._noise(spec, Nq1g, Nq2g)            # (Nq2g, Nq1g)
     noise_af = af.Array._wrap(noise.T[None, None])  # (1, 1, Nq1g, Nq2g)
 
-    def make_f(ini):
+    def make_f(ini, record=None):
         def fn(q1, q2, p1, p2, p3, params):
             m = params.mass
             k = params.boltzmann_constant
@@ -80,6 +84,8 @@ def build_modules(spec, af):
             for d, p in enumerate((p1, p2, p3)[:params.p_dim]):
                 out = out * af.sqrt(m / (2 * np.pi * k * T[d])) \
                     * af.exp(-m * (p - u[d]) ** 2 / (2 * k * T[d]))
+            if record is not None:
+                record['n'], record['out'] = n, out
             return n * out
         return fn
 
@@ -87,7 +93,7 @@ def build_modules(spec, af):
     ini = dict(init_defaults)
     ini.update(spec['init'])
     initialize = types.ModuleType('initialize')
-    initialize.initialize_f = make_f(ini)
+    initialize.initialize_f = make_f(ini, record)
     if spec.get('field_init'):
         for k, fn in C.field_functions(spec['field_init'], af.sin, af.cos).items():
             setattr(initialize, k, fn)
@@ -196,11 +202,14 @@ def run_case(name, spec):
     # prints a number; skip its 100 x 268 MB numpy additions
     import bolt.lib.nonlinear.nonlinear_solver as nsmod
     nsmod.bandwidth_test = lambda n_evals: 0.0
-    dom, bc, params, initialize = build_modules(spec, af)
+    record = {}
+    dom, bc, params, initialize = build_modules(spec, af, record)
     system = physical_system(dom, bc, params, initialize, adv, col.BGK, mom)
     nls = nonlinear_solver(system)
     out = {}
     out['f0'] = interior(af_to_layout(nls.f, spec), spec)
+    if spec.get('compact'):
+        out['n_q'], out['v_p'] = init_factors(record, spec, out['f0'])
     # df/dt of the halo-refreshed initial state (fields at their initial level)
     f_save = nls.f
     nls._communicate_f()
@@ -228,6 +237,32 @@ def run_case(name, spec):
         out['fields_yee'] = np.transpose(np.asarray(nls.fields_solver.yee_grid_EM_fields)
                                          .reshape(6, 1, Nq(spec, 1), Nq(spec, 2))[:, 0], (0, 2, 1))
     out['time_elapsed'] = np.array(nls.time_elapsed)
+    return compact(out, spec) if spec.get('compact') else out
+
+
+def init_factors(record, spec, f0):
+    """initialize_f's factors in the fixture layout: n_q (Nq2g, Nq1g) and v_p
+    (Np3, Np2, Np1), checked to rebuild the reference's f0 bit for bit."""
+    n = np.asarray(record['n'])
+    n = n.reshape(n.shape + (1,) * (4 - n.ndim))[0, 0].T.copy()
+    v = np.asarray(record['out']).reshape(spec['N_p3'], spec['N_p2'], spec['N_p1']).copy()
+    assert np.array_equal(interior(C.compact_f0({'n_q': n, 'v_p': v}), spec), f0)
+    return n, v
+
+
+def compact(out, spec):
+    """A compact fixture for a case whose f is too large to store: the factors
+    of f0, the halo-refreshed f0 checked to be its periodic wrap, df/dt and
+    f_final in full at the q-cells C.COMPACT_SEL and as per-q-cell velocity
+    sums (C.qcell_sums) everywhere, and the moments."""
+    full = C.compact_f0(out)
+    assert np.array_equal(out.pop('f0_refreshed'), C.periodic_wrap(full, spec))
+    out.pop('f0')
+    sel = np.array(C.COMPACT_SEL)
+    for k in ('dfdt0', 'f_final'):
+        a = out.pop(k)
+        out[k + '_sel'] = a[sel[:, 0], sel[:, 1]].copy()
+        out[k + '_qsum'] = C.qcell_sums(spec, a)
     return out
 
 
@@ -240,18 +275,28 @@ def Nq(spec, d):
     return spec['N_q%d' % d] + 2 * spec['N_ghost']
 
 
-def main(argv):
-    ref = '/root/reference'
+def reference_dir(argv):
+    """The reference project's root: the first argument that is a directory,
+    else $BOLT_REFERENCE_DIR; the remaining arguments are case names."""
+    ref = os.environ.get('BOLT_REFERENCE_DIR')
     names = []
     for a in argv:
         if os.path.isdir(a):
             ref = a
         else:
             names.append(a)
+    if not ref or not os.path.isdir(os.path.join(ref, 'bolt')):
+        raise SystemExit('give the reference project root (containing bolt/) as an argument '
+                         'or in BOLT_REFERENCE_DIR')
+    return ref, names
+
+
+def main(argv):
+    ref, names = reference_dir(argv)
     sys.path.insert(1, ref)
-    names = names or sorted(C.CASES)
+    names = names or sorted(C.CASES) + sorted(C.COMPACT_CASES)
     for name in names:
-        spec = C.CASES[name]
+        spec = C.CASES[name] if name in C.CASES else C.COMPACT_CASES[name]
         out = run_case(name, spec)
         np.savez_compressed(os.path.join(HERE, name + '.npz'), **out)
         print('wrote', name, {k: v.shape for k, v in out.items()})

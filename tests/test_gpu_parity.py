@@ -20,7 +20,7 @@ import torch
 
 import cases as C
 from _modules import make_solver, to_layout, moments_layout
-from _util import load_golden, rel, interior, moment_errors
+from _util import load_golden, rel, interior, moment_errors, check_compact
 
 pytestmark = pytest.mark.gpu
 
@@ -261,3 +261,94 @@ def test_paired_kernel_matches_scalar_kernel(monkeypatch, recon):
     errs = moment_errors({k: interior(v, g) for k, v in out['pair'][1].items()},
                          {k: interior(v, g) for k, v in out['scalar'][1].items()})
     assert max(errs.values()) < 1e-6, errs
+
+
+# ---------------------------------------------------------------------------
+# The headline velocity grid: 24^3 p-cells per q-cell (432 chunks of 32 p, so
+# a chunk, and a p-split's first chunk, can start inside a p1 row)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_reference_at_headline_velocity_grid(precision):
+    """8x8 q x 24^3 p, WENO5 + LLF, BGK, RK4, 3 steps, from the compact
+    reference fixture: df/dt of the refreshed initial state and f after the
+    steps, in full at the fixture's q-cells and as per-q-cell velocity sums
+    everywhere, and the five moments.  FP32 steps run the paired kernel."""
+    name = 'c3_2d3v_weno5_rk4_p24'
+    spec = C.COMPACT_CASES[name]
+    G = load_golden(name)
+    tol = TOL[precision]
+    g = spec['N_ghost']
+    nls = make_solver(spec, precision)
+    f0 = C.compact_f0(G)
+    assert rel(interior(to_layout(nls.f, spec), g), interior(f0, g)) < tol['f0']
+    nls.f = af_from_layout(C.periodic_wrap(f0, spec)).to('cuda')
+    nls.dt = spec['dt']
+    d = interior(to_layout(nls.df_dt(), spec), g)
+    pair0 = nls.paired_launch_count()
+    for _ in range(spec['steps']):
+        nls.strang_timestep(spec['dt'])
+    torch.cuda.synchronize()
+    if precision == 'fp32':
+        assert nls.paired_launch_count() - pair0 == 4 * spec['steps']
+    m = {k: interior(moments_layout(nls.compute_moments(k)), g) for k in MOMENTS}
+    check_compact(spec, G, interior(to_layout(nls.f, spec), g), m, dfdt0=d,
+                  tol_f=tol['f'], tol_dfdt=tol['dfdt'], tol_mom=tol['mom'])
+    assert abs(nls.time_elapsed - float(G['time_elapsed'])) < 1e-12
+    nls.synchronize()
+
+
+HEADLINE_P_MULTI = C.make(
+    N_q1=16, N_q2=16, N_p1=24, N_p2=24, N_p3=24,
+    p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0], p2_end=[6.0],
+    p3_start=[-6.0], p3_end=[6.0], mass=[1.0], charge=[0.0], p_dim=3,
+    tau=0.05, dt=1e-3, steps=2, integrator='RK4',
+    riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+    init=dict(amp=0.05, k1=1, k2=1, noise=1e-3, seed=2, u=[0.1, -0.2, 0.05]))
+
+
+@pytest.fixture(scope='module')
+def headline_multi_ref():
+    """The C restatement's two RK4 steps of HEADLINE_P_MULTI from the FP64
+    solver's initial state (the restatement is pinned to the numpy oracle and
+    the fixtures by tests/test_c_oracle.py)."""
+    from oracle import c_oracle
+    from oracle.bolt_oracle import Oracle
+    spec = HEADLINE_P_MULTI
+    f = np.ascontiguousarray(to_layout(make_solver(spec, 'fp64').f, spec))
+    f0 = f.copy()
+    for _ in range(spec['steps']):
+        c_oracle.rk_step(f, spec, spec['dt'], integrator=4)
+    o = Oracle(spec, f)
+    g = spec['N_ghost']
+    return f0, interior(f, g), {k: interior(o.moments(k), g) for k in MOMENTS}
+
+
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-12), ('fp32', 2e-6)])
+@pytest.mark.parametrize('cps', [None, 432, 54, 7, 5])
+def test_headline_velocity_grid_multi_tile_vs_oracle(monkeypatch, headline_multi_ref, precision,
+                                                     tol, cps):
+    """16x16 q (four 8x8 tiles) x 24^3 p with density noise, two RK4 steps,
+    under the automatic p-split and under fixed splits of 432 (one split), 54,
+    7 and 5 chunks per CTA (a split's first p lies at p1 offset 0, 8 or 16 of
+    a row): f and the moments against the C restatement from the same state."""
+    spec = HEADLINE_P_MULTI
+    if cps is not None:
+        monkeypatch.setenv('BOLT_CHUNKS_PER_SPLIT', str(cps))
+    f0, ref_f, ref_m = headline_multi_ref
+    nls = make_solver(spec, precision)
+    nsplit, got_cps = nls.split_info()
+    if cps is not None:
+        assert got_cps == cps and nsplit == -(-432 // cps)
+    nls.f = af_from_layout(f0).to('cuda')
+    for _ in range(spec['steps']):
+        nls.strang_timestep(spec['dt'])
+    torch.cuda.synchronize()
+    if precision == 'fp32':
+        assert nls.paired_launch_count() == 4 * spec['steps']
+    g = spec['N_ghost']
+    e = rel(interior(to_layout(nls.f, spec), g), ref_f)
+    assert e < tol, e
+    m = {k: interior(moments_layout(nls.compute_moments(k)), g) for k in MOMENTS}
+    errs = moment_errors(m, ref_m)
+    assert max(errs.values()) < tol, errs
+    nls.synchronize()

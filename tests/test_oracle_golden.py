@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import cases as C
-from _util import load_golden, rel, interior, moment_errors
+from _util import load_golden, rel, interior, moment_errors, check_compact
 from oracle.bolt_oracle import Oracle, Grid, moment
 
 MOMENTS = ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy')
@@ -44,6 +44,26 @@ def test_oracle_matches_reference(name):
         assert rel(o.fields.cell, G['fields_cell']) < 1e-11
         assert rel(o.fields.yee, G['fields_yee']) < 1e-11
     assert abs(o.time_elapsed - float(G['time_elapsed'])) < 1e-15
+
+
+def test_oracle_matches_reference_at_24c3():
+    """The compact fixture of the bench's velocity grid (8x8 q x 24^3 p, WENO5,
+    BGK, RK4): f0 rebuilt from the stored factors, df/dt of the refreshed
+    state and f after three steps (in full at the stored q-cells, as per-q-cell
+    velocity sums everywhere), and the moments."""
+    name = 'c3_2d3v_weno5_rk4_p24'
+    spec = C.COMPACT_CASES[name]
+    G = load_golden(name)
+    g = spec['N_ghost']
+    f0 = C.compact_f0(G)
+    assert rel(interior(C.initial_f(spec), g), interior(f0, g)) < 1e-14
+    o = Oracle(spec, C.periodic_wrap(f0, spec))
+    o.dt = spec['dt']
+    d = interior(o.dfdt(o.refresh(o.f)), g)
+    for _ in range(spec['steps']):
+        o.step(spec['dt'])
+    m = {k: interior(o.moments(k), g) for k in MOMENTS}
+    check_compact(spec, G, interior(o.f, g), m, dfdt0=d)
 
 
 def test_moment_kat():

@@ -6,9 +6,12 @@ synchronisation of cudaMalloc/cudaFree, an embedder that owns all device
 memory) call bolt_dfdt_noalloc, whose only scratch is a fixed array inside the
 library.  These tests call it through the C ABI and compare it with the
 context-based bolt_dfdt on the same f, twice in a row (the shared scratch keeps
-the previous call's contents, which must not leak into the next result).
-Tolerance: 1e-12 normwise (FP64) and 1e-6 (FP32); both paths run the same
-kernels, so agreement is expected to be exact."""
+the previous call's contents, which must not leak into the next result), and
+with the reference's df/dt of that f.  Tolerances: 1e-12 normwise (FP64) and
+1e-6 (FP32) against bolt_dfdt (the same kernels, so agreement is expected to
+be exact); against the reference fixture 1e-12 (FP64) and 1e-3 (FP32: flux
+differences cancel, as in the other parity tests).  bolt_noalloc_status reads
+the call's error word and non-finite flag."""
 
 import ctypes
 
@@ -18,6 +21,7 @@ import torch
 
 import cases as C
 import bolt_b200._native as N
+from _util import load_golden
 
 SPEC = C.CASES['c3_2d3v_weno5_rk4_small']
 
@@ -49,19 +53,26 @@ def grid_params(spec, dtype):
     return g, p
 
 
+def _status(lib, stream):
+    st = ctypes.c_int(-1)
+    assert lib.bolt_noalloc_status(stream, ctypes.byref(st)) == N.BOLT_OK
+    return st.value
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize('dtype,tol', [(N.F64, 1e-12), (N.F32, 1e-6)])
-def test_noalloc_matches_context_dfdt_twice(dtype, tol):
+@pytest.mark.parametrize('dtype,tol,tol_ref', [(N.F64, 1e-12, 1e-12), (N.F32, 1e-6, 1e-3)])
+def test_noalloc_matches_context_dfdt_twice(dtype, tol, tol_ref):
     lib = N.load()
     torch.cuda.set_device(0)
     tdt = torch.float64 if dtype == N.F64 else torch.float32
     g, p = grid_params(SPEC, dtype)
-    f = torch.from_numpy(np.ascontiguousarray(C.initial_f(SPEC))).to('cuda', tdt)
+    G = load_golden('c3_2d3v_weno5_rk4_small')
+    # the reference's halo-refreshed initial state, whose df/dt the fixture holds
+    f = torch.from_numpy(np.ascontiguousarray(G['f0_refreshed'])).to('cuda', tdt)
     stream = torch.cuda.current_stream().cuda_stream
     ctx = ctypes.c_void_p()
     assert lib.bolt_ctx_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(ctx)) == N.BOLT_OK
     try:
-        assert lib.bolt_fill_ghosts(ctx, f.data_ptr(), stream) == N.BOLT_OK
         ref = torch.zeros_like(f)
         assert lib.bolt_dfdt(ctx, f.data_ptr(), ref.data_ptr(), 0, 0.0, stream) == N.BOLT_OK
         assert lib.bolt_status_sync(ctx, stream) == N.BOLT_OK
@@ -70,15 +81,40 @@ def test_noalloc_matches_context_dfdt_twice(dtype, tol):
     Ng = SPEC['N_ghost']
     inner = lambda t: t[Ng:-Ng, Ng:-Ng].double().cpu().numpy()
     r = inner(ref)
+    outs = [torch.zeros_like(f), torch.full_like(f, float('nan'))]
+    torch.cuda.synchronize()
     for call in range(2):
-        out = torch.full_like(f, float('nan')) if call else torch.zeros_like(f)
+        free0 = torch.cuda.mem_get_info()[0]
         rc = lib.bolt_dfdt_noalloc(ctypes.byref(g), ctypes.byref(p), f.data_ptr(),
-                                   out.data_ptr(), stream)
+                                   outs[call].data_ptr(), stream)
         assert rc == N.BOLT_OK, N.strerror(rc)
-        torch.cuda.synchronize()
-        got = inner(out)
+        assert _status(lib, stream) == N.BOLT_OK
+        if call:
+            # no device memory was taken by the call (the first call on the
+            # device may load the library's module; the second allocates nothing)
+            assert torch.cuda.mem_get_info()[0] == free0
+        got = inner(outs[call])
         err = np.linalg.norm(got - r) / np.linalg.norm(r)
         assert err < tol, (call, err)
+        e_ref = np.linalg.norm(got - G['dfdt0']) / np.linalg.norm(G['dfdt0'])
+        assert e_ref < tol_ref, (call, e_ref)
+
+
+@pytest.mark.gpu
+def test_noalloc_status_reports_nonfinite_and_clears():
+    lib = N.load()
+    torch.cuda.set_device(0)
+    g, p = grid_params(SPEC, N.F64)
+    G = load_golden('c3_2d3v_weno5_rk4_small')
+    f = torch.from_numpy(np.ascontiguousarray(G['f0_refreshed'])).to('cuda', torch.float64)
+    Ng = SPEC['N_ghost']
+    f[Ng + 1, Ng + 2, 0, 1, 2, 3] = float('nan')
+    out = torch.zeros_like(f)
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.bolt_dfdt_noalloc(ctypes.byref(g), ctypes.byref(p), f.data_ptr(), out.data_ptr(),
+                                 stream) == N.BOLT_OK
+    assert _status(lib, stream) == N.BOLT_ERR_NONFINITE
+    assert _status(lib, stream) == N.BOLT_OK          # read once, then cleared
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
@@ -94,3 +130,23 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     g2, _ = grid_params(SPEC, N.F64)
     assert lib.bolt_dfdt_noalloc(ctypes.byref(g2), ctypes.byref(p), ctypes.c_void_p(16),
                                  ctypes.c_void_p(16), None) == N.BOLT_ERR_UNSUPPORTED
+
+
+def test_noalloc_validates_like_the_context():
+    """Grids and parameters bolt_ctx_create refuses are refused alike, before
+    any device work: unknown boundary codes, a mirror deeper than the grid, a
+    non-periodic axis without ghost cells, BGK without a positive tau."""
+    lib = N.load()
+
+    def call(**kw):
+        g, p = grid_params(SPEC, N.F64)
+        for k, v in kw.items():
+            setattr(g if hasattr(g, k) and k.startswith('N_') else p, k, v)
+        return lib.bolt_dfdt_noalloc(ctypes.byref(g), ctypes.byref(p), ctypes.c_void_p(16),
+                                     ctypes.c_void_p(16), None)
+    assert call(bc_q1=9) == N.BOLT_ERR_ARG
+    assert call(bc_q2=-1) == N.BOLT_ERR_ARG
+    assert call(bc_q1=N.BC['mirror'], N_ghost=9) == N.BOLT_ERR_UNSUPPORTED
+    assert call(bc_q2=N.BC['dirichlet'], N_ghost=0) == N.BOLT_ERR_UNSUPPORTED
+    assert call(tau=0.0) == N.BOLT_ERR_ARG
+    assert lib.bolt_noalloc_status(None, None) == N.BOLT_ERR_ARG
