@@ -213,6 +213,19 @@ class ClockSampler(object):
                 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or the platform's."""
+    try:
+        with open('/proc/cpuinfo') as fh:
+            for ln in fh:
+                if ln.lower().startswith('model name'):
+                    return ln.split(':', 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
 def cpu_sample_spec(spec):
     s = dict(spec)
     s['N_q1'] = s['N_q2'] = 32
@@ -259,7 +272,7 @@ def run_reference(args, rank, world):
         'config': {'workload': 'Bolt FVM 2D3V 128^2 x 24^3 WENO5+LLF RK4 BGK (sampled)',
                    'parallelism': 'cpu-openmp'},
         'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': threads, 'kind': 'port',
-                         'sample': sample},
+                         'cpu_model': cpu_model(), 'sample': sample},
         'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
     print(json.dumps(line), flush=True)
@@ -427,6 +440,16 @@ def run_ours(args, rank, world, local_rank):
                 'error_after_steps': args.warmup + args.steps}
         del nls64
 
+    # the benchmark set's other targets, on one GPU (kept out of the scaling runs)
+    targets = None
+    if world == 1 and not args.no_extras:
+        f_gb = nls._fstore.numel() * (4 if args.precision == 'fp32' else 8) / 1e9
+        del nls
+        torch.cuda.empty_cache()
+        targets = other_targets(args, local_rank)
+    else:
+        f_gb = nls._fstore.numel() * (4 if args.precision == 'fp32' else 8) / 1e9
+
     if rank != 0:
         return
     word = 4 if args.precision == 'fp32' else 8
@@ -455,6 +478,7 @@ def run_ours(args, rank, world, local_rank):
         threads = os.cpu_count() or 1
         v, sps, s = time_cpu_reference(spec, 2, 1, threads)
         cpu = {'value': v, 'unit': UNIT, 'cores': threads, 'kind': 'port',
+               'cpu_model': cpu_model(),
                'sample': '%dx%d x 24^3 of the workload, FP64 C/OpenMP restatement, 2 RK4 steps'
                          % (s['N_q1'], s['N_q2'])}
     line = {
@@ -465,8 +489,7 @@ def run_ours(args, rank, world, local_rank):
         'config': {'workload': '2D3V %dx%d x 24^3 (%d cells) Maxwellian n=1+0.05cos(2pi q1)cos(2pi q2),'
                                ' BGK tau=0.05, WENO5+LLF, RK4, dt=1e-3, %s f + FP64 moments'
                                % (spec['N_q1'], spec['N_q2'], cells, args.precision.upper()),
-                   'cells': cells, 'l2': 'inputs larger than L2 (f %.2f GB), no flush'
-                                         % (nls._fstore.numel() * word / 1e9),
+                   'cells': cells, 'l2': 'inputs larger than L2 (f %.2f GB), no flush' % f_gb,
                    'parallelism': 'replicas' if world > 1 else 'single'},
         'roofline': roofline,
         'cpu_baseline': cpu,
@@ -475,16 +498,61 @@ def run_ours(args, rank, world, local_rank):
         'launches_per_step': launches_per_step,
         'clocks': clk.summary(),
         'fp64_plain': fp64,
+        'targets': targets,
     }
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, rank, world, local_rank):
+def other_targets(args, local_rank):
+    """The benchmark set's other targets, measured after the headline so the
+    default run records them: the ragged 256-run batch against sequential
+    plain runs (target >= 5x), the adjoint's gradient time and its checks
+    against central differences and FP64 autograd (target 1e-4), and the
+    FDTD-coupled 2D2V run's FP32 / FP64 throughput ratio.  Each entry is
+    measured as its own --workload measures it (see batch_result,
+    adjoint_result, c2_result); sequential runs time --seq-steps steps each,
+    scaled to the batch's step count."""
+    import torch
+    out = {}
+    t0 = time.perf_counter()
+    b = batch_result(args, 1, local_rank, seq_steps=args.seq_steps)
+    out['ragged_batch'] = {k: b[k] for k in ('value', 'sequential_value', 'speedup_vs_sequential',
+                                             'batch_s', 'sequential_s', 'sequential_steps_timed',
+                                             'schedule', 'steps')}
+    out['ragged_batch']['runs'] = b['config']['runs']
+    out['ragged_batch']['cells'] = b['config']['cells']
+    out['ragged_batch']['stage_kernel_hbm_frac'] = b['roofline']['frac']
+    torch.cuda.empty_cache()
+    t1 = time.perf_counter()
+    a = adjoint_result(args, local_rank)
+    c = a['check']
+    out['adjoint'] = {'gradient_s': a['value'], 'forward_s': a['forward_s'],
+                      'forward_to_gradient': a['forward_to_gradient'], 'steps': a['steps'],
+                      'recomputed_steps': a['recomputed_steps'],
+                      'fp64_gradient_s': a['fp64']['gradient_s'],
+                      'rel_fp64_vs_fd': c['rel_fp64_vs_fd'],
+                      'rel_fp64_vs_autograd': c['rel_fp64_vs_autograd'],
+                      'rel_fp32_vs_fp64': c['rel_fp32_vs_fp64']}
+    torch.cuda.empty_cache()
+    t2 = time.perf_counter()
+    c2 = c2_result(args, local_rank)
+    out['c2_fdtd'] = {'fp32_over_fp64': c2['fp32_over_fp64'], 'fp32_value': c2['fp32']['value'],
+                      'fp64_value': c2['fp64']['value'], 'steps': c2['steps'],
+                      'fp32_vs_fp64_after_steps': c2['fp32_vs_fp64_after_steps']}
+    t3 = time.perf_counter()
+    out['wall_s'] = {'ragged_batch': t1 - t0, 'adjoint': t2 - t1, 'c2_fdtd': t3 - t2}
+    return out
+
+
+def batch_result(args, world, local_rank, seq_steps=None):
     """The ragged 1D1V sweep: all runs advanced by BatchSolver (one launch per
     RK stage over the packed runs, the steps replayed as one CUDA graph)
     against the same runs advanced one after another by nonlinear_solver
     (sequential plain runs, same FP32 f + FP64 moments), both timed with CUDA
-    events; value = total cell-updates/s of the batch."""
+    events; value = total cell-updates/s of the batch.  With seq_steps, each
+    sequential run times seq_steps steps and its time is scaled to the
+    batch's step count (a plain run's step time does not change from step to
+    step: every step launches the same kernels)."""
     import torch
     from bolt_b200.batch import BatchSolver
     from bolt_b200.nonlinear_solver import nonlinear_solver
@@ -509,7 +577,8 @@ def run_batch(args, rank, world, local_rank):
     t_batch = e0.elapsed_time(e1) * 1e-3
     bs.synchronize()
     del bs
-    # sequential plain runs: each run constructed, then nsteps strang_timestep calls timed
+    # sequential plain runs: each run constructed, then its steps timed
+    ns = nsteps if seq_steps is None else min(seq_steps, nsteps)
     t_seq = 0.0
     for r in runs:
         nls = nonlinear_solver(ragged_system(r))
@@ -517,16 +586,14 @@ def run_batch(args, rank, world, local_rank):
             nls.strang_timestep(r['dt'])
         torch.cuda.synchronize()
         e0.record()
-        for _ in range(nsteps):
+        for _ in range(ns):
             nls.strang_timestep(r['dt'])
         e1.record()
         e1.synchronize()
-        t_seq += e0.elapsed_time(e1) * 1e-3
+        t_seq += e0.elapsed_time(e1) * 1e-3 * nsteps / ns
         del nls
     t_batch = max_over_ranks(t_batch, world)
     t_seq = max_over_ranks(t_seq, world)
-    if rank != 0:
-        return
     value = job_value(cells * nsteps, world, t_batch * 1e3)
     seq = job_value(cells * nsteps, world, t_seq * 1e3)
     line = {
@@ -539,6 +606,7 @@ def run_batch(args, rank, world, local_rank):
                                'WENO5+LLF, RK4, dt = 0.5 dq1/10, FP32 f + FP64 moments'
                                % len(runs), 'cells': cells, 'runs': len(runs)},
         'batch_s': t_batch, 'sequential_s': t_seq, 'sequential_value': seq,
+        'sequential_steps_timed': ns,
         'speedup_vs_sequential': t_seq / t_batch,
         # launch schedule picked by the batch's autotuner before the timed run
         'schedule': tuning['chosen'] if tuning else
@@ -558,10 +626,16 @@ def run_batch(args, rank, world, local_rank):
                         'frac': achieved / peak, 'traffic': None, 'peak_kind': kind,
                         'kernel': 'batch_stage_kernel', 'avg_launch_ms': launch_s * 1e3,
                         'note': 'working set comparable to L2 (126 MB)'}
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_adjoint(args, rank, world, local_rank):
+def run_batch(args, rank, world, local_rank):
+    line = batch_result(args, world, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def adjoint_result(args, local_rank):
     """Adjoint workload: gradients of J = sum_n dt |nhat_1(n)|^2 for 1D1V 128 x 256,
     p1 in [-10, 10], n = 1 + a cos(2 pi q1) (a = 0.01), Maxwellian T = 1,
     tau = 0.02, RK4, dt = 2e-4, 2000 steps, binomial checkpointing with 20
@@ -614,8 +688,6 @@ def run_adjoint(args, rank, world, local_rank):
     Jt.backward()
     rel = lambda x, y: abs(x - y) / abs(y)
     o32, o64 = out['fp32'], out['fp64']
-    if rank != 0:
-        return
     line = {
         'metric': 'adjoint of the 1D1V WENO5+LLF RK4 BGK update: gradient wall time',
         'value': o32['grad_s'], 'unit': 's', 'higher_is_better': False, 'n_gpus': 1,
@@ -639,7 +711,13 @@ def run_adjoint(args, rank, world, local_rank):
                                  'f0': float((o32['gf'] - o64['gf']).norm() / o64['gf'].norm())},
         },
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_adjoint(args, rank, world, local_rank):
+    line = adjoint_result(args, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def c2_spec():
@@ -724,7 +802,7 @@ def run_c1(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def run_c2(args, rank, world, local_rank):
+def c2_result(args, local_rank):
     """2D2V FDTD-coupled workload, FP64 and FP32 f (FP64 moments): cell-updates/s over the timed
     steps (CUDA events) and, after all steps, the FP32 error in density,
     energy and the cell-centred fields against the FP64 run."""
@@ -756,8 +834,6 @@ def run_c2(args, rank, world, local_rank):
         del nls
         torch.cuda.empty_cache()
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
-    if rank != 0:
-        return
     line = {
         'metric': 'cell-updates/s 2D2V FDTD-coupled WENO5+LLF RK4, FP32 vs FP64',
         'value': res['fp32']['value'], 'unit': UNIT, 'n_gpus': 1, 'steps': args.c2_steps,
@@ -771,7 +847,13 @@ def run_c2(args, rank, world, local_rank):
             'energy': rel(state['fp32']['energy'], state['fp64']['energy']),
             'fields': rel(state['fp32']['fields'], state['fp64']['fields'])},
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_c2(args, rank, world, local_rank):
+    line = c2_result(args, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def main():
@@ -799,6 +881,10 @@ def main():
     ap.add_argument('--batch-schedule', default=None, metavar='TILE,CTAS,LPT',
                     help='fix the batch launch schedule (e.g. 16,4,1) instead of autotuning; '
                          'the warm-up run then launches exactly 4 x batch-steps stage kernels')
+    ap.add_argument('--no-extras', action='store_true',
+                    help='skip the other targets (batch, adjoint, 2D2V) after the headline')
+    ap.add_argument('--seq-steps', type=int, default=20,
+                    help='steps timed per sequential run in the default line\'s batch target')
     ap.add_argument('--traffic', type=float, default=None,
                     help='ncu dram bytes per launch of the dominant kernel (recorded in roofline)')
     args = ap.parse_args()
