@@ -409,36 +409,55 @@ def run_ours(args, rank, world, local_rank):
            'frac_of_copy_floor': copy_ms / e2e_ms,
            'pcie_gbs_per_direction': fbytes / (copy_ms * 1e-3) / 1e9}
 
-    # FP64 plain form of the same workload (reported beside the FP32 number)
-    fp64 = None
+    # the FP64 forms of the same workload, reported beside the FP32 number:
+    # 'fp64' keeps the reference's operation order (-fmad=false, IEEE
+    # divisions; the 1e-12 parity path), 'fp64-fast' runs the paired kernel
+    # on FP64 pairs with FMA and Newton-refined reciprocals
+    fp64 = fp64f = None
     if args.precision == 'fp32' and not args.no_fp64:
         del host_in, host_out, stage_in, stage_out
-        nls64 = make_solver(spec, 'fp64')
-        for _ in range(args.warmup):
-            nls64.strang_timestep(dt)
-        torch.cuda.synchronize()
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        n64 = max(1, args.steps // 2)
-        a0.record()
-        for _ in range(n64):
-            nls64.strang_timestep(dt)
-        a1.record()
-        a1.synchronize()
-        ms64 = max_over_ranks(a0.elapsed_time(a1) / n64, world)
-        # untimed steps up to the FP32 run's count, then the relative L2
-        # error of the FP32 result's density and energy against FP64
-        for _ in range(args.steps - n64):
-            nls64.strang_timestep(dt)
-        err = {}
-        for k, v32 in mom32.items():
-            v64 = nls64.compute_moments(k)[..., g:-g, g:-g]
-            err[k] = float((v32 - v64).norm() / v64.norm())
+        res = {}
+        for form in ('fp64', 'fp64-fast'):
+            nls64 = make_solver(spec, form)
+            for _ in range(args.warmup):
+                nls64.strang_timestep(dt)
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            n64 = max(1, args.steps // 2)
+            a0.record()
+            for _ in range(n64):
+                nls64.strang_timestep(dt)
+            a1.record()
+            a1.synchronize()
+            ms64 = max_over_ranks(a0.elapsed_time(a1) / n64, world)
+            # untimed steps up to the FP32 run's count, for the error checks
+            for _ in range(args.steps - n64):
+                nls64.strang_timestep(dt)
+            mom = {k: nls64.compute_moments(k)[..., g:-g, g:-g].clone() for k in mom32}
+            res[form] = (ms64, mom, nls64.paired_launch_count())
+            del nls64
+            torch.cuda.empty_cache()
+        ms64, mom64, _ = res['fp64']
+        msf, momf, pairf = res['fp64-fast']
+        err = lambda got: {k: float((got[k] - v64).norm() / v64.norm()) for k, v64 in mom64.items()}
+        peak, _ = measured_peak()
         fp64 = {'value': job_value(cells, world, ms64), 'ms_per_step': ms64,
                 'bytes_per_cell_update': 136,
-                'fp32_rel_l2_error_vs_fp64': err,
+                'hbm_frac': 136 * cells / (ms64 * 1e-3) / (peak * 1e9),
+                'kernel': 'qstage_kernel<double> (reference operation order, -fmad=false)',
+                'fp32_rel_l2_error_vs_fp64': err(mom32),
+                'fp32_over_fp64': ms64 / ms,
                 'error_after_steps': args.warmup + args.steps}
-        del nls64
+        fp64f = {'value': job_value(cells, world, msf), 'ms_per_step': msf,
+                 'bytes_per_cell_update': 136,
+                 'hbm_frac': 136 * cells / (msf * 1e-3) / (peak * 1e9),
+                 'kernel': 'qpair_kernel<double> (FMA, Newton-refined reciprocals)',
+                 'paired_launches': pairf,
+                 'rel_l2_error_vs_fp64': err(momf),
+                 'fp32_over_fp64_fast': msf / ms,
+                 'speedup_vs_fp64': ms64 / msf,
+                 'error_after_steps': args.warmup + args.steps}
 
     # the benchmark set's other targets, on one GPU (kept out of the scaling runs)
     targets = None
@@ -498,6 +517,7 @@ def run_ours(args, rank, world, local_rank):
         'launches_per_step': launches_per_step,
         'clocks': clk.summary(),
         'fp64_plain': fp64,
+        'fp64_fast': fp64f,
         'targets': targets,
     }
     print(json.dumps(line), flush=True)
@@ -524,13 +544,14 @@ def other_targets(args, local_rank):
     out['ragged_batch']['stage_kernel_hbm_frac'] = b['roofline']['frac']
     torch.cuda.empty_cache()
     t1 = time.perf_counter()
-    a = adjoint_result(args, local_rank)
+    a = adjoint_result(args, local_rank, autograd_steps=args.autograd_steps)
     c = a['check']
     out['adjoint'] = {'gradient_s': a['value'], 'forward_s': a['forward_s'],
                       'forward_to_gradient': a['forward_to_gradient'], 'steps': a['steps'],
                       'recomputed_steps': a['recomputed_steps'],
                       'fp64_gradient_s': a['fp64']['gradient_s'],
                       'rel_fp64_vs_fd': c['rel_fp64_vs_fd'],
+                      'autograd_steps': c['autograd_steps'],
                       'rel_fp64_vs_autograd': c['rel_fp64_vs_autograd'],
                       'rel_fp32_vs_fp64': c['rel_fp32_vs_fp64']}
     torch.cuda.empty_cache()
@@ -635,7 +656,7 @@ def run_batch(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
-def adjoint_result(args, local_rank):
+def adjoint_result(args, local_rank, autograd_steps=None):
     """Adjoint workload: gradients of J = sum_n dt |nhat_1(n)|^2 for 1D1V 128 x 256,
     p1 in [-10, 10], n = 1 + a cos(2 pi q1) (a = 0.01), Maxwellian T = 1,
     tau = 0.02, RK4, dt = 2e-4, 2000 steps, binomial checkpointing with 20
@@ -676,15 +697,25 @@ def adjoint_result(args, local_rank):
             Jf = lambda aa, tt: float(r.forward(f_of(aa), tt)[0])
             out['fd_da'] = (Jf(AMP * (1 + h), TAU) - Jf(AMP * (1 - h), TAU)) / (2 * AMP * h)
             out['fd_dtau'] = (Jf(AMP, TAU * (1 + h)) - Jf(AMP, TAU * (1 - h))) / (2 * TAU * h)
-    # FP64 autograd of the transcription (checkpointed every 50 steps)
+    # FP64 autograd of the transcription (checkpointed every 50 steps), over
+    # the whole horizon or, with autograd_steps, a shorter one (the FP64
+    # adjoint is then evaluated over that horizon as well)
     sys.path.insert(0, ROOT)
     from oracle.bolt_torch import Problem1D1V
+    AG = STEPS if not autograd_steps else min(autograd_steps, STEPS)
+    o64ag = out['fp64']
+    if AG != STEPS:
+        r = Rollout1D1V(NQ, NP, P0, P1, DT, TAU, AG, snapshots=20, precision='fp64')
+        a = torch.tensor(AMP, dtype=torch.float64, device=dev, requires_grad=True)
+        tau = torch.tensor(TAU, dtype=torch.float64, device=dev, requires_grad=True)
+        rollout(f_of(a), tau, r).backward()
+        o64ag = dict(da=float(a.grad), dtau=float(tau.grad), gf=r.gradient(f_of(AMP))[0].double())
     pr = Problem1D1V(NQ, NP, P0, P1, DT, TAU, device=dev)
     a = torch.tensor(AMP, dtype=torch.float64, device=dev, requires_grad=True)
     tau = torch.tensor(TAU, dtype=torch.float64, device=dev, requires_grad=True)
     f0 = f_of(a)
     f0.retain_grad()
-    Jt, _ = pr.objective(f0, tau, STEPS, checkpoint_every=50)
+    Jt, _ = pr.objective(f0, tau, AG, checkpoint_every=50)
     Jt.backward()
     rel = lambda x, y: abs(x - y) / abs(y)
     o32, o64 = out['fp32'], out['fp64']
@@ -700,13 +731,16 @@ def adjoint_result(args, local_rank):
         'fp64': {'J': o64['J'], 'forward_s': o64['fwd_s'], 'gradient_s': o64['grad_s']},
         'check': {
             'dJ_da': {'fp64_adjoint': o64['da'], 'central_difference': out['fd_da'],
-                      'autograd_fp64': float(a.grad), 'fp32_adjoint': o32['da']},
+                      'fp32_adjoint': o32['da']},
             'dJ_dtau': {'fp64_adjoint': o64['dtau'], 'central_difference': out['fd_dtau'],
-                        'autograd_fp64': float(tau.grad), 'fp32_adjoint': o32['dtau']},
+                        'fp32_adjoint': o32['dtau']},
+            'autograd_steps': AG,
+            'autograd_fp64': {'dJ_da': float(a.grad), 'dJ_dtau': float(tau.grad),
+                              'fp64_adjoint_da': o64ag['da'], 'fp64_adjoint_dtau': o64ag['dtau']},
             'rel_fp64_vs_fd': {'a': rel(o64['da'], out['fd_da']), 'tau': rel(o64['dtau'], out['fd_dtau'])},
-            'rel_fp64_vs_autograd': {'a': rel(o64['da'], float(a.grad)),
-                                     'tau': rel(o64['dtau'], float(tau.grad)),
-                                     'f0': float((o64['gf'] - f0.grad).norm() / f0.grad.norm())},
+            'rel_fp64_vs_autograd': {'a': rel(o64ag['da'], float(a.grad)),
+                                     'tau': rel(o64ag['dtau'], float(tau.grad)),
+                                     'f0': float((o64ag['gf'] - f0.grad).norm() / f0.grad.norm())},
             'rel_fp32_vs_fp64': {'a': rel(o32['da'], o64['da']), 'tau': rel(o32['dtau'], o64['dtau']),
                                  'f0': float((o32['gf'] - o64['gf']).norm() / o64['gf'].norm())},
         },
@@ -883,6 +917,9 @@ def main():
                          'the warm-up run then launches exactly 4 x batch-steps stage kernels')
     ap.add_argument('--no-extras', action='store_true',
                     help='skip the other targets (batch, adjoint, 2D2V) after the headline')
+    ap.add_argument('--autograd-steps', type=int, default=200,
+                    help='horizon of the FP64 autograd check in the default line\'s adjoint target '
+                         '(--workload adjoint checks the whole horizon)')
     ap.add_argument('--seq-steps', type=int, default=20,
                     help='steps timed per sequential run in the default line\'s batch target')
     ap.add_argument('--traffic', type=float, default=None,

@@ -21,11 +21,12 @@ BOLT_ERR_TIMEOUT = 4
 BOLT_ERR_UNSUPPORTED = 5
 BOLT_ERR_NOMEM = 6
 
-F64, F32 = 0, 1
+F64, F32, F64_FAST = 0, 1, 2
 RECON = {'piecewise-constant': 0, 'minmod': 1, 'ppm': 2, 'weno5': 3}
 FLUX = {'upwind-flux': 0, 'upwind': 0, 'lax-friedrichs': 1, 'llf': 1,
         'local-lax-friedrichs': 1}
-BC = {'periodic': 0, 'dirichlet': 1, 'external': 2, 'mirror': 3, 'mirror+dirichlet': 4}
+BC = {'periodic': 0, 'dirichlet': 1, 'external': 2, 'mirror': 3, 'mirror+dirichlet': 4,
+      'shearing-box': 5}
 RK = {'RK2': 2, 'RK4': 4}
 FIELDS = {'electrodynamic': 0, 'electrostatic': 1}
 MOMENT_IDS = {'density': 0, 'mom_v1_bulk': 1, 'mom_v2_bulk': 2, 'mom_v3_bulk': 3,
@@ -85,8 +86,12 @@ SIGNATURES = {
     'bolt_set_tau_array': (ctypes.c_int, [_VP, _VP]),
     'bolt_set_dirichlet': (ctypes.c_int, [_VP, ctypes.c_int, _VP]),
     'bolt_fill_ghosts': (ctypes.c_int, [_VP, _VP, _VP]),
+    'bolt_set_shear': (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double]),
+    'bolt_set_time': (ctypes.c_int, [_VP, ctypes.c_double]),
     'bolt_invalidate': (ctypes.c_int, [_VP]),
     'bolt_dfdt': (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_double, _VP]),
+    'bolt_dfdt_term': (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, _VP]),
     'bolt_step': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),
     'bolt_run': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
     'bolt_stage_count': (ctypes.c_int, [_VP]),
@@ -111,6 +116,8 @@ SIGNATURES = {
     'bolt_clear_error': (ctypes.c_int, [_VP]),
     'bolt_set_wait_budget': (ctypes.c_int, [_VP, ctypes.c_longlong]),
     'bolt_test_stall_waits': (ctypes.c_int, [_VP, ctypes.c_int]),
+    'bolt_set_timing': (ctypes.c_int, [_VP, ctypes.c_int]),
+    'bolt_timings': (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_double)]),
     'bolt_strerror': (ctypes.c_char_p, [ctypes.c_int]),
     'bolt_launch_count': (ctypes.c_longlong, [_VP]),
     'bolt_paired_launch_count': (ctypes.c_longlong, [_VP]),
@@ -146,6 +153,7 @@ SIGNATURES = {
 }
 
 NOALLOC_MAX_QCELLS = 65536
+TIMING_NAMES = ('ghosts', 'moments', 'q-stage', 'p-stage', 'fields')
 
 _lib = None
 

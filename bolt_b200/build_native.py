@@ -3,8 +3,9 @@
     python -m bolt_b200.build_native          # -> bolt_b200/_native/libbolt_b200.so
 
 The FP64 kernels are compiled with -fmad=false so that their arithmetic
-follows the reference's operation order; the FP32 kernels use FMA and
-approximate division.  The library links the CUDA runtime statically and
+follows the reference's operation order; the FP32 kernels and the paired FP64
+kernel of the fast FP64 form use FMA and approximate division (FP32) or
+Newton-refined reciprocals (FP64).  The library links the CUDA runtime statically and
 loads cuTensorMapEncodeTiled through the runtime's driver entry point.
 """
 
@@ -23,6 +24,7 @@ COMMON = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '--expt-relax
 UNITS = [
     ('kernels_f64.cu', ['-fmad=false']),
     ('kernels_f32.cu', ['-prec-div=false', '-prec-sqrt=false', '-ftz=true']),
+    ('kernels_f64pair.cu', []),
     ('bolt_capi.cu', []),
     ('bolt_noalloc.cu', []),
     ('bolt_batch.cu', ['-prec-div=false', '-prec-sqrt=false', '-ftz=true']),

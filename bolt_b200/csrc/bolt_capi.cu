@@ -7,10 +7,13 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "../../include/bolt_b200.h"
 #include "launch.h"
@@ -93,15 +96,27 @@ struct BoltCtx {
     int* dflag;
     int* herr;              // device error word: pinned, mapped (host view)
     int* derr;              // (device view)
+    double shear_q, shear_omega, time;   // shearing-box constants and strip time
+    int ghost_stale_time;   // the time changed since the ghosts of f were sheared
     long long wait_cycles;  // budget of the stage kernels' tile waits
     int stall_test;         // test hook: the stage kernels issue no tile copies
     int sticky;
     long long launches;
-    long long pair_launches;    // of which the paired FP32 stage kernel
+    long long pair_launches;    // of which the paired stage kernel
     size_t scratch_bytes;
     TmapEntry tmaps[kTmapSlots];
     int ntmaps, next_tmap;
-    int pair_enabled;       // paired FP32 kernel allowed (BOLT_NO_PAIR unset)
+    // per-component device timing (bolt_set_timing): event pairs of launch
+    // groups not yet read back, recycled events, accumulated milliseconds
+    struct Timed {
+        int cat;
+        cudaEvent_t e0, e1;
+    };
+    std::vector<Timed>* timed;
+    std::vector<cudaEvent_t>* free_events;
+    double timing_ms[BOLT_TIMING_COUNT];
+    int timing_on, timing_depth;
+    int pair_enabled;       // paired kernel allowed (BOLT_NO_PAIR unset)
     int pair_shape_ok;      // grid/method meet the paired kernel's shape conditions
 };
 
@@ -113,6 +128,8 @@ struct BoltCtx {
             return BOLT_ERR_CUDA;                         \
         }                                                 \
     } while (0)
+
+static int drain_timing(BoltCtx* ctx);
 
 static inline int bc_dirichlet(int bc) {
     return bc == BOLT_BC_DIRICHLET || bc == BOLT_BC_MIRROR_DIRICHLET;
@@ -148,6 +165,9 @@ static const CUtensorMap* get_tmap(BoltCtx* ctx, const void* ptr, int kind) {
         box[1] = 8;
         box[2] = 8;
     }
+    // the 128-byte swizzle covers rows of at most 128 bytes: FP64 staging
+    // tiles go out as two boxes of 16 p
+    if (kind == TMAP_TILE_SWZ && ctx->elem == 8) box[0] = 16;
     cuuint32_t estr[3] = {1, 1, 1};
     CUtensorMap m;
     CUresult r = enc(&m, ctx->elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
@@ -201,7 +221,7 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
     ctx->Nq1g = g.N_q1 + 2 * g.N_ghost;
     ctx->Nq2g = g.N_q2 + 2 * g.N_ghost;
     ctx->Np = g.N_p1 * g.N_p2 * g.N_p3;
-    ctx->elem = p.dtype == BOLT_F64 ? 8 : 4;
+    ctx->elem = p.dtype == BOLT_F32 ? 4 : 8;
     ctx->fcount = (size_t)ctx->Nq1g * ctx->Nq2g * g.N_s * ctx->Np;
     for (int s = 0; s < g.N_s; ++s) {
         ctx->sg.p1_start[s] = g.p1_start[s];
@@ -230,16 +250,24 @@ int bolt_ctx_create(const BoltGrid* grid, const BoltParams* params, BoltCtx** ou
     ctx->ntab = g.N_p1 + g.N_p2 + g.N_p3;
     ctx->bgk_direct = (p.p_dim == 1 ||
                        (size_t)t.tq1 * t.tq2 * ctx->ntab * sizeof(double) > 64 * 1024) ? 1 : 0;
-    // the paired FP32 kernel's shape conditions (the per-call ones are checked at launch)
-    ctx->pair_shape_ok = ctx->elem == 4 &&
+    // the paired kernel's shape conditions (the per-call ones are checked at
+    // launch): FP32, or FP64 in its throughput form
+    ctx->pair_shape_ok = (ctx->elem == 4 || p.dtype == BOLT_F64_FAST) &&
                          ctx->tiling == TILING_2D && !(ctx->bgk && ctx->bgk_direct) &&
                          g.N_q1 % 8 == 0 && g.N_q2 % 8 == 0 && ctx->Np % PW == 0 &&
                          g.N_p1 % 8 == 0 && 2 * g.N_ghost <= g.N_q1 &&
                          2 * g.N_ghost <= g.N_q2 && ctx->fcount < (1ull << 31);
+    if (ctx->pair_shape_ok) {
+        // its shared memory (exp tables grow with N_p1 + N_p2 + N_p3) must fit a CTA
+        int dev = 0, optin = 232448;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (qpair_smem(ctx->ntab, ctx->bgk, ctx->elem) > (size_t)optin) ctx->pair_shape_ok = 0;
+    }
     // p-splits: the grid is (q-tiles, species x splits)
     {
         const size_t smem_est = ctx->pair_shape_ok
-            ? qpair_smem(ctx->ntab, ctx->bgk)
+            ? qpair_smem(ctx->ntab, ctx->bgk, ctx->elem)
             : qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct, ctx->ntab);
         const int nchunks = (ctx->Np + PW - 1) / PW;
         const long long base_ctas = (long long)ctx->ntiles1 * ctx->ntiles2 * g.N_s;
@@ -332,6 +360,17 @@ void bolt_ctx_destroy(BoltCtx* ctx) {
     cudaFree(ctx->es_e);
     poisson_plans_destroy(ctx->es_fwd, ctx->es_inv);
     if (ctx->hflag) cudaFreeHost(ctx->hflag);
+    if (ctx->timed) {
+        for (auto& t : *ctx->timed) {
+            cudaEventDestroy(t.e0);
+            cudaEventDestroy(t.e1);
+        }
+        delete ctx->timed;
+    }
+    if (ctx->free_events) {
+        for (cudaEvent_t e : *ctx->free_events) cudaEventDestroy(e);
+        delete ctx->free_events;
+    }
     delete ctx;
 }
 
@@ -453,6 +492,28 @@ int bolt_set_wait_budget(BoltCtx* ctx, long long cycles) {
     return BOLT_OK;
 }
 
+int bolt_set_timing(BoltCtx* ctx, int on) {
+    if (!ctx) return BOLT_ERR_ARG;
+    if (on && !ctx->timed) {
+        ctx->timed = new (std::nothrow) std::vector<BoltCtx::Timed>();
+        ctx->free_events = new (std::nothrow) std::vector<cudaEvent_t>();
+        if (!ctx->timed || !ctx->free_events) return BOLT_ERR_NOMEM;
+    }
+    ctx->timing_on = on ? 1 : 0;
+    ctx->timing_depth = 0;
+    return BOLT_OK;
+}
+
+int bolt_timings(BoltCtx* ctx, double* ms_out) {
+    if (!ctx || !ms_out) return BOLT_ERR_ARG;
+    const int rc = drain_timing(ctx);
+    for (int i = 0; i < BOLT_TIMING_COUNT; ++i) {
+        ms_out[i] = ctx->timing_ms[i];
+        ctx->timing_ms[i] = 0.0;
+    }
+    return rc;
+}
+
 int bolt_test_stall_waits(BoltCtx* ctx, int on) {
     if (!ctx) return BOLT_ERR_ARG;
     ctx->stall_test = on ? 1 : 0;
@@ -464,13 +525,90 @@ int bolt_test_stall_waits(BoltCtx* ctx, int on) {
 // ---------------------------------------------------------------------------
 // internal launch helpers
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// per-component timing: a TimedScope brackets one launch group with CUDA
+// events (outermost scope only) and names it for NVTX-based profilers
+// ---------------------------------------------------------------------------
+static cudaEvent_t timing_event(BoltCtx* ctx) {
+    if (!ctx->free_events->empty()) {
+        cudaEvent_t e = ctx->free_events->back();
+        ctx->free_events->pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// read back every recorded pair (synchronising on the last one)
+static int drain_timing(BoltCtx* ctx) {
+    if (!ctx->timed) return BOLT_OK;
+    int rc = BOLT_OK;
+    for (auto& t : *ctx->timed) {
+        float ms = 0.0f;
+        if (cudaEventSynchronize(t.e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, t.e0, t.e1) != cudaSuccess)
+            rc = BOLT_ERR_CUDA;
+        else
+            ctx->timing_ms[t.cat] += ms;
+        ctx->free_events->push_back(t.e0);
+        ctx->free_events->push_back(t.e1);
+    }
+    ctx->timed->clear();
+    return rc;
+}
+
+static const char* const kTimingNames[BOLT_TIMING_COUNT] = {
+    "bolt: ghosts", "bolt: moments", "bolt: q-stage", "bolt: p-stage", "bolt: fields"};
+
+struct TimedScope {
+    BoltCtx* ctx;
+    cudaStream_t st;
+    int cat;
+    bool rec;
+    cudaEvent_t e0;
+    TimedScope(BoltCtx* c, int category, cudaStream_t s) : ctx(c), st(s), cat(category) {
+        nvtxRangePushA(kTimingNames[cat]);
+        rec = ctx->timing_on && ctx->timing_depth++ == 0;
+        if (rec) {
+            e0 = timing_event(ctx);
+            cudaEventRecord(e0, st);
+        }
+    }
+    ~TimedScope() {
+        if (ctx->timing_on) --ctx->timing_depth;
+        if (rec) {
+            cudaEvent_t e1 = timing_event(ctx);
+            cudaEventRecord(e1, st);
+            ctx->timed->push_back({cat, e0, e1});
+            if (ctx->timed->size() >= 4096) drain_timing(ctx);   // bounded event use
+        }
+        nvtxRangePop();
+    }
+};
+
 static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
+    TimedScope ts(ctx, BOLT_TIMING_GHOSTS, st);
     const BoltGrid& g = ctx->g;
     const int dir1 = bc_dirichlet(ctx->p.bc_q1), dir2 = bc_dirichlet(ctx->p.bc_q2);
     const int mir1 = bc_mirror(ctx->p.bc_q1), mir2 = bc_mirror(ctx->p.bc_q2);
     const int ext1 = ctx->p.bc_q1 == BOLT_BC_EXTERNAL, ext2 = ctx->p.bc_q2 == BOLT_BC_EXTERNAL;
     const int per1 = ctx->p.bc_q1 == BOLT_BC_PERIODIC, per2 = ctx->p.bc_q2 == BOLT_BC_PERIODIC;
     if (g.N_ghost == 0) return BOLT_OK;
+    GhostShear sh;
+    memset(&sh, 0, sizeof(sh));
+    if (ctx->p.bc_q1 == BOLT_BC_SHEARING_BOX || ctx->p.bc_q2 == BOLT_BC_SHEARING_BOX) {
+        // boundaries.py:19-22: shift q omega L t along the other axis, L the
+        // length of the strip's own axis, reduced modulo the other's length
+        const bool a1 = ctx->p.bc_q1 == BOLT_BC_SHEARING_BOX;
+        const double L_own = a1 ? g.N_q1 * g.dq1 : g.N_q2 * g.dq2;
+        sh.axis = a1 ? 1 : 2;
+        sh.start = a1 ? g.q2_start : g.q1_start;
+        sh.dq = a1 ? g.dq2 : g.dq1;
+        sh.end = sh.start + (a1 ? g.N_q2 : g.N_q1) * sh.dq;
+        sh.shift = fmod(ctx->shear_q * ctx->shear_omega * L_own * ctx->time, sh.end - sh.start);
+        if (!(sh.shift == sh.shift)) sh.shift = 0.0;          // a non-finite time
+    }
     if ((dir1 && (!ctx->dirichlet[0] || !ctx->dirichlet[1])) ||
         (dir2 && (!ctx->dirichlet[2] || !ctx->dirichlet[3])))
         return BOLT_ERR_ARG;
@@ -478,17 +616,20 @@ static int launch_ghosts(BoltCtx* ctx, void* f, cudaStream_t st) {
     if (ctx->elem == 8)
         e = launch_ghost_f64(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
                              ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
-                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, ctx->sg, st);
+                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, ctx->sg,
+                             sh, st);
     else
         e = launch_ghost_f32(f, ctx->dirichlet[0], ctx->dirichlet[1], ctx->dirichlet[2],
                              ctx->dirichlet[3], g.N_q1, g.N_q2, g.N_ghost, g.N_s, ctx->Np,
-                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, ctx->sg, st);
+                             g.N_p1, g.N_p2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, ctx->sg,
+                             sh, st);
     ctx->launches++;
     CK(e);
     return BOLT_OK;
 }
 
 static int launch_moments5(BoltCtx* ctx, const void* f, double* part, cudaStream_t st) {
+    TimedScope ts(ctx, BOLT_TIMING_MOMENTS, st);
     const BoltGrid& g = ctx->g;
     cudaError_t e = ctx->elem == 8
         ? launch_moments5_f64(f, part, g.N_s, g.N_p1, g.N_p2, g.N_p3, g.N_q1, g.N_q2, g.N_ghost,
@@ -521,6 +662,7 @@ struct StageIO {
 // q-part of one stage.  write_k: out1 <- k_q (no moments, no ghosts).
 static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_j,
                          cudaStream_t st) {
+    TimedScope ts(ctx, BOLT_TIMING_QSTAGE, st);
     const BoltGrid& g = ctx->g;
     QStageArgs a;
     memset(&a, 0, sizeof(a));
@@ -571,7 +713,7 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     a.full_chunks = (ctx->Np % PW) == 0;
     a.sg = ctx->sg;
     dim3 grid(ctx->ntiles1 * ctx->ntiles2, g.N_s * ctx->nsplit);
-    // the paired FP32 kernel covers the fused WENO5 2-D stage with every
+    // the paired kernel (FP32, or FP64 throughput form) covers the fused 2-D stage with every
     // buffer reachable by TMA; everything else (FP64, other reconstructions,
     // 1-D tilings, write-k mode, currents, tau arrays) runs the scalar kernel
     // (so do the write-k stages of field-coupled steps, unless they also
@@ -603,11 +745,12 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
             if ((m = get_tmap(ctx, a.out2, TMAP_TILE))) a.tm_o2 = *m; else pair = false;
         }
     }
-    const size_t smem = pair ? qpair_smem(ctx->ntab, ctx->bgk)
+    const size_t smem = pair ? qpair_smem(ctx->ntab, ctx->bgk, ctx->elem)
                              : qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct,
                                            ctx->ntab);
     cudaError_t e = ctx->elem == 8
-        ? launch_qstage_f64(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st)
+        ? (pair ? launch_qpair_f64(a, ctx->bgk, ctx->recon_q, grid, smem, st)
+                : launch_qstage_f64(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st))
         : (pair ? launch_qpair_f32(a, ctx->bgk, ctx->recon_q, grid, smem, st)
                 : launch_qstage_f32(a, ctx->recon_q, ctx->tiling, ctx->bgk, grid, smem, st));
     ctx->launches++;
@@ -616,7 +759,9 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     return BOLT_OK;
 }
 
-static int launch_pstage(BoltCtx* ctx, const StageIO& io, const void* kq, cudaStream_t st) {
+static int launch_pstage(BoltCtx* ctx, const StageIO& io, const void* kq, cudaStream_t st,
+                         int term = 0) {
+    TimedScope ts(ctx, BOLT_TIMING_PSTAGE, st);
     const BoltGrid& g = ctx->g;
     PStageArgs a;
     memset(&a, 0, sizeof(a));
@@ -636,6 +781,12 @@ static int launch_pstage(BoltCtx* ctx, const StageIO& io, const void* kq, cudaSt
     a.Nq1g = ctx->Nq1g; a.Nq2g = ctx->Nq2g;
     a.periodic1 = io.base1 != nullptr && ctx->p.bc_q1 == BOLT_BC_PERIODIC && g.N_ghost > 0;
     a.periodic2 = io.base1 != nullptr && ctx->p.bc_q2 == BOLT_BC_PERIODIC && g.N_ghost > 0;
+    a.term = term;
+    if (term) {
+        a.periodic1 = a.periodic2 = 0;
+        a.mom_out = nullptr;
+        a.flag = nullptr;
+    }
     a.sg = ctx->sg;
     const size_t smem = pstage_smem(ctx->Np, ctx->elem, g.N_p1 + g.N_p2 + g.N_p3);
     if (smem > 200 * 1024) return BOLT_ERR_UNSUPPORTED;
@@ -649,6 +800,7 @@ static int launch_pstage(BoltCtx* ctx, const StageIO& io, const void* kq, cudaSt
 
 static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st,
                          const double* j_given = nullptr) {
+    TimedScope ts(ctx, BOLT_TIMING_FIELDS, st);
     const BoltGrid& g = ctx->g;
     FieldArgs a;
     memset(&a, 0, sizeof(a));
@@ -677,6 +829,7 @@ static int electrostatic(const BoltCtx* ctx) {
 // electrostatic fields of the df/dt argument f (df_dt_fvm.py:234-242): its
 // species densities, then the FFT Poisson solve into the cell-centred E1, E2
 static int launch_electrostatic(BoltCtx* ctx, const void* f, cudaStream_t st) {
+    TimedScope ts(ctx, BOLT_TIMING_FIELDS, st);
     const BoltGrid& g = ctx->g;
     int rc = launch_moments5(ctx, f, ctx->es_part, st);
     if (rc) return rc;
@@ -725,7 +878,13 @@ static int ensure_state(BoltCtx* ctx, void* f, cudaStream_t st) {
         if (rc) return rc;
         ctx->ghost_owner = f;
         ctx->mom_owner = nullptr;
+    } else if (ctx->ghost_stale_time) {
+        // shearing-box strips of the new time (the interior, and so the
+        // moments, are unchanged)
+        rc = launch_ghosts(ctx, f, st);
+        if (rc) return rc;
     }
+    ctx->ghost_stale_time = 0;
     if (ctx->bgk && ctx->mom_owner != f) {
         rc = launch_moments5(ctx, f, ctx->momP[ctx->cur_mom], st);
         if (rc) return rc;
@@ -747,7 +906,17 @@ static void* stage_input(BoltCtx* ctx, void* f, int k) {
     return k == 2 ? ctx->buf[1] : ctx->buf[0];
 }
 
+static const char* const kStageNames[4] = {"bolt: RK stage 1", "bolt: RK stage 2",
+                                           "bolt: RK stage 3", "bolt: RK stage 4"};
+
+// one NVTX range per RK stage (pushed and popped around run_rk_stage)
+struct StageRange {
+    explicit StageRange(int k) { nvtxRangePushA(kStageNames[k & 3]); }
+    ~StageRange() { nvtxRangePop(); }
+};
+
 static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st) {
+    StageRange range(k);
     int rc = BOLT_OK;
     if (k == 0) {
         rc = ensure_state(ctx, f, st);
@@ -850,6 +1019,24 @@ int bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream) {
     if (rc) return rc;
     ctx->ghost_owner = f_dev;
     ctx->mom_owner = nullptr;
+    ctx->ghost_stale_time = 0;
+    return BOLT_OK;
+}
+
+int bolt_set_shear(BoltCtx* ctx, double q, double omega) {
+    if (!ctx) return BOLT_ERR_ARG;
+    ctx->shear_q = q;
+    ctx->shear_omega = omega;
+    ctx->ghost_stale_time = 1;
+    return BOLT_OK;
+}
+
+int bolt_set_time(BoltCtx* ctx, double t) {
+    if (!ctx) return BOLT_ERR_ARG;
+    const bool shearing = ctx->p.bc_q1 == BOLT_BC_SHEARING_BOX ||
+                          ctx->p.bc_q2 == BOLT_BC_SHEARING_BOX;
+    if (shearing && t != ctx->time) ctx->ghost_stale_time = 1;
+    ctx->time = t;
     return BOLT_OK;
 }
 
@@ -886,10 +1073,28 @@ int bolt_run(BoltCtx* ctx, void* f_dev, double dt, int n_steps, void* stream) {
     return BOLT_OK;
 }
 
+static int dfdt_impl(BoltCtx* ctx, const void* f_dev, void* dfdt_dev, int evolve_fields,
+                     double dt, int term, cudaStream_t st);
+
 int bolt_dfdt(BoltCtx* ctx, const void* f_dev, void* dfdt_dev, int evolve_fields, double dt,
               void* stream) {
     if (!ctx || !f_dev || !dfdt_dev) return BOLT_ERR_ARG;
-    cudaStream_t st = (cudaStream_t)stream;
+    return dfdt_impl(ctx, f_dev, dfdt_dev, evolve_fields, dt, 0, (cudaStream_t)stream);
+}
+
+int bolt_dfdt_term(BoltCtx* ctx, const void* f_dev, void* out_dev, int term, int evolve_fields,
+                   double dt, void* stream) {
+    if (!ctx || !f_dev || !out_dev || term < 1 || term > 3) return BOLT_ERR_ARG;
+    if (!ctx->p.fields_enabled) return BOLT_ERR_UNSUPPORTED;
+    return dfdt_impl(ctx, f_dev, out_dev, evolve_fields, dt, term, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// df/dt of f (term 0) or, with fields, one p-flux divergence (term 1..3)
+// after the same field evaluation df_dt_fvm performs
+static int dfdt_impl(BoltCtx* ctx, const void* f_dev, void* dfdt_dev, int evolve_fields,
+                     double dt, int term, cudaStream_t st) {
     int rc = BOLT_OK;
     double* m = ctx->momP[ctx->cur_mom ^ 1];
     if (ctx->bgk) rc = launch_moments5(ctx, f_dev, m, st);
@@ -914,10 +1119,12 @@ int bolt_dfdt(BoltCtx* ctx, const void* f_dev, void* dfdt_dev, int evolve_fields
     if (!rc && evolve_fields) rc = launch_fields(ctx, dt, ctx->nsplit, st);
     if (!rc) {
         io.out1 = dfdt_dev;
-        rc = launch_pstage(ctx, io, ctx->kbuf, st);
+        rc = launch_pstage(ctx, io, ctx->kbuf, st, term);
     }
     return rc;
 }
+
+extern "C" {
 
 int bolt_moments(BoltCtx* ctx, const void* f_dev, int moment_id, double* out_dev,
                  void* stream) {

@@ -112,7 +112,7 @@ extern "C" int bolt_dfdt_noalloc(const BoltGrid* grid, const BoltParams* params,
 
     const int Np = g.N_p1 * g.N_p2 * g.N_p3;
     const int Nq1g = g.N_q1 + 2 * g.N_ghost, Nq2g = g.N_q2 + 2 * g.N_ghost;
-    const size_t elem = p.dtype == BOLT_F64 ? 8 : 4;
+    const size_t elem = p.dtype == BOLT_F32 ? 4 : 8;
     SpeciesGrid sg;
     memset(&sg, 0, sizeof(sg));
     for (int s = 0; s < g.N_s; ++s) {

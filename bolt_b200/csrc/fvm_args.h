@@ -62,33 +62,45 @@ __host__ __device__ inline QLayout qstage_layout(int tq1, int tq2, int q2, int e
     return qstage_layout_n(tq1, tq2, q2, elem, bgk, bgk_direct, ntab, 1);
 }
 
-// Shared-memory carve-up of the paired FP32 kernel (8x8 q-tile), offsets from
-// a 1024-byte aligned base (the 128-byte swizzled output tile needs it; the
-// kernel aligns the dynamic base itself, hence the 1 KB of slack in total).
+// Shared-memory carve-up of the paired kernel (8x8 q-tile, FP32 or FP64
+// elements of `elem` bytes), offsets from a 1024-byte aligned base (the
+// 128-byte swizzled output tile needs it; the kernel aligns the dynamic base
+// itself, hence the 1 KB of slack in total).  FP32: 111.8 KB (two CTAs per
+// SM); FP64: 216.7 KB (one).
 struct PLayout {
     unsigned x, o1, o2, b1, d1, tabs, vgrid, bars, total;
 };
 
-constexpr unsigned kPairTile = 8 * 8 * PW * 4;                       // 8 KB
-constexpr unsigned kPairHalo = (8 + 2 * HALO) * (8 + 2 * HALO) * PW * 4;  // 24.5 KB
+constexpr unsigned kPairTileElems = 8 * 8 * PW;                        // one 8x8 tile
+constexpr unsigned kPairHaloElems = (8 + 2 * HALO) * (8 + 2 * HALO) * PW;  // 14x14 halo tile
 constexpr unsigned kTabPitch = 33;       // exp-table row: 32 q-cell pairs + 1 pad
 
-__host__ __device__ inline PLayout qpair_layout(int ntab, int bgk) {
+__host__ __device__ inline PLayout qpair_layout(int ntab, int bgk, unsigned elem) {
     PLayout L;
     unsigned o = 0;
-    L.x = o;  o += 2 * kPairHalo;                 // double-buffered halo tile
+    const unsigned tile = kPairTileElems * elem;
+    L.x = o;  o += 2 * kPairHaloElems * elem;     // double-buffered halo tile
     o = qalign(o, 1024);
-    L.o1 = o; o += kPairTile;                     // out1 staging (128B swizzle)
-    L.o2 = o; o += kPairTile;                     // out2 staging
-    L.b1 = o; o += 2 * kPairTile;                 // base1 tile, double-buffered
-    L.d1 = o; o += kPairTile;                     // q1 part of df/dt (prologue: Maxwellian
+    L.o1 = o; o += tile;                          // out1 staging (128B swizzle)
+    L.o2 = o; o += tile;                          // out2 staging
+    L.b1 = o; o += 2 * tile;                      // base1 tile, double-buffered
+    L.d1 = o; o += tile;                          // q1 part of df/dt (prologue: Maxwellian
                                                   // parameters of the 64 q-cells)
-    L.tabs = o; o += bgk ? kTabPitch * ntab * 8u : 0u;  // exp tables, float2 per q-cell pair
+    L.tabs = o; o += bgk ? kTabPitch * ntab * 2 * elem : 0u;  // exp tables, a pair per q-cell pair
     L.vgrid = o; o += ntab * sizeof(double);
     L.bars = qalign(o, 8); o = L.bars + 4 * sizeof(unsigned long long);
     L.total = o + 1024;
     return L;
 }
+
+// Shearing-box ghost strips (boundaries.py:6-145): axis 1 (q1 strips,
+// resampled along q2) or axis 2 (q2 strips, resampled along q1), with the
+// shift already reduced modulo the resampled axis's length
+struct GhostShear {
+    int axis;                   // 0: none, 1: q1 strips, 2: q2 strips
+    double shift;               // q omega L t mod L_other (>= 0 or < 0)
+    double start, end, dq;      // the resampled axis: domain and spacing
+};
 
 struct SpeciesGrid {
     double p1_start[kMaxSpecies], p2_start[kMaxSpecies], p3_start[kMaxSpecies];
@@ -150,6 +162,7 @@ struct PStageArgs {
     double c1, c2;
     int Nq1, Nq2, Ng, Ns, Np1, Np2, Np3, Np, Nq1g, Nq2g;
     int periodic1, periodic2;
+    int term;              // 0: the stage combine; 1..3: out1 <- d_flux_pk_dpk alone
     SpeciesGrid sg;
 };
 

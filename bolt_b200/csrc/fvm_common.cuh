@@ -281,11 +281,13 @@ struct FaceWalker {
 };
 
 // ---------------------------------------------------------------------------
-// Paired FP32 (two q-cells per thread, same p) WENO5 walker, using the
-// sm_100 f32x2 arithmetic.  Both components share the lane's upwind side, so
-// they share the coefficient set.  Smoothness indicators use a constant
-// 1e-17 floor (the reference's 1e-17*(1+|a|+|b|+|c|) differs from it only
-// where f varies by less than FP32 resolves).
+// Paired WENO5 walker: two q-cells per thread at the same p.  FP32 pairs use
+// the sm_100 f32x2 arithmetic; FP64 pairs are two scalar FP64 operations with
+// FMA and a Newton-refined reciprocal.  Both components share the lane's
+// upwind side, so they share the coefficient set.  Smoothness indicators use
+// a constant 1e-17 floor (the reference's 1e-17*(1+|a|+|b|+|c|) differs from
+// it only where f is flat to 1e-17: there every weight takes the floor and
+// the substencil values coincide, so the face value does not depend on it).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
@@ -293,6 +295,48 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
 __device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(fast_rcp(a.x), fast_rcp(a.y)); }
+
+// 1/x in FP64 for finite normal x: the hardware approximation refined by two
+// Newton-Raphson steps for f(r) = 1/r - x, r <- r + r (1 - x r); each step
+// doubles the number of correct bits, the last one lands within an ulp
+__device__ __forceinline__ double rcp_nr(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
+__device__ __forceinline__ double2 f2(double a) { return make_double2(a, a); }
+__device__ __forceinline__ double2 fma2(double2 a, double2 b, double2 c) {
+    return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+__device__ __forceinline__ double2 mul2(double2 a, double2 b) {
+    return make_double2(a.x * b.x, a.y * b.y);
+}
+__device__ __forceinline__ double2 add2(double2 a, double2 b) {
+    return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 sub2(double2 a, double2 b) {
+    return make_double2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ double2 rcp2(double2 a) { return make_double2(rcp_nr(a.x), rcp_nr(a.y)); }
+
+// element type -> pair type and the walker's constants in that type
+template <typename E> struct PairOf;
+template <> struct PairOf<float> {
+    typedef float2 P;
+    __device__ static constexpr float c(float f, double) { return f; }
+};
+template <> struct PairOf<double> {
+    typedef double2 P;
+    __device__ static constexpr double c(float, double d) { return d; }
+};
+// a constant in the element type: the float literal for FP32 (the exact
+// value the FP32 path has always used), the double literal for FP64
+#define BOLT_K(E, v) (PairOf<E>::c(float(v##f), double(v)))
+#define BOLT_KQ(E, n, d) (PairOf<E>::c(float(n##.0f / d##.0f), double(n##.0 / d##.0)))
 
 // Per-lane coefficients of the upwind side.  With D2_k the second difference
 // of substencil k and the third differences D3a = y0 - 3y1 + 3y2 - y3 =
@@ -304,64 +348,70 @@ __device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(fast_rcp(a
 // (5, 10, 1)/16 (left), the walker returns TWICE the face value as
 //   (y2 + ys - D2_2/4) + (q3 D3b + r q1 D3a) / (a1 q1 + a2 q2 + a3 q3),
 // r = (w1 k1)/(w3 k3) and a_k = w_k / (2 w3 k3); callers halve the flux factor.
-struct Weno5Pair {
-    float2 r, a1, a2, a3;
+template <typename E>
+struct Weno5PairT {
+    typedef typename PairOf<E>::P P;
+    P r, a1, a2, a3;
     bool right;
     __device__ __forceinline__ void set(bool rt) {
         right = rt;
-        r = f2(rt ? 0.6f : 5.0f / 3.0f);
-        a1 = f2(rt ? 0.8f : -20.0f / 3.0f);
-        a2 = f2(rt ? 8.0f : -40.0f / 3.0f);
-        a3 = f2(rt ? 4.0f : -4.0f / 3.0f);
+        r = f2(rt ? BOLT_K(E, 0.6) : BOLT_KQ(E, 5, 3));
+        a1 = f2(rt ? BOLT_K(E, 0.8) : BOLT_KQ(E, -20, 3));
+        a2 = f2(rt ? BOLT_K(E, 8.0) : BOLT_KQ(E, -40, 3));
+        a3 = f2(rt ? BOLT_K(E, 4.0) : BOLT_KQ(E, -4, 3));
     }
 };
 
 // smoothness indicator of substencil (a, b, c) given its second difference
 // D2 = a - 2b + c: 13/12 D2^2 + 1/4 (a - 4b + 3c)^2 + 1e-17, where
 // (a - 4b + 3c)/2 = D2/2 + (c - b)
-__device__ __forceinline__ float2 beta_pair(float2 D2, float2 b, float2 c) {
-    const float2 e = fma2(f2(0.5f), D2, sub2(c, b));
-    return fma2(mul2(f2(13.0f / 12.0f), D2), D2, fma2(e, e, f2(1e-17f)));
+template <typename P>
+__device__ __forceinline__ P beta_pair(P D2, P b, P c) {
+    typedef decltype(D2.x) E;
+    const P e = fma2(f2(BOLT_K(E, 0.5)), D2, sub2(c, b));
+    return fma2(mul2(f2(BOLT_KQ(E, 13, 12)), D2), D2, fma2(e, e, f2(BOLT_K(E, 1e-17))));
 }
 
-__device__ __forceinline__ float2 second_diff(float2 a, float2 b, float2 c) {
-    return fma2(f2(-2.0f), b, add2(a, c));
+template <typename P>
+__device__ __forceinline__ P second_diff(P a, P b, P c) {
+    typedef decltype(a.x) E;
+    return fma2(f2(BOLT_K(E, -2.0)), b, add2(a, c));
 }
 
 // Sliding walker: carries 1/beta^2 of substencils 2 and 3, the second
 // difference of substencil 3 and the third difference D3b of the last face.
-struct Weno5PairWalker {
-    float2 q2, q3, d23, d3b;
-    __device__ __forceinline__ static float2 inv_sq(float2 b) {
-        const float2 r = rcp2(b);
+template <typename E>
+struct Weno5PairWalkerT {
+    typedef typename PairOf<E>::P P;
+    P q2, q3, d23, d3b;
+    __device__ __forceinline__ static P inv_sq(P b) {
+        const P r = rcp2(b);
         return mul2(r, r);
     }
-    __device__ __forceinline__ float2 eval(float2 q1, float2 d3a, float2 d22, float2 y1, float2 y2,
-                                           float2 y3, const Weno5Pair& S) const {
-        const float2 ys = S.right ? y3 : y1;
-        const float2 base = fma2(f2(-0.25f), d22, add2(y2, ys));
-        const float2 num = fma2(q3, d3b, mul2(mul2(S.r, q1), d3a));
-        const float2 den = fma2(S.a3, q3, fma2(S.a2, q2, mul2(S.a1, q1)));
+    __device__ __forceinline__ P eval(P q1, P d3a, P d22, P y1, P y2, P y3,
+                                      const Weno5PairT<E>& S) const {
+        const P ys = S.right ? y3 : y1;
+        const P base = fma2(f2(BOLT_K(E, -0.25)), d22, add2(y2, ys));
+        const P num = fma2(q3, d3b, mul2(mul2(S.r, q1), d3a));
+        const P den = fma2(S.a3, q3, fma2(S.a2, q2, mul2(S.a1, q1)));
         return fma2(num, rcp2(den), base);
     }
-    __device__ __forceinline__ float2 first(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
-                                            const Weno5Pair& S) {
-        const float2 d21 = second_diff(y0, y1, y2);
-        const float2 d22 = second_diff(y1, y2, y3);
+    __device__ __forceinline__ P first(P y0, P y1, P y2, P y3, P y4, const Weno5PairT<E>& S) {
+        const P d21 = second_diff(y0, y1, y2);
+        const P d22 = second_diff(y1, y2, y3);
         d23 = second_diff(y2, y3, y4);
-        const float2 q1 = inv_sq(beta_pair(d21, y1, y2));
+        const P q1 = inv_sq(beta_pair(d21, y1, y2));
         q2 = inv_sq(beta_pair(d22, y2, y3));
         q3 = inv_sq(beta_pair(d23, y3, y4));
-        const float2 d3a = sub2(d21, d22);
+        const P d3a = sub2(d21, d22);
         d3b = sub2(d22, d23);
         return eval(q1, d3a, d22, y1, y2, y3, S);
     }
     // window advanced by one cell: y0..y4 are the new window's values
-    __device__ __forceinline__ float2 next(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
-                                           const Weno5Pair& S) {
-        const float2 q1 = q2;
-        const float2 d3a = d3b;
-        const float2 d22 = d23;
+    __device__ __forceinline__ P next(P y0, P y1, P y2, P y3, P y4, const Weno5PairT<E>& S) {
+        const P q1 = q2;
+        const P d3a = d3b;
+        const P d22 = d23;
         q2 = q3;
         d23 = second_diff(y2, y3, y4);
         q3 = inv_sq(beta_pair(d23, y3, y4));
@@ -370,47 +420,51 @@ struct Weno5PairWalker {
     }
 };
 
-// Minmod faces for the paired kernel, same interface as Weno5PairWalker:
+// Minmod faces for the paired kernel, same interface as Weno5PairWalkerT:
 // twice the face value of the window's centre cell y2 (its right face for
 // right-moving lanes, its left face otherwise), 2 y2 +- the limited slope of
 // (y1, y2, y3) (minmod.py:4-71).  No state is carried between faces.
-struct MinmodPairWalker {
-    __device__ __forceinline__ static float2 face(float2 y1, float2 y2, float2 y3, bool right) {
-        float2 sl = make_float2(minmod_slope(y1.x, y2.x, y3.x), minmod_slope(y1.y, y2.y, y3.y));
-        if (!right) sl = make_float2(-sl.x, -sl.y);
-        return fma2(f2(2.0f), y2, sl);
+template <typename E>
+struct MinmodPairWalkerT {
+    typedef typename PairOf<E>::P P;
+    __device__ __forceinline__ static P face(P y1, P y2, P y3, bool right) {
+        P sl;
+        sl.x = minmod_slope(y1.x, y2.x, y3.x);
+        sl.y = minmod_slope(y1.y, y2.y, y3.y);
+        if (!right) { sl.x = -sl.x; sl.y = -sl.y; }
+        return fma2(f2(BOLT_K(E, 2.0)), y2, sl);
     }
-    __device__ __forceinline__ float2 first(float2, float2 y1, float2 y2, float2 y3, float2,
-                                            const Weno5Pair& S) {
+    __device__ __forceinline__ P first(P, P y1, P y2, P y3, P, const Weno5PairT<E>& S) {
         return face(y1, y2, y3, S.right);
     }
-    __device__ __forceinline__ float2 next(float2, float2 y1, float2 y2, float2 y3, float2,
-                                           const Weno5Pair& S) {
+    __device__ __forceinline__ P next(P, P y1, P y2, P y3, P, const Weno5PairT<E>& S) {
         return face(y1, y2, y3, S.right);
     }
 };
 
 // PPM (ppm.py:4-100) and piecewise-constant faces for the paired kernel:
 // twice the face value of the window's centre cell y2, per element
-struct PpmPairWalker {
-    __device__ __forceinline__ float2 first(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
-                                            const Weno5Pair& S) {
+template <typename E>
+struct PpmPairWalkerT {
+    typedef typename PairOf<E>::P P;
+    __device__ __forceinline__ P first(P y0, P y1, P y2, P y3, P y4, const Weno5PairT<E>& S) {
         return next(y0, y1, y2, y3, y4, S);
     }
-    __device__ __forceinline__ float2 next(float2 y0, float2 y1, float2 y2, float2 y3, float2 y4,
-                                           const Weno5Pair& S) {
-        return make_float2(2.0f * ppm_face(y0.x, y1.x, y2.x, y3.x, y4.x, S.right),
-                           2.0f * ppm_face(y0.y, y1.y, y2.y, y3.y, y4.y, S.right));
+    __device__ __forceinline__ P next(P y0, P y1, P y2, P y3, P y4, const Weno5PairT<E>& S) {
+        P o;
+        o.x = E(2) * ppm_face(y0.x, y1.x, y2.x, y3.x, y4.x, S.right);
+        o.y = E(2) * ppm_face(y0.y, y1.y, y2.y, y3.y, y4.y, S.right);
+        return o;
     }
 };
 
-struct ConstPairWalker {
-    __device__ __forceinline__ float2 first(float2, float2, float2 y2, float2, float2,
-                                            const Weno5Pair&) {
+template <typename E>
+struct ConstPairWalkerT {
+    typedef typename PairOf<E>::P P;
+    __device__ __forceinline__ P first(P, P, P y2, P, P, const Weno5PairT<E>&) {
         return add2(y2, y2);
     }
-    __device__ __forceinline__ float2 next(float2, float2, float2 y2, float2, float2,
-                                           const Weno5Pair&) {
+    __device__ __forceinline__ P next(P, P, P y2, P, P, const Weno5PairT<E>&) {
         return add2(y2, y2);
     }
 };

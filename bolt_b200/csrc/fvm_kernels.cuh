@@ -685,6 +685,11 @@ pstage_kernel(const __grid_constant__ PStageArgs a) {
             t3 = (Fx[2][cn] - Fx[2][c]) * inv3;
         }
         const long long g = cbase + c;
+        if (a.term) {
+            // one p-flux divergence (df_dt_fvm.py:325-335 term_to_return)
+            out1[g] = a.term == 1 ? t1 : (a.term == 2 ? t2 : t3);
+            continue;
+        }
         T kk = kq[g] + (-((t1 + t2) + t3));
         T o1 = base1 ? base1[g] + kk * c1 : kk;
         out1[g] = o1;
@@ -809,7 +814,8 @@ template <typename T>
 __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const T* dt,
                              int Nq1, int Nq2, int Ng, int Ns, int Np, int Np1, int Np2,
                              int per1, int per2, int dir1, int dir2, int mir1, int mir2,
-                             int ext1, int ext2, SpeciesGrid sg, long long nghost_cells) {
+                             int ext1, int ext2, SpeciesGrid sg, GhostShear sh,
+                             long long nghost_cells) {
     const int Nq1g = Nq1 + 2 * Ng;
     const long long rowstride = (long long)Ns * Np;
     const long long colstride = rowstride * Nq1g;
@@ -837,6 +843,37 @@ __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const 
         const bool in1 = i >= 0 && i < Nq1, in2 = j >= 0 && j < Nq2;
         // ghost rows / columns of an external axis belong to the caller
         if ((ext1 && !in1) || (ext2 && !in2)) continue;
+        // a shearing-box strip (every cell of the N_g ghost columns or rows,
+        // corners included): the periodic image resampled along the other axis
+        if ((sh.axis == 1 && !in1) || (sh.axis == 2 && !in2)) {
+            const bool lo = sh.axis == 1 ? i < 0 : j < 0;
+            const int N = sh.axis == 1 ? Nq2 : Nq1;           // resampled axis
+            const int own = sh.axis == 1 ? g2 : g1;           // position along it
+            double pos = (sh.start + (own - Ng) * sh.dq) + 0.5 * sh.dq;     // ghosted centre
+            pos = lo ? pos - sh.shift : pos + sh.shift;
+            const double L = sh.end - sh.start;
+            for (int it = 0; it < 4 && pos > sh.end; ++it) pos -= L;
+            for (int it = 0; it < 4 && pos < sh.start; ++it) pos += L;
+            // continuous index among the ghosted centres, then interior indices
+            const double x = (pos - ((sh.start + (-Ng) * sh.dq) + 0.5 * sh.dq)) / sh.dq;
+            const int jb = (int)floor(x);
+            const double t = x - jb;
+            const int fixed = sh.axis == 1 ? ((i % Nq1) + Nq1) % Nq1 : ((j % Nq2) + Nq2) % Nq2;
+            double pv[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int m = (((jb - 1 + k - Ng) % N) + N) % N;   // periodic extension
+                const int ci = sh.axis == 1 ? fixed : m, cj = sh.axis == 1 ? m : fixed;
+                pv[k] = double(f[(long long)(cj + Ng) * colstride + (long long)(ci + Ng) * rowstride +
+                                 (long long)s * Np + p]);
+            }
+            // Catmull-Rom cubic between pv[1] and pv[2] (tangents (pv[k+1]-pv[k-1])/2)
+            const double v = pv[1] + 0.5 * t * ((pv[2] - pv[0]) +
+                             t * ((2.0 * pv[0] - 5.0 * pv[1] + 4.0 * pv[2] - pv[3]) +
+                                  t * (3.0 * (pv[1] - pv[2]) + pv[3] - pv[0])));
+            f[(long long)g2 * colstride + (long long)g1 * rowstride + sp] = T(v);
+            continue;
+        }
         const int i1 = p % Np1, i2 = (p / Np1) % Np2;
         // source cell and p index: periodic wrap, or the mirror image across
         // the edge (ghost i < 0 <- interior -1-i, i >= N <- 2N-1-i) with the

@@ -87,7 +87,8 @@ cudaError_t BOLT_CAT(launch_ghost_, BOLT_SUFFIX)(void* f, const void* dl, const 
                                                  int Ng, int Ns, int Np, int Np1, int Np2,
                                                  int per1, int per2, int dir1, int dir2,
                                                  int mir1, int mir2, int ext1, int ext2,
-                                                 const SpeciesGrid& sg, cudaStream_t st) {
+                                                 const SpeciesGrid& sg, const GhostShear& sh,
+                                                 cudaStream_t st) {
     const long long Nq1g = Nq1 + 2 * Ng;
     const long long ncells = 2LL * Ng * Nq1g + 2LL * Ng * Nq2;
     if (ncells == 0) return cudaSuccess;
@@ -97,7 +98,7 @@ cudaError_t BOLT_CAT(launch_ghost_, BOLT_SUFFIX)(void* f, const void* dl, const 
     ghost_kernel<BOLT_T><<<(unsigned)blocks, 256, 0, st>>>(
         static_cast<BOLT_T*>(f), static_cast<const BOLT_T*>(dl), static_cast<const BOLT_T*>(dr),
         static_cast<const BOLT_T*>(db), static_cast<const BOLT_T*>(dt), Nq1, Nq2, Ng, Ns, Np, Np1,
-        Np2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, sg, ncells);
+        Np2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, sg, sh, ncells);
     return cudaGetLastError();
 }
 

@@ -29,8 +29,10 @@ inline size_t qstage_smem(int tiling, size_t elem, int bgk, int bgk_direct, int 
     return qstage_layout(t.tq1, t.tq2, t.q2, (int)elem, bgk, bgk_direct, ntab).total;
 }
 
-// bytes of dynamic shared memory of the paired FP32 kernel
-inline size_t qpair_smem(int ntab, int bgk) { return qpair_layout(ntab, bgk).total; }
+// bytes of dynamic shared memory of the paired kernel (elem: 4 FP32, 8 FP64)
+inline size_t qpair_smem(int ntab, int bgk, size_t elem) {
+    return qpair_layout(ntab, bgk, (unsigned)elem).total;
+}
 
 // p-split of the q-stage grid (q-tiles x species x splits): the split that
 // minimises (waves, rounded up) x (chunks per CTA + ~2 chunks of prologue), a
@@ -89,7 +91,7 @@ inline size_t pstage_smem(int Np, size_t elem, int ntab) {
                                       int Ng, int Ns, int Np, int Np1, int Np2, int per1,    \
                                       int per2, int dir1, int dir2, int mir1, int mir2,      \
                                       int ext1, int ext2, const SpeciesGrid& sg,             \
-                                      cudaStream_t st);
+                                      const GhostShear& sh, cudaStream_t st);
 
 // electrostatic field solve of one df/dt argument (poisson.cu)
 struct PoissonArgs {
@@ -109,8 +111,11 @@ cudaError_t launch_poisson(const PoissonArgs& a, int fwd, int inv, cudaStream_t 
 BOLT_DECLARE_LAUNCHERS(f64, double)
 BOLT_DECLARE_LAUNCHERS(f32, float)
 
-// paired FP32 WENO5 q-stage (8x8 tiling, fields off, fused combine, TMA in and out)
+// paired q-stage (8x8 tiling, fused combine, TMA in and out): FP32, and FP64
+// with FMA contraction and Newton-refined reciprocals (BOLT_F64_FAST)
 cudaError_t launch_qpair_f32(const QStageArgs& a, int bgk, int recon, dim3 grid, size_t smem,
+                             cudaStream_t st);
+cudaError_t launch_qpair_f64(const QStageArgs& a, int bgk, int recon, dim3 grid, size_t smem,
                              cudaStream_t st);
 
 // FDTD sequence (FP64): prepare -> halo -> E -> halo -> B -> to_cell

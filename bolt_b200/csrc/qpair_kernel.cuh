@@ -1,11 +1,12 @@
-// qpair_kernel.cuh - paired FP32 WENO5 q-stage kernel (sm_100a).
+// qpair_kernel.cuh - paired WENO5 q-stage kernel (sm_100a), FP32 or FP64.
 //
 // The fused RK stage of the 2D3V FVM update with fields off
 // (df_dt_fvm.py:56-97 q-part + BGK source, combined with the stage update of
 // integrators.py:15-28 / fvm_operator.py:26,33) for an 8x8 q-tile and 32
 // consecutive p-cells of one species per chunk.  Every thread walks two
-// adjacent q-rows (phase A) or q-columns (phase B) of the same p at once with
-// f32x2 arithmetic:
+// adjacent q-rows (phase A) or q-columns (phase B) of the same p at once, as
+// a pair: f32x2 arithmetic in FP32, two FMA-contracted FP64 operations with
+// Newton-refined reciprocals in FP64:
 //
 //   phase A  warp w: rows 2(w%4), 2(w%4)+1, cells 4(w/4)..+3 (5 faces each);
 //            q1 part of df/dt -> D1 tile
@@ -23,7 +24,13 @@
 // two conflict-free 16-byte loads.  Barrier waits are time-bounded and a
 // failure is made CTA-uniform, recorded in the error word, and ends the work.
 //
-// Launch conditions (checked by the host): FP32, any reconstruction in q, 8x8 tiling,
+// FP64 differences: the out1 staging tile is two 128-byte-swizzled halves of
+// 16 p each (the swizzle covers 128-byte rows), stored by two TMA stores; the
+// RK4 accumulator's increment goes out by one bulk reduce-add (.add.f64) per
+// q-cell row, issued by the lanes of warp 0; one CTA per SM (221 KB of
+// shared memory).
+//
+// Launch conditions (checked by the host): FP32 or FP64, any reconstruction in q, 8x8 tiling,
 // N_q1, N_q2 multiples of 8 and at least 2 N_g, N_p multiple of 32, N_p1
 // multiple of 8, BGK by exp tables, all five buffers 16-byte aligned, f with
 // fewer than 2^31 elements (32-bit offsets).
@@ -35,21 +42,62 @@
 
 namespace bolt {
 
-// Swizzled position of element p (0..31) of q-cell row c in a 128-byte
-// swizzled tile: 16-byte chunk index XOR (c mod 8).
-__device__ __forceinline__ int swz(int c, int p) {
-    return c * PW + ((((p >> 2) ^ (c & 7)) << 2) | (p & 3));
+// Geometry of the out1 staging tile: CS elements of one q-cell per 128-byte
+// row (32 FP32, or 16 FP64 with the 32 p split into two halves of 64 rows),
+// VE elements per 16-byte chunk; the 128-byte swizzle XORs the chunk index
+// with (q-cell mod 8).
+template <typename E> struct PairStage;
+template <> struct PairStage<float> {
+    static constexpr int CS = 32, VE = 4;
+};
+template <> struct PairStage<double> {
+    static constexpr int CS = 16, VE = 2;
+};
+
+// staging-tile index of element p (0..31) of q-cell c
+template <typename E>
+__device__ __forceinline__ int stg(int c, int p) {
+    constexpr int CS = PairStage<E>::CS, VE = PairStage<E>::VE;
+    const int h = p / CS, pp = p % CS;
+    return h * 64 * CS + c * CS + ((((pp / VE) ^ (c & 7)) * VE) | (pp % VE));
+}
+
+// the 8 consecutive elements of a q-cell row starting at 16-byte chunk ch0
+// (key = q-cell mod 8), as FP64
+__device__ __forceinline__ void load8(const float* row, int ch0, int key, double (&o)[8]) {
+    const float4 u = reinterpret_cast<const float4*>(row)[ch0 ^ key];
+    const float4 w = reinterpret_cast<const float4*>(row)[(ch0 + 1) ^ key];
+    o[0] = u.x; o[1] = u.y; o[2] = u.z; o[3] = u.w;
+    o[4] = w.x; o[5] = w.y; o[6] = w.z; o[7] = w.w;
+}
+__device__ __forceinline__ void load8(const double* row, int ch0, int key, double (&o)[8]) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double2 v = reinterpret_cast<const double2*>(row)[(ch0 + j) ^ key];
+        o[2 * j] = v.x;
+        o[2 * j + 1] = v.y;
+    }
+}
+
+__device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
+
+// shared -> global bulk reduce-add of n FP64 values (16-byte aligned, n*8 a
+// multiple of 16), bulk-group completion of the issuing thread
+__device__ __forceinline__ void bulk_reduce_add_f64(double* gdst, const double* ssrc, unsigned bytes) {
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;"
+                 ::"l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes) : "memory");
 }
 
 // Prologue: p-cell centres of the species, barriers, and for BGK the
-// Maxwellian of the stage input per q-cell with exp tables stored as float2
-// over q-cell pairs P = row*4 + j (cells 2j, 2j+1 of one tile row):
+// Maxwellian of the stage input per q-cell with exp tables stored as element
+// pairs over q-cell pairs P = row*4 + j (cells 2j, 2j+1 of one tile row):
 // tab[q*kTabPitch + P], the pitch of 33 pairs keeping a warp's reads of
 // different q (one per lane) on distinct banks.
-template <bool BGK>
+template <typename E, bool BGK>
 __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i0, int j0,
-                                               double* vgrid, double* qc, float2* tabs,
-                                               uint64_t* bars) {
+                                               double* vgrid, double* qc,
+                                               typename PairOf<E>::P* tabs, uint64_t* bars) {
     const int tid = threadIdx.x;
     const int Np1 = a.Np1, Np2 = a.Np2;
     const int ntab = Np1 + Np2 + a.Np3;
@@ -79,8 +127,8 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
         for (int e = tid; e < 32 * ntab; e += NTHREADS) {
             const int q = e >> 5, P = e & 31;
             const int c0 = (P >> 2) * 8 + 2 * (P & 3);
-            tabs[q * kTabPitch + P] = make_float2(float(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
-                                  float(bgk_table_entry(a, qc + (c0 + 1) * 5, vgrid, q, m)));
+            tabs[q * kTabPitch + P] = mk2(E(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
+                                          E(bgk_table_entry(a, qc + (c0 + 1) * 5, vgrid, q, m)));
         }
     }
     __syncthreads();
@@ -97,37 +145,42 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
 //           enabled), no base, no moments
 enum QPairMode { QP_X1 = 0, QP_X2 = 1, QP_B1 = 2, QP_B1R2 = 3, QP_K = 4 };
 
-template <bool BGK, int MODE, int RECON>
-__global__ void __launch_bounds__(NTHREADS, 2)
+template <typename E, bool BGK, int MODE, int RECON>
+__global__ void __launch_bounds__(NTHREADS, sizeof(E) == 4 ? 2 : 1)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
+    typedef typename PairOf<E>::P P;
     // WENO5 faces with the sliding walker, or minmod / PPM / piecewise-constant faces
     using Walker = typename std::conditional<
-        RECON == BOLT_RECON_MINMOD, MinmodPairWalker,
+        RECON == BOLT_RECON_MINMOD, MinmodPairWalkerT<E>,
         typename std::conditional<
-            RECON == BOLT_RECON_PPM, PpmPairWalker,
-            typename std::conditional<RECON == BOLT_RECON_PC, ConstPairWalker,
-                                      Weno5PairWalker>::type>::type>::type;
+            RECON == BOLT_RECON_PPM, PpmPairWalkerT<E>,
+            typename std::conditional<RECON == BOLT_RECON_PC, ConstPairWalkerT<E>,
+                                      Weno5PairWalkerT<E>>::type>::type>::type;
+    typedef Weno5PairT<E> Side;
+    constexpr int CS = PairStage<E>::CS, VE = PairStage<E>::VE;
+    constexpr bool F64 = sizeof(E) == 8;
     constexpr bool BX = MODE == QP_X1 || MODE == QP_X2 || MODE == QP_K;   // no base tiles
     constexpr bool KOUT = MODE == QP_K;
     constexpr bool HAS2 = MODE == QP_X2 || MODE == QP_B1R2;
     constexpr bool RED2 = MODE == QP_B1R2;
     constexpr int TQ = 8, HX = TQ + 2 * HALO, NQ = TQ * TQ, NWARP = NTHREADS / 32;
-    constexpr int XT = HX * HX * PW;                 // floats of one halo tile
+    constexpr int XT = HX * HX * PW;                 // elements of one halo tile
+    constexpr int TE = TQ * TQ * PW;                 // elements of one 8x8 tile
     constexpr int NQUART = NTHREADS / NQ;            // phase C: threads per q-cell
     static_assert(NWARP == 8 && NQUART == 4, "pair mapping assumes 8 warps");
 
     const int Np1 = a.Np1, Np2 = a.Np2, Np = a.Np, Ng = a.Ng;
     const int Nq1 = a.Nq1, Nq2 = a.Nq2;
     const int ntab = Np1 + Np2 + a.Np3;
-    const PLayout Lo = qpair_layout(ntab, BGK);
+    const PLayout Lo = qpair_layout(ntab, BGK, sizeof(E));
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* sm = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-    float* X = reinterpret_cast<float*>(sm + Lo.x);
-    float* o1s = reinterpret_cast<float*>(sm + Lo.o1);
-    float* o2s = reinterpret_cast<float*>(sm + Lo.o2);
-    float* b1s = reinterpret_cast<float*>(sm + Lo.b1);
-    float* d1s = reinterpret_cast<float*>(sm + Lo.d1);
-    float2* tabs = reinterpret_cast<float2*>(sm + Lo.tabs);
+    E* X = reinterpret_cast<E*>(sm + Lo.x);
+    E* o1s = reinterpret_cast<E*>(sm + Lo.o1);
+    E* o2s = reinterpret_cast<E*>(sm + Lo.o2);
+    E* b1s = reinterpret_cast<E*>(sm + Lo.b1);
+    E* d1s = reinterpret_cast<E*>(sm + Lo.d1);
+    P* tabs = reinterpret_cast<P*>(sm + Lo.tabs);
     double* vgrid = reinterpret_cast<double*>(sm + Lo.vgrid);
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + Lo.bars);
 
@@ -143,14 +196,14 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const bool border = ((a.periodic1 || peer1) && (i0 < Ng || i0 + TQ > Nq1 - Ng)) ||
                         ((a.periodic2 || peer2) && (j0 < Ng || j0 + TQ > Nq2 - Ng));
 
-    qpair_prologue<BGK>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, bars);
+    qpair_prologue<E, BGK>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, bars);
 
     bool failed = false;
     unsigned pend = 0u;        // thread 0: barriers with a load in flight
     auto load_x = [&](int k, int b) {
         if (k < k_end && !a.stall_test) {       // test hook: no copy, the wait runs out
             pend |= 1u << b;
-            mbar_arrive_expect_tx(&bars[b], XT * 4);
+            mbar_arrive_expect_tx(&bars[b], XT * sizeof(E));
             tma_load_3d(X + b * XT, &a.tmap, &bars[b], xs + k * PW, i0 + Ng - HALO,
                         j0 + Ng - HALO);
         }
@@ -158,9 +211,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     auto load_b = [&](int k, int b) {          // base1 tile of chunk k -> buffer b
         if (!BX && k < k_end && !a.stall_test) {
             pend |= 4u << b;
-            mbar_arrive_expect_tx(&bars[2 + b], kPairTile);
-            tma_load_3d(b1s + b * (kPairTile / 4), &a.tm_b1, &bars[2 + b], xs + k * PW, i0 + Ng,
-                        j0 + Ng);
+            mbar_arrive_expect_tx(&bars[2 + b], TE * sizeof(E));
+            tma_load_3d(b1s + b * TE, &a.tm_b1, &bars[2 + b], xs + k * PW, i0 + Ng, j0 + Ng);
         }
     };
     if (tid == 0) {
@@ -170,10 +222,10 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         load_b(k_begin + 1, 1);
     }
 
-    float* __restrict__ out1 = static_cast<float*>(a.out1);
-    const float2 c1 = f2(float(a.c1)), c2 = f2(float(a.c2));
-    const float inv_dq1 = float(1.0 / a.dq1), inv_dq2 = float(1.0 / a.dq2);
-    const float2 inv_tau = f2(float(1.0 / a.tau));
+    E* __restrict__ out1 = static_cast<E*>(a.out1);
+    const P c1 = f2(E(a.c1)), c2 = f2(E(a.c2));
+    const E inv_dq1 = E(1.0 / a.dq1), inv_dq2 = E(1.0 / a.dq2);
+    const P inv_tau = f2(E(1.0 / a.tau));
     const bool want_mom = a.mom_out != nullptr;
     const bool check = a.flag != nullptr;
     const unsigned rowstride = (unsigned)(a.Ns * Np);
@@ -197,11 +249,12 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const int rp = warp & 3, seg = warp >> 2;
     const int a_row = 2 * rp, a_c0 = 4 * seg;        // phase A: rows a_row, a_row+1
     const int b_col = 2 * rp, b_r0 = 4 * seg;        // phase B: cols b_col, b_col+1
-    const int sw0 = swz(b_col, lane) - b_col * PW;   // swizzled lane slot, column b_col
-    const int sw1 = swz(b_col + 1, lane) - (b_col + 1) * PW;
-    const float4* c_src0 = reinterpret_cast<const float4*>(o1s + pc_c * PW) + ((2 * pc_q) ^ (pc_c & 7));
-    const float4* c_src1 = reinterpret_cast<const float4*>(o1s + pc_c * PW) + ((2 * pc_q + 1) ^ (pc_c & 7));
-    const float2* tb_row = tabs + b_r0 * 4 + rp;           // pair of row b_r0, cols b_col..+1
+    const int sw0 = stg<E>(b_col, lane) - b_col * CS;   // swizzled lane slot, column b_col
+    const int sw1 = stg<E>(b_col + 1, lane) - (b_col + 1) * CS;
+    // phase C source: 8 p from 16-byte chunk c_ch0 of q-cell pc_c's staging row
+    const E* c_row = o1s + (8 * pc_q / CS) * 64 * CS + pc_c * CS;
+    const int c_ch0 = (8 * pc_q % CS) / VE, c_key = pc_c & 7;
+    const P* tb_row = tabs + b_r0 * 4 + rp;                // pair of row b_r0, cols b_col..+1
 
     // periodic ghost images (border CTAs): offsets of column `warp` of the
     // tile, the q1 image shift g_d1, and the rows [0, g_bot) with a q2 image
@@ -209,7 +262,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     int g_src = 0, g_dst = 0, g_d1 = 0, g_d2 = 0, g_bot = 0, g_top = TQ;
     if (border) {
         const int ii = i0 + warp;
-        g_src = swz(warp, lane);                           // row r adds r*TQ*PW
+        g_src = stg<E>(warp, lane);                        // row r adds r*TQ*CS
         g_dst = (j0 + Ng) * (int)colstride + (ii + Ng) * (int)rowstride + xs + lane;
         if (a.periodic1 || peer1)
             g_d1 = ii < Ng ? Nq1 * (int)rowstride : (ii >= Nq1 - Ng ? -Nq1 * (int)rowstride : 0);
@@ -230,31 +283,31 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         // no CTA barrier here: each thread has waited for the halo tile itself,
         // D1 was last read before the previous chunk's third barrier, and a
         // failed wait reaches every thread through the next barrier
-        const float* Xb = X + buf * XT;
+        const E* Xb = X + buf * XT;
         const double V1 = vgrid[ip1], V2 = vgrid[Np1 + ip2];
 
         // ---- phase A: q1 faces of rows a_row, a_row+1 -> D1 -------------------
         {
-            const float v1 = float(V1);
-            const bool right = v1 > 0.0f;
-            Weno5Pair S; S.set(right);
-            const float* ra = Xb + ((a_row + HALO) * HX + a_c0 + (right ? 0 : 1)) * PW + lane;
-            const float* rb = ra + HX * PW;
-            float2 y0 = make_float2(ra[0 * PW], rb[0 * PW]);
-            float2 y1 = make_float2(ra[1 * PW], rb[1 * PW]);
-            float2 y2 = make_float2(ra[2 * PW], rb[2 * PW]);
-            float2 y3 = make_float2(ra[3 * PW], rb[3 * PW]);
-            float2 y4 = make_float2(ra[4 * PW], rb[4 * PW]);
+            const E v1 = E(V1);
+            const bool right = v1 > E(0);
+            Side S; S.set(right);
+            const E* ra = Xb + ((a_row + HALO) * HX + a_c0 + (right ? 0 : 1)) * PW + lane;
+            const E* rb = ra + HX * PW;
+            P y0 = mk2(ra[0 * PW], rb[0 * PW]);
+            P y1 = mk2(ra[1 * PW], rb[1 * PW]);
+            P y2 = mk2(ra[2 * PW], rb[2 * PW]);
+            P y3 = mk2(ra[3 * PW], rb[3 * PW]);
+            P y4 = mk2(ra[4 * PW], rb[4 * PW]);
             Walker W;
-            const float2 vq = f2(0.5f * v1 * inv_dq1);   // walker returns 2x face value
-            float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
-            float* da = d1s + (a_row * TQ + a_c0) * PW + lane;
+            const P vq = f2(E(0.5) * v1 * inv_dq1);   // walker returns 2x face value
+            P Fprev = W.first(y0, y1, y2, y3, y4, S);
+            E* da = d1s + (a_row * TQ + a_c0) * PW + lane;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                y4 = make_float2(ra[(c + 5) * PW], rb[(c + 5) * PW]);
-                const float2 Fn = W.next(y0, y1, y2, y3, y4, S);
-                const float2 d = mul2(sub2(Fprev, Fn), vq);
+                y4 = mk2(ra[(c + 5) * PW], rb[(c + 5) * PW]);
+                const P Fn = W.next(y0, y1, y2, y3, y4, S);
+                const P d = mul2(sub2(Fprev, Fn), vq);
                 da[c * PW] = d.x;
                 da[(TQ + c) * PW] = d.y;
                 Fprev = Fn;
@@ -262,7 +315,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         }
         // the store of chunk k-1 must be done reading the staging tiles, and
         // the base tiles of chunk k must have landed, before phase B
-        if (tid == 0) bulk_wait_read_all();
+        if (warp == 0) bulk_wait_read_all();
         if (!BX) {
             if (!failed && !mbar_wait_bounded(&bars[2 + buf], buf ? phb1 : phb0, a.wait_cycles))
                 failed = true;
@@ -274,49 +327,49 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
 
         // ---- phase B: q2 faces of cols b_col, b_col+1, BGK, combine ------------
         {
-            const float v2 = float(V2);
-            const bool right = v2 > 0.0f;
-            Weno5Pair S; S.set(right);
-            const float* ca = Xb + ((b_r0 + (right ? 0 : 1)) * HX + b_col + HALO) * PW + lane;
-            const float* cb = ca + PW;
-            const float* cella = Xb + ((b_r0 + HALO) * HX + b_col + HALO) * PW + lane;
-            float2 y0 = make_float2(ca[0 * HX * PW], cb[0 * HX * PW]);
-            float2 y1 = make_float2(ca[1 * HX * PW], cb[1 * HX * PW]);
-            float2 y2 = make_float2(ca[2 * HX * PW], cb[2 * HX * PW]);
-            float2 y3 = make_float2(ca[3 * HX * PW], cb[3 * HX * PW]);
-            float2 y4 = make_float2(ca[4 * HX * PW], cb[4 * HX * PW]);
+            const E v2 = E(V2);
+            const bool right = v2 > E(0);
+            Side S; S.set(right);
+            const E* ca = Xb + ((b_r0 + (right ? 0 : 1)) * HX + b_col + HALO) * PW + lane;
+            const E* cb = ca + PW;
+            const E* cella = Xb + ((b_r0 + HALO) * HX + b_col + HALO) * PW + lane;
+            P y0 = mk2(ca[0 * HX * PW], cb[0 * HX * PW]);
+            P y1 = mk2(ca[1 * HX * PW], cb[1 * HX * PW]);
+            P y2 = mk2(ca[2 * HX * PW], cb[2 * HX * PW]);
+            P y3 = mk2(ca[3 * HX * PW], cb[3 * HX * PW]);
+            P y4 = mk2(ca[4 * HX * PW], cb[4 * HX * PW]);
             Walker W;
-            const float2 vq = f2(0.5f * v2 * inv_dq2);   // walker returns 2x face value
-            float2 Fprev = W.first(y0, y1, y2, y3, y4, S);
+            const P vq = f2(E(0.5) * v2 * inv_dq2);   // walker returns 2x face value
+            P Fprev = W.first(y0, y1, y2, y3, y4, S);
             const int cb0 = b_r0 * TQ + b_col;                   // q-cell of row 0, col b_col
-            const float* dk = d1s + cb0 * PW + lane;
-            const float* bb1 = b1s + buf * (kPairTile / 4) + cb0 * PW + lane;
-            float* ob1 = o1s + cb0 * PW;
-            float* ob2 = o2s + cb0 * PW + lane;
-            const float2* t1 = tb_row + ip1 * kTabPitch;
-            const float2* t2 = tb_row + (Np1 + ip2) * kTabPitch;
-            const float2* t3 = tb_row + (Np1 + Np2 + ip3) * kTabPitch;
+            const E* dk = d1s + cb0 * PW + lane;
+            const E* bb1 = b1s + buf * TE + cb0 * PW + lane;
+            E* ob1 = o1s + cb0 * CS;
+            E* ob2 = o2s + cb0 * PW + lane;
+            const P* t1 = tb_row + ip1 * kTabPitch;
+            const P* t2 = tb_row + (Np1 + ip2) * kTabPitch;
+            const P* t3 = tb_row + (Np1 + Np2 + ip3) * kTabPitch;
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                y4 = make_float2(ca[(r + 5) * HX * PW], cb[(r + 5) * HX * PW]);
-                const float2 Fn = W.next(y0, y1, y2, y3, y4, S);
-                const float2 kq = make_float2(dk[r * TQ * PW], dk[r * TQ * PW + PW]);
-                float2 kk = fma2(sub2(Fprev, Fn), vq, kq);
+                y4 = mk2(ca[(r + 5) * HX * PW], cb[(r + 5) * HX * PW]);
+                const P Fn = W.next(y0, y1, y2, y3, y4, S);
+                const P kq = mk2(dk[r * TQ * PW], dk[r * TQ * PW + PW]);
+                P kk = fma2(sub2(Fprev, Fn), vq, kq);
                 Fprev = Fn;
-                const float2 fcell = make_float2(cella[r * HX * PW], cella[r * HX * PW + PW]);
+                const P fcell = mk2(cella[r * HX * PW], cella[r * HX * PW + PW]);
                 if (BGK) {
-                    const float2 f0 = mul2(mul2(t1[r * 4], t2[r * 4]), t3[r * 4]);
+                    const P f0 = mul2(mul2(t1[r * 4], t2[r * 4]), t3[r * 4]);
                     kk = fma2(sub2(f0, fcell), inv_tau, kk);
                 }
-                const float2 o1 = KOUT ? kk
-                                       : fma2(kk, c1, BX ? fcell : make_float2(bb1[r * TQ * PW],
-                                                                               bb1[r * TQ * PW + PW]));
-                ob1[r * TQ * PW + sw0] = o1.x;
-                ob1[r * TQ * PW + PW + sw1] = o1.y;
+                const P o1 = KOUT ? kk
+                                  : fma2(kk, c1, BX ? fcell : mk2(bb1[r * TQ * PW],
+                                                                  bb1[r * TQ * PW + PW]));
+                ob1[r * TQ * CS + sw0] = o1.x;
+                ob1[r * TQ * CS + CS + sw1] = o1.y;
                 if (HAS2) {
                     // QP_X2: the full out2; QP_B1R2: the increment c2 k
-                    const float2 o2 = RED2 ? mul2(kk, c2) : fma2(kk, c2, fcell);
+                    const P o2 = RED2 ? mul2(kk, c2) : fma2(kk, c2, fcell);
                     ob2[r * TQ * PW] = o2.x;
                     ob2[r * TQ * PW + PW] = o2.y;
                 }
@@ -326,39 +379,57 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         __syncthreads();                                          // barrier 2
         if (tid == 0) {
             tma_store_3d(&a.tm_o1, o1s, xs + k * PW, i0 + Ng, j0 + Ng);
+            if (F64)        // second half of the 32 p (the swizzled rows hold 16)
+                tma_store_3d(&a.tm_o1, o1s + 64 * CS, xs + k * PW + CS, i0 + Ng, j0 + Ng);
             if (MODE == QP_X2) tma_store_3d(&a.tm_o2, o2s, xs + k * PW, i0 + Ng, j0 + Ng);
-            if (RED2) tma_reduce_add_3d(&a.tm_o2, o2s, xs + k * PW, i0 + Ng, j0 + Ng);
+            if (RED2 && !F64) tma_reduce_add_3d(&a.tm_o2, o2s, xs + k * PW, i0 + Ng, j0 + Ng);
             bulk_commit();
             load_x(k + 2, buf);
             load_b(k + 2, buf);
+        }
+        if constexpr (RED2 && F64) {
+            if (warp == 0) {
+                // the accumulator increment, one 256-byte row per q-cell, two per lane
+                double* acc = static_cast<double*>(a.out2);
+                const double* inc = reinterpret_cast<const double*>(o2s);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = lane + 32 * h;
+                    const int ii = i0 + (c & 7), jj = j0 + (c >> 3);
+                    bulk_reduce_add_f64(acc + ((long long)(jj + Ng) * colstride +
+                                               (long long)(ii + Ng) * rowstride + xs + k * PW),
+                                        inc + c * PW, PW * sizeof(double));
+                }
+                bulk_commit();
+            }
         }
 
         // ---- periodic ghost images of border cells, from the staged out1 -------
         // warp w owns tile column w; images along q1 (whole column), along q2
         // (rows below g_bot and from g_top) and at the corners (2 N_g <= N_q)
         if (border) {
-            const float* src = o1s + g_src;
-            float* dst = out1 + (g_dst + k * PW);
+            const E* src = o1s + g_src;
+            E* dst = out1 + (g_dst + k * PW);
             // q1 / q2 images: this buffer (periodic axis) or the neighbours'
             // copies (a cut axis; then no corner cell is needed)
-            float* dlo = peer2 ? static_cast<float*>(a.peer_lo) + (g_dst + k * PW) : dst;
-            float* dhi = peer2 ? static_cast<float*>(a.peer_hi) + (g_dst + k * PW) : dst;
+            E* dlo = peer2 ? static_cast<E*>(a.peer_lo) + (g_dst + k * PW) : dst;
+            E* dhi = peer2 ? static_cast<E*>(a.peer_hi) + (g_dst + k * PW) : dst;
             const int gc1 = (peer1 || peer2) ? 0 : g_d1;
             if (g_d1) {
-                float* d1 = peer1 ? static_cast<float*>(g_d1 > 0 ? a.peer_left : a.peer_right) +
-                                        (g_dst + k * PW)
-                                  : dst;
+                E* d1 = peer1 ? static_cast<E*>(g_d1 > 0 ? a.peer_left : a.peer_right) +
+                                    (g_dst + k * PW)
+                              : dst;
 #pragma unroll
                 for (int r = 0; r < TQ; ++r)
-                    d1[r * (int)colstride + g_d1] = src[r * TQ * PW];
+                    d1[r * (int)colstride + g_d1] = src[r * TQ * CS];
             }
             for (int r = 0; r < g_bot; ++r) {
-                const float v = src[r * TQ * PW];
+                const E v = src[r * TQ * CS];
                 dlo[r * (int)colstride + g_d2] = v;
                 if (gc1) dst[r * (int)colstride + gc1 + g_d2] = v;
             }
             for (int r = g_top; r < TQ; ++r) {
-                const float v = src[r * TQ * PW];
+                const E v = src[r * TQ * CS];
                 dhi[r * (int)colstride - g_d2] = v;
                 if (gc1) dst[r * (int)colstride + gc1 - g_d2] = v;
             }
@@ -369,9 +440,10 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         // fixed, so every moment follows from S0 = sum o_t, S1 = sum t o_t and
         // S2 = sum t^2 o_t (moments.py:6-24 / compute_moments.py:7-59)
         if (want_mom || check) {
-            const float4 u = *c_src0, w = *c_src1;
-            const double o0 = u.x, o1 = u.y, o2 = u.z, o3 = u.w;
-            const double o4 = w.x, o5 = w.y, o6 = w.z, o7 = w.w;
+            double ov[8];
+            load8(c_row, c_ch0, c_key, ov);
+            const double o0 = ov[0], o1 = ov[1], o2 = ov[2], o3 = ov[3];
+            const double o4 = ov[4], o5 = ov[5], o6 = ov[6], o7 = ov[7];
             const double S0 = ((o0 + o1) + (o2 + o3)) + ((o4 + o5) + (o6 + o7));
             const double S1 = fma(7.0, o7, fma(6.0, o6, fma(5.0, o5, fma(4.0, o4,
                               fma(3.0, o3, fma(2.0, o2, o1))))));
@@ -397,9 +469,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     if (failed) {
         // a barrier wait ran out: record it, then let the copies still in
         // flight land (bounded) before the CTA releases its shared memory
+        if (warp == 0) bulk_wait_all();
         if (tid == 0) {
             atomicExch(a.err, 4);
-            bulk_wait_all();
             if (pend & 1u) mbar_wait_bounded(&bars[0], phx0);
             if (pend & 2u) mbar_wait_bounded(&bars[1], phx1);
             if (pend & 4u) mbar_wait_bounded(&bars[2], phb0);
@@ -407,7 +479,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         }
         return;
     }
-    if (tid == 0) bulk_wait_all();
+    if (warp == 0) bulk_wait_all();
     // one flag write per CTA (the flag may live in host memory)
     if (__syncthreads_or(check && nonfinite) && tid == 0) atomicOr(a.flag, 1);
 
@@ -427,6 +499,44 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
                       + (long long)jj * Nq1 + ii] = v;
         }
     }
+}
+
+template <typename E, int R>
+static void (*pick_qpair(int bgk, int mode))(QStageArgs) {
+    switch (mode) {
+        case QP_X1: return bgk ? qpair_kernel<E, true, QP_X1, R> : qpair_kernel<E, false, QP_X1, R>;
+        case QP_X2: return bgk ? qpair_kernel<E, true, QP_X2, R> : qpair_kernel<E, false, QP_X2, R>;
+        case QP_B1: return bgk ? qpair_kernel<E, true, QP_B1, R> : qpair_kernel<E, false, QP_B1, R>;
+        case QP_K: return bgk ? qpair_kernel<E, true, QP_K, R> : qpair_kernel<E, false, QP_K, R>;
+        default: return bgk ? qpair_kernel<E, true, QP_B1R2, R> : qpair_kernel<E, false, QP_B1R2, R>;
+    }
+}
+
+// the stage mode from which buffers the stage reads and writes, then the
+// reconstruction's instantiation
+template <typename E>
+static cudaError_t launch_qpair(const QStageArgs& a, int bgk, int recon, dim3 grid, size_t smem,
+                                cudaStream_t st) {
+    const bool has2 = a.out2 != nullptr;
+    // first RK4 / RK2 stage: the bases are the stage input
+    const bool bx = a.base1 == a.fs && (!has2 || a.base2 == a.fs);
+    int mode;
+    if (a.base1 == nullptr && !has2) mode = QP_K;
+    else if (bx) mode = has2 ? QP_X2 : QP_X1;
+    else if (!has2) mode = QP_B1;
+    else if (a.base2 == a.out2) mode = QP_B1R2;
+    else return cudaErrorInvalidValue;        // excluded by the host's dispatch
+    void (*k)(QStageArgs);
+    switch (recon) {
+        case BOLT_RECON_MINMOD: k = pick_qpair<E, BOLT_RECON_MINMOD>(bgk, mode); break;
+        case BOLT_RECON_PPM: k = pick_qpair<E, BOLT_RECON_PPM>(bgk, mode); break;
+        case BOLT_RECON_PC: k = pick_qpair<E, BOLT_RECON_PC>(bgk, mode); break;
+        default: k = pick_qpair<E, BOLT_RECON_WENO5>(bgk, mode); break;
+    }
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, NTHREADS, smem, st>>>(a);
+    return cudaGetLastError();
 }
 
 }  // namespace bolt

@@ -15,13 +15,19 @@ inline int check_grid_params(const BoltGrid& g, const BoltParams& p) {
     if (g.N_q1 < 1 || g.N_q2 < 1 || g.N_p1 < 1 || g.N_p2 < 1 || g.N_p3 < 1 || g.N_ghost < 0 ||
         g.N_s < 1 || g.N_s > BOLT_MAX_SPECIES)
         return BOLT_ERR_ARG;
-    if (p.dtype != BOLT_F64 && p.dtype != BOLT_F32) return BOLT_ERR_ARG;
+    if (p.dtype != BOLT_F64 && p.dtype != BOLT_F32 && p.dtype != BOLT_F64_FAST)
+        return BOLT_ERR_ARG;
     if (p.recon_q < 0 || p.recon_q > 3 || p.recon_p < 0 || p.recon_p > 3) return BOLT_ERR_ARG;
     if (p.integrator != BOLT_RK2 && p.integrator != BOLT_RK4) return BOLT_ERR_ARG;
     if (p.p_dim < 1 || p.p_dim > 3) return BOLT_ERR_ARG;
-    if (p.bc_q1 < BOLT_BC_PERIODIC || p.bc_q1 > BOLT_BC_MIRROR_DIRICHLET ||
-        p.bc_q2 < BOLT_BC_PERIODIC || p.bc_q2 > BOLT_BC_MIRROR_DIRICHLET)
+    if (p.bc_q1 < BOLT_BC_PERIODIC || p.bc_q1 > BOLT_BC_SHEARING_BOX ||
+        p.bc_q2 < BOLT_BC_PERIODIC || p.bc_q2 > BOLT_BC_SHEARING_BOX)
         return BOLT_ERR_ARG;
+    // shearing box: one axis, the other periodic, a 4-point stencil in the strip
+    if (p.bc_q1 == BOLT_BC_SHEARING_BOX || p.bc_q2 == BOLT_BC_SHEARING_BOX) {
+        const int other = p.bc_q1 == BOLT_BC_SHEARING_BOX ? p.bc_q2 : p.bc_q1;
+        if (other != BOLT_BC_PERIODIC || g.N_ghost < 2) return BOLT_ERR_UNSUPPORTED;
+    }
     if (p.fields_enabled && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
         return BOLT_ERR_UNSUPPORTED;
     if (p.fields_enabled && p.fields_type != BOLT_FIELDS_ELECTRODYNAMIC &&

@@ -219,8 +219,12 @@ class nonlinear_solver(object):
         self.i_q2_start, self.i_q2_end = N_g, -N_g if N_g else None
         self._mass = [float(m) for m in _as_list(params.mass, Ns)]
         self._charge = [float(c) for c in _as_list(params.charge, Ns)]
-        self.dtype = torch.float32 if getattr(params, 'precision', 'fp64') in \
-            ('fp32', 'float32', 'single') else torch.float64
+        prec = getattr(params, 'precision', 'fp64')
+        self.dtype = torch.float32 if prec in ('fp32', 'float32', 'single') else torch.float64
+        # 'fp64-fast': FP64 f whose fused q-stage runs the paired kernel with
+        # FMA and Newton-refined reciprocals (the reference's operation order
+        # is kept by 'fp64')
+        self._fast64 = prec == 'fp64-fast'
         self.time_integrator = getattr(params, 'time_integrator', 'RK2')
         if self.time_integrator not in N.RK:
             raise NotImplementedError('time_integrator %r' % self.time_integrator)
@@ -244,6 +248,10 @@ class nonlinear_solver(object):
         self._A_q, self._C_q, self._A_p, self._C_p = ps.A_q, ps.C_q, ps.A_p, ps.C_p
         self._source = ps.source
         self._perf = {'time_ts': 0.0, 'steps': 0}
+        self._perf_parts = np.zeros(len(N.TIMING_NAMES))
+        if performance_test_flag:
+            # per-component device time of every launch group (CUDA events)
+            N.check(self._lib.bolt_set_timing(self._ctx, 1), 'bolt_set_timing')
 
     # -----------------------------------------------------------------------------
     def _stream(self):
@@ -303,7 +311,7 @@ class nonlinear_solver(object):
             g.p1_start[s], g.p2_start[s], g.p3_start[s] = ps.p1_start[s], ps.p2_start[s], ps.p3_start[s]
             g.dp1[s], g.dp2[s], g.dp3[s] = ps.dp1[s], ps.dp2[s], ps.dp3[s]
         p = N.BoltParams()
-        p.dtype = N.F32 if self.dtype == torch.float32 else N.F64
+        p.dtype = N.F32 if self.dtype == torch.float32 else (N.F64_FAST if self._fast64 else N.F64)
         try:
             p.recon_q = N.RECON[params.reconstruction_method_in_q]
             p.recon_p = N.RECON[params.reconstruction_method_in_p]
@@ -340,6 +348,11 @@ class nonlinear_solver(object):
         self._ctx = ctx
         if self._tau_arr is not None:
             N.check(self._lib.bolt_set_tau_array(ctx, self._tau_arr.data_ptr()), 'bolt_set_tau_array')
+        self._shearing = 'shearing-box' in (self._bc_q1, self._bc_q2)
+        if self._shearing:
+            # boundaries.py:17-18: the shear rate q omega of the params module
+            N.check(self._lib.bolt_set_shear(ctx, float(params.q), float(params.omega)),
+                    'bolt_set_shear')
 
     def __del__(self):
         try:
@@ -543,6 +556,10 @@ class nonlinear_solver(object):
             t0.record()
         if self._has_dirichlet():
             self._refresh_boundaries()
+        if self._shearing:
+            # the strips of every stage are sheared to the step's start time
+            # (the reference's time_elapsed, advanced after the step)
+            self._lib.bolt_set_time(self._ctx, float(self.time_elapsed))
         N.check(self._lib.bolt_step(self._ctx, self._fstore.data_ptr(), float(dt), self._stream()),
                 'bolt_step')
         self._seen_version = self._fstore._version
@@ -561,6 +578,8 @@ class nonlinear_solver(object):
         self._sync_external_edits()
         if self._has_dirichlet():
             self._refresh_boundaries()
+        if self._shearing:
+            self._lib.bolt_set_time(self._ctx, float(self.time_elapsed))
         N.check(self._lib.bolt_fill_ghosts(self._ctx, self._fstore.data_ptr(), self._stream()),
                 'bolt_fill_ghosts')
         self._seen_version = self._fstore._version
@@ -607,7 +626,8 @@ class nonlinear_solver(object):
         """n_steps strang steps launched back to back (no per-step host work)."""
         self.dt = dt
         self._sync_external_edits()
-        if self._has_dirichlet():
+        if self._has_dirichlet() or self._shearing:
+            # per-step host work: boundary values / the strips' shear time
             for _ in range(n_steps):
                 self._step(dt)
             return
@@ -643,16 +663,28 @@ class nonlinear_solver(object):
                                      self._stream()), 'bolt_stage')
         self._seen_version = self._fstore._version
 
-    def df_dt(self, f=None, evolve_fields=None):
+    _TERMS = {'d_flux_p1_dp1': 1, 'd_flux_p2_dp2': 2, 'd_flux_p3_dp3': 3}
+
+    def df_dt(self, f=None, evolve_fields=None, term_to_return=None):
         """df/dt of f (df_dt_fvm.py:33-339) as an AF-ordered tensor.  Ghost
         cells of f are refreshed first (as fvm_operator.py does before every
         evaluation); with fields, evolve_fields=None follows the reference's
-        at_n alternation."""
+        at_n alternation.  term_to_return = 'd_flux_p1_dp1', 'd_flux_p2_dp2'
+        or 'd_flux_p3_dp3' returns that p-flux divergence alone
+        (df_dt_fvm.py:325-339); like the reference it needs fields."""
+        term = 0
+        if term_to_return is not None and term_to_return in self._TERMS:
+            if not self.fields_enabled:
+                raise ValueError('term_to_return=%r needs fields_enabled (the p-fluxes are '
+                                 'computed only with fields)' % term_to_return)
+            term = self._TERMS[term_to_return]
         if f is None:
             self._sync_external_edits()
             src = self._fstore.clone()
         else:
             src = self._to_store(torch.as_tensor(f, device=self.device))
+        if self._shearing:
+            self._lib.bolt_set_time(self._ctx, float(self.time_elapsed))
         N.check(self._lib.bolt_fill_ghosts(self._ctx, src.data_ptr(), self._stream()),
                 'bolt_fill_ghosts')
         self._invalidate()
@@ -662,8 +694,14 @@ class nonlinear_solver(object):
             at_n = bool(self._lib.bolt_get_at_n(self._ctx))
             ev = int((not at_n) if evolve_fields is None else bool(evolve_fields))
             self._lib.bolt_set_at_n(self._ctx, 0 if at_n else 1)
-        N.check(self._lib.bolt_dfdt(self._ctx, src.data_ptr(), out.data_ptr(), ev,
-                                    float(getattr(self, 'dt', 0.0)), self._stream()), 'bolt_dfdt')
+        if term:
+            N.check(self._lib.bolt_dfdt_term(self._ctx, src.data_ptr(), out.data_ptr(), term, ev,
+                                             float(getattr(self, 'dt', 0.0)), self._stream()),
+                    'bolt_dfdt_term')
+        else:
+            N.check(self._lib.bolt_dfdt(self._ctx, src.data_ptr(), out.data_ptr(), ev,
+                                        float(getattr(self, 'dt', 0.0)), self._stream()),
+                    'bolt_dfdt')
         return out.permute(3, 2, 1, 0)
 
     # ---- moments (compute_moments.py:7-59) -------------------------------------------------
@@ -752,14 +790,47 @@ class nonlinear_solver(object):
                                           self._stream()), 'bolt_fields_set')
 
     # ---- diagnostics (performance_timings.py:9-165) ----------------------------------------
+    def performance_timings(self):
+        """Device seconds spent in each component since the solver was made
+        (performance_test_flag=True): the timestep total and the ghost pass,
+        moments, q-stage, p-stage and field solve (CUDA events)."""
+        import ctypes
+        if self.performance_test_flag:
+            buf = (ctypes.c_double * len(N.TIMING_NAMES))()
+            N.check(self._lib.bolt_timings(self._ctx, buf), 'bolt_timings')
+            self._perf_parts += np.array(list(buf)) * 1e-3
+        out = {'timestep': self._perf['time_ts']}
+        out.update({k: float(v) for k, v in zip(N.TIMING_NAMES, self._perf_parts)})
+        return out
+
     def print_performance_timings(self, N_iters):
+        """performance_timings.py:9-165: seconds per iteration of the step and
+        of its parts, as a table, then Spatial Zone Cycles/s.  The reference's
+        FVM_SOLVER row splits into RECONSTRUCTION, RIEMANN-SOLVER and
+        DFDT_INTEGRATION; those are fused in one kernel here, so the rows are
+        the kernels: the q-stage (q-fluxes, BGK, RK combine, moments of the
+        result) and, with fields, the p-stage; FIELD-STEP is the FDTD update
+        or the electrostatic solve; APPLY_BCS_F + COMMUNICATE_F is the one
+        ghost pass that does both."""
         n = max(N_iters, 1)
-        t = self._perf['time_ts'] / n
+        t = self.performance_timings()
+        ts = t['timestep'] / n
         cells = self.N_q1 * self.N_q2 * self.N_species * self.N_p1 * self.N_p2 * self.N_p3
-        print('Time per step            : %.6e s' % t)
-        if t > 0:
-            print('Spatial Zone Cycles/s =', self.N_q1 * self.N_q2 / t)
-            print('Phase-space cell updates/s =', cells / t)
+        rows = [('TIMESTEP', t['timestep']),
+                ('FVM_SOLVER', t['q-stage'] + t['p-stage']),
+                ('  Q-STAGE (fluxes + BGK + combine)', t['q-stage']),
+                ('  P-STAGE (p-fluxes)', t['p-stage']),
+                ('FIELD-STEP', t['fields']),
+                ('MOMENTS (BGK input)', t['moments']),
+                ('APPLY_BCS_F + COMMUNICATE_F', t['ghosts'])]
+        w = max(len(r[0]) for r in rows)
+        print('%-*s | %-18s | %s' % (w, 'Method', 'Time-Taken(s/iter)', 'Percentage(%)'))
+        for name, v in rows:
+            pct = 100.0 * v / t['timestep'] if t['timestep'] > 0 else 0.0
+            print('%-*s | %-18.6e | %.2f' % (w, name, v / n, pct))
+        if ts > 0:
+            print('Spatial Zone Cycles/s =', self.N_q1 * self.N_q2 / ts)
+            print('Phase-space cell updates/s =', cells / ts)
 
     def launch_count(self):
         return int(self._lib.bolt_launch_count(self._ctx))

@@ -48,6 +48,10 @@ extern "C" {
 /* dtype of f */
 #define BOLT_F64 0
 #define BOLT_F32 1
+/* f in FP64; the fused q-stage of 8x8-tiled grids runs the paired kernel with
+ * FMA contraction and Newton-refined reciprocals (throughput form, agreeing
+ * with BOLT_F64 to rounding), every other kernel as for BOLT_F64 */
+#define BOLT_F64_FAST 2
 
 /* reconstruction (reconstruct.py:29-44) */
 #define BOLT_RECON_PC     0   /* 'piecewise-constant' */
@@ -74,6 +78,13 @@ extern "C" {
 /* mirror, then the Dirichlet inflow values where the velocity normal to the
  * edge points into the domain (apply_bcs_f's 'mirror+dirichlet') */
 #define BOLT_BC_MIRROR_DIRICHLET 4
+/* shearing box (boundaries.py:6-145): periodic, then each ghost strip
+ * resampled along the other q axis at positions shifted by -/+ q omega L t
+ * (L the length of the strip's own axis, t the time set by bolt_set_time;
+ * q, omega from bolt_set_shear), wrapped into the domain, by the
+ * one-dimensional Catmull-Rom cubic.  One axis at most, the other periodic;
+ * needs N_ghost >= 2. */
+#define BOLT_BC_SHEARING_BOX 5
 
 /* field models (fields.py:559-690): electrodynamic fields advanced by FDTD
  * once per step, or electrostatic fields re-solved from the charge density of
@@ -139,6 +150,12 @@ int  bolt_set_tau_array(BoltCtx* ctx, const void* tau_dev);
  * zero elsewhere (boundaries.py:147-225; PETSc ghosted halos stay zero). */
 int  bolt_set_dirichlet(BoltCtx* ctx, int side, const void* values_dev);
 
+/* Shearing-box constants (params.q, params.omega of boundaries.py:17-18) and
+ * the time the ghost strips are sheared to (the reference's time_elapsed,
+ * constant over the stages of a step). */
+int  bolt_set_shear(BoltCtx* ctx, double q, double omega);
+int  bolt_set_time(BoltCtx* ctx, double t);
+
 /* Halo refresh of f in place (periodic wrap + Dirichlet inflow). */
 int  bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream);
 
@@ -151,6 +168,15 @@ int  bolt_invalidate(BoltCtx* ctx);
  * currents of this f (the reference's at_n == False branch). */
 int  bolt_dfdt(BoltCtx* ctx, const void* f_dev, void* dfdt_dev, int evolve_fields,
                double dt, void* stream);
+
+/* One p-flux divergence of f (fields enabled): term = 1, 2 or 3 writes
+ * d_flux_pk_dpk = (F_pk(right face) - F_pk(left face)) / dpk into the
+ * interior cells of out, after the same field evaluation bolt_dfdt performs
+ * (evolve_fields as there).  Replaces df_dt_fvm's term_to_return
+ * (df_dt_fvm.py:325-339); BOLT_ERR_UNSUPPORTED without fields, where the
+ * reference has no p-fluxes either. */
+int  bolt_dfdt_term(BoltCtx* ctx, const void* f_dev, void* out_dev, int term, int evolve_fields,
+                    double dt, void* stream);
 
 /* One full RK step of f in place (ghosts refreshed by the call). */
 int  bolt_step(BoltCtx* ctx, void* f_dev, double dt, void* stream);
@@ -274,9 +300,27 @@ int  bolt_set_wait_budget(BoltCtx* ctx, long long cycles);
 int  bolt_test_stall_waits(BoltCtx* ctx, int on);
 const char* bolt_strerror(int code);
 
+/* Per-component device time (performance_timings.py:9-165 reports the same
+ * split of a step for the reference's ArrayFire path).  With bolt_set_timing
+ * on, every launch group is bracketed by CUDA events on its stream;
+ * bolt_timings synchronises on them, writes the accumulated milliseconds per
+ * component since the last call to ms_out[BOLT_TIMING_COUNT] and resets
+ * them.  Each launch group is also an NVTX range ("bolt: q-stage", ...),
+ * inside one range per RK stage ("bolt: RK stage k"), whether or not timing
+ * is on. */
+#define BOLT_TIMING_GHOSTS  0   /* communicate_f + apply_bcs_f: the ghost pass     */
+#define BOLT_TIMING_MOMENTS 1   /* velocity moments of a stage input (BGK)        */
+#define BOLT_TIMING_QSTAGE  2   /* q-advection + BGK + RK combine (+ moments out) */
+#define BOLT_TIMING_PSTAGE  3   /* p-advection from the cell-centred fields       */
+#define BOLT_TIMING_FIELDS  4   /* FDTD update or electrostatic FFT solve          */
+#define BOLT_TIMING_COUNT   5
+int  bolt_set_timing(BoltCtx* ctx, int on);
+int  bolt_timings(BoltCtx* ctx, double* ms_out);
+
 /* Number of kernels launched through this context so far, and how many of
- * them were the paired FP32 stage kernel (the fused q-stage taken for FP32
- * 8x8-tiled grids; every other stage runs the one-cell-per-thread kernel).
+ * them were the paired stage kernel (the fused q-stage taken for FP32 and
+ * BOLT_F64_FAST 8x8-tiled grids; every other stage runs the
+ * one-cell-per-thread kernel).
  * Diagnostics: the reference has no counterpart. */
 long long bolt_launch_count(BoltCtx* ctx);
 long long bolt_paired_launch_count(BoltCtx* ctx);

@@ -529,8 +529,9 @@ class Oracle(object):
         out[sl] = f[sl]
         # periodic wrap for periodic axes (DMDA globalToLocal); ghosts on
         # 'ghosted' axes hold the local buffer's contents, which stay zero
-        per1 = sp['bc_q1'] == 'periodic'
-        per2 = sp['bc_q2'] == 'periodic'
+        # (a shearing-box axis is periodic in the DMDA, nonlinear_solver.py:186-194)
+        per1 = sp['bc_q1'] in ('periodic', 'shearing-box')
+        per2 = sp['bc_q2'] in ('periodic', 'shearing-box')
         i1 = np.arange(-Ng, g.Nq1 + Ng)
         i2 = np.arange(-Ng, g.Nq2 + Ng)
         src1 = np.where((i1 >= 0) & (i1 < g.Nq1), i1, i1 % g.Nq1)
@@ -554,6 +555,9 @@ class Oracle(object):
         # the Dirichlet inflow values (boundaries.py:147-225)
         for side in ('left', 'right', 'bottom', 'top'):
             axis_bc = sp['bc_q1'] if side in ('left', 'right') else sp['bc_q2']
+            if axis_bc == 'shearing-box':
+                self._shear_strip(out, side)
+                continue
             if axis_bc in ('mirror', 'mirror+dirichlet'):
                 # ghost cells take the interior cells mirrored across the edge,
                 # with the p-index normal to the edge reversed (p1 for q1 edges,
@@ -586,6 +590,57 @@ class Oracle(object):
                 sel = np.where(v < 0, val, out)
                 out[-Ng:] = sel[-Ng:]
         return out
+
+    def _shear_strip(self, out, side):
+        """Shearing-box ghost strip (boundaries.py:6-145): the strip of N_g
+        ghost columns (left/right) or rows (bottom/top), already filled
+        periodically, resampled along the other q axis at the positions
+        sheared by -/+ q omega L t (L the length of the strip's own axis,
+        t = time_elapsed), wrapped into the domain.  The reference resamples
+        with ArrayFire's approx2(BICUBIC_SPLINE); at the strip's own grid
+        positions that is the one-dimensional Catmull-Rom cubic (Catmull and
+        Rom 1974: the cubic Hermite segment whose end tangents are the
+        centred differences (p_{k+1} - p_{k-1})/2) along the sheared axis,
+        which is what this evaluates.  The shift is first reduced modulo the
+        period with the exact fmod, so the wrap below takes at most two steps
+        (the reference subtracts the period repeatedly; the two agree to
+        rounding)."""
+        g, sp, Ng = self.g, self.spec, self.g.Ng
+        shear = sp['shear_q'] * sp['shear_omega'] * self.time_elapsed
+        if side in ('left', 'right'):
+            lo, hi, N, d = sp['q2_start'], sp['q2_end'], g.Nq2, g.dq2
+            shift = shear * (sp['q1_end'] - sp['q1_start'])
+            centres = g.q2_center[:, 0]                     # ghosted q2 centres
+            strip = (slice(None), slice(0, Ng)) if side == 'left' \
+                else (slice(None), slice(g.Nq1g - Ng, g.Nq1g))
+            axis = 0
+        else:
+            lo, hi, N, d = sp['q1_start'], sp['q1_end'], g.Nq1, g.dq1
+            shift = shear * (sp['q2_end'] - sp['q2_start'])
+            centres = g.q1_center[0, :]
+            strip = (slice(0, Ng), slice(None)) if side == 'bottom' \
+                else (slice(g.Nq2g - Ng, g.Nq2g), slice(None))
+            axis = 1
+        L = hi - lo
+        shift = np.fmod(shift, L)
+        pos = centres - shift if side in ('left', 'bottom') else centres + shift
+        while np.any(pos > hi):
+            pos = np.where(pos > hi, pos - L, pos)
+        while np.any(pos < lo):
+            pos = np.where(pos < lo, pos + L, pos)
+        x = (pos - centres[0]) / d                          # index in the ghosted strip
+        j = np.floor(x).astype(int)
+        t = x - j
+        assert j.min() - 1 >= 0 and j.max() + 2 <= N + 2 * Ng - 1
+        data = out[strip].copy()
+        take = lambda k: np.take(data, j + k, axis=axis)
+        p0, p1, p2, p3 = take(-1), take(0), take(1), take(2)
+        shp = [1] * data.ndim
+        shp[axis] = -1
+        t = t.reshape(shp)
+        val = p1 + 0.5 * t * ((p2 - p0) + t * ((2.0 * p0 - 5.0 * p1 + 4.0 * p2 - p3)
+                                             + t * (3.0 * (p1 - p2) + p3 - p0)))
+        out[strip] = val
 
     # -----------------------------------------------------------------------
     def dfdt(self, f, evolve_fields=None, term='all'):

@@ -86,6 +86,9 @@ def build_modules(spec, precision='fp64', integrator=None):
     params.p_space_grid = 'cartesian'
     params.time_integrator = integrator or spec['integrator']
     params.precision = precision
+    # shearing-box rate q omega (boundaries.py:17-18)
+    params.q = spec.get('shear_q', 0.0)
+    params.omega = spec.get('shear_omega', 0.0)
     tau = spec['tau']
 
     def tau_fn(q1, q2, p1, p2, p3):

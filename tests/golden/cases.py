@@ -247,6 +247,16 @@ for _name, _init, _form in (
     CASES[_name] = make(fields_initialize=_init, field_init=_form,
                         **copy.deepcopy(_FIELD_INIT_BASE))
 
+# 2D3V with user-defined E and B: every field component nonzero, so each of
+# the three p-flux divergences (term_to_return) is pinned
+CASES['fields_user_E_B_2d3v'] = make(
+    N_q1=6, N_q2=4, N_p1=6, N_p2=6, N_p3=4,
+    p1_start=[-4.0], p1_end=[4.0], p2_start=[-4.0], p2_end=[4.0],
+    p3_start=[-4.0], p3_end=[4.0], mass=[1.0], charge=[-1.0], p_dim=3,
+    fields_enabled=True, fields_initialize='user-defined', field_init='E_B',
+    tau=0.1, dt=1e-3, steps=2,
+    init=dict(amp=0.05, k1=1, k2=1, T=[1.0, 1.2, 0.9], u=[0.1, -0.1, 0.2]))
+
 
 def field_functions(form, sin, cos):
     """The initialize-module field functions of the 'field_init' cases, written

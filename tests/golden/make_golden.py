@@ -21,7 +21,8 @@ thin wrappers, exactly as the oracle restates them:
     same mathematical flux (the oracle evaluates the LLF formula).
 
 Writes tests/golden/<case>.npz with arrays in the (q2, q1, s, p3, p2, p1)
-layout; f0, dfdt0, f_final and the moments hold interior cells only,
+layout; f0, dfdt0 (and, with fields, dfdt0_p1..p3: the term_to_return
+p-flux divergences), f_final and the moments hold interior cells only,
 f0_refreshed (the initial state after the halo/BC refresh) and the field arrays
 hold ghost cells too.  Only this script reads the reference; the fixtures travel.
 """
@@ -220,6 +221,12 @@ def run_case(name, spec):
         at_n = nls.fields_solver.at_n
     out['dfdt0'] = interior(af_to_layout(df_dt_fvm(nls.f, nls), spec), spec)
     if spec['fields_enabled']:
+        # the single p-flux divergences of the same state (term_to_return,
+        # df_dt_fvm.py:325-335), each from the same field time level
+        for k in (1, 2, 3):
+            nls.fields_solver.at_n = at_n
+            term = df_dt_fvm(nls.f, nls, term_to_return='d_flux_p%d_dp%d' % (k, k))
+            out['dfdt0_p%d' % k] = interior(af_to_layout(term, spec), spec)
         nls.fields_solver.at_n = at_n
         out['fields_cell0'] = np.transpose(np.asarray(nls.fields_solver.cell_centered_EM_fields)
                                            .reshape(6, 1, Nq(spec, 1), Nq(spec, 2))[:, 0], (0, 2, 1))

@@ -175,3 +175,63 @@ def test_fdtd_tm_mode_with_currents_second_order():
     for c, e in errs.items():
         slope = np.polyfit(np.log10(Ns), np.log10(e), 1)[0]
         assert abs(slope + 2) < 0.25, (c, e, slope)
+
+
+def shear_spec(N, axis):
+    """The reference's shearing-box known-answer setup
+    (test_shearing_boundaries/test_shear.py:22-88): N x N q-grid on [0, 1]^2,
+    one p-cell, density 1 + 0.01 sin-like wave along the sheared axis
+    (here 1 + 0.01 cos(2 pi q)), q = omega = 1; the other axis periodic."""
+    bc = dict(bc_q1='shearing-box', bc_q2='periodic') if axis == 1 else \
+        dict(bc_q1='periodic', bc_q2='shearing-box')
+    k = dict(k1=0, k2=1) if axis == 1 else dict(k1=1, k2=0)
+    return C.make(N_q1=N, N_q2=N, N_p1=1, N_p2=1, N_p3=1, p1_start=[-0.5], p1_end=[0.5],
+                  p2_start=[-0.5], p2_end=[0.5], p3_start=[-0.5], p3_end=[0.5], mass=[1.0],
+                  charge=[0.0], p_dim=3, shear_q=1.0, shear_omega=1.0,
+                  init=dict(amp=0.01, **k), **bc)
+
+
+def shear_errors(spec, fghost_fn, t, axis):
+    """Mean |ghost - exact| over both strips' interior rows (columns): the
+    exact values are the initial density at the sheared, wrapped positions."""
+    g = spec['N_ghost']
+    N = spec['N_q1']
+    centres = (np.arange(-g, N + g) + 0.5) / N
+    vel = float(C.maxwellian_p(spec, 0, 0.0, 0.0, 0.0))    # the single p-cell's factor
+    err = 0.0
+    for side, sgn in (('lo', -1), ('hi', +1)):
+        pos = np.mod(centres + sgn * t, 1.0)
+        exact = (1 + 0.01 * np.cos(2 * np.pi * pos)) * vel
+        got = fghost_fn(side)                     # (N_rows of the strip, N_g)
+        err += np.mean(np.abs(got - exact[g:N + g, None]))
+    return err
+
+
+@pytest.mark.parametrize('axis', [1, 2])
+def test_shearing_box_kat_third_order(axis):
+    """boundaries.py:6-145 on the oracle: after the halo refresh at time t the
+    ghost strips equal the initial data shifted by -/+ q omega L t along the
+    other axis, with error O(N^-3) (slope of log error vs log N within 0.3 of
+    -3, as test_shear.py asserts) for N = 32 .. 512.  The error constant
+    depends on where the shift falls within a cell, so each N sums the errors
+    of seven shifts spread over the period (test_shear.py draws one at
+    random)."""
+    Ns = [32, 64, 128, 256, 512]
+    errs = []
+    for N in Ns:
+        spec = shear_spec(N, axis)
+        o = Oracle(spec, C.initial_f(spec))
+        g = spec['N_ghost']
+        e = 0.0
+        for t in np.linspace(0.11, 0.89, 7):
+            o.time_elapsed = t
+            out = o.refresh(o.f)[..., 0, 0, 0, 0]     # (Nq2g, Nq1g)
+
+            def strip(side):
+                if axis == 1:
+                    return out[g:N + g, :g] if side == 'lo' else out[g:N + g, N + g:]
+                return (out[:g, g:N + g] if side == 'lo' else out[N + g:, g:N + g]).T
+            e += shear_errors(spec, strip, t, axis)
+        errs.append(e)
+    slope = np.polyfit(np.log10(Ns), np.log10(errs), 1)[0]
+    assert abs(slope + 3) < 0.3, (errs, slope)
