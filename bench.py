@@ -1,15 +1,17 @@
 """Benchmark of the FVM kinetic update on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp32|fp64] [--small]
+                    [--precision fp32|fp64|fp64-fast] [--small]
+                    [--parallelism replicas|slabs] [--workload ...]
 
 Workload (one step = one classic RK4 step over the whole phase space):
   2D3V, N_q1 = N_q2 = 128 on [0,1]^2 periodic, N_p1 = N_p2 = N_p3 = 24 on
   [-6,6]^3 (226,492,416 cells), f0 = Maxwellian (T = 1) with
   n = 1 + 0.05 cos(2 pi q1) cos(2 pi q2), BGK tau = 0.05, fields off,
-  WENO5 + LLF, dt = 1e-3; f in FP32 with FP64 moments (the FP64 form is
+  WENO5 + LLF, dt = 1e-3; f in FP32 with FP64 moments (both FP64 forms are
   measured as well).  Synthetic data; f (0.99 GB FP32) is larger than L2, so
-  no L2 flush is needed between steps.
+  no L2 flush is needed between steps.  On one GPU the line also holds the
+  benchmark set's other targets (ragged batch, adjoint, 2D2V FDTD).
 
 --impl reference times the FP64 C/OpenMP restatement of the same path
 (oracle/bolt_oracle_c.c) on all host cores, on a sample of the workload (the
@@ -17,7 +19,9 @@ reference itself is Python over ArrayFire/PETSc and cannot run on the GPU box).
 
 Multi-GPU (torchrun): every rank advances an independent replica of the
 workload (no data-path collective); value = cell-updates of all ranks / the
-slowest rank's time.
+slowest rank's time.  The line's "decomposed" entry times the same workload
+as one run cut into q2 slabs over the ranks (strong scaling, peer halos);
+--parallelism slabs makes that the line's value.
 """
 
 import argparse
@@ -298,6 +302,55 @@ def job_value(cells_per_rank, world, ms_max):
     return cells_per_rank * world / (ms_max * 1e-3)
 
 
+def slab_result(args, rank, world, local_rank, spec):
+    """The same run cut into ``world`` q2 slabs, one per rank (SlabSolver: the
+    reference's DMDA split, nonlinear_solver.py:251-280), strong scaling:
+    with a process group the stage kernels store their boundary rows straight
+    into the neighbouring GPUs' buffers (peer halos over NVLink, CUDA IPC) and
+    the ranks order their stages with a one-element all-reduce; a single
+    process steps one slab whose halo wraps onto itself.  Time per step is
+    the slowest rank's (CUDA events), value = the whole run's cells / time."""
+    import torch
+    import torch.distributed as dist
+    from bolt_b200.distributed import SlabSolver
+    from bolt_b200.physical_system import physical_system
+    import bolt_b200.src.nonrelativistic_boltzmann.advection_terms as adv
+    import bolt_b200.src.nonrelativistic_boltzmann.collision_operator as col
+    import bolt_b200.src.nonrelativistic_boltzmann.moments as mom
+    dom, bc, params, ini = config_modules(spec, args.precision)
+    slab = SlabSolver(physical_system(dom, bc, params, ini, adv, col.BGK, mom))
+    peer = world > 1 and dist.is_initialized()
+    if peer:
+        slab.enable_peer_halos()
+    dt = spec['dt']
+    for _ in range(args.warmup):
+        slab.strang_timestep(dt)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = slab.local.launch_count()
+    paired0 = slab.local.paired_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        slab.strang_timestep(dt)
+    e1.record()
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    launches = slab.local.launch_count() - launches0
+    paired = slab.local.paired_launch_count() - paired0
+    slab.local.synchronize()
+    if peer:
+        dist.barrier()
+        slab.disable_peer_halos()
+    cells = interior_cells(spec)
+    return {'value': cells / (ms * 1e-3), 'ms_per_step': ms, 'scaling': 'strong',
+            'slabs': world, 'rows_per_slab': spec['N_q2'] // world,
+            'halos': 'peer stores over NVLink' if peer else 'single slab (wraps onto itself)',
+            'gpu_launches_per_rank': launches,
+            'paired_launches_per_rank': paired}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -305,6 +358,19 @@ def run_ours(args, rank, world, local_rank):
     spec = workload_spec(args.small)
     cells = interior_cells(spec)
     dt = spec['dt']
+    if args.parallelism == 'slabs':
+        res = slab_result(args, rank, world, local_rank, spec)
+        if rank == 0:
+            print(json.dumps({
+                'metric': METRIC, 'value': res['value'], 'unit': UNIT, 'n_gpus': world,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': res['ms_per_step'],
+                'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None,
+                'dtype': 'f32' if args.precision == 'fp32' else 'f64', 'data': 'synthetic',
+                'config': {'workload': '2D3V %dx%d x 24^3, one run in %d q2 slabs'
+                                       % (spec['N_q1'], spec['N_q2'], world),
+                           'parallelism': 'q2-slabs'},
+                'decomposed': res, 'gpu_launches': res['gpu_launches_per_rank']}), flush=True)
+        return
     nls = make_solver(spec, args.precision)
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -459,6 +525,12 @@ def run_ours(args, rank, world, local_rank):
                  'speedup_vs_fp64': ms64 / msf,
                  'error_after_steps': args.warmup + args.steps}
 
+    # with several ranks: the same workload as one run cut into q2 slabs
+    # (strong scaling), beside the replicas of the headline
+    decomposed = None
+    if world > 1 and not args.no_decompose:
+        decomposed = slab_result(args, rank, world, local_rank, spec)
+
     # the benchmark set's other targets, on one GPU (kept out of the scaling runs)
     targets = None
     if world == 1 and not args.no_extras:
@@ -518,6 +590,7 @@ def run_ours(args, rank, world, local_rank):
         'clocks': clk.summary(),
         'fp64_plain': fp64,
         'fp64_fast': fp64f,
+        'decomposed': decomposed,
         'targets': targets,
     }
     print(json.dumps(line), flush=True)
@@ -896,7 +969,7 @@ def main():
     ap.add_argument('--steps', type=int, default=30)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp64'])
+    ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp64', 'fp64-fast'])
     ap.add_argument('--small', action='store_true', help='64x64 x 24^3 (profiling size)')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-fp64', action='store_true')
@@ -915,6 +988,12 @@ def main():
     ap.add_argument('--batch-schedule', default=None, metavar='TILE,CTAS,LPT',
                     help='fix the batch launch schedule (e.g. 16,4,1) instead of autotuning; '
                          'the warm-up run then launches exactly 4 x batch-steps stage kernels')
+    ap.add_argument('--parallelism', default='replicas', choices=['replicas', 'slabs'],
+                    help='replicas: every rank advances its own copy of the workload (the line\'s '
+                         'value; with several ranks the line also holds the slab split as '
+                         '"decomposed"); slabs: one run cut into q2 slabs over the ranks')
+    ap.add_argument('--no-decompose', action='store_true',
+                    help='with several ranks, skip the slab-split measurement')
     ap.add_argument('--no-extras', action='store_true',
                     help='skip the other targets (batch, adjoint, 2D2V) after the headline')
     ap.add_argument('--autograd-steps', type=int, default=200,

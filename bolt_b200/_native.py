@@ -97,6 +97,9 @@ SIGNATURES = {
     'bolt_stage_count': (ctypes.c_int, [_VP]),
     'bolt_stage_input': (_VP, [_VP, _VP, ctypes.c_int]),
     'bolt_stage': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
+    'bolt_stage_parts': (ctypes.c_int, [_VP, ctypes.c_int]),
+    'bolt_stage_part': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, ctypes.c_int, _VP]),
+    'bolt_fields_yee': (_VP, [_VP]),
     'bolt_set_peer_halos': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     'bolt_set_peer_halos_q1': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     'bolt_fields_evolve': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),

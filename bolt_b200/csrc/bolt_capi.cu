@@ -798,8 +798,10 @@ static int launch_pstage(BoltCtx* ctx, const StageIO& io, const void* kq, cudaSt
     return BOLT_OK;
 }
 
+// the FDTD update (part -1), or one of its three parts (a field-evolving
+// stage of a block whose Yee ghosts are exchanged between the parts)
 static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st,
-                         const double* j_given = nullptr) {
+                         const double* j_given = nullptr, int part = -1) {
     TimedScope ts(ctx, BOLT_TIMING_FIELDS, st);
     const BoltGrid& g = ctx->g;
     FieldArgs a;
@@ -813,12 +815,15 @@ static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st,
     a.nsplit = nsplit_j;
     a.Ns = g.N_s; a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost;
     a.Nq1g = ctx->Nq1g; a.Nq2g = ctx->Nq2g;
+    a.ext1 = ctx->p.bc_q1 == BOLT_BC_EXTERNAL;
+    a.ext2 = ctx->p.bc_q2 == BOLT_BC_EXTERNAL;
     a.dq1 = g.dq1; a.dq2 = g.dq2; a.dt = dt; a.eps = ctx->p.eps; a.mu = ctx->p.mu;
     for (int s = 0; s < g.N_s; ++s) {
         a.charge[s] = ctx->p.charge[s];
         a.measure[s] = (g.dp3[s] * g.dp2[s]) * g.dp1[s];
     }
-    CK(launch_fdtd(a, st, &ctx->launches));
+    if (part < 0) CK(launch_fdtd(a, st, &ctx->launches));
+    else CK(launch_fdtd_part(a, part, st, &ctx->launches));
     return BOLT_OK;
 }
 
@@ -850,8 +855,12 @@ static int launch_electrostatic(BoltCtx* ctx, const void* f, cudaStream_t st) {
 }
 
 // one df/dt evaluation + stage update: q-part (fused combine when there is no
-// p-advection), then p-part when fields are enabled
-static int run_stage(BoltCtx* ctx, StageIO io, int evolve, double dt, cudaStream_t st) {
+// p-advection), then p-part when fields are enabled.  part -1 runs the whole
+// stage; a field-evolving stage of a block runs as parts 0..2 with the Yee
+// ghosts exchanged between them (0: q-part, currents, halo; 1: E update;
+// 2: B update, cell fields, p-part)
+static int run_stage(BoltCtx* ctx, StageIO io, int evolve, double dt, cudaStream_t st,
+                     int part = -1) {
     int rc;
     if (!ctx->p.fields_enabled) {
         rc = launch_qstage(ctx, io, 0, 0, st);
@@ -864,9 +873,10 @@ static int run_stage(BoltCtx* ctx, StageIO io, int evolve, double dt, cudaStream
     } else {
         StageIO qio = io;
         qio.out1 = ctx->kbuf;
-        rc = launch_qstage(ctx, qio, 1, evolve, st);
-        if (rc == BOLT_OK && evolve) rc = launch_fields(ctx, dt, ctx->nsplit, st);
-        if (rc == BOLT_OK) rc = launch_pstage(ctx, io, ctx->kbuf, st);
+        rc = BOLT_OK;
+        if (part <= 0) rc = launch_qstage(ctx, qio, 1, evolve, st);
+        if (rc == BOLT_OK && evolve) rc = launch_fields(ctx, dt, ctx->nsplit, st, nullptr, part);
+        if (rc == BOLT_OK && (part < 0 || part == 2)) rc = launch_pstage(ctx, io, ctx->kbuf, st);
     }
     return rc;
 }
@@ -915,10 +925,27 @@ struct StageRange {
     ~StageRange() { nvtxRangePop(); }
 };
 
-static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st) {
+// whether stage k of the next step advances FDTD fields (RK4: stage 2;
+// RK2: the stage entered with the time-level flag at 0)
+static int stage_evolves(const BoltCtx* ctx, int k) {
+    if (!ctx->p.fields_enabled || ctx->p.fields_type != BOLT_FIELDS_ELECTRODYNAMIC) return 0;
+    return ctx->p.integrator == BOLT_RK2 ? !ctx->at_n : k == 1;
+}
+
+// parts of stage k: 3 when it advances the fields of a block (Yee ghosts
+// exchanged in between), else 1
+static int stage_parts(const BoltCtx* ctx, int k) {
+    const bool ext = ctx->p.bc_q1 == BOLT_BC_EXTERNAL || ctx->p.bc_q2 == BOLT_BC_EXTERNAL;
+    return ext && stage_evolves(ctx, k) ? 3 : 1;
+}
+
+static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st,
+                        int part = -1) {
     StageRange range(k);
     int rc = BOLT_OK;
-    if (k == 0) {
+    // with parts: the bookkeeping happens once, after the last part
+    const bool first_part = part <= 0, last_part = part < 0 || part == 2;
+    if (k == 0 && first_part) {
         rc = ensure_state(ctx, f, st);
         if (rc) return rc;
     }
@@ -965,8 +992,8 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         io.out1 = out1 = k == 0 ? A : f;
         peers_of(out1);
         ev = fe && !ctx->at_n;
-        rc = run_stage(ctx, io, ev, dt, st);
-        if (fe) ctx->at_n ^= 1;
+        rc = run_stage(ctx, io, ev, dt, st, ev ? part : -1);
+        if (fe && last_part) ctx->at_n ^= 1;
     } else {
         // classic RK4 (integrators.py:15-28) in accumulator form:
         //   f1 = f + (dt/2) k1, acc = f + (dt/6) k1
@@ -991,8 +1018,9 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         io.out1 = out1 = stages[k].o1; io.base2 = stages[k].b2; io.c2 = stages[k].c2;
         io.out2 = stages[k].o2;
         peers_of(out1);
-        rc = run_stage(ctx, io, fe && stages[k].ev, dt, st);
+        rc = run_stage(ctx, io, fe && stages[k].ev, dt, st, fe && stages[k].ev ? part : -1);
     }
+    if (!last_part) return rc;
     if (!rc && dir) rc = launch_ghosts(ctx, out1, st);
     if (rc) return rc;
     if (last) {
@@ -1063,6 +1091,20 @@ int bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream) {
     if (!ctx || !f_dev || k < 0 || k >= stage_count(ctx)) return BOLT_ERR_ARG;
     return run_rk_stage(ctx, f_dev, dt, k, (cudaStream_t)stream);
 }
+
+int bolt_stage_parts(BoltCtx* ctx, int k) {
+    if (!ctx || k < 0 || k >= stage_count(ctx)) return -1;
+    return stage_parts(ctx, k);
+}
+
+int bolt_stage_part(BoltCtx* ctx, void* f_dev, double dt, int k, int part, void* stream) {
+    if (!ctx || !f_dev || k < 0 || k >= stage_count(ctx)) return BOLT_ERR_ARG;
+    const int n = stage_parts(ctx, k);
+    if (part < 0 || part >= n) return BOLT_ERR_ARG;
+    return run_rk_stage(ctx, f_dev, dt, k, (cudaStream_t)stream, n == 1 ? -1 : part);
+}
+
+double* bolt_fields_yee(BoltCtx* ctx) { return ctx ? ctx->yee : nullptr; }
 
 int bolt_run(BoltCtx* ctx, void* f_dev, double dt, int n_steps, void* stream) {
     if (!ctx || !f_dev || n_steps < 0) return BOLT_ERR_ARG;

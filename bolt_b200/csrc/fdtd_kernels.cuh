@@ -39,13 +39,17 @@ __global__ void fdtd_prepare_kernel(FieldArgs a) {
     }
 }
 
-// periodic refresh of the 6 Yee components' halos (communicate_fields)
+// periodic refresh of the 6 Yee components' halos (communicate_fields); the
+// ghosts of an external axis (a block's cut), corners included, are the
+// caller's: it exchanges them with the neighbouring blocks afterwards
 __global__ void fdtd_halo_kernel(FieldArgs a) {
     const int n = a.Nq1g * a.Nq2g;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const int g1 = t % a.Nq1g, g2 = t / a.Nq1g;
         const int i = g1 - a.Ng, j = g2 - a.Ng;
-        if (i >= 0 && i < a.Nq1 && j >= 0 && j < a.Nq2) continue;
+        const bool in1 = i >= 0 && i < a.Nq1, in2 = j >= 0 && j < a.Nq2;
+        if (in1 && in2) continue;
+        if ((!in1 && a.ext1) || (!in2 && a.ext2)) continue;
         const int si = wrapi(i, a.Nq1) + a.Ng, sj = wrapi(j, a.Nq2) + a.Ng;
         for (int c = 0; c < 6; ++c) a.yee[c * n + t] = a.yee[c * n + sj * a.Nq1g + si];
     }

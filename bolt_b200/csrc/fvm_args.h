@@ -176,6 +176,7 @@ struct FieldArgs {
     const double* jpart;    // [nsplit][3][Ns][Nq2][Nq1]
     const double* j_given;  // [3][Nq2g][Nq1g] species-summed currents from the caller, or null
     int nsplit, Ns, Nq1, Nq2, Ng, Nq1g, Nq2g;
+    int ext1, ext2;         // external axes: their ghosts come from the neighbouring blocks
     double dq1, dq2, dt, eps, mu;
     double charge[kMaxSpecies], measure[kMaxSpecies];
 };

@@ -21,14 +21,30 @@ cudaError_t launch_field_halo(const FieldArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_fdtd(const FieldArgs& a, cudaStream_t st, long long* launches) {
+    for (int part = 0; part < 3; ++part) {
+        const cudaError_t e = launch_fdtd_part(a, part, st, launches);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// the FDTD update in three parts, each ending where the Yee ghosts of a
+// block's external axes must come from its neighbours: 0 the currents and the
+// halo before the E update, 1 the E update and the halo before the B update,
+// 2 the B update and the cell-centred fields
+cudaError_t launch_fdtd_part(const FieldArgs& a, int part, cudaStream_t st, long long* launches) {
     const unsigned nb = field_blocks(a);
-    fdtd_prepare_kernel<<<nb, 256, 0, st>>>(a);
-    fdtd_halo_kernel<<<nb, 256, 0, st>>>(a);
-    fdtd_e_kernel<<<nb, 256, 0, st>>>(a);
-    fdtd_halo_kernel<<<nb, 256, 0, st>>>(a);
-    fdtd_b_kernel<<<nb, 256, 0, st>>>(a);
-    fdtd_to_cell_kernel<<<nb, 256, 0, st>>>(a);
-    if (launches) *launches += 6;
+    if (part == 0) {
+        fdtd_prepare_kernel<<<nb, 256, 0, st>>>(a);
+        fdtd_halo_kernel<<<nb, 256, 0, st>>>(a);
+    } else if (part == 1) {
+        fdtd_e_kernel<<<nb, 256, 0, st>>>(a);
+        fdtd_halo_kernel<<<nb, 256, 0, st>>>(a);
+    } else {
+        fdtd_b_kernel<<<nb, 256, 0, st>>>(a);
+        fdtd_to_cell_kernel<<<nb, 256, 0, st>>>(a);
+    }
+    if (launches) *launches += 2;
     return cudaGetLastError();
 }
 

@@ -120,6 +120,7 @@ cudaError_t launch_qpair_f64(const QStageArgs& a, int bgk, int recon, dim3 grid,
 
 // FDTD sequence (FP64): prepare -> halo -> E -> halo -> B -> to_cell
 cudaError_t launch_fdtd(const FieldArgs& a, cudaStream_t st, long long* launches);
+cudaError_t launch_fdtd_part(const FieldArgs& a, int part, cudaStream_t st, long long* launches);
 cudaError_t launch_field_halo(const FieldArgs& a, cudaStream_t st);
 
 }  // namespace bolt

@@ -28,8 +28,15 @@ inline int check_grid_params(const BoltGrid& g, const BoltParams& p) {
         const int other = p.bc_q1 == BOLT_BC_SHEARING_BOX ? p.bc_q2 : p.bc_q1;
         if (other != BOLT_BC_PERIODIC || g.N_ghost < 2) return BOLT_ERR_UNSUPPORTED;
     }
-    if (p.fields_enabled && (p.bc_q1 != BOLT_BC_PERIODIC || p.bc_q2 != BOLT_BC_PERIODIC))
-        return BOLT_ERR_UNSUPPORTED;
+    // fields: periodic axes, or a block's external cuts (electrodynamic only:
+    // the FFT solve is serial, fft.py:26-27)
+    if (p.fields_enabled) {
+        for (int bc : {p.bc_q1, p.bc_q2}) {
+            if (bc == BOLT_BC_PERIODIC) continue;
+            if (bc == BOLT_BC_EXTERNAL && p.fields_type == BOLT_FIELDS_ELECTRODYNAMIC) continue;
+            return BOLT_ERR_UNSUPPORTED;
+        }
+    }
     if (p.fields_enabled && p.fields_type != BOLT_FIELDS_ELECTRODYNAMIC &&
         p.fields_type != BOLT_FIELDS_ELECTROSTATIC)
         return BOLT_ERR_ARG;

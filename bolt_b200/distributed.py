@@ -18,8 +18,17 @@ between CPU processes:
 
 Corner cells (ghost in both q1 and q2) are not exchanged: no interior update
 reads them, because the q1 and q2 stencils are separate.  An axis kept whole
-(P = 1) keeps the global problem's boundary condition.  Fields are not
-distributed: the reference's FFT initial solve is serial too (fft.py:26-27).
+(P = 1) keeps the global problem's boundary condition.
+
+Electrodynamic fields are distributed like f: each block holds the Yee and
+cell-centred fields of its q-cells plus ghosts, and the stage that advances
+them (RK4: stage 2; RK2: every other stage) runs in three parts with the Yee
+ghosts exchanged before parts 1 and 2 -- where the reference's FDTD update
+calls communicate_fields (fields.py:169-180, communicate.py:40-77) -- q1
+columns first, then q2 rows over the full width, so corner ghosts (read by
+the cell-centring of B3) arrive from the diagonal neighbours.  The fields
+must be user-defined initially: the FFT solve of the reference runs only in
+serial (fft.py:26-27).
 
 Restart files stay those of a single-process run: PETSc writes a DMDA
 vector in the natural (q2, q1, dof) order whatever the process grid
@@ -92,6 +101,36 @@ def exchange_q1_halos(store, Ng, group=None, neighbours=None):
     _swap(lo_inner.contiguous(), hi_inner.contiguous(), recv_lo, recv_hi, left, right, group)
     store[:, :Ng].copy_(recv_lo)
     store[:, n1g - Ng:].copy_(recv_hi)
+
+
+def exchange_field_halos(yee, Ng, external, group=None, q1_neighbours=None,
+                         q2_neighbours=None):
+    """Yee ghosts of a block's external axes from its neighbours, in place:
+    ``yee`` is (..., N_q2 + 2 N_g, N_q1 + 2 N_g); q1 columns over every row
+    first, then q2 rows over every column (corners from the diagonal
+    neighbours).  ``external`` = (q1 cut, q2 cut); neighbours as for f."""
+    rank, world = _group_info(group)
+    n2g, n1g = yee.shape[-2], yee.shape[-1]
+    if external[0]:
+        left, right = q1_neighbours if q1_neighbours is not None else \
+            ((rank - 1) % world, (rank + 1) % world)
+        lo_in, hi_in = yee[..., Ng:2 * Ng], yee[..., n1g - 2 * Ng:n1g - Ng]
+        if left == rank and right == rank:
+            yee[..., :Ng], yee[..., n1g - Ng:] = hi_in.clone(), lo_in.clone()
+        else:
+            recv_lo, recv_hi = torch.empty_like(lo_in.contiguous()), torch.empty_like(hi_in.contiguous())
+            _swap(lo_in.contiguous(), hi_in.contiguous(), recv_lo, recv_hi, left, right, group)
+            yee[..., :Ng], yee[..., n1g - Ng:] = recv_lo, recv_hi
+    if external[1]:
+        down, up = q2_neighbours if q2_neighbours is not None else \
+            ((rank - 1) % world, (rank + 1) % world)
+        lo_in, hi_in = yee[..., Ng:2 * Ng, :], yee[..., n2g - 2 * Ng:n2g - Ng, :]
+        if down == rank and up == rank:
+            yee[..., :Ng, :], yee[..., n2g - Ng:, :] = hi_in.clone(), lo_in.clone()
+        else:
+            recv_lo, recv_hi = torch.empty_like(lo_in.contiguous()), torch.empty_like(hi_in.contiguous())
+            _swap(lo_in.contiguous(), hi_in.contiguous(), recv_lo, recv_hi, down, up, group)
+            yee[..., :Ng, :], yee[..., n2g - Ng:, :] = recv_lo, recv_hi
 
 
 def _barrier(group):
@@ -203,8 +242,13 @@ class BlockSolver(object):
             raise NotImplementedError('a q1 cut into blocks must be periodic')
         if ext2 and (bc.in_q2_bottom != 'periodic' or bc.in_q2_top != 'periodic'):
             raise NotImplementedError('a q2 cut into blocks must be periodic')
-        if getattr(ps.params, 'fields_enabled', False):
-            raise NotImplementedError('fields are not distributed')
+        if getattr(ps.params, 'fields_enabled', False) and (ext1 or ext2):
+            # the FFT solves of the reference run only in serial (fft.py:26-27)
+            if getattr(ps.params, 'fields_type', 'electrodynamic') != 'electrodynamic':
+                raise NotImplementedError('electrostatic fields are solved by a serial FFT')
+            if getattr(ps.params, 'fields_initialize', 'fft') != 'user-defined':
+                raise NotImplementedError('a run cut into blocks needs user-defined initial '
+                                          'fields (the FFT solve is serial)')
         dom = types.ModuleType('domain')
         for k in ('N_p1', 'N_p2', 'N_p3', 'N_ghost'):
             setattr(dom, k, getattr(ps, k))
@@ -339,6 +383,34 @@ class BlockSolver(object):
     def stage(self, k, dt):
         self.local.stage(k, dt)
 
+    def stage_parts(self, k):
+        """Parts of stage k: 3 when it advances the fields (the Yee ghosts of
+        the cut axes exchanged before parts 1 and 2), else 1."""
+        return int(self.local._lib.bolt_stage_parts(self.local._ctx, int(k)))
+
+    def stage_part(self, k, part, dt):
+        from . import _native as N
+        loc = self.local
+        loc.dt = dt
+        N.check(loc._lib.bolt_stage_part(loc._ctx, loc._fstore.data_ptr(), float(dt), int(k),
+                                         int(part), loc._stream()), 'bolt_stage_part')
+        loc._seen_version = loc._fstore._version
+
+    def fields_yee(self):
+        """The block's Yee-grid fields on the device, (6, N_q2g, N_q1g) FP64."""
+        from . import _native as N
+        loc = self.local
+        n = 6 * loc.N_q2_local_with_Ng * loc.N_q1_local_with_Ng
+        ptr = loc._lib.bolt_fields_yee(loc._ctx)
+        t = torch.as_tensor(N.DeviceArray(ptr, n, '<f8'), device=loc.device)
+        return t.view(6, loc.N_q2_local_with_Ng, loc.N_q1_local_with_Ng)
+
+    def exchange_fields(self):
+        """The Yee ghosts of the cut axes from the neighbouring blocks (every
+        rank calls it between the parts of a field-advancing stage)."""
+        exchange_field_halos(self.fields_yee(), self.Ng, self.external, self.group,
+                             self.q1_neighbours, self.q2_neighbours)
+
     def end_step(self, dt):
         self.local.time_elapsed += dt
         self.time_elapsed += dt
@@ -379,7 +451,11 @@ class BlockSolver(object):
         for k in range(self.stage_count()):
             if self.needs_exchange(k):
                 self.exchange(self.stage_input(k))
-            self.stage(k, dt)
+            parts = self.stage_parts(k)
+            for part in range(parts):
+                if part:
+                    self.exchange_fields()
+                self.stage_part(k, part, dt)
             if self._peer:
                 self._stage_barrier()
         self.end_step(dt)

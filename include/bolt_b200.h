@@ -23,6 +23,9 @@
  *   bolt_moments         compute_moments             bolt/lib/nonlinear/compute_moments.py:7-59
  *   bolt_fields_set/get  fields_solver state         bolt/lib/nonlinear/fields/fields.py:421-495,649-690
  *   bolt_divergence_flag check_divergence            bolt/lib/nonlinear/timestep.py:28-38
+ *   bolt_dfdt_term       df_dt_fvm(term_to_return)   bolt/lib/nonlinear/finite_volume/df_dt_fvm.py:325-339
+ *   bolt_set_shear/time  apply_shearing_box_bcs_f    bolt/lib/nonlinear/boundaries.py:6-145
+ *   bolt_timings         print_table                 bolt/lib/utils/performance_timings.py:9-165
  */
 #ifndef BOLT_B200_H
 #define BOLT_B200_H
@@ -195,6 +198,19 @@ int  bolt_run(BoltCtx* ctx, void* f_dev, double dt, int n_steps, void* stream);
 int   bolt_stage_count(BoltCtx* ctx);
 void* bolt_stage_input(BoltCtx* ctx, void* f_dev, int k);
 int   bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream);
+
+/* A block with electrodynamic fields (an external axis): the stage that
+ * advances the FDTD fields runs in bolt_stage_parts(ctx, k) = 3 parts, and
+ * before parts 1 and 2 the caller refreshes the Yee ghosts of the external
+ * axes from the neighbouring blocks, q1 columns (all rows) first, then q2
+ * rows (all columns) -- the reference's communicate_fields between the
+ * halves of the FDTD update (fields.py:169-180, fdtd_explicit.py:141-177,
+ * communicate.py:40-77).  The Yee array is bolt_fields_yee(ctx),
+ * [6][N_q2+2N_g][N_q1+2N_g] FP64 on the device.  Every other stage has one
+ * part; parts 0..n-1 in order equal bolt_stage. */
+int     bolt_stage_parts(BoltCtx* ctx, int k);
+int     bolt_stage_part(BoltCtx* ctx, void* f_dev, double dt, int k, int part, void* stream);
+double* bolt_fields_yee(BoltCtx* ctx);
 
 /* Peer halos of a q2 slab (bc_q2 = BOLT_BC_EXTERNAL, fields off): below[] and
  * above[] are the lower and upper neighbours' device copies of

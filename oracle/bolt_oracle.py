@@ -342,6 +342,9 @@ class FieldState(object):
         Nq2g, Nq1g = grid.Nq2g, grid.Nq1g
         self.cell = np.zeros((6, Nq2g, Nq1g))
         self.yee = np.zeros((6, Nq2g, Nq1g))
+        # a q-block: fills the Yee ghosts of its external axes from the
+        # neighbouring blocks after every periodic halo refresh of the update
+        self.exchange = None
         init = sp.get('fields_initialize', 'fft')
         user = user or {}
         if init == 'user-defined':
@@ -458,13 +461,19 @@ class FieldState(object):
         out[5] = 0.25 * (y[5] + _sh(y[5], 0, -1) + _sh(y[5], -1, 0) + _sh(y[5], -1, -1))
         return out
 
+    def _halo(self, y):
+        """communicate_fields (communicate.py:40-77): the periodic refresh,
+        then, for a block, its external ghosts from the neighbours."""
+        y = _periodic_fill(self.g, y)
+        return self.exchange(y) if self.exchange is not None else y
+
     def evolve(self, J1, J2, J3, dt):
         """evolve_electrodynamic_fields (fields.py:568-647) with the aliasing of
         the three cell-centred names taken into account: the result is
         cell[:3] = 0.5*(E_before + E_after), cell[3:] = B_after."""
         E_before = self.cell[:3].copy()
         # fdtd (fdtd_explicit.py:141-177)
-        y = _periodic_fill(self.g, self.yee)
+        y = self._halo(self.yee)
         eps, mu = self.eps, self.mu
         dq1, dq2 = self.g.dq1, self.g.dq2
         B1, B2, B3 = y[3], y[4], y[5]
@@ -474,7 +483,7 @@ class FieldState(object):
         y[0] = y[0] + ((dt / (mu * eps)) * curlB_1 - J1 * dt / eps)
         y[1] = y[1] + ((dt / (mu * eps)) * curlB_2 - J2 * dt / eps)
         y[2] = y[2] + ((dt / (mu * eps)) * curlB_3 - J3 * dt / eps)
-        y = _periodic_fill(self.g, y)
+        y = self._halo(y)
         E1, E2, E3 = y[0], y[1], y[2]
         curlE_1 = (E3 - _sh(E3, 0, 1)) / dq2
         curlE_2 = -(E3 - _sh(E3, 1, 0)) / dq1

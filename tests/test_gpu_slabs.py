@@ -390,3 +390,86 @@ def test_peer_halos_through_a_process_group(monkeypatch, tmp_path):
         slab.disable_peer_halos()
     finally:
         dist.destroy_process_group()
+
+
+def _exchange_fields_blocks(blocks, dims):
+    """Yee ghosts between blocks held in one process: q1 columns over all rows,
+    then q2 rows over all columns (corners from the diagonal neighbours), what
+    exchange_field_halos does between ranks."""
+    P1, P2 = dims
+    Ng = blocks[0].Ng
+    ys = [b.fields_yee() for b in blocks]
+    at = lambda a, c: (a % P1) + P1 * (c % P2)
+    if P1 > 1:
+        n = ys[0].shape[2]
+        lft = [ys[at(i % P1 - 1, i // P1)][..., n - 2 * Ng:n - Ng].clone() for i in range(len(ys))]
+        rgt = [ys[at(i % P1 + 1, i // P1)][..., Ng:2 * Ng].clone() for i in range(len(ys))]
+        for i, y in enumerate(ys):
+            y[..., :Ng].copy_(lft[i])
+            y[..., n - Ng:].copy_(rgt[i])
+    if P2 > 1:
+        n = ys[0].shape[1]
+        bot = [ys[at(i % P1, i // P1 - 1)][:, n - 2 * Ng:n - Ng].clone() for i in range(len(ys))]
+        top = [ys[at(i % P1, i // P1 + 1)][:, Ng:2 * Ng].clone() for i in range(len(ys))]
+        for i, y in enumerate(ys):
+            y[:, :Ng].copy_(bot[i])
+            y[:, n - Ng:].copy_(top[i])
+
+
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-12), ('fp32', 2e-6)])
+@pytest.mark.parametrize('dims,integrator', [((2, 2), 'RK4'), ((2, 1), 'RK2'), ((1, 3), 'RK4')])
+def test_field_blocks_in_lockstep_equal_whole_domain(dims, integrator, precision, tol):
+    """FDTD-coupled q-blocks on one GPU (user-defined initial E and B): f
+    exchanged before every stage, the Yee ghosts between the three parts of
+    the field-advancing stage; f, the Yee-grid and the cell-centred fields
+    equal the whole-domain run (the blocks evaluate the initial field
+    functions at their own coordinates, which differ from the whole grid's
+    in the last bits, hence 1e-12 in FP64)."""
+    from bolt_b200.distributed import BlockSolver
+    P1, P2 = dims
+    spec = C.make(N_q1=8 * P1, N_q2=8 * P2, N_p1=8, N_p2=6, N_p3=1,
+                  p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+                  p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0], p_dim=2,
+                  fields_enabled=True, fields_initialize='user-defined', field_init='E_B',
+                  tau=0.1, dt=1e-3, steps=3, integrator=integrator,
+                  riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                  init=dict(amp=0.05, k1=1, k2=1, T=[1.0, 1.2, 1.0]))
+    whole = make_solver(spec, precision)
+    blocks = [BlockSolver(whole.physical_system, dims, block=(i % P1, i // P1))
+              for i in range(P1 * P2)]
+    Ng, n = spec['N_ghost'], 8
+    for i, b in enumerate(blocks):
+        r1, r2 = i % P1, i // P1
+        b.local.f = whole.f[:, :, r1 * n:r1 * n + n + 2 * Ng, r2 * n:r2 * n + n + 2 * Ng].clone()
+    dt = spec['dt']
+    for _ in range(spec['steps']):
+        whole.strang_timestep(dt)
+        for b in blocks:
+            b.begin_step()
+        for k in range(blocks[0].stage_count()):
+            _exchange_blocks(blocks, dims, k)
+            parts = blocks[0].stage_parts(k)
+            assert all(b.stage_parts(k) == parts for b in blocks)
+            for part in range(parts):
+                if part:
+                    _exchange_fields_blocks(blocks, dims)
+                for b in blocks:
+                    b.stage_part(k, part, dt)
+        for b in blocks:
+            b.end_step(dt)
+    torch.cuda.synchronize()
+
+    def stitched(arrs):
+        rows = [torch.cat([arrs[r1 + P1 * r2] for r1 in range(P1)], dim=-1) for r2 in range(P2)]
+        return torch.cat(rows, dim=-2)
+    # f as (q2, q1, ...) interiors
+    fs = [b.local._fstore[Ng:Ng + n, Ng:Ng + n].double().permute(2, 3, 0, 1) for b in blocks]
+    got = stitched(fs)
+    ref = whole._fstore[Ng:-Ng, Ng:-Ng].double().permute(2, 3, 0, 1)
+    err = float((got - ref).abs().max() / ref.abs().max())
+    assert err < tol, ('f', err)
+    yw = whole.fields_solver.yee_grid_EM_fields[:, 0].permute(0, 2, 1)[:, Ng:-Ng, Ng:-Ng]
+    yb = stitched([b.fields_yee()[:, Ng:Ng + n, Ng:Ng + n] for b in blocks])
+    ftol = 1e-12 if precision == 'fp64' else 1e-4
+    err = float((yb - yw).abs().max() / yw.abs().max())
+    assert err < ftol, ('yee', err)
