@@ -452,3 +452,31 @@ def test_fp64_fast_matches_reference_order_on_a_discontinuity(recon):
     errs = moment_errors({k: interior(v, g) for k, v in out['fp64-fast'][1].items()},
                          {k: interior(v, g) for k, v in out['fp64'][1].items()})
     assert max(errs.values()) < 1e-13, errs
+
+
+@pytest.mark.parametrize('name', ['c1_1d1v_weno5_rk2', 'c3_2d3v_weno5_rk4_small',
+                                  'mirror_dirichlet_2d3v_rk4', 'dirichlet_1d1v_weno5',
+                                  'pc_2d3v_fields', 'fields_user_E_B_2d3v',
+                                  'minmod_2d2v_fields_bgk'])
+def test_fp32_dfdt_arithmetic_error(name):
+    """The FP32 df/dt against the FP64 df/dt of the same FP32-rounded state,
+    so that only the FP32 arithmetic differs: 1e-5 normwise on these cases
+    (smooth or mildly noisy data).  The fixture comparison's 1e-3 bound
+    also absorbs the rounding of the input itself, which the flux
+    differences amplify on the noisy cases."""
+    spec = C.CASES[name]
+    G = load_golden(name)
+    g = spec['N_ghost']
+    f32 = G['f0_refreshed'].astype(np.float32).astype(np.float64)
+    out = {}
+    for prec in ('fp64', 'fp32'):
+        nls = make_solver(spec, prec)
+        nls.f = af_from_layout(f32).to('cuda')
+        if spec['fields_enabled']:
+            nls.fields_solver.cell_centered_EM_fields = fields_af(G['fields_cell0'])
+            nls.fields_solver.yee_grid_EM_fields = fields_af(G['fields_yee0'])
+        nls.dt = spec['dt']
+        out[prec] = interior(to_layout(nls.df_dt(), spec), g)
+        nls.synchronize()
+    e = rel(out['fp32'], out['fp64'])
+    assert e < 1e-5, e
