@@ -460,10 +460,14 @@ def test_fp64_fast_matches_reference_order_on_a_discontinuity(recon):
                                   'minmod_2d2v_fields_bgk'])
 def test_fp32_dfdt_arithmetic_error(name):
     """The FP32 df/dt against the FP64 df/dt of the same FP32-rounded state,
-    so that only the FP32 arithmetic differs: 1e-5 normwise on these cases
-    (smooth or mildly noisy data).  The fixture comparison's 1e-3 bound
-    also absorbs the rounding of the input itself, which the flux
-    differences amplify on the noisy cases."""
+    so that only the FP32 arithmetic differs: 1e-5 normwise, plus the
+    rounding of the BGK Maxwellian to FP32 amplified by 1/tau.  On a near-
+    equilibrium f the term (f0 - f)/tau cancels to a small df/dt, and each
+    rounded f0 carries up to 2^-24 |f0| of error, so the bound adds
+    2 * 2^-24 ||f|| / (tau ||df/dt||) (3.9e-4 on the 1D1V case with
+    tau = 0.01, where 1.5e-4 is seen; at most 2.2e-5 on the others).  The
+    fixture comparison's 1e-3 bound also absorbs the rounding of the input
+    itself, which the flux differences amplify on the noisy cases."""
     spec = C.CASES[name]
     G = load_golden(name)
     g = spec['N_ghost']
@@ -479,4 +483,6 @@ def test_fp32_dfdt_arithmetic_error(name):
         out[prec] = interior(to_layout(nls.df_dt(), spec), g)
         nls.synchronize()
     e = rel(out['fp32'], out['fp64'])
-    assert e < 1e-5, e
+    tol = 1e-5 + 2 * 2.0 ** -24 * np.linalg.norm(interior(f32, g)) / (
+        spec['tau'] * np.linalg.norm(out['fp64']))
+    assert e < tol, (e, tol)
