@@ -4,16 +4,19 @@
 // (df_dt_fvm.py:56-97 q-part + BGK source, combined with the stage update of
 // integrators.py:15-28 / fvm_operator.py:26,33) for an 8x8 q-tile and 32
 // consecutive p-cells of one species per chunk.  Every thread walks two
-// adjacent q-rows (phase A) or q-columns (phase B) of the same p at once, as
-// a pair: f32x2 arithmetic in FP32, two FMA-contracted FP64 operations with
-// Newton-refined reciprocals in FP64:
+// adjacent q-rows or q-columns of the same p at once, as a pair: f32x2
+// arithmetic in FP32, two FMA-contracted FP64 operations with Newton-refined
+// reciprocals in FP64.  The two directions run side by side in different
+// warps, each walker covering a whole 8-cell line (9 faces):
 //
-//   phase A  warp w: rows 2(w%4), 2(w%4)+1, cells 4(w/4)..+3 (5 faces each);
-//            q1 part of df/dt -> D1 tile
-//   phase B  warp w: cols 2(w%4), 2(w%4)+1, rows 4(w/4)..+3 (5 faces each);
-//            q2 part + D1 + BGK, then out1 = base1 + c1 k, out2 = base2 + c2 k
-//            into shared staging tiles
-//   phase C  FP64 velocity moments of out1 and the divergence check
+//   q1 walkers  warps 0-3, warp w: rows 2w, 2w+1; q1 part of df/dt + BGK
+//               source -> D1 tile, then a named-barrier arrival
+//   q2 walkers  warps 4-7, warp w: cols 2(w-4), 2(w-4)+1; q2 flux differences
+//               held in registers, then (after the named barrier) k = D1 +
+//               q2 part, out1 = base1 + c1 k, out2 = base2 + c2 k into shared
+//               staging tiles
+//   phase C     all warps, after the CTA barrier that closes the chunk: FP64
+//               velocity moments of out1 and the divergence check
 //
 // All global traffic is TMA: the halo tile of the stage input (14x14x32,
 // double-buffered), the base1 tile (8x8x32, double-buffered; taken from the
@@ -91,9 +94,9 @@ __device__ __forceinline__ void bulk_reduce_add_f64(double* gdst, const double* 
 
 // Prologue: p-cell centres of the species, barriers, and for BGK the
 // Maxwellian of the stage input per q-cell with exp tables stored as element
-// pairs over q-cell pairs P = row*4 + j (cells 2j, 2j+1 of one tile row):
-// tab[q*kTabPitch + P], the pitch of 33 pairs keeping a warp's reads of
-// different q (one per lane) on distinct banks.
+// pairs over q-cell pairs P = m*8 + col (cells of rows 2m and 2m+1 in one tile
+// column, the pair a q1 walker holds): tab[q*kTabPitch + P], the pitch of 33
+// pairs keeping a warp's reads of different q (one per lane) on distinct banks.
 template <typename E, bool BGK>
 __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i0, int j0,
                                                double* vgrid, double* qc,
@@ -126,9 +129,9 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
         const double m = a.sg.mass[s];
         for (int e = tid; e < 32 * ntab; e += NTHREADS) {
             const int q = e >> 5, P = e & 31;
-            const int c0 = (P >> 2) * 8 + 2 * (P & 3);
+            const int c0 = (P >> 3) * 16 + (P & 7);
             tabs[q * kTabPitch + P] = mk2(E(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
-                                          E(bgk_table_entry(a, qc + (c0 + 1) * 5, vgrid, q, m)));
+                                          E(bgk_table_entry(a, qc + (c0 + 8) * 5, vgrid, q, m)));
         }
     }
     __syncthreads();
@@ -246,15 +249,16 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const double t_own = double(lane & 7);
     double macc[kNumMom] = {0, 0, 0, 0, 0};
 
-    const int rp = warp & 3, seg = warp >> 2;
-    const int a_row = 2 * rp, a_c0 = 4 * seg;        // phase A: rows a_row, a_row+1
-    const int b_col = 2 * rp, b_r0 = 4 * seg;        // phase B: cols b_col, b_col+1
-    const int sw0 = stg<E>(b_col, lane) - b_col * CS;   // swizzled lane slot, column b_col
-    const int sw1 = stg<E>(b_col + 1, lane) - (b_col + 1) * CS;
+    // q1 walkers (warps 0-3): rows 2w, 2w+1; q2 walkers (warps 4-7): columns
+    // 2(w-4), 2(w-4)+1; each walks the 8 cells of its line
+    const bool q1w = warp < 4;
+    const int lp = 2 * (warp & 3);                    // first row (q1) or column (q2)
+    const int sw0 = stg<E>(lp, lane) - lp * CS;       // swizzled lane slot, column lp
+    const int sw1 = stg<E>(lp + 1, lane) - (lp + 1) * CS;
     // phase C source: 8 p from 16-byte chunk c_ch0 of q-cell pc_c's staging row
     const E* c_row = o1s + (8 * pc_q / CS) * 64 * CS + pc_c * CS;
     const int c_ch0 = (8 * pc_q % CS) / VE, c_key = pc_c & 7;
-    const P* tb_row = tabs + b_r0 * 4 + rp;                // pair of row b_r0, cols b_col..+1
+    const P* tb_row = tabs + (warp & 3) * TQ;             // pairs of rows lp, lp+1 (q1)
 
     // periodic ghost images (border CTAs): offsets of column `warp` of the
     // tile, the q1 image shift g_d1, and the rows [0, g_bot) with a q2 image
@@ -276,22 +280,21 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     unsigned phx0 = 0u, phx1 = 0u, phb0 = 0u, phb1 = 0u;
     int buf = 0;
     for (int k = k_begin; k < k_end; ++k, buf ^= 1) {
+        // every thread waits for the halo tile itself; a failed wait (here or
+        // for the base tile) leaves the chunk's shared-memory results unused
+        // and reaches every thread at the CTA barrier that ends the chunk
         if (!failed && !mbar_wait_bounded(&bars[buf], buf ? phx1 : phx0, a.wait_cycles))
             failed = true;
-        if (buf) phx1 ^= 1u; else phx0 ^= 1u;
-        pend &= ~(1u << buf);
-        // no CTA barrier here: each thread has waited for the halo tile itself,
-        // D1 was last read before the previous chunk's third barrier, and a
-        // failed wait reaches every thread through the next barrier
         const E* Xb = X + buf * XT;
         const double V1 = vgrid[ip1], V2 = vgrid[Np1 + ip2];
 
-        // ---- phase A: q1 faces of rows a_row, a_row+1 -> D1 -------------------
-        {
+        if (q1w) {
+            // ---- q1 faces of rows lp, lp+1, BGK -> D1 --------------------------
+            // D1 of the previous chunk was last read before its closing barrier
             const E v1 = E(V1);
             const bool right = v1 > E(0);
             Side S; S.set(right);
-            const E* ra = Xb + ((a_row + HALO) * HX + a_c0 + (right ? 0 : 1)) * PW + lane;
+            const E* ra = Xb + ((lp + HALO) * HX + (right ? 0 : 1)) * PW + lane;
             const E* rb = ra + HX * PW;
             P y0 = mk2(ra[0 * PW], rb[0 * PW]);
             P y1 = mk2(ra[1 * PW], rb[1 * PW]);
@@ -301,67 +304,68 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             Walker W;
             const P vq = f2(E(0.5) * v1 * inv_dq1);   // walker returns 2x face value
             P Fprev = W.first(y0, y1, y2, y3, y4, S);
-            E* da = d1s + (a_row * TQ + a_c0) * PW + lane;
+            E* da = d1s + lp * TQ * PW + lane;
+            const P* t1 = tb_row + ip1 * kTabPitch;
+            const P* t2 = tb_row + (Np1 + ip2) * kTabPitch;
+            const P* t3 = tb_row + (Np1 + Np2 + ip3) * kTabPitch;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
+            for (int c = 0; c < TQ; ++c) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
                 y4 = mk2(ra[(c + 5) * PW], rb[(c + 5) * PW]);
                 const P Fn = W.next(y0, y1, y2, y3, y4, S);
-                const P d = mul2(sub2(Fprev, Fn), vq);
+                P d = mul2(sub2(Fprev, Fn), vq);
+                Fprev = Fn;
+                if (BGK) {
+                    // the cell itself is the window's y2 (right-moving) or y1
+                    const P fcell = right ? y2 : y1;
+                    const P f0 = mul2(mul2(t1[c], t2[c]), t3[c]);
+                    d = fma2(sub2(f0, fcell), inv_tau, d);
+                }
                 da[c * PW] = d.x;
                 da[(TQ + c) * PW] = d.y;
-                Fprev = Fn;
             }
-        }
-        // the store of chunk k-1 must be done reading the staging tiles, and
-        // the base tiles of chunk k must have landed, before phase B
-        if (warp == 0) bulk_wait_read_all();
-        if (!BX) {
-            if (!failed && !mbar_wait_bounded(&bars[2 + buf], buf ? phb1 : phb0, a.wait_cycles))
-                failed = true;
-            if (buf) phb1 ^= 1u; else phb0 ^= 1u;
-            pend &= ~(4u << buf);
-        }
-        failed = __syncthreads_or(failed);                        // barrier 1
-        if (failed) break;
-
-        // ---- phase B: q2 faces of cols b_col, b_col+1, BGK, combine ------------
-        {
+            // the store of chunk k-1 must be done reading the staging tiles
+            // before the q2 walkers write them
+            if (warp == 0) bulk_wait_read_all();
+            named_bar_arrive(1, NTHREADS);
+        } else {
+            // ---- q2 faces of columns lp, lp+1, then combine with D1 ---------------
             const E v2 = E(V2);
             const bool right = v2 > E(0);
             Side S; S.set(right);
-            const E* ca = Xb + ((b_r0 + (right ? 0 : 1)) * HX + b_col + HALO) * PW + lane;
+            const E* ca = Xb + ((right ? 0 : 1) * HX + lp + HALO) * PW + lane;
             const E* cb = ca + PW;
-            const E* cella = Xb + ((b_r0 + HALO) * HX + b_col + HALO) * PW + lane;
             P y0 = mk2(ca[0 * HX * PW], cb[0 * HX * PW]);
             P y1 = mk2(ca[1 * HX * PW], cb[1 * HX * PW]);
             P y2 = mk2(ca[2 * HX * PW], cb[2 * HX * PW]);
             P y3 = mk2(ca[3 * HX * PW], cb[3 * HX * PW]);
             P y4 = mk2(ca[4 * HX * PW], cb[4 * HX * PW]);
             Walker W;
-            const P vq = f2(E(0.5) * v2 * inv_dq2);   // walker returns 2x face value
             P Fprev = W.first(y0, y1, y2, y3, y4, S);
-            const int cb0 = b_r0 * TQ + b_col;                   // q-cell of row 0, col b_col
-            const E* dk = d1s + cb0 * PW + lane;
-            const E* bb1 = b1s + buf * TE + cb0 * PW + lane;
-            E* ob1 = o1s + cb0 * CS;
-            E* ob2 = o2s + cb0 * PW + lane;
-            const P* t1 = tb_row + ip1 * kTabPitch;
-            const P* t2 = tb_row + (Np1 + ip2) * kTabPitch;
-            const P* t3 = tb_row + (Np1 + Np2 + ip3) * kTabPitch;
+            P dq[TQ];                                  // flux differences of rows 0..7
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
+            for (int r = 0; r < TQ; ++r) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
                 y4 = mk2(ca[(r + 5) * HX * PW], cb[(r + 5) * HX * PW]);
                 const P Fn = W.next(y0, y1, y2, y3, y4, S);
-                const P kq = mk2(dk[r * TQ * PW], dk[r * TQ * PW + PW]);
-                P kk = fma2(sub2(Fprev, Fn), vq, kq);
+                dq[r] = sub2(Fprev, Fn);
                 Fprev = Fn;
-                const P fcell = mk2(cella[r * HX * PW], cella[r * HX * PW + PW]);
-                if (BGK) {
-                    const P f0 = mul2(mul2(t1[r * 4], t2[r * 4]), t3[r * 4]);
-                    kk = fma2(sub2(f0, fcell), inv_tau, kk);
-                }
+            }
+            if (!BX && !failed &&
+                !mbar_wait_bounded(&bars[2 + buf], buf ? phb1 : phb0, a.wait_cycles))
+                failed = true;
+            named_bar_sync(1, NTHREADS);              // D1 written, staging tiles free
+            const P vq = f2(E(0.5) * v2 * inv_dq2);
+            const E* dk = d1s + lp * PW + lane;
+            const E* bb1 = b1s + buf * TE + lp * PW + lane;
+            const E* cella = Xb + (HALO * HX + lp + HALO) * PW + lane;
+            E* ob1 = o1s + lp * CS;
+            E* ob2 = o2s + lp * PW + lane;
+#pragma unroll
+            for (int r = 0; r < TQ; ++r) {
+                const P kq = mk2(dk[r * TQ * PW], dk[r * TQ * PW + PW]);
+                const P kk = fma2(dq[r], vq, kq);
+                const P fcell = BX ? mk2(cella[r * HX * PW], cella[r * HX * PW + PW]) : kk;
                 const P o1 = KOUT ? kk
                                   : fma2(kk, c1, BX ? fcell : mk2(bb1[r * TQ * PW],
                                                                   bb1[r * TQ * PW + PW]));
@@ -376,7 +380,10 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             }
         }
         fence_proxy_async();       // staging writes -> visible to the bulk-copy proxy
-        __syncthreads();                                          // barrier 2
+        failed = __syncthreads_or(failed);                        // closes the chunk
+        if (failed) break;
+        if (buf) { phx1 ^= 1u; phb1 ^= 1u; } else { phx0 ^= 1u; phb0 ^= 1u; }
+        pend &= ~(5u << buf);
         if (tid == 0) {
             tma_store_3d(&a.tm_o1, o1s, xs + k * PW, i0 + Ng, j0 + Ng);
             if (F64)        // second half of the 32 p (the swizzled rows hold 16)
