@@ -92,15 +92,16 @@ __device__ __forceinline__ void bulk_reduce_add_f64(double* gdst, const double* 
                  ::"l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes) : "memory");
 }
 
-// Prologue: p-cell centres of the species, barriers, and for BGK the
-// Maxwellian of the stage input per q-cell with exp tables stored as element
+// Prologue (the tile loads already in flight): p-cell centres of the species,
+// and for BGK the Maxwellian of the stage input per q-cell with exp tables
+// over the p1 and p2 cells and the CTA's p3 rows [p3lo, p3lo + n3) stored as element
 // pairs over q-cell pairs P = m*8 + col (cells of rows 2m and 2m+1 in one tile
 // column, the pair a q1 walker holds): tab[q*kTabPitch + P], the pitch of 33
 // pairs keeping a warp's reads of different q (one per lane) on distinct banks.
 template <typename E, bool BGK>
 __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i0, int j0,
                                                double* vgrid, double* qc,
-                                               typename PairOf<E>::P* tabs, uint64_t* bars) {
+                                               typename PairOf<E>::P* tabs, int p3lo, int n3) {
     const int tid = threadIdx.x;
     const int Np1 = a.Np1, Np2 = a.Np2;
     const int ntab = Np1 + Np2 + a.Np3;
@@ -109,17 +110,6 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
         else if (q < Np1 + Np2) vgrid[q] = a.sg.p2_start[s] + (0.5 + (q - Np1)) * a.sg.dp2[s];
         else vgrid[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
     }
-    if (tid == 0) {
-        prefetch_tmap(&a.tmap);
-        prefetch_tmap(&a.tm_b1);
-        prefetch_tmap(&a.tm_o1);
-        prefetch_tmap(&a.tm_o2);
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        mbar_init(&bars[2], 1);
-        mbar_init(&bars[3], 1);
-        fence_barrier_init();
-    }
     if (BGK) {
         for (int c = tid; c < 64; c += NTHREADS)
             bgk_cell_params(a, s, i0 + (c & 7), j0 + (c >> 3), qc + c * 5);
@@ -127,10 +117,12 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
     __syncthreads();
     if (BGK) {
         const double m = a.sg.mass[s];
-        for (int e = tid; e < 32 * ntab; e += NTHREADS) {
-            const int q = e >> 5, P = e & 31;
+        const int n12 = Np1 + Np2;
+        for (int e = tid; e < 32 * (n12 + n3); e += NTHREADS) {
+            const int r = e >> 5, P = e & 31;          // table row r: p1, p2, then p3 rows
+            const int q = r < n12 ? r : r + p3lo;      // its p-cell in the p-cell centres
             const int c0 = (P >> 3) * 16 + (P & 7);
-            tabs[q * kTabPitch + P] = mk2(E(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
+            tabs[r * kTabPitch + P] = mk2(E(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
                                           E(bgk_table_entry(a, qc + (c0 + 8) * 5, vgrid, q, m)));
         }
     }
@@ -199,7 +191,17 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const bool border = ((a.periodic1 || peer1) && (i0 < Ng || i0 + TQ > Nq1 - Ng)) ||
                         ((a.periodic2 || peer2) && (j0 < Ng || j0 + TQ > Nq2 - Ng));
 
-    qpair_prologue<E, BGK>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, bars);
+    if (tid == 0) {
+        prefetch_tmap(&a.tmap);
+        prefetch_tmap(&a.tm_b1);
+        prefetch_tmap(&a.tm_o1);
+        prefetch_tmap(&a.tm_o2);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
+        mbar_init(&bars[3], 1);
+        fence_barrier_init();
+    }
 
     bool failed = false;
     unsigned pend = 0u;        // thread 0: barriers with a load in flight
@@ -218,12 +220,18 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             tma_load_3d(b1s + b * TE, &a.tm_b1, &bars[2 + b], xs + k * PW, i0 + Ng, j0 + Ng);
         }
     };
+    // the first tiles load while the tables are built: thread 0 initialised
+    // the barriers itself, the other threads reach them after the prologue
     if (tid == 0) {
         load_x(k_begin, 0);
         load_x(k_begin + 1, 1);
         load_b(k_begin, 0);
         load_b(k_begin + 1, 1);
     }
+    // p3 rows of this CTA's p-range (the tables hold only those)
+    const int p3lo = (k_begin * PW) / (Np1 * Np2);
+    const int n3 = k_begin < k_end ? (k_end * PW - 1) / (Np1 * Np2) - p3lo + 1 : 0;
+    qpair_prologue<E, BGK>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, p3lo, n3);
 
     E* __restrict__ out1 = static_cast<E*>(a.out1);
     const P c1 = f2(E(a.c1)), c2 = f2(E(a.c2));
@@ -307,7 +315,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             E* da = d1s + lp * TQ * PW + lane;
             const P* t1 = tb_row + ip1 * kTabPitch;
             const P* t2 = tb_row + (Np1 + ip2) * kTabPitch;
-            const P* t3 = tb_row + (Np1 + Np2 + ip3) * kTabPitch;
+            const P* t3 = tb_row + (Np1 + Np2 + ip3 - p3lo) * kTabPitch;
 #pragma unroll
             for (int c = 0; c < TQ; ++c) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
