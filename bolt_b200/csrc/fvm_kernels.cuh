@@ -73,22 +73,12 @@ __device__ __forceinline__ void write_ghost_images(T* out, T v, int ii, int jj, 
 // qq = {n*A, u1, u2, u3, 2 kB T} with A the normalisation of the p_dim-D
 // Maxwellian.  Cells outside the grid get the parameters of zero moments.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void bgk_cell_params(const QStageArgs& a, int s, int ii, int jj,
-                                                double* qq) {
-    const int Nq1 = a.Nq1, Nq2 = a.Nq2;
+// the parameters from the moment sums mm (sum over the partial slots)
+__device__ __forceinline__ void bgk_params_from_sums(const QStageArgs& a, int s, const double* mm,
+                                                     double* qq) {
     const double m = a.sg.mass[s];
     const double kB = a.kB;
     const double measure = (a.sg.dp3[s] * a.sg.dp2[s]) * a.sg.dp1[s];
-    const long long plane = (long long)Nq2 * Nq1;
-    double mm[kNumMom] = {0, 0, 0, 0, 0};
-    if (ii < Nq1 && jj < Nq2) {
-        for (int sp = 0; sp < a.nsplit_in; ++sp) {
-#pragma unroll
-            for (int q = 0; q < kNumMom; ++q)
-                mm[q] += a.mom_in[(((long long)sp * kNumMom + q) * a.Ns + s) * plane
-                                  + (long long)jj * Nq1 + ii];
-        }
-    }
     const double eps = 1e-30;
     double n = mm[0] * measure;
     double u1 = (mm[1] * measure) / (n + eps);
@@ -106,6 +96,29 @@ __device__ __forceinline__ void bgk_cell_params(const QStageArgs& a, int s, int 
     qq[2] = u2;
     qq[3] = u3;
     qq[4] = twokT;
+}
+
+// moment q of q-cell (ii, jj): the partial slots summed in slot order
+__device__ __forceinline__ double bgk_moment_sum(const QStageArgs& a, int s, int ii, int jj,
+                                                 int q) {
+    const long long plane = (long long)a.Nq2 * a.Nq1;
+    double v = 0.0;
+    if (ii < a.Nq1 && jj < a.Nq2) {
+        const double* src = a.mom_in + ((long long)q * a.Ns + s) * plane +
+                            (long long)jj * a.Nq1 + ii;
+        const long long step = (long long)kNumMom * a.Ns * plane;
+#pragma unroll 4
+        for (int sp = 0; sp < a.nsplit_in; ++sp) v += src[sp * step];
+    }
+    return v;
+}
+
+__device__ __forceinline__ void bgk_cell_params(const QStageArgs& a, int s, int ii, int jj,
+                                                double* qq) {
+    double mm[kNumMom];
+#pragma unroll
+    for (int q = 0; q < kNumMom; ++q) mm[q] = bgk_moment_sum(a, s, ii, jj, q);
+    bgk_params_from_sums(a, s, mm, qq);
 }
 
 // exp table entry q of a q-cell: p1 entries carry n*A, inactive axes are 1

@@ -111,19 +111,65 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
         else vgrid[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
     }
     if (BGK) {
+        // the 64 cells' moment sums, one (cell, moment) per thread so that the
+        // partial-slot loads of all cells are in flight together, then each
+        // cell's parameters from its sums
+        double* mm = qc + 64 * kNumMom;
+        for (int e = tid; e < 64 * kNumMom; e += NTHREADS) {
+            const int c = e & 63, q = e >> 6;
+            mm[c * kNumMom + q] = bgk_moment_sum(a, s, i0 + (c & 7), j0 + (c >> 3), q);
+        }
+        __syncthreads();
         for (int c = tid; c < 64; c += NTHREADS)
-            bgk_cell_params(a, s, i0 + (c & 7), j0 + (c >> 3), qc + c * 5);
+            bgk_params_from_sums(a, s, mm + c * kNumMom, qc + c * 5);
     }
     __syncthreads();
     if (BGK) {
+        // One (q-cell, axis) per thread: the axis's exp factors
+        // e_j = exp(-beta x_j^2), x_j = v_j - u, beta = m / (2 kB T), from the
+        // row nearest u outwards by e_{j+1} = e_j g_j, g_{j+1} = g_j exp(-2 beta dv^2)
+        // (and mirrored below it), so each factor shrinks away from the maximum
+        // and nothing overflows; three exps per axis instead of one per row.  The
+        // products carry about j^2/2 roundings (under 1e-13 relative at 24 rows).
         const double m = a.sg.mass[s];
         const int n12 = Np1 + Np2;
-        for (int e = tid; e < 32 * (n12 + n3); e += NTHREADS) {
-            const int r = e >> 5, P = e & 31;          // table row r: p1, p2, then p3 rows
-            const int q = r < n12 ? r : r + p3lo;      // its p-cell in the p-cell centres
-            const int c0 = (P >> 3) * 16 + (P & 7);
-            tabs[r * kTabPitch + P] = mk2(E(bgk_table_entry(a, qc + c0 * 5, vgrid, q, m)),
-                                          E(bgk_table_entry(a, qc + (c0 + 8) * 5, vgrid, q, m)));
+        E* tel = reinterpret_cast<E*>(tabs);
+        for (int t = tid; t < 64 * 3; t += NTHREADS) {
+            const int c = t & 63, ax = t >> 6;
+            const double* qq = qc + c * 5;
+            // the table column of cell c: pair P, component hi (row 2m+1 of the pair)
+            E* col = tel + 2 * ((c >> 4) * 8 + (c & 7)) + ((c >> 3) & 1);
+            const int r0 = ax == 0 ? 0 : (ax == 1 ? Np1 : n12);
+            const int nr = ax == 0 ? Np1 : (ax == 1 ? Np2 : n3);
+            const int q0 = ax == 2 ? n12 + p3lo : r0;           // p-cell of row r0
+            const double dv = ax == 0 ? a.sg.dp1[s] : (ax == 1 ? a.sg.dp2[s] : a.sg.dp3[s]);
+            const double scale = ax == 0 ? qq[0] : 1.0;         // p1 rows carry n*A
+            const bool act = ax == 0 || (ax == 1 ? a.p_dim >= 2 : a.p_dim == 3);
+            E* out = col + 2 * kTabPitch * r0;
+            if (!act) {
+                for (int j = 0; j < nr; ++j) out[2 * kTabPitch * j] = E(scale);
+                continue;
+            }
+            const double u = qq[1 + ax], beta = m / qq[4];
+            int jc = (int)floor((u - vgrid[q0]) / dv + 0.5);
+            jc = min(max(jc, 0), nr - 1);
+            const double x = vgrid[q0 + jc] - u;
+            const double e = exp(-beta * (x * x));
+            const double cc = exp(-2.0 * beta * (dv * dv));
+            out[2 * kTabPitch * jc] = E(scale * e);
+            double ej = e, g = exp(-beta * fma(2.0 * x, dv, dv * dv));
+            for (int j = jc + 1; j < nr; ++j) {
+                ej *= g;
+                g *= cc;
+                out[2 * kTabPitch * j] = E(scale * ej);
+            }
+            ej = e;
+            g = exp(-beta * fma(-2.0 * x, dv, dv * dv));
+            for (int j = jc - 1; j >= 0; --j) {
+                ej *= g;
+                g *= cc;
+                out[2 * kTabPitch * j] = E(scale * ej);
+            }
         }
     }
     __syncthreads();
