@@ -73,7 +73,10 @@ __device__ __forceinline__ void write_ghost_images(T* out, T v, int ii, int jj, 
 // qq = {n*A, u1, u2, u3, 2 kB T} with A the normalisation of the p_dim-D
 // Maxwellian.  Cells outside the grid get the parameters of zero moments.
 // ---------------------------------------------------------------------------
-// the parameters from the moment sums mm (sum over the partial slots)
+// the parameters from the moment sums mm (sum over the partial slots);
+// SQRT_POW: the 3-D normalisation base^1.5 as base*sqrt(base) (within an ulp
+// or two of pow, which the reference-order path keeps)
+template <bool SQRT_POW = false>
 __device__ __forceinline__ void bgk_params_from_sums(const QStageArgs& a, int s, const double* mm,
                                                      double* qq) {
     const double m = a.sg.mass[s];
@@ -90,7 +93,8 @@ __device__ __forceinline__ void bgk_params_from_sums(const QStageArgs& a, int s,
                                     - nm * (u3 * u3))) / (n + eps) + eps;
     double twokT = (2.0 * kB) * Tt;
     double base = m / ((2.0 * 3.141592653589793 * kB) * Tt);
-    double A = a.p_dim == 3 ? pow(base, 1.5) : (a.p_dim == 2 ? base : sqrt(base));
+    const double rb = sqrt(base);
+    double A = a.p_dim == 3 ? (SQRT_POW ? base * rb : pow(base, 1.5)) : (a.p_dim == 2 ? base : rb);
     qq[0] = n * A;
     qq[1] = u1;
     qq[2] = u2;

@@ -111,17 +111,54 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
         else vgrid[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
     }
     if (BGK) {
-        // the 64 cells' moment sums, one (cell, moment) per thread so that the
-        // partial-slot loads of all cells are in flight together, then each
-        // cell's parameters from its sums
+        // the 64 cells' moment sums: thread t sums moment t/64 of cell t%64
+        // (threads 0-63 also moment 4), all its partial-slot loads issued
+        // before the first add, so the CTA waits for one round of loads; then
+        // each cell's parameters from its sums
+        static_assert(NTHREADS == 256 && kNumMom == 5, "moment-sum mapping");
         double* mm = qc + 64 * kNumMom;
-        for (int e = tid; e < 64 * kNumMom; e += NTHREADS) {
-            const int c = e & 63, q = e >> 6;
-            mm[c * kNumMom + q] = bgk_moment_sum(a, s, i0 + (c & 7), j0 + (c >> 3), q);
+        {
+            const int c = tid & 63, q = tid >> 6;
+            const int ii = i0 + (c & 7), jj = j0 + (c >> 3);
+            const long long plane = (long long)a.Nq2 * a.Nq1;
+            const long long step = (long long)kNumMom * a.Ns * plane;
+            const double* src = a.mom_in + ((long long)q * a.Ns + s) * plane +
+                                (long long)jj * a.Nq1 + ii;
+            const double* src4 = src + 4 * (long long)a.Ns * plane;
+            double v = 0.0, v4 = 0.0;
+            const int n = a.nsplit_in;
+            int sp = 0;
+            if (q == 0) {
+                for (; sp + 4 <= n; sp += 4) {
+                    double l[4], l4[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        l[i] = src[(sp + i) * step];
+                        l4[i] = src4[(sp + i) * step];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        v += l[i];
+                        v4 += l4[i];
+                    }
+                }
+                for (; sp < n; ++sp) { v += src[sp * step]; v4 += src4[sp * step]; }
+                mm[c * kNumMom + 4] = v4;
+            } else {
+                for (; sp + 8 <= n; sp += 8) {
+                    double l[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) l[i] = src[(sp + i) * step];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) v += l[i];
+                }
+                for (; sp < n; ++sp) v += src[sp * step];
+            }
+            mm[c * kNumMom + q] = v;
         }
         __syncthreads();
         for (int c = tid; c < 64; c += NTHREADS)
-            bgk_params_from_sums(a, s, mm + c * kNumMom, qc + c * 5);
+            bgk_params_from_sums<true>(a, s, mm + c * kNumMom, qc + c * 5);
     }
     __syncthreads();
     if (BGK) {
