@@ -99,6 +99,8 @@ SIGNATURES = {
     'bolt_stage': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
     'bolt_stage_parts': (ctypes.c_int, [_VP, ctypes.c_int]),
     'bolt_stage_part': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, ctypes.c_int, _VP]),
+    'bolt_stage_region': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                         _VP]),
     'bolt_fields_yee': (_VP, [_VP]),
     'bolt_set_peer_halos': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     'bolt_set_peer_halos_q1': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),

@@ -660,8 +660,11 @@ struct StageIO {
 };
 
 // q-part of one stage.  write_k: out1 <- k_q (no moments, no ghosts).
+// region -1: every q-tile; 0: the tiles whose stencils stay inside the block
+// along its external axes; 1: the other tiles (0 and 1 need the paired
+// kernel: BOLT_ERR_UNSUPPORTED, with nothing launched, where it does not run)
 static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_j,
-                         cudaStream_t st) {
+                         cudaStream_t st, int region = -1) {
     TimedScope ts(ctx, BOLT_TIMING_QSTAGE, st);
     const BoltGrid& g = ctx->g;
     QStageArgs a;
@@ -707,6 +710,10 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
     a.nsplit = ctx->nsplit;
     a.chunks_per_split = ctx->chunks_per_split;
     a.ntiles1 = ctx->ntiles1;
+    a.ntiles2 = ctx->ntiles2;
+    a.ext1 = ctx->p.bc_q1 == BOLT_BC_EXTERNAL;
+    a.ext2 = ctx->p.bc_q2 == BOLT_BC_EXTERNAL;
+    a.tile_sel = region < 0 ? 0 : region + 1;
     a.p_dim = ctx->p.p_dim;
     a.want_j = want_j;
     a.bgk_direct = ctx->bgk_direct;
@@ -744,6 +751,14 @@ static int launch_qstage(BoltCtx* ctx, const StageIO& io, int write_k, int want_
         if (pair && a.out2) {
             if ((m = get_tmap(ctx, a.out2, TMAP_TILE))) a.tm_o2 = *m; else pair = false;
         }
+    }
+    if (region >= 0) {
+        if (!pair) return BOLT_ERR_UNSUPPORTED;
+        const int n1 = ctx->ntiles1, n2 = ctx->ntiles2;
+        const int inner = std::max(0, n1 - 2 * a.ext1) * std::max(0, n2 - 2 * a.ext2);
+        const int count = region == 0 ? inner : n1 * n2 - inner;
+        if (count == 0) return BOLT_OK;
+        grid.x = (unsigned)count;
     }
     const size_t smem = pair ? qpair_smem(ctx->ntab, ctx->bgk, ctx->elem)
                              : qstage_smem(ctx->tiling, ctx->elem, ctx->bgk, ctx->bgk_direct,
@@ -860,10 +875,10 @@ static int launch_electrostatic(BoltCtx* ctx, const void* f, cudaStream_t st) {
 // ghosts exchanged between them (0: q-part, currents, halo; 1: E update;
 // 2: B update, cell fields, p-part)
 static int run_stage(BoltCtx* ctx, StageIO io, int evolve, double dt, cudaStream_t st,
-                     int part = -1) {
+                     int part = -1, int region = -1) {
     int rc;
     if (!ctx->p.fields_enabled) {
-        rc = launch_qstage(ctx, io, 0, 0, st);
+        rc = launch_qstage(ctx, io, 0, 0, st, region);
     } else if (electrostatic(ctx)) {
         rc = launch_electrostatic(ctx, io.fs, st);
         StageIO qio = io;
@@ -939,10 +954,21 @@ static int stage_parts(const BoltCtx* ctx, int k) {
     return ext && stage_evolves(ctx, k) ? 3 : 1;
 }
 
+// region (see launch_qstage): -1 the whole stage; 0 the q-tiles whose stencils
+// stay inside a block along its external axes, nothing else; 1 the other
+// tiles, then the rest of the stage.  0 and 1 need a stage without fields on
+// the paired kernel, no peer halos, and (stage 0) the ghosts and moments of f
+// current; otherwise they return BOLT_ERR_UNSUPPORTED having launched nothing.
 static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st,
-                        int part = -1) {
+                        int part = -1, int region = -1) {
     StageRange range(k);
     int rc = BOLT_OK;
+    if (region >= 0) {
+        const bool current = ctx->ghost_owner == f && !ctx->ghost_stale_time &&
+                             (!ctx->bgk || ctx->mom_owner == f);
+        if (ctx->p.fields_enabled || ctx->peer_on || (k == 0 && !current))
+            return BOLT_ERR_UNSUPPORTED;
+    }
     // with parts: the bookkeeping happens once, after the last part
     const bool first_part = part <= 0, last_part = part < 0 || part == 2;
     if (k == 0 && first_part) {
@@ -992,7 +1018,8 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         io.out1 = out1 = k == 0 ? A : f;
         peers_of(out1);
         ev = fe && !ctx->at_n;
-        rc = run_stage(ctx, io, ev, dt, st, ev ? part : -1);
+        rc = run_stage(ctx, io, ev, dt, st, ev ? part : -1, region);
+        if (region == 0) return rc;
         if (fe && last_part) ctx->at_n ^= 1;
     } else {
         // classic RK4 (integrators.py:15-28) in accumulator form:
@@ -1018,7 +1045,9 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         io.out1 = out1 = stages[k].o1; io.base2 = stages[k].b2; io.c2 = stages[k].c2;
         io.out2 = stages[k].o2;
         peers_of(out1);
-        rc = run_stage(ctx, io, fe && stages[k].ev, dt, st, fe && stages[k].ev ? part : -1);
+        rc = run_stage(ctx, io, fe && stages[k].ev, dt, st, fe && stages[k].ev ? part : -1,
+                       region);
+        if (region == 0) return rc;
     }
     if (!last_part) return rc;
     if (!rc && dir) rc = launch_ghosts(ctx, out1, st);
@@ -1090,6 +1119,12 @@ void* bolt_stage_input(BoltCtx* ctx, void* f_dev, int k) {
 int bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream) {
     if (!ctx || !f_dev || k < 0 || k >= stage_count(ctx)) return BOLT_ERR_ARG;
     return run_rk_stage(ctx, f_dev, dt, k, (cudaStream_t)stream);
+}
+
+int bolt_stage_region(BoltCtx* ctx, void* f_dev, double dt, int k, int region, void* stream) {
+    if (!ctx || !f_dev || k < 0 || k >= stage_count(ctx) || region < 0 || region > 1)
+        return BOLT_ERR_ARG;
+    return run_rk_stage(ctx, f_dev, dt, k, (cudaStream_t)stream, -1, region);
 }
 
 int bolt_stage_parts(BoltCtx* ctx, int k) {

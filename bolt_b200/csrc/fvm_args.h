@@ -136,6 +136,10 @@ struct QStageArgs {
     SpeciesGrid sg;
     // paired kernel only: 8x8x32 boxes over base1, out1 (128B swizzle), out2
     CUtensorMap tm_b1, tm_o1, tm_o2;
+    // paired kernel only: which q-tiles the grid's columns cover -- all (0),
+    // the tiles whose halo stays inside the block along its external axes
+    // ext1 (q1) / ext2 (q2) (1), or the remaining ones (2); ntiles2 tile rows
+    int tile_sel, ext1, ext2, ntiles2;
     // q2 slab neighbours' copies of out1 (or null): the bottom N_g interior
     // rows are also stored N_q2 rows higher in peer_lo (the lower neighbour's
     // top ghost rows), the top N_g rows N_q2 rows lower in peer_hi

@@ -212,6 +212,45 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
     __syncthreads();
 }
 
+// The q-tile of grid column bx: row-major over every tile (tile_sel 0), over
+// the tiles whose halo stays inside the block's interior along its external
+// axes (1: tile columns 1..n1-2 if q1 is external, rows 1..n2-2 if q2 is), or
+// over the others (2: the bottom rows, then the outer columns of the middle
+// rows, then the top rows).  An 8x8 tile's halo reaches 3 cells past it, so
+// only the outermost tiles read ghost cells.
+__device__ __forceinline__ void qpair_tile(const QStageArgs& a, int bx, int& t1, int& t2) {
+    const int n1 = a.ntiles1, n2 = a.ntiles2;
+    if (a.tile_sel == 0) {
+        t1 = bx % n1;
+        t2 = bx / n1;
+        return;
+    }
+    const int e1 = a.ext1 ? 1 : 0, e2 = a.ext2 ? 1 : 0;
+    if (a.tile_sel == 1) {
+        const int w = n1 - 2 * e1;
+        t1 = e1 + bx % w;
+        t2 = e2 + bx / w;
+        return;
+    }
+    if (bx < e2 * n1) {                         // bottom rows
+        t1 = bx % n1;
+        t2 = bx / n1;
+        return;
+    }
+    bx -= e2 * n1;
+    const int mid = max(0, n2 - 2 * e2);        // middle rows
+    const int m = n1 > 2 * e1 ? 2 * e1 : n1;    // their border tiles
+    if (bx < mid * m) {
+        t2 = e2 + bx / m;
+        const int c = bx % m;
+        t1 = m == n1 ? c : (c < e1 ? c : n1 - 2 * e1 + c);
+        return;
+    }
+    bx -= mid * m;                              // top rows
+    t1 = bx % n1;
+    t2 = n2 - e2 + bx / n1;
+}
+
 // Stage modes (which of out1 = base1 + c1 k, out2 = base2 + c2 k exist and
 // where their bases come from):
 //   QP_X1   base1 = stage input (from the halo tile), out1 only
@@ -263,7 +302,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + Lo.bars);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tile1 = blockIdx.x % a.ntiles1, tile2 = blockIdx.x / a.ntiles1;
+    int tile1, tile2;
+    qpair_tile(a, (int)blockIdx.x, tile1, tile2);
     const int s = blockIdx.y / a.nsplit, split = blockIdx.y % a.nsplit;
     const int i0 = tile1 * TQ, j0 = tile2 * TQ;
     const int k_begin = split * a.chunks_per_split;

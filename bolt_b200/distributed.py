@@ -217,7 +217,8 @@ class BlockSolver(object):
     blocks in one process, stepped in lockstep through begin_step /
     stage_input / stage / end_step)."""
 
-    def __init__(self, physical_system, dims, group=None, block=None, external=None):
+    def __init__(self, physical_system, dims, group=None, block=None, external=None,
+                 overlap=True):
         from .physical_system import physical_system as PS
         from .nonlinear_solver import nonlinear_solver
         ps = physical_system
@@ -283,6 +284,10 @@ class BlockSolver(object):
         self.time_elapsed = 0.0
         self._peer = False          # peer halos off: exchange before every stage
         self._halos_ready = False
+        # exchange on a side stream beside the stage's inner tiles (see
+        # overlapped_stage); False: exchange, then the whole stage
+        self.overlap = bool(overlap)
+        self._comm = None
         # neighbour ranks: (left, right) along q1, (down, up) along q2
         at = lambda a, b: (a % P1) + P1 * (b % P2)
         self.q1_neighbours = (at(r1 - 1, r2), at(r1 + 1, r2))
@@ -383,6 +388,36 @@ class BlockSolver(object):
     def stage(self, k, dt):
         self.local.stage(k, dt)
 
+    def stage_region(self, k, region, dt):
+        """Region 0 (the q-tiles that read no ghost cell of a cut axis) or 1
+        (the rest, then the stage's end) of stage k; False when the stage
+        cannot be split (nothing was run)."""
+        return self.local.stage_region(k, region, dt)
+
+    def overlapped_stage(self, k, dt):
+        """Stage k with its input's halo exchange overlapped: the exchange runs
+        on a side stream (after everything already queued on the solver's
+        stream) while the tiles whose stencils stay inside the block run on
+        the solver's stream; the solver's stream then waits for the exchange
+        and runs the outer tiles.  Falls back to exchange-then-stage when the
+        stage cannot be split (fields, the scalar kernel, the first stage
+        after f was set from outside)."""
+        loc = self.local
+        main = torch.cuda.current_stream(loc.device)
+        if self._comm is None:
+            self._comm = torch.cuda.Stream(loc.device)
+        comm = self._comm
+        comm.wait_stream(main)
+        with torch.cuda.stream(comm):
+            self.exchange(self.stage_input(k))
+        split = self.stage_region(k, 0, dt)
+        main.wait_stream(comm)
+        if split:
+            self.stage_region(k, 1, dt)
+        else:
+            self.stage(k, dt)
+        return split
+
     def stage_parts(self, k):
         """Parts of stage k: 3 when it advances the fields (the Yee ghosts of
         the cut axes exchanged before parts 1 and 2), else 1."""
@@ -449,13 +484,16 @@ class BlockSolver(object):
         """One step of the whole distributed run (every rank calls it)."""
         self.begin_step()
         for k in range(self.stage_count()):
-            if self.needs_exchange(k):
-                self.exchange(self.stage_input(k))
             parts = self.stage_parts(k)
-            for part in range(parts):
-                if part:
-                    self.exchange_fields()
-                self.stage_part(k, part, dt)
+            if self.overlap and parts == 1 and self.needs_exchange(k):
+                self.overlapped_stage(k, dt)
+            else:
+                if self.needs_exchange(k):
+                    self.exchange(self.stage_input(k))
+                for part in range(parts):
+                    if part:
+                        self.exchange_fields()
+                    self.stage_part(k, part, dt)
             if self._peer:
                 self._stage_barrier()
         self.end_step(dt)
@@ -522,13 +560,14 @@ class SlabSolver(BlockSolver):
     builds that slab without a process group).  With one rank the slab is the
     whole domain and its q2 halo wraps onto itself."""
 
-    def __init__(self, physical_system, group=None, slab=None):
+    def __init__(self, physical_system, group=None, slab=None, overlap=True):
         if slab is not None:
             rank, world = slab
             super(SlabSolver, self).__init__(physical_system, (1, world), group,
-                                             block=(0, rank), external=(False, True))
+                                             block=(0, rank), external=(False, True),
+                                             overlap=overlap)
         else:
             _, world = _group_info(group)
             super(SlabSolver, self).__init__(physical_system, (1, world), group,
-                                             external=(False, True))
+                                             external=(False, True), overlap=overlap)
         self.world = world

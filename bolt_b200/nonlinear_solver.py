@@ -663,6 +663,20 @@ class nonlinear_solver(object):
                                      self._stream()), 'bolt_stage')
         self._seen_version = self._fstore._version
 
+    def stage_region(self, k, region, dt):
+        """Half of RK stage k of a block (bolt_stage_region): region 0 updates
+        the q-tiles that read no ghost cell of an external axis, region 1 the
+        rest and finishes the stage.  Returns False, having done nothing, when
+        the stage cannot be split; the caller then runs stage(k, dt)."""
+        self.dt = dt
+        rc = self._lib.bolt_stage_region(self._ctx, self._fstore.data_ptr(), float(dt), int(k),
+                                         int(region), self._stream())
+        if rc == N.BOLT_ERR_UNSUPPORTED:
+            return False
+        N.check(rc, 'bolt_stage_region')
+        self._seen_version = self._fstore._version
+        return True
+
     _TERMS = {'d_flux_p1_dp1': 1, 'd_flux_p2_dp2': 2, 'd_flux_p3_dp3': 3}
 
     def df_dt(self, f=None, evolve_fields=None, term_to_return=None):

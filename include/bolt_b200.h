@@ -210,6 +210,21 @@ int   bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream);
  * part; parts 0..n-1 in order equal bolt_stage. */
 int     bolt_stage_parts(BoltCtx* ctx, int k);
 int     bolt_stage_part(BoltCtx* ctx, void* f_dev, double dt, int k, int part, void* stream);
+
+/* Stage k of a block in two halves, so that the halo exchange of its input
+ * overlaps the first (the reference exchanges, then computes:
+ * communicate.py:8-38 before each df/dt, fvm_operator.py:22-33).  region 0
+ * updates the q-tiles whose stencils stay inside the block along its external
+ * axes (every 8x8 tile but the outermost ring of tiles on those axes) and
+ * reads none of their ghost cells, so it may run while they are being filled;
+ * region 1, after the exchange, updates the other tiles and finishes the
+ * stage.  Regions 0 then 1 equal bolt_stage.  Both return
+ * BOLT_ERR_UNSUPPORTED, having launched nothing, for a stage that cannot be
+ * split: fields enabled, a stage outside the paired kernel, peer halos on, or
+ * stage 0 while the ghosts or moments of f are stale (bolt_fill_ghosts /
+ * a previous step make them current); the caller then runs bolt_stage after
+ * the exchange. */
+int     bolt_stage_region(BoltCtx* ctx, void* f_dev, double dt, int k, int region, void* stream);
 double* bolt_fields_yee(BoltCtx* ctx);
 
 /* Peer halos of a q2 slab (bc_q2 = BOLT_BC_EXTERNAL, fields off): below[] and

@@ -473,3 +473,113 @@ def test_field_blocks_in_lockstep_equal_whole_domain(dims, integrator, precision
     ftol = 1e-12 if precision == 'fp64' else 1e-4
     err = float((yb - yw).abs().max() / yw.abs().max())
     assert err < ftol, ('yee', err)
+
+
+# ---------------------------------------------------------------------------
+# Exchange overlapped with the inner tiles (bolt_stage_region)
+# ---------------------------------------------------------------------------
+def _poison_ghosts(blocks, dims, k):
+    """NaN into the cut axes' ghost cells of every block's stage-k input: a
+    region-0 update that read any of them would carry the NaN into f."""
+    P1, P2 = dims
+    Ng = blocks[0].Ng
+    for b in blocks:
+        x = b.stage_input(k)
+        if P2 > 1:
+            x[:Ng] = float('nan')
+            x[x.shape[0] - Ng:] = float('nan')
+        if P1 > 1:
+            x[:, :Ng] = float('nan')
+            x[:, x.shape[1] - Ng:] = float('nan')
+
+
+@pytest.mark.parametrize('precision,tol', [('fp32', 2e-6), ('fp64-fast', 1e-12)])
+@pytest.mark.parametrize('dims,integrator', [((1, 2), 'RK4'), ((2, 2), 'RK4'), ((1, 3), 'RK2')])
+def test_inner_tiles_need_no_ghosts(dims, integrator, precision, tol):
+    """Blocks of 24x24 q-cells (3x3 tiles) in lockstep: per stage, the cut axes'
+    ghost cells of every stage input are set to NaN, region 0 runs, then the
+    halos are exchanged and region 1 runs -- what a rank does while its
+    exchange is in flight.  After three steps the blocks equal the
+    whole-domain run, so region 0 read no ghost cell; every stage after the
+    first step split."""
+    from bolt_b200.distributed import BlockSolver
+    P1, P2 = dims
+    n = 24
+    spec = C.make(N_q1=n * P1, N_q2=n * P2, N_p1=8, N_p2=8, N_p3=4,
+                  p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+                  p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+                  tau=0.05, dt=1e-3, steps=3, integrator=integrator,
+                  riemann_q='lax-friedrichs', riemann_p='lax-friedrichs',
+                  init=dict(amp=0.1, k1=1, k2=1, u=[0.2, -0.1, 0.05]))
+    whole = make_solver(spec, precision)
+    Ng = spec['N_ghost']
+    blocks = [BlockSolver(whole.physical_system, dims, block=(r % P1, r // P1))
+              for r in range(P1 * P2)]
+    for r, b in enumerate(blocks):
+        r1, r2 = r % P1, r // P1
+        b.local.f = whole.f[:, :, r1 * n:r1 * n + n + 2 * Ng, r2 * n:r2 * n + n + 2 * Ng].clone()
+    dt = spec['dt']
+    split = []
+    for step in range(spec['steps']):
+        whole.strang_timestep(dt)
+        for b in blocks:
+            b.begin_step()
+        for k in range(blocks[0].stage_count()):
+            _poison_ghosts(blocks, dims, k)
+            done = [b.stage_region(k, 0, dt) for b in blocks]
+            _exchange_blocks(blocks, dims, k)
+            for b, d in zip(blocks, done):
+                if d:
+                    assert b.stage_region(k, 1, dt)
+                else:
+                    b.stage(k, dt)
+            if step > 0:
+                split += done
+        for b in blocks:
+            b.end_step(dt)
+    assert split and all(split)
+    cols = [torch.cat([_interior(blocks[r1 + P1 * r2].local.f, Ng) for r2 in range(P2)], dim=3)
+            for r1 in range(P1)]
+    got = torch.cat(cols, dim=2).double()
+    ref = _interior(whole.f, Ng).double()
+    err = float((got - ref).abs().max() / ref.abs().max())
+    assert err < tol, err
+
+
+@pytest.mark.parametrize('precision', ['fp32', 'fp64-fast'])
+def test_overlapped_single_slab_equals_periodic_run(precision):
+    """One slab (no process group) stepped by strang_timestep with the exchange
+    on a side stream beside the inner tiles: the run equals the periodic
+    solver to the bit, and the stages after the first split."""
+    from bolt_b200.distributed import SlabSolver
+    spec = _spec(24, 'RK4')
+    whole = make_solver(spec, precision)
+    slab = SlabSolver(whole.physical_system)
+    assert slab.overlap
+    slab.local.f = whole.f.clone()
+    calls = []
+    orig = slab.overlapped_stage
+    slab.overlapped_stage = lambda k, dt: calls.append(orig(k, dt))
+    for _ in range(spec['steps']):
+        whole.strang_timestep(spec['dt'])
+        slab.strang_timestep(spec['dt'])
+    torch.cuda.synchronize()
+    Ng = spec['N_ghost']
+    assert torch.equal(_interior(slab.local.f, Ng), _interior(whole.f, Ng))
+    assert len(calls) == 4 * spec['steps'] and calls[0] is False and all(calls[1:])
+
+
+def test_stage_region_refuses_fp64_reference_order():
+    """The FP64 reference-order kernel has no tile regions: region 0 returns
+    False (nothing run) and the stage runs whole after the exchange."""
+    from bolt_b200.distributed import SlabSolver
+    spec = _spec(24, 'RK4')
+    whole = make_solver(spec, 'fp64')
+    slab = SlabSolver(whole.physical_system)
+    slab.local.f = whole.f.clone()
+    for _ in range(2):
+        whole.strang_timestep(spec['dt'])
+        slab.strang_timestep(spec['dt'])
+    assert not slab.stage_region(1, 0, spec['dt'])
+    Ng = spec['N_ghost']
+    assert torch.equal(_interior(slab.local.f, Ng), _interior(whole.f, Ng))
