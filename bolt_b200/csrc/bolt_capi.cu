@@ -955,10 +955,11 @@ static int stage_parts(const BoltCtx* ctx, int k) {
 }
 
 // region (see launch_qstage): -1 the whole stage; 0 the q-tiles whose stencils
-// stay inside a block along its external axes, nothing else; 1 the other
-// tiles, then the rest of the stage.  0 and 1 need a stage without fields on
-// the paired kernel, no peer halos, and (stage 0) the ghosts and moments of f
-// current; otherwise they return BOLT_ERR_UNSUPPORTED having launched nothing.
+// stay inside a block along its external axes; 1 the other tiles; 2 the rest
+// of the stage (the ghost pass of non-periodic axes, the step's bookkeeping),
+// after both.  0-2 need a stage without fields on the paired kernel, no peer
+// halos, and (stage 0) the ghosts and moments of f current; otherwise they
+// return BOLT_ERR_UNSUPPORTED having launched nothing.
 static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st,
                         int part = -1, int region = -1) {
     StageRange range(k);
@@ -1018,8 +1019,8 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         io.out1 = out1 = k == 0 ? A : f;
         peers_of(out1);
         ev = fe && !ctx->at_n;
-        rc = run_stage(ctx, io, ev, dt, st, ev ? part : -1, region);
-        if (region == 0) return rc;
+        if (region != 2) rc = run_stage(ctx, io, ev, dt, st, ev ? part : -1, region);
+        if (region == 0 || region == 1) return rc;
         if (fe && last_part) ctx->at_n ^= 1;
     } else {
         // classic RK4 (integrators.py:15-28) in accumulator form:
@@ -1045,9 +1046,10 @@ static int run_rk_stage(BoltCtx* ctx, void* f, double dt, int k, cudaStream_t st
         io.out1 = out1 = stages[k].o1; io.base2 = stages[k].b2; io.c2 = stages[k].c2;
         io.out2 = stages[k].o2;
         peers_of(out1);
-        rc = run_stage(ctx, io, fe && stages[k].ev, dt, st, fe && stages[k].ev ? part : -1,
-                       region);
-        if (region == 0) return rc;
+        if (region != 2)
+            rc = run_stage(ctx, io, fe && stages[k].ev, dt, st, fe && stages[k].ev ? part : -1,
+                           region);
+        if (region == 0 || region == 1) return rc;
     }
     if (!last_part) return rc;
     if (!rc && dir) rc = launch_ghosts(ctx, out1, st);
@@ -1122,7 +1124,7 @@ int bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream) {
 }
 
 int bolt_stage_region(BoltCtx* ctx, void* f_dev, double dt, int k, int region, void* stream) {
-    if (!ctx || !f_dev || k < 0 || k >= stage_count(ctx) || region < 0 || region > 1)
+    if (!ctx || !f_dev || k < 0 || k >= stage_count(ctx) || region < 0 || region > 2)
         return BOLT_ERR_ARG;
     return run_rk_stage(ctx, f_dev, dt, k, (cudaStream_t)stream, -1, region);
 }

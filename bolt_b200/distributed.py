@@ -389,19 +389,20 @@ class BlockSolver(object):
         self.local.stage(k, dt)
 
     def stage_region(self, k, region, dt):
-        """Region 0 (the q-tiles that read no ghost cell of a cut axis) or 1
-        (the rest, then the stage's end) of stage k; False when the stage
-        cannot be split (nothing was run)."""
+        """Region 0 (the q-tiles that read no ghost cell of a cut axis), 1 (the
+        other tiles) or 2 (the stage's end, after both) of stage k; False when
+        the stage cannot be split (nothing was run)."""
         return self.local.stage_region(k, region, dt)
 
     def overlapped_stage(self, k, dt):
         """Stage k with its input's halo exchange overlapped: the exchange runs
         on a side stream (after everything already queued on the solver's
-        stream) while the tiles whose stencils stay inside the block run on
-        the solver's stream; the solver's stream then waits for the exchange
-        and runs the outer tiles.  Falls back to exchange-then-stage when the
-        stage cannot be split (fields, the scalar kernel, the first stage
-        after f was set from outside)."""
+        stream) and is followed there by the outer tiles, while the tiles
+        whose stencils stay inside the block run on the solver's stream, so
+        the outer tiles also fill the inner launch's last wave; the solver's
+        stream then waits for the side stream and finishes the stage.  Falls
+        back to exchange-then-stage when the stage cannot be split (fields,
+        the scalar kernel, the first stage after f was set from outside)."""
         loc = self.local
         main = torch.cuda.current_stream(loc.device)
         if self._comm is None:
@@ -411,10 +412,13 @@ class BlockSolver(object):
         with torch.cuda.stream(comm):
             self.exchange(self.stage_input(k))
         split = self.stage_region(k, 0, dt)
-        main.wait_stream(comm)
         if split:
-            self.stage_region(k, 1, dt)
+            with torch.cuda.stream(comm):
+                self.stage_region(k, 1, dt)
+            main.wait_stream(comm)
+            self.stage_region(k, 2, dt)
         else:
+            main.wait_stream(comm)
             self.stage(k, dt)
         return split
 

@@ -664,10 +664,11 @@ class nonlinear_solver(object):
         self._seen_version = self._fstore._version
 
     def stage_region(self, k, region, dt):
-        """Half of RK stage k of a block (bolt_stage_region): region 0 updates
+        """Part of RK stage k of a block (bolt_stage_region): region 0 updates
         the q-tiles that read no ghost cell of an external axis, region 1 the
-        rest and finishes the stage.  Returns False, having done nothing, when
-        the stage cannot be split; the caller then runs stage(k, dt)."""
+        others, region 2 finishes the stage after both.  Returns False, having
+        done nothing, when the stage cannot be split; the caller then runs
+        stage(k, dt)."""
         self.dt = dt
         rc = self._lib.bolt_stage_region(self._ctx, self._fstore.data_ptr(), float(dt), int(k),
                                          int(region), self._stream())

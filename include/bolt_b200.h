@@ -211,14 +211,16 @@ int   bolt_stage(BoltCtx* ctx, void* f_dev, double dt, int k, void* stream);
 int     bolt_stage_parts(BoltCtx* ctx, int k);
 int     bolt_stage_part(BoltCtx* ctx, void* f_dev, double dt, int k, int part, void* stream);
 
-/* Stage k of a block in two halves, so that the halo exchange of its input
- * overlaps the first (the reference exchanges, then computes:
+/* Stage k of a block in three calls, so that the halo exchange of its input
+ * overlaps computation (the reference exchanges, then computes:
  * communicate.py:8-38 before each df/dt, fvm_operator.py:22-33).  region 0
  * updates the q-tiles whose stencils stay inside the block along its external
  * axes (every 8x8 tile but the outermost ring of tiles on those axes) and
  * reads none of their ghost cells, so it may run while they are being filled;
- * region 1, after the exchange, updates the other tiles and finishes the
- * stage.  Regions 0 then 1 equal bolt_stage.  Both return
+ * region 1, once they are filled, updates the other tiles (it may run on
+ * another stream beside region 0: the two write different tiles); region 2,
+ * after both, finishes the stage (ghost pass of non-periodic axes, the step's
+ * bookkeeping).  Regions 0, 1, 2 equal bolt_stage.  Each returns
  * BOLT_ERR_UNSUPPORTED, having launched nothing, for a stage that cannot be
  * split: fields enabled, a stage outside the paired kernel, peer halos on, or
  * stage 0 while the ghosts or moments of f are stale (bolt_fill_ghosts /

@@ -498,7 +498,7 @@ def _poison_ghosts(blocks, dims, k):
 def test_inner_tiles_need_no_ghosts(dims, integrator, precision, tol):
     """Blocks of 24x24 q-cells (3x3 tiles) in lockstep: per stage, the cut axes'
     ghost cells of every stage input are set to NaN, region 0 runs, then the
-    halos are exchanged and region 1 runs -- what a rank does while its
+    halos are exchanged and regions 1 and 2 run -- what a rank does while its
     exchange is in flight.  After three steps the blocks equal the
     whole-domain run, so region 0 read no ghost cell; every stage after the
     first step split."""
@@ -530,7 +530,7 @@ def test_inner_tiles_need_no_ghosts(dims, integrator, precision, tol):
             _exchange_blocks(blocks, dims, k)
             for b, d in zip(blocks, done):
                 if d:
-                    assert b.stage_region(k, 1, dt)
+                    assert b.stage_region(k, 1, dt) and b.stage_region(k, 2, dt)
                 else:
                     b.stage(k, dt)
             if step > 0:
@@ -547,12 +547,14 @@ def test_inner_tiles_need_no_ghosts(dims, integrator, precision, tol):
 
 
 @pytest.mark.parametrize('precision', ['fp32', 'fp64-fast'])
-def test_overlapped_single_slab_equals_periodic_run(precision):
+@pytest.mark.parametrize('bc_q1', ['periodic', 'mirror'])
+def test_overlapped_single_slab_equals_periodic_run(precision, bc_q1):
     """One slab (no process group) stepped by strang_timestep with the exchange
-    on a side stream beside the inner tiles: the run equals the periodic
-    solver to the bit, and the stages after the first split."""
+    and then the outer tiles on a side stream beside the inner tiles: the run
+    equals the periodic solver to the bit, and the stages after the first
+    split."""
     from bolt_b200.distributed import SlabSolver
-    spec = _spec(24, 'RK4')
+    spec = _spec(24, 'RK4', bc_q1)
     whole = make_solver(spec, precision)
     slab = SlabSolver(whole.physical_system)
     assert slab.overlap
