@@ -346,7 +346,8 @@ def slab_result(args, rank, world, local_rank, spec):
     cells = interior_cells(spec)
     return {'value': cells / (ms * 1e-3), 'ms_per_step': ms, 'scaling': 'strong',
             'slabs': world, 'rows_per_slab': spec['N_q2'] // world,
-            'halos': 'peer stores over NVLink' if peer else 'single slab (wraps onto itself)',
+            'halos': 'peer stores over NVLink' if peer else
+                     'single slab (wraps onto itself), exchange overlapped with the inner tiles',
             'gpu_launches_per_rank': launches,
             'paired_launches_per_rank': paired}
 
