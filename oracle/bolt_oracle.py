@@ -768,3 +768,117 @@ class Oracle(object):
 
     def moments(self, name, f=None):
         return moment(self.g, self.f if f is None else f, name)
+
+    # advective semi-Lagrangian in q (asl_operators.py:20-83) --------------------
+    def asl_advect_q(self, dt):
+        """op_advect_q: ghost refresh, then every cell's value taken at the foot
+        of its characteristic, q - A_q dt with A_q = (p1, p2)
+        (advection_terms.py:29-61), by bicubic interpolation over the ghosted
+        q-plane (interpolation_routines.py:9-56)."""
+        g = self.g
+        f = self.refresh(self.exchange(self.f) if self.exchange else self.f)
+        q1c = g.q1_center[0]                     # (Nq1g,)
+        q2c = g.q2_center[:, 0]                  # (Nq2g,)
+        v1 = g.p1c[None, None]                   # (1, 1, Ns, Np3, Np2, Np1)
+        v2 = g.p2c[None, None]
+        x = ((q1c[None, :, None, None, None, None] - v1 * dt) - q1c[0]) / (q1c[1] - q1c[0])
+        if g.Nq2g > 1:
+            y = ((q2c[:, None, None, None, None, None] - v2 * dt) - q2c[0]) / (q2c[1] - q2c[0])
+        else:
+            y = np.zeros((1, 1) + v2.shape[2:]) + 0.0 * v2
+        self.f = interp2_catmull_rom(f, x, y)
+
+    def asl_source(self, dt):
+        """op_solve_src (asl_operators.py:40-83): f <- f_MB where collisions are
+        instantaneous, else one RK2 step (integrators.py:6-13) of the BGK
+        source when the source is enabled."""
+        g = self.g
+        if self.spec.get('instantaneous', False):
+            n, u1, u2, u3, T = maxwell_params(g, self.f)
+            self.f = f_maxwellian(g, n, u1, u2, u3, T)
+        elif self.spec.get('source_enabled', True):
+            x = self.f + bgk(g, self.f, self.tau) * (dt / 2)
+            self.f = self.f + bgk(g, x, self.tau) * dt
+
+    def split_step(self, dt, scheme=None):
+        """One timestep of ASL in q without fields: the splitting of op_advect_q
+        and op_solve_src named by ``scheme`` (timestep.py:39-240,
+        operator_splitting_methods.py)."""
+        scheme = scheme or self.spec.get('splitting', 'strang')
+        op1, op2 = self.asl_advect_q, self.asl_source
+
+        def strang(a, b):
+            a(0.5 * dt)
+            b(dt)
+            a(0.5 * dt)
+
+        def swss(a, b):
+            f_start = self.f
+            a(dt)
+            b(dt)
+            f_mid = self.f
+            self.f = f_start
+            b(dt)
+            a(dt)
+            self.f = 0.5 * (self.f + f_mid)
+
+        if scheme == 'strang':
+            strang(op1, op2)
+        elif scheme == 'lie':
+            op1(dt)
+            op2(dt)
+        elif scheme == 'swss':
+            swss(op1, op2)
+        elif scheme == 'jia':
+            f_start = self.f
+            strang(op1, op2)
+            f1 = self.f
+            self.f = f_start
+            strang(op2, op1)
+            f2 = self.f
+            self.f = f_start
+            swss(op1, op2)
+            self.f = (2 / 3) * (f1 + f2) - (1 / 3) * self.f
+        else:
+            raise NotImplementedError(scheme)
+        if np.any(np.isinf(self.f)) or np.any(np.isnan(self.f)):
+            raise SystemExit('Solver Diverging!')
+        self.time_elapsed += dt
+
+
+def catmull_rom(t):
+    """Weights of the Catmull-Rom cubic through samples at -1, 0, 1, 2 for a
+    point t in [0, 1) past sample 0 (Catmull and Rom 1974)."""
+    t2, t3 = t * t, t * t * t
+    return (0.5 * (-t + 2 * t2 - t3), 0.5 * (2 - 5 * t2 + 3 * t3),
+            0.5 * (t + 4 * t2 - 3 * t3), 0.5 * (t3 - t2))
+
+
+def interp2_catmull_rom(a, x, y):
+    """a (Nq2g, Nq1g, ...) at q1 index positions x and q2 index positions y
+    (broadcast against a): the tensor product of Catmull-Rom cubics, the
+    neighbouring samples clamped to the array, 0 where a position lies
+    outside [0, n - 1] -- the restatement of ArrayFire's approx2 with
+    BICUBIC_SPLINE that the semi-Lagrangian step calls (ArrayFire itself,
+    a third-party library, is absent: parity of this interpolation is
+    unpinned beyond its own restatement)."""
+    n2, n1 = a.shape[0], a.shape[1]
+    shape = np.broadcast_shapes(a.shape, np.shape(x), np.shape(y))
+    x = np.broadcast_to(x, shape)
+    y = np.broadcast_to(y, shape)
+    off = (x < 0) | (x > n1 - 1) | (y < 0) | (y > n2 - 1)
+    xs, ys = np.clip(x, 0, n1 - 1), np.clip(y, 0, n2 - 1)
+    i0 = np.floor(xs).astype(np.int64)
+    j0 = np.floor(ys).astype(np.int64)
+    wx, wy = catmull_rom(xs - i0), catmull_rom(ys - j0)
+    idx = np.indices(shape[2:])
+    out = np.zeros(shape)
+    for b in range(4):
+        jj = np.clip(j0 - 1 + b, 0, n2 - 1)
+        row = np.zeros(shape)
+        for c in range(4):
+            ii = np.clip(i0 - 1 + c, 0, n1 - 1)
+            row = row + wx[c] * a[(jj, ii) + tuple(np.broadcast_to(k, shape) for k in idx)]
+        out = out + wy[b] * row
+    out[off] = 0.0
+    return out

@@ -258,6 +258,45 @@ CASES['fields_user_E_B_2d3v'] = make(
     init=dict(amp=0.05, k1=1, k2=1, T=[1.0, 1.2, 0.9], u=[0.1, -0.1, 0.2]))
 
 
+# Advective semi-Lagrangian (ASL) in q (solver_method_in_q = 'ASL', fields
+# off): the step splits q-advection (back-traced characteristics, bicubic
+# interpolation) and the BGK source (RK2) by the named scheme
+# (timestep.py, operator_splitting_methods.py, asl_operators.py:20-83)
+_ASL_1D = dict(N_q1=64, N_q2=1, N_p1=64, N_p2=1, N_p3=1,
+               p1_start=[-6.0], p1_end=[6.0], p2_start=[-0.5], p2_end=[0.5],
+               p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=1,
+               solver_q='ASL', tau=0.05, dt=2e-3, steps=10,
+               init=dict(amp=0.05, k1=1, k2=0, u=[0.2, 0.0, 0.0]))
+_ASL_2D = dict(N_q1=16, N_q2=12, N_p1=10, N_p2=8, N_p3=1,
+               p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+               p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=2,
+               solver_q='ASL', tau=0.1, dt=5e-3, steps=5,
+               init=dict(amp=0.1, k1=1, k2=1, u=[0.3, -0.2, 0.0], T=[1.0, 1.5, 1.0]))
+CASES['asl_1d1v_strang'] = make(splitting='strang', **copy.deepcopy(_ASL_1D))
+CASES['asl_1d1v_cfl17_lie'] = make(splitting='lie', **dict(copy.deepcopy(_ASL_1D),
+                                                             dt=4.4e-3, steps=6))
+CASES['asl_1d1v_instant_strang'] = make(splitting='strang', instantaneous=True,
+                                        **copy.deepcopy(_ASL_1D))
+CASES['asl_2d2v_lie'] = make(splitting='lie', **copy.deepcopy(_ASL_2D))
+CASES['asl_2d2v_swss'] = make(splitting='swss', **copy.deepcopy(_ASL_2D))
+CASES['asl_2d2v_jia'] = make(splitting='jia', **copy.deepcopy(_ASL_2D))
+CASES['asl_2d2v_free_strang'] = make(splitting='strang', source_enabled=False,
+                                     **copy.deepcopy(_ASL_2D))
+CASES['asl_2d2v_mirror_strang'] = make(splitting='strang', bc_q1='mirror',
+                                       **copy.deepcopy(_ASL_2D))
+CASES['asl_2d3v_strang'] = make(
+    N_q1=8, N_q2=8, N_p1=8, N_p2=8, N_p3=4,
+    p1_start=[-5.0], p1_end=[5.0], p2_start=[-5.0], p2_end=[5.0],
+    p3_start=[-5.0], p3_end=[5.0], mass=[1.0], charge=[0.0], p_dim=3,
+    solver_q='ASL', splitting='strang', tau=0.05, dt=4e-3, steps=3,
+    init=dict(amp=0.1, k1=1, k2=1, u=[0.2, -0.1, 0.05]))
+
+
+# the finite-volume cases and the semi-Lagrangian ones
+FVM_NAMES = sorted(n for n, s in CASES.items() if s.get('solver_q', 'FVM') == 'FVM')
+ASL_NAMES = sorted(n for n, s in CASES.items() if s.get('solver_q', 'FVM') == 'ASL')
+
+
 def field_functions(form, sin, cos):
     """The initialize-module field functions of the 'field_init' cases, written
     against a math namespace (numpy, torch, or the ArrayFire stand-in):

@@ -115,7 +115,7 @@ def build_modules(spec, af, record=None):
     params.fields_type = spec['fields_type']
     params.fields_initialize = spec['fields_initialize']
     params.fields_solver = spec['fields_solver']
-    params.solver_method_in_q = 'FVM'
+    params.solver_method_in_q = spec.get('solver_q', 'FVM')
     params.solver_method_in_p = 'FVM'
     params.reconstruction_method_in_q = spec['recon_q']
     params.reconstruction_method_in_p = spec['recon_p']
@@ -128,7 +128,7 @@ def build_modules(spec, af, record=None):
     params.boltzmann_constant = spec['boltzmann_constant']
     params.fields_enabled = spec['fields_enabled']
     params.source_enabled = spec['source_enabled']
-    params.instantaneous_collisions = False
+    params.instantaneous_collisions = bool(spec.get('instantaneous', False))
     params.hybrid_model_enabled = False
     params.eps = spec['eps']
     params.mu = spec['mu']
@@ -219,7 +219,8 @@ def run_case(name, spec):
     nls.dt = spec['dt']
     if spec['fields_enabled']:
         at_n = nls.fields_solver.at_n
-    out['dfdt0'] = interior(af_to_layout(df_dt_fvm(nls.f, nls), spec), spec)
+    if spec.get('solver_q', 'FVM') == 'FVM':
+        out['dfdt0'] = interior(af_to_layout(df_dt_fvm(nls.f, nls), spec), spec)
     if spec['fields_enabled']:
         # the single p-flux divergences of the same state (term_to_return,
         # df_dt_fvm.py:325-335), each from the same field time level
@@ -233,8 +234,10 @@ def run_case(name, spec):
         out['fields_yee0'] = np.transpose(np.asarray(nls.fields_solver.yee_grid_EM_fields)
                                           .reshape(6, 1, Nq(spec, 1), Nq(spec, 2))[:, 0], (0, 2, 1))
     nls.f = f_save
+    # the splitting scheme (all four are the same step for FVM in q and p)
+    step = getattr(nls, spec.get('splitting', 'strang') + '_timestep')
     for _ in range(spec['steps']):
-        nls.strang_timestep(spec['dt'])
+        step(spec['dt'])
     out['f_final'] = interior(af_to_layout(nls.f, spec), spec)
     for mname in ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy'):
         out['mom_' + mname] = interior(q_to_layout(nls.compute_moments(mname)), spec)

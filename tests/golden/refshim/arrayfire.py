@@ -29,6 +29,19 @@ class Dtype(object):
     s64 = np.int64
 
 
+class INTERP(object):
+    NEAREST = 0
+    LINEAR = 1
+    BILINEAR = 2
+    CUBIC = 3
+    LOWER = 4
+    LINEAR_COSINE = 5
+    BILINEAR_COSINE = 6
+    BICUBIC = 7
+    CUBIC_SPLINE = 8
+    BICUBIC_SPLINE = 9
+
+
 def _as4(a):
     a = np.asarray(a)
     if a.ndim > 4:
@@ -372,3 +385,61 @@ class _ArrayModule(object):
 
 
 array = _ArrayModule()
+
+
+# -- interpolation ---------------------------------------------------------------
+def _catmull_rom(t):
+    """Weights of the Catmull-Rom cubic through samples at -1, 0, 1, 2 for a
+    point at t in [0, 1) past sample 0 (Catmull and Rom 1974)."""
+    t2, t3 = t * t, t * t * t
+    return (0.5 * (-t + 2 * t2 - t3), 0.5 * (2 - 5 * t2 + 3 * t3),
+            0.5 * (t + 4 * t2 - 3 * t3), 0.5 * (t3 - t2))
+
+
+def approx2(signal, pos0, pos1, method=INTERP.LINEAR, off_grid=0.0, xp=None, yp=None):
+    """Interpolation of dims 0 and 1 of ``signal`` at (pos0, pos1), batched over
+    dims 2 and 3 (ArrayFire's approx2).  Positions are sample indices; with xp
+    (yp) the positions are coordinates on the uniform grid xp[:, 0, 0, 0]
+    (yp[0, :, 0, 0]) and are first mapped to indices, (x - xp0) / dxp.  Only
+    BICUBIC_SPLINE is restated: ArrayFire documents it as bicubic
+    interpolation with Catmull-Rom splines, here the tensor product of the 1-D
+    Catmull-Rom cubic; the neighbouring samples are clamped to the signal and a
+    position outside [0, n - 1] on either dim takes ``off_grid``.  (ArrayFire
+    itself is not available here: this stands in for its kernel.)"""
+    if method != INTERP.BICUBIC_SPLINE:
+        raise NotImplementedError('approx2: only BICUBIC_SPLINE is restated')
+    f = _unwrap(signal)
+    x = np.array(_unwrap(pos0), dtype=np.float64)
+    y = np.array(_unwrap(pos1), dtype=np.float64)
+    if xp is not None:
+        g = _unwrap(xp)
+        x = (x - g[0, 0, 0, 0]) / (g[1, 0, 0, 0] - g[0, 0, 0, 0])
+    if yp is not None:
+        g = _unwrap(yp)
+        y = (y - g[0, 0, 0, 0]) / (g[0, 1, 0, 0] - g[0, 0, 0, 0])
+    n0, n1 = f.shape[0], f.shape[1]
+    x = np.broadcast_to(x, f.shape[:2] + x.shape[2:]) if x.shape[:2] != f.shape[:2] else x
+    shape = np.broadcast_shapes(x.shape, y.shape, (1, 1) + f.shape[2:])
+    x = np.broadcast_to(x, shape)
+    y = np.broadcast_to(y, shape)
+    off = (x < 0) | (x > n0 - 1) | (y < 0) | (y > n1 - 1)
+    xs = np.clip(x, 0, n0 - 1)
+    ys = np.clip(y, 0, n1 - 1)
+    i0 = np.floor(xs).astype(np.int64)
+    j0 = np.floor(ys).astype(np.int64)
+    wx = _catmull_rom(xs - i0)
+    wy = _catmull_rom(ys - j0)
+    b2 = np.arange(shape[2]).reshape(1, 1, -1, 1)
+    b3 = np.arange(shape[3]).reshape(1, 1, 1, -1)
+    b2 = np.broadcast_to(b2 if f.shape[2] > 1 else 0 * b2, shape)
+    b3 = np.broadcast_to(b3 if f.shape[3] > 1 else 0 * b3, shape)
+    out = np.zeros(shape, dtype=np.result_type(f.dtype, np.float64))
+    for b in range(4):
+        jj = np.clip(j0 - 1 + b, 0, n1 - 1)
+        row = np.zeros(shape)
+        for a in range(4):
+            ii = np.clip(i0 - 1 + a, 0, n0 - 1)
+            row = row + wx[a] * f[ii, jj, b2, b3]
+        out = out + wy[b] * row
+    out[off] = off_grid
+    return Array._wrap(out.astype(f.dtype))

@@ -25,7 +25,7 @@ from _util import load_golden, rel, interior, moment_errors, check_compact
 pytestmark = pytest.mark.gpu
 
 MOMENTS = ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy')
-NAMES = sorted(C.CASES)
+NAMES = C.FVM_NAMES
 TOL = {'fp64': dict(f0=1e-14, fields0=1e-11, dfdt=1e-12, f=1e-12, mom=1e-12, fields=1e-10),
        'fp32': dict(f0=1e-7, fields0=1e-3, dfdt=1e-3, f=2e-6, mom=2e-6, fields=1e-4),
        # FP64 throughput form: the paired kernel with FMA contraction and
