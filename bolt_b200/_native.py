@@ -101,6 +101,8 @@ SIGNATURES = {
     'bolt_stage_part': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, ctypes.c_int, _VP]),
     'bolt_stage_region': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                          _VP]),
+    'bolt_asl_advect_q': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),
+    'bolt_asl_source': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
     'bolt_fields_yee': (_VP, [_VP]),
     'bolt_set_peer_halos': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     'bolt_set_peer_halos_q1': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),

@@ -1,0 +1,131 @@
+// asl_kernels.cuh - advective semi-Lagrangian step in q (sm_100a), FP64 / FP32.
+//
+// Bolt's ASL solver in q (asl_operators.py:20-83, interpolation_routines.py:
+// 9-56) splits two operators by Strang, Lie, SWSS or Jia splitting (timestep.py,
+// operator_splitting_methods.py):
+//   op_advect_q  every cell takes the value at the foot of its characteristic,
+//                q - A_q dt with A_q = (p1, p2) (advection_terms.py:29-61): one
+//                bicubic interpolation over the ghosted q-plane per p-cell;
+//   op_solve_src f <- f_MB (instantaneous collisions) or one RK2 step
+//                (integrators.py:6-13) of the BGK source -(f - f_MB)/tau.
+// The interpolation is ArrayFire's approx2 with BICUBIC_SPLINE, a third-party
+// kernel absent here: it is restated as the tensor product of 1-D Catmull-Rom
+// cubics (Catmull and Rom 1974), the neighbouring samples clamped to the
+// ghosted array and 0 where a foot lies outside it.  The displacement
+// (p1 dt / dq1, p2 dt / dq2) depends on p only, so consecutive lanes (p) of a
+// warp gather from nearby cells of the same rows.
+#pragma once
+
+#include "fvm_kernels.cuh"
+
+namespace bolt {
+
+// weights of the Catmull-Rom cubic through samples -1, 0, 1, 2 at t in [0, 1)
+__device__ __forceinline__ void catmull_rom_w(double t, double (&w)[4]) {
+    const double t2 = t * t, t3 = t * t * t;
+    w[0] = 0.5 * ((-t + 2.0 * t2) - t3);
+    w[1] = 0.5 * ((2.0 - 5.0 * t2) + 3.0 * t3);
+    w[2] = 0.5 * ((t + 4.0 * t2) - 3.0 * t3);
+    w[3] = 0.5 * (t3 - t2);
+}
+
+// a position in sample units on an axis of n samples: first sample, weights
+// (0 weights when the position lies off the samples)
+__device__ __forceinline__ bool catmull_rom_axis(double x, int n, int& i0, double (&w)[4]) {
+    const bool off = !(x >= 0.0 && x <= double(n - 1));
+    const double xs = fmin(fmax(x, 0.0), double(n - 1));
+    const double fl = floor(xs);
+    i0 = (int)fl;
+    catmull_rom_w(xs - fl, w);
+    return off;
+}
+
+// one thread per interior (q2, q1, s, p) element, p fastest
+template <typename T>
+__global__ void __launch_bounds__(256) asl_q_kernel(const AslArgs a) {
+    const long long total = (long long)a.Nq2 * a.Nq1 * a.Ns * a.Np;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int p = (int)(e % a.Np);
+    long long r = e / a.Np;
+    const int s = (int)(r % a.Ns);
+    r /= a.Ns;
+    const int i = (int)(r % a.Nq1), j = (int)(r / a.Nq1);
+    const int Ng = a.Ng, Nq1g = a.Nq1 + 2 * Ng, Nq2g = a.Nq2 + 2 * Ng;
+    const int ip1 = p % a.Np1, ip2 = (p / a.Np1) % a.Np2;
+    const double v1 = a.sg.p1_start[s] + (0.5 + ip1) * a.sg.dp1[s];
+    const double v2 = a.sg.p2_start[s] + (0.5 + ip2) * a.sg.dp2[s];
+    // cell centres of the ghosted grid (calculate_q.py:7-41) and the foot
+    // of the characteristic in sample units, as approx2's xp / yp mapping
+    // computes it: ((q - A dt) - q_0) / (q_1 - q_0)
+    const double q10 = a.q1_start + (0.5 - Ng) * a.dq1, q11 = a.q1_start + (1.5 - Ng) * a.dq1;
+    const double q20 = a.q2_start + (0.5 - Ng) * a.dq2, q21 = a.q2_start + (1.5 - Ng) * a.dq2;
+    const double qi = a.q1_start + (0.5 + i) * a.dq1, qj = a.q2_start + (0.5 + j) * a.dq2;
+    const double x = ((qi - v1 * a.dt) - q10) / (q11 - q10);
+    const double y = ((qj - v2 * a.dt) - q20) / (q21 - q20);
+    int i0, j0;
+    double wx[4], wy[4];
+    const bool off = catmull_rom_axis(x, Nq1g, i0, wx) | catmull_rom_axis(y, Nq2g, j0, wy);
+    const long long rowstride = (long long)a.Ns * a.Np;
+    const long long colstride = rowstride * Nq1g;
+    const T* f = static_cast<const T*>(a.f) + (long long)s * a.Np + p;
+    double acc = 0.0;
+    if (!off) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int jj = min(max(j0 - 1 + b, 0), Nq2g - 1);
+            double row = 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int ii = min(max(i0 - 1 + c, 0), Nq1g - 1);
+                row = row + wx[c] * double(f[jj * colstride + ii * rowstride]);
+            }
+            acc = acc + wy[b] * row;
+        }
+    }
+    static_cast<T*>(a.out)[(j + Ng) * colstride + (i + Ng) * rowstride + (long long)s * a.Np + p] =
+        T(acc);
+}
+
+// the BGK source of one interior q-cell of species blockIdx.y (blockIdx.x =
+// q-cell): mode 0, out = base + c * (-(in - f_MB) / tau) with f_MB from the
+// moments of `in` (a.mom_in, one partial slot); mode 1, out = f_MB
+template <typename T>
+__global__ void __launch_bounds__(256) asl_src_kernel(const QStageArgs a, const void* in,
+                                                      const void* base, void* out, double c,
+                                                      int mode) {
+    __shared__ double qq[5];
+    __shared__ double vg[3 * 256];
+    const int cell = blockIdx.x, s = blockIdx.y;
+    const int ii = cell % a.Nq1, jj = cell / a.Nq1;
+    const int Np1 = a.Np1, Np2 = a.Np2, Np3 = a.Np3;
+    const int ntab = Np1 + Np2 + Np3;
+    if (threadIdx.x == 0) bgk_cell_params(a, s, ii, jj, qq);
+    for (int q = threadIdx.x; q < ntab && q < 3 * 256; q += blockDim.x) {
+        if (q < Np1) vg[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
+        else if (q < Np1 + Np2) vg[q] = a.sg.p2_start[s] + (0.5 + (q - Np1)) * a.sg.dp2[s];
+        else vg[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
+    }
+    __syncthreads();
+    const double m = a.sg.mass[s];
+    const long long rowstride = (long long)a.Ns * a.Np;
+    const long long colstride = rowstride * a.Nq1g;
+    const long long o = (jj + a.Ng) * colstride + (ii + a.Ng) * rowstride + (long long)s * a.Np;
+    const T* fi = static_cast<const T*>(in) + o;
+    const T* fb = static_cast<const T*>(base) + o;
+    T* fo = static_cast<T*>(out) + o;
+    for (int p = threadIdx.x; p < a.Np; p += blockDim.x) {
+        const int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
+        const double f0 = (bgk_table_entry(a, qq, vg, ip1, m) *
+                           bgk_table_entry(a, qq, vg, Np1 + ip2, m)) *
+                          bgk_table_entry(a, qq, vg, Np1 + Np2 + ip3, m);
+        if (mode == 1) {
+            fo[p] = T(f0);
+        } else {
+            const double src = -(double(fi[p]) - f0) / a.tau;
+            fo[p] = T(double(fb[p]) + src * c);
+        }
+    }
+}
+
+}  // namespace bolt

@@ -1082,6 +1082,87 @@ int bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream) {
     return BOLT_OK;
 }
 
+// ---- advective semi-Lagrangian step in q (asl_operators.py:20-83) ----------
+int bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
+    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+    const BoltGrid& g = ctx->g;
+    if (ctx->p.fields_enabled || g.N_ghost < 2) return BOLT_ERR_UNSUPPORTED;
+    cudaStream_t st = (cudaStream_t)stream;
+    // op_advect_q: communicate_f + apply_bcs_f, then the interpolation
+    int rc = launch_ghosts(ctx, f_dev, st);
+    if (rc) return rc;
+    AslArgs a;
+    memset(&a, 0, sizeof(a));
+    a.f = f_dev;
+    a.out = ctx->buf[0];
+    a.dt = dt;
+    a.q1_start = g.q1_start;
+    a.q2_start = g.q2_start;
+    a.dq1 = g.dq1;
+    a.dq2 = g.dq2;
+    a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost; a.Ns = g.N_s;
+    a.Np1 = g.N_p1; a.Np2 = g.N_p2; a.Np3 = g.N_p3; a.Np = ctx->Np;
+    a.sg = ctx->sg;
+    cudaError_t e = ctx->elem == 8 ? launch_asl_q_f64(a, st) : launch_asl_q_f32(a, st);
+    ctx->launches++;
+    CK(e);
+    // the interpolated interior back into f (one row of q1 cells per q2 row),
+    // then f's ghost cells from it
+    const size_t row = (size_t)g.N_s * ctx->Np * ctx->elem;
+    const size_t pitch = row * ctx->Nq1g;
+    const size_t off = (size_t)g.N_ghost * pitch + (size_t)g.N_ghost * row;
+    CK(cudaMemcpy2DAsync(static_cast<char*>(f_dev) + off, pitch,
+                         static_cast<const char*>(ctx->buf[0]) + off, pitch, row * g.N_q1,
+                         g.N_q2, cudaMemcpyDeviceToDevice, st));
+    rc = launch_ghosts(ctx, f_dev, st);
+    ctx->ghost_owner = f_dev;
+    ctx->ghost_stale_time = 0;
+    ctx->mom_owner = nullptr;
+    return rc;
+}
+
+int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream) {
+    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+    const BoltGrid& g = ctx->g;
+    if (ctx->p.fields_enabled || !ctx->bgk || ctx->tau_arr || ctx->ntab > 768)
+        return BOLT_ERR_UNSUPPORTED;
+    cudaStream_t st = (cudaStream_t)stream;
+    QStageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost; a.Ns = g.N_s;
+    a.Np1 = g.N_p1; a.Np2 = g.N_p2; a.Np3 = g.N_p3; a.Np = ctx->Np;
+    a.Nq1g = ctx->Nq1g; a.Nq2g = ctx->Nq2g;
+    a.sg = ctx->sg;
+    a.kB = ctx->p.boltzmann_constant;
+    a.p_dim = ctx->p.p_dim;
+    a.tau = ctx->p.tau;
+    a.mom_in = ctx->momP[0];
+    a.nsplit_in = 1;
+    auto src = [&](const void* in, const void* base, void* out, double c, int mode) {
+        int r = launch_moments5(ctx, in, ctx->momP[0], st);
+        if (r) return r;
+        cudaError_t e = ctx->elem == 8 ? launch_asl_src_f64(a, in, base, out, c, mode, st)
+                                       : launch_asl_src_f32(a, in, base, out, c, mode, st);
+        ctx->launches++;
+        CK(e);
+        return BOLT_OK;
+    };
+    int rc;
+    if (instantaneous) {
+        // f <- f_MB (asl_operators.py:56-64, collision_operator.py:126-128)
+        rc = src(f_dev, f_dev, f_dev, 0.0, 1);
+    } else {
+        // integrators.RK2: f_half = f + S(f) dt/2; f = f + S(f_half) dt
+        rc = src(f_dev, f_dev, ctx->buf[0], 0.5 * dt, 0);
+        if (!rc) rc = src(ctx->buf[0], f_dev, f_dev, dt, 0);
+    }
+    if (!rc) rc = launch_ghosts(ctx, f_dev, st);
+    ctx->ghost_owner = f_dev;
+    ctx->ghost_stale_time = 0;
+    ctx->mom_owner = nullptr;
+    return rc;
+}
+
 int bolt_set_shear(BoltCtx* ctx, double q, double omega) {
     if (!ctx) return BOLT_ERR_ARG;
     ctx->shear_q = q;

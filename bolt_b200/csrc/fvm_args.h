@@ -153,6 +153,16 @@ struct QStageArgs {
     void* peer_right;
 };
 
+// semi-Lagrangian q-step (asl_kernels.cuh): interpolation of the interior
+struct AslArgs {
+    const void* f;       // ghosted input (Nq2g, Nq1g, Ns, Np)
+    void* out;           // interior cells written, same layout
+    double dt;
+    double q1_start, q2_start, dq1, dq2;
+    int Nq1, Nq2, Ng, Ns, Np1, Np2, Np3, Np;
+    SpeciesGrid sg;
+};
+
 struct PStageArgs {
     const void* fs;        // stage input (ghosted)
     const void* kq;        // q-part of df/dt (ghosted layout, interior valid)

@@ -4,6 +4,7 @@
 
 #include "launch.h"
 #include "fvm_kernels.cuh"
+#include "asl_kernels.cuh"
 
 namespace bolt {
 
@@ -99,6 +100,21 @@ cudaError_t BOLT_CAT(launch_ghost_, BOLT_SUFFIX)(void* f, const void* dl, const 
         static_cast<BOLT_T*>(f), static_cast<const BOLT_T*>(dl), static_cast<const BOLT_T*>(dr),
         static_cast<const BOLT_T*>(db), static_cast<const BOLT_T*>(dt), Nq1, Nq2, Ng, Ns, Np, Np1,
         Np2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, sg, sh, ncells);
+    return cudaGetLastError();
+}
+
+cudaError_t BOLT_CAT(launch_asl_q_, BOLT_SUFFIX)(const AslArgs& a, cudaStream_t st) {
+    const long long total = (long long)a.Nq2 * a.Nq1 * a.Ns * a.Np;
+    if (total == 0) return cudaSuccess;
+    asl_q_kernel<BOLT_T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t BOLT_CAT(launch_asl_src_, BOLT_SUFFIX)(const QStageArgs& a, const void* in,
+                                                   const void* base, void* out, double c,
+                                                   int mode, cudaStream_t st) {
+    dim3 grid(a.Nq1 * a.Nq2, a.Ns);
+    asl_src_kernel<BOLT_T><<<grid, 256, 0, st>>>(a, in, base, out, c, mode);
     return cudaGetLastError();
 }
 

@@ -162,9 +162,16 @@ class nonlinear_solver(object):
         self.device = torch.device('cuda', torch.cuda.current_device())
 
         # ---- path checks ----------------------------------------------------
-        if params.solver_method_in_q != 'FVM' or params.solver_method_in_p != 'FVM':
-            raise NotImplementedError('only the finite-volume method (FVM) in q and p '
-                                      'is implemented')
+        # FVM in q and p, or the advective semi-Lagrangian method (ASL) in q
+        # with fields off (timestep.py: with fields off the method in p is not
+        # used); ASL in p, and ASL in q with fields, are not implemented
+        self._asl = params.solver_method_in_q == 'ASL'
+        fields_on = bool(getattr(params, 'fields_enabled', False))
+        if not ((params.solver_method_in_q == 'FVM' and params.solver_method_in_p == 'FVM') or
+                (self._asl and not fields_on)):
+            raise NotImplementedError('solver methods: FVM in q and p, or ASL in q without '
+                                      'fields')
+        self._instantaneous = bool(getattr(params, 'instantaneous_collisions', False))
         if not (_plugin_ok(ps.C_q, 'advection_terms', 'C_q') and
                 _plugin_ok(ps.C_p, 'advection_terms', 'C_p')):
             raise NotImplementedError('advection terms must be the nonrelativistic_boltzmann '
@@ -349,6 +356,10 @@ class nonlinear_solver(object):
         if self._tau_arr is not None:
             N.check(self._lib.bolt_set_tau_array(ctx, self._tau_arr.data_ptr()), 'bolt_set_tau_array')
         self._shearing = 'shearing-box' in (self._bc_q1, self._bc_q2)
+        if self._asl and (self._has_dirichlet() or self._shearing or
+                          self._tau_arr is not None):
+            raise NotImplementedError('the semi-Lagrangian q-step takes periodic or mirror '
+                                      'q boundaries and a constant tau')
         if self._shearing:
             # boundaries.py:17-18: the shear rate q omega of the params module
             N.check(self._lib.bolt_set_shear(ctx, float(params.q), float(params.omega)),
@@ -609,18 +620,91 @@ class nonlinear_solver(object):
                 'bolt_set_wait_budget')
 
     # with the FVM in both q and p every splitting scheme is the same step
-    # (timestep.py:13-15)
+    # (timestep.py:13-15); ASL in q splits op_advect_q and op_solve_src
     def strang_timestep(self, dt):
-        self._step(dt)
+        self._asl_step(dt, 'strang') if self._asl else self._step(dt)
 
     def lie_timestep(self, dt):
-        self._step(dt)
+        self._asl_step(dt, 'lie') if self._asl else self._step(dt)
 
     def swss_timestep(self, dt):
-        self._step(dt)
+        self._asl_step(dt, 'swss') if self._asl else self._step(dt)
 
     def jia_timestep(self, dt):
-        self._step(dt)
+        self._asl_step(dt, 'jia') if self._asl else self._step(dt)
+
+    # ---- advective semi-Lagrangian in q (asl_operators.py:20-83) ------------------
+    def _op_advect_q(self, dt):
+        N.check(self._lib.bolt_asl_advect_q(self._ctx, self._fstore.data_ptr(), float(dt),
+                                            self._stream()), 'bolt_asl_advect_q')
+
+    def _op_solve_src(self, dt):
+        # f <- f_MB where collisions are instantaneous, else RK2 of the source
+        # when it is enabled (asl_operators.py:40-83)
+        if self._instantaneous or self.physical_system.params.source_enabled:
+            N.check(self._lib.bolt_asl_source(self._ctx, self._fstore.data_ptr(), float(dt),
+                                              int(self._instantaneous), self._stream()),
+                    'bolt_asl_source')
+
+    def _asl_step(self, dt, scheme):
+        """One timestep of ASL in q without fields: op_advect_q and
+        op_solve_src composed by the named splitting (timestep.py:39-240,
+        operator_splitting_methods.py); SWSS and Jia keep copies of f."""
+        self.dt = dt
+        self._sync_external_edits()
+        if self.performance_test_flag:
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record()
+        op1, op2 = self._op_advect_q, self._op_solve_src
+        f = self._fstore
+
+        def strang(a, b):
+            a(0.5 * dt)
+            b(dt)
+            a(0.5 * dt)
+
+        def swss(a, b):
+            start = f.clone()
+            a(dt)
+            b(dt)
+            mid = f.clone()
+            f.copy_(start)
+            b(dt)
+            a(dt)
+            f.add_(mid).mul_(0.5)
+
+        if scheme == 'strang':
+            strang(op1, op2)
+        elif scheme == 'lie':
+            op1(dt)
+            op2(dt)
+        elif scheme == 'swss':
+            swss(op1, op2)
+        else:                                            # jia
+            start = f.clone()
+            strang(op1, op2)
+            f1 = f.clone()
+            f.copy_(start)
+            strang(op2, op1)
+            f2 = f.clone()
+            f.copy_(start)
+            swss(op1, op2)
+            f.copy_((2 / 3) * (f1 + f2) - (1 / 3) * f)
+        if scheme in ('swss', 'jia'):
+            # f was combined outside the context: its ghosts and moments are new
+            self._lib.bolt_invalidate(self._ctx)
+        self._seen_version = self._fstore._version
+        if self.performance_test_flag:
+            t1.record()
+            t1.synchronize()
+            self._perf['time_ts'] += t0.elapsed_time(t1) * 1e-3
+            self._perf['steps'] += 1
+        # timestep.py:28-38 (a synchronous check of the interior here)
+        g = self.N_ghost
+        if not bool(torch.isfinite(f[g:f.shape[0] - g, g:f.shape[1] - g]).all()):
+            raise SystemExit('Solver Diverging!')
+        self.time_elapsed += dt
 
     def run(self, dt, n_steps):
         """n_steps strang steps launched back to back (no per-step host work)."""

@@ -162,6 +162,24 @@ int  bolt_set_time(BoltCtx* ctx, double t);
 /* Halo refresh of f in place (periodic wrap + Dirichlet inflow). */
 int  bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream);
 
+/* Advective semi-Lagrangian (ASL) method in q, fields disabled -- the two
+ * operators that Bolt's timesteps split (asl_operators.py:20-83;
+ * timestep.py:39-240 composes them by Strang, Lie, SWSS or Jia splitting,
+ * operator_splitting_methods.py).
+ * bolt_asl_advect_q is op_advect_q (interpolation_routines.py:9-56): ghost
+ * refresh, then every interior cell takes f at the foot of its
+ * characteristic q - (p1, p2) dt, by the bicubic interpolation that Bolt gets
+ * from ArrayFire's approx2(BICUBIC_SPLINE), restated here as the tensor
+ * product of Catmull-Rom cubics over the ghosted grid (neighbours clamped to
+ * it, 0 for a foot outside it); N_ghost >= 2, feet up to N_ghost - 1 cells
+ * away read real ghost data.  bolt_asl_source is op_solve_src: f <- f_MB of
+ * f's own moments when instantaneous != 0, else one RK2 step of the BGK
+ * source with the constant tau (needs params->source_enabled; no tau array).
+ * Both write f in place (the context's first stage buffer is their scratch)
+ * and leave its ghost cells refreshed; BOLT_ERR_UNSUPPORTED with fields. */
+int  bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream);
+int  bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream);
+
 /* Forget cached halo/moment state (call after f was modified outside the
  * library; bolt_step then refreshes halos and moments before stepping). */
 int  bolt_invalidate(BoltCtx* ctx);

@@ -66,7 +66,7 @@ def build_modules(spec, precision='fp64', integrator=None):
     params.fields_type = spec['fields_type']
     params.fields_initialize = spec['fields_initialize']
     params.fields_solver = spec['fields_solver']
-    params.solver_method_in_q = 'FVM'
+    params.solver_method_in_q = spec.get('solver_q', 'FVM')
     params.solver_method_in_p = 'FVM'
     params.reconstruction_method_in_q = spec['recon_q']
     params.reconstruction_method_in_p = spec['recon_p']
@@ -79,7 +79,7 @@ def build_modules(spec, precision='fp64', integrator=None):
     params.boltzmann_constant = spec['boltzmann_constant']
     params.fields_enabled = spec['fields_enabled']
     params.source_enabled = spec['source_enabled']
-    params.instantaneous_collisions = False
+    params.instantaneous_collisions = bool(spec.get('instantaneous', False))
     params.hybrid_model_enabled = False
     params.eps = spec['eps']
     params.mu = spec['mu']
