@@ -40,74 +40,113 @@ __device__ __forceinline__ bool catmull_rom_axis(double x, int n, int& i0, doubl
     return off;
 }
 
-// one thread per interior (q2, q1, s, p) element, p fastest
+// One thread per (interior q2 row j, species s, p-cell p), p fastest across
+// lanes, walking the row's q1 cells.  The feet of a thread's cells are its
+// first foot plus 0, 1, 2, ... samples (the displacement depends on p only),
+// so the weights are computed once and the 4 x 4 source window slides along
+// q1: each cell loads one new column of 4 samples (neighbours clamped to the
+// ghosted array; a foot off the array gives 0).  Arithmetic in T.
 template <typename T>
 __global__ void __launch_bounds__(256) asl_q_kernel(const AslArgs a) {
-    const long long total = (long long)a.Nq2 * a.Nq1 * a.Ns * a.Np;
+    const long long nthr = (long long)a.Nq2 * a.Ns * a.Np;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= total) return;
+    if (e >= nthr) return;
     const int p = (int)(e % a.Np);
-    long long r = e / a.Np;
-    const int s = (int)(r % a.Ns);
-    r /= a.Ns;
-    const int i = (int)(r % a.Nq1), j = (int)(r / a.Nq1);
+    const long long r = e / a.Np;
+    const int s = (int)(r % a.Ns), j = (int)(r / a.Ns);
     const int Ng = a.Ng, Nq1g = a.Nq1 + 2 * Ng, Nq2g = a.Nq2 + 2 * Ng;
     const int ip1 = p % a.Np1, ip2 = (p / a.Np1) % a.Np2;
     const double v1 = a.sg.p1_start[s] + (0.5 + ip1) * a.sg.dp1[s];
     const double v2 = a.sg.p2_start[s] + (0.5 + ip2) * a.sg.dp2[s];
-    // cell centres of the ghosted grid (calculate_q.py:7-41) and the foot
-    // of the characteristic in sample units, as approx2's xp / yp mapping
+    // cell centres of the ghosted grid (calculate_q.py:7-41) and the foot of
+    // the characteristic in sample units, as approx2's xp / yp mapping
     // computes it: ((q - A dt) - q_0) / (q_1 - q_0)
     const double q10 = a.q1_start + (0.5 - Ng) * a.dq1, q11 = a.q1_start + (1.5 - Ng) * a.dq1;
     const double q20 = a.q2_start + (0.5 - Ng) * a.dq2, q21 = a.q2_start + (1.5 - Ng) * a.dq2;
-    const double qi = a.q1_start + (0.5 + i) * a.dq1, qj = a.q2_start + (0.5 + j) * a.dq2;
-    const double x = ((qi - v1 * a.dt) - q10) / (q11 - q10);
+    const double qj = a.q2_start + (0.5 + j) * a.dq2;
     const double y = ((qj - v2 * a.dt) - q20) / (q21 - q20);
-    int i0, j0;
-    double wx[4], wy[4];
-    const bool off = catmull_rom_axis(x, Nq1g, i0, wx) | catmull_rom_axis(y, Nq2g, j0, wy);
+    int j0;
+    double wyd[4];
+    const bool offy = catmull_rom_axis(y, Nq2g, j0, wyd);
+    // the foot of the row's first cell, its sample and weights
+    const double x0 = ((a.q1_start + 0.5 * a.dq1 - v1 * a.dt) - q10) / (q11 - q10);
+    const double fl0 = floor(x0);
+    const int i00 = (int)fl0;
+    double wxd[4];
+    catmull_rom_w(x0 - fl0, wxd);
+    T wx[4], wy[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        wx[c] = T(wxd[c]);
+        wy[c] = T(wyd[c]);
+    }
     const long long rowstride = (long long)a.Ns * a.Np;
     const long long colstride = rowstride * Nq1g;
     const T* f = static_cast<const T*>(a.f) + (long long)s * a.Np + p;
-    double acc = 0.0;
-    if (!off) {
+    const T* rows[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) rows[b] = f + min(max(j0 - 1 + b, 0), Nq2g - 1) * colstride;
+    T* out = static_cast<T*>(a.out) + (j + Ng) * colstride + (long long)Ng * rowstride +
+             (long long)s * a.Np + p;
+    // window[b][c]: row b, column clamp(i00 + i - 1 + c) of cell i
+    T win[4][4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            win[b][c + 1] = rows[b][min(max(i00 - 1 + c, 0), Nq1g - 1) * rowstride];
+    for (int i = 0; i < a.Nq1; ++i) {
+        const int ni = i00 + i;
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            const int jj = min(max(j0 - 1 + b, 0), Nq2g - 1);
-            double row = 0.0;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int ii = min(max(i0 - 1 + c, 0), Nq1g - 1);
-                row = row + wx[c] * double(f[jj * colstride + ii * rowstride]);
-            }
-            acc = acc + wy[b] * row;
+            win[b][0] = win[b][1];
+            win[b][1] = win[b][2];
+            win[b][2] = win[b][3];
+            win[b][3] = rows[b][min(max(ni + 2, 0), Nq1g - 1) * rowstride];
         }
+        const double x = x0 + i;
+        const bool off = offy || !(x >= 0.0 && x <= double(Nq1g - 1));
+        T acc = T(0);
+        if (!off) {
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                T row = T(0);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) row = row + wx[c] * win[b][c];
+                acc = acc + wy[b] * row;
+            }
+        }
+        out[(long long)i * rowstride] = acc;
     }
-    static_cast<T*>(a.out)[(j + Ng) * colstride + (i + Ng) * rowstride + (long long)s * a.Np + p] =
-        T(acc);
 }
 
 // the BGK source of one interior q-cell of species blockIdx.y (blockIdx.x =
 // q-cell): mode 0, out = base + c * (-(in - f_MB) / tau) with f_MB from the
-// moments of `in` (a.mom_in, one partial slot); mode 1, out = f_MB
+// moments of `in` (a.mom_in, one partial slot); mode 1, out = f_MB.  The
+// Maxwellian is the product of its per-axis factors, tabulated once per
+// q-cell (the p1 factor carries n times the normalisation).
+constexpr int kAslMaxTab = 768;
 template <typename T>
 __global__ void __launch_bounds__(256) asl_src_kernel(const QStageArgs a, const void* in,
                                                       const void* base, void* out, double c,
                                                       int mode) {
     __shared__ double qq[5];
-    __shared__ double vg[3 * 256];
+    __shared__ double vg[kAslMaxTab];
+    __shared__ double tab[kAslMaxTab];
     const int cell = blockIdx.x, s = blockIdx.y;
     const int ii = cell % a.Nq1, jj = cell / a.Nq1;
     const int Np1 = a.Np1, Np2 = a.Np2, Np3 = a.Np3;
-    const int ntab = Np1 + Np2 + Np3;
+    const int ntab = Np1 + Np2 + Np3;             // <= kAslMaxTab (checked by the host)
     if (threadIdx.x == 0) bgk_cell_params(a, s, ii, jj, qq);
-    for (int q = threadIdx.x; q < ntab && q < 3 * 256; q += blockDim.x) {
+    for (int q = threadIdx.x; q < ntab; q += blockDim.x) {
         if (q < Np1) vg[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
         else if (q < Np1 + Np2) vg[q] = a.sg.p2_start[s] + (0.5 + (q - Np1)) * a.sg.dp2[s];
         else vg[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
     }
     __syncthreads();
     const double m = a.sg.mass[s];
+    for (int q = threadIdx.x; q < ntab; q += blockDim.x) tab[q] = bgk_table_entry(a, qq, vg, q, m);
+    __syncthreads();
     const long long rowstride = (long long)a.Ns * a.Np;
     const long long colstride = rowstride * a.Nq1g;
     const long long o = (jj + a.Ng) * colstride + (ii + a.Ng) * rowstride + (long long)s * a.Np;
@@ -116,9 +155,7 @@ __global__ void __launch_bounds__(256) asl_src_kernel(const QStageArgs a, const 
     T* fo = static_cast<T*>(out) + o;
     for (int p = threadIdx.x; p < a.Np; p += blockDim.x) {
         const int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
-        const double f0 = (bgk_table_entry(a, qq, vg, ip1, m) *
-                           bgk_table_entry(a, qq, vg, Np1 + ip2, m)) *
-                          bgk_table_entry(a, qq, vg, Np1 + Np2 + ip3, m);
+        const double f0 = (tab[ip1] * tab[Np1 + ip2]) * tab[Np1 + Np2 + ip3];
         if (mode == 1) {
             fo[p] = T(f0);
         } else {

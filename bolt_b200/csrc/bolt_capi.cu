@@ -1106,19 +1106,17 @@ int bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
     cudaError_t e = ctx->elem == 8 ? launch_asl_q_f64(a, st) : launch_asl_q_f32(a, st);
     ctx->launches++;
     CK(e);
-    // the interpolated interior back into f (one row of q1 cells per q2 row),
-    // then f's ghost cells from it
+    // the interpolated interior back into f (one row of q1 cells per q2 row);
+    // f's ghost cells are stale until the next refresh
     const size_t row = (size_t)g.N_s * ctx->Np * ctx->elem;
     const size_t pitch = row * ctx->Nq1g;
     const size_t off = (size_t)g.N_ghost * pitch + (size_t)g.N_ghost * row;
     CK(cudaMemcpy2DAsync(static_cast<char*>(f_dev) + off, pitch,
                          static_cast<const char*>(ctx->buf[0]) + off, pitch, row * g.N_q1,
                          g.N_q2, cudaMemcpyDeviceToDevice, st));
-    rc = launch_ghosts(ctx, f_dev, st);
-    ctx->ghost_owner = f_dev;
-    ctx->ghost_stale_time = 0;
+    ctx->ghost_owner = nullptr;
     ctx->mom_owner = nullptr;
-    return rc;
+    return BOLT_OK;
 }
 
 int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream) {
@@ -1156,9 +1154,8 @@ int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, voi
         rc = src(f_dev, f_dev, ctx->buf[0], 0.5 * dt, 0);
         if (!rc) rc = src(ctx->buf[0], f_dev, f_dev, dt, 0);
     }
-    if (!rc) rc = launch_ghosts(ctx, f_dev, st);
-    ctx->ghost_owner = f_dev;
-    ctx->ghost_stale_time = 0;
+    // f's interior changed: its ghost cells and cached moments are stale
+    ctx->ghost_owner = nullptr;
     ctx->mom_owner = nullptr;
     return rc;
 }

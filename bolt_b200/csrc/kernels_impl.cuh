@@ -104,7 +104,7 @@ cudaError_t BOLT_CAT(launch_ghost_, BOLT_SUFFIX)(void* f, const void* dl, const 
 }
 
 cudaError_t BOLT_CAT(launch_asl_q_, BOLT_SUFFIX)(const AslArgs& a, cudaStream_t st) {
-    const long long total = (long long)a.Nq2 * a.Nq1 * a.Ns * a.Np;
+    const long long total = (long long)a.Nq2 * a.Ns * a.Np;          // threads
     if (total == 0) return cudaSuccess;
     asl_q_kernel<BOLT_T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
     return cudaGetLastError();

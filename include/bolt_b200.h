@@ -175,8 +175,9 @@ int  bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream);
  * away read real ghost data.  bolt_asl_source is op_solve_src: f <- f_MB of
  * f's own moments when instantaneous != 0, else one RK2 step of the BGK
  * source with the constant tau (needs params->source_enabled; no tau array).
- * Both write f in place (the context's first stage buffer is their scratch)
- * and leave its ghost cells refreshed; BOLT_ERR_UNSUPPORTED with fields. */
+ * Both write f's interior in place (the context's first stage buffer is
+ * their scratch) and leave its ghost cells stale (the next refresh, or
+ * bolt_asl_advect_q itself, fills them); BOLT_ERR_UNSUPPORTED with fields. */
 int  bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream);
 int  bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream);
 
