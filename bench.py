@@ -602,7 +602,8 @@ def other_targets(args, local_rank):
     default run records them: the ragged 256-run batch against sequential
     plain runs (target >= 5x), the adjoint's gradient time and its checks
     against central differences and FP64 autograd (target 1e-4), and the
-    FDTD-coupled 2D2V run's FP32 / FP64 throughput ratio.  Each entry is
+    FDTD-coupled 2D2V run's FP32 / FP64 throughput ratio, and the
+    semi-Lagrangian q-step on the headline grid.  Each entry is
     measured as its own --workload measures it (see batch_result,
     adjoint_result, c2_result); sequential runs time --seq-steps steps each,
     scaled to the batch's step count."""
@@ -635,7 +636,10 @@ def other_targets(args, local_rank):
                       'fp64_value': c2['fp64']['value'], 'steps': c2['steps'],
                       'fp32_vs_fp64_after_steps': c2['fp32_vs_fp64_after_steps']}
     t3 = time.perf_counter()
-    out['wall_s'] = {'ragged_batch': t1 - t0, 'adjoint': t2 - t1, 'c2_fdtd': t3 - t2}
+    out['asl_q'] = asl_result(args, local_rank)
+    t4 = time.perf_counter()
+    out['wall_s'] = {'ragged_batch': t1 - t0, 'adjoint': t2 - t1, 'c2_fdtd': t3 - t2,
+                     'asl_q': t4 - t3}
     return out
 
 
@@ -908,6 +912,43 @@ def run_c1(args, rank, world, local_rank):
     line['python_loop_value'] = cells / (res['python_loop_ms_per_step'] * 1e-3)
     line['bolt_run_value'] = cells / (res['bolt_run_ms_per_step'] * 1e-3)
     print(json.dumps(line), flush=True)
+
+
+def asl_result(args, local_rank, steps=10):
+    """The semi-Lagrangian q-step (solver_method_in_q = 'ASL', Strang
+    splitting of the bicubic q-advection and the RK2 BGK source) on the
+    headline grid, 2D3V 128^2 x 24^3 (Maxwellian, n = 1 + 0.05 cos cos, BGK
+    tau = 0.05, dt = 1e-3), FP32 and FP64 f: cell-updates/s over ``steps``
+    timed steps (CUDA events) after 3 warm-up steps."""
+    import torch
+    c2_spec()                            # puts the case builders on sys.path
+    import cases as C
+    from _modules import make_solver as make_case_solver
+    torch.cuda.set_device(local_rank)
+    spec = C.make(N_q1=128, N_q2=128, N_p1=24, N_p2=24, N_p3=24,
+                  p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0], p2_end=[6.0],
+                  p3_start=[-6.0], p3_end=[6.0], mass=[1.0], charge=[0.0], p_dim=3,
+                  solver_q='ASL', splitting='strang', tau=0.05, dt=1e-3,
+                  init=dict(amp=0.05, k1=1, k2=1))
+    cells = 128 * 128 * 24 ** 3
+    out = {'steps': steps, 'splitting': 'strang', 'cells': cells}
+    for prec in ('fp32', 'fp64'):
+        nls = make_case_solver(spec, prec)
+        for _ in range(3):
+            nls.strang_timestep(spec['dt'])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            nls.strang_timestep(spec['dt'])
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[prec] = {'value': cells / (ms * 1e-3), 'ms_per_step': ms}
+        nls.synchronize()
+        del nls
+        torch.cuda.empty_cache()
+    return out
 
 
 def c2_result(args, local_rank):
