@@ -103,6 +103,7 @@ SIGNATURES = {
                                          _VP]),
     'bolt_asl_advect_q': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),
     'bolt_asl_source': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
+    'bolt_fvm_p_step': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),
     'bolt_fields_yee': (_VP, [_VP]),
     'bolt_set_peer_halos': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     'bolt_set_peer_halos_q1': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),

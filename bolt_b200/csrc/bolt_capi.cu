@@ -68,6 +68,7 @@ struct BoltCtx {
     int bgk, bgk_direct, ntab;
     int ntiles1, ntiles2, nsplit, chunks_per_split;
     int use_tma_ok;
+    int p_only;             // 1 during bolt_fvm_p_step: df/dt without its q-part
     // scratch
     void* buf[3];
     void* kbuf;
@@ -883,7 +884,13 @@ static int run_stage(BoltCtx* ctx, StageIO io, int evolve, double dt, cudaStream
         rc = launch_electrostatic(ctx, io.fs, st);
         StageIO qio = io;
         qio.out1 = ctx->kbuf;
-        if (rc == BOLT_OK) rc = launch_qstage(ctx, qio, 1, 0, st);
+        if (rc == BOLT_OK && ctx->p_only) {
+            // the q-part (and the source) belong to the semi-Lagrangian q-step
+            const cudaError_t e = cudaMemsetAsync(ctx->kbuf, 0, ctx->fcount * ctx->elem, st);
+            if (e != cudaSuccess) rc = BOLT_ERR_CUDA;
+        } else if (rc == BOLT_OK) {
+            rc = launch_qstage(ctx, qio, 1, 0, st);
+        }
         if (rc == BOLT_OK) rc = launch_pstage(ctx, io, ctx->kbuf, st);
     } else {
         StageIO qio = io;
@@ -1086,7 +1093,8 @@ int bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream) {
 int bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
     if (!ctx || !f_dev) return BOLT_ERR_ARG;
     const BoltGrid& g = ctx->g;
-    if (ctx->p.fields_enabled || g.N_ghost < 2) return BOLT_ERR_UNSUPPORTED;
+    if ((ctx->p.fields_enabled && !electrostatic(ctx)) || g.N_ghost < 2)
+        return BOLT_ERR_UNSUPPORTED;
     cudaStream_t st = (cudaStream_t)stream;
     // op_advect_q: communicate_f + apply_bcs_f, then the interpolation
     int rc = launch_ghosts(ctx, f_dev, st);
@@ -1119,10 +1127,20 @@ int bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
     return BOLT_OK;
 }
 
+int bolt_fvm_p_step(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
+    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+    if (!electrostatic(ctx)) return BOLT_ERR_UNSUPPORTED;
+    ctx->p_only = 1;
+    const int rc = step_once(ctx, f_dev, dt, (cudaStream_t)stream);
+    ctx->p_only = 0;
+    return rc;
+}
+
 int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream) {
     if (!ctx || !f_dev) return BOLT_ERR_ARG;
     const BoltGrid& g = ctx->g;
-    if (ctx->p.fields_enabled || !ctx->bgk || ctx->tau_arr || ctx->ntab > 768)
+    if ((ctx->p.fields_enabled && !electrostatic(ctx)) || !ctx->bgk || ctx->tau_arr ||
+        ctx->ntab > 768)
         return BOLT_ERR_UNSUPPORTED;
     cudaStream_t st = (cudaStream_t)stream;
     QStageArgs a;

@@ -163,14 +163,17 @@ class nonlinear_solver(object):
 
         # ---- path checks ----------------------------------------------------
         # FVM in q and p, or the advective semi-Lagrangian method (ASL) in q
-        # with fields off (timestep.py: with fields off the method in p is not
-        # used); ASL in p, and ASL in q with fields, are not implemented
+        # with fields off (timestep.py: then the method in p is not used) or
+        # electrostatic fields and the FVM in p; ASL in p, and ASL in q with
+        # electrodynamic fields, are not implemented
         self._asl = params.solver_method_in_q == 'ASL'
         fields_on = bool(getattr(params, 'fields_enabled', False))
+        es = getattr(params, 'fields_type', 'electrodynamic') == 'electrostatic'
         if not ((params.solver_method_in_q == 'FVM' and params.solver_method_in_p == 'FVM') or
-                (self._asl and not fields_on)):
+                (self._asl and (not fields_on or
+                                (es and params.solver_method_in_p == 'FVM')))):
             raise NotImplementedError('solver methods: FVM in q and p, or ASL in q without '
-                                      'fields')
+                                      'fields or with electrostatic fields and the FVM in p')
         self._instantaneous = bool(getattr(params, 'instantaneous_collisions', False))
         if not (_plugin_ok(ps.C_q, 'advection_terms', 'C_q') and
                 _plugin_ok(ps.C_p, 'advection_terms', 'C_p')):
@@ -658,6 +661,26 @@ class nonlinear_solver(object):
             t0.record()
         op1, op2 = self._op_advect_q, self._op_solve_src
         f = self._fstore
+        if self.fields_enabled:
+            # (op_advect_q, op_solve_src) by the scheme, split again with op_fvm,
+            # the FVM in p (timestep.py:134-148)
+            if scheme not in ('strang', 'lie'):
+                raise NotImplementedError('ASL in q with fields: Strang or Lie splitting')
+            adv, src = op1, op2
+
+            def pair(d):
+                if scheme == 'strang':
+                    adv(0.5 * d)
+                    src(d)
+                    adv(0.5 * d)
+                else:
+                    adv(d)
+                    src(d)
+
+            def op_fvm(d):
+                N.check(self._lib.bolt_fvm_p_step(self._ctx, f.data_ptr(), float(d),
+                                                  self._stream()), 'bolt_fvm_p_step')
+            op1, op2 = pair, op_fvm
 
         def strang(a, b):
             a(0.5 * dt)

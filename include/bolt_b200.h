@@ -162,8 +162,8 @@ int  bolt_set_time(BoltCtx* ctx, double t);
 /* Halo refresh of f in place (periodic wrap + Dirichlet inflow). */
 int  bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream);
 
-/* Advective semi-Lagrangian (ASL) method in q, fields disabled -- the two
- * operators that Bolt's timesteps split (asl_operators.py:20-83;
+/* Advective semi-Lagrangian (ASL) method in q, fields off or electrostatic --
+ * the operators that Bolt's timesteps split (asl_operators.py:20-83;
  * timestep.py:39-240 composes them by Strang, Lie, SWSS or Jia splitting,
  * operator_splitting_methods.py).
  * bolt_asl_advect_q is op_advect_q (interpolation_routines.py:9-56): ghost
@@ -177,9 +177,14 @@ int  bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream);
  * source with the constant tau (needs params->source_enabled; no tau array).
  * Both write f's interior in place (the context's first stage buffer is
  * their scratch) and leave its ghost cells stale (the next refresh, or
- * bolt_asl_advect_q itself, fills them); BOLT_ERR_UNSUPPORTED with fields. */
+ * bolt_asl_advect_q itself, fills them); BOLT_ERR_UNSUPPORTED with
+ * electrodynamic fields.  With electrostatic fields the pair is split again
+ * with op_fvm, the FVM in p (timestep.py:134-148), whose df/dt then has no
+ * q-part and no source (df_dt_fvm.py:56-99): bolt_fvm_p_step is that step
+ * (the context's integrator, the FFT field solve of every stage input). */
 int  bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream);
 int  bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream);
+int  bolt_fvm_p_step(BoltCtx* ctx, void* f_dev, double dt, void* stream);
 
 /* Forget cached halo/moment state (call after f was modified outside the
  * library; bolt_step then refreshes halos and moments before stepping). */

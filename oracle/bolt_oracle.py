@@ -660,18 +660,20 @@ class Oracle(object):
         v1 = np.broadcast_to(g.p1c[None, None], f.shape)
         v2 = np.broadcast_to(g.p2c[None, None], f.shape)
         df = 0.0
-        # q-space (df_dt_fvm.py:56-97)
-        lp, rm = reconstruct(f, AX_Q1, rq)
-        bp, tm = reconstruct(f, AX_Q2, rq)
-        lm = _nb(rm, 1, AX_Q1)
-        bm = _nb(tm, 1, AX_Q2)
-        left_flux = riemann(lm, lp, v1, fq)
-        bot_flux = riemann(bm, bp, v2, fq)
-        right_flux = _nb(left_flux, -1, AX_Q1)
-        top_flux = _nb(bot_flux, -1, AX_Q2)
-        df = df - (right_flux - left_flux) / g.dq1 - (top_flux - bot_flux) / g.dq2
-        if sp.get('source_enabled', False):
-            df = df + bgk(g, f, self.tau)
+        # q-space (df_dt_fvm.py:56-97), with the source: only for the FVM in q
+        # (the semi-Lagrangian q-step advects and collides by itself)
+        if sp.get('solver_q', 'FVM') == 'FVM':
+            lp, rm = reconstruct(f, AX_Q1, rq)
+            bp, tm = reconstruct(f, AX_Q2, rq)
+            lm = _nb(rm, 1, AX_Q1)
+            bm = _nb(tm, 1, AX_Q2)
+            left_flux = riemann(lm, lp, v1, fq)
+            bot_flux = riemann(bm, bp, v2, fq)
+            right_flux = _nb(left_flux, -1, AX_Q1)
+            top_flux = _nb(bot_flux, -1, AX_Q2)
+            df = df - (right_flux - left_flux) / g.dq1 - (top_flux - bot_flux) / g.dq2
+            if sp.get('source_enabled', False):
+                df = df + bgk(g, f, self.tau)
         # p-space (df_dt_fvm.py:99-323)
         if sp.get('fields_enabled', False):
             fs = self.fields
@@ -732,6 +734,13 @@ class Oracle(object):
     # time stepping ---------------------------------------------------------
     def step(self, dt):
         """One strang_timestep with the FVM in q and p (timestep.py:101-160)."""
+        self.fvm_step(dt)
+        if np.any(np.isinf(self.f)) or np.any(np.isnan(self.f)):
+            raise SystemExit('Solver Diverging!')
+        self.time_elapsed += dt
+
+    def fvm_step(self, dt):
+        """op_fvm (fvm_operator.py:37-50): the RK step of df_dt_fvm."""
         self.dt = dt
         integ = self.spec.get('integrator', 'RK2')
 
@@ -762,9 +771,6 @@ class Oracle(object):
             self.f = f_initial + ((k1 + 2 * k2 + 2 * k3 + k4) / 6) * dt
         else:
             raise NotImplementedError(integ)
-        if np.any(np.isinf(self.f)) or np.any(np.isnan(self.f)):
-            raise SystemExit('Solver Diverging!')
-        self.time_elapsed += dt
 
     def moments(self, name, f=None):
         return moment(self.g, self.f if f is None else f, name)
@@ -801,11 +807,28 @@ class Oracle(object):
             self.f = self.f + bgk(g, x, self.tau) * dt
 
     def split_step(self, dt, scheme=None):
-        """One timestep of ASL in q without fields: the splitting of op_advect_q
-        and op_solve_src named by ``scheme`` (timestep.py:39-240,
-        operator_splitting_methods.py)."""
+        """One timestep of ASL in q: the splitting of op_advect_q and
+        op_solve_src named by ``scheme`` (timestep.py:39-240,
+        operator_splitting_methods.py); with (electrostatic) fields that pair,
+        split by the same scheme, is itself split with op_fvm, the FVM in p
+        (Strang and Lie only here)."""
         scheme = scheme or self.spec.get('splitting', 'strang')
         op1, op2 = self.asl_advect_q, self.asl_source
+        if self.fields is not None:
+            if scheme not in ('strang', 'lie'):
+                raise NotImplementedError('ASL with fields: Strang or Lie splitting')
+
+            adv, src = op1, op2
+
+            def pair(d):
+                if scheme == 'strang':
+                    adv(0.5 * d)
+                    src(d)
+                    adv(0.5 * d)
+                else:
+                    adv(d)
+                    src(d)
+            op1, op2 = pair, self.fvm_step
 
         def strang(a, b):
             a(0.5 * dt)

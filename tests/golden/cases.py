@@ -292,6 +292,25 @@ CASES['asl_2d3v_strang'] = make(
     init=dict(amp=0.1, k1=1, k2=1, u=[0.2, -0.1, 0.05]))
 
 
+# ASL in q with electrostatic fields and the FVM in p: the splitting of
+# (op_advect_q, op_solve_src) and op_fvm, whose df/dt is then the p-part with
+# the FFT field solve of its argument (timestep.py:134-148, df_dt_fvm.py:56-99)
+CASES['asl_es_1d1v_strang'] = make(
+    N_q1=32, N_q2=3, N_p1=48, N_p2=1, N_p3=1, recon_p='minmod',
+    p1_start=[-6.0], p1_end=[6.0], p2_start=[-0.5], p2_end=[0.5],
+    p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[-1.0], p_dim=1,
+    solver_q='ASL', splitting='strang', source_enabled=False, fields_enabled=True,
+    fields_type='electrostatic', fields_solver='fft', dt=2e-3, steps=5,
+    init=dict(amp=0.05, k1=1, k2=0))
+CASES['asl_es_2d2v_lie_rk4'] = make(
+    N_q1=8, N_q2=8, N_p1=8, N_p2=8, N_p3=1,
+    p1_start=[-5.0, -2.0], p1_end=[5.0, 2.0], p2_start=[-5.0, -2.0], p2_end=[5.0, 2.0],
+    p3_start=[-0.5, -0.5], p3_end=[0.5, 0.5], mass=[1.0, 6.0], charge=[-1.0, 0.5],
+    p_dim=2, solver_q='ASL', splitting='lie', fields_enabled=True,
+    fields_type='electrostatic', fields_solver='fft', tau=0.1, dt=2e-3, steps=3,
+    integrator='RK4', riemann_p='lax-friedrichs',
+    init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=11, u=[0.2, -0.1, 0.0]))
+
 # the finite-volume cases and the semi-Lagrangian ones
 FVM_NAMES = sorted(n for n, s in CASES.items() if s.get('solver_q', 'FVM') == 'FVM')
 ASL_NAMES = sorted(n for n, s in CASES.items() if s.get('solver_q', 'FVM') == 'ASL')

@@ -16,7 +16,8 @@ MOMENTS = ('density', 'mom_v1_bulk', 'mom_v2_bulk', 'mom_v3_bulk', 'energy')
 def test_oracle_asl_matches_reference(name):
     """Semi-Lagrangian q-advection split with the BGK source (Strang, Lie,
     SWSS, Jia; instantaneous and collisionless variants; periodic and mirror
-    walls; a characteristic crossing 1.7 cells per step) against the
+    walls; a characteristic crossing 1.7 cells per step; with electrostatic
+    fields split again with the FVM in p) against the
     reference's own operators run over the numpy stand-ins, whose approx2 is
     the Catmull-Rom restatement the oracle shares (so the interpolation itself
     is unpinned; everything around it -- back-tracing, ghost refresh, source
@@ -31,6 +32,8 @@ def test_oracle_asl_matches_reference(name):
     for _ in range(spec['steps']):
         o.split_step(spec['dt'])
     assert rel(interior(o.f, g), G['f_final']) < 1e-13
+    if spec['fields_enabled']:
+        assert rel(o.fields.cell, G['fields_cell']) < 1e-11
     m = {k: interior(o.moments(k), g) for k in MOMENTS}
     errs = moment_errors(m, {k: G['mom_' + k] for k in MOMENTS})
     assert max(errs.values()) < 1e-13, errs
