@@ -999,6 +999,16 @@ def c2_result(args, local_rank):
     return line
 
 
+def run_asl(args, rank, world, local_rank):
+    line = {'metric': 'cell-updates/s, semi-Lagrangian q-step (Strang split with the BGK '
+                      'source)', 'unit': 'cell-updates/s', 'higher_is_better': True,
+            'data': 'synthetic', 'n_gpus': 1}
+    line.update(asl_result(args, local_rank, steps=args.steps))
+    line['value'] = line['fp32']['value']
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_c2(args, rank, world, local_rank):
     line = c2_result(args, local_rank)
     if rank == 0:
@@ -1017,11 +1027,12 @@ def main():
     ap.add_argument('--no-fp64', action='store_true')
     ap.add_argument('--workload', default='2d3v',
                     choices=['2d3v', '1d1v-relax', '2d2v-fdtd', 'ragged-batch', 'adjoint',
-                             'c3', 'c1', 'c2'],
+                             'asl-q', 'c3', 'c1', 'c2'],
                     help='2d3v: the 128^2 x 24^3 BGK throughput headline; 1d1v-relax: the '
                          '64 x 128 FP64 relaxation (launch-bound); 2d2v-fdtd: the 64^2 x 32^2 '
                          'FDTD-coupled run, FP32 vs FP64; ragged-batch: the 1D1V sweep; adjoint: '
-                         'gradients of the 1D1V density-mode functional (c3, c1, c2: short names '
+                         'gradients of the 1D1V density-mode functional; asl-q: the '
+                         'semi-Lagrangian q-step on the 128^2 x 24^3 grid (c3, c1, c2: short names '
                          'of the first three)')
     ap.add_argument('--adj-steps', type=int, default=2000)
     ap.add_argument('--c2-steps', type=int, default=500, help='steps of the 2d2v-fdtd workload')
@@ -1065,6 +1076,8 @@ def main():
             run_adjoint(args, rank, world, local_rank)
         elif args.workload in ('2d2v-fdtd', 'c2'):
             run_c2(args, rank, world, local_rank)
+        elif args.workload == 'asl-q':
+            run_asl(args, rank, world, local_rank)
         elif args.workload in ('1d1v-relax', 'c1'):
             run_c1(args, rank, world, local_rank)
         else:

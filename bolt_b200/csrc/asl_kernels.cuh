@@ -40,17 +40,11 @@ __device__ __forceinline__ bool catmull_rom_axis(double x, int n, int& i0, doubl
     return off;
 }
 
-// One thread per (interior q2 row j, species s, p-cell p), p fastest across
-// lanes, walking the row's q1 cells.  The feet of a thread's cells are its
-// first foot plus 0, 1, 2, ... samples (the displacement depends on p only),
-// so the weights are computed once and the 4 x 4 source window slides along
-// q1: each cell loads one new column of 4 samples (neighbours clamped to the
-// ghosted array; a foot off the array gives 0).  Arithmetic in T.
+// the q2 row, species and p-cell of thread e (see asl_q_kernel); true if a
+// written value is not finite
 template <typename T>
-__global__ void __launch_bounds__(256) asl_q_kernel(const AslArgs a) {
-    const long long nthr = (long long)a.Nq2 * a.Ns * a.Np;
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nthr) return;
+__device__ __forceinline__ bool asl_q_row(const AslArgs& a, long long e) {
+    bool bad = false;
     const int p = (int)(e % a.Np);
     const long long r = e / a.Np;
     const int s = (int)(r % a.Ns), j = (int)(r / a.Ns);
@@ -117,7 +111,24 @@ __global__ void __launch_bounds__(256) asl_q_kernel(const AslArgs a) {
             }
         }
         out[(long long)i * rowstride] = acc;
+        bad |= !isfinite(double(acc));
     }
+    return bad;
+}
+
+// One thread per (interior q2 row j, species s, p-cell p), p fastest across
+// lanes, walking the row's q1 cells.  The feet of a thread's cells are its
+// first foot plus 0, 1, 2, ... samples (the displacement depends on p only),
+// so the weights are computed once and the 4 x 4 source window slides along
+// q1: each cell loads one new column of 4 samples (neighbours clamped to the
+// ghosted array; a foot off the array gives 0).  Arithmetic in T.  A written
+// value that is not finite sets *flag (one atomic per warp that saw one).
+template <typename T>
+__global__ void __launch_bounds__(256) asl_q_kernel(const AslArgs a, int* flag) {
+    const long long nthr = (long long)a.Nq2 * a.Ns * a.Np;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool bad = e < nthr && asl_q_row<T>(a, e);
+    if (flag && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
 // the BGK source of one interior q-cell of species blockIdx.y (blockIdx.x =
@@ -129,7 +140,7 @@ constexpr int kAslMaxTab = 768;
 template <typename T>
 __global__ void __launch_bounds__(256) asl_src_kernel(const QStageArgs a, const void* in,
                                                       const void* base, void* out, double c,
-                                                      int mode) {
+                                                      int mode, int* flag) {
     __shared__ double qq[5];
     __shared__ double vg[kAslMaxTab];
     __shared__ double tab[kAslMaxTab];
@@ -153,16 +164,21 @@ __global__ void __launch_bounds__(256) asl_src_kernel(const QStageArgs a, const 
     const T* fi = static_cast<const T*>(in) + o;
     const T* fb = static_cast<const T*>(base) + o;
     T* fo = static_cast<T*>(out) + o;
+    bool bad = false;
     for (int p = threadIdx.x; p < a.Np; p += blockDim.x) {
         const int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
         const double f0 = (tab[ip1] * tab[Np1 + ip2]) * tab[Np1 + Np2 + ip3];
+        T v;
         if (mode == 1) {
-            fo[p] = T(f0);
+            v = T(f0);
         } else {
             const double src = -(double(fi[p]) - f0) / a.tau;
-            fo[p] = T(double(fb[p]) + src * c);
+            v = T(double(fb[p]) + src * c);
         }
+        fo[p] = v;
+        bad |= !isfinite(double(v));
     }
+    if (flag && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
 }  // namespace bolt

@@ -1111,7 +1111,9 @@ int bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
     a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost; a.Ns = g.N_s;
     a.Np1 = g.N_p1; a.Np2 = g.N_p2; a.Np3 = g.N_p3; a.Np = ctx->Np;
     a.sg = ctx->sg;
-    cudaError_t e = ctx->elem == 8 ? launch_asl_q_f64(a, st) : launch_asl_q_f32(a, st);
+    // a non-finite interpolated value raises the divergence flag
+    cudaError_t e = ctx->elem == 8 ? launch_asl_q_f64(a, ctx->dflag, st)
+                                   : launch_asl_q_f32(a, ctx->dflag, st);
     ctx->launches++;
     CK(e);
     // the interpolated interior back into f (one row of q1 cells per q2 row);
@@ -1157,8 +1159,9 @@ int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, voi
     auto src = [&](const void* in, const void* base, void* out, double c, int mode) {
         int r = launch_moments5(ctx, in, ctx->momP[0], st);
         if (r) return r;
-        cudaError_t e = ctx->elem == 8 ? launch_asl_src_f64(a, in, base, out, c, mode, st)
-                                       : launch_asl_src_f32(a, in, base, out, c, mode, st);
+        cudaError_t e = ctx->elem == 8
+            ? launch_asl_src_f64(a, in, base, out, c, mode, ctx->dflag, st)
+            : launch_asl_src_f32(a, in, base, out, c, mode, ctx->dflag, st);
         ctx->launches++;
         CK(e);
         return BOLT_OK;

@@ -103,18 +103,18 @@ cudaError_t BOLT_CAT(launch_ghost_, BOLT_SUFFIX)(void* f, const void* dl, const 
     return cudaGetLastError();
 }
 
-cudaError_t BOLT_CAT(launch_asl_q_, BOLT_SUFFIX)(const AslArgs& a, cudaStream_t st) {
+cudaError_t BOLT_CAT(launch_asl_q_, BOLT_SUFFIX)(const AslArgs& a, int* flag, cudaStream_t st) {
     const long long total = (long long)a.Nq2 * a.Ns * a.Np;          // threads
     if (total == 0) return cudaSuccess;
-    asl_q_kernel<BOLT_T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
+    asl_q_kernel<BOLT_T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a, flag);
     return cudaGetLastError();
 }
 
 cudaError_t BOLT_CAT(launch_asl_src_, BOLT_SUFFIX)(const QStageArgs& a, const void* in,
                                                    const void* base, void* out, double c,
-                                                   int mode, cudaStream_t st) {
+                                                   int mode, int* flag, cudaStream_t st) {
     dim3 grid(a.Nq1 * a.Nq2, a.Ns);
-    asl_src_kernel<BOLT_T><<<grid, 256, 0, st>>>(a, in, base, out, c, mode);
+    asl_src_kernel<BOLT_T><<<grid, 256, 0, st>>>(a, in, base, out, c, mode, flag);
     return cudaGetLastError();
 }
 

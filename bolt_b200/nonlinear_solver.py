@@ -723,10 +723,9 @@ class nonlinear_solver(object):
             t1.synchronize()
             self._perf['time_ts'] += t0.elapsed_time(t1) * 1e-3
             self._perf['steps'] += 1
-        # timestep.py:28-38 (a synchronous check of the interior here)
-        g = self.N_ghost
-        if not bool(torch.isfinite(f[g:f.shape[0] - g, g:f.shape[1] - g]).all()):
-            raise SystemExit('Solver Diverging!')
+        # timestep.py:28-38: the operators' kernels flag a non-finite value
+        # they write (read from pinned memory without synchronising)
+        self.check_divergence()
         self.time_elapsed += dt
 
     def run(self, dt, n_steps):

@@ -73,3 +73,24 @@ def test_asl_advection_of_a_linear_profile_is_exact():
     want = 2.0 + 3.0 * (q1[0, 0, :, g].double() - 0.5 * spec['dt'])
     inner = slice(g + 2, 32 + g - 2)
     assert float((got[inner] - want[inner]).abs().max()) < 1e-13
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_asl_nan_raises_solver_diverging(precision):
+    """A NaN written into f from the host reaches the interpolation and the
+    source; their kernels raise the divergence flag, and the timestep raises
+    SystemExit('Solver Diverging!') (timestep.py:28-38)."""
+    spec = C.CASES['asl_2d2v_lie']
+    nls = make_solver(spec, precision)
+    nls.lie_timestep(spec['dt'])
+    torch.cuda.synchronize()
+    nls.check_divergence()                          # a clean step leaves no flag
+    f = nls.f.clone()
+    g = spec['N_ghost']
+    f[3, 0, g + 5, g + 4] = float('nan')
+    nls.f = f
+    with pytest.raises(SystemExit, match='Solver Diverging!'):
+        for _ in range(3):
+            nls.lie_timestep(spec['dt'])
+            torch.cuda.synchronize()
+    nls.synchronize()
