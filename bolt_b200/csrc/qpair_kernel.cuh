@@ -212,43 +212,55 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
     __syncthreads();
 }
 
-// The q-tile of grid column bx: row-major over every tile (tile_sel 0), over
-// the tiles whose halo stays inside the block's interior along its external
-// axes (1: tile columns 1..n1-2 if q1 is external, rows 1..n2-2 if q2 is), or
-// over the others (2: the bottom rows, then the outer columns of the middle
-// rows, then the top rows).  An 8x8 tile's halo reaches 3 cells past it, so
-// only the outermost tiles read ghost cells.
-__device__ __forceinline__ void qpair_tile(const QStageArgs& a, int bx, int& t1, int& t2) {
-    const int n1 = a.ntiles1, n2 = a.ntiles2;
-    if (a.tile_sel == 0) {
-        t1 = bx % n1;
-        t2 = bx / n1;
-        return;
-    }
-    const int e1 = a.ext1 ? 1 : 0, e2 = a.ext2 ? 1 : 0;
-    if (a.tile_sel == 1) {
-        const int w = n1 - 2 * e1;
-        t1 = e1 + bx % w;
-        t2 = e2 + bx / w;
-        return;
-    }
-    if (bx < e2 * n1) {                         // bottom rows
+// Tiles of an n1 x n2 tile grid split by a ring e1 tiles wide along q1 and e2
+// along q2: the inner rectangle, row-major ...
+__device__ __forceinline__ void tile_inner(int n1, int e1, int e2, int bx, int& t1, int& t2) {
+    const int w = n1 - 2 * e1;
+    t1 = e1 + bx % w;
+    t2 = e2 + bx / w;
+}
+
+// ... and the ring: its bottom rows, the outer columns of the middle rows,
+// its top rows
+__device__ __forceinline__ void tile_ring(int n1, int n2, int e1, int e2, int bx, int& t1,
+                                          int& t2) {
+    if (bx < e2 * n1) {
         t1 = bx % n1;
         t2 = bx / n1;
         return;
     }
     bx -= e2 * n1;
-    const int mid = max(0, n2 - 2 * e2);        // middle rows
-    const int m = n1 > 2 * e1 ? 2 * e1 : n1;    // their border tiles
+    const int mid = max(0, n2 - 2 * e2);
+    const int m = n1 > 2 * e1 ? 2 * e1 : n1;    // ring tiles of a middle row
     if (bx < mid * m) {
         t2 = e2 + bx / m;
         const int c = bx % m;
         t1 = m == n1 ? c : (c < e1 ? c : n1 - 2 * e1 + c);
         return;
     }
-    bx -= mid * m;                              // top rows
+    bx -= mid * m;
     t1 = bx % n1;
     t2 = n2 - e2 + bx / n1;
+}
+
+// The q-tile of grid column bx.  tile_sel 0: every tile, those that write
+// periodic images (the ring along periodic axes) first, so that the last CTAs
+// of a launch are the shorter inner ones; 1: the tiles whose halo stays inside
+// the block's interior along its external axes (ext1 / ext2); 2: the other
+// tiles.  An 8x8 tile's halo reaches 3 cells past it, so only the outermost
+// tiles read ghost cells.
+__device__ __forceinline__ void qpair_tile(const QStageArgs& a, int bx, int& t1, int& t2) {
+    const int n1 = a.ntiles1, n2 = a.ntiles2;
+    if (a.tile_sel == 0) {
+        const int e1 = a.periodic1 ? 1 : 0, e2 = a.periodic2 ? 1 : 0;
+        const int ring = n1 * n2 - max(0, n1 - 2 * e1) * max(0, n2 - 2 * e2);
+        if (bx < ring) tile_ring(n1, n2, e1, e2, bx, t1, t2);
+        else tile_inner(n1, e1, e2, bx - ring, t1, t2);
+        return;
+    }
+    const int e1 = a.ext1 ? 1 : 0, e2 = a.ext2 ? 1 : 0;
+    if (a.tile_sel == 1) tile_inner(n1, e1, e2, bx, t1, t2);
+    else tile_ring(n1, n2, e1, e2, bx, t1, t2);
 }
 
 // Stage modes (which of out1 = base1 + c1 k, out2 = base2 + c2 k exist and
