@@ -530,7 +530,14 @@ def run_ours(args, rank, world, local_rank):
     # (strong scaling), beside the replicas of the headline
     decomposed = None
     if world > 1 and not args.no_decompose:
-        decomposed = slab_result(args, rank, world, local_rank, spec)
+        # the headline above stands whatever happens here: a failure of the
+        # slab split (e.g. peer mappings refused between the GPUs) is recorded
+        # in the line instead of ending the run
+        try:
+            decomposed = slab_result(args, rank, world, local_rank, spec)
+        except Exception as exc:                       # noqa: BLE001
+            decomposed = {'error': '%s: %s' % (type(exc).__name__, str(exc)[:300])}
+            torch.cuda.synchronize()
 
     # the benchmark set's other targets, on one GPU (kept out of the scaling runs)
     targets = None
