@@ -283,7 +283,9 @@ struct FaceWalker {
 // ---------------------------------------------------------------------------
 // Paired WENO5 walker: two q-cells per thread at the same p.  FP32 pairs use
 // the sm_100 f32x2 arithmetic; FP64 pairs are two scalar FP64 operations with
-// FMA and a Newton-refined reciprocal.  Both components share the lane's
+// FMA and a Newton-refined reciprocal.  The same walkers also run on a single
+// FP64 value per thread (P = double), for the one-row-per-thread form of the
+// stage kernel.  Both components share the lane's
 // upwind side, so they share the coefficient set.  Smoothness indicators use
 // a constant 1e-17 floor (the reference's 1e-17*(1+|a|+|b|+|c|) differs from
 // it only where f is flat to 1e-17: there every weight takes the floor and
@@ -323,6 +325,36 @@ __device__ __forceinline__ double2 sub2(double2 a, double2 b) {
 }
 __device__ __forceinline__ double2 rcp2(double2 a) { return make_double2(rcp_nr(a.x), rcp_nr(a.y)); }
 
+// one FP64 value per thread: the same operations on a scalar
+__device__ __forceinline__ double fma2(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ double mul2(double a, double b) { return a * b; }
+__device__ __forceinline__ double add2(double a, double b) { return a + b; }
+__device__ __forceinline__ double sub2(double a, double b) { return a - b; }
+__device__ __forceinline__ double rcp2(double a) { return rcp_nr(a); }
+
+// lane value -> its element type, a constant broadcast to it, and its
+// components (n = 2 for a pair, 1 for a scalar)
+template <typename P> struct LaneOf;
+template <> struct LaneOf<float2> {
+    typedef float E;
+    static constexpr int n = 2;
+    __device__ static float2 splat(float a) { return make_float2(a, a); }
+};
+template <> struct LaneOf<double2> {
+    typedef double E;
+    static constexpr int n = 2;
+    __device__ static double2 splat(double a) { return make_double2(a, a); }
+};
+template <> struct LaneOf<double> {
+    typedef double E;
+    static constexpr int n = 1;
+    __device__ static double splat(double a) { return a; }
+};
+// component c of a lane value
+__device__ __forceinline__ float& comp(float2& v, int c) { return c ? v.y : v.x; }
+__device__ __forceinline__ double& comp(double2& v, int c) { return c ? v.y : v.x; }
+__device__ __forceinline__ double& comp(double& v, int) { return v; }
+
 // element type -> pair type and the walker's constants in that type
 template <typename E> struct PairOf;
 template <> struct PairOf<float> {
@@ -348,17 +380,16 @@ template <> struct PairOf<double> {
 // (5, 10, 1)/16 (left), the walker returns TWICE the face value as
 //   (y2 + ys - D2_2/4) + (q3 D3b + r q1 D3a) / (a1 q1 + a2 q2 + a3 q3),
 // r = (w1 k1)/(w3 k3) and a_k = w_k / (2 w3 k3); callers halve the flux factor.
-template <typename E>
+template <typename E, typename P = typename PairOf<E>::P>
 struct Weno5PairT {
-    typedef typename PairOf<E>::P P;
     P r, a1, a2, a3;
     bool right;
     __device__ __forceinline__ void set(bool rt) {
         right = rt;
-        r = f2(rt ? BOLT_K(E, 0.6) : BOLT_KQ(E, 5, 3));
-        a1 = f2(rt ? BOLT_K(E, 0.8) : BOLT_KQ(E, -20, 3));
-        a2 = f2(rt ? BOLT_K(E, 8.0) : BOLT_KQ(E, -40, 3));
-        a3 = f2(rt ? BOLT_K(E, 4.0) : BOLT_KQ(E, -4, 3));
+        r = LaneOf<P>::splat(rt ? BOLT_K(E, 0.6) : BOLT_KQ(E, 5, 3));
+        a1 = LaneOf<P>::splat(rt ? BOLT_K(E, 0.8) : BOLT_KQ(E, -20, 3));
+        a2 = LaneOf<P>::splat(rt ? BOLT_K(E, 8.0) : BOLT_KQ(E, -40, 3));
+        a3 = LaneOf<P>::splat(rt ? BOLT_K(E, 4.0) : BOLT_KQ(E, -4, 3));
     }
 };
 
@@ -367,36 +398,37 @@ struct Weno5PairT {
 // (a - 4b + 3c)/2 = D2/2 + (c - b)
 template <typename P>
 __device__ __forceinline__ P beta_pair(P D2, P b, P c) {
-    typedef decltype(D2.x) E;
-    const P e = fma2(f2(BOLT_K(E, 0.5)), D2, sub2(c, b));
-    return fma2(mul2(f2(BOLT_KQ(E, 13, 12)), D2), D2, fma2(e, e, f2(BOLT_K(E, 1e-17))));
+    typedef typename LaneOf<P>::E E;
+    const P e = fma2(LaneOf<P>::splat(BOLT_K(E, 0.5)), D2, sub2(c, b));
+    return fma2(mul2(LaneOf<P>::splat(BOLT_KQ(E, 13, 12)), D2), D2,
+                fma2(e, e, LaneOf<P>::splat(BOLT_K(E, 1e-17))));
 }
 
 template <typename P>
 __device__ __forceinline__ P second_diff(P a, P b, P c) {
-    typedef decltype(a.x) E;
-    return fma2(f2(BOLT_K(E, -2.0)), b, add2(a, c));
+    typedef typename LaneOf<P>::E E;
+    return fma2(LaneOf<P>::splat(BOLT_K(E, -2.0)), b, add2(a, c));
 }
 
 // Sliding walker: carries 1/beta^2 of substencils 2 and 3, the second
 // difference of substencil 3 and the third difference D3b of the last face.
-template <typename E>
+template <typename E, typename P = typename PairOf<E>::P>
 struct Weno5PairWalkerT {
-    typedef typename PairOf<E>::P P;
+    typedef Weno5PairT<E, P> Side;
     P q2, q3, d23, d3b;
     __device__ __forceinline__ static P inv_sq(P b) {
         const P r = rcp2(b);
         return mul2(r, r);
     }
     __device__ __forceinline__ P eval(P q1, P d3a, P d22, P y1, P y2, P y3,
-                                      const Weno5PairT<E>& S) const {
+                                      const Side& S) const {
         const P ys = S.right ? y3 : y1;
-        const P base = fma2(f2(BOLT_K(E, -0.25)), d22, add2(y2, ys));
+        const P base = fma2(LaneOf<P>::splat(BOLT_K(E, -0.25)), d22, add2(y2, ys));
         const P num = fma2(q3, d3b, mul2(mul2(S.r, q1), d3a));
         const P den = fma2(S.a3, q3, fma2(S.a2, q2, mul2(S.a1, q1)));
         return fma2(num, rcp2(den), base);
     }
-    __device__ __forceinline__ P first(P y0, P y1, P y2, P y3, P y4, const Weno5PairT<E>& S) {
+    __device__ __forceinline__ P first(P y0, P y1, P y2, P y3, P y4, const Side& S) {
         const P d21 = second_diff(y0, y1, y2);
         const P d22 = second_diff(y1, y2, y3);
         d23 = second_diff(y2, y3, y4);
@@ -408,7 +440,7 @@ struct Weno5PairWalkerT {
         return eval(q1, d3a, d22, y1, y2, y3, S);
     }
     // window advanced by one cell: y0..y4 are the new window's values
-    __device__ __forceinline__ P next(P y0, P y1, P y2, P y3, P y4, const Weno5PairT<E>& S) {
+    __device__ __forceinline__ P next(P y0, P y1, P y2, P y3, P y4, const Side& S) {
         const P q1 = q2;
         const P d3a = d3b;
         const P d22 = d23;
@@ -424,47 +456,51 @@ struct Weno5PairWalkerT {
 // twice the face value of the window's centre cell y2 (its right face for
 // right-moving lanes, its left face otherwise), 2 y2 +- the limited slope of
 // (y1, y2, y3) (minmod.py:4-71).  No state is carried between faces.
-template <typename E>
+template <typename E, typename P = typename PairOf<E>::P>
 struct MinmodPairWalkerT {
-    typedef typename PairOf<E>::P P;
+    typedef Weno5PairT<E, P> Side;
     __device__ __forceinline__ static P face(P y1, P y2, P y3, bool right) {
         P sl;
-        sl.x = minmod_slope(y1.x, y2.x, y3.x);
-        sl.y = minmod_slope(y1.y, y2.y, y3.y);
-        if (!right) { sl.x = -sl.x; sl.y = -sl.y; }
-        return fma2(f2(BOLT_K(E, 2.0)), y2, sl);
+#pragma unroll
+        for (int c = 0; c < LaneOf<P>::n; ++c) {
+            const E m = minmod_slope(comp(y1, c), comp(y2, c), comp(y3, c));
+            comp(sl, c) = right ? m : -m;
+        }
+        return fma2(LaneOf<P>::splat(BOLT_K(E, 2.0)), y2, sl);
     }
-    __device__ __forceinline__ P first(P, P y1, P y2, P y3, P, const Weno5PairT<E>& S) {
+    __device__ __forceinline__ P first(P, P y1, P y2, P y3, P, const Side& S) {
         return face(y1, y2, y3, S.right);
     }
-    __device__ __forceinline__ P next(P, P y1, P y2, P y3, P, const Weno5PairT<E>& S) {
+    __device__ __forceinline__ P next(P, P y1, P y2, P y3, P, const Side& S) {
         return face(y1, y2, y3, S.right);
     }
 };
 
 // PPM (ppm.py:4-100) and piecewise-constant faces for the paired kernel:
 // twice the face value of the window's centre cell y2, per element
-template <typename E>
+template <typename E, typename P = typename PairOf<E>::P>
 struct PpmPairWalkerT {
-    typedef typename PairOf<E>::P P;
-    __device__ __forceinline__ P first(P y0, P y1, P y2, P y3, P y4, const Weno5PairT<E>& S) {
+    typedef Weno5PairT<E, P> Side;
+    __device__ __forceinline__ P first(P y0, P y1, P y2, P y3, P y4, const Side& S) {
         return next(y0, y1, y2, y3, y4, S);
     }
-    __device__ __forceinline__ P next(P y0, P y1, P y2, P y3, P y4, const Weno5PairT<E>& S) {
+    __device__ __forceinline__ P next(P y0, P y1, P y2, P y3, P y4, const Side& S) {
         P o;
-        o.x = E(2) * ppm_face(y0.x, y1.x, y2.x, y3.x, y4.x, S.right);
-        o.y = E(2) * ppm_face(y0.y, y1.y, y2.y, y3.y, y4.y, S.right);
+#pragma unroll
+        for (int c = 0; c < LaneOf<P>::n; ++c)
+            comp(o, c) = E(2) * ppm_face(comp(y0, c), comp(y1, c), comp(y2, c), comp(y3, c),
+                                         comp(y4, c), S.right);
         return o;
     }
 };
 
-template <typename E>
+template <typename E, typename P = typename PairOf<E>::P>
 struct ConstPairWalkerT {
-    typedef typename PairOf<E>::P P;
-    __device__ __forceinline__ P first(P, P, P y2, P, P, const Weno5PairT<E>&) {
+    typedef Weno5PairT<E, P> Side;
+    __device__ __forceinline__ P first(P, P, P y2, P, P, const Side&) {
         return add2(y2, y2);
     }
-    __device__ __forceinline__ P next(P, P, P y2, P, P, const Weno5PairT<E>&) {
+    __device__ __forceinline__ P next(P, P, P y2, P, P, const Side&) {
         return add2(y2, y2);
     }
 };

@@ -31,7 +31,11 @@
 // 16 p each (the swizzle covers 128-byte rows), stored by two TMA stores; the
 // RK4 accumulator's increment goes out by one bulk reduce-add (.add.f64) per
 // q-cell row, issued by the lanes of warp 0; one CTA per SM (221 KB of
-// shared memory).
+// shared memory).  With one CTA per SM the FP64 form walks ONE row (column)
+// per thread (ROWS = 1): 16 warps, q1 walkers warps 0-7 (row w, + BGK, then
+// the periodic ghost images), q2 walkers warps 8-15 (column w-8, then phase
+// C), at most 128 registers, so that twice the warps hide the FP64 latencies
+// that a single 8-warp CTA left exposed.
 //
 // Launch conditions (checked by the host): FP32 or FP64, any reconstruction in q, 8x8 tiling,
 // N_q1, N_q2 multiples of 8 and at least 2 N_g, N_p multiple of 32, N_p1
@@ -98,14 +102,15 @@ __device__ __forceinline__ void bulk_reduce_add_f64(double* gdst, const double* 
 // pairs over q-cell pairs P = m*8 + col (cells of rows 2m and 2m+1 in one tile
 // column, the pair a q1 walker holds): tab[q*kTabPitch + P], the pitch of 33
 // pairs keeping a warp's reads of different q (one per lane) on distinct banks.
-template <typename E, bool BGK>
+template <typename E, bool BGK, int NT>
 __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i0, int j0,
                                                double* vgrid, double* qc,
                                                typename PairOf<E>::P* tabs, int p3lo, int n3) {
+    static_assert(NT >= 256, "moment-sum mapping needs 256 threads");
     const int tid = threadIdx.x;
     const int Np1 = a.Np1, Np2 = a.Np2;
     const int ntab = Np1 + Np2 + a.Np3;
-    for (int q = tid; q < ntab; q += NTHREADS) {
+    for (int q = tid; q < ntab; q += NT) {
         if (q < Np1) vgrid[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
         else if (q < Np1 + Np2) vgrid[q] = a.sg.p2_start[s] + (0.5 + (q - Np1)) * a.sg.dp2[s];
         else vgrid[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
@@ -115,9 +120,9 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
         // (threads 0-63 also moment 4), all its partial-slot loads issued
         // before the first add, so the CTA waits for one round of loads; then
         // each cell's parameters from its sums
-        static_assert(NTHREADS == 256 && kNumMom == 5, "moment-sum mapping");
+        static_assert(kNumMom == 5, "moment-sum mapping");
         double* mm = qc + 64 * kNumMom;
-        {
+        if (NT == 256 || tid < 256) {
             const int c = tid & 63, q = tid >> 6;
             const int ii = i0 + (c & 7), jj = j0 + (c >> 3);
             const long long plane = (long long)a.Nq2 * a.Nq1;
@@ -157,7 +162,7 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
             mm[c * kNumMom + q] = v;
         }
         __syncthreads();
-        for (int c = tid; c < 64; c += NTHREADS)
+        for (int c = tid; c < 64; c += NT)
             bgk_params_from_sums<true>(a, s, mm + c * kNumMom, qc + c * 5);
     }
     __syncthreads();
@@ -171,7 +176,7 @@ __device__ __forceinline__ void qpair_prologue(const QStageArgs& a, int s, int i
         const double m = a.sg.mass[s];
         const int n12 = Np1 + Np2;
         E* tel = reinterpret_cast<E*>(tabs);
-        for (int t = tid; t < 64 * 3; t += NTHREADS) {
+        for (int t = tid; t < 64 * 3; t += NT) {
             const int c = t & 63, ax = t >> 6;
             const double* qq = qc + c * 5;
             // the table column of cell c: pair P, component hi (row 2m+1 of the pair)
@@ -274,29 +279,34 @@ __device__ __forceinline__ void qpair_tile(const QStageArgs& a, int bx, int& t1,
 //           enabled), no base, no moments
 enum QPairMode { QP_X1 = 0, QP_X2 = 1, QP_B1 = 2, QP_B1R2 = 3, QP_K = 4 };
 
-template <typename E, bool BGK, int MODE, int RECON>
-__global__ void __launch_bounds__(NTHREADS, sizeof(E) == 4 ? 2 : 1)
+template <typename E, bool BGK, int MODE, int RECON, int ROWS>
+__global__ void __launch_bounds__(ROWS == 2 ? NTHREADS : 2 * NTHREADS,
+                                  (sizeof(E) == 4 && ROWS == 2) ? 2 : 1)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
-    typedef typename PairOf<E>::P P;
+    static_assert(ROWS == 2 || (ROWS == 1 && sizeof(E) == 8), "single rows are FP64 only");
+    // a lane value: two rows (columns) as a pair, or one
+    typedef typename std::conditional<ROWS == 2, typename PairOf<E>::P, E>::type P;
     // WENO5 faces with the sliding walker, or minmod / PPM / piecewise-constant faces
     using Walker = typename std::conditional<
-        RECON == BOLT_RECON_MINMOD, MinmodPairWalkerT<E>,
+        RECON == BOLT_RECON_MINMOD, MinmodPairWalkerT<E, P>,
         typename std::conditional<
-            RECON == BOLT_RECON_PPM, PpmPairWalkerT<E>,
-            typename std::conditional<RECON == BOLT_RECON_PC, ConstPairWalkerT<E>,
-                                      Weno5PairWalkerT<E>>::type>::type>::type;
-    typedef Weno5PairT<E> Side;
+            RECON == BOLT_RECON_PPM, PpmPairWalkerT<E, P>,
+            typename std::conditional<RECON == BOLT_RECON_PC, ConstPairWalkerT<E, P>,
+                                      Weno5PairWalkerT<E, P>>::type>::type>::type;
+    typedef Weno5PairT<E, P> Side;
+    typedef typename PairOf<E>::P TabP;               // table entries: row pairs
+    constexpr int NT = ROWS == 2 ? NTHREADS : 2 * NTHREADS;
     constexpr int CS = PairStage<E>::CS, VE = PairStage<E>::VE;
     constexpr bool F64 = sizeof(E) == 8;
     constexpr bool BX = MODE == QP_X1 || MODE == QP_X2 || MODE == QP_K;   // no base tiles
     constexpr bool KOUT = MODE == QP_K;
     constexpr bool HAS2 = MODE == QP_X2 || MODE == QP_B1R2;
     constexpr bool RED2 = MODE == QP_B1R2;
-    constexpr int TQ = 8, HX = TQ + 2 * HALO, NQ = TQ * TQ, NWARP = NTHREADS / 32;
+    constexpr int TQ = 8, HX = TQ + 2 * HALO, NQ = TQ * TQ, NWARP = NT / 32;
     constexpr int XT = HX * HX * PW;                 // elements of one halo tile
     constexpr int TE = TQ * TQ * PW;                 // elements of one 8x8 tile
     constexpr int NQUART = NTHREADS / NQ;            // phase C: threads per q-cell
-    static_assert(NWARP == 8 && NQUART == 4, "pair mapping assumes 8 warps");
+    static_assert(NWARP == 8 * (3 - ROWS) && NQUART == 4, "8 walkers per direction");
 
     const int Np1 = a.Np1, Np2 = a.Np2, Np = a.Np, Ng = a.Ng;
     const int Nq1 = a.Nq1, Nq2 = a.Nq2;
@@ -309,7 +319,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     E* o2s = reinterpret_cast<E*>(sm + Lo.o2);
     E* b1s = reinterpret_cast<E*>(sm + Lo.b1);
     E* d1s = reinterpret_cast<E*>(sm + Lo.d1);
-    P* tabs = reinterpret_cast<P*>(sm + Lo.tabs);
+    TabP* tabs = reinterpret_cast<TabP*>(sm + Lo.tabs);
     double* vgrid = reinterpret_cast<double*>(sm + Lo.vgrid);
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + Lo.bars);
 
@@ -366,12 +376,13 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     // p3 rows of this CTA's p-range (the tables hold only those)
     const int p3lo = (k_begin * PW) / (Np1 * Np2);
     const int n3 = k_begin < k_end ? (k_end * PW - 1) / (Np1 * Np2) - p3lo + 1 : 0;
-    qpair_prologue<E, BGK>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, p3lo, n3);
+    qpair_prologue<E, BGK, NT>(a, s, i0, j0, vgrid, reinterpret_cast<double*>(d1s), tabs, p3lo,
+                               n3);
 
     E* __restrict__ out1 = static_cast<E*>(a.out1);
-    const P c1 = f2(E(a.c1)), c2 = f2(E(a.c2));
+    const P c1 = LaneOf<P>::splat(E(a.c1)), c2 = LaneOf<P>::splat(E(a.c2));
     const E inv_dq1 = E(1.0 / a.dq1), inv_dq2 = E(1.0 / a.dq2);
-    const P inv_tau = f2(E(1.0 / a.tau));
+    const P inv_tau = LaneOf<P>::splat(E(1.0 / a.tau));
     const bool want_mom = a.mom_out != nullptr;
     const bool check = a.flag != nullptr;
     const unsigned rowstride = (unsigned)(a.Ns * Np);
@@ -384,32 +395,51 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         const int p = k_begin * PW + lane;
         ip1 = p % Np1; ip2 = (p / Np1) % Np2; ip3 = p / (Np1 * Np2);
     }
-    // phase C: q-cell pc_c = (row warp, col lane%8), p = k*32 + 8*pc_q .. +7
+    // phase C (all warps of the pair form, the q2 walkers of the single-row
+    // form): q-cell pc_c = (row warp%8, col lane%8), p = k*32 + 8*pc_q .. +7
     // with pc_q = lane/8: the group holds the lane's own p and lies in one p1
     // row (N_p1 % 8 == 0), so its velocities follow from the lane's
-    const int pc_c = warp * TQ + (lane & 7), pc_q = lane >> 3;
+    const int pc_w = ROWS == 2 ? warp : (warp & 7);
+    const int pc_c = pc_w * TQ + (lane & 7), pc_q = lane >> 3;
     const double dp1 = a.sg.dp1[s];
     const double t_own = double(lane & 7);
     double macc[kNumMom] = {0, 0, 0, 0, 0};
 
-    // q1 walkers (warps 0-3): rows 2w, 2w+1; q2 walkers (warps 4-7): columns
-    // 2(w-4), 2(w-4)+1; each walks the 8 cells of its line
-    const bool q1w = warp < 4;
-    const int lp = 2 * (warp & 3);                    // first row (q1) or column (q2)
+    // pairs: q1 walkers (warps 0-3) rows 2w, 2w+1, q2 walkers (warps 4-7)
+    // columns 2(w-4), 2(w-4)+1; single rows: q1 walkers (warps 0-7) row w, q2
+    // walkers (warps 8-15) column w-8; each walks the 8 cells of its line
+    const bool q1w = warp < NWARP / 2;
+    const bool pc_on = ROWS == 2 || !q1w;             // this warp runs phase C
+    const int lp = ROWS == 2 ? 2 * (warp & 3) : (warp & 7);   // first row / column
     const int sw0 = stg<E>(lp, lane) - lp * CS;       // swizzled lane slot, column lp
     const int sw1 = stg<E>(lp + 1, lane) - (lp + 1) * CS;
+    // a lane value from element p (and p + off, the pair's second line), and back
+    auto ld = [](const E* p, int off) -> P {
+        if constexpr (ROWS == 2) return mk2(p[0], p[off]);
+        else return p[0];
+    };
+    auto st = [](E* p, int off, P v) {
+        if constexpr (ROWS == 2) { p[0] = v.x; p[off] = v.y; }
+        else p[0] = v;
+    };
     // phase C source: 8 p from 16-byte chunk c_ch0 of q-cell pc_c's staging row
     const E* c_row = o1s + (8 * pc_q / CS) * 64 * CS + pc_c * CS;
     const int c_ch0 = (8 * pc_q % CS) / VE, c_key = pc_c & 7;
-    const P* tb_row = tabs + (warp & 3) * TQ;             // pairs of rows lp, lp+1 (q1)
+    // table entries of row lp (its pair, or its component of the pair), TW
+    // lane values per table pair
+    constexpr int TW = 3 - ROWS;
+    const P* tb_row = reinterpret_cast<const P*>(reinterpret_cast<const E*>(tabs) +
+                                                 2 * (lp >> 1) * TQ + (ROWS == 2 ? 0 : (lp & 1)));
 
     // periodic ghost images (border CTAs): offsets of column `warp` of the
     // tile, the q1 image shift g_d1, and the rows [0, g_bot) with a q2 image
     // at +N_q2 and [g_top, TQ) with one at -N_q2 (element offsets)
+    // (pairs: every warp; single rows: the q1 walkers)
     int g_src = 0, g_dst = 0, g_d1 = 0, g_d2 = 0, g_bot = 0, g_top = TQ;
-    if (border) {
-        const int ii = i0 + warp;
-        g_src = stg<E>(warp, lane);                        // row r adds r*TQ*CS
+    const bool g_on = border && (ROWS == 2 || q1w);
+    if (g_on) {
+        const int ii = i0 + pc_w;
+        g_src = stg<E>(pc_w, lane);                        // row r adds r*TQ*CS
         g_dst = (j0 + Ng) * (int)colstride + (ii + Ng) * (int)rowstride + xs + lane;
         if (a.periodic1 || peer1)
             g_d1 = ii < Ng ? Nq1 * (int)rowstride : (ii >= Nq1 - Ng ? -Nq1 * (int)rowstride : 0);
@@ -438,58 +468,57 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             const bool right = v1 > E(0);
             Side S; S.set(right);
             const E* ra = Xb + ((lp + HALO) * HX + (right ? 0 : 1)) * PW + lane;
-            const E* rb = ra + HX * PW;
-            P y0 = mk2(ra[0 * PW], rb[0 * PW]);
-            P y1 = mk2(ra[1 * PW], rb[1 * PW]);
-            P y2 = mk2(ra[2 * PW], rb[2 * PW]);
-            P y3 = mk2(ra[3 * PW], rb[3 * PW]);
-            P y4 = mk2(ra[4 * PW], rb[4 * PW]);
+            constexpr int rb = HX * PW;                // the pair's second row
+            P y0 = ld(ra + 0 * PW, rb);
+            P y1 = ld(ra + 1 * PW, rb);
+            P y2 = ld(ra + 2 * PW, rb);
+            P y3 = ld(ra + 3 * PW, rb);
+            P y4 = ld(ra + 4 * PW, rb);
             Walker W;
-            const P vq = f2(E(0.5) * v1 * inv_dq1);   // walker returns 2x face value
+            const P vq = LaneOf<P>::splat(E(0.5) * v1 * inv_dq1);   // walker: 2x face value
             P Fprev = W.first(y0, y1, y2, y3, y4, S);
             E* da = d1s + lp * TQ * PW + lane;
-            const P* t1 = tb_row + ip1 * kTabPitch;
-            const P* t2 = tb_row + (Np1 + ip2) * kTabPitch;
-            const P* t3 = tb_row + (Np1 + Np2 + ip3 - p3lo) * kTabPitch;
+            const P* t1 = tb_row + ip1 * kTabPitch * TW;
+            const P* t2 = tb_row + (Np1 + ip2) * kTabPitch * TW;
+            const P* t3 = tb_row + (Np1 + Np2 + ip3 - p3lo) * kTabPitch * TW;
 #pragma unroll
             for (int c = 0; c < TQ; ++c) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                y4 = mk2(ra[(c + 5) * PW], rb[(c + 5) * PW]);
+                y4 = ld(ra + (c + 5) * PW, rb);
                 const P Fn = W.next(y0, y1, y2, y3, y4, S);
                 P d = mul2(sub2(Fprev, Fn), vq);
                 Fprev = Fn;
                 if (BGK) {
                     // the cell itself is the window's y2 (right-moving) or y1
                     const P fcell = right ? y2 : y1;
-                    const P f0 = mul2(mul2(t1[c], t2[c]), t3[c]);
+                    const P f0 = mul2(mul2(t1[c * TW], t2[c * TW]), t3[c * TW]);
                     d = fma2(sub2(f0, fcell), inv_tau, d);
                 }
-                da[c * PW] = d.x;
-                da[(TQ + c) * PW] = d.y;
+                st(da + c * PW, TQ * PW, d);
             }
             // the store of chunk k-1 must be done reading the staging tiles
             // before the q2 walkers write them
             if (warp == 0) bulk_wait_read_all();
-            named_bar_arrive(1, NTHREADS);
+            named_bar_arrive(1, NT);
         } else {
             // ---- q2 faces of columns lp, lp+1, then combine with D1 ---------------
             const E v2 = E(V2);
             const bool right = v2 > E(0);
             Side S; S.set(right);
             const E* ca = Xb + ((right ? 0 : 1) * HX + lp + HALO) * PW + lane;
-            const E* cb = ca + PW;
-            P y0 = mk2(ca[0 * HX * PW], cb[0 * HX * PW]);
-            P y1 = mk2(ca[1 * HX * PW], cb[1 * HX * PW]);
-            P y2 = mk2(ca[2 * HX * PW], cb[2 * HX * PW]);
-            P y3 = mk2(ca[3 * HX * PW], cb[3 * HX * PW]);
-            P y4 = mk2(ca[4 * HX * PW], cb[4 * HX * PW]);
+            constexpr int cb = PW;                     // the pair's second column
+            P y0 = ld(ca + 0 * HX * PW, cb);
+            P y1 = ld(ca + 1 * HX * PW, cb);
+            P y2 = ld(ca + 2 * HX * PW, cb);
+            P y3 = ld(ca + 3 * HX * PW, cb);
+            P y4 = ld(ca + 4 * HX * PW, cb);
             Walker W;
             P Fprev = W.first(y0, y1, y2, y3, y4, S);
             P dq[TQ];                                  // flux differences of rows 0..7
 #pragma unroll
             for (int r = 0; r < TQ; ++r) {
                 y0 = y1; y1 = y2; y2 = y3; y3 = y4;
-                y4 = mk2(ca[(r + 5) * HX * PW], cb[(r + 5) * HX * PW]);
+                y4 = ld(ca + (r + 5) * HX * PW, cb);
                 const P Fn = W.next(y0, y1, y2, y3, y4, S);
                 dq[r] = sub2(Fprev, Fn);
                 Fprev = Fn;
@@ -497,8 +526,8 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             if (!BX && !failed &&
                 !mbar_wait_bounded(&bars[2 + buf], buf ? phb1 : phb0, a.wait_cycles))
                 failed = true;
-            named_bar_sync(1, NTHREADS);              // D1 written, staging tiles free
-            const P vq = f2(E(0.5) * v2 * inv_dq2);
+            named_bar_sync(1, NT);                    // D1 written, staging tiles free
+            const P vq = LaneOf<P>::splat(E(0.5) * v2 * inv_dq2);
             const E* dk = d1s + lp * PW + lane;
             const E* bb1 = b1s + buf * TE + lp * PW + lane;
             const E* cella = Xb + (HALO * HX + lp + HALO) * PW + lane;
@@ -506,19 +535,20 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             E* ob2 = o2s + lp * PW + lane;
 #pragma unroll
             for (int r = 0; r < TQ; ++r) {
-                const P kq = mk2(dk[r * TQ * PW], dk[r * TQ * PW + PW]);
+                const P kq = ld(dk + r * TQ * PW, PW);
                 const P kk = fma2(dq[r], vq, kq);
-                const P fcell = BX ? mk2(cella[r * HX * PW], cella[r * HX * PW + PW]) : kk;
-                const P o1 = KOUT ? kk
-                                  : fma2(kk, c1, BX ? fcell : mk2(bb1[r * TQ * PW],
-                                                                  bb1[r * TQ * PW + PW]));
-                ob1[r * TQ * CS + sw0] = o1.x;
-                ob1[r * TQ * CS + CS + sw1] = o1.y;
+                const P fcell = BX ? ld(cella + r * HX * PW, PW) : kk;
+                const P o1 = KOUT ? kk : fma2(kk, c1, BX ? fcell : ld(bb1 + r * TQ * PW, PW));
+                if constexpr (ROWS == 2) {
+                    ob1[r * TQ * CS + sw0] = o1.x;
+                    ob1[r * TQ * CS + CS + sw1] = o1.y;
+                } else {
+                    ob1[r * TQ * CS + sw0] = o1;
+                }
                 if (HAS2) {
                     // QP_X2: the full out2; QP_B1R2: the increment c2 k
                     const P o2 = RED2 ? mul2(kk, c2) : fma2(kk, c2, fcell);
-                    ob2[r * TQ * PW] = o2.x;
-                    ob2[r * TQ * PW + PW] = o2.y;
+                    st(ob2 + r * TQ * PW, PW, o2);
                 }
             }
         }
@@ -555,9 +585,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         }
 
         // ---- periodic ghost images of border cells, from the staged out1 -------
-        // warp w owns tile column w; images along q1 (whole column), along q2
+        // warp w owns tile column w%8; images along q1 (whole column), along q2
         // (rows below g_bot and from g_top) and at the corners (2 N_g <= N_q)
-        if (border) {
+        if (g_on) {
             const E* src = o1s + g_src;
             E* dst = out1 + (g_dst + k * PW);
             // q1 / q2 images: this buffer (periodic axis) or the neighbours'
@@ -589,7 +619,7 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
         // 8 consecutive p of one p1 row: v1 = V1_0 + t dp1 (t = 0..7), v2, v3
         // fixed, so every moment follows from S0 = sum o_t, S1 = sum t o_t and
         // S2 = sum t^2 o_t (moments.py:6-24 / compute_moments.py:7-59)
-        if (want_mom || check) {
+        if ((want_mom || check) && pc_on) {
             double ov[8];
             load8(c_row, c_ch0, c_key, ov);
             const double o0 = ov[0], o1 = ov[1], o2 = ov[2], o3 = ov[3];
@@ -636,10 +666,12 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     const long long plane = (long long)Nq2 * Nq1;
     if (want_mom) {
         double* red = reinterpret_cast<double*>(sm + Lo.x);
+        if (pc_on) {
 #pragma unroll
-        for (int q = 0; q < kNumMom; ++q) red[(pc_q * NQ + pc_c) * kNumMom + q] = macc[q];
+            for (int q = 0; q < kNumMom; ++q) red[(pc_q * NQ + pc_c) * kNumMom + q] = macc[q];
+        }
         __syncthreads();
-        for (int c = tid; c < NQ * kNumMom; c += NTHREADS) {
+        for (int c = tid; c < NQ * kNumMom; c += NT) {
             const int cq = c / kNumMom, q = c % kNumMom;
             double v = 0.0;
 #pragma unroll
@@ -651,14 +683,20 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
     }
 }
 
-template <typename E, int R>
+template <typename E, int R, int W>
 static void (*pick_qpair(int bgk, int mode))(QStageArgs) {
     switch (mode) {
-        case QP_X1: return bgk ? qpair_kernel<E, true, QP_X1, R> : qpair_kernel<E, false, QP_X1, R>;
-        case QP_X2: return bgk ? qpair_kernel<E, true, QP_X2, R> : qpair_kernel<E, false, QP_X2, R>;
-        case QP_B1: return bgk ? qpair_kernel<E, true, QP_B1, R> : qpair_kernel<E, false, QP_B1, R>;
-        case QP_K: return bgk ? qpair_kernel<E, true, QP_K, R> : qpair_kernel<E, false, QP_K, R>;
-        default: return bgk ? qpair_kernel<E, true, QP_B1R2, R> : qpair_kernel<E, false, QP_B1R2, R>;
+        case QP_X1:
+            return bgk ? qpair_kernel<E, true, QP_X1, R, W> : qpair_kernel<E, false, QP_X1, R, W>;
+        case QP_X2:
+            return bgk ? qpair_kernel<E, true, QP_X2, R, W> : qpair_kernel<E, false, QP_X2, R, W>;
+        case QP_B1:
+            return bgk ? qpair_kernel<E, true, QP_B1, R, W> : qpair_kernel<E, false, QP_B1, R, W>;
+        case QP_K:
+            return bgk ? qpair_kernel<E, true, QP_K, R, W> : qpair_kernel<E, false, QP_K, R, W>;
+        default:
+            return bgk ? qpair_kernel<E, true, QP_B1R2, R, W>
+                       : qpair_kernel<E, false, QP_B1R2, R, W>;
     }
 }
 
@@ -676,16 +714,19 @@ static cudaError_t launch_qpair(const QStageArgs& a, int bgk, int recon, dim3 gr
     else if (!has2) mode = QP_B1;
     else if (a.base2 == a.out2) mode = QP_B1R2;
     else return cudaErrorInvalidValue;        // excluded by the host's dispatch
+    // FP32: row pairs, 8 warps, 2 CTAs per SM; FP64: one row per thread, 16
+    // warps, 1 CTA per SM (the shared memory of the double-buffered tiles)
+    constexpr int W = sizeof(E) == 4 ? 2 : 1;
     void (*k)(QStageArgs);
     switch (recon) {
-        case BOLT_RECON_MINMOD: k = pick_qpair<E, BOLT_RECON_MINMOD>(bgk, mode); break;
-        case BOLT_RECON_PPM: k = pick_qpair<E, BOLT_RECON_PPM>(bgk, mode); break;
-        case BOLT_RECON_PC: k = pick_qpair<E, BOLT_RECON_PC>(bgk, mode); break;
-        default: k = pick_qpair<E, BOLT_RECON_WENO5>(bgk, mode); break;
+        case BOLT_RECON_MINMOD: k = pick_qpair<E, BOLT_RECON_MINMOD, W>(bgk, mode); break;
+        case BOLT_RECON_PPM: k = pick_qpair<E, BOLT_RECON_PPM, W>(bgk, mode); break;
+        case BOLT_RECON_PC: k = pick_qpair<E, BOLT_RECON_PC, W>(bgk, mode); break;
+        default: k = pick_qpair<E, BOLT_RECON_WENO5, W>(bgk, mode); break;
     }
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k<<<grid, NTHREADS, smem, st>>>(a);
+    k<<<grid, W == 2 ? NTHREADS : 2 * NTHREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 
