@@ -1,6 +1,6 @@
-// Paired FP64 stage kernel (dtype BOLT_F64_FAST): the fused RK stage of
-// qpair_kernel.cuh on FP64 pairs, built with FMA contraction (no -fmad=false)
-// and Newton-refined reciprocals instead of IEEE divisions.  Its results
+// FP64 throughput stage kernel (dtype BOLT_F64_FAST): the fused RK stage of
+// qpair_kernel.cuh on FP64, one q-row per thread, built with FMA contraction
+// (no -fmad=false) and Newton-refined reciprocals instead of IEEE divisions.  Its results
 // differ from the reference-order FP64 kernels in rounding only.
 #include "launch.h"
 #include "qpair_kernel.cuh"

@@ -18,7 +18,7 @@
 //   phase C     all warps, after the CTA barrier that closes the chunk: FP64
 //               velocity moments of out1 and the divergence check
 //
-// All global traffic is TMA: the halo tile of the stage input (14x14x32,
+// All global traffic of the FP32 form is TMA: the halo tile of the stage input (14x14x32,
 // double-buffered), the base1 tile (8x8x32, double-buffered; taken from the
 // halo tile when it is the stage input itself) and the out1/out2 tiles; an
 // out2 that is its own base (the RK4 accumulator) gets c2 k by TMA reduce-add
@@ -29,8 +29,10 @@
 //
 // FP64 differences: the out1 staging tile is two 128-byte-swizzled halves of
 // 16 p each (the swizzle covers 128-byte rows), stored by two TMA stores; the
-// RK4 accumulator's increment goes out by one bulk reduce-add (.add.f64) per
-// q-cell row, issued by the lanes of warp 0; one CTA per SM (221 KB of
+// RK4 accumulator's increment goes from the q2 walkers' registers into global
+// memory by red.global.add.f64 (coalesced 256-byte rows; the TMA unit has no
+// FP64 tensor reduction, and 64 row-wise bulk reductions issued by one warp
+// held that warp back by a third of each chunk); one CTA per SM (221 KB of
 // shared memory).  With one CTA per SM the FP64 form walks ONE row (column)
 // per thread (ROWS = 1): 16 warps, q1 walkers warps 0-7 (row w, + BGK, then
 // the periodic ghost images), q2 walkers warps 8-15 (column w-8, then phase
@@ -88,13 +90,6 @@ __device__ __forceinline__ void load8(const double* row, int ch0, int key, doubl
 
 __device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
-
-// shared -> global bulk reduce-add of n FP64 values (16-byte aligned, n*8 a
-// multiple of 16), bulk-group completion of the issuing thread
-__device__ __forceinline__ void bulk_reduce_add_f64(double* gdst, const double* ssrc, unsigned bytes) {
-    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;"
-                 ::"l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes) : "memory");
-}
 
 // Prologue (the tile loads already in flight): p-cell centres of the species,
 // and for BGK the Maxwellian of the stage input per q-cell with exp tables
@@ -283,7 +278,7 @@ template <typename E, bool BGK, int MODE, int RECON, int ROWS>
 __global__ void __launch_bounds__(ROWS == 2 ? NTHREADS : 2 * NTHREADS,
                                   (sizeof(E) == 4 && ROWS == 2) ? 2 : 1)
 qpair_kernel(const __grid_constant__ QStageArgs a) {
-    static_assert(ROWS == 2 || (ROWS == 1 && sizeof(E) == 8), "single rows are FP64 only");
+    static_assert((ROWS == 1) == (sizeof(E) == 8), "FP64 walks single rows, FP32 row pairs");
     // a lane value: two rows (columns) as a pair, or one
     typedef typename std::conditional<ROWS == 2, typename PairOf<E>::P, E>::type P;
     // WENO5 faces with the sliding walker, or minmod / PPM / piecewise-constant faces
@@ -533,6 +528,9 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             const E* cella = Xb + (HALO * HX + lp + HALO) * PW + lane;
             E* ob1 = o1s + lp * CS;
             E* ob2 = o2s + lp * PW + lane;
+            // FP64 accumulator: element (row r, column lp, p) of chunk k
+            E* accp = static_cast<E*>(a.out2) + ((j0 + Ng) * colstride +
+                                                 (i0 + lp + Ng) * rowstride + xs + k * PW + lane);
 #pragma unroll
             for (int r = 0; r < TQ; ++r) {
                 const P kq = ld(dk + r * TQ * PW, PW);
@@ -545,7 +543,11 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
                 } else {
                     ob1[r * TQ * CS + sw0] = o1;
                 }
-                if (HAS2) {
+                if constexpr (RED2 && F64) {
+                    // the increment c2 k straight into the accumulator: one
+                    // add per element and stage, so acc + inc exactly
+                    atomicAdd(accp + r * colstride, mul2(kk, c2));
+                } else if (HAS2) {
                     // QP_X2: the full out2; QP_B1R2: the increment c2 k
                     const P o2 = RED2 ? mul2(kk, c2) : fma2(kk, c2, fcell);
                     st(ob2 + r * TQ * PW, PW, o2);
@@ -566,22 +568,6 @@ qpair_kernel(const __grid_constant__ QStageArgs a) {
             bulk_commit();
             load_x(k + 2, buf);
             load_b(k + 2, buf);
-        }
-        if constexpr (RED2 && F64) {
-            if (warp == 0) {
-                // the accumulator increment, one 256-byte row per q-cell, two per lane
-                double* acc = static_cast<double*>(a.out2);
-                const double* inc = reinterpret_cast<const double*>(o2s);
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int c = lane + 32 * h;
-                    const int ii = i0 + (c & 7), jj = j0 + (c >> 3);
-                    bulk_reduce_add_f64(acc + ((long long)(jj + Ng) * colstride +
-                                               (long long)(ii + Ng) * rowstride + xs + k * PW),
-                                        inc + c * PW, PW * sizeof(double));
-                }
-                bulk_commit();
-            }
         }
 
         // ---- periodic ghost images of border cells, from the staged out1 -------
