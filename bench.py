@@ -478,8 +478,8 @@ def run_ours(args, rank, world, local_rank):
 
     # the FP64 forms of the same workload, reported beside the FP32 number:
     # 'fp64' keeps the reference's operation order (-fmad=false, IEEE
-    # divisions; the 1e-12 parity path), 'fp64-fast' runs the paired kernel
-    # on FP64 pairs with FMA and Newton-refined reciprocals
+    # divisions; the 1e-12 parity path), 'fp64-fast' runs the paired kernel's
+    # FP64 form (one q-row per thread) with FMA and Newton-refined reciprocals
     fp64 = fp64f = None
     if args.precision == 'fp32' and not args.no_fp64:
         del host_in, host_out, stage_in, stage_out
@@ -519,7 +519,7 @@ def run_ours(args, rank, world, local_rank):
         fp64f = {'value': job_value(cells, world, msf), 'ms_per_step': msf,
                  'bytes_per_cell_update': 136,
                  'hbm_frac': 136 * cells / (msf * 1e-3) / (peak * 1e9),
-                 'kernel': 'qpair_kernel<double> (FMA, Newton-refined reciprocals)',
+                 'kernel': 'qpair_kernel<double> (one q-row per thread, FMA, Newton-refined reciprocals)',
                  'paired_launches': pairf,
                  'rel_l2_error_vs_fp64': err(momf),
                  'fp32_over_fp64_fast': msf / ms,

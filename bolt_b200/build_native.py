@@ -3,7 +3,7 @@
     python -m bolt_b200.build_native          # -> bolt_b200/_native/libbolt_b200.so
 
 The FP64 kernels are compiled with -fmad=false so that their arithmetic
-follows the reference's operation order; the FP32 kernels and the paired FP64
+follows the reference's operation order; the FP32 kernels and the FP64
 kernel of the fast FP64 form use FMA and approximate division (FP32) or
 Newton-refined reciprocals (FP64).  The library links the CUDA runtime statically and
 loads cuTensorMapEncodeTiled through the runtime's driver entry point.
