@@ -48,7 +48,7 @@ __device__ __forceinline__ bool asl_q_row(const AslArgs& a, long long e) {
     const int p = (int)(e % a.Np);
     const long long r = e / a.Np;
     const int s = (int)(r % a.Ns), j = (int)(r / a.Ns);
-    const int Ng = a.Ng, Nq1g = a.Nq1 + 2 * Ng, Nq2g = a.Nq2 + 2 * Ng;
+    const int Ng = a.Ng, Nq1 = a.Nq1, Nq1g = a.Nq1 + 2 * Ng, Nq2g = a.Nq2 + 2 * Ng;
     const int ip1 = p % a.Np1, ip2 = (p / a.Np1) % a.Np2;
     const double v1 = a.sg.p1_start[s] + (0.5 + ip1) * a.sg.dp1[s];
     const double v2 = a.sg.p2_start[s] + (0.5 + ip2) * a.sg.dp2[s];
@@ -80,38 +80,67 @@ __device__ __forceinline__ bool asl_q_row(const AslArgs& a, long long e) {
     const T* rows[4];
 #pragma unroll
     for (int b = 0; b < 4; ++b) rows[b] = f + min(max(j0 - 1 + b, 0), Nq2g - 1) * colstride;
-    T* out = static_cast<T*>(a.out) + (j + Ng) * colstride + (long long)Ng * rowstride +
-             (long long)s * a.Np + p;
+    T* __restrict__ out = static_cast<T*>(a.out) + (j + Ng) * colstride +
+                          (long long)Ng * rowstride + (long long)s * a.Np + p;
+    // column c of the ghosted row, clamped
+    auto col = [&](int b, int c) { return rows[b][min(max(c, 0), Nq1g - 1) * rowstride]; };
+    // the cell's value from the window (0 where the foot lies off the array)
+    auto cell = [&](const T (&w)[4][4], int i) {
+        const double x = x0 + i;
+        const bool off = offy || !(x >= 0.0 && x <= double(Nq1g - 1));
+        T acc = T(0);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            T row = T(0);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) row = row + wx[c] * w[b][c];
+            acc = acc + wy[b] * row;
+        }
+        return off ? T(0) : acc;
+    };
     // window[b][c]: row b, column clamp(i00 + i - 1 + c) of cell i
     T win[4][4];
 #pragma unroll
     for (int b = 0; b < 4; ++b)
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            win[b][c + 1] = rows[b][min(max(i00 - 1 + c, 0), Nq1g - 1) * rowstride];
-    for (int i = 0; i < a.Nq1; ++i) {
-        const int ni = i00 + i;
+        for (int c = 0; c < 3; ++c) win[b][c + 1] = col(b, i00 - 1 + c);
+    int i = 0;
+    // G cells per round (8 in FP32, 4 in FP64): their 4 G new samples are all
+    // loaded before the first of the G cells is computed and stored (the
+    // interpolation is latency-bound: many loads in flight per thread pay
+    // more than occupancy)
+    constexpr int G = sizeof(T) == 4 ? 8 : 4;
+    for (; i + G <= Nq1; i += G) {
+        T nc[G][4];
+#pragma unroll
+        for (int u = 0; u < G; ++u)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) nc[u][b] = col(b, i00 + i + u + 2);
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                win[b][0] = win[b][1];
+                win[b][1] = win[b][2];
+                win[b][2] = win[b][3];
+                win[b][3] = nc[u][b];
+            }
+            const T v = cell(win, i + u);
+            out[(long long)(i + u) * rowstride] = v;
+            bad |= !isfinite(double(v));
+        }
+    }
+    for (; i < Nq1; ++i) {
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             win[b][0] = win[b][1];
             win[b][1] = win[b][2];
             win[b][2] = win[b][3];
-            win[b][3] = rows[b][min(max(ni + 2, 0), Nq1g - 1) * rowstride];
+            win[b][3] = col(b, i00 + i + 2);
         }
-        const double x = x0 + i;
-        const bool off = offy || !(x >= 0.0 && x <= double(Nq1g - 1));
-        T acc = T(0);
-        if (!off) {
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                T row = T(0);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) row = row + wx[c] * win[b][c];
-                acc = acc + wy[b] * row;
-            }
-        }
-        out[(long long)i * rowstride] = acc;
-        bad |= !isfinite(double(acc));
+        const T v = cell(win, i);
+        out[(long long)i * rowstride] = v;
+        bad |= !isfinite(double(v));
     }
     return bad;
 }
@@ -135,50 +164,125 @@ __global__ void __launch_bounds__(256) asl_q_kernel(const AslArgs a, int* flag) 
 // q-cell): mode 0, out = base + c * (-(in - f_MB) / tau) with f_MB from the
 // moments of `in` (a.mom_in, one partial slot); mode 1, out = f_MB.  The
 // Maxwellian is the product of its per-axis factors, tabulated once per
-// q-cell (the p1 factor carries n times the normalisation).
+// q-cell (the p1 factor carries n times the normalisation).  With mom_out,
+// the five moment sums of the written values go to that partial slot (the
+// next source evaluation needs no separate moment pass).  The p-block is
+// streamed in 16-byte vectors when N_p1 is a multiple of the vector width and
+// the buffers are 16-byte aligned; four CTAs per SM (at most 64 registers)
+// overlap one CTA's Maxwellian set-up with the others' streaming.
 constexpr int kAslMaxTab = 768;
 template <typename T>
-__global__ void __launch_bounds__(256) asl_src_kernel(const QStageArgs a, const void* in,
-                                                      const void* base, void* out, double c,
-                                                      int mode, int* flag) {
+__global__ void __launch_bounds__(256, 4) asl_src_kernel(const QStageArgs a, const void* in,
+                                                         const void* base, void* out, double c,
+                                                         int mode, int* flag, double* mom_out) {
     __shared__ double qq[5];
     __shared__ double vg[kAslMaxTab];
     __shared__ double tab[kAslMaxTab];
-    const int cell = blockIdx.x, s = blockIdx.y;
+    __shared__ double red[8][kNumMom];
+    const int cell = blockIdx.x, s = blockIdx.y, tid = threadIdx.x;
     const int ii = cell % a.Nq1, jj = cell / a.Nq1;
     const int Np1 = a.Np1, Np2 = a.Np2, Np3 = a.Np3;
     const int ntab = Np1 + Np2 + Np3;             // <= kAslMaxTab (checked by the host)
-    if (threadIdx.x == 0) bgk_cell_params(a, s, ii, jj, qq);
-    for (int q = threadIdx.x; q < ntab; q += blockDim.x) {
-        if (q < Np1) vg[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
-        else if (q < Np1 + Np2) vg[q] = a.sg.p2_start[s] + (0.5 + (q - Np1)) * a.sg.dp2[s];
-        else vg[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
-    }
-    __syncthreads();
-    const double m = a.sg.mass[s];
-    for (int q = threadIdx.x; q < ntab; q += blockDim.x) tab[q] = bgk_table_entry(a, qq, vg, q, m);
-    __syncthreads();
     const long long rowstride = (long long)a.Ns * a.Np;
     const long long colstride = rowstride * a.Nq1g;
     const long long o = (jj + a.Ng) * colstride + (ii + a.Ng) * rowstride + (long long)s * a.Np;
     const T* fi = static_cast<const T*>(in) + o;
     const T* fb = static_cast<const T*>(base) + o;
     T* fo = static_cast<T*>(out) + o;
-    bool bad = false;
-    for (int p = threadIdx.x; p < a.Np; p += blockDim.x) {
-        const int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
-        const double f0 = (tab[ip1] * tab[Np1 + ip2]) * tab[Np1 + Np2 + ip3];
-        T v;
-        if (mode == 1) {
-            v = T(f0);
-        } else {
-            const double src = -(double(fi[p]) - f0) / a.tau;
-            v = T(double(fb[p]) + src * c);
-        }
-        fo[p] = v;
-        bad |= !isfinite(double(v));
+    typedef Vec16<T> VT;
+    typedef typename VT::V V;
+    constexpr int VN = VT::n;
+    const bool vec = Np1 % VN == 0 &&
+                     ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(base) |
+                       reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+    const V* vi = reinterpret_cast<const V*>(fi);
+    const V* vb = reinterpret_cast<const V*>(fb);
+    const int nv = a.Np / VN;
+    if (tid == 0) bgk_cell_params(a, s, ii, jj, qq);
+    for (int q = tid; q < ntab; q += blockDim.x) {
+        if (q < Np1) vg[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
+        else if (q < Np1 + Np2) vg[q] = a.sg.p2_start[s] + (0.5 + (q - Np1)) * a.sg.dp2[s];
+        else vg[q] = a.sg.p3_start[s] + (0.5 + (q - Np1 - Np2)) * a.sg.dp3[s];
     }
-    if (flag && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+    __syncthreads();
+    const double m = a.sg.mass[s];
+    for (int q = tid; q < ntab; q += blockDim.x) tab[q] = bgk_table_entry(a, qq, vg, q, m);
+    __syncthreads();
+    const double inv_tau = 1.0 / a.tau;
+    const double dp1 = a.sg.dp1[s];
+    bool bad = false;
+    double acc[kNumMom] = {0, 0, 0, 0, 0};
+    // the value written at p-cell (i1, i2, i3) from its input and base values
+    auto value = [&](double f0, double vin, double vbase) -> T {
+        return mode == 1 ? T(f0) : T(vbase + (-(vin - f0) * inv_tau) * c);
+    };
+    if (vec) {
+        V* vo = reinterpret_cast<V*>(fo);
+        // two vectors of input and base per round, loaded before either is
+        // written (out may be base: every element is read, then written, by
+        // one thread)
+        for (int c0 = tid; c0 < nv; c0 += 2 * 256) {
+            V ci[2], cb[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (c0 + u * 256 < nv && mode != 1) {
+                    ci[u] = vi[c0 + u * 256];
+                    cb[u] = fb == fi ? ci[u] : vb[c0 + u * 256];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int cv = c0 + u * 256;
+                if (cv >= nv) break;
+                const int p = cv * VN;
+                const int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
+                double di[VN], db[VN], ov[VN];
+                if (mode != 1) {
+                    VT::get(ci[u], di);
+                    VT::get(cb[u], db);
+                }
+                T w[VN];
+#pragma unroll
+                for (int t = 0; t < VN; ++t) {
+                    const double f0 = (tab[ip1 + t] * tab[Np1 + ip2]) * tab[Np1 + Np2 + ip3];
+                    w[t] = value(f0, mode == 1 ? 0.0 : di[t], mode == 1 ? 0.0 : db[t]);
+                    ov[t] = double(w[t]);
+                    bad |= !isfinite(ov[t]);
+                }
+                V wv;
+                if constexpr (VN == 4) wv = make_float4(w[0], w[1], w[2], w[3]);
+                else wv = make_double2(w[0], w[1]);
+                vo[cv] = wv;
+                if (mom_out)
+                    add_moment_run<VN>(ov, vg[ip1], dp1, vg[Np1 + ip2], vg[Np1 + Np2 + ip3], acc);
+            }
+        }
+    } else {
+        for (int p = tid; p < a.Np; p += blockDim.x) {
+            const int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
+            const double f0 = (tab[ip1] * tab[Np1 + ip2]) * tab[Np1 + Np2 + ip3];
+            const T v = value(f0, mode == 1 ? 0.0 : double(fi[p]), mode == 1 ? 0.0 : double(fb[p]));
+            fo[p] = v;
+            const double ov[1] = {double(v)};
+            bad |= !isfinite(ov[0]);
+            if (mom_out)
+                add_moment_run<1>(ov, vg[ip1], dp1, vg[Np1 + ip2], vg[Np1 + Np2 + ip3], acc);
+        }
+    }
+    if (flag && __any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(flag, 1);
+    if (mom_out) {
+#pragma unroll
+        for (int q = 0; q < kNumMom; ++q) {
+            const double v = warp_sum(acc[q]);
+            if ((tid & 31) == 0) red[tid >> 5][q] = v;
+        }
+        __syncthreads();
+        if (tid < kNumMom) {
+            double v = 0.0;
+            for (int w = 0; w < 8; ++w) v += red[w][tid];
+            mom_out[((long long)tid * a.Ns + s) * a.Nq2 * a.Nq1 + (long long)jj * a.Nq1 + ii] = v;
+        }
+    }
 }
 
 }  // namespace bolt

@@ -1154,14 +1154,21 @@ int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, voi
     a.kB = ctx->p.boltzmann_constant;
     a.p_dim = ctx->p.p_dim;
     a.tau = ctx->p.tau;
-    a.mom_in = ctx->momP[0];
     a.nsplit_in = 1;
-    auto src = [&](const void* in, const void* base, void* out, double c, int mode) {
-        int r = launch_moments5(ctx, in, ctx->momP[0], st);
-        if (r) return r;
+    // one source evaluation; the moments of `in` come from a moment pass
+    // (mom_in null) or from the previous evaluation, which wrote them with
+    // its output (mom_out)
+    auto src = [&](const void* in, const void* base, void* out, double c, int mode,
+                   double* mom_in, double* mom_out) {
+        if (!mom_in) {
+            int r = launch_moments5(ctx, in, ctx->momP[0], st);
+            if (r) return r;
+            mom_in = ctx->momP[0];
+        }
+        a.mom_in = mom_in;
         cudaError_t e = ctx->elem == 8
-            ? launch_asl_src_f64(a, in, base, out, c, mode, ctx->dflag, st)
-            : launch_asl_src_f32(a, in, base, out, c, mode, ctx->dflag, st);
+            ? launch_asl_src_f64(a, in, base, out, c, mode, ctx->dflag, mom_out, st)
+            : launch_asl_src_f32(a, in, base, out, c, mode, ctx->dflag, mom_out, st);
         ctx->launches++;
         CK(e);
         return BOLT_OK;
@@ -1169,11 +1176,11 @@ int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, voi
     int rc;
     if (instantaneous) {
         // f <- f_MB (asl_operators.py:56-64, collision_operator.py:126-128)
-        rc = src(f_dev, f_dev, f_dev, 0.0, 1);
+        rc = src(f_dev, f_dev, f_dev, 0.0, 1, nullptr, nullptr);
     } else {
         // integrators.RK2: f_half = f + S(f) dt/2; f = f + S(f_half) dt
-        rc = src(f_dev, f_dev, ctx->buf[0], 0.5 * dt, 0);
-        if (!rc) rc = src(ctx->buf[0], f_dev, f_dev, dt, 0);
+        rc = src(f_dev, f_dev, ctx->buf[0], 0.5 * dt, 0, nullptr, ctx->momP[1]);
+        if (!rc) rc = src(ctx->buf[0], f_dev, f_dev, dt, 0, ctx->momP[1], nullptr);
     }
     // f's interior changed: its ghost cells and cached moments are stale
     ctx->ghost_owner = nullptr;

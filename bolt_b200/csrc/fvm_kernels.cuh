@@ -784,8 +784,44 @@ moment_kernel(const T* f, int mid, double* out, int Ns, int Np1, int Np2, int Np
     }
 }
 
+// 16-byte vectors of f: 4 FP32 or 2 FP64 values
+template <typename T> struct Vec16;
+template <> struct Vec16<float> {
+    typedef float4 V;
+    static constexpr int n = 4;
+    __device__ static void get(const V& v, double (&o)[4]) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+};
+template <> struct Vec16<double> {
+    typedef double2 V;
+    static constexpr int n = 2;
+    __device__ static void get(const V& v, double (&o)[2]) { o[0] = v.x; o[1] = v.y; }
+};
+
+// Moment sums of n consecutive p of one p1 row, values o_t at v1 = V1 + t dp1
+// (t = 0..n-1), v2, v3 fixed: from S0 = sum o_t, S1 = sum t o_t, S2 = sum t^2 o_t
+// (moments.py:6-24 with the p1 velocities of the row)
+template <int n>
+__device__ __forceinline__ void add_moment_run(const double (&o)[n], double V1, double dp1,
+                                               double v2, double v3, double (&acc)[kNumMom]) {
+    double S0 = 0.0, S1 = 0.0, S2 = 0.0;
+#pragma unroll
+    for (int t = 0; t < n; ++t) {
+        S0 += o[t];
+        S1 = fma(double(t), o[t], S1);
+        S2 = fma(double(t * t), o[t], S2);
+    }
+    acc[0] += S0;
+    acc[1] = fma(V1, S0, fma(dp1, S1, acc[1]));
+    acc[2] = fma(v2, S0, acc[2]);
+    acc[3] = fma(v3, S0, acc[3]);
+    const double e0 = fma(V1, V1, fma(v2, v2, v3 * v3));
+    acc[4] = fma(0.5, fma(e0, S0, fma(2.0 * V1 * dp1, S1, (dp1 * dp1) * S2)), acc[4]);
+}
+
 // The five BGK moments of the interior cells as one "split" of partial sums
-// ([1][5][Ns][Nq2][Nq1], sums without the measure factor).
+// ([1][5][Ns][Nq2][Nq1], sums without the measure factor).  One CTA per q-cell
+// streams its p-block in 16-byte vectors, four in flight per thread (N_p1 a
+// multiple of the vector width; otherwise one value at a time).
 template <typename T>
 __global__ void __launch_bounds__(256)
 moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int Nq1, int Nq2,
@@ -797,12 +833,38 @@ moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int
     const int Nq1g = Nq1 + 2 * Ng;
     const T* fp = f + (((long long)(jj + Ng) * Nq1g + (ii + Ng)) * Ns + s) * Np;
     double acc[kNumMom] = {0, 0, 0, 0, 0};
-    for (int c = tid; c < Np; c += 256) {
-        const int i1 = c % Np1, i2 = (c / Np1) % Np2, i3 = c / (Np1 * Np2);
-        const PVel V = lane_velocity(sg, s, i1, i2, i3);
-        const double fv = double(fp[c]);
-        acc[0] += fv; acc[1] += fv * V.v1; acc[2] += fv * V.v2; acc[3] += fv * V.v3;
-        acc[4] += (0.5 * fv) * V.vsq;
+    typedef Vec16<T> VT;
+    constexpr int VN = VT::n;
+    if (Np1 % VN == 0 && (reinterpret_cast<uintptr_t>(f) & 15) == 0) {
+        const typename VT::V* fv = reinterpret_cast<const typename VT::V*>(fp);
+        const int nv = Np / VN;
+        const double p1s = sg.p1_start[s], p2s = sg.p2_start[s], p3s = sg.p3_start[s];
+        const double dp1 = sg.dp1[s], dp2 = sg.dp2[s], dp3 = sg.dp3[s];
+        for (int c0 = tid; c0 < nv; c0 += 4 * 256) {
+            typename VT::V v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (c0 + u * 256 < nv) v[u] = __ldg(fv + c0 + u * 256);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int c = c0 + u * 256;
+                if (c >= nv) break;
+                const int p = c * VN;
+                const int i1 = p % Np1, i2 = (p / Np1) % Np2, i3 = p / (Np1 * Np2);
+                double o[VN];
+                VT::get(v[u], o);
+                add_moment_run<VN>(o, p1s + (0.5 + i1) * dp1, dp1, p2s + (0.5 + i2) * dp2,
+                                   p3s + (0.5 + i3) * dp3, acc);
+            }
+        }
+    } else {
+        for (int c = tid; c < Np; c += 256) {
+            const int i1 = c % Np1, i2 = (c / Np1) % Np2, i3 = c / (Np1 * Np2);
+            const PVel V = lane_velocity(sg, s, i1, i2, i3);
+            const double fv = double(fp[c]);
+            acc[0] += fv; acc[1] += fv * V.v1; acc[2] += fv * V.v2; acc[3] += fv * V.v3;
+            acc[4] += (0.5 * fv) * V.vsq;
+        }
     }
 #pragma unroll
     for (int m = 0; m < kNumMom; ++m) {

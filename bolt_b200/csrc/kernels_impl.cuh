@@ -112,9 +112,10 @@ cudaError_t BOLT_CAT(launch_asl_q_, BOLT_SUFFIX)(const AslArgs& a, int* flag, cu
 
 cudaError_t BOLT_CAT(launch_asl_src_, BOLT_SUFFIX)(const QStageArgs& a, const void* in,
                                                    const void* base, void* out, double c,
-                                                   int mode, int* flag, cudaStream_t st) {
+                                                   int mode, int* flag, double* mom_out,
+                                                   cudaStream_t st) {
     dim3 grid(a.Nq1 * a.Nq2, a.Ns);
-    asl_src_kernel<BOLT_T><<<grid, 256, 0, st>>>(a, in, base, out, c, mode, flag);
+    asl_src_kernel<BOLT_T><<<grid, 256, 0, st>>>(a, in, base, out, c, mode, flag, mom_out);
     return cudaGetLastError();
 }
 

@@ -116,9 +116,9 @@ BOLT_DECLARE_LAUNCHERS(f32, float)
 cudaError_t launch_asl_q_f64(const AslArgs& a, int* flag, cudaStream_t st);
 cudaError_t launch_asl_q_f32(const AslArgs& a, int* flag, cudaStream_t st);
 cudaError_t launch_asl_src_f64(const QStageArgs& a, const void* in, const void* base, void* out,
-                               double c, int mode, int* flag, cudaStream_t st);
+                               double c, int mode, int* flag, double* mom_out, cudaStream_t st);
 cudaError_t launch_asl_src_f32(const QStageArgs& a, const void* in, const void* base, void* out,
-                               double c, int mode, int* flag, cudaStream_t st);
+                               double c, int mode, int* flag, double* mom_out, cudaStream_t st);
 
 // paired q-stage (8x8 tiling, fused combine, TMA in and out): FP32, and FP64
 // with FMA contraction and Newton-refined reciprocals (BOLT_F64_FAST)
