@@ -104,6 +104,10 @@ SIGNATURES = {
     'bolt_asl_advect_q': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),
     'bolt_asl_source': (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP]),
     'bolt_fvm_p_step': (ctypes.c_int, [_VP, _VP, ctypes.c_double, _VP]),
+    'bolt_asl_advect_q_to': (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_double, _VP]),
+    'bolt_asl_source_to': (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_double, ctypes.c_int,
+                                          _VP]),
+    'bolt_work_buffer': (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     'bolt_fields_yee': (_VP, [_VP]),
     'bolt_set_peer_halos': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
     'bolt_set_peer_halos_q1': (ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),

@@ -146,6 +146,9 @@ static int dev_alloc(BoltCtx* ctx, void** p, size_t bytes) {
         *p = nullptr;
         return BOLT_ERR_NOMEM;
     }
+    // zeroed once: cells that no kernel writes (ghost cells of the work
+    // buffers, which a copy may carry into f) hold finite values
+    if (cudaMemset(*p, 0, bytes) != cudaSuccess) return BOLT_ERR_CUDA;
     ctx->scratch_bytes += bytes;
     return BOLT_OK;
 }
@@ -1090,19 +1093,18 @@ int bolt_fill_ghosts(BoltCtx* ctx, void* f_dev, void* stream) {
 }
 
 // ---- advective semi-Lagrangian step in q (asl_operators.py:20-83) ----------
-int bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
-    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+// op_advect_q from f_in into out's interior (out != f_in)
+static int asl_advect(BoltCtx* ctx, void* f_in, void* out, double dt, cudaStream_t st) {
     const BoltGrid& g = ctx->g;
     if ((ctx->p.fields_enabled && !electrostatic(ctx)) || g.N_ghost < 2)
         return BOLT_ERR_UNSUPPORTED;
-    cudaStream_t st = (cudaStream_t)stream;
     // op_advect_q: communicate_f + apply_bcs_f, then the interpolation
-    int rc = launch_ghosts(ctx, f_dev, st);
+    int rc = launch_ghosts(ctx, f_in, st);
     if (rc) return rc;
     AslArgs a;
     memset(&a, 0, sizeof(a));
-    a.f = f_dev;
-    a.out = ctx->buf[0];
+    a.f = f_in;
+    a.out = out;
     a.dt = dt;
     a.q1_start = g.q1_start;
     a.q2_start = g.q2_start;
@@ -1116,14 +1118,27 @@ int bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
                                    : launch_asl_q_f32(a, ctx->dflag, st);
     ctx->launches++;
     CK(e);
-    // the interpolated interior back into f (one row of q1 cells per q2 row);
-    // f's ghost cells are stale until the next refresh
+    ctx->ghost_owner = nullptr;
+    ctx->mom_owner = nullptr;
+    return BOLT_OK;
+}
+
+int bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
+    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+    const BoltGrid& g = ctx->g;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = asl_advect(ctx, f_dev, ctx->buf[0], dt, st);
+    if (rc) return rc;
+    // the interpolated interior back into f: the interior q2 rows as one
+    // contiguous copy (a 2-D copy of the interior cells alone ran at a third
+    // of the bandwidth); it carries the work buffer's stale q1 ghost cells
+    // into f's, which are stale until the next refresh in any case
     const size_t row = (size_t)g.N_s * ctx->Np * ctx->elem;
     const size_t pitch = row * ctx->Nq1g;
-    const size_t off = (size_t)g.N_ghost * pitch + (size_t)g.N_ghost * row;
-    CK(cudaMemcpy2DAsync(static_cast<char*>(f_dev) + off, pitch,
-                         static_cast<const char*>(ctx->buf[0]) + off, pitch, row * g.N_q1,
-                         g.N_q2, cudaMemcpyDeviceToDevice, st));
+    const size_t off = (size_t)g.N_ghost * pitch;
+    CK(cudaMemcpyAsync(static_cast<char*>(f_dev) + off,
+                       static_cast<const char*>(ctx->buf[0]) + off, pitch * g.N_q2,
+                       cudaMemcpyDeviceToDevice, st));
     ctx->ghost_owner = nullptr;
     ctx->mom_owner = nullptr;
     return BOLT_OK;
@@ -1138,13 +1153,19 @@ int bolt_fvm_p_step(BoltCtx* ctx, void* f_dev, double dt, void* stream) {
     return rc;
 }
 
-int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream) {
-    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+int bolt_asl_advect_q_to(BoltCtx* ctx, void* f_in, void* out, double dt, void* stream) {
+    if (!ctx || !f_in || !out || out == f_in) return BOLT_ERR_ARG;
+    return asl_advect(ctx, f_in, out, dt, (cudaStream_t)stream);
+}
+
+// op_solve_src from f_in into out's interior; scratch (!= f_in, may be out)
+// holds the RK2 half step
+static int asl_source(BoltCtx* ctx, const void* f_in, void* out, void* scratch, double dt,
+                      int instantaneous, cudaStream_t st) {
     const BoltGrid& g = ctx->g;
     if ((ctx->p.fields_enabled && !electrostatic(ctx)) || !ctx->bgk || ctx->tau_arr ||
         ctx->ntab > 768)
         return BOLT_ERR_UNSUPPORTED;
-    cudaStream_t st = (cudaStream_t)stream;
     QStageArgs a;
     memset(&a, 0, sizeof(a));
     a.Nq1 = g.N_q1; a.Nq2 = g.N_q2; a.Ng = g.N_ghost; a.Ns = g.N_s;
@@ -1158,7 +1179,7 @@ int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, voi
     // one source evaluation; the moments of `in` come from a moment pass
     // (mom_in null) or from the previous evaluation, which wrote them with
     // its output (mom_out)
-    auto src = [&](const void* in, const void* base, void* out, double c, int mode,
+    auto src = [&](const void* in, const void* base, void* dst, double c, int mode,
                    double* mom_in, double* mom_out) {
         if (!mom_in) {
             int r = launch_moments5(ctx, in, ctx->momP[0], st);
@@ -1167,8 +1188,8 @@ int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, voi
         }
         a.mom_in = mom_in;
         cudaError_t e = ctx->elem == 8
-            ? launch_asl_src_f64(a, in, base, out, c, mode, ctx->dflag, mom_out, st)
-            : launch_asl_src_f32(a, in, base, out, c, mode, ctx->dflag, mom_out, st);
+            ? launch_asl_src_f64(a, in, base, dst, c, mode, ctx->dflag, mom_out, st)
+            : launch_asl_src_f32(a, in, base, dst, c, mode, ctx->dflag, mom_out, st);
         ctx->launches++;
         CK(e);
         return BOLT_OK;
@@ -1176,16 +1197,36 @@ int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, voi
     int rc;
     if (instantaneous) {
         // f <- f_MB (asl_operators.py:56-64, collision_operator.py:126-128)
-        rc = src(f_dev, f_dev, f_dev, 0.0, 1, nullptr, nullptr);
+        rc = src(f_in, f_in, out, 0.0, 1, nullptr, nullptr);
     } else {
         // integrators.RK2: f_half = f + S(f) dt/2; f = f + S(f_half) dt
-        rc = src(f_dev, f_dev, ctx->buf[0], 0.5 * dt, 0, nullptr, ctx->momP[1]);
-        if (!rc) rc = src(ctx->buf[0], f_dev, f_dev, dt, 0, ctx->momP[1], nullptr);
+        // (each element of the second evaluation reads f_half and f, then
+        // writes out, in one thread: out may be either of them)
+        rc = src(f_in, f_in, scratch, 0.5 * dt, 0, nullptr, ctx->momP[1]);
+        if (!rc) rc = src(scratch, f_in, out, dt, 0, ctx->momP[1], nullptr);
     }
-    // f's interior changed: its ghost cells and cached moments are stale
+    // the written interiors changed: ghost cells and cached moments are stale
     ctx->ghost_owner = nullptr;
     ctx->mom_owner = nullptr;
     return rc;
+}
+
+int bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream) {
+    if (!ctx || !f_dev) return BOLT_ERR_ARG;
+    return asl_source(ctx, f_dev, f_dev, ctx->buf[0], dt, instantaneous, (cudaStream_t)stream);
+}
+
+int bolt_asl_source_to(BoltCtx* ctx, const void* f_in, void* out, void* scratch, double dt,
+                       int instantaneous, void* stream) {
+    if (!ctx || !f_in || !out || (!instantaneous && (!scratch || scratch == f_in)))
+        return BOLT_ERR_ARG;
+    return asl_source(ctx, f_in, out, scratch, dt, instantaneous, (cudaStream_t)stream);
+}
+
+int bolt_work_buffer(BoltCtx* ctx, int i, void** ptr) {
+    if (!ctx || !ptr || i < 0 || i >= 3 || !ctx->buf[i]) return BOLT_ERR_ARG;
+    *ptr = ctx->buf[i];
+    return BOLT_OK;
 }
 
 int bolt_set_shear(BoltCtx* ctx, double q, double omega) {

@@ -17,6 +17,7 @@ of the same name) C_q / C_p / BGK / moments.  Other plug-ins raise
 NotImplementedError.
 """
 
+import ctypes
 import math
 import os
 
@@ -637,6 +638,15 @@ class nonlinear_solver(object):
         self._asl_step(dt, 'jia') if self._asl else self._step(dt)
 
     # ---- advective semi-Lagrangian in q (asl_operators.py:20-83) ------------------
+    def _work_buffer(self):
+        # device address of the context's f-shaped work buffer 0
+        if getattr(self, '_wbuf', None) is None:
+            ptr = ctypes.c_void_p()
+            N.check(self._lib.bolt_work_buffer(self._ctx, 0, ctypes.byref(ptr)),
+                    'bolt_work_buffer')
+            self._wbuf = ptr.value
+        return self._wbuf
+
     def _op_advect_q(self, dt):
         N.check(self._lib.bolt_asl_advect_q(self._ctx, self._fstore.data_ptr(), float(dt),
                                             self._stream()), 'bolt_asl_advect_q')
@@ -687,6 +697,31 @@ class nonlinear_solver(object):
             b(dt)
             a(0.5 * dt)
 
+        src_on = self._instantaneous or self.physical_system.params.source_enabled
+        if not self.fields_enabled and src_on and scheme in ('strang', 'lie'):
+            # f handed between the operators through the context's work
+            # buffer w, no copy back: Strang f -> w -> w -> f, Lie f -> w -> f
+            w = self._work_buffer()
+            fp = f.data_ptr()
+
+            def adv_to(src, dst, d):
+                N.check(self._lib.bolt_asl_advect_q_to(self._ctx, src, dst, float(d),
+                                                       self._stream()), 'bolt_asl_advect_q_to')
+
+            def src_to(src, dst, d):
+                N.check(self._lib.bolt_asl_source_to(self._ctx, src, dst, fp, float(d),
+                                                     int(self._instantaneous), self._stream()),
+                        'bolt_asl_source_to')
+
+            if scheme == 'strang':
+                adv_to(fp, w, 0.5 * dt)
+                src_to(w, w, dt)
+                adv_to(w, fp, 0.5 * dt)
+            else:
+                adv_to(fp, w, dt)
+                src_to(w, fp, dt)
+            scheme = None
+
         def swss(a, b):
             start = f.clone()
             a(dt)
@@ -697,7 +732,9 @@ class nonlinear_solver(object):
             a(dt)
             f.add_(mid).mul_(0.5)
 
-        if scheme == 'strang':
+        if scheme is None:
+            pass
+        elif scheme == 'strang':
             strang(op1, op2)
         elif scheme == 'lie':
             op1(dt)

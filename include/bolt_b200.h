@@ -186,6 +186,20 @@ int  bolt_asl_advect_q(BoltCtx* ctx, void* f_dev, double dt, void* stream);
 int  bolt_asl_source(BoltCtx* ctx, void* f_dev, double dt, int instantaneous, void* stream);
 int  bolt_fvm_p_step(BoltCtx* ctx, void* f_dev, double dt, void* stream);
 
+/* The same two operators between separate f-shaped buffers, so that a
+ * splitting hands f from one operator to the next without copying it back
+ * (Strang: f -> w -> w -> f; Lie: f -> w -> f, w the context's work buffer
+ * 0).  bolt_asl_advect_q_to refreshes f_in's ghost cells and writes the
+ * interpolated interior into out (out != f_in).  bolt_asl_source_to reads
+ * f_in and writes out's interior (out may be f_in); scratch (!= f_in, may be
+ * out; unused when instantaneous) holds the RK2 half step.  Ghost cells of
+ * the written buffers are stale afterwards.  bolt_work_buffer gives the
+ * context's f-shaped work buffer i (0 always exists; 1 and 2 with RK4). */
+int  bolt_asl_advect_q_to(BoltCtx* ctx, void* f_in, void* out, double dt, void* stream);
+int  bolt_asl_source_to(BoltCtx* ctx, const void* f_in, void* out, void* scratch, double dt,
+                        int instantaneous, void* stream);
+int  bolt_work_buffer(BoltCtx* ctx, int i, void** ptr);
+
 /* Forget cached halo/moment state (call after f was modified outside the
  * library; bolt_step then refreshes halos and moments before stepping). */
 int  bolt_invalidate(BoltCtx* ctx);
