@@ -29,134 +29,146 @@ __device__ __forceinline__ void catmull_rom_w(double t, double (&w)[4]) {
     w[3] = 0.5 * (t3 - t2);
 }
 
-// a position in sample units on an axis of n samples: first sample, weights
-// (0 weights when the position lies off the samples)
-__device__ __forceinline__ bool catmull_rom_axis(double x, int n, int& i0, double (&w)[4]) {
-    const bool off = !(x >= 0.0 && x <= double(n - 1));
-    const double xs = fmin(fmax(x, 0.0), double(n - 1));
-    const double fl = floor(xs);
-    i0 = (int)fl;
-    catmull_rom_w(xs - fl, w);
-    return off;
-}
+// q2 rows per interpolation thread: consecutive output rows of one p-cell
+// have feet one sample apart in q2 (the displacement depends on p only), so
+// R rows share R + 3 source rows.  G cells' samples are loaded together.
+// Measured on 128^2 x 24^3 (the walk is latency-bound: more rows per thread
+// cost registers and occupancy): FP32 2 rows, 4 cells as fast as 1 row, 8
+// cells, 10 % ahead of 1 row, 4 or 6 cells and 2 rows, 2 cells; FP64 2 rows,
+// 2 cells 11 % ahead of 1 row, 4 cells.
+template <typename T> struct AslRows {
+    static constexpr int R = 2;
+    static constexpr int G = sizeof(T) == 4 ? 4 : 2;
+};
 
-// the q2 row, species and p-cell of thread e (see asl_q_kernel); true if a
-// written value is not finite
+// the q2 rows [R jb, R jb + R), species and p-cell of thread e (see
+// asl_q_kernel); true if a written value is not finite
 template <typename T>
-__device__ __forceinline__ bool asl_q_row(const AslArgs& a, long long e) {
+__device__ __forceinline__ bool asl_q_rows(const AslArgs& a, long long e) {
+    constexpr int R = AslRows<T>::R, NS = R + 3, G = AslRows<T>::G;
     bool bad = false;
     const int p = (int)(e % a.Np);
     const long long r = e / a.Np;
-    const int s = (int)(r % a.Ns), j = (int)(r / a.Ns);
+    const int s = (int)(r % a.Ns), jb = R * (int)(r / a.Ns);
     const int Ng = a.Ng, Nq1 = a.Nq1, Nq1g = a.Nq1 + 2 * Ng, Nq2g = a.Nq2 + 2 * Ng;
+    const int nr = min(R, a.Nq2 - jb);                   // rows of this thread
     const int ip1 = p % a.Np1, ip2 = (p / a.Np1) % a.Np2;
     const double v1 = a.sg.p1_start[s] + (0.5 + ip1) * a.sg.dp1[s];
     const double v2 = a.sg.p2_start[s] + (0.5 + ip2) * a.sg.dp2[s];
     // cell centres of the ghosted grid (calculate_q.py:7-41) and the foot of
     // the characteristic in sample units, as approx2's xp / yp mapping
-    // computes it: ((q - A dt) - q_0) / (q_1 - q_0)
+    // computes it: ((q - A dt) - q_0) / (q_1 - q_0); row jb + k has its foot
+    // at y + k, cell i at x0 + i
     const double q10 = a.q1_start + (0.5 - Ng) * a.dq1, q11 = a.q1_start + (1.5 - Ng) * a.dq1;
     const double q20 = a.q2_start + (0.5 - Ng) * a.dq2, q21 = a.q2_start + (1.5 - Ng) * a.dq2;
-    const double qj = a.q2_start + (0.5 + j) * a.dq2;
+    const double qj = a.q2_start + (0.5 + jb) * a.dq2;
     const double y = ((qj - v2 * a.dt) - q20) / (q21 - q20);
-    int j0;
-    double wyd[4];
-    const bool offy = catmull_rom_axis(y, Nq2g, j0, wyd);
-    // the foot of the row's first cell, its sample and weights
     const double x0 = ((a.q1_start + 0.5 * a.dq1 - v1 * a.dt) - q10) / (q11 - q10);
-    const double fl0 = floor(x0);
-    const int i00 = (int)fl0;
-    double wxd[4];
-    catmull_rom_w(x0 - fl0, wxd);
+    // first samples and weights; the positions are clamped a few samples
+    // beyond the ranges where some row or cell of the thread lies on the
+    // array (beyond them every value is 0), which keeps the sample indices
+    // exact where they matter and finite everywhere
+    const double yc = fmin(fmax(y, -double(R + 4)), double(Nq2g + 4));
+    const double xc = fmin(fmax(x0, -double(Nq1 + 4)), double(Nq1g + 4));
+    const double fy = floor(yc), fl0 = floor(xc);
+    const int j0 = (int)fy, i00 = (int)fl0;
+    double wyd[4], wxd[4];
+    catmull_rom_w(yc - fy, wyd);
+    catmull_rom_w(xc - fl0, wxd);
     T wx[4], wy[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         wx[c] = T(wxd[c]);
         wy[c] = T(wyd[c]);
     }
+    // an output row whose foot lies off the ghosted rows is 0
+    bool offy[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) offy[k] = !(y + k >= 0.0 && y + k <= double(Nq2g - 1));
     const long long rowstride = (long long)a.Ns * a.Np;
     const long long colstride = rowstride * Nq1g;
     const T* f = static_cast<const T*>(a.f) + (long long)s * a.Np + p;
-    const T* rows[4];
+    // source rows j0 - 1 .. j0 + R + 1, clamped to the ghosted array
+    const T* rows[NS];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) rows[b] = f + min(max(j0 - 1 + b, 0), Nq2g - 1) * colstride;
-    T* __restrict__ out = static_cast<T*>(a.out) + (j + Ng) * colstride +
+    for (int b = 0; b < NS; ++b) rows[b] = f + min(max(j0 - 1 + b, 0), Nq2g - 1) * colstride;
+    T* __restrict__ out = static_cast<T*>(a.out) + (jb + Ng) * colstride +
                           (long long)Ng * rowstride + (long long)s * a.Np + p;
-    // column c of the ghosted row, clamped
     auto col = [&](int b, int c) { return rows[b][min(max(c, 0), Nq1g - 1) * rowstride]; };
-    // the cell's value from the window (0 where the foot lies off the array)
-    auto cell = [&](const T (&w)[4][4], int i) {
-        const double x = x0 + i;
-        const bool off = offy || !(x >= 0.0 && x <= double(Nq1g - 1));
-        T acc = T(0);
+    // win[b][c]: source row b, column clamp(i00 + i - 1 + c) of cell i
+    T win[NS][4];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            T row = T(0);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) row = row + wx[c] * w[b][c];
-            acc = acc + wy[b] * row;
-        }
-        return off ? T(0) : acc;
-    };
-    // window[b][c]: row b, column clamp(i00 + i - 1 + c) of cell i
-    T win[4][4];
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
+    for (int b = 0; b < NS; ++b)
 #pragma unroll
         for (int c = 0; c < 3; ++c) win[b][c + 1] = col(b, i00 - 1 + c);
-    int i = 0;
-    // G cells per round (8 in FP32, 4 in FP64): their 4 G new samples are all
-    // loaded before the first of the G cells is computed and stored (the
-    // interpolation is latency-bound: many loads in flight per thread pay
-    // more than occupancy)
-    constexpr int G = sizeof(T) == 4 ? 8 : 4;
-    for (; i + G <= Nq1; i += G) {
-        T nc[G][4];
+    // cell i of every row: the window slid by one column, the q1 sums of the
+    // source rows, then per output row k the q2 sum over rows k .. k+3
+    auto cell = [&](int i, const T (&nc)[NS]) {
 #pragma unroll
-        for (int u = 0; u < G; ++u)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) nc[u][b] = col(b, i00 + i + u + 2);
-#pragma unroll
-        for (int u = 0; u < G; ++u) {
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                win[b][0] = win[b][1];
-                win[b][1] = win[b][2];
-                win[b][2] = win[b][3];
-                win[b][3] = nc[u][b];
-            }
-            const T v = cell(win, i + u);
-            out[(long long)(i + u) * rowstride] = v;
-            bad |= !isfinite(double(v));
-        }
-    }
-    for (; i < Nq1; ++i) {
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < NS; ++b) {
             win[b][0] = win[b][1];
             win[b][1] = win[b][2];
             win[b][2] = win[b][3];
-            win[b][3] = col(b, i00 + i + 2);
+            win[b][3] = nc[b];
         }
-        const T v = cell(win, i);
-        out[(long long)i * rowstride] = v;
-        bad |= !isfinite(double(v));
+        T xs[NS];
+#pragma unroll
+        for (int b = 0; b < NS; ++b) {
+            T row = T(0);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) row = row + wx[c] * win[b][c];
+            xs[b] = row;
+        }
+        const double x = x0 + i;
+        const bool offx = !(x >= 0.0 && x <= double(Nq1g - 1));
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            if (k < nr) {
+                T acc = T(0);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc = acc + wy[b] * xs[k + b];
+                const T v = (offx || offy[k]) ? T(0) : acc;
+                out[(long long)k * colstride + (long long)i * rowstride] = v;
+                bad |= !isfinite(v);
+            }
+        }
+    };
+    int i = 0;
+    // G cells per round: their new samples are loaded before any is computed
+    for (; i + G <= Nq1; i += G) {
+        T nc[G][NS];
+#pragma unroll
+        for (int u = 0; u < G; ++u)
+#pragma unroll
+            for (int b = 0; b < NS; ++b) nc[u][b] = col(b, i00 + i + u + 2);
+#pragma unroll
+        for (int u = 0; u < G; ++u) cell(i + u, nc[u]);
+    }
+    for (; i < Nq1; ++i) {
+        T nc[NS];
+#pragma unroll
+        for (int b = 0; b < NS; ++b) nc[b] = col(b, i00 + i + 2);
+        cell(i, nc);
     }
     return bad;
 }
 
-// One thread per (interior q2 row j, species s, p-cell p), p fastest across
-// lanes, walking the row's q1 cells.  The feet of a thread's cells are its
-// first foot plus 0, 1, 2, ... samples (the displacement depends on p only),
-// so the weights are computed once and the 4 x 4 source window slides along
-// q1: each cell loads one new column of 4 samples (neighbours clamped to the
-// ghosted array; a foot off the array gives 0).  Arithmetic in T.  A written
-// value that is not finite sets *flag (one atomic per warp that saw one).
+// One thread per (block of R interior q2 rows, species s, p-cell p), p
+// fastest across lanes, walking the rows' q1 cells.  The feet of a thread's
+// cells are its first foot plus whole samples in q1 and q2 (the displacement
+// depends on p only), so the weights are computed once, the R rows share
+// R + 3 source rows, and the source window slides along q1: each cell loads
+// one new column of R + 3 samples (neighbours clamped to the ghosted array;
+// a foot off the array gives 0).  Arithmetic in T: per source row the q1
+// cubic, then per output row the q2 cubic, the order of a tensor-product
+// evaluation row by row.  A written value that is not finite sets *flag (one
+// atomic per warp that saw one).
 template <typename T>
 __global__ void __launch_bounds__(256) asl_q_kernel(const AslArgs a, int* flag) {
-    const long long nthr = (long long)a.Nq2 * a.Ns * a.Np;
+    constexpr int R = AslRows<T>::R;
+    const long long nthr = (long long)((a.Nq2 + R - 1) / R) * a.Ns * a.Np;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool bad = e < nthr && asl_q_row<T>(a, e);
+    const bool bad = e < nthr && asl_q_rows<T>(a, e);
     if (flag && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 

@@ -104,7 +104,8 @@ cudaError_t BOLT_CAT(launch_ghost_, BOLT_SUFFIX)(void* f, const void* dl, const 
 }
 
 cudaError_t BOLT_CAT(launch_asl_q_, BOLT_SUFFIX)(const AslArgs& a, int* flag, cudaStream_t st) {
-    const long long total = (long long)a.Nq2 * a.Ns * a.Np;          // threads
+    constexpr int R = AslRows<BOLT_T>::R;
+    const long long total = (long long)((a.Nq2 + R - 1) / R) * a.Ns * a.Np;   // threads
     if (total == 0) return cudaSuccess;
     asl_q_kernel<BOLT_T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a, flag);
     return cudaGetLastError();
