@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 import torch
 
+import bolt_b200._native as N
 import cases as C
 from _modules import make_solver, to_layout, moments_layout
 from _util import load_golden, rel, interior, moment_errors
@@ -81,6 +82,11 @@ def test_asl_buffer_passing_step_equals_in_place_operators(scheme, precision):
     g = spec['N_ghost']
     fa, fb = interior(to_layout(a.f, spec), g), interior(to_layout(b.f, spec), g)
     assert np.array_equal(fa, fb)
+    # the buffer forms refuse aliasing they cannot honour
+    fp, w = a._fstore.data_ptr(), a._work_buffer()
+    assert a._lib.bolt_asl_advect_q_to(a._ctx, fp, fp, float(dt), a._stream()) == N.BOLT_ERR_ARG
+    assert a._lib.bolt_asl_source_to(a._ctx, w, fp, w, float(dt), 0,
+                                     a._stream()) == N.BOLT_ERR_ARG
     a.synchronize()
     b.synchronize()
 

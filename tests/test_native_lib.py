@@ -39,6 +39,13 @@ def test_strerror_and_null_args():
     assert lib.bolt_ctx_create(None, None, None) == N.BOLT_ERR_ARG
     assert lib.bolt_step(None, None, 0.0, None) == N.BOLT_ERR_ARG
     assert lib.bolt_launch_count(None) == 0
+    # the semi-Lagrangian operators, in place and between buffers
+    assert lib.bolt_asl_advect_q(None, None, 0.0, None) == N.BOLT_ERR_ARG
+    assert lib.bolt_asl_source(None, None, 0.0, 0, None) == N.BOLT_ERR_ARG
+    assert lib.bolt_asl_advect_q_to(None, None, None, 0.0, None) == N.BOLT_ERR_ARG
+    assert lib.bolt_asl_source_to(None, None, None, None, 0.0, 0, None) == N.BOLT_ERR_ARG
+    ptr = ctypes.c_void_p()
+    assert lib.bolt_work_buffer(None, 0, ctypes.byref(ptr)) == N.BOLT_ERR_ARG
 
 
 def test_ctx_create_rejects_bad_grids_without_gpu():
