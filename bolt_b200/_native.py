@@ -28,6 +28,7 @@ FLUX = {'upwind-flux': 0, 'upwind': 0, 'lax-friedrichs': 1, 'llf': 1,
 BC = {'periodic': 0, 'dirichlet': 1, 'external': 2, 'mirror': 3, 'mirror+dirichlet': 4,
       'shearing-box': 5}
 RK = {'RK2': 2, 'RK4': 4}
+PGRID = {'cartesian': 0, 'polar2D': 1}
 FIELDS = {'electrodynamic': 0, 'electrostatic': 1}
 MOMENT_IDS = {'density': 0, 'mom_v1_bulk': 1, 'mom_v2_bulk': 2, 'mom_v3_bulk': 3,
               'energy': 4, 'energy_q1': 5, 'energy_q2': 6, 'energy_q3': 7,
@@ -87,6 +88,7 @@ SIGNATURES = {
     'bolt_set_dirichlet': (ctypes.c_int, [_VP, ctypes.c_int, _VP]),
     'bolt_fill_ghosts': (ctypes.c_int, [_VP, _VP, _VP]),
     'bolt_set_shear': (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double]),
+    'bolt_set_p_space_grid': (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_double]),
     'bolt_set_time': (ctypes.c_int, [_VP, ctypes.c_double]),
     'bolt_invalidate': (ctypes.c_int, [_VP]),
     'bolt_dfdt': (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_double, _VP]),

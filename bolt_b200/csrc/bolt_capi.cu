@@ -1237,6 +1237,23 @@ int bolt_set_shear(BoltCtx* ctx, double q, double omega) {
     return BOLT_OK;
 }
 
+int bolt_set_p_space_grid(BoltCtx* ctx, int grid, double initial_mu) {
+    if (!ctx || (grid != BOLT_PGRID_CARTESIAN && grid != BOLT_PGRID_POLAR2D)) return BOLT_ERR_ARG;
+    if (grid == BOLT_PGRID_POLAR2D) {
+        if (!(initial_mu == initial_mu)) return BOLT_ERR_ARG;
+        // the moments of the field sources would carry the factor too; the
+        // polar2D grid is served with fields off only
+        if (ctx->p.fields_enabled) return BOLT_ERR_UNSUPPORTED;
+        // a q1 mirror edge splits the angle axis into two halves
+        if ((ctx->p.bc_q1 == BOLT_BC_MIRROR || ctx->p.bc_q1 == BOLT_BC_MIRROR_DIRICHLET) &&
+            ctx->g.N_p2 % 2)
+            return BOLT_ERR_UNSUPPORTED;
+    }
+    ctx->sg.polar2d = grid == BOLT_PGRID_POLAR2D ? 1 : 0;
+    ctx->sg.mom_scale = grid == BOLT_PGRID_POLAR2D ? initial_mu : 0.0;
+    return BOLT_OK;
+}
+
 int bolt_set_time(BoltCtx* ctx, double t) {
     if (!ctx) return BOLT_ERR_ARG;
     const bool shearing = ctx->p.bc_q1 == BOLT_BC_SHEARING_BOX ||

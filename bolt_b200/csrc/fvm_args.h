@@ -106,6 +106,12 @@ struct SpeciesGrid {
     double p1_start[kMaxSpecies], p2_start[kMaxSpecies], p3_start[kMaxSpecies];
     double dp1[kMaxSpecies], dp2[kMaxSpecies], dp3[kMaxSpecies];
     double mass[kMaxSpecies], charge[kMaxSpecies];
+    // p-space grid (params.p_space_grid): 0 cartesian; 1 polar2D, whose
+    // moments carry the factor mom_scale = params.initial_mu
+    // (compute_moments.py:48-53) and whose mirror edges map the angle p2
+    // (boundaries.py:313-413)
+    int polar2d;
+    double mom_scale;
 };
 
 struct QStageArgs {

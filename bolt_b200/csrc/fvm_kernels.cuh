@@ -83,11 +83,18 @@ __device__ __forceinline__ void bgk_params_from_sums(const QStageArgs& a, int s,
     const double kB = a.kB;
     const double measure = (a.sg.dp3[s] * a.sg.dp2[s]) * a.sg.dp1[s];
     const double eps = 1e-30;
-    double n = mm[0] * measure;
-    double u1 = (mm[1] * measure) / (n + eps);
-    double u2 = (mm[2] * measure) / (n + eps);
-    double u3 = (mm[3] * measure) / (n + eps);
-    double E = mm[4] * measure;
+    // moments as compute_moments returns them: sum * measure, times initial_mu
+    // on the polar2D grid
+    const bool polar = a.sg.polar2d != 0;
+    const double sc = a.sg.mom_scale;
+    double mv[kNumMom];
+#pragma unroll
+    for (int q = 0; q < kNumMom; ++q) mv[q] = polar ? sc * (mm[q] * measure) : mm[q] * measure;
+    double n = mv[0];
+    double u1 = mv[1] / (n + eps);
+    double u2 = mv[2] / (n + eps);
+    double u3 = mv[3] / (n + eps);
+    double E = mv[4];
     double nm = n * m;
     double Tt = (1.0 / a.p_dim) * ((((2.0 * (E * m) - nm * (u1 * u1)) - nm * (u2 * u2))
                                     - nm * (u3 * u3))) / (n + eps) + eps;
@@ -780,7 +787,7 @@ moment_kernel(const T* f, int mid, double* out, int Ns, int Np1, int Np2, int Np
         double v = 0.0;
         for (int w = 0; w < 8; ++w) v += red[w];
         const double measure = (sg.dp3[s] * sg.dp2[s]) * sg.dp1[s];
-        out[(long long)q * Ns + s] = v * measure;
+        out[(long long)q * Ns + s] = sg.polar2d ? sg.mom_scale * (v * measure) : v * measure;
     }
 }
 
@@ -882,7 +889,7 @@ moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int
 // ---------------------------------------------------------------------------
 // halo refresh: communicate_f (periodic wrap; ghosted halos are zero), then
 // apply_bcs_f per axis (boundaries.py:415-577): the mirror image
-// (boundaries.py:226-301, cartesian p-grid) and/or the Dirichlet inflow
+// (boundaries.py:226-413, cartesian or polar2D p-grid) and/or the Dirichlet inflow
 // select (:147-225).  One thread per (ghost cell, s, p); every value is read
 // from an interior cell, so one pass gives the reference's sequential
 // left, right, bottom, top result everywhere except in the corner cells
@@ -956,29 +963,42 @@ __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const 
         const int i1 = p % Np1, i2 = (p / Np1) % Np2;
         // source cell and p index: periodic wrap, or the mirror image across
         // the edge (ghost i < 0 <- interior -1-i, i >= N <- 2N-1-i) with the
-        // normal velocity index reversed (boundaries.py:226-301)
+        // velocity reflected.  Cartesian grid (boundaries.py:226-301): the
+        // normal velocity index reversed, p1 at q1 edges, p2 at q2 edges.
+        // Polar2D grid (boundaries.py:313-413, p2 the angle theta): at q2
+        // edges theta -> -theta, the p2 index reversed; at q1 edges
+        // theta -> pi - theta, each half of the p2 index range reversed on its
+        // own.  The reference applies the q1 edges before the q2 edges, so a
+        // corner ghost takes the q1 map of the q2 map of its own p2 index.
         int si = i, sj = j, ps = p;
+        int k2 = i2;                                   // source p2 index
         bool have = true;
-        if (!in1) {
-            if (per1) {
-                si = ((i % Nq1) + Nq1) % Nq1;
-            } else if (mir1) {
-                si = i < 0 ? -1 - i : 2 * Nq1 - 1 - i;
-                ps += Np1 - 1 - 2 * i1;
-            } else {
-                have = false;
-            }
-        }
         if (!in2) {
             if (per2) {
                 sj = ((j % Nq2) + Nq2) % Nq2;
             } else if (mir2) {
                 sj = j < 0 ? -1 - j : 2 * Nq2 - 1 - j;
-                ps += Np1 * (Np2 - 1 - 2 * i2);
+                k2 = Np2 - 1 - k2;
             } else {
                 have = false;
             }
         }
+        if (!in1) {
+            if (per1) {
+                si = ((i % Nq1) + Nq1) % Nq1;
+            } else if (mir1) {
+                si = i < 0 ? -1 - i : 2 * Nq1 - 1 - i;
+                if (sg.polar2d) {
+                    const int H = Np2 / 2;
+                    k2 = k2 < H ? H - 1 - k2 : Np2 - 1 + H - k2;
+                } else {
+                    ps += Np1 - 1 - 2 * i1;
+                }
+            } else {
+                have = false;
+            }
+        }
+        ps += Np1 * (k2 - i2);
         T v = T(0);
         if (have)
             v = f[(long long)(sj + Ng) * colstride + (long long)(si + Ng) * rowstride +

@@ -184,8 +184,13 @@ class nonlinear_solver(object):
             raise NotImplementedError('source must be nonrelativistic_boltzmann BGK')
         if getattr(params, 'hybrid_model_enabled', False):
             raise NotImplementedError('hybrid model')
-        if getattr(params, 'p_space_grid', 'cartesian') != 'cartesian':
-            raise NotImplementedError('only the cartesian p-space grid is implemented')
+        # p-space grid (compute_moments.py:42-56, boundaries.py:432-553): cartesian,
+        # or polar2D (p1 the radius, p2 the angle) with fields off
+        self._p_space_grid = getattr(params, 'p_space_grid', 'cartesian')
+        if self._p_space_grid not in ('cartesian', 'polar2D'):
+            raise NotImplementedError('Unsupported coordinate system in p_space')
+        if self._p_space_grid == 'polar2D' and getattr(params, 'fields_enabled', False):
+            raise NotImplementedError('the polar2D p-space grid is served with fields off')
         self.fields_enabled = bool(getattr(params, 'fields_enabled', False))
         self.fields_type = getattr(params, 'fields_type', 'electrodynamic')
         if self.fields_enabled:
@@ -359,6 +364,10 @@ class nonlinear_solver(object):
         self._ctx = ctx
         if self._tau_arr is not None:
             N.check(self._lib.bolt_set_tau_array(ctx, self._tau_arr.data_ptr()), 'bolt_set_tau_array')
+        if self._p_space_grid == 'polar2D':
+            N.check(self._lib.bolt_set_p_space_grid(ctx, N.PGRID['polar2D'],
+                                                    float(params.initial_mu)),
+                    'bolt_set_p_space_grid')
         self._shearing = 'shearing-box' in (self._bc_q1, self._bc_q2)
         if self._asl and (self._has_dirichlet() or self._shearing or
                           self._tau_arr is not None):
@@ -867,8 +876,6 @@ class nonlinear_solver(object):
         if moment_name not in N.MOMENT_IDS:
             raise NotImplementedError('moment %r is not one of the nonrelativistic moments'
                                       % moment_name)
-        if getattr(self.physical_system.params, 'p_space_grid', 'cartesian') != 'cartesian':
-            raise NotImplementedError('Unsupported coordinate system in p_space')
         src = self._fstore if store is None else store
         out = torch.empty((self.N_q2_local_with_Ng, self.N_q1_local_with_Ng, self.N_species),
                           dtype=torch.float64, device=self.device)

@@ -25,6 +25,8 @@
  *   bolt_divergence_flag check_divergence            bolt/lib/nonlinear/timestep.py:28-38
  *   bolt_dfdt_term       df_dt_fvm(term_to_return)   bolt/lib/nonlinear/finite_volume/df_dt_fvm.py:325-339
  *   bolt_set_shear/time  apply_shearing_box_bcs_f    bolt/lib/nonlinear/boundaries.py:6-145
+ *   bolt_set_p_space_grid params.p_space_grid        bolt/lib/nonlinear/boundaries.py:313-413,
+ *                                                    bolt/lib/nonlinear/compute_moments.py:42-56
  *   bolt_timings         print_table                 bolt/lib/utils/performance_timings.py:9-165
  */
 #ifndef BOLT_B200_H
@@ -88,6 +90,16 @@ extern "C" {
  * one-dimensional Catmull-Rom cubic.  One axis at most, the other periodic;
  * needs N_ghost >= 2. */
 #define BOLT_BC_SHEARING_BOX 5
+
+/* p-space grids (params.p_space_grid).  On BOLT_PGRID_POLAR2D, p1 is the
+ * radius and p2 the angle theta over a full turn: every moment -- the BGK
+ * Maxwellian's and bolt_moments' -- carries the factor initial_mu
+ * (compute_moments.py:48-53), and a mirror edge reflects theta
+ * (boundaries.py:313-413): theta -> -theta at q2 edges (the p2 index
+ * reversed), theta -> pi - theta at q1 edges (each half of the p2 index range
+ * reversed on its own; needs an even N_p2). */
+#define BOLT_PGRID_CARTESIAN 0
+#define BOLT_PGRID_POLAR2D   1
 
 /* field models (fields.py:559-690): electrodynamic fields advanced by FDTD
  * once per step, or electrostatic fields re-solved from the charge density of
@@ -157,6 +169,12 @@ int  bolt_set_dirichlet(BoltCtx* ctx, int side, const void* values_dev);
  * the time the ghost strips are sheared to (the reference's time_elapsed,
  * constant over the stages of a step). */
 int  bolt_set_shear(BoltCtx* ctx, double q, double omega);
+
+/* The context's p-space grid (BOLT_PGRID_*; cartesian after create) and, for
+ * polar2D, params.initial_mu.  Set it before the first step.  Polar2D with
+ * fields enabled, or with a q1 mirror edge and an odd N_p2, is
+ * BOLT_ERR_UNSUPPORTED. */
+int  bolt_set_p_space_grid(BoltCtx* ctx, int grid, double initial_mu);
 int  bolt_set_time(BoltCtx* ctx, double t);
 
 /* Halo refresh of f in place (periodic wrap + Dirichlet inflow). */

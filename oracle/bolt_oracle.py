@@ -201,6 +201,10 @@ class Grid(object):
         self.q1c6 = self.q1_center[:, :, None, None, None, None]
         self.q2c6 = self.q2_center[:, :, None, None, None, None]
         self.measure = (self.dp3 * self.dp2 * self.dp1)[None, None, :]  # (1,1,Ns)
+        # p-space grid (compute_moments.py:42-56): on 'polar2D' every moment is
+        # scaled by params.initial_mu
+        self.polar2d = s.get('p_space_grid', 'cartesian') == 'polar2D'
+        self.initial_mu = float(s.get('initial_mu', 1.0))
 
     @property
     def fshape(self):
@@ -239,6 +243,8 @@ def moment(grid, f, name):
     else:
         raise KeyError(name)
     s = integrand.reshape(integrand.shape[:3] + (-1,)).sum(axis=3)
+    if g.polar2d:
+        return g.initial_mu * (s * g.measure)
     return s * g.measure
 
 
@@ -570,8 +576,20 @@ class Oracle(object):
             if axis_bc in ('mirror', 'mirror+dirichlet'):
                 # ghost cells take the interior cells mirrored across the edge,
                 # with the p-index normal to the edge reversed (p1 for q1 edges,
-                # p2 for q2 edges; axes -1 / -2 of (q2, q1, s, p3, p2, p1))
-                if side == 'left':
+                # p2 for q2 edges; axes -1 / -2 of (q2, q1, s, p3, p2, p1));
+                # on the polar2D grid the q2 edges are the same (theta -> -theta)
+                if side in ('left', 'right') and g.polar2d:
+                    # polar2D (boundaries.py:313-413), p2 the angle: a q1 edge
+                    # maps theta -> pi - theta, each half of the p2 range
+                    # reversed on its own (N_p2 // 2 cells in the first half)
+                    H = g.Np2 // 2
+                    k = np.arange(g.Np2)
+                    perm = np.where(k < H, H - 1 - k, g.Np2 - 1 + H - k)
+                    if side == 'left':
+                        out[:, :Ng] = out[:, Ng:2 * Ng][:, ::-1][..., perm, :]
+                    else:
+                        out[:, -Ng:] = out[:, -2 * Ng:-Ng][:, ::-1][..., perm, :]
+                elif side == 'left':
                     out[:, :Ng] = out[:, Ng:2 * Ng][:, ::-1][..., ::-1]
                 elif side == 'right':
                     out[:, -Ng:] = out[:, -2 * Ng:-Ng][:, ::-1][..., ::-1]

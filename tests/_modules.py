@@ -83,7 +83,8 @@ def build_modules(spec, precision='fp64', integrator=None):
     params.hybrid_model_enabled = False
     params.eps = spec['eps']
     params.mu = spec['mu']
-    params.p_space_grid = 'cartesian'
+    params.p_space_grid = spec.get('p_space_grid', 'cartesian')
+    params.initial_mu = spec.get('initial_mu', 1.0)
     params.time_integrator = integrator or spec['integrator']
     params.precision = precision
     # shearing-box rate q omega (boundaries.py:17-18)

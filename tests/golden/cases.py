@@ -311,6 +311,30 @@ CASES['asl_es_2d2v_lie_rk4'] = make(
     integrator='RK4', riemann_p='lax-friedrichs',
     init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=11, u=[0.2, -0.1, 0.0]))
 
+# polar2D p-grid (p1 the radius, p2 the angle over a full turn): every moment
+# scaled by initial_mu (compute_moments.py:48-53), mirror edges reflecting the
+# angle (boundaries.py:313-413): both q axes mirrored, RK4, WENO5; a q1
+# Dirichlet-inflow left edge (every radius moves inwards there) with the mirror
+# on the right, minmod, RK2; and the semi-Lagrangian q-step between mirrors
+_POLAR = dict(N_q1=8, N_q2=8, N_p1=8, N_p2=8, N_p3=1,
+              p1_start=[0.0], p1_end=[4.0], p2_start=[-np.pi], p2_end=[np.pi],
+              p3_start=[-0.5], p3_end=[0.5], mass=[1.0], charge=[0.0], p_dim=2,
+              p_space_grid='polar2D', initial_mu=0.7)
+CASES['polar2d_mirror_2d2v_rk4'] = make(
+    bc_q1='mirror', bc_q2='mirror', tau=0.05, dt=2e-3, steps=3, integrator='RK4',
+    init=dict(amp=0.1, k1=1, k2=1, u=[1.5, 0.3, 0.0], T=[1.0, 0.8, 1.0]),
+    **copy.deepcopy(_POLAR))
+CASES['polar2d_mirror_dirichlet_minmod_rk2'] = make(
+    bc_q1='mirror+dirichlet', recon_q='minmod', recon_p='minmod', tau=0.05, dt=2e-3,
+    steps=3, dirichlet=dict(left=dict(base=1.2, T=[1.0, 1.0, 1.0], u=[1.0, 0.2, 0]),
+                            right=dict(base=0.8, T=[1.2, 1.0, 1.0], u=[2.0, -0.1, 0])),
+    init=dict(amp=0.1, k1=1, k2=2, u=[1.2, -0.2, 0.0], T=[1.0, 1.2, 1.0]),
+    **copy.deepcopy(_POLAR))
+CASES['asl_polar2d_mirror_strang'] = make(
+    solver_q='ASL', splitting='strang', bc_q1='mirror', bc_q2='mirror', tau=0.1, dt=5e-3,
+    steps=3, init=dict(amp=0.1, k1=1, k2=1, u=[1.5, 0.3, 0.0], T=[1.0, 0.8, 1.0]),
+    **copy.deepcopy(_POLAR))
+
 # the finite-volume cases and the semi-Lagrangian ones
 FVM_NAMES = sorted(n for n, s in CASES.items() if s.get('solver_q', 'FVM') == 'FVM')
 ASL_NAMES = sorted(n for n, s in CASES.items() if s.get('solver_q', 'FVM') == 'ASL')

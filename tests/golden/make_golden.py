@@ -132,7 +132,8 @@ def build_modules(spec, af, record=None):
     params.hybrid_model_enabled = False
     params.eps = spec['eps']
     params.mu = spec['mu']
-    params.p_space_grid = 'cartesian'
+    params.p_space_grid = spec.get('p_space_grid', 'cartesian')
+    params.initial_mu = spec.get('initial_mu', 1.0)
     params.time_integrator = spec['integrator']
     tau = spec['tau']
 

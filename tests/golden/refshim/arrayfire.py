@@ -60,6 +60,16 @@ def _numdims(shape4):
     return nd
 
 
+def _seq_bound(b):
+    """A slice bound as ArrayFire's af_seq takes it: integral floats index
+    like ints; fractional bounds are refused."""
+    if b is None or isinstance(b, (int, np.integer)):
+        return b
+    if float(b) != int(b):
+        raise NotImplementedError('fractional slice bound %r' % (b,))
+    return int(b)
+
+
 class Array(object):
     __array_priority__ = 1000
 
@@ -127,6 +137,10 @@ class Array(object):
         return 'af.Array(shape=%s)' % (self.shape,)
 
     # -- indexing (ArrayFire keeps indexed dims) --------------------------
+    # ArrayFire's Python indexing turns a slice into an af_seq, whose bounds
+    # are doubles, so a float bound such as N_theta/2 (boundaries.py:345)
+    # indexes like the integer of the same value; _seq_bound accepts those
+    # and refuses fractional ones, whose af_seq meaning is not restated here
     def _key(self, key):
         if not isinstance(key, tuple):
             key = (key,)
@@ -136,6 +150,8 @@ class Array(object):
                 out.append(slice(int(k), int(k) + 1 if int(k) != -1 else None))
             elif isinstance(k, Array):
                 out.append(np.asarray(k._a).reshape(-1))
+            elif isinstance(k, slice):
+                out.append(slice(_seq_bound(k.start), _seq_bound(k.stop), _seq_bound(k.step)))
             else:
                 out.append(k)
         while len(out) < 4:
