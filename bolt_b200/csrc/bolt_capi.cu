@@ -841,6 +841,7 @@ static int launch_fields(BoltCtx* ctx, double dt, int nsplit_j, cudaStream_t st,
         a.charge[s] = ctx->p.charge[s];
         a.measure[s] = (g.dp3[s] * g.dp2[s]) * g.dp1[s];
     }
+    a.mom_scale = ctx->sg.polar2d ? ctx->sg.mom_scale : 1.0;
     if (part < 0) CK(launch_fdtd(a, st, &ctx->launches));
     else CK(launch_fdtd_part(a, part, st, &ctx->launches));
     return BOLT_OK;
@@ -869,6 +870,7 @@ static int launch_electrostatic(BoltCtx* ctx, const void* f, cudaStream_t st) {
         a.charge[s] = ctx->p.charge[s];
         a.measure[s] = (g.dp3[s] * g.dp2[s]) * g.dp1[s];
     }
+    a.mom_scale = ctx->sg.polar2d ? ctx->sg.mom_scale : 1.0;
     CK(launch_poisson(a, ctx->es_fwd, ctx->es_inv, st, &ctx->launches));
     return BOLT_OK;
 }
@@ -1241,9 +1243,6 @@ int bolt_set_p_space_grid(BoltCtx* ctx, int grid, double initial_mu) {
     if (!ctx || (grid != BOLT_PGRID_CARTESIAN && grid != BOLT_PGRID_POLAR2D)) return BOLT_ERR_ARG;
     if (grid == BOLT_PGRID_POLAR2D) {
         if (!(initial_mu == initial_mu)) return BOLT_ERR_ARG;
-        // the moments of the field sources would carry the factor too; the
-        // polar2D grid is served with fields off only
-        if (ctx->p.fields_enabled) return BOLT_ERR_UNSUPPORTED;
         // a q1 mirror edge splits the angle axis into two halves
         if ((ctx->p.bc_q1 == BOLT_BC_MIRROR || ctx->p.bc_q1 == BOLT_BC_MIRROR_DIRICHLET) &&
             ctx->g.N_p2 % 2)

@@ -24,13 +24,15 @@ __global__ void fdtd_prepare_kernel(FieldArgs a) {
             if (a.j_given) {
                 v = a.j_given[c * n + t];
             } else if (i >= 0 && i < a.Nq1 && j >= 0 && j < a.Nq2) {
-                // per species: charge * (sum * measure); then the species sum
+                // per species: charge * moment, the moment sum * measure
+                // (times initial_mu on the polar2D grid); then the species sum
                 for (int s = 0; s < a.Ns; ++s) {
                     double sum = 0.0;
                     for (int sp = 0; sp < a.nsplit; ++sp)
                         sum += a.jpart[(((long long)sp * 3 + c) * a.Ns + s) * a.Nq2 * a.Nq1
                                        + (long long)j * a.Nq1 + i];
-                    v += a.charge[s] * (sum * a.measure[s]);
+                    const double mom = sum * a.measure[s];
+                    v += a.charge[s] * (a.mom_scale * mom);
                 }
             }
             a.J[c * n + t] = v;

@@ -199,6 +199,7 @@ struct FieldArgs {
     int ext1, ext2;         // external axes: their ghosts come from the neighbouring blocks
     double dq1, dq2, dt, eps, mu;
     double charge[kMaxSpecies], measure[kMaxSpecies];
+    double mom_scale;           // the moments' factor: initial_mu on polar2D, else 1
 };
 
 }  // namespace bolt

@@ -102,6 +102,7 @@ struct PoissonArgs {
     int Nq1, Nq2, Ng, Ns;
     double dq1, dq2, eps;
     double charge[kMaxSpecies], measure[kMaxSpecies];
+    double mom_scale;         // the moments' factor: initial_mu on polar2D, else 1
 };
 int poisson_plans_create(int Nq1, int Nq2, int* fwd, int* inv);
 void poisson_plans_destroy(int fwd, int inv);

@@ -34,8 +34,12 @@ poisson_rho_kernel(PoissonArgs a) {
     double local = 0.0;
     for (int q = threadIdx.x; q < n; q += kRhoThreads) {
         double r = 0.0;
-        for (int s = 0; s < a.Ns; ++s)
-            r += a.charge[s] * (a.measure[s] * a.part[(long long)s * n + q]);
+        for (int s = 0; s < a.Ns; ++s) {
+            // charge * density; the density times initial_mu on the polar2D
+            // grid (mom_scale; 1 on the cartesian grid, an exact product)
+            const double dens = a.measure[s] * a.part[(long long)s * n + q];
+            r += a.charge[s] * (a.mom_scale * dens);
+        }
         a.rho_hat[q] = make_double2(r, 0.0);
         local += r;
     }

@@ -185,12 +185,10 @@ class nonlinear_solver(object):
         if getattr(params, 'hybrid_model_enabled', False):
             raise NotImplementedError('hybrid model')
         # p-space grid (compute_moments.py:42-56, boundaries.py:432-553): cartesian,
-        # or polar2D (p1 the radius, p2 the angle) with fields off
+        # or polar2D (p1 the radius, p2 the angle)
         self._p_space_grid = getattr(params, 'p_space_grid', 'cartesian')
         if self._p_space_grid not in ('cartesian', 'polar2D'):
             raise NotImplementedError('Unsupported coordinate system in p_space')
-        if self._p_space_grid == 'polar2D' and getattr(params, 'fields_enabled', False):
-            raise NotImplementedError('the polar2D p-space grid is served with fields off')
         self.fields_enabled = bool(getattr(params, 'fields_enabled', False))
         self.fields_type = getattr(params, 'fields_type', 'electrodynamic')
         if self.fields_enabled:

@@ -93,8 +93,8 @@ extern "C" {
 
 /* p-space grids (params.p_space_grid).  On BOLT_PGRID_POLAR2D, p1 is the
  * radius and p2 the angle theta over a full turn: every moment -- the BGK
- * Maxwellian's and bolt_moments' -- carries the factor initial_mu
- * (compute_moments.py:48-53), and a mirror edge reflects theta
+ * Maxwellian's, bolt_moments', the field sources' -- carries the factor
+ * initial_mu (compute_moments.py:48-53), and a mirror edge reflects theta
  * (boundaries.py:313-413): theta -> -theta at q2 edges (the p2 index
  * reversed), theta -> pi - theta at q1 edges (each half of the p2 index range
  * reversed on its own; needs an even N_p2). */
@@ -171,9 +171,8 @@ int  bolt_set_dirichlet(BoltCtx* ctx, int side, const void* values_dev);
 int  bolt_set_shear(BoltCtx* ctx, double q, double omega);
 
 /* The context's p-space grid (BOLT_PGRID_*; cartesian after create) and, for
- * polar2D, params.initial_mu.  Set it before the first step.  Polar2D with
- * fields enabled, or with a q1 mirror edge and an odd N_p2, is
- * BOLT_ERR_UNSUPPORTED. */
+ * polar2D, params.initial_mu.  Set it before the first step.  Polar2D with a
+ * q1 mirror edge and an odd N_p2 is BOLT_ERR_UNSUPPORTED. */
 int  bolt_set_p_space_grid(BoltCtx* ctx, int grid, double initial_mu);
 int  bolt_set_time(BoltCtx* ctx, double t);
 

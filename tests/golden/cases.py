@@ -330,6 +330,18 @@ CASES['polar2d_mirror_dirichlet_minmod_rk2'] = make(
                             right=dict(base=0.8, T=[1.2, 1.0, 1.0], u=[2.0, -0.1, 0])),
     init=dict(amp=0.1, k1=1, k2=2, u=[1.2, -0.2, 0.0], T=[1.0, 1.2, 1.0]),
     **copy.deepcopy(_POLAR))
+# with fields: the charge density and the currents carry the factor too
+# (df_dt_fvm.py:213-242), FDTD from the FFT initial solve, and the
+# electrostatic FFT solve at every df/dt
+CASES['polar2d_fdtd_2d2v_rk4'] = make(
+    fields_enabled=True, tau=0.05, dt=1e-3, steps=3, integrator='RK4',
+    init=dict(amp=0.1, k1=1, k2=1, noise=1e-2, seed=5, u=[1.5, 0.3, 0.0], T=[1.0, 0.8, 1.0]),
+    **dict(copy.deepcopy(_POLAR), initial_mu=1.3, charge=[-1.0]))
+CASES['polar2d_es_2d2v_rk2'] = make(
+    fields_enabled=True, fields_type='electrostatic', fields_solver='fft',
+    source_enabled=False, dt=1e-3, steps=3,
+    init=dict(amp=0.1, k1=1, k2=0, u=[1.5, 0.3, 0.0], T=[1.0, 0.8, 1.0]),
+    **dict(copy.deepcopy(_POLAR), initial_mu=1.3, charge=[-1.0]))
 CASES['asl_polar2d_mirror_strang'] = make(
     solver_q='ASL', splitting='strang', bc_q1='mirror', bc_q2='mirror', tau=0.1, dt=5e-3,
     steps=3, init=dict(amp=0.1, k1=1, k2=1, u=[1.5, 0.3, 0.0], T=[1.0, 0.8, 1.0]),

@@ -10,8 +10,8 @@ the grid changes one at a time:
   * a mirror edge reflects the angle (boundaries.py:313-413): theta -> -theta
     at q2 edges, theta -> pi - theta at q1 edges, checked cell by cell
     against the oracle's halo refresh;
-and the configurations the path refuses: fields with polar2D, and a q1 mirror
-edge with an odd N_p2 (the reference splits the angle range in two halves)."""
+and the configuration the path refuses: a q1 mirror edge with an odd N_p2
+(the reference splits the angle range in two halves)."""
 
 import copy
 
@@ -66,11 +66,7 @@ def test_polar_mirror_halo_matches_oracle(name):
 
 
 @pytest.mark.gpu
-def test_polar_refuses_fields_and_odd_angle_count_at_q1_mirror():
-    spec = copy.deepcopy(C.CASES[NAME])
-    spec.update(fields_enabled=True, charge=[-1.0])
-    with pytest.raises(NotImplementedError):
-        make_solver(spec)
+def test_polar_refuses_odd_angle_count_at_q1_mirror():
     spec = copy.deepcopy(C.CASES[NAME])
     spec['N_p2'] = 7
     with pytest.raises(Exception) as e:
