@@ -320,8 +320,20 @@ def slab_result(args, rank, world, local_rank, spec):
     dom, bc, params, ini = config_modules(spec, args.precision)
     slab = SlabSolver(physical_system(dom, bc, params, ini, adv, col.BGK, mom))
     peer = world > 1 and dist.is_initialized()
+    peer_error = None
     if peer:
-        slab.enable_peer_halos()
+        # every rank takes the same halo path: if mapping a neighbour's
+        # buffers fails on any rank, all fall back to the send/recv exchange
+        ok = 1
+        try:
+            slab.enable_peer_halos()
+        except Exception as exc:                       # noqa: BLE001
+            ok, peer_error = 0, '%s: %s' % (type(exc).__name__, str(exc)[:200])
+        flag = torch.tensor([ok], dtype=torch.int32, device='cuda')
+        dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+        if int(flag.item()) == 0:
+            slab.disable_peer_halos()
+            peer = False
     dt = spec['dt']
     for _ in range(args.warmup):
         slab.strang_timestep(dt)
@@ -347,7 +359,9 @@ def slab_result(args, rank, world, local_rank, spec):
     return {'value': cells / (ms * 1e-3), 'ms_per_step': ms, 'scaling': 'strong',
             'slabs': world, 'rows_per_slab': spec['N_q2'] // world,
             'halos': 'peer stores over NVLink' if peer else
-                     'single slab (wraps onto itself), exchange overlapped with the inner tiles',
+                     ('send/recv exchange, overlapped with the inner tiles' if world > 1 else
+                      'single slab (wraps onto itself), exchange overlapped with the inner tiles'),
+            'peer_halo_error': peer_error,
             'gpu_launches_per_rank': launches,
             'paired_launches_per_rank': paired}
 
