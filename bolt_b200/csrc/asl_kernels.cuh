@@ -42,8 +42,11 @@ template <typename T> struct AslRows {
 };
 
 // the q2 rows [R jb, R jb + R), species and p-cell of thread e (see
-// asl_q_kernel); true if a written value is not finite
-template <typename T>
+// asl_q_kernel); true if a written value is not finite.  I: the type of the
+// element offsets from the thread's own (species, p) base -- int when the
+// ghosted array holds fewer than 2^31 elements (fewer registers and no 64-bit
+// multiplies in the walk), else long long
+template <typename T, typename I>
 __device__ __forceinline__ bool asl_q_rows(const AslArgs& a, long long e) {
     constexpr int R = AslRows<T>::R, NS = R + 3, G = AslRows<T>::G;
     bool bad = false;
@@ -85,16 +88,16 @@ __device__ __forceinline__ bool asl_q_rows(const AslArgs& a, long long e) {
     bool offy[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) offy[k] = !(y + k >= 0.0 && y + k <= double(Nq2g - 1));
-    const long long rowstride = (long long)a.Ns * a.Np;
-    const long long colstride = rowstride * Nq1g;
+    const I rowstride = I(a.Ns) * I(a.Np);
+    const I colstride = rowstride * I(Nq1g);
     const T* f = static_cast<const T*>(a.f) + (long long)s * a.Np + p;
     // source rows j0 - 1 .. j0 + R + 1, clamped to the ghosted array
-    const T* rows[NS];
+    I rows[NS];
 #pragma unroll
-    for (int b = 0; b < NS; ++b) rows[b] = f + min(max(j0 - 1 + b, 0), Nq2g - 1) * colstride;
-    T* __restrict__ out = static_cast<T*>(a.out) + (jb + Ng) * colstride +
+    for (int b = 0; b < NS; ++b) rows[b] = I(min(max(j0 - 1 + b, 0), Nq2g - 1)) * colstride;
+    T* __restrict__ out = static_cast<T*>(a.out) + (long long)(jb + Ng) * colstride +
                           (long long)Ng * rowstride + (long long)s * a.Np + p;
-    auto col = [&](int b, int c) { return rows[b][min(max(c, 0), Nq1g - 1) * rowstride]; };
+    auto col = [&](int b, int c) { return f[rows[b] + I(min(max(c, 0), Nq1g - 1)) * rowstride]; };
     // win[b][c]: source row b, column clamp(i00 + i - 1 + c) of cell i
     T win[NS][4];
 #pragma unroll
@@ -128,7 +131,7 @@ __device__ __forceinline__ bool asl_q_rows(const AslArgs& a, long long e) {
 #pragma unroll
                 for (int b = 0; b < 4; ++b) acc = acc + wy[b] * xs[k + b];
                 const T v = (offx || offy[k]) ? T(0) : acc;
-                out[(long long)k * colstride + (long long)i * rowstride] = v;
+                out[I(k) * colstride + I(i) * rowstride] = v;
                 bad |= !isfinite(v);
             }
         }
@@ -163,12 +166,12 @@ __device__ __forceinline__ bool asl_q_rows(const AslArgs& a, long long e) {
 // cubic, then per output row the q2 cubic, the order of a tensor-product
 // evaluation row by row.  A written value that is not finite sets *flag (one
 // atomic per warp that saw one).
-template <typename T>
+template <typename T, typename I>
 __global__ void __launch_bounds__(256) asl_q_kernel(const AslArgs a, int* flag) {
     constexpr int R = AslRows<T>::R;
     const long long nthr = (long long)((a.Nq2 + R - 1) / R) * a.Ns * a.Np;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool bad = e < nthr && asl_q_rows<T>(a, e);
+    const bool bad = e < nthr && asl_q_rows<T, I>(a, e);
     if (flag && __any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 

@@ -107,7 +107,12 @@ cudaError_t BOLT_CAT(launch_asl_q_, BOLT_SUFFIX)(const AslArgs& a, int* flag, cu
     constexpr int R = AslRows<BOLT_T>::R;
     const long long total = (long long)((a.Nq2 + R - 1) / R) * a.Ns * a.Np;   // threads
     if (total == 0) return cudaSuccess;
-    asl_q_kernel<BOLT_T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a, flag);
+    // 32-bit element offsets when the ghosted array has fewer than 2^31 elements
+    const long long elems = (long long)(a.Nq2 + 2 * a.Ng) * (a.Nq1 + 2 * a.Ng) * a.Ns * a.Np;
+    if (elems < (1LL << 31))
+        asl_q_kernel<BOLT_T, int><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a, flag);
+    else
+        asl_q_kernel<BOLT_T, long long><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a, flag);
     return cudaGetLastError();
 }
 
