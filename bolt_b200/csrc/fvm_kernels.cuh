@@ -890,31 +890,35 @@ moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int
 // halo refresh: communicate_f (periodic wrap; ghosted halos are zero), then
 // apply_bcs_f per axis (boundaries.py:415-577): the mirror image
 // (boundaries.py:226-413, cartesian or polar2D p-grid) and/or the Dirichlet inflow
-// select (:147-225).  One thread per (ghost cell, s, p); every value is read
-// from an interior cell, so one pass gives the reference's sequential
-// left, right, bottom, top result everywhere except in the corner cells
-// (ghost in both q1 and q2) of mixed mirror / Dirichlet axes, which no
-// interior update reads (the q1 and q2 stencils are separate).
+// select (:147-225).  Every value is read from an interior cell, so one pass
+// gives the reference's sequential left, right, bottom, top result everywhere
+// except in the corner cells (ghost in both q1 and q2) of mixed mirror /
+// Dirichlet axes, which no interior update reads (the q1 and q2 stencils are
+// separate).
+// One CTA per ghost cell (grid-stride over the cells): the cell, its source
+// cell and its kind are worked out once; the cell's (species, p) block is
+// contiguous, so a plain image (periodic, or zero) is a copy of the source
+// cell's block in 16-byte vectors, and only cells whose values depend on p
+// (a mirror's velocity reflection, a Dirichlet inflow select, a shearing-box
+// resample) go element by element.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const T* dt,
-                             int Nq1, int Nq2, int Ng, int Ns, int Np, int Np1, int Np2,
-                             int per1, int per2, int dir1, int dir2, int mir1, int mir2,
-                             int ext1, int ext2, SpeciesGrid sg, GhostShear sh,
-                             long long nghost_cells) {
+__global__ void __launch_bounds__(256)
+ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const T* dt,
+             int Nq1, int Nq2, int Ng, int Ns, int Np, int Np1, int Np2,
+             int per1, int per2, int dir1, int dir2, int mir1, int mir2,
+             int ext1, int ext2, SpeciesGrid sg, GhostShear sh,
+             long long nghost_cells) {
     const int Nq1g = Nq1 + 2 * Ng;
-    const long long rowstride = (long long)Ns * Np;
+    const int rowlen = Ns * Np;                            // one q-cell's values
+    const long long rowstride = rowlen;
     const long long colstride = rowstride * Nq1g;
-    const long long total = nghost_cells * rowstride;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long gc = t / rowstride;
-        const int sp = int(t % rowstride);
-        const int s = sp / Np, p = sp % Np;
+    const long long nrow = (long long)Ng * Nq1g;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (long long gc = blockIdx.x; gc < nghost_cells; gc += gridDim.x) {
         // enumerate ghost cells: rows [0,Ng) and [Nq2+Ng, Nq2g) full width, then
         // the left/right ghost columns of the interior rows
         int g1, g2;
-        const long long nrow = (long long)Ng * Nq1g;
         if (gc < 2 * nrow) {
             const int r = int(gc / Nq1g), c = int(gc % Nq1g);
             g2 = r < Ng ? r : Nq2 + r;          // r in [Ng, 2Ng) -> Nq2+Ng .. Nq2+2Ng-1
@@ -929,6 +933,8 @@ __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const 
         const bool in1 = i >= 0 && i < Nq1, in2 = j >= 0 && j < Nq2;
         // ghost rows / columns of an external axis belong to the caller
         if ((ext1 && !in1) || (ext2 && !in2)) continue;
+        const long long g = (long long)g2 * colstride + (long long)g1 * rowstride;
+        T* dst = f + g;
         // a shearing-box strip (every cell of the N_g ghost columns or rows,
         // corners included): the periodic image resampled along the other axis
         if ((sh.axis == 1 && !in1) || (sh.axis == 2 && !in2)) {
@@ -945,72 +951,97 @@ __global__ void ghost_kernel(T* f, const T* dl, const T* dr, const T* db, const 
             const int jb = (int)floor(x);
             const double t = x - jb;
             const int fixed = sh.axis == 1 ? ((i % Nq1) + Nq1) % Nq1 : ((j % Nq2) + Nq2) % Nq2;
-            double pv[4];
+            const T* src[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int m = (((jb - 1 + k - Ng) % N) + N) % N;   // periodic extension
                 const int ci = sh.axis == 1 ? fixed : m, cj = sh.axis == 1 ? m : fixed;
-                pv[k] = double(f[(long long)(cj + Ng) * colstride + (long long)(ci + Ng) * rowstride +
-                                 (long long)s * Np + p]);
+                src[k] = f + (long long)(cj + Ng) * colstride + (long long)(ci + Ng) * rowstride;
             }
-            // Catmull-Rom cubic between pv[1] and pv[2] (tangents (pv[k+1]-pv[k-1])/2)
-            const double v = pv[1] + 0.5 * t * ((pv[2] - pv[0]) +
-                             t * ((2.0 * pv[0] - 5.0 * pv[1] + 4.0 * pv[2] - pv[3]) +
-                                  t * (3.0 * (pv[1] - pv[2]) + pv[3] - pv[0])));
-            f[(long long)g2 * colstride + (long long)g1 * rowstride + sp] = T(v);
+            for (int sp = tid; sp < rowlen; sp += nt) {
+                double pv[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) pv[k] = double(src[k][sp]);
+                // Catmull-Rom cubic between pv[1] and pv[2] (tangents (pv[k+1]-pv[k-1])/2)
+                const double v = pv[1] + 0.5 * t * ((pv[2] - pv[0]) +
+                                 t * ((2.0 * pv[0] - 5.0 * pv[1] + 4.0 * pv[2] - pv[3]) +
+                                      t * (3.0 * (pv[1] - pv[2]) + pv[3] - pv[0])));
+                dst[sp] = T(v);
+            }
             continue;
         }
-        const int i1 = p % Np1, i2 = (p / Np1) % Np2;
-        // source cell and p index: periodic wrap, or the mirror image across
-        // the edge (ghost i < 0 <- interior -1-i, i >= N <- 2N-1-i) with the
-        // velocity reflected.  Cartesian grid (boundaries.py:226-301): the
-        // normal velocity index reversed, p1 at q1 edges, p2 at q2 edges.
-        // Polar2D grid (boundaries.py:313-413, p2 the angle theta): at q2
-        // edges theta -> -theta, the p2 index reversed; at q1 edges
+        // source cell: periodic wrap, or the mirror image across the edge
+        // (ghost i < 0 <- interior -1-i, i >= N <- 2N-1-i); none (zero) for a
+        // non-periodic, non-mirror axis
+        int si = i, sj = j;
+        bool have = true;
+        const bool m1 = !in1 && !per1 && mir1, m2 = !in2 && !per2 && mir2;
+        if (!in2) {
+            if (per2) sj = ((j % Nq2) + Nq2) % Nq2;
+            else if (mir2) sj = j < 0 ? -1 - j : 2 * Nq2 - 1 - j;
+            else have = false;
+        }
+        if (!in1) {
+            if (per1) si = ((i % Nq1) + Nq1) % Nq1;
+            else if (mir1) si = i < 0 ? -1 - i : 2 * Nq1 - 1 - i;
+            else have = false;
+        }
+        const bool d1 = dir1 && !in1, d2 = dir2 && !in2;
+        const T* src = f + (long long)(sj + Ng) * colstride + (long long)(si + Ng) * rowstride;
+        if (!m1 && !m2 && !d1 && !d2) {
+            // the same (species, p) block as the source cell, or zeros
+            constexpr int VW = 16 / (int)sizeof(T);
+            if ((rowlen % VW) == 0 && (reinterpret_cast<uintptr_t>(f) & 15) == 0) {
+                typedef typename Vec16<T>::V V;
+                const V* s4 = reinterpret_cast<const V*>(src);
+                V* d4 = reinterpret_cast<V*>(dst);
+                const int nv = rowlen / VW;
+                if (have) {
+                    for (int k = tid; k < nv; k += nt) d4[k] = s4[k];
+                } else {
+                    V z;
+                    memset(&z, 0, sizeof(z));
+                    for (int k = tid; k < nv; k += nt) d4[k] = z;
+                }
+            } else {
+                for (int sp = tid; sp < rowlen; sp += nt) dst[sp] = have ? src[sp] : T(0);
+            }
+            continue;
+        }
+        // element by element: the velocity reflected across a mirror edge.
+        // Cartesian grid (boundaries.py:226-301): the normal velocity index
+        // reversed, p1 at q1 edges, p2 at q2 edges.  Polar2D grid
+        // (boundaries.py:313-413, p2 the angle theta): at q2 edges
+        // theta -> -theta, the p2 index reversed; at q1 edges
         // theta -> pi - theta, each half of the p2 index range reversed on its
         // own.  The reference applies the q1 edges before the q2 edges, so a
         // corner ghost takes the q1 map of the q2 map of its own p2 index.
-        int si = i, sj = j, ps = p;
-        int k2 = i2;                                   // source p2 index
-        bool have = true;
-        if (!in2) {
-            if (per2) {
-                sj = ((j % Nq2) + Nq2) % Nq2;
-            } else if (mir2) {
-                sj = j < 0 ? -1 - j : 2 * Nq2 - 1 - j;
-                k2 = Np2 - 1 - k2;
-            } else {
-                have = false;
-            }
-        }
-        if (!in1) {
-            if (per1) {
-                si = ((i % Nq1) + Nq1) % Nq1;
-            } else if (mir1) {
-                si = i < 0 ? -1 - i : 2 * Nq1 - 1 - i;
+        // Then the Dirichlet inflow values where the velocity normal to the
+        // edge points into the domain.
+        for (int sp = tid; sp < rowlen; sp += nt) {
+            const int p = sp % Np;
+            const int i1 = p % Np1, i2 = (p / Np1) % Np2;
+            int ps = sp, k2 = i2;                          // source p2 index
+            if (m2) k2 = Np2 - 1 - k2;
+            if (m1) {
                 if (sg.polar2d) {
                     const int H = Np2 / 2;
                     k2 = k2 < H ? H - 1 - k2 : Np2 - 1 + H - k2;
                 } else {
                     ps += Np1 - 1 - 2 * i1;
                 }
-            } else {
-                have = false;
             }
+            ps += Np1 * (k2 - i2);
+            T v = have ? src[ps] : T(0);
+            const int s = sp / Np;
+            const double v1 = sg.p1_start[s] + (0.5 + i1) * sg.dp1[s];
+            const double v2 = sg.p2_start[s] + (0.5 + i2) * sg.dp2[s];
+            if (d1 && i < 0 && v1 > 0) v = dl[g + sp];
+            if (d1 && i >= Nq1 && v1 < 0) v = dr[g + sp];
+            if (d2 && j < 0 && v2 > 0) v = db[g + sp];
+            if (d2 && j >= Nq2 && v2 < 0) v = dt[g + sp];
+            dst[sp] = v;
         }
-        ps += Np1 * (k2 - i2);
-        T v = T(0);
-        if (have)
-            v = f[(long long)(sj + Ng) * colstride + (long long)(si + Ng) * rowstride +
-                  (long long)s * Np + ps];
-        const long long g = (long long)g2 * colstride + (long long)g1 * rowstride + sp;
-        const double v1 = sg.p1_start[s] + (0.5 + i1) * sg.dp1[s];
-        const double v2 = sg.p2_start[s] + (0.5 + i2) * sg.dp2[s];
-        if (dir1 && i < 0 && v1 > 0) v = dl[g];
-        if (dir1 && i >= Nq1 && v1 < 0) v = dr[g];
-        if (dir2 && j < 0 && v2 > 0) v = db[g];
-        if (dir2 && j >= Nq2 && v2 < 0) v = dt[g];
-        f[g] = v;
     }
 }
 

@@ -93,10 +93,12 @@ cudaError_t BOLT_CAT(launch_ghost_, BOLT_SUFFIX)(void* f, const void* dl, const 
     const long long Nq1g = Nq1 + 2 * Ng;
     const long long ncells = 2LL * Ng * Nq1g + 2LL * Ng * Nq2;
     if (ncells == 0) return cudaSuccess;
-    const long long total = ncells * Ns * Np;
-    long long blocks = (total + 255) / 256;
-    if (blocks > 148 * 32) blocks = 148 * 32;
-    ghost_kernel<BOLT_T><<<(unsigned)blocks, 256, 0, st>>>(
+    // one CTA per ghost cell (grid-stride beyond 16 CTAs per SM), its threads
+    // over the cell's (species, p) block
+    const long long rowlen = (long long)Ns * Np;
+    const long long blocks = ncells < 148 * 16 ? ncells : 148 * 16;
+    const int threads = rowlen >= 2048 ? 256 : (rowlen >= 512 ? 128 : 64);
+    ghost_kernel<BOLT_T><<<(unsigned)blocks, threads, 0, st>>>(
         static_cast<BOLT_T*>(f), static_cast<const BOLT_T*>(dl), static_cast<const BOLT_T*>(dr),
         static_cast<const BOLT_T*>(db), static_cast<const BOLT_T*>(dt), Nq1, Nq2, Ng, Ns, Np, Np1,
         Np2, per1, per2, dir1, dir2, mir1, mir2, ext1, ext2, sg, sh, ncells);
