@@ -236,6 +236,8 @@ __global__ void __launch_bounds__(256, 4) asl_src_kernel(const QStageArgs a, con
         // two vectors of input and base per round, loaded before either is
         // written (out may be base: every element is read, then written, by
         // one thread)
+        // the vectors cv = tid, tid + 256, ... in that order: p-cell cv * VN
+        PCellWalk pw(tid * VN, 256 * VN, Np1, Np2);
         for (int c0 = tid; c0 < nv; c0 += 2 * 256) {
             V ci[2], cb[2];
 #pragma unroll
@@ -249,8 +251,8 @@ __global__ void __launch_bounds__(256, 4) asl_src_kernel(const QStageArgs a, con
             for (int u = 0; u < 2; ++u) {
                 const int cv = c0 + u * 256;
                 if (cv >= nv) break;
-                const int p = cv * VN;
-                const int ip1 = p % Np1, ip2 = (p / Np1) % Np2, ip3 = p / (Np1 * Np2);
+                const int ip1 = pw.i1, ip2 = pw.i2, ip3 = pw.i3;
+                pw.advance();
                 double di[VN], db[VN], ov[VN];
                 if (mode != 1) {
                     VT::get(ci[u], di);

@@ -825,6 +825,36 @@ __device__ __forceinline__ void add_moment_run(const double (&o)[n], double V1, 
     acc[4] = fma(0.5, fma(e0, S0, fma(2.0 * V1 * dp1, S1, (dp1 * dp1) * S2)), acc[4]);
 }
 
+// (i1, i2, i3) of a p-cell index that a thread advances by a fixed stride,
+// kept without divisions: the stride is split once into its p1 remainder and
+// its p2 / p3 row steps, and each advance carries from p1 into p2 and from p2
+// into p3 (each part stays below twice its range, so one subtraction does)
+struct PCellWalk {
+    int i1, i2, i3;        // current p-cell
+    int d1, d2, d3;        // the stride as (p1, p2, p3) steps
+    int Np1, Np2;
+    __device__ __forceinline__ PCellWalk(int p, int stride, int np1, int np2)
+        : Np1(np1), Np2(np2) {
+        i1 = p % np1;
+        const int r = p / np1;
+        i2 = r % np2;
+        i3 = r / np2;
+        d1 = stride % np1;
+        const int rs = stride / np1;
+        d2 = rs % np2;
+        d3 = rs / np2;
+    }
+    __device__ __forceinline__ void advance() {
+        i1 += d1;
+        int c = 0;
+        if (i1 >= Np1) { i1 -= Np1; c = 1; }
+        i2 += d2 + c;
+        c = 0;
+        if (i2 >= Np2) { i2 -= Np2; c = 1; }
+        i3 += d3 + c;
+    }
+};
+
 // The five BGK moments of the interior cells as one "split" of partial sums
 // ([1][5][Ns][Nq2][Nq1], sums without the measure factor).  One CTA per q-cell
 // streams its p-block in 16-byte vectors, four in flight per thread (N_p1 a
@@ -847,6 +877,8 @@ moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int
         const int nv = Np / VN;
         const double p1s = sg.p1_start[s], p2s = sg.p2_start[s], p3s = sg.p3_start[s];
         const double dp1 = sg.dp1[s], dp2 = sg.dp2[s], dp3 = sg.dp3[s];
+        // the vectors c = tid, tid + 256, ... in that order: p-cell c * VN
+        PCellWalk w(tid * VN, 256 * VN, Np1, Np2);
         for (int c0 = tid; c0 < nv; c0 += 4 * 256) {
             typename VT::V v[4];
 #pragma unroll
@@ -856,12 +888,11 @@ moments5_kernel(const T* f, double* part, int Ns, int Np1, int Np2, int Np3, int
             for (int u = 0; u < 4; ++u) {
                 const int c = c0 + u * 256;
                 if (c >= nv) break;
-                const int p = c * VN;
-                const int i1 = p % Np1, i2 = (p / Np1) % Np2, i3 = p / (Np1 * Np2);
                 double o[VN];
                 VT::get(v[u], o);
-                add_moment_run<VN>(o, p1s + (0.5 + i1) * dp1, dp1, p2s + (0.5 + i2) * dp2,
-                                   p3s + (0.5 + i3) * dp3, acc);
+                add_moment_run<VN>(o, p1s + (0.5 + w.i1) * dp1, dp1, p2s + (0.5 + w.i2) * dp2,
+                                   p3s + (0.5 + w.i3) * dp3, acc);
+                w.advance();
             }
         }
     } else {
