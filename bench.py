@@ -940,18 +940,20 @@ def asl_result(args, local_rank, steps=10):
     splitting of the bicubic q-advection and the RK2 BGK source) on the
     headline grid, 2D3V 128^2 x 24^3 (Maxwellian, n = 1 + 0.05 cos cos, BGK
     tau = 0.05, dt = 1e-3), FP32 and FP64 f: cell-updates/s over ``steps``
-    timed steps (CUDA events) after 3 warm-up steps."""
+    timed steps (CUDA events) after 3 warm-up steps.  --small: 64^2 x 24^3
+    (for profiler captures)."""
     import torch
     c2_spec()                            # puts the case builders on sys.path
     import cases as C
     from _modules import make_solver as make_case_solver
     torch.cuda.set_device(local_rank)
-    spec = C.make(N_q1=128, N_q2=128, N_p1=24, N_p2=24, N_p3=24,
+    n = 64 if getattr(args, 'small', False) else 128
+    spec = C.make(N_q1=n, N_q2=n, N_p1=24, N_p2=24, N_p3=24,
                   p1_start=[-6.0], p1_end=[6.0], p2_start=[-6.0], p2_end=[6.0],
                   p3_start=[-6.0], p3_end=[6.0], mass=[1.0], charge=[0.0], p_dim=3,
                   solver_q='ASL', splitting='strang', tau=0.05, dt=1e-3,
                   init=dict(amp=0.05, k1=1, k2=1))
-    cells = 128 * 128 * 24 ** 3
+    cells = n * n * 24 ** 3
     out = {'steps': steps, 'splitting': 'strang', 'cells': cells}
     for prec in ('fp32', 'fp64'):
         nls = make_case_solver(spec, prec)

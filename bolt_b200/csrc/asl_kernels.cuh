@@ -213,6 +213,18 @@ __global__ void __launch_bounds__(256, 4) asl_src_kernel(const QStageArgs a, con
     const V* vi = reinterpret_cast<const V*>(fi);
     const V* vb = reinterpret_cast<const V*>(fb);
     const int nv = a.Np / VN;
+    // the first round's input and base vectors are loaded before the
+    // Maxwellian set-up, so that their latency overlaps it
+    V ci[2], cb[2];
+    if (vec && mode != 1) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (tid + u * 256 < nv) {
+                ci[u] = vi[tid + u * 256];
+                cb[u] = fb == fi ? ci[u] : vb[tid + u * 256];
+            }
+        }
+    }
     if (tid == 0) bgk_cell_params(a, s, ii, jj, qq);
     for (int q = tid; q < ntab; q += blockDim.x) {
         if (q < Np1) vg[q] = a.sg.p1_start[s] + (0.5 + q) * a.sg.dp1[s];
@@ -239,10 +251,9 @@ __global__ void __launch_bounds__(256, 4) asl_src_kernel(const QStageArgs a, con
         // the vectors cv = tid, tid + 256, ... in that order: p-cell cv * VN
         PCellWalk pw(tid * VN, 256 * VN, Np1, Np2);
         for (int c0 = tid; c0 < nv; c0 += 2 * 256) {
-            V ci[2], cb[2];
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
-                if (c0 + u * 256 < nv && mode != 1) {
+                if (c0 != tid && c0 + u * 256 < nv && mode != 1) {
                     ci[u] = vi[c0 + u * 256];
                     cb[u] = fb == fi ? ci[u] : vb[c0 + u * 256];
                 }
