@@ -98,6 +98,74 @@ __device__ __forceinline__ bool asl_q_rows(const AslArgs& a, long long e) {
     T* __restrict__ out = static_cast<T*>(a.out) + (long long)(jb + Ng) * colstride +
                           (long long)Ng * rowstride + (long long)s * a.Np + p;
     auto col = [&](int b, int c) { return f[rows[b] + I(min(max(c, 0), Nq1g - 1)) * rowstride]; };
+    if constexpr (sizeof(T) == 4 && R == 2) {
+        // FP32: the q1 cubics of source rows (0, 1) and (2, 3) as f32x2 pairs
+        // (two FMAs per instruction, each lane the same operations in the
+        // same order as the scalar form below, so the values are identical);
+        // row 4 scalar
+        float2 w01[4], w23[4];
+        float w4[4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            w01[c + 1] = make_float2(col(0, i00 - 1 + c), col(1, i00 - 1 + c));
+            w23[c + 1] = make_float2(col(2, i00 - 1 + c), col(3, i00 - 1 + c));
+            w4[c + 1] = col(4, i00 - 1 + c);
+        }
+        auto cell2 = [&](int i, float2 n01, float2 n23, float n4) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                w01[c] = w01[c + 1];
+                w23[c] = w23[c + 1];
+                w4[c] = w4[c + 1];
+            }
+            w01[3] = n01;
+            w23[3] = n23;
+            w4[3] = n4;
+            float2 x01 = make_float2(0.0f, 0.0f), x23 = make_float2(0.0f, 0.0f);
+            float x4 = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float2 wc = make_float2(wx[c], wx[c]);
+                x01 = __ffma2_rn(wc, w01[c], x01);
+                x23 = __ffma2_rn(wc, w23[c], x23);
+                x4 = x4 + wx[c] * w4[c];
+            }
+            const float xs[5] = {x01.x, x01.y, x23.x, x23.y, x4};
+            const double x = x0 + i;
+            const bool offx = !(x >= 0.0 && x <= double(Nq1g - 1));
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                if (k < nr) {
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) acc = acc + wy[b] * xs[k + b];
+                    const float v = (offx || offy[k]) ? 0.0f : acc;
+                    out[I(k) * colstride + I(i) * rowstride] = v;
+                    bad |= !isfinite(v);
+                }
+            }
+        };
+        int i = 0;
+        for (; i + G <= Nq1; i += G) {
+            float2 n01[G], n23[G];
+            float n4[G];
+#pragma unroll
+            for (int u = 0; u < G; ++u) {
+                const int c = i00 + i + u + 2;
+                n01[u] = make_float2(col(0, c), col(1, c));
+                n23[u] = make_float2(col(2, c), col(3, c));
+                n4[u] = col(4, c);
+            }
+#pragma unroll
+            for (int u = 0; u < G; ++u) cell2(i + u, n01[u], n23[u], n4[u]);
+        }
+        for (; i < Nq1; ++i) {
+            const int c = i00 + i + 2;
+            cell2(i, make_float2(col(0, c), col(1, c)), make_float2(col(2, c), col(3, c)),
+                  col(4, c));
+        }
+        return bad;
+    }
     // win[b][c]: source row b, column clamp(i00 + i - 1 + c) of cell i
     T win[NS][4];
 #pragma unroll

@@ -46,6 +46,8 @@ def test_strerror_and_null_args():
     assert lib.bolt_asl_source_to(None, None, None, None, 0.0, 0, None) == N.BOLT_ERR_ARG
     ptr = ctypes.c_void_p()
     assert lib.bolt_work_buffer(None, 0, ctypes.byref(ptr)) == N.BOLT_ERR_ARG
+    # the p-space grid setter: a context is required
+    assert lib.bolt_set_p_space_grid(None, N.PGRID['polar2D'], 1.0) == N.BOLT_ERR_ARG
 
 
 def test_ctx_create_rejects_bad_grids_without_gpu():
